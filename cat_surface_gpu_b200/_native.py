@@ -1,0 +1,119 @@
+"""ctypes binding of ``libcatsurf_b200.so`` (the C ABI in include/catsurf_b200.h).
+
+The product path has no CPU fallback: if the library is missing or a CUDA
+device is absent, calls raise ``RuntimeError`` / ``DeviceUnavailable``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_double, c_int, c_size_t, c_void_p
+from pathlib import Path
+import threading
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "libcatsurf_b200.so"
+
+CSG_OK = 0
+CSG_ERR_ARG = -1
+CSG_ERR_CUDA = -2
+CSG_ERR_TIMEOUT = -3
+CSG_ERR_LAUNCH = -4
+CSG_ERR_TOPOLOGY = -5
+CSG_ERR_UNSUPPORTED = -6
+CSG_ERR_COVERAGE = -7
+
+ARITH = {"cat": 0, "fp32": 1, "fp64": 2}
+
+_P = c_void_p
+_I = c_int
+
+# name -> (restype, argtypes).  Kept in the order of include/catsurf_b200.h.
+SIGNATURES: dict[str, tuple[object, list[object]]] = {
+    "csg_last_error": (ctypes.c_char_p, []),
+    "csg_abi_version": (_I, []),
+    "csg_mesh_incidence": (_I, [_I, _P, _I, _P, _P]),
+    "csg_mesh_neighbours": (_I, [_I, _P, _I, _P, _P, _I]),
+    "csg_dependency_levels": (_I, [_I, _P, _P, _P]),
+    "csg_greedy_colours": (_I, [_I, _P, _P, _P]),
+    "csg_areal_plan_build": (_I, [_I, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "csg_areal_scratch_bytes": (c_size_t, [_I, _I]),
+    "csg_areal_sweeps": (
+        _I,
+        [_P, _I, _P, _P, _P, _P, _P, _I, _I, _I, _I, c_double, _I, _P, c_size_t, _I, _I, _I, c_double, _P],
+    ),
+    "csg_selftest_barrier_timeout": (_I, [_P, c_size_t, c_double, _P]),
+    "csg_read_status": (_I, [_P, _P, _P, _P]),
+}
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_vertices", ctypes.c_int32),
+        ("n_faces", ctypes.c_int32),
+        ("n_levels", ctypes.c_int32),
+        ("level_stride", ctypes.c_int32),
+        ("max_degree", ctypes.c_int32),
+        ("n_slots", ctypes.c_int32),
+    ]
+
+
+_lock = threading.Lock()
+_lib: ctypes.CDLL | None = None
+
+
+def library() -> ctypes.CDLL:
+    """Load the native library once; raise if it has not been built."""
+
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not LIBRARY_PATH.exists():
+                raise RuntimeError(
+                    f"{LIBRARY_PATH.name} is not built; run `python -m cat_surface_gpu_b200.build` "
+                    "(there is no CPU fallback)"
+                )
+            lib = ctypes.CDLL(str(LIBRARY_PATH))
+            for name, (restype, argtypes) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = restype
+                fn.argtypes = argtypes
+            _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    message = library().csg_last_error()
+    return message.decode("utf-8", "replace") if message else ""
+
+
+def check(status: int, what: str) -> int:
+    """Raise on a negative status: ValueError for argument errors, RuntimeError otherwise."""
+
+    if status >= 0:
+        return status
+    message = f"{what}: {last_error()} (status {status})"
+    if status in (CSG_ERR_ARG, CSG_ERR_TOPOLOGY):
+        raise ValueError(message)
+    raise RuntimeError(message)
+
+
+def ptr(tensor) -> int:
+    """Raw address of a torch tensor or numpy array (None -> 0)."""
+
+    if tensor is None:
+        return 0
+    if hasattr(tensor, "data_ptr"):
+        return int(tensor.data_ptr())
+    return int(tensor.ctypes.data)
+
+
+def stream_handle(stream=None) -> int:
+    """cudaStream_t of the given (or current) torch CUDA stream."""
+
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return int(stream.cuda_stream)

@@ -1,0 +1,447 @@
+// Surf2Sphere ordered area-smoothing sweeps as ONE persistent cooperative
+// kernel for sm_100a.
+//
+// Semantics follow the reference's ordered Gauss-Seidel sweeps
+// (src/cat_surface_gpu/surf2sphere.py:35-280 and 1039-1092): every vertex,
+// in index order, moves to the area-weighted centroid of its incident faces
+// (faces in ascending id, areas clamped to [0, 1]); after sweep s with
+// s % project_every == 0 all points are projected to `radius`.
+//
+// Schedule: instead of one launch per dependency level per sweep (the
+// reference launches sum(levels) x 4,999 kernels), vertex v of sweep s runs at
+// wavefront step s * stride + level(v) inside one launch.  With
+// stride = 1 + max_{edges v<w} (level(w) - level(v)) every read sees exactly
+// the value the sequential order would see (lower neighbours: this sweep;
+// higher neighbours: previous sweep), so the in-place buffer needs no copy.
+// Steps are separated by a bounded grid barrier; projections drain the
+// wavefront (one barrier before and after).
+//
+// Data layout: positions live in a float4 (or double4) working copy in HBM
+// (L2-resident for cortical meshes), read with 16-byte ld.global.cg loads so
+// no stale L1 line can be observed across steps.  Each vertex's incident
+// faces are stored CSR-contiguous as int4 {v0, v1, v2, face}: a group of G
+// lanes reads G consecutive slots (coalesced), computes one face per lane and
+// accumulates the per-face terms in slot order through warp shuffles, which
+// keeps the reference's sequential accumulation order exactly.
+//
+// Arithmetic: CSG_ARITH_CAT reproduces the reference's mixed precision
+// (float32 edge/cross/sum-of-squares, float64 sqrt/centre/accumulate/divide,
+// float32 store) with one IEEE rounding per operation (explicit _rn
+// intrinsics, no contraction), so results are bit-identical to the CPU
+// restatement compiled with -ffp-contract=off.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "errors.h"
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct ArealParams {
+    void* points;  // caller's [n,3] float32 or float64
+    void* work;    // float4[n] or double4[n] working copy (scratch)
+    csg::Control* ctl;
+    const int4* slot_tri;
+    const int* slot_off;
+    const int* order;
+    const int* level_begin;
+    const int* level_end;
+    int n;
+    int n_levels;
+    int stride;
+    int iterations;
+    int project_every;
+    double radius;
+    unsigned long long timeout_ns;
+};
+
+struct alignas(32) D4 {
+    double x, y, z, w;
+};
+
+template <int MODE>
+struct Traits;
+
+// CAT mixed: float32 storage, float64 accumulation.
+template <>
+struct Traits<CSG_ARITH_CAT> {
+    using Store = float4;
+    using Acc = double;
+    struct P3 {
+        float x, y, z;
+    };
+    static __device__ __forceinline__ P3 load(const void* w, int v) {
+        float4 q = __ldcg(static_cast<const float4*>(w) + v);
+        return {q.x, q.y, q.z};
+    }
+    static __device__ __forceinline__ void face(const P3& a, const P3& b, const P3& c, double& area, double& mx,
+                                                double& my, double& mz) {
+        float e0x = __fsub_rn(b.x, a.x), e0y = __fsub_rn(b.y, a.y), e0z = __fsub_rn(b.z, a.z);
+        float e1x = __fsub_rn(c.x, a.x), e1y = __fsub_rn(c.y, a.y), e1z = __fsub_rn(c.z, a.z);
+        float cx = __fsub_rn(__fmul_rn(e0y, e1z), __fmul_rn(e0z, e1y));
+        float cy = __fsub_rn(__fmul_rn(e0z, e1x), __fmul_rn(e0x, e1z));
+        float cz = __fsub_rn(__fmul_rn(e0x, e1y), __fmul_rn(e0y, e1x));
+        float sq = __fadd_rn(__fadd_rn(__fmul_rn(cx, cx), __fmul_rn(cy, cy)), __fmul_rn(cz, cz));
+        area = __dmul_rn(0.5, __dsqrt_rn(static_cast<double>(sq)));
+        mx = __ddiv_rn(__dadd_rn(__dadd_rn((double)a.x, (double)b.x), (double)c.x), 3.0);
+        my = __ddiv_rn(__dadd_rn(__dadd_rn((double)a.y, (double)b.y), (double)c.y), 3.0);
+        mz = __ddiv_rn(__dadd_rn(__dadd_rn((double)a.z, (double)b.z), (double)c.z), 3.0);
+        area = area > 0.0 ? area : 0.0;
+        area = area < 1.0 ? area : 1.0;
+    }
+    static __device__ __forceinline__ void store(void* w, int v, double total, double wx, double wy, double wz) {
+        double safe = total > 1.0e-20 ? total : 1.0e-20;
+        float4 q = make_float4(__double2float_rn(__ddiv_rn(wx, safe)), __double2float_rn(__ddiv_rn(wy, safe)),
+                               __double2float_rn(__ddiv_rn(wz, safe)), 0.0f);
+        __stcg(static_cast<float4*>(w) + v, q);
+    }
+    static __device__ __forceinline__ void project(void* w, int v, double radius) {
+        float4 q = __ldcg(static_cast<float4*>(w) + v);
+        float sq = __fadd_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.y, q.y)), __fmul_rn(q.z, q.z));
+        double norm = __dsqrt_rn(static_cast<double>(sq));
+        double scale = __ddiv_rn(radius, norm > 1.0e-20 ? norm : 1.0e-20);
+        q = make_float4(__double2float_rn(__dmul_rn((double)q.x, scale)), __double2float_rn(__dmul_rn((double)q.y, scale)),
+                        __double2float_rn(__dmul_rn((double)q.z, scale)), 0.0f);
+        __stcg(static_cast<float4*>(w) + v, q);
+    }
+    static __device__ __forceinline__ void pack(const void* in, void* w, int v) {
+        const float* p = static_cast<const float*>(in) + 3LL * v;
+        static_cast<float4*>(w)[v] = make_float4(p[0], p[1], p[2], 0.0f);
+    }
+    static __device__ __forceinline__ void unpack(const void* w, void* out, int v) {
+        float4 q = __ldcg(static_cast<const float4*>(w) + v);
+        float* p = static_cast<float*>(out) + 3LL * v;
+        p[0] = q.x;
+        p[1] = q.y;
+        p[2] = q.z;
+    }
+};
+
+// Plain float32 storage and arithmetic.
+template <>
+struct Traits<CSG_ARITH_FP32> {
+    using Acc = float;
+    using P3 = Traits<CSG_ARITH_CAT>::P3;
+    static __device__ __forceinline__ P3 load(const void* w, int v) { return Traits<CSG_ARITH_CAT>::load(w, v); }
+    static __device__ __forceinline__ void face(const P3& a, const P3& b, const P3& c, float& area, float& mx,
+                                                float& my, float& mz) {
+        float e0x = __fsub_rn(b.x, a.x), e0y = __fsub_rn(b.y, a.y), e0z = __fsub_rn(b.z, a.z);
+        float e1x = __fsub_rn(c.x, a.x), e1y = __fsub_rn(c.y, a.y), e1z = __fsub_rn(c.z, a.z);
+        float cx = __fsub_rn(__fmul_rn(e0y, e1z), __fmul_rn(e0z, e1y));
+        float cy = __fsub_rn(__fmul_rn(e0z, e1x), __fmul_rn(e0x, e1z));
+        float cz = __fsub_rn(__fmul_rn(e0x, e1y), __fmul_rn(e0y, e1x));
+        float sq = __fadd_rn(__fadd_rn(__fmul_rn(cx, cx), __fmul_rn(cy, cy)), __fmul_rn(cz, cz));
+        area = __fmul_rn(0.5f, __fsqrt_rn(sq));
+        mx = __fdiv_rn(__fadd_rn(__fadd_rn(a.x, b.x), c.x), 3.0f);
+        my = __fdiv_rn(__fadd_rn(__fadd_rn(a.y, b.y), c.y), 3.0f);
+        mz = __fdiv_rn(__fadd_rn(__fadd_rn(a.z, b.z), c.z), 3.0f);
+        area = area > 0.0f ? area : 0.0f;
+        area = area < 1.0f ? area : 1.0f;
+    }
+    static __device__ __forceinline__ void store(void* w, int v, float total, float wx, float wy, float wz) {
+        float safe = total > 1.0e-20f ? total : 1.0e-20f;
+        __stcg(static_cast<float4*>(w) + v,
+               make_float4(__fdiv_rn(wx, safe), __fdiv_rn(wy, safe), __fdiv_rn(wz, safe), 0.0f));
+    }
+    static __device__ __forceinline__ void project(void* w, int v, double radius) {
+        const float r = static_cast<float>(radius);
+        float4 q = __ldcg(static_cast<float4*>(w) + v);
+        float sq = __fadd_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.y, q.y)), __fmul_rn(q.z, q.z));
+        float norm = __fsqrt_rn(sq);
+        float scale = __fdiv_rn(r, norm > 1.0e-20f ? norm : 1.0e-20f);
+        __stcg(static_cast<float4*>(w) + v,
+               make_float4(__fmul_rn(q.x, scale), __fmul_rn(q.y, scale), __fmul_rn(q.z, scale), 0.0f));
+    }
+    static __device__ __forceinline__ void pack(const void* in, void* w, int v) { Traits<CSG_ARITH_CAT>::pack(in, w, v); }
+    static __device__ __forceinline__ void unpack(const void* w, void* out, int v) {
+        Traits<CSG_ARITH_CAT>::unpack(w, out, v);
+    }
+};
+
+// Float64 storage and arithmetic.
+template <>
+struct Traits<CSG_ARITH_FP64> {
+    using Acc = double;
+    struct P3 {
+        double x, y, z;
+    };
+    static __device__ __forceinline__ P3 load(const void* w, int v) {
+        const double2* base = reinterpret_cast<const double2*>(static_cast<const D4*>(w) + v);
+        double2 xy = __ldcg(base);
+        double2 zw = __ldcg(base + 1);
+        return {xy.x, xy.y, zw.x};
+    }
+    static __device__ __forceinline__ void face(const P3& a, const P3& b, const P3& c, double& area, double& mx,
+                                                double& my, double& mz) {
+        double e0x = __dsub_rn(b.x, a.x), e0y = __dsub_rn(b.y, a.y), e0z = __dsub_rn(b.z, a.z);
+        double e1x = __dsub_rn(c.x, a.x), e1y = __dsub_rn(c.y, a.y), e1z = __dsub_rn(c.z, a.z);
+        double cx = __dsub_rn(__dmul_rn(e0y, e1z), __dmul_rn(e0z, e1y));
+        double cy = __dsub_rn(__dmul_rn(e0z, e1x), __dmul_rn(e0x, e1z));
+        double cz = __dsub_rn(__dmul_rn(e0x, e1y), __dmul_rn(e0y, e1x));
+        double sq = __dadd_rn(__dadd_rn(__dmul_rn(cx, cx), __dmul_rn(cy, cy)), __dmul_rn(cz, cz));
+        area = __dmul_rn(0.5, __dsqrt_rn(sq));
+        mx = __ddiv_rn(__dadd_rn(__dadd_rn(a.x, b.x), c.x), 3.0);
+        my = __ddiv_rn(__dadd_rn(__dadd_rn(a.y, b.y), c.y), 3.0);
+        mz = __ddiv_rn(__dadd_rn(__dadd_rn(a.z, b.z), c.z), 3.0);
+        area = area > 0.0 ? area : 0.0;
+        area = area < 1.0 ? area : 1.0;
+    }
+    static __device__ __forceinline__ void write(void* w, int v, double x, double y, double z) {
+        double2* base = reinterpret_cast<double2*>(static_cast<D4*>(w) + v);
+        __stcg(base, make_double2(x, y));
+        __stcg(base + 1, make_double2(z, 0.0));
+    }
+    static __device__ __forceinline__ void store(void* w, int v, double total, double wx, double wy, double wz) {
+        double safe = total > 1.0e-20 ? total : 1.0e-20;
+        write(w, v, __ddiv_rn(wx, safe), __ddiv_rn(wy, safe), __ddiv_rn(wz, safe));
+    }
+    static __device__ __forceinline__ void project(void* w, int v, double radius) {
+        P3 q = load(w, v);
+        double sq = __dadd_rn(__dadd_rn(__dmul_rn(q.x, q.x), __dmul_rn(q.y, q.y)), __dmul_rn(q.z, q.z));
+        double norm = __dsqrt_rn(sq);
+        double scale = __ddiv_rn(radius, norm > 1.0e-20 ? norm : 1.0e-20);
+        write(w, v, __dmul_rn(q.x, scale), __dmul_rn(q.y, scale), __dmul_rn(q.z, scale));
+    }
+    static __device__ __forceinline__ void pack(const void* in, void* w, int v) {
+        const double* p = static_cast<const double*>(in) + 3LL * v;
+        write(w, v, p[0], p[1], p[2]);
+    }
+    static __device__ __forceinline__ void unpack(const void* w, void* out, int v) {
+        P3 q = load(w, v);
+        double* p = static_cast<double*>(out) + 3LL * v;
+        p[0] = q.x;
+        p[1] = q.y;
+        p[2] = q.z;
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ T dadd(T a, T b);
+template <>
+__device__ __forceinline__ double dadd<double>(double a, double b) { return __dadd_rn(a, b); }
+template <>
+__device__ __forceinline__ float dadd<float>(float a, float b) { return __fadd_rn(a, b); }
+template <typename T>
+__device__ __forceinline__ T dmul(T a, T b);
+template <>
+__device__ __forceinline__ double dmul<double>(double a, double b) { return __dmul_rn(a, b); }
+template <>
+__device__ __forceinline__ float dmul<float>(float a, float b) { return __fmul_rn(a, b); }
+
+// One vertex update by a group of G lanes.  All 32 lanes of the warp must
+// call this together (warp shuffles); inactive groups pass v < 0.
+template <int MODE, int G>
+__device__ __forceinline__ void update_vertex(const ArealParams& p, int v) {
+    using T = Traits<MODE>;
+    using Acc = typename T::Acc;
+    const int lane = threadIdx.x & 31;
+    const int glane = lane & (G - 1);
+    const int gbase = lane & ~(G - 1);
+    int s0 = 0, deg = 0;
+    if (v >= 0) {
+        s0 = __ldg(p.slot_off + v);
+        deg = __ldg(p.slot_off + v + 1) - s0;
+    }
+    const int wdeg = __reduce_max_sync(kFull, deg);
+    Acc total = 0, wx = 0, wy = 0, wz = 0;
+    for (int c0 = 0; c0 < wdeg; c0 += G) {
+        const int j = c0 + glane;
+        Acc fa = 0, fx = 0, fy = 0, fz = 0;
+        if (j < deg) {
+            const int4 tri = __ldg(p.slot_tri + s0 + j);
+            auto a = T::load(p.work, tri.x);
+            auto b = T::load(p.work, tri.y);
+            auto c = T::load(p.work, tri.z);
+            T::face(a, b, c, fa, fx, fy, fz);
+        }
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            const Acc a = __shfl_sync(kFull, fa, gbase + q);
+            const Acc x = __shfl_sync(kFull, fx, gbase + q);
+            const Acc y = __shfl_sync(kFull, fy, gbase + q);
+            const Acc z = __shfl_sync(kFull, fz, gbase + q);
+            if (c0 + q < deg) {  // slot order == ascending face id
+                total = dadd<Acc>(total, a);
+                wx = dadd<Acc>(wx, dmul<Acc>(a, x));
+                wy = dadd<Acc>(wy, dmul<Acc>(a, y));
+                wz = dadd<Acc>(wz, dmul<Acc>(a, z));
+            }
+        }
+    }
+    if (v >= 0 && glane == 0 && total > Acc(0)) T::store(p.work, v, total, wx, wy, wz);
+}
+
+__device__ __forceinline__ int mod_pos(long long a, int m) {
+    long long r = a % m;
+    return static_cast<int>(r < 0 ? r + m : r);
+}
+
+template <int MODE, int G>
+__global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
+    using T = Traits<MODE>;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthreads = gridDim.x * blockDim.x;
+    const int groups_per_warp = 32 / G;
+    const int ngroups = nthreads / G;
+    const int warp_first_group = (tid >> 5) * groups_per_warp;
+    unsigned int phase = 0;
+    int barrier_id = 0;
+
+    for (int v = tid; v < p.n; v += nthreads) T::pack(p.points, p.work, v);
+    if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+
+    const int last = p.iterations - 1;
+    const int L = p.n_levels;
+    const int D = p.stride;
+    for (int start = 1; start <= last;) {
+        int end = last;
+        if (p.project_every > 0) end = min(last, ((start - 1) / p.project_every + 1) * p.project_every);
+        const int S = end - start + 1;
+        const long long nsteps = static_cast<long long>(S - 1) * D + L;
+        for (long long t = 0; t < nsteps; ++t) {
+            const int r = mod_pos(t, D);
+            long long hi = t < L - 1 ? t : L - 1;
+            hi -= mod_pos(hi - r, D);
+            long long lo = t - static_cast<long long>(S - 1) * D;
+            if (lo < r) lo = r;
+            lo += mod_pos(r - lo, D);
+            if (hi < lo) continue;  // no vertex of any sweep sits on this step
+            const int b = __ldg(p.level_begin + lo);
+            const int e = __ldg(p.level_end + hi);
+            for (int base = b + warp_first_group; base < e; base += ngroups) {
+                const int k = base + ((threadIdx.x & 31) / G);
+                update_vertex<MODE, G>(p, k < e ? __ldg(p.order + k) : -1);
+            }
+            if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+        }
+        if (p.project_every > 0 && end % p.project_every == 0) {
+            for (int v = tid; v < p.n; v += nthreads) T::project(p.work, v, p.radius);
+            if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+        }
+        start = end + 1;
+    }
+    for (int v = tid; v < p.n; v += nthreads) T::unpack(p.work, p.points, v);
+}
+
+template <int MODE, int G>
+int launch(const ArealParams& params, int n_ctas, int threads, cudaStream_t stream) {
+    auto kernel = areal_sweeps_kernel<MODE, G>;
+    int device = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    int sms = 0, per_sm = 0;
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+    if (n_ctas <= 0) n_ctas = sms;
+    if (per_sm < 1 || n_ctas > per_sm * sms)
+        return csg::fail(CSG_ERR_LAUNCH, "areal sweeps: %d CTAs x %d threads cannot be co-resident (%d per SM, %d SMs)",
+                         n_ctas, threads, per_sm, sms);
+    ArealParams local = params;
+    void* args[] = {&local};
+    CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(n_ctas), dim3(threads), args,
+                                               0, stream));
+    return CSG_OK;
+}
+
+template <int MODE>
+int dispatch_lanes(const ArealParams& params, int n_ctas, int threads, int lanes, cudaStream_t stream) {
+    switch (lanes) {
+        case 4: return launch<MODE, 4>(params, n_ctas, threads, stream);
+        case 8: return launch<MODE, 8>(params, n_ctas, threads, stream);
+        case 16: return launch<MODE, 16>(params, n_ctas, threads, stream);
+        default: return csg::fail(CSG_ERR_ARG, "lanes_per_vertex must be 4, 8 or 16 (got %d)", lanes);
+    }
+}
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+// Barrier whose expected arrival count is one more than the grid holds: the
+// bounded wait must give up and record CSG_ERR_TIMEOUT.
+__global__ void barrier_timeout_selftest_kernel(csg::Control* ctl, unsigned long long timeout_ns) {
+    unsigned int phase = 1;
+    csg::grid_barrier(ctl, phase, timeout_ns, 1);
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t csg_areal_scratch_bytes(int n_vertices, int arithmetic) {
+    if (n_vertices < 1) return 0;
+    size_t per = arithmetic == CSG_ARITH_FP64 ? sizeof(D4) : sizeof(float4);
+    return sizeof(csg::Control) + align256(per * static_cast<size_t>(n_vertices));
+}
+
+int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, const int32_t* slot_tri,
+                     const int32_t* order, const int32_t* level_begin, const int32_t* level_end, int n_levels,
+                     int level_stride, int iterations, int project_every, double radius, int arithmetic, void* scratch,
+                     size_t scratch_bytes, int n_ctas, int threads_per_cta, int lanes_per_vertex, double timeout_s,
+                     csg_stream_t stream) {
+    if (!points || n_vertices < 1 || !slot_off || !order || !level_begin || !level_end || !scratch)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps: null pointer or empty mesh");
+    if (n_levels < 1 || n_levels > n_vertices || level_stride < 1 || iterations < 1 || project_every < 0)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps: bad schedule (levels %d, stride %d, iterations %d, project %d)",
+                         n_levels, level_stride, iterations, project_every);
+    if (arithmetic < CSG_ARITH_CAT || arithmetic > CSG_ARITH_FP64)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps: unknown arithmetic %d", arithmetic);
+    if (scratch_bytes < csg_areal_scratch_bytes(n_vertices, arithmetic))
+        return csg::fail(CSG_ERR_ARG, "areal sweeps: scratch %zu bytes < required %zu", scratch_bytes,
+                         csg_areal_scratch_bytes(n_vertices, arithmetic));
+    if (reinterpret_cast<uintptr_t>(scratch) % 256 != 0 || reinterpret_cast<uintptr_t>(slot_tri) % 16 != 0)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps: scratch must be 256-byte and slot_tri 16-byte aligned");
+    if (threads_per_cta <= 0) threads_per_cta = 256;
+    if (lanes_per_vertex <= 0) lanes_per_vertex = 8;
+    if (threads_per_cta % 32 != 0 || threads_per_cta > 512)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps: threads_per_cta must be a multiple of 32 up to 512");
+    if (timeout_s <= 0.0) timeout_s = 2.0;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    ArealParams p{};
+    p.points = points;
+    p.ctl = static_cast<csg::Control*>(scratch);
+    p.work = static_cast<char*>(scratch) + sizeof(csg::Control);
+    p.slot_tri = reinterpret_cast<const int4*>(slot_tri);
+    p.slot_off = slot_off;
+    p.order = order;
+    p.level_begin = level_begin;
+    p.level_end = level_end;
+    p.n = n_vertices;
+    p.n_levels = n_levels;
+    p.stride = level_stride;
+    p.iterations = iterations;
+    p.project_every = project_every;
+    p.radius = radius;
+    p.timeout_ns = static_cast<unsigned long long>(timeout_s * 1e9);
+    CSG_CUDA_CHECK(cudaMemsetAsync(scratch, 0, sizeof(csg::Control), s));
+    switch (arithmetic) {
+        case CSG_ARITH_CAT: return dispatch_lanes<CSG_ARITH_CAT>(p, n_ctas, threads_per_cta, lanes_per_vertex, s);
+        case CSG_ARITH_FP32: return dispatch_lanes<CSG_ARITH_FP32>(p, n_ctas, threads_per_cta, lanes_per_vertex, s);
+        default: return dispatch_lanes<CSG_ARITH_FP64>(p, n_ctas, threads_per_cta, lanes_per_vertex, s);
+    }
+}
+
+int csg_selftest_barrier_timeout(void* scratch, size_t scratch_bytes, double timeout_s, csg_stream_t stream) {
+    if (!scratch || scratch_bytes < sizeof(csg::Control) || timeout_s <= 0.0 || timeout_s > 10.0)
+        return csg::fail(CSG_ERR_ARG, "barrier self-test: need 256 bytes of scratch and 0 < timeout_s <= 10");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    csg::Control* ctl = static_cast<csg::Control*>(scratch);
+    unsigned long long timeout_ns = static_cast<unsigned long long>(timeout_s * 1e9);
+    CSG_CUDA_CHECK(cudaMemsetAsync(scratch, 0, sizeof(csg::Control), s));
+    void* args[] = {&ctl, &timeout_ns};
+    CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(barrier_timeout_selftest_kernel), dim3(2),
+                                               dim3(32), args, 0, s));
+    return CSG_OK;
+}
+
+int csg_read_status(const void* scratch, csg_stream_t stream, int* status, int* where) {
+    if (!scratch || !status) return csg::fail(CSG_ERR_ARG, "read_status: null pointer");
+    csg::Control ctl{};
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    CSG_CUDA_CHECK(cudaMemcpyAsync(&ctl, scratch, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+    CSG_CUDA_CHECK(cudaStreamSynchronize(s));
+    *status = ctl.status;
+    if (where) *where = ctl.where;
+    return CSG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,202 @@
+// Host-side mesh topology and wavefront planning for the ordered
+// Surf2Sphere sweeps.  Plain C++, no device memory; O(faces) everywhere.
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/catsurf_b200.h"
+#include "errors.h"
+
+namespace {
+
+int check_faces(int n_vertices, const int32_t* faces, int n_faces) {
+    if (n_vertices < 1 || n_faces < 0 || (n_faces > 0 && faces == nullptr))
+        return csg::fail(CSG_ERR_ARG, "mesh needs n_vertices >= 1 and a face array");
+    for (int64_t i = 0; i < 3LL * n_faces; ++i)
+        if (faces[i] < 0 || faces[i] >= n_vertices)
+            return csg::fail(CSG_ERR_TOPOLOGY, "face index %d at position %lld is outside [0, %d)", faces[i],
+                             static_cast<long long>(i), n_vertices);
+    return CSG_OK;
+}
+
+void incidence(int n, const int32_t* faces, int n_faces, int32_t* off, int32_t* inc) {
+    std::fill(off, off + n + 1, 0);
+    for (int64_t i = 0; i < 3LL * n_faces; ++i) off[faces[i] + 1]++;
+    for (int v = 0; v < n; ++v) off[v + 1] += off[v];
+    std::vector<int32_t> fill(off, off + n);
+    for (int f = 0; f < n_faces; ++f)
+        for (int k = 0; k < 3; ++k) inc[fill[faces[3 * f + k]]++] = f;  // ascending face id
+}
+
+}  // namespace
+
+namespace csg {
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buffer[1024];
+    va_list args;
+    va_start(args, fmt);
+    std::vsnprintf(buffer, sizeof(buffer), fmt, args);
+    va_end(args);
+    g_last_error = buffer;
+    return code;
+}
+}  // namespace csg
+
+extern "C" {
+
+const char* csg_last_error(void) { return csg::g_last_error.c_str(); }
+
+int csg_abi_version(void) { return 1; }
+
+int csg_mesh_incidence(int n_vertices, const int32_t* faces, int n_faces, int32_t* inc_off, int32_t* inc_face) {
+    int rc = check_faces(n_vertices, faces, n_faces);
+    if (rc) return rc;
+    if (!inc_off || (n_faces > 0 && !inc_face)) return csg::fail(CSG_ERR_ARG, "null output");
+    incidence(n_vertices, faces, n_faces, inc_off, inc_face);
+    return CSG_OK;
+}
+
+int csg_mesh_neighbours(int n_vertices, const int32_t* faces, int n_faces, int32_t* nbr_off, int32_t* nbr,
+                        int nbr_capacity) {
+    int rc = check_faces(n_vertices, faces, n_faces);
+    if (rc) return rc;
+    if (!nbr_off) return csg::fail(CSG_ERR_ARG, "null output");
+    // Directed edges of every triangle, then unique + sorted per source vertex.
+    std::vector<int32_t> count(static_cast<size_t>(n_vertices) + 1, 0);
+    for (int f = 0; f < n_faces; ++f)
+        for (int k = 0; k < 3; ++k) count[faces[3 * f + k] + 1] += 2;
+    for (int v = 0; v < n_vertices; ++v) count[v + 1] += count[v];
+    std::vector<int32_t> raw(static_cast<size_t>(count[n_vertices]));
+    std::vector<int32_t> fill(count.begin(), count.end() - 1);
+    for (int f = 0; f < n_faces; ++f) {
+        const int32_t* t = faces + 3 * f;
+        for (int k = 0; k < 3; ++k) {
+            int a = t[k], b = t[(k + 1) % 3], c = t[(k + 2) % 3];
+            raw[fill[a]++] = b;
+            raw[fill[a]++] = c;
+        }
+    }
+    int64_t written = 0;
+    nbr_off[0] = 0;
+    for (int v = 0; v < n_vertices; ++v) {
+        auto first = raw.begin() + count[v], last = raw.begin() + count[v + 1];
+        std::sort(first, last);
+        last = std::unique(first, last);
+        // A face may repeat a vertex; a vertex is never its own neighbour.
+        last = std::remove(first, last, v);
+        int64_t m = last - first;
+        if (nbr) {
+            if (written + m > nbr_capacity) return csg::fail(CSG_ERR_ARG, "neighbour capacity too small");
+            std::copy(first, last, nbr + written);
+        }
+        written += m;
+        nbr_off[v + 1] = static_cast<int32_t>(written);
+    }
+    return static_cast<int>(written);
+}
+
+int csg_dependency_levels(int n_vertices, const int32_t* nbr_off, const int32_t* nbr, int32_t* levels) {
+    if (n_vertices < 1 || !nbr_off || !levels) return csg::fail(CSG_ERR_ARG, "bad arguments");
+    int count = 0;
+    for (int v = 0; v < n_vertices; ++v) {
+        int level = 0;
+        for (int k = nbr_off[v]; k < nbr_off[v + 1]; ++k) {
+            int u = nbr[k];
+            if (u < v) level = std::max(level, levels[u] + 1);
+        }
+        levels[v] = level;
+        count = std::max(count, level + 1);
+    }
+    return count;
+}
+
+int csg_greedy_colours(int n_vertices, const int32_t* nbr_off, const int32_t* nbr, int32_t* colours) {
+    if (n_vertices < 1 || !nbr_off || !colours) return csg::fail(CSG_ERR_ARG, "bad arguments");
+    std::vector<int32_t> stamp;
+    int n_colours = 0;
+    for (int v = 0; v < n_vertices; ++v) colours[v] = -1;
+    for (int v = 0; v < n_vertices; ++v) {
+        int deg = nbr_off[v + 1] - nbr_off[v];
+        if (static_cast<int>(stamp.size()) < deg + 2) stamp.resize(deg + 2, -1);
+        for (int k = nbr_off[v]; k < nbr_off[v + 1]; ++k) {
+            int c = colours[nbr[k]];
+            if (c >= 0 && c <= deg) stamp[c] = v;
+        }
+        int colour = 0;
+        while (stamp[colour] == v) ++colour;
+        colours[v] = colour;
+        n_colours = std::max(n_colours, colour + 1);
+    }
+    return n_colours;
+}
+
+int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int32_t* slot_off, int32_t* slot_tri,
+                         int32_t* order, int32_t* level_begin, int32_t* level_end, csg_areal_plan_info* info) {
+    int rc = check_faces(n_vertices, faces, n_faces);
+    if (rc) return rc;
+    if (!slot_off || !order || !level_begin || !level_end || !info || (n_faces > 0 && !slot_tri))
+        return csg::fail(CSG_ERR_ARG, "null output");
+    const int n = n_vertices;
+    std::vector<int32_t> inc(static_cast<size_t>(3) * n_faces);
+    incidence(n, faces, n_faces, slot_off, inc.data());
+    int max_degree = 0;
+    for (int v = 0; v < n; ++v) max_degree = std::max(max_degree, slot_off[v + 1] - slot_off[v]);
+    for (int64_t s = 0; s < 3LL * n_faces; ++s) {
+        const int32_t* t = faces + 3 * inc[s];
+        slot_tri[4 * s + 0] = t[0];
+        slot_tri[4 * s + 1] = t[1];
+        slot_tri[4 * s + 2] = t[2];
+        slot_tri[4 * s + 3] = inc[s];
+    }
+    // Levels over the face 1-ring (the vertices a sweep update reads).
+    std::vector<int32_t> levels(n, 0);
+    int n_levels = 0;
+    for (int v = 0; v < n; ++v) {
+        int level = 0;
+        for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
+            for (int k = 0; k < 3; ++k) {
+                int u = slot_tri[4 * s + k];
+                if (u < v) level = std::max(level, levels[u] + 1);
+            }
+        levels[v] = level;
+        n_levels = std::max(n_levels, level + 1);
+    }
+    int stride = 1;
+    for (int v = 0; v < n; ++v)
+        for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
+            for (int k = 0; k < 3; ++k) {
+                int w = slot_tri[4 * s + k];
+                if (w > v) stride = std::max(stride, levels[w] - levels[v] + 1);
+            }
+    // order: by (level mod stride, level, id) -- counting sort on level.
+    std::vector<int32_t> per_level(static_cast<size_t>(n_levels) + 1, 0);
+    for (int v = 0; v < n; ++v) per_level[levels[v] + 1]++;
+    std::vector<int32_t> level_order;
+    level_order.reserve(n_levels);
+    for (int r = 0; r < stride; ++r)
+        for (int l = r; l < n_levels; l += stride) level_order.push_back(l);
+    int32_t cursor = 0;
+    std::fill(level_begin, level_begin + n, 0);
+    std::fill(level_end, level_end + n, 0);
+    for (int l : level_order) {
+        level_begin[l] = cursor;
+        cursor += per_level[l + 1];
+        level_end[l] = cursor;
+    }
+    std::vector<int32_t> fill(level_begin, level_begin + n_levels);
+    for (int v = 0; v < n; ++v) order[fill[levels[v]]++] = v;
+    info->n_vertices = n;
+    info->n_faces = n_faces;
+    info->n_levels = n_levels;
+    info->level_stride = stride;
+    info->max_degree = max_degree;
+    info->n_slots = 3 * n_faces;
+    return CSG_OK;
+}
+
+}  // extern "C"

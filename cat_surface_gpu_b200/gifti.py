@@ -1,0 +1,183 @@
+"""Self-contained GIFTI surface codec (two-array point/triangle files).
+
+The reference reads and writes GIFTI through nibabel
+(``src/cat_surface_gpu/gpu_pipeline.py:52-110``: ``read_gifti_mesh`` and
+``write_gifti_mesh``).  This module keeps the same two public functions and the
+same ``GiftiMesh`` record, but is written on the standard library only
+(``xml.etree``, ``base64``, ``zlib``) so the package has no nibabel dependency.
+
+Supported encodings on read: ``ASCII``, ``Base64Binary`` and
+``GZipBase64Binary`` with little- or big-endian payloads and row- or
+column-major ordering.  Writes always use ``GZipBase64Binary`` little-endian,
+which is what CAT-Surface's gifticlib produces and accepts.
+"""
+
+from __future__ import annotations
+
+import base64
+from dataclasses import dataclass
+from pathlib import Path
+import xml.etree.ElementTree as ET
+import zlib
+
+import numpy as np
+
+_DTYPES = {
+    "NIFTI_TYPE_FLOAT32": np.float32,
+    "NIFTI_TYPE_FLOAT64": np.float64,
+    "NIFTI_TYPE_INT32": np.int32,
+    "NIFTI_TYPE_UINT8": np.uint8,
+    "NIFTI_TYPE_INT16": np.int16,
+    "NIFTI_TYPE_INT64": np.int64,
+}
+_INTENT_CODES = {
+    "NIFTI_INTENT_POINTSET": 1008,
+    "NIFTI_INTENT_TRIANGLE": 1009,
+}
+_INTENT_NAMES = {value: key for key, value in _INTENT_CODES.items()}
+
+
+@dataclass(frozen=True)
+class GiftiMesh:
+    """One GIFTI surface: float32 vertices ``[n, 3]`` and int32 faces ``[m, 3]``."""
+
+    vertices: np.ndarray
+    faces: np.ndarray
+
+
+def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
+    attrs = element.attrib
+    dtype_name = attrs.get("DataType", "NIFTI_TYPE_FLOAT32")
+    if dtype_name not in _DTYPES:
+        raise ValueError(f"Unsupported GIFTI DataType {dtype_name}")
+    dtype = np.dtype(_DTYPES[dtype_name])
+    dims = int(attrs.get("Dimensionality", "1"))
+    shape = tuple(int(attrs[f"Dim{i}"]) for i in range(dims))
+    encoding = attrs.get("Encoding", "ASCII")
+    endian = attrs.get("Endian", "LittleEndian")
+    order = "F" if attrs.get("ArrayIndexingOrder", "RowMajorOrder") == "ColumnMajorOrder" else "C"
+    data_element = element.find("Data")
+    text = "" if data_element is None or data_element.text is None else data_element.text
+    count = int(np.prod(shape)) if shape else 0
+    if encoding == "ASCII":
+        values = np.array(text.split(), dtype=np.float64 if dtype.kind == "f" else np.int64)
+        values = values.astype(dtype)
+    elif encoding in ("Base64Binary", "GZipBase64Binary"):
+        raw = base64.b64decode("".join(text.split()))
+        if encoding == "GZipBase64Binary":
+            raw = zlib.decompress(raw)
+        wire = dtype.newbyteorder("<" if endian == "LittleEndian" else ">")
+        values = np.frombuffer(raw, dtype=wire).astype(dtype)
+    else:
+        raise ValueError(f"Unsupported GIFTI encoding {encoding}")
+    if values.size != count:
+        raise ValueError(f"GIFTI array holds {values.size} values, header says {count}")
+    intent_attr = attrs.get("Intent", "NIFTI_INTENT_NONE")
+    intent = _INTENT_CODES.get(intent_attr, 0)
+    return np.ascontiguousarray(values.reshape(shape, order=order)), intent
+
+
+def read_gifti_arrays(path: str | Path) -> list[tuple[np.ndarray, int]]:
+    """Return every data array of a GIFTI file with its NIfTI intent code."""
+
+    root = ET.parse(str(path)).getroot()
+    if root.tag != "GIFTI":
+        raise ValueError(f"Not a GIFTI file: {path}")
+    return [_decode_array(item) for item in root.findall("DataArray")]
+
+
+def read_gifti_mesh(path: str | Path) -> GiftiMesh:
+    """Read the first point-set and triangle arrays of a GIFTI surface.
+
+    Mirrors ``read_gifti_mesh`` of the reference (``gpu_pipeline.py:52-71``):
+    ``ValueError`` when fewer than two arrays are present or when either array
+    is not ``[*, 3]``.
+    """
+
+    arrays = read_gifti_arrays(path)
+    if len(arrays) < 2:
+        raise ValueError(f"GIFTI file must contain vertex and face arrays: {path}")
+    vertices = arrays[0][0]
+    faces = arrays[1][0]
+    if vertices.ndim != 2 or vertices.shape[1] != 3:
+        raise ValueError(f"Vertex array must have shape [n, 3]: {path} -> {vertices.shape}")
+    if faces.ndim != 2 or faces.shape[1] != 3:
+        raise ValueError(f"Face array must have shape [m, 3]: {path} -> {faces.shape}")
+    return GiftiMesh(
+        vertices=np.ascontiguousarray(vertices, dtype=np.float32),
+        faces=np.ascontiguousarray(faces, dtype=np.int32),
+    )
+
+
+def _encode_array(values: np.ndarray, intent: int, dtype_name: str) -> str:
+    payload = base64.b64encode(zlib.compress(np.ascontiguousarray(values).astype(values.dtype.newbyteorder("<")).tobytes(), 6)).decode("ascii")
+    dims = "".join(f' Dim{i}="{size}"' for i, size in enumerate(values.shape))
+    intent_name = _INTENT_NAMES.get(intent, "NIFTI_INTENT_NONE")
+    transform = ""
+    if intent == _INTENT_CODES["NIFTI_INTENT_POINTSET"]:
+        transform = (
+            "<CoordinateSystemTransformMatrix>"
+            "<DataSpace><![CDATA[NIFTI_XFORM_UNKNOWN]]></DataSpace>"
+            "<TransformedSpace><![CDATA[NIFTI_XFORM_UNKNOWN]]></TransformedSpace>"
+            "<MatrixData>1 0 0 0 0 1 0 0 0 0 1 0 0 0 0 1</MatrixData>"
+            "</CoordinateSystemTransformMatrix>\n"
+        )
+    return (
+        f'<DataArray Intent="{intent_name}" DataType="{dtype_name}" '
+        f'ArrayIndexingOrder="RowMajorOrder" Dimensionality="{values.ndim}"{dims} '
+        'Encoding="GZipBase64Binary" Endian="LittleEndian" ExternalFileName="" ExternalFileOffset="">\n'
+        "<MetaData/>\n"
+        f"{transform}<Data>{payload}</Data>\n</DataArray>\n"
+    )
+
+
+def write_gifti_mesh(
+    path: str | Path,
+    mesh: GiftiMesh,
+    *,
+    reference_path: str | Path | None = None,
+) -> None:
+    """Write vertices (float32) and faces (int32) as a two-array GIFTI file.
+
+    Mirrors ``write_gifti_mesh`` of the reference (``gpu_pipeline.py:74-110``):
+    array intents are copied from ``reference_path`` when it is given.
+    """
+
+    point_intent = _INTENT_CODES["NIFTI_INTENT_POINTSET"]
+    triangle_intent = _INTENT_CODES["NIFTI_INTENT_TRIANGLE"]
+    if reference_path is not None:
+        arrays = read_gifti_arrays(reference_path)
+        if len(arrays) >= 1 and arrays[0][1]:
+            point_intent = arrays[0][1]
+        if len(arrays) >= 2 and arrays[1][1]:
+            triangle_intent = arrays[1][1]
+    vertices = np.ascontiguousarray(mesh.vertices, dtype=np.float32)
+    faces = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    if vertices.ndim != 2 or vertices.shape[1] != 3 or faces.ndim != 2 or faces.shape[1] != 3:
+        raise ValueError("GIFTI mesh arrays must have shape [n, 3] and [m, 3]")
+    text = (
+        '<?xml version="1.0" encoding="UTF-8"?>\n'
+        '<!DOCTYPE GIFTI SYSTEM "http://www.nitrc.org/frs/download.php/115/gifti.dtd">\n'
+        '<GIFTI Version="1.0" NumberOfDataArrays="2">\n<MetaData/>\n<LabelTable/>\n'
+        + _encode_array(vertices, point_intent, "NIFTI_TYPE_FLOAT32")
+        + _encode_array(faces, triangle_intent, "NIFTI_TYPE_INT32")
+        + "</GIFTI>\n"
+    )
+    output = Path(path)
+    output.parent.mkdir(parents=True, exist_ok=True)
+    output.write_text(text, encoding="utf-8")
+
+
+def write_vertices_like(reference_path: str | Path, output_path: str | Path, vertices: np.ndarray) -> None:
+    """Copy a GIFTI surface and replace its vertices; faces are byte-identical.
+
+    Same contract as the reference's ``_write_vertices_like``
+    (``surf2sphere.py:899-916``): topology is carried over from
+    ``reference_path`` unchanged, so triangle arrays are exact by construction.
+    """
+
+    mesh = read_gifti_mesh(reference_path)
+    values = np.ascontiguousarray(vertices, dtype=np.float32)
+    if values.shape != mesh.vertices.shape:
+        raise ValueError(f"vertices shape {values.shape} does not match {mesh.vertices.shape}")
+    write_gifti_mesh(output_path, GiftiMesh(values, mesh.faces), reference_path=reference_path)

@@ -1,0 +1,442 @@
+"""CAT_Surf2Sphere with the ordered area-smoothing sweeps on a B200.
+
+Public names and signatures follow the reference module
+``src/cat_surface_gpu/surf2sphere.py``:
+
+* ``Surf2SphereTopology.from_mesh`` (reference 401-448) -- built by the native
+  host builders (C++, O(faces)) instead of Python loops.
+* ``run_areal_smoothing_cuda`` (reference 940-1104) -- all sweeps in ONE
+  persistent cooperative CUDA launch (``csg_areal_sweeps``) instead of one
+  Triton launch per dependency level per sweep.
+* ``convert_ellipsoid_to_sphere_with_surface_area`` (reference 919-937) and
+  ``surface_area`` (reference 461-471) -- host NumPy, same arithmetic.
+* ``run_cat_surf2sphere_gpu`` (reference 1107-1295) -- upstream binary for
+  stages 1-5, then the GPU sweeps, then the ellipsoid-to-sphere step.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+import math
+from pathlib import Path
+import subprocess
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+from . import _native
+from .device import DeviceUnavailable, resolve_device
+from .gifti import GiftiMesh, read_gifti_mesh, write_vertices_like
+
+
+@dataclass(frozen=True)
+class SweepPlan:
+    """Host arrays of the wavefront schedule (see include/catsurf_b200.h)."""
+
+    slot_off: np.ndarray
+    slot_tri: np.ndarray
+    order: np.ndarray
+    level_begin: np.ndarray
+    level_end: np.ndarray
+    n_levels: int
+    level_stride: int
+    max_degree: int
+
+    @classmethod
+    def build(cls, faces: np.ndarray, n_points: int) -> "SweepPlan":
+        tri = np.ascontiguousarray(faces, dtype=np.int32)
+        if tri.ndim != 2 or tri.shape[1] != 3:
+            raise ValueError(f"faces must have shape [m, 3], got {tri.shape}")
+        n = int(n_points)
+        slot_off = np.zeros(n + 1, dtype=np.int32)
+        slot_tri = np.zeros((max(1, 3 * tri.shape[0]), 4), dtype=np.int32)
+        order = np.zeros(n, dtype=np.int32)
+        level_begin = np.zeros(n, dtype=np.int32)
+        level_end = np.zeros(n, dtype=np.int32)
+        info = _native.PlanInfo()
+        lib = _native.library()
+        _native.check(
+            lib.csg_areal_plan_build(
+                n, _native.ptr(tri), tri.shape[0], _native.ptr(slot_off), _native.ptr(slot_tri),
+                _native.ptr(order), _native.ptr(level_begin), _native.ptr(level_end), ctypes_ref(info),
+            ),
+            "csg_areal_plan_build",
+        )
+        return cls(
+            slot_off=slot_off,
+            slot_tri=slot_tri,
+            order=order,
+            level_begin=level_begin,
+            level_end=level_end,
+            n_levels=int(info.n_levels),
+            level_stride=int(info.level_stride),
+            max_degree=int(info.max_degree),
+        )
+
+    def to_device(self, device: torch.device) -> dict[str, torch.Tensor]:
+        return {
+            name: torch.from_numpy(getattr(self, name)).to(device, non_blocking=False)
+            for name in ("slot_off", "slot_tri", "order", "level_begin", "level_end")
+        }
+
+
+def ctypes_ref(struct) -> int:
+    import ctypes
+
+    return ctypes.addressof(struct)
+
+
+def _padded(off: np.ndarray, values: np.ndarray, n: int) -> tuple[np.ndarray, np.ndarray]:
+    counts = np.diff(off)
+    width = max(1, int(counts.max()) if counts.size else 1)
+    table = np.zeros((n, width), dtype=np.int64)
+    mask = np.arange(width)[None, :] < counts[:, None]
+    table[mask] = values[: int(off[-1])]
+    return table, mask
+
+
+def _groups(labels: np.ndarray, count: int) -> tuple[np.ndarray, ...]:
+    order = np.argsort(labels, kind="stable")
+    bounds = np.searchsorted(labels[order], np.arange(count + 1))
+    return tuple(order[bounds[i] : bounds[i + 1]].astype(np.int64) for i in range(count))
+
+
+@dataclass(frozen=True)
+class Surf2SphereTopology:
+    """Triangle incidence, 1-ring neighbours, colour and dependency-level groups.
+
+    Same fields as the reference (``surf2sphere.py:401-448``); built by the
+    native host builders.  ``plan`` holds the wavefront schedule of the sweeps.
+    """
+
+    incident_faces: np.ndarray
+    incident_mask: np.ndarray
+    neighbours: np.ndarray
+    neighbour_mask: np.ndarray
+    color_groups: tuple[np.ndarray, ...]
+    ordered_groups: tuple[np.ndarray, ...]
+    plan: SweepPlan | None = field(default=None, compare=False, repr=False)
+
+    @classmethod
+    def from_mesh(cls, mesh: GiftiMesh) -> "Surf2SphereTopology":
+        faces = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+        n = int(mesh.vertices.shape[0])
+        if faces.ndim != 2 or faces.shape[1] != 3:
+            raise ValueError(f"faces must have shape [m, 3], got {faces.shape}")
+        lib = _native.library()
+        inc_off = np.zeros(n + 1, dtype=np.int32)
+        inc = np.zeros(max(1, 3 * faces.shape[0]), dtype=np.int32)
+        _native.check(
+            lib.csg_mesh_incidence(n, _native.ptr(faces), faces.shape[0], _native.ptr(inc_off), _native.ptr(inc)),
+            "csg_mesh_incidence",
+        )
+        nbr_off = np.zeros(n + 1, dtype=np.int32)
+        nbr = np.zeros(max(1, 6 * faces.shape[0]), dtype=np.int32)
+        _native.check(
+            lib.csg_mesh_neighbours(
+                n, _native.ptr(faces), faces.shape[0], _native.ptr(nbr_off), _native.ptr(nbr), nbr.size
+            ),
+            "csg_mesh_neighbours",
+        )
+        colours = np.zeros(n, dtype=np.int32)
+        n_colours = _native.check(
+            lib.csg_greedy_colours(n, _native.ptr(nbr_off), _native.ptr(nbr), _native.ptr(colours)),
+            "csg_greedy_colours",
+        )
+        levels = np.zeros(n, dtype=np.int32)
+        n_levels = _native.check(
+            lib.csg_dependency_levels(n, _native.ptr(nbr_off), _native.ptr(nbr), _native.ptr(levels)),
+            "csg_dependency_levels",
+        )
+        incident_faces, incident_mask = _padded(inc_off, inc, n)
+        neighbours, neighbour_mask = _padded(nbr_off, nbr, n)
+        return cls(
+            incident_faces=incident_faces,
+            incident_mask=incident_mask,
+            neighbours=neighbours,
+            neighbour_mask=neighbour_mask,
+            color_groups=_groups(colours, n_colours),
+            ordered_groups=_groups(levels, n_levels),
+            plan=SweepPlan.build(faces, n),
+        )
+
+
+@dataclass(frozen=True)
+class CatSurf2SphereGpuResult:
+    """Store the generated sphere path and synchronized stage timings."""
+
+    vertices: np.ndarray
+    faces: np.ndarray
+    timings: dict[str, float]
+    output_path: Path
+
+
+def surface_area(mesh: GiftiMesh) -> float:
+    """Total surface area in float64 (reference ``surf2sphere.py:461-471``)."""
+
+    vertices = mesh.vertices.astype(np.float64, copy=False)
+    triangles = vertices[mesh.faces.astype(np.int64, copy=False)]
+    cross = np.cross(triangles[:, 1] - triangles[:, 0], triangles[:, 2] - triangles[:, 0])
+    return float(0.5 * np.linalg.norm(cross, axis=1).sum(dtype=np.float64))
+
+
+def convert_ellipsoid_to_sphere_with_surface_area(vertices: np.ndarray, desired_surface_area: float) -> np.ndarray:
+    """Scale to the sphere of area ``desired_surface_area`` (reference 919-937)."""
+
+    geometry = np.ascontiguousarray(vertices, dtype=np.float32)
+    radius = math.sqrt(desired_surface_area / (4.0 * math.pi))
+    bounds = np.stack((geometry.min(axis=0), geometry.max(axis=0)), axis=1)
+    axes = (np.abs(bounds[:, 0]) + np.abs(bounds[:, 1])) * 0.5
+    axes = np.maximum(axes, 1.0e-20)
+    values = geometry.astype(np.float64)
+    scaled = values / axes[None, :]
+    norm = np.sqrt((scaled * scaled).sum(axis=1))
+    result = np.zeros_like(values)
+    nonzero = norm != 0.0
+    result[nonzero] = radius * values[nonzero] / norm[nonzero, None]
+    result[nonzero] /= axes[None, :]
+    return np.ascontiguousarray(result, dtype=np.float32)
+
+
+def _resolve_dtype(dtype: str | torch.dtype) -> torch.dtype:
+    if isinstance(dtype, torch.dtype):
+        result = dtype
+    else:
+        mapping = {"float32": torch.float32, "fp32": torch.float32, "float64": torch.float64, "fp64": torch.float64}
+        try:
+            result = mapping[str(dtype).lower().replace("torch.", "")]
+        except KeyError as exc:
+            raise ValueError(f"Unsupported CAT_Surf2Sphere dtype: {dtype}") from exc
+    if result not in (torch.float32, torch.float64):
+        raise ValueError(f"CAT_Surf2Sphere supports only FP32 and FP64, got {result}")
+    return result
+
+
+DEFAULT_LAUNCH = {"n_ctas": 0, "threads_per_cta": 256, "lanes_per_vertex": 8}
+
+
+def areal_sweeps_device(
+    points: torch.Tensor,
+    plan_device: dict[str, torch.Tensor],
+    plan: SweepPlan,
+    *,
+    iterations: int,
+    project_every: int,
+    radius: float,
+    arithmetic: str,
+    launch: dict | None = None,
+    timeout_s: float = 2.0,
+    scratch: torch.Tensor | None = None,
+    stream: torch.cuda.Stream | None = None,
+) -> torch.Tensor:
+    """Run the sweeps in place on a device tensor (no host synchronisation).
+
+    Returns the scratch tensor; its first 256 bytes hold the kernel's status
+    word (read it with :func:`read_status` once the stream is synchronised).
+    """
+
+    mode = _native.ARITH[arithmetic]
+    n = int(points.shape[0])
+    lib = _native.library()
+    need = int(lib.csg_areal_scratch_bytes(n, mode))
+    if scratch is None or scratch.numel() < need:
+        scratch = torch.empty(need, dtype=torch.uint8, device=points.device)
+    cfg = dict(DEFAULT_LAUNCH)
+    if launch:
+        cfg.update(launch)
+    _native.check(
+        lib.csg_areal_sweeps(
+            _native.ptr(points), n, _native.ptr(plan_device["slot_off"]), _native.ptr(plan_device["slot_tri"]),
+            _native.ptr(plan_device["order"]), _native.ptr(plan_device["level_begin"]),
+            _native.ptr(plan_device["level_end"]), plan.n_levels, plan.level_stride, int(iterations),
+            int(project_every), float(radius), mode, _native.ptr(scratch), scratch.numel(),
+            int(cfg["n_ctas"]), int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s),
+            _native.stream_handle(stream),
+        ),
+        "csg_areal_sweeps",
+    )
+    return scratch
+
+
+def read_status(scratch: torch.Tensor) -> tuple[int, int]:
+    """(status, where) of a finished persistent launch (synchronises the stream)."""
+
+    words = scratch[:12].cpu().view(torch.int32).tolist()
+    return int(words[1]), int(words[2])
+
+
+def run_areal_smoothing_cuda(
+    vertices: np.ndarray,
+    faces: np.ndarray,
+    topology: Surf2SphereTopology,
+    *,
+    iterations: int,
+    project_every: int,
+    radius: float,
+    device: str | torch.device = "cuda",
+    dtype: str | torch.dtype = torch.float32,
+    kernel: str = "triton",
+    schedule: str = "ordered",
+    arithmetic: str = "cat",
+    schedule_block_size: int | None = None,
+    launch: dict | None = None,
+) -> tuple[np.ndarray, dict[str, float]]:
+    """Run every CAT area-smoothing sweep on CUDA in dependency order.
+
+    Same contract as the reference (``surf2sphere.py:940-1104``): sweeps
+    ``1 .. iterations-1``, projection to ``radius`` after sweep ``s`` when
+    ``s % project_every == 0``; returns ``(float32 [N, 3], timings)``.
+    ``kernel`` accepts the reference's names ("triton", "torch") and both run
+    the native sm_100a kernel.  Only the exact ``"ordered"`` schedule exists.
+    ``dtype=float64`` runs float64 storage and arithmetic and, unlike the
+    reference's float64 Triton path, applies the sphere projection.
+    """
+
+    try:
+        target = resolve_device(device)
+    except DeviceUnavailable as exc:
+        raise RuntimeError(f"CAT_Surf2Sphere CUDA backend: {exc}") from exc
+    geometry_dtype = _resolve_dtype(dtype)
+    if kernel not in ("torch", "triton", "cuda"):
+        raise ValueError(f"Unsupported CAT_Surf2Sphere kernel: {kernel}")
+    if schedule not in ("ordered", "color"):
+        raise ValueError(f"Unsupported CAT_Surf2Sphere schedule: {schedule}")
+    if schedule != "ordered":
+        raise NotImplementedError("only the exact ordered schedule is implemented (it is also the fastest)")
+    if arithmetic not in ("cat", "fp32"):
+        raise ValueError(f"Unsupported CAT_Surf2Sphere arithmetic: {arithmetic}")
+    if iterations < 1:
+        raise ValueError("Must be at least 1")
+    if project_every < 0:
+        raise ValueError("sphere projection period must be non-negative")
+    points_host = np.asarray(vertices)
+    if points_host.ndim != 2 or points_host.shape[1] != 3:
+        raise ValueError(f"vertices must have shape [n, 3], got {points_host.shape}")
+    if geometry_dtype == torch.float64:
+        mode = "fp64"
+    else:
+        mode = "cat" if arithmetic == "cat" else "fp32"
+    plan = topology.plan
+    if plan is None or plan.slot_off.shape[0] != points_host.shape[0] + 1:
+        plan = SweepPlan.build(faces, points_host.shape[0])
+
+    with torch.no_grad(), torch.cuda.device(target):
+        points = torch.as_tensor(np.ascontiguousarray(points_host), dtype=geometry_dtype).to(target).contiguous()
+        plan_device = plan.to_device(target)
+        torch.cuda.synchronize(target)
+        start = time.perf_counter()
+        scratch = areal_sweeps_device(
+            points, plan_device, plan, iterations=iterations, project_every=project_every, radius=radius,
+            arithmetic=mode, launch=launch,
+        )
+        torch.cuda.synchronize(target)
+        elapsed = time.perf_counter() - start
+        status, where = read_status(scratch)
+        if status != 0:
+            raise RuntimeError(f"areal sweep kernel reported status {status} at barrier {where}")
+        result = points.cpu().numpy()
+    return np.ascontiguousarray(result, dtype=np.float32), {
+        "areal_smoothing_seconds": elapsed,
+        "color_groups": float(plan.n_levels),
+        "ordered_schedule": 1.0,
+        "cat_mixed_arithmetic": float(mode == "cat"),
+        "iterations_requested": float(iterations),
+        "iterations_executed": float(max(0, iterations - 1)),
+        "wavefront_stride": float(plan.level_stride),
+    }
+
+
+def run_surf2sphere_preprocess_cuda(*args, **kwargs):
+    """GPU stages 1-5 are not part of this package; the upstream binary runs them."""
+
+    raise NotImplementedError(
+        "Surf2Sphere stages 1-5 on the GPU are not implemented; use preprocess_kernel='cpu' "
+        "(the upstream CAT_Surf2Sphere binary), as the reference does by default"
+    )
+
+
+def _run_reference(reference_cli: Path, input_path: Path, output_path: Path, stop_at: int) -> None:
+    completed = subprocess.run(
+        [str(reference_cli), str(input_path), str(output_path), str(stop_at), "0"],
+        check=False,
+        capture_output=True,
+        text=True,
+    )
+    if completed.returncode != 0:
+        raise RuntimeError("CAT_Surf2Sphere CPU preprocessing failed:\n" + completed.stderr[-4000:])
+
+
+def run_cat_surf2sphere_gpu(
+    input_surface: str | Path,
+    output_surface: str | Path,
+    *,
+    reference_cli: str | Path,
+    stop_at: int = 10,
+    device: str | torch.device = "cuda",
+    dtype: str | torch.dtype = torch.float32,
+    kernel: str = "triton",
+    preprocess_kernel: str = "cpu",
+    preprocess_block_size: int | None = 131072,
+    areal_schedule: str = "ordered",
+    areal_arithmetic: str = "cat",
+    areal_block_size: int | None = None,
+) -> CatSurf2SphereGpuResult:
+    """Upstream stages 1-5 on the CPU binary, sweeps on the GPU (reference 1107-1295)."""
+
+    if stop_at < 1:
+        raise ValueError("stop_at must be at least 1")
+    if preprocess_kernel not in ("cpu", "triton"):
+        raise ValueError(f"Unsupported CAT_Surf2Sphere preprocess kernel: {preprocess_kernel}")
+    if preprocess_kernel != "cpu":
+        run_surf2sphere_preprocess_cuda()
+    input_path = Path(input_surface)
+    output_path = Path(output_surface)
+    reference_path = Path(reference_cli)
+    timings: dict[str, float] = {}
+    total_start = time.perf_counter()
+    if stop_at <= 5:
+        start = time.perf_counter()
+        _run_reference(reference_path, input_path, output_path, stop_at)
+        timings["reference_prefix_seconds"] = time.perf_counter() - start
+        mesh = read_gifti_mesh(output_path)
+        timings["total_seconds"] = time.perf_counter() - total_start
+        return CatSurf2SphereGpuResult(mesh.vertices, mesh.faces, timings, output_path)
+
+    with tempfile.TemporaryDirectory(prefix="cat_surface_b200_surf2sphere_") as temp_dir:
+        prefix_path = Path(temp_dir) / "stage5.gii"
+        start = time.perf_counter()
+        _run_reference(reference_path, input_path, prefix_path, 5)
+        timings["reference_prefix_seconds"] = time.perf_counter() - start
+        prefix_mesh = read_gifti_mesh(prefix_path)
+        topology_start = time.perf_counter()
+        topology = Surf2SphereTopology.from_mesh(prefix_mesh)
+        timings["topology_build_seconds"] = time.perf_counter() - topology_start
+        radius = float(np.sqrt(np.max(np.sum(prefix_mesh.vertices.astype(np.float64) ** 2, axis=1))))
+        smoothed, smooth_timings = run_areal_smoothing_cuda(
+            prefix_mesh.vertices,
+            prefix_mesh.faces,
+            topology,
+            iterations=1000 * (stop_at - 5),
+            project_every=1000,
+            radius=radius,
+            device=device,
+            dtype=dtype,
+            kernel=kernel,
+            schedule=areal_schedule,
+            arithmetic=areal_arithmetic,
+            schedule_block_size=areal_block_size,
+        )
+        timings.update(smooth_timings)
+        conversion_start = time.perf_counter()
+        converted = convert_ellipsoid_to_sphere_with_surface_area(
+            smoothed, surface_area(read_gifti_mesh(input_path))
+        )
+        timings["ellipsoid_to_sphere_seconds"] = time.perf_counter() - conversion_start
+        write_start = time.perf_counter()
+        write_vertices_like(prefix_path, output_path, converted)
+        timings["output_write_seconds"] = time.perf_counter() - write_start
+    result_mesh = read_gifti_mesh(output_path)
+    timings["total_seconds"] = time.perf_counter() - total_start
+    return CatSurf2SphereGpuResult(result_mesh.vertices, result_mesh.faces, timings, output_path)
