@@ -39,7 +39,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_areal_scratch_bytes": (c_size_t, [_I, _I]),
     "csg_areal_sweeps": (
         _I,
-        [_P, _I, _P, _P, _P, _P, _P, _I, _I, _I, _I, c_double, _I, _P, c_size_t, _I, _I, _I, c_double, _P],
+        [_P, _I, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, c_double, _I, _P, c_size_t, _I, _I, _I, c_double, _P],
     ),
     "csg_selftest_barrier_timeout": (_I, [_P, c_size_t, c_double, _P]),
     "csg_read_status": (_I, [_P, _P, _P, _P]),

@@ -51,6 +51,8 @@ struct ArealParams {
     int n;
     int n_levels;
     int stride;
+    int max_degree;
+    int nloc_max;  // vertices owned by one CTA (set at launch)
     int iterations;
     int project_every;
     double radius;
@@ -231,29 +233,26 @@ template <>
 __device__ __forceinline__ float dmul<float>(float a, float b) { return __fmul_rn(a, b); }
 
 // One vertex update by a group of G lanes.  All 32 lanes of the warp must
-// call this together (warp shuffles); inactive groups pass v < 0.
-template <int MODE, int G>
-__device__ __forceinline__ void update_vertex(const ArealParams& p, int v) {
+// call this together (warp shuffles); inactive groups pass v < 0.  `tri`
+// points at the vertex's incident-face slots (shared or global memory).
+template <int MODE, int G, bool SMEM>
+__device__ __forceinline__ void update_vertex(const ArealParams& p, int v, const int4* tri, int deg) {
     using T = Traits<MODE>;
     using Acc = typename T::Acc;
     const int lane = threadIdx.x & 31;
     const int glane = lane & (G - 1);
     const int gbase = lane & ~(G - 1);
-    int s0 = 0, deg = 0;
-    if (v >= 0) {
-        s0 = __ldg(p.slot_off + v);
-        deg = __ldg(p.slot_off + v + 1) - s0;
-    }
+    if (v < 0) deg = 0;
     const int wdeg = __reduce_max_sync(kFull, deg);
     Acc total = 0, wx = 0, wy = 0, wz = 0;
     for (int c0 = 0; c0 < wdeg; c0 += G) {
         const int j = c0 + glane;
         Acc fa = 0, fx = 0, fy = 0, fz = 0;
         if (j < deg) {
-            const int4 tri = __ldg(p.slot_tri + s0 + j);
-            auto a = T::load(p.work, tri.x);
-            auto b = T::load(p.work, tri.y);
-            auto c = T::load(p.work, tri.z);
+            const int4 t = SMEM ? tri[j] : __ldg(tri + j);
+            auto a = T::load(p.work, t.x);
+            auto b = T::load(p.work, t.y);
+            auto c = T::load(p.work, t.z);
             T::face(a, b, c, fa, fx, fy, fz);
         }
 #pragma unroll
@@ -273,46 +272,98 @@ __device__ __forceinline__ void update_vertex(const ArealParams& p, int v) {
     if (v >= 0 && glane == 0 && total > Acc(0)) T::store(p.work, v, total, wx, wy, wz);
 }
 
-__device__ __forceinline__ int mod_pos(long long a, int m) {
-    long long r = a % m;
-    return static_cast<int>(r < 0 ? r + m : r);
-}
+// Number of positions c, c + nc, c + 2 nc, ... that lie below `bound`.
+__device__ __forceinline__ int owned_below(int bound, int c, int nc) { return bound > c ? (bound - c + nc - 1) / nc : 0; }
 
-template <int MODE, int G>
+// Vertex ownership: CTA c owns the vertices at positions c, c + n_ctas, ...
+// of `order`, so every dependency level (a contiguous run of `order`) is
+// spread evenly over all CTAs and a CTA always updates the same vertices.
+// With SMEM the CTA copies those vertices' incident-face slots into shared
+// memory once; each wavefront step then only gathers positions from L2.
+template <int MODE, int G, bool SMEM>
 __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
     using T = Traits<MODE>;
+    extern __shared__ __align__(16) unsigned char smem[];
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthreads = gridDim.x * blockDim.x;
-    const int groups_per_warp = 32 / G;
-    const int ngroups = nthreads / G;
-    const int warp_first_group = (tid >> 5) * groups_per_warp;
+    const int c = blockIdx.x;
+    const int nc = gridDim.x;
+    const int groups = blockDim.x / G;
+    const int warp_first_group = (threadIdx.x >> 5) * (32 / G);
+    const int my_group = (threadIdx.x & 31) / G;
+    const int nloc = owned_below(p.n, c, nc);
+    const int L = p.n_levels;
+    const int D = p.stride;
+    // shared-memory image (SMEM only): face slots, vertex ids and degrees of
+    // the owned vertices, then per-level owned ranges and per-residue top level
+    int4* ltri = reinterpret_cast<int4*>(smem);
+    int* lvid = reinterpret_cast<int*>(ltri + (SMEM ? p.nloc_max * p.max_degree : 0));
+    int* ldeg = lvid + p.nloc_max;
+    int* lbeg = ldeg + p.nloc_max;
+    int* lend = lbeg + L;
+    int* hitop = lend + L;
     unsigned int phase = 0;
     int barrier_id = 0;
 
+    if (SMEM) {
+        for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
+            const int v = __ldg(p.order + c + i * nc);
+            const int s0 = __ldg(p.slot_off + v);
+            const int d = __ldg(p.slot_off + v + 1) - s0;
+            lvid[i] = v;
+            ldeg[i] = d;
+            for (int j = 0; j < d; ++j) ltri[i * p.max_degree + j] = __ldg(p.slot_tri + s0 + j);
+        }
+        for (int l = threadIdx.x; l < L; l += blockDim.x) {
+            lbeg[l] = owned_below(__ldg(p.level_begin + l), c, nc);
+            lend[l] = owned_below(__ldg(p.level_end + l), c, nc);
+        }
+        for (int r = threadIdx.x; r < D; r += blockDim.x) hitop[r] = (L - 1) - ((L - 1 - r) % D + D) % D;
+    }
     for (int v = tid; v < p.n; v += nthreads) T::pack(p.points, p.work, v);
     if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
 
     const int last = p.iterations - 1;
-    const int L = p.n_levels;
-    const int D = p.stride;
     for (int start = 1; start <= last;) {
         int end = last;
         if (p.project_every > 0) end = min(last, ((start - 1) / p.project_every + 1) * p.project_every);
         const int S = end - start + 1;
-        const long long nsteps = static_cast<long long>(S - 1) * D + L;
-        for (long long t = 0; t < nsteps; ++t) {
-            const int r = mod_pos(t, D);
-            long long hi = t < L - 1 ? t : L - 1;
-            hi -= mod_pos(hi - r, D);
-            long long lo = t - static_cast<long long>(S - 1) * D;
+        const int span = (S - 1) * D;        // host guarantees span + L < 2^31
+        const int nsteps = span + L;
+        int r = 0;                           // r == t mod D, kept incrementally
+        for (int t = 0; t < nsteps; ++t, r = (r + 1 == D) ? 0 : r + 1) {
+            // active levels: lo, lo + D, ..., hi (all congruent to t mod D)
+            int hi, lo = t - span;
             if (lo < r) lo = r;
-            lo += mod_pos(r - lo, D);
-            if (hi < lo) continue;  // no vertex of any sweep sits on this step
-            const int b = __ldg(p.level_begin + lo);
-            const int e = __ldg(p.level_end + hi);
-            for (int base = b + warp_first_group; base < e; base += ngroups) {
-                const int k = base + ((threadIdx.x & 31) / G);
-                update_vertex<MODE, G>(p, k < e ? __ldg(p.order + k) : -1);
+            int i0, i1;
+            if (SMEM) {
+                hi = t < L ? t : hitop[r];
+                if (hi < lo) continue;  // no vertex of any sweep sits on this step
+                i0 = lbeg[lo];
+                i1 = lend[hi];
+            } else {
+                hi = t < L ? t : (L - 1) - ((L - 1 - r) % D + D) % D;
+                if (hi < lo) continue;
+                i0 = owned_below(__ldg(p.level_begin + lo), c, nc);
+                i1 = owned_below(__ldg(p.level_end + hi), c, nc);
+            }
+            for (int base = i0 + warp_first_group; base < i1; base += groups) {
+                const int i = base + my_group;
+                int v = -1, deg = 0;
+                const int4* tri = nullptr;
+                if (i < i1) {
+                    if (SMEM) {
+                        v = lvid[i];
+                        deg = ldeg[i];
+                        tri = ltri + i * p.max_degree;
+                    } else {
+                        v = __ldg(p.order + c + i * nc);
+                        const int s0 = __ldg(p.slot_off + v);
+                        deg = __ldg(p.slot_off + v + 1) - s0;
+                        tri = p.slot_tri + s0;
+                    }
+                }
+                update_vertex<MODE, G, SMEM>(p, v, tri, deg);
             }
             if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
         }
@@ -325,23 +376,37 @@ __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
     for (int v = tid; v < p.n; v += nthreads) T::unpack(p.work, p.points, v);
 }
 
-template <int MODE, int G>
-int launch(const ArealParams& params, int n_ctas, int threads, cudaStream_t stream) {
-    auto kernel = areal_sweeps_kernel<MODE, G>;
-    int device = 0;
+constexpr size_t kMaxTopologySmem = 200 * 1024;
+
+template <int MODE, int G, bool SMEM>
+int launch_variant(ArealParams params, int n_ctas, int threads, size_t smem, cudaStream_t stream) {
+    auto kernel = areal_sweeps_kernel<MODE, G, SMEM>;
+    int device = 0, sms = 0, per_sm = 0;
     CSG_CUDA_CHECK(cudaGetDevice(&device));
-    int sms = 0, per_sm = 0;
     CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
-    if (n_ctas <= 0) n_ctas = sms;
+    if (SMEM) CSG_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
     if (per_sm < 1 || n_ctas > per_sm * sms)
-        return csg::fail(CSG_ERR_LAUNCH, "areal sweeps: %d CTAs x %d threads cannot be co-resident (%d per SM, %d SMs)",
-                         n_ctas, threads, per_sm, sms);
-    ArealParams local = params;
-    void* args[] = {&local};
+        return csg::fail(CSG_ERR_LAUNCH, "areal sweeps: %d CTAs x %d threads (%zu B smem) cannot be co-resident (%d per SM, %d SMs)",
+                         n_ctas, threads, smem, per_sm, sms);
+    void* args[] = {&params};
     CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(n_ctas), dim3(threads), args,
-                                               0, stream));
+                                               smem, stream));
     return CSG_OK;
+}
+
+template <int MODE, int G>
+int launch(ArealParams params, int n_ctas, int threads, cudaStream_t stream) {
+    int device = 0, sms = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    if (n_ctas <= 0) n_ctas = sms;
+    params.nloc_max = (params.n + n_ctas - 1) / n_ctas;
+    const size_t smem = static_cast<size_t>(params.nloc_max) * (params.max_degree * sizeof(int4) + 2 * sizeof(int)) +
+                        sizeof(int) * (2 * static_cast<size_t>(params.n_levels) + params.stride);
+    if (params.max_degree > 0 && smem <= kMaxTopologySmem)
+        return launch_variant<MODE, G, true>(params, n_ctas, threads, smem, stream);
+    return launch_variant<MODE, G, false>(params, n_ctas, threads, 0, stream);
 }
 
 template <int MODE>
@@ -375,14 +440,20 @@ size_t csg_areal_scratch_bytes(int n_vertices, int arithmetic) {
 
 int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, const int32_t* slot_tri,
                      const int32_t* order, const int32_t* level_begin, const int32_t* level_end, int n_levels,
-                     int level_stride, int iterations, int project_every, double radius, int arithmetic, void* scratch,
+                     int level_stride, int max_degree, int iterations, int project_every, double radius, int arithmetic, void* scratch,
                      size_t scratch_bytes, int n_ctas, int threads_per_cta, int lanes_per_vertex, double timeout_s,
                      csg_stream_t stream) {
     if (!points || n_vertices < 1 || !slot_off || !order || !level_begin || !level_end || !scratch)
         return csg::fail(CSG_ERR_ARG, "areal sweeps: null pointer or empty mesh");
-    if (n_levels < 1 || n_levels > n_vertices || level_stride < 1 || iterations < 1 || project_every < 0)
+    if (n_levels < 1 || n_levels > n_vertices || level_stride < 1 || iterations < 1 || project_every < 0 ||
+        max_degree < 0)
         return csg::fail(CSG_ERR_ARG, "areal sweeps: bad schedule (levels %d, stride %d, iterations %d, project %d)",
                          n_levels, level_stride, iterations, project_every);
+    {
+        const long long sweeps_per_epoch = project_every > 0 ? project_every : iterations;
+        if ((sweeps_per_epoch - 1) * static_cast<long long>(level_stride) + n_levels >= (1LL << 31))
+            return csg::fail(CSG_ERR_ARG, "areal sweeps: wavefront epoch longer than 2^31 steps");
+    }
     if (arithmetic < CSG_ARITH_CAT || arithmetic > CSG_ARITH_FP64)
         return csg::fail(CSG_ERR_ARG, "areal sweeps: unknown arithmetic %d", arithmetic);
     if (scratch_bytes < csg_areal_scratch_bytes(n_vertices, arithmetic))
@@ -390,7 +461,7 @@ int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, cons
                          csg_areal_scratch_bytes(n_vertices, arithmetic));
     if (reinterpret_cast<uintptr_t>(scratch) % 256 != 0 || reinterpret_cast<uintptr_t>(slot_tri) % 16 != 0)
         return csg::fail(CSG_ERR_ARG, "areal sweeps: scratch must be 256-byte and slot_tri 16-byte aligned");
-    if (threads_per_cta <= 0) threads_per_cta = 256;
+    if (threads_per_cta <= 0) threads_per_cta = 512;
     if (lanes_per_vertex <= 0) lanes_per_vertex = 8;
     if (threads_per_cta % 32 != 0 || threads_per_cta > 512)
         return csg::fail(CSG_ERR_ARG, "areal sweeps: threads_per_cta must be a multiple of 32 up to 512");
@@ -408,6 +479,7 @@ int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, cons
     p.n = n_vertices;
     p.n_levels = n_levels;
     p.stride = level_stride;
+    p.max_degree = max_degree;
     p.iterations = iterations;
     p.project_every = project_every;
     p.radius = radius;

@@ -214,7 +214,7 @@ def _resolve_dtype(dtype: str | torch.dtype) -> torch.dtype:
     return result
 
 
-DEFAULT_LAUNCH = {"n_ctas": 0, "threads_per_cta": 256, "lanes_per_vertex": 8}
+DEFAULT_LAUNCH = {"n_ctas": 0, "threads_per_cta": 512, "lanes_per_vertex": 8}
 
 
 def areal_sweeps_device(
@@ -250,7 +250,7 @@ def areal_sweeps_device(
         lib.csg_areal_sweeps(
             _native.ptr(points), n, _native.ptr(plan_device["slot_off"]), _native.ptr(plan_device["slot_tri"]),
             _native.ptr(plan_device["order"]), _native.ptr(plan_device["level_begin"]),
-            _native.ptr(plan_device["level_end"]), plan.n_levels, plan.level_stride, int(iterations),
+            _native.ptr(plan_device["level_end"]), plan.n_levels, plan.level_stride, plan.max_degree, int(iterations),
             int(project_every), float(radius), mode, _native.ptr(scratch), scratch.numel(),
             int(cfg["n_ctas"]), int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s),
             _native.stream_handle(stream),

@@ -102,7 +102,9 @@ CSG_API int csg_areal_plan_build(int n_vertices, const int32_t *faces, int n_fac
  * s % project_every == 0.  One persistent cooperative launch.
  * points: device float32 [n,3] (CSG_ARITH_CAT / _FP32) or float64 [n,3]
  * (CSG_ARITH_FP64), updated in place.  Plan arrays are device copies of
- * csg_areal_plan_build's outputs.  n_ctas / threads_per_cta /
+ * csg_areal_plan_build's outputs (max_degree from its info: the largest
+ * incident-face count; each CTA caches its vertices' face slots in shared
+ * memory when they fit).  n_ctas / threads_per_cta /
  * lanes_per_vertex of 0 pick defaults; timeout_s bounds every device wait.
  * The kernel's status lands in scratch; read it with csg_read_status.
  * ---------------------------------------------------------------------- */
@@ -110,7 +112,7 @@ CSG_API size_t csg_areal_scratch_bytes(int n_vertices, int arithmetic);
 
 CSG_API int csg_areal_sweeps(void *points, int n_vertices, const int32_t *slot_off, const int32_t *slot_tri,
                      const int32_t *order, const int32_t *level_begin, const int32_t *level_end, int n_levels,
-                     int level_stride, int iterations, int project_every, double radius, int arithmetic, void *scratch,
+                     int level_stride, int max_degree, int iterations, int project_every, double radius, int arithmetic, void *scratch,
                      size_t scratch_bytes, int n_ctas, int threads_per_cta, int lanes_per_vertex, double timeout_s,
                      csg_stream_t stream);
 
