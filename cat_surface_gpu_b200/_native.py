@@ -23,6 +23,8 @@ CSG_ERR_UNSUPPORTED = -6
 CSG_ERR_COVERAGE = -7
 
 ARITH = {"cat": 0, "fp32": 1, "fp64": 2}
+CSG_DTYPE_F32 = 0
+CSG_DTYPE_F64 = 1
 
 _P = c_void_p
 _I = c_int
@@ -42,6 +44,23 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         [_P, _I, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, c_double, _I, _P, c_size_t, _I, _I, _I, c_double, _P],
     ),
     "csg_selftest_barrier_timeout": (_I, [_P, c_size_t, c_double, _P]),
+    "csg_dartel_scratch_bytes": (c_size_t, [_I, _I, _I, _I]),
+    "csg_dartel_solve": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _I, c_double, _I, _I, _I, _I, _P, c_size_t, _P]),
+    "csg_dartel_step": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _I, _P, c_double, _I, _I, _I, _I, _P, c_size_t, _P]),
+    "csg_dartel_smalldef": (_I, [_I, _I, _I, _I, _P, c_double, _P, _P, _P]),
+    "csg_dartel_compose": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "csg_dartel_jac_div": (_I, [_I, _I, _I, _I, _P, _P, c_double, _P, _P]),
+    "csg_dartel_objfun": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, c_size_t, _P]),
+    "csg_dartel_squaring": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P, c_size_t, _P]),
+    "csg_dartel_regularization": (_I, [_I, _I, _I, _I, _P, _P, _I, _P, _P]),
+    "csg_dartel_membrane_apply": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P]),
+    "csg_dartel_relax": (_I, [_I, _I, _I, _I, _P, _P, _P, _I, _P, _P]),
+    "csg_dartel_resize": (_I, [_I, _I, _I, _I, _P, _I, _I, _P, _I, _P]),
+    "csg_dartel_fmg": (_I, [_I, _I, _I, _I, _P, _P, _P, _I, _I, _P, _I, _I, _P, c_size_t, _P]),
+    "csg_dartel_expdef": (_I, [_I, _I, _I, _I, _P, _I, _P, _P, _P, c_size_t, _P]),
+    "csg_dartel_sample": (_I, [_I, _I, _I, _P, _I, _P, _P, _P, _P]),
+    "csg_apply_flow_to_sphere": (_I, [_I, _I, _P, _I, _I, _P, _I, _P, _P]),
+    "csg_average_xz": (_I, [_I, _P, _P, _P, _P]),
     "csg_read_status": (_I, [_P, _P, _P, _P]),
 }
 
@@ -117,3 +136,10 @@ def stream_handle(stream=None) -> int:
     if stream is None:
         stream = torch.cuda.current_stream()
     return int(stream.cuda_stream)
+
+
+def doubles(values) -> "ctypes.Array":
+    """A C array of doubles (kept alive by the caller for the call's duration)."""
+
+    values = [float(v) for v in values]
+    return (ctypes.c_double * len(values))(*values)

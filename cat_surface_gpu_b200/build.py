@@ -42,7 +42,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     nvcc = os.environ.get("NVCC", "nvcc")
     objdir = HERE / "_build"
     objdir.mkdir(exist_ok=True)
-    common = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", *ARCH]
+    common = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", *ARCH]
     if verbose:
         common += ["-Xptxas", "-v"]
     objects = []

@@ -1,0 +1,1242 @@
+// 2-D DARTEL on the spherical lat-lon sheet, batched, for sm_100a.
+//
+// Every kernel works on a batch of B independent grids of the same size
+// (fields laid out [B][channels][ny][nx], contiguous).  Arithmetic follows
+// the reference's torch path operation by operation
+// (src/cat_surface_gpu/dartel_grid.py, surface_warp.py); this file is
+// compiled with --fmad=false so each multiply and add rounds once, which
+// makes float64 and float32 results bit-identical to a sequential
+// restatement with the same association order.
+//
+// Boundary rule (dartel_grid.py:190-208): x periodic, y reflected with
+// period 2 ny (ny == 1 collapses y to row 0).  Maps are one-based; Jacobians
+// are stored (j00, j10, j01, j11).
+//
+// The host half of this file orchestrates dartel_step (dartel_grid.py:
+// 1420-1616), the membrane full multigrid (1211-1417) and the whole solve
+// (surface_warp.py:239-367) as launch sequences on one stream, so a caller
+// can capture a complete solve in one CUDA graph.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/catsurf_b200.h"
+#include "errors.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ int wrap_x(int ix, int nx) {
+    int r = ix % nx;
+    return r < 0 ? r + nx : r;
+}
+
+__device__ __forceinline__ int reflect_y(int iy, int ny) {
+    if (ny == 1) return 0;
+    const int period = 2 * ny;
+    int r = iy % period;
+    if (r < 0) r += period;
+    return r >= ny ? period - r - 1 : r;
+}
+
+// Bilinear stencil of dartel_grid.py:348-366 at (x, y) (zero-based).
+template <typename T>
+struct Stencil {
+    int i22, i12, i21, i11;  // flat offsets inside one channel
+    T dx1, dx2, dy1, dy2;
+    __device__ __forceinline__ Stencil(T x, T y, int nx, int ny) {
+        const T fx = floor(x), fy = floor(y);
+        const int ix = static_cast<int>(fx), iy = static_cast<int>(fy);
+        dx1 = x - static_cast<T>(ix);
+        dy1 = y - static_cast<T>(iy);
+        dx2 = T(1) - dx1;
+        dy2 = T(1) - dy1;
+        const int x0 = wrap_x(ix, nx), x1 = wrap_x(ix + 1, nx);
+        const int y0 = reflect_y(iy, ny), y1 = reflect_y(iy + 1, ny);
+        i22 = y0 * nx + x0;
+        i12 = y0 * nx + x1;
+        i21 = y1 * nx + x0;
+        i11 = y1 * nx + x1;
+    }
+    __device__ __forceinline__ T interp(const T* f) const {
+        return (f[i22] * dx2 + f[i12] * dx1) * dy2 + (f[i21] * dx2 + f[i11] * dx1) * dy1;
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ T unwrap(T c, T c22, T period) {
+    return c - floor((c - c22) / period + T(0.5)) * period;
+}
+
+struct Pt {
+    int b, x, y, i;  // batch, column, row, flat index in a channel
+};
+
+__device__ __forceinline__ bool point(int nx, int ny, Pt& p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx * ny) return false;
+    p.b = blockIdx.y;
+    p.i = i;
+    p.x = i % nx;
+    p.y = i / nx;
+    return true;
+}
+
+// Neighbour offsets with the boundary rule.
+__device__ __forceinline__ int nb(int x, int y, int dx, int dy, int nx, int ny) {
+    return reflect_y(y + dy, ny) * nx + wrap_x(x + dx, nx);
+}
+
+// ---------------------------------------------------------------- kernels
+
+// map = id + v * s (dartel_grid.py:655-675 / 1644-1645) and
+// jac = jacobian_of_displacement(v, s) (624-652); either output may be null.
+template <typename T>
+__global__ void k_smalldef(const T* __restrict__ v, T* __restrict__ map, T* __restrict__ jac, int nx, int ny, T s,
+                           T hs) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const T* vx = v + static_cast<size_t>(p.b) * 2 * P;
+    const T* vy = vx + P;
+    if (map) {
+        T* m = map + static_cast<size_t>(p.b) * 2 * P;
+        m[p.i] = static_cast<T>(p.x + 1) + vx[p.i] * s;
+        m[P + p.i] = static_cast<T>(p.y + 1) + vy[p.i] * s;
+    }
+    if (jac) {
+        const int xm = nb(p.x, p.y, -1, 0, nx, ny), xp = nb(p.x, p.y, 1, 0, nx, ny);
+        const int ym = nb(p.x, p.y, 0, -1, nx, ny), yp = nb(p.x, p.y, 0, 1, nx, ny);
+        T* j = jac + static_cast<size_t>(p.b) * 4 * P;
+        j[p.i] = (vx[xm] * T(-1) + vx[xp]) * hs + T(1);
+        j[P + p.i] = (vy[xm] * T(-1) + vy[xp]) * hs;
+        j[2 * P + p.i] = (vx[ym] * T(-1) + vx[yp]) * hs;
+        j[3 * P + p.i] = (vy[ym] * T(-1) + vy[yp]) * hs + T(1);
+    }
+}
+
+// (c, jc) = (b o a, J_b(a) . J_a) (dartel_grid.py:407-507); jac pointers may be null.
+template <typename T>
+__global__ void k_compose(const T* __restrict__ a, const T* __restrict__ ja, const T* __restrict__ b,
+                          const T* __restrict__ jb, T* __restrict__ c, T* __restrict__ jc, int nx, int ny) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const size_t o2 = static_cast<size_t>(p.b) * 2 * P, o4 = static_cast<size_t>(p.b) * 4 * P;
+    const T* A = a + o2;
+    const T* Bm = b + o2;
+    const Stencil<T> st(A[p.i] - T(1), A[P + p.i] - T(1), nx, ny);
+    T* C = c + o2;
+#pragma unroll
+    for (int ch = 0; ch < 2; ++ch) {
+        const T* f = Bm + ch * P;
+        const T period = static_cast<T>(ch == 0 ? nx : ny);
+        const T c22 = f[st.i22] - T(1);
+        const T c12 = unwrap(f[st.i12] - T(1), c22, period);
+        const T c21 = unwrap(f[st.i21] - T(1), c22, period);
+        const T c11 = unwrap(f[st.i11] - T(1), c22, period);
+        C[ch * P + p.i] = (c22 * st.dx2 + c12 * st.dx1) * st.dy2 + (c21 * st.dx2 + c11 * st.dx1) * st.dy1 + T(1);
+    }
+    if (jc) {
+        const T* JA = ja + o4;
+        const T* JB = jb + o4;
+        const T jb00 = st.interp(JB), jb01 = st.interp(JB + P), jb10 = st.interp(JB + 2 * P),
+                jb11 = st.interp(JB + 3 * P);
+        const T ja0 = JA[p.i], ja1 = JA[P + p.i], ja2 = JA[2 * P + p.i], ja3 = JA[3 * P + p.i];
+        T* J = jc + o4;
+        J[p.i] = jb00 * ja0 + jb10 * ja1;
+        J[P + p.i] = jb01 * ja0 + jb11 * ja1;
+        J[2 * P + p.i] = jb00 * ja2 + jb10 * ja3;
+        J[3 * P + p.i] = jb01 * ja2 + jb11 * ja3;
+    }
+}
+
+// jac_div_smalldef (dartel_grid.py:678-720) at one point.
+template <typename T>
+__device__ __forceinline__ void jacdiv_at(const T* J, const T* vx, const T* vy, const Pt& p, int nx, int ny, T hs,
+                                          T out[4]) {
+    const int P = nx * ny;
+    const int xm = nb(p.x, p.y, -1, 0, nx, ny), xp = nb(p.x, p.y, 1, 0, nx, ny);
+    const int ym = nb(p.x, p.y, 0, -1, nx, ny), yp = nb(p.x, p.y, 0, 1, nx, ny);
+    const T d00 = (vx[xm] * T(-1) + vx[xp]) * hs + T(1);
+    const T d10 = (vy[xm] * T(-1) + vy[xp]) * hs;
+    const T d01 = (vx[ym] * T(-1) + vx[yp]) * hs;
+    const T d11 = (vy[ym] * T(-1) + vy[yp]) * hs + T(1);
+    const T det = d00 * d11 - d01 * d10;
+    const T i00 = d11 / det, i10 = -d10 / det, i01 = -d01 / det, i11 = d00 / det;
+    const T o00 = J[p.i], o10 = J[P + p.i], o01 = J[2 * P + p.i], o11 = J[3 * P + p.i];
+    out[0] = o00 * i00 + o01 * i10;
+    out[1] = o10 * i00 + o11 * i10;
+    out[2] = o00 * i01 + o01 * i11;
+    out[3] = o10 * i01 + o11 * i11;
+}
+
+template <typename T>
+__global__ void k_jacdiv(const T* __restrict__ jac, const T* __restrict__ v, T* __restrict__ out, int nx, int ny,
+                         T hs) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const T* vx = v + static_cast<size_t>(p.b) * 2 * P;
+    T r[4];
+    jacdiv_at(jac + static_cast<size_t>(p.b) * 4 * P, vx, vx + P, p, nx, ny, hs, r);
+    T* o = out + static_cast<size_t>(p.b) * 4 * P;
+    for (int k = 0; k < 4; ++k) o[k * P + p.i] = r[k];
+}
+
+// Block-level deterministic sum; partial[b * gridDim.x + blockIdx.x].
+template <typename T>
+__device__ __forceinline__ void block_sum(T value, T* partial) {
+    __shared__ T buf[kThreads];
+    buf[threadIdx.x] = value;
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) buf[threadIdx.x] = buf[threadIdx.x] + buf[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[static_cast<size_t>(blockIdx.y) * gridDim.x + blockIdx.x] = buf[0];
+}
+
+// initialise_objfun (dartel_grid.py:723-775), optionally preceded by
+// jac_div_smalldef (dartel_step's use, 1497-1512 / 1546-1561).  weights may
+// be null (all ones).  Writes rhs [2], hess [3] and the objective partials.
+template <typename T, bool JACDIV>
+__global__ void k_objfun(const T* __restrict__ source, const T* __restrict__ target, const T* __restrict__ map,
+                         const T* __restrict__ jac, const T* __restrict__ v, const T* __restrict__ weights,
+                         T* __restrict__ rhs, T* __restrict__ hess, T* __restrict__ partial, int nx, int ny, T hs) {
+    Pt p;
+    const bool ok = point(nx, ny, p);
+    T contrib = T(0);
+    if (ok) {
+        const int P = nx * ny;
+        const size_t o1 = static_cast<size_t>(p.b) * P;
+        const T* src = source + o1;
+        const T* M = map + 2 * o1;
+        T J[4];
+        if (JACDIV) {
+            const T* vx = v + 2 * o1;
+            jacdiv_at(jac + 4 * o1, vx, vx + P, p, nx, ny, hs, J);
+        } else {
+            const T* JJ = jac + 4 * o1;
+            for (int k = 0; k < 4; ++k) J[k] = JJ[k * P + p.i];
+        }
+        const Stencil<T> st(M[p.i] - T(1), M[P + p.i] - T(1), nx, ny);
+        const T k22 = src[st.i22], k12 = src[st.i12], k21 = src[st.i21], k11 = src[st.i11];
+        const T sampled = (k22 * st.dx2 + k12 * st.dx1) * st.dy2 + (k21 * st.dx2 + k11 * st.dx1) * st.dy1;
+        const T diff = sampled - target[o1 + p.i];
+        const T ddx = (k11 - k21) * st.dy1 + (k12 - k22) * st.dy2;
+        const T ddy = (k11 * st.dx1 + k21 * st.dx2) - (k12 * st.dx1 + k22 * st.dx2);
+        const T gx = J[0] * ddx + J[1] * ddy;
+        const T gy = J[2] * ddx + J[3] * ddy;
+        const T w = weights ? weights[o1 + p.i] : T(1);
+        T* H = hess + 3 * o1;
+        T* R = rhs + 2 * o1;
+        H[p.i] = gx * gx * w;
+        H[P + p.i] = gy * gy * w;
+        H[2 * P + p.i] = gx * gy * w;
+        R[p.i] = gx * diff * w;
+        R[P + p.i] = gy * diff * w;
+        contrib = diff * diff * w;
+    }
+    if (partial) block_sum(contrib, partial);
+}
+
+// One scaling-and-squaring increment (dartel_grid.py:832-893; the fused
+// form of dartel_triton.py:345-477): b_out = b + inc_b, a_out = a + inc_a,
+// inc = inc_b.  Out of place (the gathers read b and a at other points).
+template <typename T>
+__global__ void k_squaring(const T* __restrict__ b, const T* __restrict__ a, const T* __restrict__ map,
+                           const T* __restrict__ jac, T* __restrict__ b_out, T* __restrict__ a_out,
+                           T* __restrict__ inc, int nx, int ny) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const size_t o1 = static_cast<size_t>(p.b) * P;
+    const T* M = map + 2 * o1;
+    const T* J = jac + 4 * o1;
+    const T* Bv = b + 2 * o1;
+    const T* Av = a + 3 * o1;
+    const Stencil<T> st(M[p.i] - T(1), M[P + p.i] - T(1), nx, ny);
+    const T j00 = J[p.i], j10 = J[P + p.i], j01 = J[2 * P + p.i], j11 = J[3 * P + p.i];
+    const T det = j00 * j11 - j01 * j10;
+    const T sbx = st.interp(Bv), sby = st.interp(Bv + P);
+    const T sa00 = st.interp(Av), sa11 = st.interp(Av + P), sa01 = st.interp(Av + 2 * P);
+    const T ibx = det * (sbx * j00 + sby * j10);
+    const T iby = det * (sbx * j01 + sby * j11);
+    const T t1 = sa00 * j00 + sa01 * j10;
+    const T t2 = sa01 * j00 + sa11 * j10;
+    const T t3 = sa00 * j01 + sa01 * j11;
+    const T t4 = sa01 * j01 + sa11 * j11;
+    const T ia00 = det * (t1 * j00 + t2 * j10);
+    const T ia11 = det * (t3 * j01 + t4 * j11);
+    const T ia01 = det * (t1 * j01 + t2 * j11);
+    T* BO = b_out + 2 * o1;
+    T* AO = a_out + 3 * o1;
+    BO[p.i] = Bv[p.i] + ibx;
+    BO[P + p.i] = Bv[P + p.i] + iby;
+    AO[p.i] = Av[p.i] + ia00;
+    AO[P + p.i] = Av[P + p.i] + ia11;
+    AO[2 * P + p.i] = Av[2 * P + p.i] + ia01;
+    T* I = inc + 2 * o1;
+    I[p.i] = ibx;
+    I[P + p.i] = iby;
+}
+
+// regularization_operator weights (dartel_grid.py:937-1015), host-computed
+// in float64 exactly as the reference forms them, cast to T on use.
+//   rtype 1: w00, w01, w10
+//   rtype 0: wx0, wy0, wx1, wy1, wx2, wy2, wxy
+//   rtype 2: w00, w01, w02, w10, w11, w20
+struct RegWeights {
+    double w[8];
+};
+
+RegWeights reg_weights(const double* params, int rtype) {
+    const double sx = params[0], sy = params[1], mu = params[2], lam = params[3], id = params[4];
+    const double sx2 = sx * sx, sy2 = sy * sy;
+    RegWeights r{};
+    if (rtype == 1) {
+        r.w[0] = mu * (2.0 * sx2 + 2.0 * sy2) + id;
+        r.w[1] = -mu * sy2;
+        r.w[2] = -mu * sx2;
+    } else if (rtype == 0) {
+        r.w[0] = mu * (2.0 * sy2 + 4.0 * sx2) + 2.0 * lam * sx2 + id;
+        r.w[1] = mu * (2.0 * sx2 + 4.0 * sy2) + 2.0 * lam * sy2 + id;
+        r.w[2] = -(2.0 * mu + lam) * sx2;
+        r.w[3] = -(2.0 * mu + lam) * sy2;
+        r.w[4] = -mu * sx2;
+        r.w[5] = -mu * sy2;
+        r.w[6] = 0.25 * (lam + mu) * sx * sy;
+    } else {
+        const double sx4 = sx2 * sx2, sy4 = sy2 * sy2;
+        r.w[0] = mu * (6.0 * sx4 + 6.0 * sy4 + 8.0 * sx2 * sy2) + id;
+        r.w[1] = mu * (-4.0 * sx2 * sy2 - 4.0 * sy4);
+        r.w[2] = mu * sy4;
+        r.w[3] = mu * (-4.0 * sx4 - 4.0 * sx2 * sy2);
+        r.w[4] = mu * (2.0 * sx2 * sy2);
+        r.w[5] = mu * sx4;
+    }
+    return r;
+}
+
+// Membrane weights as relax_membrane / the Triton kernels form them
+// (dartel_grid.py:1113-1116): w00 = mu (2 sx sx + 2 sy sy) + id.
+struct MemWeights {
+    double w00, w01, w10;
+};
+
+MemWeights mem_weights(const double* params) {
+    const double sx = params[0], sy = params[1], mu = params[2], id = params[4];
+    return {mu * (2.0 * sx * sx + 2.0 * sy * sy) + id, -mu * sy * sy, -mu * sx * sx};
+}
+
+template <typename T>
+__device__ __forceinline__ void regularise_at(const T* vx, const T* vy, const Pt& p, int nx, int ny, int rtype,
+                                              const RegWeights& rw, T out[2]) {
+    auto at = [&](const T* f, int dx, int dy) { return f[nb(p.x, p.y, dx, dy, nx, ny)]; };
+    const T* f[2] = {vx, vy};
+    if (rtype == 1) {
+        const T w00 = T(rw.w[0]), w01 = T(rw.w[1]), w10 = T(rw.w[2]);
+        for (int c = 0; c < 2; ++c)
+            out[c] = w00 * f[c][p.i] + w01 * (at(f[c], 0, -1) + at(f[c], 0, 1)) + w10 * (at(f[c], -1, 0) + at(f[c], 1, 0));
+    } else if (rtype == 0) {
+        const T wx0 = T(rw.w[0]), wy0 = T(rw.w[1]), wx1 = T(rw.w[2]), wy1 = T(rw.w[3]), wx2 = T(rw.w[4]),
+                wy2 = T(rw.w[5]), wxy = T(rw.w[6]);
+        const T cross_x = at(vy, -1, -1) - at(vy, -1, 1) - at(vy, 1, -1) + at(vy, 1, 1);
+        const T cross_y = at(vx, -1, -1) - at(vx, -1, 1) - at(vx, 1, -1) + at(vx, 1, 1);
+        out[0] = wx0 * vx[p.i] + wy2 * (at(vx, 0, -1) + at(vx, 0, 1)) + wx1 * (at(vx, -1, 0) + at(vx, 1, 0)) +
+                 wxy * cross_x;
+        out[1] = wy0 * vy[p.i] + wy1 * (at(vy, 0, -1) + at(vy, 0, 1)) + wx2 * (at(vy, -1, 0) + at(vy, 1, 0)) +
+                 wxy * cross_y;
+    } else {
+        const T w00 = T(rw.w[0]), w01 = T(rw.w[1]), w02 = T(rw.w[2]), w10 = T(rw.w[3]), w11 = T(rw.w[4]),
+                w20 = T(rw.w[5]);
+        for (int c = 0; c < 2; ++c) {
+            const T* g = f[c];
+            out[c] = w00 * g[p.i] + w01 * (at(g, 0, -1) + at(g, 0, 1)) + w02 * (at(g, 0, -2) + at(g, 0, 2)) +
+                     w10 * (at(g, -1, 0) + at(g, 1, 0)) +
+                     w11 * (at(g, -1, -1) + at(g, 1, -1) + at(g, -1, 1) + at(g, 1, 1)) +
+                     w20 * (at(g, -2, 0) + at(g, 2, 0));
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_regularise(const T* __restrict__ v, T* __restrict__ out, int nx, int ny, int rtype, RegWeights rw) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const T* vx = v + static_cast<size_t>(p.b) * 2 * P;
+    T r[2];
+    regularise_at(vx, vx + P, p, nx, ny, rtype, rw, r);
+    T* o = out + static_cast<size_t>(p.b) * 2 * P;
+    o[p.i] = r[0];
+    o[P + p.i] = r[1];
+}
+
+// dartel_step's combination (dartel_grid.py:1575-1594):
+//   code 1: rhs = (rhs_f - rhs_r) * s + reg(v), hess = (hess_f + hess_r) * s
+//   code 0: rhs = rhs_f * s + reg(v),           hess = hess_f * s
+// plus the partial sums of reg(v) . v and rhs . rhs (metrics).
+template <typename T>
+__global__ void k_combine(const T* __restrict__ rf, const T* __restrict__ rr, const T* __restrict__ hf,
+                          const T* __restrict__ hr, const T* __restrict__ v, T* __restrict__ rhs, T* __restrict__ hess,
+                          T* __restrict__ partial_reg, T* __restrict__ partial_norm, int nx, int ny, T s, RegWeights rw) {
+    Pt p;
+    const bool ok = point(nx, ny, p);
+    T reg_dot = T(0), norm = T(0);
+    if (ok) {
+        const int P = nx * ny;
+        const size_t o1 = static_cast<size_t>(p.b) * P;
+        const T* vx = v + 2 * o1;
+        T reg[2];
+        regularise_at(vx, vx + P, p, nx, ny, 1, rw, reg);
+        for (int c = 0; c < 2; ++c) {
+            const T base = rr ? rf[2 * o1 + c * P + p.i] - rr[2 * o1 + c * P + p.i] : rf[2 * o1 + c * P + p.i];
+            const T r = base * s + reg[c];
+            rhs[2 * o1 + c * P + p.i] = r;
+            norm = norm + r * r;
+            reg_dot = reg_dot + reg[c] * vx[c * P + p.i];
+        }
+        for (int c = 0; c < 3; ++c) {
+            const T base = hr ? hf[3 * o1 + c * P + p.i] + hr[3 * o1 + c * P + p.i] : hf[3 * o1 + c * P + p.i];
+            hess[3 * o1 + c * P + p.i] = base * s;
+        }
+    }
+    block_sum(reg_dot, partial_reg);
+    block_sum(norm, partial_norm);
+}
+
+// (H + L_membrane) u (dartel_grid.py:1018-1070); with `b`, the residual b - (H + L) u.
+template <typename T>
+__global__ void k_membrane_apply(const T* __restrict__ hess, const T* __restrict__ u, const T* __restrict__ b,
+                                 T* __restrict__ out, int nx, int ny, RegWeights rw) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const size_t o1 = static_cast<size_t>(p.b) * P;
+    const T* ux = u + 2 * o1;
+    const T* H = hess + 3 * o1;
+    T reg[2];
+    regularise_at(ux, ux + P, p, nx, ny, 1, rw, reg);
+    const T u0 = ux[p.i], u1 = ux[P + p.i];
+    const T a0 = reg[0] + H[p.i] * u0 + H[2 * P + p.i] * u1;
+    const T a1 = reg[1] + H[2 * P + p.i] * u0 + H[P + p.i] * u1;
+    T* o = out + 2 * o1;
+    if (b) {
+        o[p.i] = b[2 * o1 + p.i] - a0;
+        o[P + p.i] = b[2 * o1 + P + p.i] - a1;
+    } else {
+        o[p.i] = a0;
+        o[P + p.i] = a1;
+    }
+}
+
+// One red-black half sweep, in place (dartel_grid.py:1187-1208 /
+// dartel_triton.py:242-291): cells with ((x + y) & 1) == colour.  Exact for
+// even nx and for nx == 1, where every neighbour read is either of the other
+// colour or the cell itself.
+template <typename T>
+__global__ void k_relax(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u, int nx, int ny,
+                        int colour, T w00, T w01, T w10) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    if (((p.x + p.y) & 1) != colour) return;
+    const int P = nx * ny;
+    const size_t o1 = static_cast<size_t>(p.b) * P;
+    T* ux = u + 2 * o1;
+    T* uy = ux + P;
+    const int xm = nb(p.x, p.y, -1, 0, nx, ny), xp = nb(p.x, p.y, 1, 0, nx, ny);
+    const int ym = nb(p.x, p.y, 0, -1, nx, ny), yp = nb(p.x, p.y, 0, 1, nx, ny);
+    const T rx = b[2 * o1 + p.i] - w01 * (ux[ym] + ux[yp]) - w10 * (ux[xm] + ux[xp]);
+    const T ry = b[2 * o1 + P + p.i] - w01 * (uy[ym] + uy[yp]) - w10 * (uy[xm] + uy[xp]);
+    const T* H = hess + 3 * o1;
+    const T dxx = H[p.i] + w00;
+    const T dyy = H[P + p.i] + w00;
+    const T cr = H[2 * P + p.i];
+    const T det = dxx * dyy * T(1.0000000001) - cr * cr;
+    const T nxv = (dyy * rx - cr * ry) / det;
+    const T nyv = (-cr * rx + dxx * ry) / det;
+    ux[p.i] = nxv;
+    uy[p.i] = nyv;
+}
+
+// Direct 2x2 point solve of the coarsest level (dartel_grid.py:1318-1334).
+template <typename T>
+__global__ void k_point_solve(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u, int P, T id) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const size_t o1 = static_cast<size_t>(blockIdx.y) * P;
+    const T* H = hess + 3 * o1;
+    const T dxx = H[i] + id, dyy = H[P + i] + id, cr = H[2 * P + i];
+    const T det = dxx * dyy * T(1.0000000001) - cr * cr;
+    const T b0 = b[2 * o1 + i], b1 = b[2 * o1 + P + i];
+    u[2 * o1 + i] = (dyy * b0 - cr * b1) / det;
+    u[2 * o1 + P + i] = (-cr * b0 + dxx * b1) / det;
+}
+
+template <typename T>
+__device__ __forceinline__ T wt2(T d) {
+    const T a = fabs(d);
+    const T inner = T(0.75) - a * a;
+    const T od = T(1.5) - a;
+    const T outer = T(0.5) * od * od;
+    return a < T(0.5) ? inner : (a < T(1.5) ? outer : T(0));
+}
+
+// Separable quadratic B-spline resize (dartel_grid.py:239-305), y pass then
+// x pass, per target point; `accumulate` adds into dst (prolongation,
+// dartel_grid.py:1380-1387).  Fields are [B * C][sny][snx] -> [B * C][tny][tnx].
+template <typename T>
+__global__ void k_resize(const T* __restrict__ src, T* __restrict__ dst, int snx, int sny, int tnx, int tny,
+                         int accumulate) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= tnx * tny) return;
+    const int x = i % tnx, y = i / tnx;
+    const T* f = src + static_cast<size_t>(blockIdx.y) * snx * sny;
+    const T yl = (static_cast<T>(y) + T(0.5)) * static_cast<T>(sny) / static_cast<T>(tny) - T(0.5);
+    const int yo = static_cast<int>(floor(yl + T(0.5)));
+    const T yof = static_cast<T>(yo);
+    const T yw = wt2(yof - yl), ywm = wt2(yof - T(1) - yl), ywp = wt2(yof + T(1) - yl);
+    const int rm = reflect_y(yo - 1, sny) * snx, rc = reflect_y(yo, sny) * snx, rp = reflect_y(yo + 1, sny) * snx;
+    const T xl = (static_cast<T>(x) + T(0.5)) * static_cast<T>(snx) / static_cast<T>(tnx) - T(0.5);
+    const int xo = static_cast<int>(floor(xl + T(0.5)));
+    const T xof = static_cast<T>(xo);
+    const T xw = wt2(xof - xl), xwm = wt2(xof - T(1) - xl), xwp = wt2(xof + T(1) - xl);
+    const int cm = wrap_x(xo - 1, snx), cc = wrap_x(xo, snx), cp = wrap_x(xo + 1, snx);
+    const T im = ywm * f[rm + cm] + yw * f[rc + cm] + ywp * f[rp + cm];
+    const T ic = ywm * f[rm + cc] + yw * f[rc + cc] + ywp * f[rp + cc];
+    const T ip = ywm * f[rm + cp] + yw * f[rc + cp] + ywp * f[rp + cp];
+    const T r = xwm * im + xw * ic + xwp * ip;
+    T* o = dst + static_cast<size_t>(blockIdx.y) * tnx * tny;
+    o[i] = accumulate ? o[i] + r : r;
+}
+
+template <typename T>
+__global__ void k_sub(T* __restrict__ v, const T* __restrict__ u, size_t n) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = v[i] - u[i];
+}
+
+template <typename T>
+__global__ void k_any_nonzero(const T* __restrict__ u, size_t n, int* flag) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n && u[i] != T(0)) atomicOr(flag, 1);
+}
+
+// Fixed-order reduction of per-block partials into metrics[b * stride + slot]
+// (objective = forward + reverse partials; reg * 0.5; sqrt(norm)).
+template <typename T>
+__global__ void k_metrics(const T* __restrict__ obj_f, const T* __restrict__ obj_r, const T* __restrict__ reg,
+                          const T* __restrict__ norm, int nblocks, T* __restrict__ metrics, int metric_stride) {
+    const int b = blockIdx.x;
+    if (threadIdx.x != 0) return;
+    T of = T(0), orv = T(0), rg = T(0), nm = T(0);
+    for (int k = 0; k < nblocks; ++k) {
+        of = of + obj_f[static_cast<size_t>(b) * nblocks + k];
+        if (obj_r) orv = orv + obj_r[static_cast<size_t>(b) * nblocks + k];
+        rg = rg + reg[static_cast<size_t>(b) * nblocks + k];
+        nm = nm + norm[static_cast<size_t>(b) * nblocks + k];
+    }
+    T* m = metrics + static_cast<size_t>(b) * metric_stride;
+    m[0] = obj_r ? T(0.5) * of + T(0.5) * orv : T(0.5) * of;
+    m[1] = rg * T(0.5);
+    m[2] = sqrt(nm);
+}
+
+template <typename T>
+__global__ void k_objective_out(const T* __restrict__ partial, int nblocks, T* __restrict__ out) {
+    if (threadIdx.x != 0) return;
+    T s = T(0);
+    for (int k = 0; k < nblocks; ++k) s = s + partial[static_cast<size_t>(blockIdx.x) * nblocks + k];
+    out[blockIdx.x] = T(0.5) * s;
+}
+
+// ------------------------------------------------------------- host side
+
+struct Arena {
+    char* base;
+    size_t size;
+    size_t used = 0;
+    bool ok = true;
+    template <typename T>
+    T* take(size_t count) {
+        const size_t bytes = (count * sizeof(T) + 255) & ~static_cast<size_t>(255);
+        if (used + bytes > size) {
+            ok = false;
+            return nullptr;
+        }
+        T* p = reinterpret_cast<T*>(base ? base + used : nullptr);
+        used += bytes;
+        return p;
+    }
+};
+
+inline dim3 grid_for(int points, int batch) { return dim3((points + kThreads - 1) / kThreads, batch); }
+
+std::vector<std::pair<int, int>> grid_levels(int nx, int ny) {
+    std::vector<std::pair<int, int>> specs{{nx, ny}};
+    while (specs.back().first >= 2 || specs.back().second >= 2) {
+        const auto prev = specs.back();
+        const std::pair<int, int> coarse{(prev.first + 1) / 2, (prev.second + 1) / 2};
+        specs.push_back(coarse);
+        if (coarse.first < 2 && coarse.second < 2) break;
+    }
+    return specs;
+}
+
+bool relax_supported(int nx) { return nx % 2 == 0 || nx == 1; }
+
+// Multigrid workspace for one (batch, nx, ny).
+template <typename T>
+struct FmgBuffers {
+    std::vector<std::pair<int, int>> specs;
+    std::vector<T*> A, B, B0, U, R;
+    int* flag = nullptr;
+    bool carve(Arena& ar, int batch, int nx, int ny) {
+        specs = grid_levels(nx, ny);
+        const size_t L = specs.size();
+        A.assign(L, nullptr);
+        B.assign(L, nullptr);
+        B0.assign(L, nullptr);
+        U.assign(L, nullptr);
+        R.assign(L, nullptr);
+        for (size_t l = 0; l < L; ++l) {
+            const size_t P = static_cast<size_t>(specs[l].first) * specs[l].second;
+            if (l > 0) {
+                A[l] = ar.take<T>(3 * P * batch);
+                B[l] = ar.take<T>(2 * P * batch);
+                B0[l] = ar.take<T>(2 * P * batch);
+                U[l] = ar.take<T>(2 * P * batch);
+            }
+            R[l] = ar.take<T>(2 * P * batch);
+        }
+        flag = ar.take<int>(1);
+        return ar.ok;
+    }
+};
+
+template <typename T>
+struct Fmg {
+    FmgBuffers<T>& buf;
+    int batch;
+    double base[5];
+    int cycles, nit;
+    cudaStream_t s;
+    int nx0, ny0;
+
+    void params_at(size_t l, double out[5]) const {
+        out[0] = base[0] * buf.specs[l].first / nx0;
+        out[1] = base[1] * buf.specs[l].second / ny0;
+        out[2] = base[2];
+        out[3] = base[3];
+        out[4] = base[4];
+    }
+    void relax(size_t l) {
+        const int nx = buf.specs[l].first, ny = buf.specs[l].second;
+        double pr[5];
+        params_at(l, pr);
+        const MemWeights w = mem_weights(pr);
+        for (int it = 0; it < 2 * nit; ++it)
+            k_relax<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(buf.A[l], buf.B[l], buf.U[l], nx, ny,
+                                                                      it % 2 == 0 ? 1 : 0, T(w.w00), T(w.w01), T(w.w10));
+    }
+    void resize(const T* src, size_t from, T* dst, size_t to, int channels, bool accumulate) {
+        const auto f = buf.specs[from], t = buf.specs[to];
+        k_resize<T><<<grid_for(t.first * t.second, batch * channels), kThreads, 0, s>>>(src, dst, f.first, f.second,
+                                                                                     t.first, t.second, accumulate);
+    }
+    void cycle(size_t start) {
+        const size_t last = buf.specs.size() - 1;
+        for (size_t l = start; l < last; ++l) {
+            relax(l);
+            const int nx = buf.specs[l].first, ny = buf.specs[l].second;
+            double pr[5];
+            params_at(l, pr);
+            k_membrane_apply<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(buf.A[l], buf.U[l], buf.B[l], buf.R[l], nx,
+                                                                               ny, reg_weights(pr, 1));
+            resize(buf.R[l], l, buf.B[l + 1], l + 1, 2, false);
+            const size_t P1 = static_cast<size_t>(buf.specs[l + 1].first) * buf.specs[l + 1].second;
+            cudaMemsetAsync(buf.U[l + 1], 0, 2 * P1 * batch * sizeof(T), s);
+        }
+        relax(last);
+        for (size_t l = last; l-- > start;) {
+            resize(buf.U[l + 1], l + 1, buf.U[l], l, 2, true);
+            relax(l);
+        }
+    }
+    // Solves into buf.U[0]; U[0] must already hold the initial guess (or
+    // zeros when `coarse_init`).  hess / rhs are level-0 A / B.
+    void run(bool coarse_init) {
+        const size_t L = buf.specs.size();
+        for (size_t l = 1; l < L; ++l) resize(buf.A[l - 1], l - 1, buf.A[l], l, 3, false);
+        if (coarse_init)
+            for (size_t l = 1; l < L; ++l) resize(l == 1 ? buf.B[0] : buf.B0[l - 1], l - 1, buf.B0[l], l, 2, false);
+        for (size_t l = 1; l < L; ++l) {
+            const size_t P = static_cast<size_t>(buf.specs[l].first) * buf.specs[l].second;
+            cudaMemsetAsync(buf.B[l], 0, 2 * P * batch * sizeof(T), s);
+            cudaMemsetAsync(buf.U[l], 0, 2 * P * batch * sizeof(T), s);
+        }
+        if (!coarse_init) {
+            for (int c = 0; c < cycles; ++c) cycle(0);
+            return;
+        }
+        const size_t last = L - 1;
+        const size_t Pl = static_cast<size_t>(buf.specs[last].first) * buf.specs[last].second;
+        k_point_solve<T><<<grid_for(static_cast<int>(Pl), batch), kThreads, 0, s>>>(
+            buf.A[last], last == 0 ? buf.B[0] : buf.B0[last], buf.U[last], static_cast<int>(Pl), T(base[4]));
+        relax(last);
+        for (size_t l = last; l-- > 0;) {
+            resize(buf.U[l + 1], l + 1, buf.U[l], l, 2, false);
+            if (l > 0) {
+                const size_t P = static_cast<size_t>(buf.specs[l].first) * buf.specs[l].second;
+                cudaMemcpyAsync(buf.B[l], buf.B0[l], 2 * P * batch * sizeof(T), cudaMemcpyDeviceToDevice, s);
+            }
+            for (int c = 0; c < cycles; ++c) cycle(l);
+        }
+    }
+};
+
+// Workspace of one dartel_step for a batch.
+template <typename T>
+struct StepBuffers {
+    T *map[2], *jac[2], *smap[2], *sjac[2], *rmap[2], *rjac[2];
+    T *rhs_f[2], *hess_f[2], *rhs_r[2], *hess_r[2];
+    T *rhs, *hess, *objf, *objr, *preg, *pnorm;
+    FmgBuffers<T> fmg;
+    int nblocks;
+    bool carve(Arena& ar, int batch, int nx, int ny) {
+        const size_t P = static_cast<size_t>(nx) * ny * batch;
+        for (int i = 0; i < 2; ++i) {
+            map[i] = ar.take<T>(2 * P);
+            jac[i] = ar.take<T>(4 * P);
+            smap[i] = ar.take<T>(2 * P);
+            sjac[i] = ar.take<T>(4 * P);
+            rmap[i] = ar.take<T>(2 * P);
+            rjac[i] = ar.take<T>(4 * P);
+            rhs_f[i] = ar.take<T>(2 * P);
+            hess_f[i] = ar.take<T>(3 * P);
+            rhs_r[i] = ar.take<T>(2 * P);
+            hess_r[i] = ar.take<T>(3 * P);
+        }
+        nblocks = (nx * ny + kThreads - 1) / kThreads;
+        objf = ar.take<T>(static_cast<size_t>(nblocks) * batch);
+        objr = ar.take<T>(static_cast<size_t>(nblocks) * batch);
+        preg = ar.take<T>(static_cast<size_t>(nblocks) * batch);
+        pnorm = ar.take<T>(static_cast<size_t>(nblocks) * batch);
+        // rhs / hess of the solve live in the multigrid's level-0 slots
+        if (!fmg.carve(ar, batch, nx, ny)) return false;
+        rhs = ar.take<T>(2 * P);
+        hess = ar.take<T>(3 * P);
+        return ar.ok;
+    }
+};
+
+// squaring_update (dartel_grid.py:778-914) with the reference's two-slot
+// bookkeeping: slot `other` receives each step's b increment and, when the
+// map is composed, the composed map; slot 0 after the loop is the
+// "scratch" dartel_step hands to the multigrid as its initial guess.
+// Returns the index of the current slot; b / a end in rb[cur_ba] / ha[cur_ba].
+template <typename T>
+struct Squaring {
+    int cur_map, cur_ba;
+};
+
+template <typename T>
+Squaring<T> run_squaring(T* rb[2], T* ha[2], T* maps[2], T* jacs[2], int k, bool save, int batch, int nx, int ny,
+                         cudaStream_t s) {
+    const dim3 g = grid_for(nx * ny, batch);
+    int cur = 0, other = 1, ba = 0;
+    for (int step = 0; step < k; ++step) {
+        k_squaring<T><<<g, kThreads, 0, s>>>(rb[ba], ha[ba], maps[cur], jacs[cur], rb[1 - ba], ha[1 - ba], maps[other],
+                                             nx, ny);
+        ba = 1 - ba;
+        if (save || step < k - 1) {
+            k_compose<T><<<g, kThreads, 0, s>>>(maps[cur], jacs[cur], maps[cur], jacs[cur], maps[other], jacs[other],
+                                                nx, ny);
+            std::swap(cur, other);
+        }
+    }
+    if (save && cur != 0) {
+        const size_t P = static_cast<size_t>(nx) * ny * batch;
+        cudaMemcpyAsync(maps[0], maps[cur], 2 * P * sizeof(T), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(jacs[0], jacs[cur], 4 * P * sizeof(T), cudaMemcpyDeviceToDevice, s);
+    }
+    return {cur, ba};
+}
+
+template <typename T>
+int dartel_step_impl(StepBuffers<T>& W, const T* source, const T* target, T* velocity, T* metrics, int metric_stride,
+                     int batch, int nx, int ny, int k, const double* params, double lmreg, int cycles, int nit,
+                     int code, int assume_initial_nonzero, cudaStream_t s) {
+    const dim3 g = grid_for(nx * ny, batch);
+    const double scale = 1.0 / static_cast<double>(1LL << k);
+    const size_t P = static_cast<size_t>(nx) * ny * batch;
+    // expdef(v, k) with Jacobian
+    k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.map[0], W.jac[0], nx, ny, T(scale), T(scale * 0.5));
+    int cur = 0;
+    for (int i = 0; i < k; ++i) {
+        k_compose<T><<<g, kThreads, 0, s>>>(W.map[cur], W.jac[cur], W.map[cur], W.jac[cur], W.map[1 - cur],
+                                            W.jac[1 - cur], nx, ny);
+        cur = 1 - cur;
+    }
+    // forward objective with jac_div_smalldef(J, v, s)
+    k_objfun<T, true><<<g, kThreads, 0, s>>>(source, target, W.map[cur], W.jac[cur], velocity, nullptr, W.rhs_f[0],
+                                             W.hess_f[0], W.objf, nx, ny, T(scale * 0.5));
+    // squaring of the forward terms from smalldef_jac(v, -s)
+    k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.smap[0], W.sjac[0], nx, ny, T(-scale), T(-scale * 0.5));
+    Squaring<T> fw = run_squaring<T>(W.rhs_f, W.hess_f, W.smap, W.sjac, k, code == 1, batch, nx, ny, s);
+    T* initial = W.smap[0];
+    T* rr = nullptr;
+    T* hr = nullptr;
+    if (code == 1) {
+        k_objfun<T, true><<<g, kThreads, 0, s>>>(target, source, W.smap[fw.cur_map], W.sjac[fw.cur_map], velocity,
+                                                 nullptr, W.rhs_r[0], W.hess_r[0], W.objr, nx, ny, T(-scale * 0.5));
+        k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.rmap[0], W.rjac[0], nx, ny, T(scale), T(scale * 0.5));
+        Squaring<T> rv = run_squaring<T>(W.rhs_r, W.hess_r, W.rmap, W.rjac, k, false, batch, nx, ny, s);
+        initial = W.rmap[0];
+        rr = W.rhs_r[rv.cur_ba];
+        hr = W.hess_r[rv.cur_ba];
+    }
+    const RegWeights rw = reg_weights(params, 1);
+    T* rhs = W.rhs;
+    k_combine<T><<<g, kThreads, 0, s>>>(W.rhs_f[fw.cur_ba], rr, W.hess_f[fw.cur_ba], hr, velocity, rhs, W.hess, W.preg,
+                                        W.pnorm, nx, ny, T(scale), rw);
+    k_metrics<T><<<batch, 32, 0, s>>>(W.objf, code == 1 ? W.objr : nullptr, W.preg, W.pnorm, W.nblocks, metrics,
+                                      metric_stride);
+    // multigrid solve of (H + L) u = rhs from the scratch initial guess
+    double solver[5] = {params[0], params[1], params[2], params[3], params[4] + lmreg};
+    Fmg<T> fmg{W.fmg, batch, {solver[0], solver[1], solver[2], solver[3], solver[4]}, cycles, nit, s, nx, ny};
+    W.fmg.A[0] = W.hess;
+    W.fmg.B[0] = rhs;
+    W.fmg.U[0] = initial;
+    bool coarse_init = false;
+    if (!assume_initial_nonzero) {
+        int flag = 0;
+        CSG_CUDA_CHECK(cudaMemsetAsync(W.fmg.flag, 0, sizeof(int), s));
+        k_any_nonzero<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(initial, 2 * P,
+                                                                                                     W.fmg.flag);
+        CSG_CUDA_CHECK(cudaMemcpyAsync(&flag, W.fmg.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CSG_CUDA_CHECK(cudaStreamSynchronize(s));
+        coarse_init = flag == 0;
+        if (coarse_init) CSG_CUDA_CHECK(cudaMemsetAsync(initial, 0, 2 * P * sizeof(T), s));
+    }
+    fmg.run(coarse_init);
+    k_sub<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(velocity, initial, 2 * P);
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+size_t dtype_size(int dtype) { return dtype == CSG_DTYPE_F64 ? 8 : 4; }
+
+bool check_dtype(int dtype) { return dtype == CSG_DTYPE_F32 || dtype == CSG_DTYPE_F64; }
+
+template <typename T>
+size_t step_bytes(int batch, int nx, int ny) {
+    Arena ar{nullptr, static_cast<size_t>(-1) / 2};
+    StepBuffers<T> W;
+    W.carve(ar, batch, nx, ny);
+    return ar.used + 256;
+}
+
+template <typename T>
+size_t expdef_bytes(int batch, int nx, int ny) {
+    return 2 * (2 + 4) * static_cast<size_t>(nx) * ny * batch * sizeof(T) + 1024;
+}
+
+template <typename T>
+int solve_typed(const void* source, const void* target, void* velocity, void* metrics, int batch, int nx,
+                       int ny, int loop, const double* params, int its, double lmreg, int cycles, int nit, int code,
+                       int assume, void* scratch, size_t bytes, cudaStream_t s) {
+    Arena ar{static_cast<char*>(scratch), bytes};
+    StepBuffers<T> W;
+    if (!W.carve(ar, batch, nx, ny)) return csg::fail(CSG_ERR_ARG, "dartel: scratch of %zu bytes is too small", bytes);
+    const int per = loop * its;
+    for (int index = 0; index < loop; ++index)
+        for (int it = 0; it < its; ++it) {
+            int rc = dartel_step_impl<T>(W, static_cast<const T*>(source), static_cast<const T*>(target),
+                                         static_cast<T*>(velocity), static_cast<T*>(metrics) + 3 * (index * its + it),
+                                         3 * per, batch, nx, ny, index, params + 5 * index, lmreg, cycles, nit, code,
+                                         assume, s);
+            if (rc) return rc;
+        }
+    return CSG_OK;
+}
+
+int check_grid(int dtype, int batch, int nx, int ny) {
+    if (!check_dtype(dtype)) return csg::fail(CSG_ERR_ARG, "dartel: dtype must be CSG_DTYPE_F32 or CSG_DTYPE_F64");
+    if (batch < 1 || nx < 1 || ny < 1) return csg::fail(CSG_ERR_ARG, "dartel: empty grid (%d x %d x %d)", batch, ny, nx);
+    if (static_cast<long long>(nx) * ny > (1LL << 30)) return csg::fail(CSG_ERR_ARG, "dartel: grid too large");
+    return CSG_OK;
+}
+
+int check_levels(int nx, int ny) {
+    for (const auto& spec : grid_levels(nx, ny))
+        if (!relax_supported(spec.first))
+            return csg::fail(CSG_ERR_UNSUPPORTED,
+                             "dartel: red-black relaxation needs an even x size on every multigrid level "
+                             "(level %d x %d)", spec.second, spec.first);
+    return CSG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t csg_dartel_scratch_bytes(int dtype, int batch, int nx, int ny) {
+    if (!check_dtype(dtype) || batch < 1 || nx < 1 || ny < 1) return 0;
+    return dtype == CSG_DTYPE_F64 ? step_bytes<double>(batch, nx, ny) : step_bytes<float>(batch, nx, ny);
+}
+
+int csg_dartel_solve(int dtype, int batch, int nx, int ny, const void* source_maps, const void* target_maps,
+                     void* velocity, void* metrics, int loop, const double* params, int its, double lmreg, int cycles,
+                     int nit, int code, int assume_initial_nonzero, void* scratch, size_t scratch_bytes,
+                     csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!source_maps || !target_maps || !velocity || !metrics || !params || !scratch)
+        return csg::fail(CSG_ERR_ARG, "dartel solve: null pointer");
+    if (loop < 1 || its < 0 || cycles < 0 || nit < 0 || (code != 0 && code != 1) || loop > 30)
+        return csg::fail(CSG_ERR_ARG, "dartel solve: bad loop/its/cycles/nit/code");
+    rc = check_levels(nx, ny);
+    if (rc) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (dtype == CSG_DTYPE_F64)
+        return solve_typed<double>(source_maps, target_maps, velocity, metrics, batch, nx, ny, loop, params, its, lmreg,
+                                   cycles, nit, code, assume_initial_nonzero, scratch, scratch_bytes, s);
+    return solve_typed<float>(source_maps, target_maps, velocity, metrics, batch, nx, ny, loop, params, its, lmreg,
+                              cycles, nit, code, assume_initial_nonzero, scratch, scratch_bytes, s);
+}
+
+int csg_dartel_step(int dtype, int batch, int nx, int ny, const void* source, const void* target, void* velocity,
+                    void* metrics, int k, const double* params, double lmreg, int cycles, int nit, int code,
+                    int assume_initial_nonzero, void* scratch, size_t scratch_bytes, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!source || !target || !velocity || !metrics || !params || !scratch)
+        return csg::fail(CSG_ERR_ARG, "dartel step: null pointer");
+    if (k < 0 || k > 30 || cycles < 0 || nit < 0 || (code != 0 && code != 1))
+        return csg::fail(CSG_ERR_ARG, "dartel step: bad k/cycles/nit/code");
+    rc = check_levels(nx, ny);
+    if (rc) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (dtype == CSG_DTYPE_F64) {
+        Arena ar{static_cast<char*>(scratch), scratch_bytes};
+        StepBuffers<double> W;
+        if (!W.carve(ar, batch, nx, ny)) return csg::fail(CSG_ERR_ARG, "dartel step: scratch too small");
+        return dartel_step_impl<double>(W, static_cast<const double*>(source), static_cast<const double*>(target),
+                                        static_cast<double*>(velocity), static_cast<double*>(metrics), 3, batch, nx, ny,
+                                        k, params, lmreg, cycles, nit, code, assume_initial_nonzero, s);
+    }
+    Arena ar{static_cast<char*>(scratch), scratch_bytes};
+    StepBuffers<float> W;
+    if (!W.carve(ar, batch, nx, ny)) return csg::fail(CSG_ERR_ARG, "dartel step: scratch too small");
+    return dartel_step_impl<float>(W, static_cast<const float*>(source), static_cast<const float*>(target),
+                                   static_cast<float*>(velocity), static_cast<float*>(metrics), 3, batch, nx, ny, k,
+                                   params, lmreg, cycles, nit, code, assume_initial_nonzero, s);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------- single operators
+
+namespace {
+
+template <typename T>
+int smalldef_typed(int batch, int nx, int ny, const void* v, double scale, void* map, void* jac, cudaStream_t s) {
+    k_smalldef<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(static_cast<const T*>(v), static_cast<T*>(map),
+                                                                 static_cast<T*>(jac), nx, ny, T(scale), T(scale * 0.5));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+template <typename T>
+int squaring_typed(int batch, int nx, int ny, const void* rhs, const void* hess, const void* map, const void* jac,
+                   int k, int save, void* b_out, void* a_out, void* map_out, void* jac_out, void* scratch_out,
+                   void* work, size_t bytes, cudaStream_t s) {
+    const size_t P = static_cast<size_t>(nx) * ny * batch;
+    Arena ar{static_cast<char*>(work), bytes};
+    T *rb[2], *ha[2], *maps[2], *jacs[2];
+    for (int i = 0; i < 2; ++i) {
+        rb[i] = ar.take<T>(2 * P);
+        ha[i] = ar.take<T>(3 * P);
+        maps[i] = ar.take<T>(2 * P);
+        jacs[i] = ar.take<T>(4 * P);
+    }
+    if (!ar.ok) return csg::fail(CSG_ERR_ARG, "squaring: scratch too small");
+    CSG_CUDA_CHECK(cudaMemcpyAsync(rb[0], rhs, 2 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    CSG_CUDA_CHECK(cudaMemcpyAsync(ha[0], hess, 3 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    CSG_CUDA_CHECK(cudaMemcpyAsync(maps[0], map, 2 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    CSG_CUDA_CHECK(cudaMemcpyAsync(jacs[0], jac, 4 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    Squaring<T> r = run_squaring<T>(rb, ha, maps, jacs, k, save != 0, batch, nx, ny, s);
+    CSG_CUDA_CHECK(cudaMemcpyAsync(b_out, rb[r.cur_ba], 2 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    CSG_CUDA_CHECK(cudaMemcpyAsync(a_out, ha[r.cur_ba], 3 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    if (map_out) CSG_CUDA_CHECK(cudaMemcpyAsync(map_out, maps[r.cur_map], 2 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    if (jac_out) CSG_CUDA_CHECK(cudaMemcpyAsync(jac_out, jacs[r.cur_map], 4 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    if (scratch_out) CSG_CUDA_CHECK(cudaMemcpyAsync(scratch_out, maps[0], 2 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+template <typename T>
+int expdef_typed(int batch, int nx, int ny, const void* v, int k, void* map_out, void* jac_out, void* work, size_t bytes,
+                 cudaStream_t s) {
+    const size_t P = static_cast<size_t>(nx) * ny * batch;
+    Arena ar{static_cast<char*>(work), bytes};
+    T* maps[2] = {ar.take<T>(2 * P), ar.take<T>(2 * P)};
+    T* jacs[2] = {ar.take<T>(4 * P), ar.take<T>(4 * P)};
+    if (!ar.ok) return csg::fail(CSG_ERR_ARG, "expdef: scratch too small");
+    const double scale = 1.0 / static_cast<double>(1LL << k);
+    const dim3 g = grid_for(nx * ny, batch);
+    const bool with_jac = jac_out != nullptr;
+    k_smalldef<T><<<g, kThreads, 0, s>>>(static_cast<const T*>(v), maps[0], with_jac ? jacs[0] : nullptr, nx, ny,
+                                         T(scale), T(scale * 0.5));
+    int cur = 0;
+    for (int i = 0; i < k; ++i) {
+        k_compose<T><<<g, kThreads, 0, s>>>(maps[cur], with_jac ? jacs[cur] : nullptr, maps[cur],
+                                            with_jac ? jacs[cur] : nullptr, maps[1 - cur],
+                                            with_jac ? jacs[1 - cur] : nullptr, nx, ny);
+        cur = 1 - cur;
+    }
+    CSG_CUDA_CHECK(cudaMemcpyAsync(map_out, maps[cur], 2 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    if (with_jac) CSG_CUDA_CHECK(cudaMemcpyAsync(jac_out, jacs[cur], 4 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+template <typename T>
+int fmg_typed(int batch, int nx, int ny, const void* hess, const void* rhs, const double* params, int cycles, int nit,
+              void* u, int has_initial, int assume_nonzero, void* work, size_t bytes, cudaStream_t s) {
+    const size_t P = static_cast<size_t>(nx) * ny * batch;
+    Arena ar{static_cast<char*>(work), bytes};
+    FmgBuffers<T> buf;
+    if (!buf.carve(ar, batch, nx, ny)) return csg::fail(CSG_ERR_ARG, "fmg: scratch too small");
+    buf.A[0] = const_cast<T*>(static_cast<const T*>(hess));
+    buf.B[0] = const_cast<T*>(static_cast<const T*>(rhs));
+    buf.U[0] = static_cast<T*>(u);
+    bool coarse_init = !has_initial;
+    if (has_initial && !assume_nonzero) {
+        int flag = 0;
+        CSG_CUDA_CHECK(cudaMemsetAsync(buf.flag, 0, sizeof(int), s));
+        k_any_nonzero<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(buf.U[0], 2 * P,
+                                                                                                     buf.flag);
+        CSG_CUDA_CHECK(cudaMemcpyAsync(&flag, buf.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CSG_CUDA_CHECK(cudaStreamSynchronize(s));
+        coarse_init = flag == 0;
+    }
+    if (coarse_init) CSG_CUDA_CHECK(cudaMemsetAsync(u, 0, 2 * P * sizeof(T), s));
+    Fmg<T> fmg{buf, batch, {params[0], params[1], params[2], params[3], params[4]}, cycles, nit, s, nx, ny};
+    fmg.run(coarse_init);
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csg_dartel_smalldef(int dtype, int batch, int nx, int ny, const void* velocity, double scale, void* map_out,
+                        void* jac_out, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!velocity || (!map_out && !jac_out)) return csg::fail(CSG_ERR_ARG, "smalldef: null pointer");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    return dtype == CSG_DTYPE_F64 ? smalldef_typed<double>(batch, nx, ny, velocity, scale, map_out, jac_out, s)
+                                  : smalldef_typed<float>(batch, nx, ny, velocity, scale, map_out, jac_out, s);
+}
+
+int csg_dartel_compose(int dtype, int batch, int nx, int ny, const void* a, const void* ja, const void* b,
+                       const void* jb, void* c_out, void* jc_out, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!a || !b || !c_out || ((ja != nullptr) != (jb != nullptr)) || ((ja != nullptr) != (jc_out != nullptr)))
+        return csg::fail(CSG_ERR_ARG, "compose: null pointer or partial Jacobian set");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const dim3 g = grid_for(nx * ny, batch);
+    if (dtype == CSG_DTYPE_F64)
+        k_compose<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(a), static_cast<const double*>(ja),
+                                                 static_cast<const double*>(b), static_cast<const double*>(jb),
+                                                 static_cast<double*>(c_out), static_cast<double*>(jc_out), nx, ny);
+    else
+        k_compose<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(a), static_cast<const float*>(ja),
+                                                static_cast<const float*>(b), static_cast<const float*>(jb),
+                                                static_cast<float*>(c_out), static_cast<float*>(jc_out), nx, ny);
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_dartel_jac_div(int dtype, int batch, int nx, int ny, const void* jac, const void* velocity, double scale,
+                       void* out, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!jac || !velocity || !out) return csg::fail(CSG_ERR_ARG, "jac_div: null pointer");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const dim3 g = grid_for(nx * ny, batch);
+    if (dtype == CSG_DTYPE_F64)
+        k_jacdiv<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(jac), static_cast<const double*>(velocity),
+                                                static_cast<double*>(out), nx, ny, scale * 0.5);
+    else
+        k_jacdiv<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(jac), static_cast<const float*>(velocity),
+                                               static_cast<float*>(out), nx, ny, static_cast<float>(scale * 0.5));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_dartel_objfun(int dtype, int batch, int nx, int ny, const void* source, const void* target, const void* map,
+                      const void* jac, const void* weights, void* rhs_out, void* hess_out, void* objective_out,
+                      void* scratch, size_t scratch_bytes, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!source || !target || !map || !jac || !rhs_out || !hess_out || !objective_out || !scratch)
+        return csg::fail(CSG_ERR_ARG, "objfun: null pointer");
+    const int nblocks = (nx * ny + kThreads - 1) / kThreads;
+    if (scratch_bytes < static_cast<size_t>(nblocks) * batch * dtype_size(dtype))
+        return csg::fail(CSG_ERR_ARG, "objfun: scratch too small");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const dim3 g = grid_for(nx * ny, batch);
+    if (dtype == CSG_DTYPE_F64) {
+        k_objfun<double, false><<<g, kThreads, 0, s>>>(
+            static_cast<const double*>(source), static_cast<const double*>(target), static_cast<const double*>(map),
+            static_cast<const double*>(jac), nullptr, static_cast<const double*>(weights), static_cast<double*>(rhs_out),
+            static_cast<double*>(hess_out), static_cast<double*>(scratch), nx, ny, 0.0);
+        k_objective_out<double><<<batch, 32, 0, s>>>(static_cast<double*>(scratch), nblocks,
+                                                     static_cast<double*>(objective_out));
+    } else {
+        k_objfun<float, false><<<g, kThreads, 0, s>>>(
+            static_cast<const float*>(source), static_cast<const float*>(target), static_cast<const float*>(map),
+            static_cast<const float*>(jac), nullptr, static_cast<const float*>(weights), static_cast<float*>(rhs_out),
+            static_cast<float*>(hess_out), static_cast<float*>(scratch), nx, ny, 0.0f);
+        k_objective_out<float><<<batch, 32, 0, s>>>(static_cast<float*>(scratch), nblocks,
+                                                    static_cast<float*>(objective_out));
+    }
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_dartel_squaring(int dtype, int batch, int nx, int ny, const void* rhs, const void* hess, const void* map,
+                        const void* jac, int k, int save_transformation, void* b_out, void* a_out, void* map_out,
+                        void* jac_out, void* scratch_map_out, void* scratch, size_t scratch_bytes,
+                        csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!rhs || !hess || !map || !jac || !b_out || !a_out || !scratch || k < 0 || k > 30)
+        return csg::fail(CSG_ERR_ARG, "squaring: null pointer or bad k");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (dtype == CSG_DTYPE_F64)
+        return squaring_typed<double>(batch, nx, ny, rhs, hess, map, jac, k, save_transformation, b_out, a_out, map_out,
+                                      jac_out, scratch_map_out, scratch, scratch_bytes, s);
+    return squaring_typed<float>(batch, nx, ny, rhs, hess, map, jac, k, save_transformation, b_out, a_out, map_out,
+                                 jac_out, scratch_map_out, scratch, scratch_bytes, s);
+}
+
+int csg_dartel_regularization(int dtype, int batch, int nx, int ny, const void* velocity, const double* params,
+                              int rtype, void* out, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!velocity || !params || !out || rtype < 0 || rtype > 2)
+        return csg::fail(CSG_ERR_ARG, "regularization: null pointer or rtype not in {0, 1, 2}");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const RegWeights rw = reg_weights(params, rtype);
+    const dim3 g = grid_for(nx * ny, batch);
+    if (dtype == CSG_DTYPE_F64)
+        k_regularise<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(velocity), static_cast<double*>(out), nx,
+                                                    ny, rtype, rw);
+    else
+        k_regularise<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(velocity), static_cast<float*>(out), nx, ny,
+                                                   rtype, rw);
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_dartel_membrane_apply(int dtype, int batch, int nx, int ny, const void* hess, const void* field,
+                              const double* params, void* out, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!hess || !field || !params || !out) return csg::fail(CSG_ERR_ARG, "membrane apply: null pointer");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const RegWeights rw = reg_weights(params, 1);
+    const dim3 g = grid_for(nx * ny, batch);
+    if (dtype == CSG_DTYPE_F64)
+        k_membrane_apply<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(hess), static_cast<const double*>(field),
+                                                        nullptr, static_cast<double*>(out), nx, ny, rw);
+    else
+        k_membrane_apply<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(hess), static_cast<const float*>(field),
+                                                       nullptr, static_cast<float*>(out), nx, ny, rw);
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_dartel_relax(int dtype, int batch, int nx, int ny, const void* hess, const void* rhs, const double* params,
+                     int nit, void* u, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!hess || !rhs || !params || !u || nit < 0) return csg::fail(CSG_ERR_ARG, "relax: null pointer or nit < 0");
+    if (!relax_supported(nx))
+        return csg::fail(CSG_ERR_UNSUPPORTED, "relax: red-black relaxation on the GPU needs an even x size (got %d)", nx);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const MemWeights w = mem_weights(params);
+    const dim3 g = grid_for(nx * ny, batch);
+    for (int it = 0; it < 2 * nit; ++it) {
+        const int colour = it % 2 == 0 ? 1 : 0;
+        if (dtype == CSG_DTYPE_F64)
+            k_relax<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(hess), static_cast<const double*>(rhs),
+                                                   static_cast<double*>(u), nx, ny, colour, w.w00, w.w01, w.w10);
+        else
+            k_relax<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(hess), static_cast<const float*>(rhs),
+                                                  static_cast<float*>(u), nx, ny, colour, static_cast<float>(w.w00),
+                                                  static_cast<float>(w.w01), static_cast<float>(w.w10));
+    }
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_dartel_resize(int dtype, int fields, int src_nx, int src_ny, const void* src, int dst_nx, int dst_ny,
+                      void* dst, int accumulate, csg_stream_t stream) {
+    if (!check_dtype(dtype) || fields < 1 || src_nx < 1 || src_ny < 1 || dst_nx < 1 || dst_ny < 1 || !src || !dst)
+        return csg::fail(CSG_ERR_ARG, "resize: bad arguments");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const dim3 g = grid_for(dst_nx * dst_ny, fields);
+    if (dtype == CSG_DTYPE_F64)
+        k_resize<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(src), static_cast<double*>(dst), src_nx,
+                                                src_ny, dst_nx, dst_ny, accumulate);
+    else
+        k_resize<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(src), static_cast<float*>(dst), src_nx, src_ny,
+                                               dst_nx, dst_ny, accumulate);
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_dartel_fmg(int dtype, int batch, int nx, int ny, const void* hess, const void* rhs, const double* params,
+                   int cycles, int nit, void* u, int has_initial, int assume_initial_nonzero, void* scratch,
+                   size_t scratch_bytes, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!hess || !rhs || !params || !u || !scratch || cycles < 0 || nit < 0)
+        return csg::fail(CSG_ERR_ARG, "fmg: null pointer or negative cycles / nit");
+    rc = check_levels(nx, ny);
+    if (rc) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (dtype == CSG_DTYPE_F64)
+        return fmg_typed<double>(batch, nx, ny, hess, rhs, params, cycles, nit, u, has_initial, assume_initial_nonzero,
+                                 scratch, scratch_bytes, s);
+    return fmg_typed<float>(batch, nx, ny, hess, rhs, params, cycles, nit, u, has_initial, assume_initial_nonzero,
+                            scratch, scratch_bytes, s);
+}
+
+int csg_dartel_expdef(int dtype, int batch, int nx, int ny, const void* velocity, int k, void* map_out, void* jac_out,
+                      void* scratch, size_t scratch_bytes, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!velocity || !map_out || !scratch || k < 0 || k > 30)
+        return csg::fail(CSG_ERR_ARG, "expdef: null pointer or bad k");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (dtype == CSG_DTYPE_F64)
+        return expdef_typed<double>(batch, nx, ny, velocity, k, map_out, jac_out, scratch, scratch_bytes, s);
+    return expdef_typed<float>(batch, nx, ny, velocity, k, map_out, jac_out, scratch, scratch_bytes, s);
+}
+
+}  // extern "C"

@@ -39,6 +39,9 @@ typedef struct CUstream_st *csg_stream_t;
 #define CSG_ERR_UNSUPPORTED (-6) /* option not supported */
 #define CSG_ERR_COVERAGE (-7)    /* a query point found no candidate triangle */
 
+#define CSG_DTYPE_F32 0 /* DARTEL / warp element type */
+#define CSG_DTYPE_F64 1
+
 #define CSG_ARITH_CAT 0  /* float32 storage, CAT mixed float32/float64 arithmetic */
 #define CSG_ARITH_FP32 1 /* float32 storage and arithmetic */
 #define CSG_ARITH_FP64 2 /* float64 storage and arithmetic */
@@ -122,6 +125,112 @@ CSG_API int csg_areal_sweeps(void *points, int n_vertices, const int32_t *slot_o
  * CSG_ERR_TIMEOUT in scratch's status word.  Exercises the timeout path
  * without faulting or hanging the GPU; the context stays usable. */
 CSG_API int csg_selftest_barrier_timeout(void *scratch, size_t scratch_bytes, double timeout_s, csg_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * SurfWarp: 2-D DARTEL on the lat-lon sheet (device, batched).
+ * Fields are [batch][channels][ny][nx] of dtype CSG_DTYPE_F32 / _F64; maps
+ * are one-based coordinates [2], Jacobians (j00, j10, j01, j11) [4],
+ * gradients [2], Hessians (h00, h11, h01) [3].  Arithmetic follows the
+ * reference's torch path operation by operation (one rounding each).
+ * params are the five regulariser values (sx, sy, mu, lambda, identity).
+ * ---------------------------------------------------------------------- */
+
+/* Scratch for csg_dartel_solve / _step / _fmg / _expdef / _squaring / _objfun. */
+CSG_API size_t csg_dartel_scratch_bytes(int dtype, int batch, int nx, int ny);
+
+/* Whole solve of `batch` independent (source, target) sheet pairs:
+ * for index in 0..loop-1, its times dartel_step(k = index, params[index]).
+ * velocity [batch][2][ny][nx] in/out (zeros for the reference's start);
+ * metrics [batch][loop*its][3] (objective, regulariser/2, |rhs|).
+ * Replaces the eager loop of solve_dartel_maps
+ * (src/cat_surface_gpu/surface_warp.py:321-353) and dartel_step
+ * (src/cat_surface_gpu/dartel_grid.py:1420-1616).  With
+ * assume_initial_nonzero the call makes no host synchronisation and can be
+ * captured in a CUDA graph. */
+CSG_API int csg_dartel_solve(int dtype, int batch, int nx, int ny, const void *source_maps, const void *target_maps,
+                             void *velocity, void *metrics, int loop, const double *params, int its, double lmreg,
+                             int cycles, int nit, int code, int assume_initial_nonzero, void *scratch,
+                             size_t scratch_bytes, csg_stream_t stream);
+
+/* One dartel_step (dartel_grid.py:1420-1616), rtype 1, no distortion. */
+CSG_API int csg_dartel_step(int dtype, int batch, int nx, int ny, const void *source, const void *target,
+                            void *velocity, void *metrics, int k, const double *params, double lmreg, int cycles,
+                            int nit, int code, int assume_initial_nonzero, void *scratch, size_t scratch_bytes,
+                            csg_stream_t stream);
+
+/* smalldef_jac / jacobian_of_displacement (dartel_grid.py:624-675):
+ * map = id + v * scale, jac = I + central differences of v * scale / 2.
+ * Either output may be NULL. */
+CSG_API int csg_dartel_smalldef(int dtype, int batch, int nx, int ny, const void *velocity, double scale,
+                                void *map_out, void *jac_out, csg_stream_t stream);
+
+/* composition / composition_jacobian (dartel_grid.py:407-507, 534-587):
+ * c = b o a with period unwrapping; jc = J_b(a) J_a.  ja, jb, jc_out are all
+ * NULL (map only) or all set. */
+CSG_API int csg_dartel_compose(int dtype, int batch, int nx, int ny, const void *a, const void *ja, const void *b,
+                               const void *jb, void *c_out, void *jc_out, csg_stream_t stream);
+
+/* jac_div_smalldef (dartel_grid.py:678-720). */
+CSG_API int csg_dartel_jac_div(int dtype, int batch, int nx, int ny, const void *jac, const void *velocity,
+                               double scale, void *out, csg_stream_t stream);
+
+/* initialise_objfun (dartel_grid.py:723-775); weights may be NULL;
+ * objective_out [batch]. */
+CSG_API int csg_dartel_objfun(int dtype, int batch, int nx, int ny, const void *source, const void *target,
+                              const void *map, const void *jac, const void *weights, void *rhs_out, void *hess_out,
+                              void *objective_out, void *scratch, size_t scratch_bytes, csg_stream_t stream);
+
+/* squaring_update (dartel_grid.py:778-914; dartel_triton.py:345-477) with
+ * the reference's scratch slot (return_scratch); map/jac/scratch outputs may
+ * be NULL. */
+CSG_API int csg_dartel_squaring(int dtype, int batch, int nx, int ny, const void *rhs, const void *hess,
+                                const void *map, const void *jac, int k, int save_transformation, void *b_out,
+                                void *a_out, void *map_out, void *jac_out, void *scratch_map_out, void *scratch,
+                                size_t scratch_bytes, csg_stream_t stream);
+
+/* regularization_operator rtype 0 / 1 / 2 (dartel_grid.py:917-1015). */
+CSG_API int csg_dartel_regularization(int dtype, int batch, int nx, int ny, const void *velocity,
+                                      const double *params, int rtype, void *out, csg_stream_t stream);
+
+/* apply_membrane_system (dartel_grid.py:1018-1070; dartel_triton.py:190-239). */
+CSG_API int csg_dartel_membrane_apply(int dtype, int batch, int nx, int ny, const void *hess, const void *field,
+                                      const double *params, void *out, csg_stream_t stream);
+
+/* relax_membrane: nit red-black sweeps in place (dartel_grid.py:1073-1208;
+ * dartel_triton.py:242-291, 606-640).  Needs an even nx (or nx == 1), as the
+ * reference's CUDA path does. */
+CSG_API int csg_dartel_relax(int dtype, int batch, int nx, int ny, const void *hess, const void *rhs,
+                             const double *params, int nit, void *u, csg_stream_t stream);
+
+/* resize_field: separable quadratic B-spline (dartel_grid.py:239-305;
+ * dartel_triton.py:59-187); `fields` = batch * channels; accumulate adds. */
+CSG_API int csg_dartel_resize(int dtype, int fields, int src_nx, int src_ny, const void *src, int dst_nx, int dst_ny,
+                              void *dst, int accumulate, csg_stream_t stream);
+
+/* fmg2_membrane (dartel_grid.py:1211-1417); u holds the initial guess when
+ * has_initial, else it is overwritten. */
+CSG_API int csg_dartel_fmg(int dtype, int batch, int nx, int ny, const void *hess, const void *rhs,
+                           const double *params, int cycles, int nit, void *u, int has_initial,
+                           int assume_initial_nonzero, void *scratch, size_t scratch_bytes, csg_stream_t stream);
+
+/* expdef: scaling and squaring of id + v / 2^k (dartel_grid.py:1619-1666);
+ * jac_out may be NULL. */
+CSG_API int csg_dartel_expdef(int dtype, int batch, int nx, int ny, const void *velocity, int k, void *map_out,
+                              void *jac_out, void *scratch, size_t scratch_bytes, csg_stream_t stream);
+
+/* sample_field: bilinear samples of a [ny][nx] field at n (x, y) points,
+ * zero-based, with the DARTEL boundary rule (dartel_grid.py:590-621). */
+CSG_API int csg_dartel_sample(int dtype, int nx, int ny, const void *field, int n, const void *x, const void *y,
+                              void *out, csg_stream_t stream);
+
+/* apply_flow_to_sphere with unit-sphere points (float32 [n][3]) and a flow
+ * [2][ny][nx]; out [n][3] of the flow's dtype (surface_warp.py:500-617). */
+CSG_API int csg_apply_flow_to_sphere(int dtype, int n, const float *unit_points, int nx, int ny, const void *flow,
+                                     int inverse, void *out, csg_stream_t stream);
+
+/* -avg blend of the x- and z-pole warped spheres, float64 [n][3] in, float32
+ * [n][3] out (src/cat_surface_gpu/gpu_pipeline.py:248-271). */
+CSG_API int csg_average_xz(int n, const double *x_surface, const double *z_surface, float *out, csg_stream_t stream);
 
 /* Synchronously read a persistent kernel's status word from its scratch. */
 CSG_API int csg_read_status(const void *scratch, csg_stream_t stream, int *status, int *where);
