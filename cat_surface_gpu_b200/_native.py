@@ -43,6 +43,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         _I,
         [_P, _I, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, c_double, _I, _P, c_size_t, _I, _I, _I, c_double, _P],
     ),
+    "csg_areal_sweeps_noalloc": (
+        _I,
+        [_P, _I, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, c_double, _I, _I, _I, _I, c_double, _P, _P],
+    ),
     "csg_selftest_barrier_timeout": (_I, [_P, c_size_t, c_double, _P]),
     "csg_dartel_scratch_bytes": (c_size_t, [_I, _I, _I, _I]),
     "csg_dartel_solve": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _I, c_double, _I, _I, _I, _I, _P, c_size_t, _P]),

@@ -30,6 +30,8 @@
 // intrinsics, no contraction), so results are bit-identical to the CPU
 // restatement compiled with -ffp-contract=off.
 #include <cstdint>
+#include <mutex>
+
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -517,3 +519,123 @@ int csg_read_status(const void* scratch, csg_stream_t stream, int* status, int* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of csg_areal_sweeps.
+//
+// Some callers cannot call cudaMalloc: code that runs while a CUDA stream
+// capture is active on its thread (cudaMalloc is refused in the default
+// capture mode), hosts that hand all device memory to their own pool
+// allocator up front, and thin foreign-function bindings that pass device
+// pointers they were given but own no device allocator.  For them the sweep
+// kernel's working memory (the 256-byte control block and the float4 /
+// double4 position working copy) lives in the file-scope array below, which
+// every GPU that loads this library holds until the process exits.
+// Limits: 262,144 vertices in the float32 modes, 131,072 in float64 mode.
+
+namespace {
+constexpr size_t kNoAllocWorkBytes = static_cast<size_t>(262144) * sizeof(float4);  // 4 MiB
+constexpr size_t kNoAllocBytes = sizeof(csg::Control) + kNoAllocWorkBytes;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_areal_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+std::mutex g_noalloc_mutex;
+constexpr int kNoAllocMaxDevices = 64;
+void* g_noalloc_address[kNoAllocMaxDevices] = {};
+
+// Device address of g_areal_noalloc_scratch on the current device, looked up
+// once per device (the name itself is only a host-side stand-in).
+int noalloc_scratch(void** out) {
+    int device = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    if (device < 0 || device >= kNoAllocMaxDevices)
+        return csg::fail(CSG_ERR_UNSUPPORTED, "areal sweeps (no-alloc): device ordinal %d >= %d", device,
+                         kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_address[device] == nullptr) {
+        void* address = nullptr;
+        const cudaError_t err = cudaGetSymbolAddress(&address, g_areal_noalloc_scratch);
+        if (err != cudaSuccess || address == nullptr)
+            return csg::fail(CSG_ERR_CUDA, "areal sweeps (no-alloc): cudaGetSymbolAddress failed: %s",
+                             cudaGetErrorString(err));
+        g_noalloc_address[device] = address;
+    }
+    *out = g_noalloc_address[device];
+    return CSG_OK;
+}
+}  // namespace
+
+extern "C" int csg_areal_sweeps_noalloc(void* points, int n_vertices, const int32_t* slot_off, const int32_t* slot_tri,
+                                        const int32_t* order, const int32_t* level_begin, const int32_t* level_end,
+                                        int n_levels, int level_stride, int max_degree, int iterations,
+                                        int project_every, double radius, int arithmetic, int n_ctas,
+                                        int threads_per_cta, int lanes_per_vertex, double timeout_s,
+                                        int* status_out, csg_stream_t stream) {
+    if (!points || n_vertices < 1 || !slot_off || !order || !level_begin || !level_end)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): null pointer or empty mesh");
+    if (arithmetic < CSG_ARITH_CAT || arithmetic > CSG_ARITH_FP64)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): unknown arithmetic %d", arithmetic);
+    const size_t need = csg_areal_scratch_bytes(n_vertices, arithmetic);
+    if (need > kNoAllocBytes)
+        return csg::fail(CSG_ERR_ARG,
+                         "areal sweeps (no-alloc): %d vertices need %zu bytes of working memory, more than the "
+                         "built-in %zu (at most %d vertices in float32 modes, %d in float64 mode)",
+                         n_vertices, need, kNoAllocBytes, 262144, 131072);
+    if (n_levels < 1 || n_levels > n_vertices || level_stride < 1 || iterations < 1 || project_every < 0 ||
+        max_degree < 0)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): bad schedule (levels %d, stride %d, iterations %d)",
+                         n_levels, level_stride, iterations);
+    {
+        const long long sweeps_per_epoch = project_every > 0 ? project_every : iterations;
+        if ((sweeps_per_epoch - 1) * static_cast<long long>(level_stride) + n_levels >= (1LL << 31))
+            return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): wavefront epoch longer than 2^31 steps");
+    }
+    if (reinterpret_cast<uintptr_t>(slot_tri) % 16 != 0)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): slot_tri must be 16-byte aligned");
+    if (threads_per_cta <= 0) threads_per_cta = 512;
+    if (lanes_per_vertex <= 0) lanes_per_vertex = 8;
+    if (threads_per_cta % 32 != 0 || threads_per_cta > 512)
+        return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): threads_per_cta must be a multiple of 32 up to 512");
+    if (timeout_s <= 0.0) timeout_s = 2.0;
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    ArealParams p{};
+    p.points = points;
+    p.ctl = static_cast<csg::Control*>(scratch);
+    p.work = static_cast<char*>(scratch) + sizeof(csg::Control);
+    p.slot_tri = reinterpret_cast<const int4*>(slot_tri);
+    p.slot_off = slot_off;
+    p.order = order;
+    p.level_begin = level_begin;
+    p.level_end = level_end;
+    p.n = n_vertices;
+    p.n_levels = n_levels;
+    p.stride = level_stride;
+    p.max_degree = max_degree;
+    p.iterations = iterations;
+    p.project_every = project_every;
+    p.radius = radius;
+    p.timeout_ns = static_cast<unsigned long long>(timeout_s * 1e9);
+    // The array keeps the previous call's contents: the control block (barrier
+    // counter and status) must start at zero; the working copy is fully
+    // rewritten from `points` by the kernel itself.
+    CSG_CUDA_CHECK(cudaMemsetAsync(scratch, 0, sizeof(csg::Control), s));
+    switch (arithmetic) {
+        case CSG_ARITH_CAT: rc = dispatch_lanes<CSG_ARITH_CAT>(p, n_ctas, threads_per_cta, lanes_per_vertex, s); break;
+        case CSG_ARITH_FP32: rc = dispatch_lanes<CSG_ARITH_FP32>(p, n_ctas, threads_per_cta, lanes_per_vertex, s); break;
+        default: rc = dispatch_lanes<CSG_ARITH_FP64>(p, n_ctas, threads_per_cta, lanes_per_vertex, s); break;
+    }
+    if (rc || status_out == nullptr) return rc;
+    csg::Control ctl{};
+    CSG_CUDA_CHECK(cudaMemcpyAsync(&ctl, scratch, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+    CSG_CUDA_CHECK(cudaStreamSynchronize(s));
+    *status_out = ctl.status;
+    if (ctl.status != CSG_OK)
+        return csg::fail(ctl.status, "areal sweeps (no-alloc): kernel reported status %d at barrier %d", ctl.status,
+                         ctl.where);
+    return CSG_OK;
+}

@@ -119,6 +119,28 @@ CSG_API int csg_areal_sweeps(void *points, int n_vertices, const int32_t *slot_o
                      size_t scratch_bytes, int n_ctas, int threads_per_cta, int lanes_per_vertex, double timeout_s,
                      csg_stream_t stream);
 
+/* Allocation-free variant of csg_areal_sweeps (no counterpart in the
+ * reference).  Some callers cannot call cudaMalloc: code running while a CUDA
+ * stream capture is active on its thread, hosts that give all device memory
+ * to their own pool allocator up front, and foreign-function bindings that
+ * own no device allocator.  This entry point takes the same inputs and
+ * in/out points as csg_areal_sweeps but no scratch: its working memory is a
+ * file-scope device array of 4 MiB + 256 bytes that every GPU loading the
+ * library holds until exit, so it handles at most 262,144 vertices in the
+ * float32 modes and 131,072 in CSG_ARITH_FP64 (larger meshes are rejected
+ * with CSG_ERR_ARG before any device work).  It allocates nothing.  The first
+ * call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array, so calls that overlap on the GPU (other
+ * streams, other threads) race; serialise them.  With status_out non-NULL the
+ * call waits for the kernel and reports its status word (also returned);
+ * with NULL it returns once the work is enqueued. */
+CSG_API int csg_areal_sweeps_noalloc(void *points, int n_vertices, const int32_t *slot_off, const int32_t *slot_tri,
+                                     const int32_t *order, const int32_t *level_begin, const int32_t *level_end,
+                                     int n_levels, int level_stride, int max_degree, int iterations, int project_every,
+                                     double radius, int arithmetic, int n_ctas, int threads_per_cta,
+                                     int lanes_per_vertex, double timeout_s, int *status_out, csg_stream_t stream);
+
 /* Self-test of the bounded device-side wait (no reference counterpart): a
  * 2-CTA cooperative grid waits on a barrier that expects one arrival more
  * than the grid has; the wait gives up after timeout_s (<= 10 s) and records
