@@ -65,8 +65,38 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_dartel_sample": (_I, [_I, _I, _I, _P, _I, _P, _P, _P, _P]),
     "csg_apply_flow_to_sphere": (_I, [_I, _I, _P, _I, _I, _P, _I, _P, _P]),
     "csg_average_xz": (_I, [_I, _P, _P, _P, _P]),
+    "csg_rotation_grid_build": (_I, [_P, _I, _P, _I, _I, _I, _P, _P, ctypes.c_longlong, _P]),
+    "csg_rotation_scratch_bytes": (c_size_t, [_I, _P, _P, _I]),
+    "csg_rotation_cost_batch": (_I, [_I, _P, _P, _I, _I, _P, c_size_t, _P]),
+    "csg_rotation_status": (_I, [_P, _I, _P, _P]),
+    "csg_feature_resample": (_I, [_I, _I, _P, _P, _P, _P, _P]),
+    "csg_feature_sheet_map": (_I, [_I, _P, _P, _P, _P, _P]),
+    "csg_feature_scratch_bytes": (c_size_t, [_I, _I, _I, _I]),
+    "csg_feature_edge_sum": (_I, [_I, _I, _P, _P, _P, _P, c_size_t, _P]),
+    "csg_feature_smooth_geometry": (_I, [_I, _P, _P, _P, _I, _P, _P, c_size_t, _P]),
+    "csg_feature_smooth_values": (_I, [_I, _P, _P, _I, _I, _P, _P, _I, _P, _P, _I, _P, _P, c_size_t, _P]),
+    "csg_feature_vertex_normals": (_I, [_I, _P, _P, _P, _P, _P, _P]),
+    "csg_feature_normal_displacement": (_I, [_I, _P, _P, _P, _P, _P]),
+    "csg_feature_curvature2": (_I, [_I, _P, _P, _P, _P, _P, _P]),
+    "csg_feature_minmax": (_I, [_I, _I, _P, _P, _P, c_size_t, _P]),
     "csg_read_status": (_I, [_P, _P, _P, _P]),
 }
+
+
+class RotationSurface(ctypes.Structure):
+    _fields_ = [
+        ("src_points", c_void_p),
+        ("src_values", c_void_p),
+        ("triangles", c_void_p),
+        ("faces", c_void_p),
+        ("tgt_values", c_void_p),
+        ("grid_offsets", c_void_p),
+        ("grid_faces", c_void_p),
+        ("matrices", c_void_p),
+        ("n_src", ctypes.c_int32),
+        ("grid_size", ctypes.c_int32),
+        ("n_candidates", ctypes.c_int32),
+    ]
 
 
 class PlanInfo(ctypes.Structure):

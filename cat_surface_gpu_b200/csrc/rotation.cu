@@ -1,0 +1,361 @@
+// SurfWarp initial-rotation search on sm_100a: closest-triangle location of
+// rotated source points on the target sphere and the SSD of the resampled
+// target feature, for many candidate rotations and many surfaces at once.
+//
+// Follows src/cat_surface_gpu/surface_rotation.py: grid index (58-120),
+// candidate query (455-477), closest point per candidate triangle -- plane
+// projection with a 1e-3 inside tolerance, else the nearer of the two edges at
+// the nearest vertex -- and the first minimum over candidates (354-453),
+// barycentric weights (335-352) and the float64 SSD (512-546).  Geometry is
+// float32 with one rounding per operation (compiled with --fmad=false):
+// 3-term dot products are (a0 b0 + a1 b1) + a2 b2.
+//
+// Work decomposition: one work item = (surface, candidate, tile of kTile
+// source points).  A persistent grid walks the flattened item list, so any
+// mix of surfaces of uneven size and candidate counts is one launch.  Each
+// item writes one float64 partial (block reduction); a second kernel sums
+// the partials of each (surface, candidate) in a fixed order, so costs are
+// deterministic.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/catsurf_b200.h"
+#include "errors.h"
+
+namespace {
+
+struct RotSurface {
+    const float* src_points;     // [n_src][3]
+    const double* src_values;    // [n_src]
+    const float* triangles;      // [n_tri][9] target triangle corners
+    const int* faces;            // [n_tri][3]
+    const double* tgt_values;    // [n_target_points]
+    const int* grid_offsets;     // [G^3 + 1]
+    const int* grid_faces;       // CSR faces
+    const float* matrices;       // [n_candidates][9] column-major
+    double* partials;            // [n_candidates][tiles]
+    int n_src;
+    int grid_size;
+    int n_candidates;
+    int tiles;                   // ceil(n_src / tile)
+    long long item_begin;        // first flat work item of this surface
+};
+
+__device__ __forceinline__ float dot3(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+
+__device__ __forceinline__ void cross3(const float* a, const float* b, float* out) {
+    out[0] = a[1] * b[2] - a[2] * b[1];
+    out[1] = a[2] * b[0] - a[0] * b[2];
+    out[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ __forceinline__ void sub3(const float* a, const float* b, float* out) {
+    out[0] = a[0] - b[0];
+    out[1] = a[1] - b[1];
+    out[2] = a[2] - b[2];
+}
+
+// Closest point of q on segment [first, second] (surface_rotation.py:315-333).
+__device__ __forceinline__ float segment(const float* q, const float* first, const float* second, float* closest) {
+    float dir[3], off[3];
+    sub3(second, first, dir);
+    sub3(q, first, off);
+    const float den = dot3(dir, dir);
+    float alpha = den != 0.0f ? dot3(off, dir) / den : 0.0f;
+    alpha = alpha < 0.0f ? 0.0f : (alpha > 1.0f ? 1.0f : alpha);
+    for (int k = 0; k < 3; ++k) closest[k] = first[k] + alpha * dir[k];
+    float d[3];
+    sub3(q, closest, d);
+    return dot3(d, d);
+}
+
+// Candidate distance and closest point for one triangle (354-440).
+__device__ __forceinline__ float candidate(const float* q, const float* t, float* point) {
+    const float* p0 = t;
+    const float* p1 = t + 3;
+    const float* p2 = t + 6;
+    float ea[3], eb[3], n[3], off[3];
+    sub3(p1, p0, ea);
+    sub3(p2, p0, eb);
+    cross3(ea, eb, n);
+    const float nsq = dot3(n, n);
+    sub3(p0, q, off);
+    const float plane_t = nsq != 0.0f ? dot3(off, n) / nsq : 0.0f;
+    float proj[3], po[3];
+    for (int k = 0; k < 3; ++k) proj[k] = q[k] + plane_t * n[k];
+    sub3(proj, p0, po);
+    const float xx = dot3(ea, ea), xy = dot3(ea, eb), xv = dot3(ea, po), yy = dot3(eb, eb), yv = dot3(eb, po);
+    const float den = xx * yy - xy * xy;
+    const float xpos = den != 0.0f ? (xv * yy - yv * xy) / den : 0.0f;
+    const float ypos = den != 0.0f ? (yv * xx - xv * xy) / den : 0.0f;
+    const float lo = -1.0e-3f, hi = static_cast<float>(1.0 + 1.0e-3);
+    const float s = xpos + ypos;
+    const bool inside = den != 0.0f && xpos >= lo && xpos <= hi && ypos >= lo && ypos <= hi && s >= lo && s <= hi;
+    if (inside) {
+        for (int k = 0; k < 3; ++k) point[k] = proj[k];
+        return plane_t * plane_t * nsq;
+    }
+    float d[3][3];
+    float vd[3];
+    for (int v = 0; v < 3; ++v) {
+        sub3(q, t + 3 * v, d[v]);
+        vd[v] = dot3(d[v], d[v]);
+    }
+    int cv = 0;  // first minimum
+    if (vd[1] < vd[cv]) cv = 1;
+    if (vd[2] < vd[cv]) cv = 2;
+    const float* closest = t + 3 * cv;
+    const float* prev = t + 3 * ((cv + 2) % 3);
+    const float* next = t + 3 * ((cv + 1) % 3);
+    float c1[3], c2[3];
+    const float d1 = segment(q, prev, closest, c1);
+    const float d2 = segment(q, closest, next, c2);
+    const bool first = d1 < d2;
+    for (int k = 0; k < 3; ++k) point[k] = first ? c1[k] : c2[k];
+    return first ? d1 : d2;
+}
+
+// Barycentric weights of `point` in triangle t (surface_rotation.py:335-352).
+__device__ __forceinline__ void barycentric(const float* point, const float* t, float w[3]) {
+    const int order[3][3] = {{1, 2, 0}, {2, 0, 1}, {0, 1, 2}};
+    for (int k = 0; k < 3; ++k) {
+        const float* a = t + 3 * order[k][0];
+        const float* b = t + 3 * order[k][1];
+        const float* c = t + 3 * order[k][2];
+        float fo[3], hz[3], up[3], n[3], vert[3];
+        sub3(point, a, fo);
+        sub3(b, a, hz);
+        sub3(c, a, up);
+        cross3(hz, up, n);
+        cross3(n, hz, vert);
+        w[k] = dot3(fo, vert) / dot3(up, vert);
+    }
+}
+
+template <int TILE>
+__global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __restrict__ surfaces, int n_surfaces,
+                                                        long long n_items, int* __restrict__ error) {
+    __shared__ double red[TILE / 32];
+    for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
+        // locate the surface of this item (few surfaces: linear scan)
+        int s = 0;
+        while (s + 1 < n_surfaces && surfaces[s + 1].item_begin <= item) ++s;
+        const RotSurface& S = surfaces[s];
+        const long long local = item - S.item_begin;
+        const int cand = static_cast<int>(local / S.tiles);
+        const int tile = static_cast<int>(local - static_cast<long long>(cand) * S.tiles);
+        const int i = tile * TILE + threadIdx.x;
+        double contrib = 0.0;
+        if (i < S.n_src) {
+            const float* m = S.matrices + 9 * cand;
+            const float px = S.src_points[3 * i], py = S.src_points[3 * i + 1], pz = S.src_points[3 * i + 2];
+            float q[3];
+            for (int j = 0; j < 3; ++j) q[j] = (px * m[3 * j] + py * m[3 * j + 1]) + pz * m[3 * j + 2];
+            const int G = S.grid_size;
+            const float half = static_cast<float>(G / 2.0);
+            int cell[3];
+            for (int k = 0; k < 3; ++k) {
+                int c = static_cast<int>(floorf((q[k] + 1.0f) * half));
+                cell[k] = c < 0 ? 0 : (c > G - 1 ? G - 1 : c);
+            }
+            const long long cid = cell[0] + static_cast<long long>(G) * (cell[1] + static_cast<long long>(G) * cell[2]);
+            const int begin = S.grid_offsets[cid], end = S.grid_offsets[cid + 1];
+            if (begin >= end) {
+                atomicExch(error, CSG_ERR_COVERAGE);
+            } else {
+                float best = INFINITY;
+                int best_face = -1;
+                float best_point[3] = {0.0f, 0.0f, 0.0f};
+                for (int k = begin; k < end; ++k) {
+                    const int f = S.grid_faces[k];
+                    float point[3];
+                    const float d = candidate(q, S.triangles + 9 * static_cast<long long>(f), point);
+                    if (d < best) {
+                        best = d;
+                        best_face = f;
+                        best_point[0] = point[0];
+                        best_point[1] = point[1];
+                        best_point[2] = point[2];
+                    }
+                }
+                if (best_face < 0) {  // every candidate produced NaN
+                    best_face = S.grid_faces[begin];
+                    candidate(q, S.triangles + 9 * static_cast<long long>(best_face), best_point);
+                }
+                float w[3];
+                barycentric(best_point, S.triangles + 9 * static_cast<long long>(best_face), w);
+                const int* fv = S.faces + 3 * static_cast<long long>(best_face);
+                const double sampled = (S.tgt_values[fv[0]] * static_cast<double>(w[0]) +
+                                        S.tgt_values[fv[1]] * static_cast<double>(w[1])) +
+                                       S.tgt_values[fv[2]] * static_cast<double>(w[2]);
+                const double diff = S.src_values[i] - sampled;
+                contrib = diff * diff;
+            }
+        }
+        // fixed-order block reduction: warp tree, then warp 0 over warp sums
+        for (int off = 16; off > 0; off >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, off);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = contrib;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double v = threadIdx.x < TILE / 32 ? red[threadIdx.x] : 0.0;
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (threadIdx.x == 0) S.partials[static_cast<long long>(cand) * S.tiles + tile] = v;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_rotation_finalize(const RotSurface* __restrict__ surfaces, int n_surfaces, double* __restrict__ costs,
+                                    const long long* __restrict__ cost_offsets) {
+    const int s = blockIdx.y;
+    if (s >= n_surfaces) return;
+    const RotSurface& S = surfaces[s];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= S.n_candidates) return;
+    double total = 0.0;
+    const double* p = S.partials + static_cast<long long>(c) * S.tiles;
+    for (int t = 0; t < S.tiles; ++t) total += p[t];
+    costs[cost_offsets[s] + c] = total;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+}  // namespace
+
+extern "C" {
+
+int csg_rotation_grid_build(const double* points, int n_points, const int32_t* faces, int n_faces, int grid_size,
+                            int margin, int32_t* offsets, int32_t* cell_faces, long long capacity, long long* count) {
+    if (!points || !faces || n_points < 1 || n_faces < 1 || grid_size < 4 || margin < 0 || !offsets || !count)
+        return csg::fail(CSG_ERR_ARG, "rotation grid: bad arguments (grid_size >= 4, margin >= 0)");
+    if (static_cast<long long>(grid_size) * grid_size * grid_size >= (1LL << 31))
+        return csg::fail(CSG_ERR_ARG, "rotation grid: grid_size too large");
+    const int G = grid_size;
+    const double cell = 2.0 / static_cast<double>(G);
+    std::vector<int> lo(3 * static_cast<size_t>(n_faces)), hi(3 * static_cast<size_t>(n_faces));
+    const long long ncell = static_cast<long long>(G) * G * G;
+    std::vector<long long> counts(ncell + 1, 0);
+    for (int f = 0; f < n_faces; ++f) {
+        for (int k = 0; k < 3; ++k) {
+            const int v0 = faces[3 * f], v1 = faces[3 * f + 1], v2 = faces[3 * f + 2];
+            if (v0 < 0 || v1 < 0 || v2 < 0 || v0 >= n_points || v1 >= n_points || v2 >= n_points)
+                return csg::fail(CSG_ERR_TOPOLOGY, "rotation grid: face %d references a missing point", f);
+            const double a = points[3 * v0 + k], b = points[3 * v1 + k], c = points[3 * v2 + k];
+            const double mn = std::min(std::min(a, b), c), mx = std::max(std::max(a, b), c);
+            long long l = static_cast<long long>(std::floor((mn + 1.0) / cell)) - margin;
+            long long h = static_cast<long long>(std::floor((mx + 1.0) / cell)) + margin;
+            lo[3 * f + k] = static_cast<int>(std::min<long long>(std::max<long long>(l, 0), G - 1));
+            hi[3 * f + k] = static_cast<int>(std::min<long long>(std::max<long long>(h, 0), G - 1));
+        }
+        for (int z = lo[3 * f + 2]; z <= hi[3 * f + 2]; ++z)
+            for (int y = lo[3 * f + 1]; y <= hi[3 * f + 1]; ++y)
+                for (int x = lo[3 * f]; x <= hi[3 * f]; ++x) counts[x + static_cast<long long>(G) * (y + static_cast<long long>(G) * z) + 1]++;
+    }
+    for (long long c = 0; c < ncell; ++c) counts[c + 1] += counts[c];
+    *count = counts[ncell];
+    if (counts[ncell] >= (1LL << 31)) return csg::fail(CSG_ERR_ARG, "rotation grid: more than 2^31 entries");
+    for (long long c = 0; c <= ncell; ++c) offsets[c] = static_cast<int32_t>(counts[c]);
+    if (!cell_faces) return CSG_OK;  // size query
+    if (capacity < counts[ncell]) return csg::fail(CSG_ERR_ARG, "rotation grid: capacity %lld < %lld", capacity, counts[ncell]);
+    std::vector<long long> fill(counts.begin(), counts.end() - 1);
+    for (int f = 0; f < n_faces; ++f)
+        for (int z = lo[3 * f + 2]; z <= hi[3 * f + 2]; ++z)
+            for (int y = lo[3 * f + 1]; y <= hi[3 * f + 1]; ++y)
+                for (int x = lo[3 * f]; x <= hi[3 * f]; ++x)
+                    cell_faces[fill[x + static_cast<long long>(G) * (y + static_cast<long long>(G) * z)]++] = f;
+    return CSG_OK;
+}
+
+size_t csg_rotation_scratch_bytes(int n_surfaces, const int* n_src, const int* n_candidates, int tile) {
+    if (n_surfaces < 1 || !n_src || !n_candidates || (tile != 128 && tile != 256 && tile != 512)) return 0;
+    size_t bytes = align256(sizeof(RotSurface) * n_surfaces) + align256(sizeof(long long) * n_surfaces) + 256;
+    for (int s = 0; s < n_surfaces; ++s) {
+        const size_t tiles = (static_cast<size_t>(n_src[s]) + tile - 1) / tile;
+        bytes += align256(sizeof(double) * tiles * static_cast<size_t>(n_candidates[s]));
+    }
+    return bytes;
+}
+
+int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces, double* costs, int tile,
+                            int n_ctas, void* scratch, size_t scratch_bytes, csg_stream_t stream) {
+    if (n_surfaces < 1 || !surfaces || !costs || !scratch) return csg::fail(CSG_ERR_ARG, "rotation cost: bad arguments");
+    if (tile <= 0) tile = 256;
+    if (tile != 128 && tile != 256 && tile != 512) return csg::fail(CSG_ERR_ARG, "rotation cost: tile must be 128, 256 or 512");
+    std::vector<int> ns(n_surfaces), nc(n_surfaces);
+    for (int s = 0; s < n_surfaces; ++s) {
+        const csg_rotation_surface& in = surfaces[s];
+        if (!in.src_points || !in.src_values || !in.triangles || !in.faces || !in.tgt_values || !in.grid_offsets ||
+            !in.grid_faces || !in.matrices || in.n_src < 1 || in.n_candidates < 1 || in.grid_size < 4)
+            return csg::fail(CSG_ERR_ARG, "rotation cost: surface %d is incomplete", s);
+        ns[s] = in.n_src;
+        nc[s] = in.n_candidates;
+    }
+    if (scratch_bytes < csg_rotation_scratch_bytes(n_surfaces, ns.data(), nc.data(), tile))
+        return csg::fail(CSG_ERR_ARG, "rotation cost: scratch too small");
+    char* base = static_cast<char*>(scratch);
+    RotSurface* d_surf = reinterpret_cast<RotSurface*>(base);
+    size_t used = align256(sizeof(RotSurface) * n_surfaces);
+    long long* d_off = reinterpret_cast<long long*>(base + used);
+    used += align256(sizeof(long long) * n_surfaces);
+    int* d_err = reinterpret_cast<int*>(base + used);
+    used += 256;
+    std::vector<RotSurface> host(n_surfaces);
+    std::vector<long long> cost_off(n_surfaces);
+    long long items = 0, coff = 0;
+    int max_c = 0;
+    for (int s = 0; s < n_surfaces; ++s) {
+        const csg_rotation_surface& in = surfaces[s];
+        RotSurface& r = host[s];
+        r.src_points = in.src_points;
+        r.src_values = in.src_values;
+        r.triangles = in.triangles;
+        r.faces = in.faces;
+        r.tgt_values = in.tgt_values;
+        r.grid_offsets = in.grid_offsets;
+        r.grid_faces = in.grid_faces;
+        r.matrices = in.matrices;
+        r.n_src = in.n_src;
+        r.grid_size = in.grid_size;
+        r.n_candidates = in.n_candidates;
+        r.tiles = (in.n_src + tile - 1) / tile;
+        r.partials = reinterpret_cast<double*>(base + used);
+        used += align256(sizeof(double) * static_cast<size_t>(r.tiles) * r.n_candidates);
+        r.item_begin = items;
+        items += static_cast<long long>(r.tiles) * r.n_candidates;
+        cost_off[s] = coff;
+        coff += r.n_candidates;
+        max_c = std::max(max_c, r.n_candidates);
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    CSG_CUDA_CHECK(cudaMemcpyAsync(d_surf, host.data(), sizeof(RotSurface) * n_surfaces, cudaMemcpyHostToDevice, st));
+    CSG_CUDA_CHECK(cudaMemcpyAsync(d_off, cost_off.data(), sizeof(long long) * n_surfaces, cudaMemcpyHostToDevice, st));
+    CSG_CUDA_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    int device = 0, sms = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const long long want = n_ctas > 0 ? n_ctas : static_cast<long long>(sms) * (2048 / tile);
+    const unsigned blocks = static_cast<unsigned>(std::min<long long>(std::max<long long>(1, want), items));
+    switch (tile) {
+        case 128: k_rotation_cost<128><<<blocks, 128, 0, st>>>(d_surf, n_surfaces, items, d_err); break;
+        case 512: k_rotation_cost<512><<<blocks, 512, 0, st>>>(d_surf, n_surfaces, items, d_err); break;
+        default: k_rotation_cost<256><<<blocks, 256, 0, st>>>(d_surf, n_surfaces, items, d_err); break;
+    }
+    k_rotation_finalize<<<dim3((max_c + 127) / 128, n_surfaces), 128, 0, st>>>(d_surf, n_surfaces, costs, d_off);
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_rotation_status(const void* scratch, int n_surfaces, csg_stream_t stream, int* status) {
+    if (!scratch || !status || n_surfaces < 1) return csg::fail(CSG_ERR_ARG, "rotation status: bad arguments");
+    const size_t off = align256(sizeof(RotSurface) * n_surfaces) + align256(sizeof(long long) * n_surfaces);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    CSG_CUDA_CHECK(cudaMemcpyAsync(status, static_cast<const char*>(scratch) + off, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CSG_CUDA_CHECK(cudaStreamSynchronize(st));
+    return CSG_OK;
+}
+
+}  // extern "C"

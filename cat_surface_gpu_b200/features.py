@@ -1,0 +1,261 @@
+"""Stencil feature operators on the B200 (the operators of SurfaceStencilDevice).
+
+Composition follows ``src/cat_surface_gpu/surface_stencil.py:282-644``;
+every numeric step is a native kernel from ``csrc/features.cu``.  The only
+host synchronisation is the one the reference also makes: reading the mean
+edge length to derive the heat-kernel iteration count (``_heat_parameters``).
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import _native
+from .surface_stencil import SurfaceStencil, SurfaceStencilDevice
+
+_TOPOLOGY_CACHE: dict[tuple, tuple[torch.Tensor, ...]] = {}
+
+
+def _topology(faces: np.ndarray, n_points: int, device: torch.device):
+    f = np.ascontiguousarray(faces, dtype=np.int32)
+    key = (device.type, device.index, f.shape, n_points, f.tobytes())
+    cached = _TOPOLOGY_CACHE.get(key)
+    if cached is not None:
+        return cached
+    lib = _native.library()
+    off = np.zeros(n_points + 1, dtype=np.int32)
+    nbr = np.zeros(max(1, 6 * f.shape[0]), dtype=np.int32)
+    count = _native.check(lib.csg_mesh_neighbours(n_points, f.ctypes.data, f.shape[0], off.ctypes.data,
+                                                  nbr.ctypes.data, nbr.size), "csg_mesh_neighbours")
+    nbr = nbr[: max(1, count)]
+    # per-vertex incidences sorted by (corner, face): the reference's three index_add_ passes
+    vertex = f.T.reshape(-1).astype(np.int64)
+    corner = np.repeat(np.arange(3), f.shape[0])
+    face = np.tile(np.arange(f.shape[0]), 3)
+    order = np.lexsort((face, corner, vertex))
+    inc = ((face[order] << 2) | corner[order]).astype(np.int32)
+    inc_off = np.concatenate(([0], np.cumsum(np.bincount(vertex, minlength=n_points)))).astype(np.int32)
+    tensors = tuple(torch.from_numpy(a).to(device) for a in (off, nbr, inc_off, inc))
+    max_degree = int(np.diff(off).max()) if n_points else 0
+    cached = tensors + (max_degree,)
+    _TOPOLOGY_CACHE[key] = cached
+    return cached
+
+
+def upload_stencil(stencil: SurfaceStencil, device: torch.device, geometry_dtype: torch.dtype,
+                   weight_dtype: torch.dtype) -> SurfaceStencilDevice:
+    if weight_dtype != torch.float64:
+        raise ValueError("stencil weights are float64")
+    off, nbr, inc_off, inc, max_degree = _topology(stencil.faces, stencil.sphere_points.shape[0], device)
+    st = SurfaceStencilDevice(
+        sphere_points=torch.as_tensor(stencil.sphere_points, dtype=geometry_dtype, device=device).contiguous(),
+        faces=torch.as_tensor(np.ascontiguousarray(stencil.faces, dtype=np.int32), device=device).contiguous(),
+        surface_indices=torch.as_tensor(np.ascontiguousarray(stencil.surface_indices, dtype=np.int32), device=device),
+        surface_weights=torch.as_tensor(stencil.surface_weights, dtype=torch.float64, device=device).contiguous(),
+        sheet_indices=torch.as_tensor(np.ascontiguousarray(stencil.sheet_indices, dtype=np.int32), device=device),
+        sheet_weights=torch.as_tensor(stencil.sheet_weights, dtype=torch.float64, device=device).contiguous(),
+        nx=int(stencil.nx),
+        ny=int(stencil.ny),
+        source_points=int(stencil.source_points),
+        unit_sphere_points=None
+        if stencil.unit_sphere_points is None
+        else torch.as_tensor(stencil.unit_sphere_points, dtype=torch.float32, device=device).contiguous(),
+        neighbour_offsets=off,
+        neighbour_indices=nbr,
+        max_degree=max_degree,
+    )
+    st._cache["incidence"] = (inc_off, inc)
+    return st
+
+
+def _stream() -> int:
+    return _native.stream_handle()
+
+
+def _scratch(st: SurfaceStencilDevice, series: int = 1) -> torch.Tensor:
+    key = ("scratch", series)
+    buf = st._cache.get(key)
+    if buf is None:
+        n = int(st.sphere_points.shape[0])
+        need = _native.library().csg_feature_scratch_bytes(n, int(st.faces.shape[0]), int(st.neighbour_indices.numel()),
+                                                          series)
+        buf = torch.empty(int(need), dtype=torch.uint8, device=st.sphere_points.device)
+        st._cache[key] = buf
+    return buf
+
+
+def resample_vertices(st: SurfaceStencilDevice, vertices) -> torch.Tensor:
+    value = torch.as_tensor(vertices, device=st.sphere_points.device)
+    if value.ndim != 2 or tuple(value.shape) != (st.source_points, 3):
+        raise ValueError(f"vertices shape must be {(st.source_points, 3)}, got {tuple(value.shape)}")
+    if value.dtype not in (torch.float32, torch.float64):
+        value = value.to(torch.float64)
+    value = value.contiguous()
+    out = torch.empty((st.surface_indices.shape[0], 3), dtype=value.dtype, device=value.device)
+    dtype = _native.CSG_DTYPE_F32 if value.dtype == torch.float32 else _native.CSG_DTYPE_F64
+    _native.check(_native.library().csg_feature_resample(dtype, int(out.shape[0]), st.surface_indices.data_ptr(),
+                                                         st.surface_weights.data_ptr(), value.data_ptr(),
+                                                         out.data_ptr(), _stream()), "csg_feature_resample")
+    return out
+
+
+def map_values_to_sheet(st: SurfaceStencilDevice, values) -> torch.Tensor:
+    value = torch.as_tensor(values, device=st.sphere_points.device).reshape(-1).to(torch.float64).contiguous()
+    if value.numel() != st.sphere_points.shape[0]:
+        raise ValueError(f"values must contain {st.sphere_points.shape[0]} elements, got {value.numel()}")
+    out = torch.empty((st.ny, st.nx), dtype=torch.float64, device=value.device)
+    _native.check(_native.library().csg_feature_sheet_map(st.nx * st.ny, st.sheet_indices.data_ptr(),
+                                                          st.sheet_weights.data_ptr(), value.data_ptr(),
+                                                          out.data_ptr(), _stream()), "csg_feature_sheet_map")
+    return out
+
+
+def heat_parameters(st: SurfaceStencilDevice, vertices: torch.Tensor, fwhm: float) -> tuple[int, float]:
+    """Iteration count and sigma of the iterative heat kernel (reference 359-369)."""
+
+    v = vertices.contiguous()
+    dtype = _native.CSG_DTYPE_F32 if v.dtype == torch.float32 else _native.CSG_DTYPE_F64
+    scratch = _scratch(st)
+    total = st._cache.setdefault("edge_sum", torch.empty(1, dtype=torch.float64, device=v.device))
+    _native.check(_native.library().csg_feature_edge_sum(dtype, int(st.faces.shape[0]), st.faces.data_ptr(), v.data_ptr(),
+                                                         total.data_ptr(), scratch.data_ptr(), scratch.numel(),
+                                                         _stream()), "csg_feature_edge_sum")
+    edge_mean = float(total.item()) / (3.0 * int(st.faces.shape[0]))
+    raw = float(fwhm) * float(fwhm) * 0.541011 / (edge_mean * edge_mean)
+    iterations = max(1, int(math.ceil(raw)))
+    sigma = float(fwhm) * 0.7355345 / float(iterations ** 0.5)
+    return iterations, sigma
+
+
+def smooth_geometry(st: SurfaceStencilDevice, vertices, fwhm: float) -> torch.Tensor:
+    value = torch.as_tensor(vertices, device=st.sphere_points.device).to(torch.float32).contiguous()
+    iterations, _ = heat_parameters(st, value, fwhm)
+    out = torch.empty_like(value)
+    scratch = _scratch(st)
+    _native.check(_native.library().csg_feature_smooth_geometry(
+        int(value.shape[0]), st.neighbour_offsets.data_ptr(), st.neighbour_indices.data_ptr(), value.data_ptr(),
+        iterations, out.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream()), "csg_feature_smooth_geometry")
+    return out
+
+
+def _smooth_series(st, values, geometry, fwhms, via_norm: bool) -> torch.Tensor:
+    n = int(st.sphere_points.shape[0])
+    base = torch.as_tensor(values, device=st.sphere_points.device).to(torch.float64).reshape(-1).contiguous()
+    if base.numel() != n:
+        raise ValueError("values must have shape [sphere_points]")
+    geom = torch.as_tensor(geometry, device=st.sphere_points.device).contiguous()
+    if tuple(geom.shape) != (n, 3):
+        raise ValueError("vertices must have shape [sphere_points, 3]")
+    if geom.dtype not in (torch.float32, torch.float64):
+        geom = geom.to(torch.float64)
+    params = [heat_parameters(st, geom, f) for f in fwhms]
+    counts = ctypes_int_array([p[0] for p in params])
+    sigmas = _native.doubles([p[1] for p in params])
+    out = torch.empty((len(fwhms), n), dtype=torch.float64, device=base.device)
+    scratch = _scratch(st, len(fwhms))
+    dtype = _native.CSG_DTYPE_F32 if geom.dtype == torch.float32 else _native.CSG_DTYPE_F64
+    import ctypes
+
+    _native.check(_native.library().csg_feature_smooth_values(
+        n, st.neighbour_offsets.data_ptr(), st.neighbour_indices.data_ptr(), int(st.neighbour_indices.numel()), dtype,
+        geom.data_ptr(), base.data_ptr(), len(fwhms), ctypes.addressof(sigmas), ctypes.addressof(counts),
+        int(via_norm), out.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream()), "csg_feature_smooth_values")
+    return out
+
+
+def ctypes_int_array(values):
+    import ctypes
+
+    values = [int(v) for v in values]
+    return (ctypes.c_int32 * len(values))(*values)
+
+
+def smooth_values(st, values, vertices, fwhm: float) -> torch.Tensor:
+    """One FWHM (reference 390-412): distances through a vector norm, then squared."""
+
+    return _smooth_series(st, values, vertices, (float(fwhm),), True)[0]
+
+
+def smooth_values_many(st, values, vertices, fwhms) -> tuple[torch.Tensor, ...]:
+    """Several FWHMs in one batched smoothing (reference 414-476): squared distances summed."""
+
+    if not fwhms:
+        return ()
+    geometry = torch.as_tensor(vertices, device=st.sphere_points.device).to(torch.float64)
+    out = _smooth_series(st, values, geometry, tuple(fwhms), False)
+    return tuple(out[i] for i in range(len(fwhms)))
+
+
+def vertex_normals(st: SurfaceStencilDevice, vertices) -> torch.Tensor:
+    geometry = torch.as_tensor(vertices, device=st.sphere_points.device).to(torch.float32).contiguous()
+    inc_off, inc = st._cache["incidence"]
+    out = torch.empty_like(geometry)
+    _native.check(_native.library().csg_feature_vertex_normals(int(geometry.shape[0]), st.faces.data_ptr(),
+                                                               inc_off.data_ptr(), inc.data_ptr(), geometry.data_ptr(),
+                                                               out.data_ptr(), _stream()), "csg_feature_vertex_normals")
+    return out
+
+
+def _minmax(st: SurfaceStencilDevice, values: torch.Tensor) -> torch.Tensor:
+    v = values.contiguous()
+    rows = 1 if v.ndim == 1 else int(v.shape[0])
+    n = v.numel() // rows
+    out = torch.empty_like(v)
+    scratch = _scratch(st, max(1, rows))
+    _native.check(_native.library().csg_feature_minmax(n, rows, v.data_ptr(), out.data_ptr(), scratch.data_ptr(),
+                                                       scratch.numel(), _stream()), "csg_feature_minmax")
+    return out
+
+
+def _type5_base(st: SurfaceStencilDevice, geometry: torch.Tensor) -> torch.Tensor:
+    smoothed = smooth_geometry(st, geometry, 50.0)
+    normals = vertex_normals(st, smoothed)
+    out = torch.empty(int(geometry.shape[0]), dtype=torch.float64, device=geometry.device)
+    _native.check(_native.library().csg_feature_normal_displacement(int(geometry.shape[0]), smoothed.data_ptr(),
+                                                                    geometry.data_ptr(), normals.data_ptr(),
+                                                                    out.data_ptr(), _stream()),
+                  "csg_feature_normal_displacement")
+    return out
+
+
+def curvature_type5(st: SurfaceStencilDevice, vertices, fwhm: float) -> torch.Tensor:
+    geometry = torch.as_tensor(vertices, device=st.sphere_points.device).to(torch.float32).contiguous()
+    values = _smooth_series(st, _type5_base(st, geometry), geometry, (float(fwhm),), True)[0]
+    return _minmax(st, values)
+
+
+def curvature_type5_to_sheet_many(st: SurfaceStencilDevice, vertices, fwhms) -> tuple[torch.Tensor, ...]:
+    if not fwhms:
+        return ()
+    geometry = torch.as_tensor(vertices, device=st.sphere_points.device).to(torch.float32).contiguous()
+    base = _type5_base(st, geometry)
+    smoothed = _smooth_series(st, base, geometry.to(torch.float64), tuple(fwhms), False)
+    normalised = _minmax(st, smoothed)
+    maps = torch.stack([map_values_to_sheet(st, normalised[i]).reshape(-1) for i in range(len(fwhms))])
+    maps = _minmax(st, maps)
+    return tuple(maps[i].reshape(st.ny, st.nx) for i in range(len(fwhms)))
+
+
+def curvature_type2(st: SurfaceStencilDevice, vertices, fwhm: float) -> torch.Tensor:
+    geometry = torch.as_tensor(vertices, device=st.sphere_points.device).to(torch.float32).contiguous()
+    normals = vertex_normals(st, geometry)
+    values = torch.empty(int(geometry.shape[0]), dtype=torch.float64, device=geometry.device)
+    _native.check(_native.library().csg_feature_curvature2(int(geometry.shape[0]), st.neighbour_offsets.data_ptr(),
+                                                           st.neighbour_indices.data_ptr(), geometry.data_ptr(),
+                                                           normals.data_ptr(), values.data_ptr(), _stream()),
+                  "csg_feature_curvature2")
+    values = _smooth_series(st, values, geometry, (float(fwhm),), True)[0]
+    return _minmax(st, values)
+
+
+def curvature_to_sheet(st: SurfaceStencilDevice, vertices, fwhm: float, curvtype: int = 5) -> torch.Tensor:
+    if curvtype == 5:
+        values = curvature_type5(st, vertices, fwhm)
+    elif curvtype == 2:
+        values = curvature_type2(st, vertices, fwhm)
+    else:
+        raise NotImplementedError("The GPU surface backend supports only upstream curvtype 2 and 5")
+    return _minmax(st, map_values_to_sheet(st, values).reshape(-1)).reshape(st.ny, st.nx)

@@ -1,0 +1,420 @@
+"""SurfWarp initial-rotation search on a B200 (drop-in for the reference's surface_rotation).
+
+Public names and behaviour follow ``src/cat_surface_gpu/surface_rotation.py``:
+the 46 official seeds, the CSR grid index over target-sphere triangles,
+candidate costs, first-equal-minimum seed choice and CAT-ordered
+Nelder-Mead.  The grid is built by the native host builder; every cost is
+evaluated by ``csg_rotation_cost_batch`` (one persistent launch for any
+number of candidates and surfaces).  Rotation matrices are float32, built on
+the host exactly as the reference builds them.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native
+from .device import resolve_device
+
+
+def official_seed_grid_angles() -> np.ndarray:
+    """46 upstream seeds: identity, then alpha x beta x gamma (reference 14-23)."""
+
+    seed0 = (-0.6, -0.3, 0.0, 0.3, 0.6)
+    seed12 = (-0.3, 0.0, 0.3)
+    values = [(0.0, 0.0, 0.0)]
+    values.extend((a, b, c) for a in seed0 for b in seed12 for c in seed12)
+    return np.asarray(values, dtype=np.float64)
+
+
+def rotation_matrices_flat(angles) -> np.ndarray:
+    """Column-major flat float32 matrices Rz (Ry Rx) per angle row (reference 223-292)."""
+
+    a = np.asarray(angles, dtype=np.float64).reshape(-1, 3).astype(np.float32)
+    al, be, ga = a[:, 0], a[:, 1], a[:, 2]
+    z, o = np.zeros_like(al), np.ones_like(al)
+    rx = np.stack((o, z, z, z, np.cos(al), np.sin(al), z, -np.sin(al), np.cos(al)), axis=1)
+    ry = np.stack((np.cos(be), z, np.sin(be), z, o, z, -np.sin(be), z, np.cos(be)), axis=1)
+    rz = np.stack((np.cos(ga), np.sin(ga), z, -np.sin(ga), np.cos(ga), z, z, z, o), axis=1)
+    first = np.empty_like(rx)
+    out = np.empty_like(rx)
+    for r in range(3):
+        for c in range(3):
+            first[:, r + 3 * c] = (ry[:, r] * rx[:, 3 * c] + ry[:, r + 3] * rx[:, 1 + 3 * c]) + ry[:, r + 6] * rx[:, 2 + 3 * c]
+    for r in range(3):
+        for c in range(3):
+            out[:, r + 3 * c] = (rz[:, r] * first[:, 3 * c] + rz[:, r + 3] * first[:, 1 + 3 * c]) + rz[:, r + 6] * first[:, 2 + 3 * c]
+    return np.ascontiguousarray(out)
+
+
+@dataclass(frozen=True)
+class RotationGridIndex:
+    """Reusable CPU spatial index over target-sphere triangles (reference 26-179)."""
+
+    points: np.ndarray
+    faces: np.ndarray
+    candidate_table: np.ndarray | None
+    grid_size: int
+    margin: int
+    candidate_offsets: np.ndarray | None = None
+    candidate_faces: np.ndarray | None = None
+
+    @classmethod
+    def from_stencil(cls, stencil, *, grid_size: int = 128, margin: int = 1,
+                     include_dense_candidate_table: bool = True) -> "RotationGridIndex":
+        return cls.from_geometry(stencil.sphere_points, stencil.faces, grid_size=grid_size, margin=margin,
+                                 include_dense_candidate_table=include_dense_candidate_table)
+
+    @classmethod
+    def from_geometry(cls, points, faces, *, grid_size: int = 128, margin: int = 1,
+                      include_dense_candidate_table: bool = True) -> "RotationGridIndex":
+        points = np.ascontiguousarray(points, dtype=np.float64)
+        faces = np.ascontiguousarray(faces, dtype=np.int32)
+        if points.ndim != 2 or points.shape[1] != 3:
+            raise ValueError("points must have shape [n, 3]")
+        if faces.ndim != 2 or faces.shape[1] != 3:
+            raise ValueError("faces must have shape [m, 3]")
+        if grid_size < 4 or margin < 0:
+            raise ValueError("grid_size must be at least 4 and margin must be non-negative")
+        lib = _native.library()
+        offsets = np.zeros(grid_size ** 3 + 1, dtype=np.int32)
+        count = ctypes.c_longlong(0)
+        _native.check(
+            lib.csg_rotation_grid_build(points.ctypes.data, points.shape[0], faces.ctypes.data, faces.shape[0],
+                                        grid_size, margin, offsets.ctypes.data, None, 0, ctypes.addressof(count)),
+            "csg_rotation_grid_build",
+        )
+        flat = np.zeros(max(1, count.value), dtype=np.int32)
+        _native.check(
+            lib.csg_rotation_grid_build(points.ctypes.data, points.shape[0], faces.ctypes.data, faces.shape[0],
+                                        grid_size, margin, offsets.ctypes.data, flat.ctypes.data, flat.size,
+                                        ctypes.addressof(count)),
+            "csg_rotation_grid_build",
+        )
+        flat = flat[: count.value]
+        if count.value == 0:
+            raise ValueError("At least one triangle does not cover any spatial grid cell")
+        table = None
+        if include_dense_candidate_table:
+            widths = np.diff(offsets)
+            table = np.full((grid_size ** 3, int(widths.max())), -1, dtype=np.int32)
+            rows = np.repeat(np.arange(grid_size ** 3), widths)
+            cols = np.arange(flat.size) - np.repeat(offsets[:-1], widths)
+            table[rows, cols] = flat
+        return cls(points=points, faces=faces, candidate_table=table, grid_size=int(grid_size), margin=int(margin),
+                   candidate_offsets=offsets, candidate_faces=flat)
+
+    @property
+    def max_candidates(self) -> int:
+        if self.candidate_offsets is not None:
+            return int(np.diff(self.candidate_offsets).max())
+        return 0 if self.candidate_table is None else int(self.candidate_table.shape[1])
+
+    def to(self, device, *, geometry_dtype: torch.dtype = torch.float32, candidate_table_dtype: torch.dtype = torch.int32,
+           compressed_candidate_table: bool = True) -> "RotationGridIndexDevice":
+        """Upload the index (CSR always; candidate_table_dtype is accepted for compatibility)."""
+
+        target = resolve_device(device)
+        if geometry_dtype != torch.float32:
+            raise ValueError("the native rotation cost evaluates geometry in float32")
+        if self.candidate_offsets is None or self.candidate_faces is None:
+            raise ValueError("RotationGridIndex is missing candidate index")
+        triangles = self.points[self.faces.astype(np.int64)].astype(np.float32)
+        return RotationGridIndexDevice(
+            target_points=torch.as_tensor(self.points, dtype=torch.float32, device=target).contiguous(),
+            target_faces=torch.as_tensor(self.faces, dtype=torch.int32, device=target).contiguous(),
+            target_triangles=torch.as_tensor(triangles, device=target).contiguous(),
+            candidate_table=torch.empty(0, dtype=candidate_table_dtype, device=target),
+            grid_size=self.grid_size,
+            candidate_offsets=torch.as_tensor(self.candidate_offsets, device=target).contiguous(),
+            candidate_faces=torch.as_tensor(self.candidate_faces, device=target).contiguous(),
+        )
+
+
+@dataclass(frozen=True)
+class RotationCostInputs:
+    """Validated device tensors reused by every rotation candidate."""
+
+    source_points: torch.Tensor
+    source_values: torch.Tensor
+    target_values: torch.Tensor
+
+
+@dataclass(frozen=True)
+class RotationSearchResult:
+    """Seed costs, refined angles, matrix, cost, and iteration count."""
+
+    seed_angle: torch.Tensor
+    seed_cost: torch.Tensor
+    seed_costs: torch.Tensor
+    angle: torch.Tensor
+    cost: torch.Tensor
+    rotation_matrix: torch.Tensor
+    iterations: int
+
+
+class _Costing:
+    """Device buffers for repeated cost evaluations of one (index, inputs) pair."""
+
+    def __init__(self, index: "RotationGridIndexDevice", inputs: RotationCostInputs, capacity: int, tile: int = 256):
+        self.index, self.inputs, self.tile = index, inputs, tile
+        self.capacity = max(1, int(capacity))
+        dev = index.device
+        self.matrices = torch.empty((self.capacity, 9), dtype=torch.float32, device=dev)
+        self.costs = torch.empty(self.capacity, dtype=torch.float64, device=dev)
+        n_src = (ctypes.c_int * 1)(int(inputs.source_points.shape[0]))
+        n_cand = (ctypes.c_int * 1)(self.capacity)
+        need = _native.library().csg_rotation_scratch_bytes(1, ctypes.addressof(n_src), ctypes.addressof(n_cand), tile)
+        self.scratch = torch.empty(int(need), dtype=torch.uint8, device=dev)
+        self.pinned = torch.empty(self.capacity, dtype=torch.float64, pin_memory=True)
+
+    def evaluate(self, angles: np.ndarray) -> torch.Tensor:
+        mats = rotation_matrices_flat(angles)
+        count = mats.shape[0]
+        if count > self.capacity:
+            raise ValueError("more candidates than this costing context holds")
+        self.matrices[:count].copy_(torch.from_numpy(mats), non_blocking=False)
+        surface = _native.RotationSurface(
+            self.inputs.source_points.data_ptr(), self.inputs.source_values.data_ptr(),
+            self.index.target_triangles.data_ptr(), self.index.target_faces.data_ptr(),
+            self.inputs.target_values.data_ptr(), self.index.candidate_offsets.data_ptr(),
+            self.index.candidate_faces.data_ptr(), self.matrices.data_ptr(),
+            int(self.inputs.source_points.shape[0]), int(self.index.grid_size), int(count),
+        )
+        lib = _native.library()
+        stream = _native.stream_handle()
+        _native.check(
+            lib.csg_rotation_cost_batch(1, ctypes.addressof(surface), self.costs.data_ptr(), self.tile, 0,
+                                        self.scratch.data_ptr(), self.scratch.numel(), stream),
+            "csg_rotation_cost_batch",
+        )
+        status = ctypes.c_int(0)
+        _native.check(lib.csg_rotation_status(self.scratch.data_ptr(), 1, stream, ctypes.addressof(status)),
+                      "csg_rotation_status")
+        if status.value != 0:
+            raise RuntimeError("Rotation is not covered by target sphere candidate index")
+        return self.costs[:count]
+
+
+@dataclass
+class RotationGridIndexDevice:
+    """Evaluate CAT rotation candidates against a device-resident spatial index."""
+
+    target_points: torch.Tensor
+    target_faces: torch.Tensor
+    target_triangles: torch.Tensor
+    candidate_table: torch.Tensor
+    grid_size: int
+    candidate_offsets: torch.Tensor | None = None
+    candidate_faces: torch.Tensor | None = None
+
+    @property
+    def device(self) -> torch.device:
+        return self.target_points.device
+
+    def _rotation_matrices(self, angles) -> torch.Tensor:
+        a = torch.as_tensor(angles, dtype=torch.float64).detach().cpu().numpy()
+        if a.ndim == 1:
+            a = a.reshape(1, 3)
+        if a.ndim != 2 or a.shape[1] != 3:
+            raise ValueError("angles must have shape [candidates, 3]")
+        return torch.as_tensor(rotation_matrices_flat(a), device=self.device).reshape(-1, 3, 3)
+
+    def rotation_matrix(self, angles) -> torch.Tensor:
+        matrices = self._rotation_matrices(angles)
+        if matrices.shape[0] != 1:
+            raise ValueError("rotation_matrix accepts exactly one angle vector")
+        return matrices[0]
+
+    def rotate_points(self, source_points, angles) -> torch.Tensor:
+        """[C, n, 3]: p'_j = (p0 m[3j] + p1 m[3j+1]) + p2 m[3j+2] (reference 294-313)."""
+
+        source = torch.as_tensor(source_points, dtype=torch.float32, device=self.device).contiguous()
+        if source.ndim != 2 or source.shape[1] != 3:
+            raise ValueError("source_points must have shape [n, 3]")
+        m = self._rotation_matrices(angles).reshape(-1, 9)
+        p = source.unsqueeze(0)
+        cols = [(p[..., 0] * m[:, 3 * j, None] + p[..., 1] * m[:, 3 * j + 1, None]) + p[..., 2] * m[:, 3 * j + 2, None]
+                for j in range(3)]
+        return torch.stack(cols, dim=-1)
+
+    def prepare_cost_inputs(self, source_points, source_values, target_values) -> RotationCostInputs:
+        source = torch.as_tensor(source_points, dtype=torch.float32, device=self.device).contiguous()
+        sv = torch.as_tensor(source_values, dtype=torch.float64, device=self.device).reshape(-1).contiguous()
+        tv = torch.as_tensor(target_values, dtype=torch.float64, device=self.device).reshape(-1).contiguous()
+        if source.ndim != 2 or source.shape[1] != 3:
+            raise ValueError("source_points must have shape [n, 3]")
+        if sv.numel() != source.shape[0]:
+            raise ValueError("source_values length does not match source_points")
+        if tv.numel() != self.target_points.shape[0]:
+            raise ValueError("target_values length does not match the target sphere")
+        return RotationCostInputs(source_points=source, source_values=sv, target_values=tv)
+
+    def _costing(self, inputs: RotationCostInputs, capacity: int) -> _Costing:
+        cache = self.__dict__.setdefault("_costing_cache", {})
+        key = (id(inputs), capacity)
+        if key not in cache:
+            cache.clear()
+            cache[key] = _Costing(self, inputs, capacity)
+        return cache[key]
+
+    def cost_batch_prepared(self, inputs: RotationCostInputs, angles, *, point_chunk: int = 1024) -> torch.Tensor:
+        """float64 SSD per candidate rotation [C] (reference 512-546)."""
+
+        if point_chunk < 1:
+            raise ValueError("point_chunk must be positive")
+        if inputs.source_points.device != self.device:
+            raise ValueError("RotationCostInputs and the index must be on the same device")
+        a = torch.as_tensor(angles, dtype=torch.float64).detach().cpu().numpy()
+        if a.ndim == 1:
+            a = a.reshape(1, 3)
+        if a.ndim != 2 or a.shape[1] != 3:
+            raise ValueError("angles must have shape [candidates, 3]")
+        costing = self._costing(inputs, max(64, a.shape[0]))
+        return costing.evaluate(a).clone()
+
+    def cost_batch(self, source_points, source_values, target_values, angles, *, point_chunk: int = 1024):
+        inputs = self.prepare_cost_inputs(source_points, source_values, target_values)
+        return self.cost_batch_prepared(inputs, angles, point_chunk=point_chunk)
+
+    def coarse_seed_search_prepared(self, inputs: RotationCostInputs, *, point_chunk: int = 1024):
+        angles = torch.as_tensor(official_seed_grid_angles(), dtype=torch.float64, device=self.device)
+        costs = self.cost_batch_prepared(inputs, angles, point_chunk=point_chunk)
+        best = torch.argmin(costs)
+        return angles[best], costs[best], costs
+
+    def coarse_seed_search(self, source_points, source_values, target_values, *, point_chunk: int = 1024):
+        inputs = self.prepare_cost_inputs(source_points, source_values, target_values)
+        return self.coarse_seed_search_prepared(inputs, point_chunk=point_chunk)
+
+    def refine_nelder_mead_prepared(self, inputs: RotationCostInputs, initial_angles, *, point_chunk: int = 1024,
+                                    max_iter: int = 500, tol: float = 1.0e-4, simplex_step: float = 0.1):
+        """CAT-ordered Nelder-Mead with device-evaluated costs (reference 594-699)."""
+
+        if max_iter < 1 or tol < 0.0 or simplex_step <= 0.0:
+            raise ValueError("max_iter, tol, and simplex_step must be positive")
+        seed = torch.as_tensor(initial_angles, dtype=torch.float64).detach().cpu().numpy().reshape(-1)
+        if seed.size != 3:
+            raise ValueError("initial_angles must contain exactly three angles")
+        costing = self._costing(inputs, 64)
+
+        def cost(points: np.ndarray) -> np.ndarray:
+            return costing.evaluate(points).cpu().numpy()
+
+        simplex = np.stack((seed, seed + (simplex_step, 0.0, 0.0), seed + (0.0, simplex_step, 0.0),
+                            seed + (0.0, 0.0, simplex_step)))
+        f = cost(simplex).astype(np.float64)
+        iteration = 0
+        for iteration in range(max_iter):
+            highest, lowest, second = 0, 0, 1
+            for index in range(4):
+                if f[index] > f[highest]:
+                    second, highest = highest, index
+                elif f[index] > f[second] and index != highest:
+                    second = index
+                if f[index] < f[lowest]:
+                    lowest = index
+            centroid = np.zeros(3)
+            for index in range(4):
+                if index != highest:
+                    centroid += simplex[index]
+            centroid /= 3.0
+            reflected = centroid + (centroid - simplex[highest])
+            fr = cost(reflected[None])[0]
+            if fr < f[lowest]:
+                expanded = centroid + 2.0 * (reflected - centroid)
+                fe = cost(expanded[None])[0]
+                if fe < fr:
+                    simplex[highest], f[highest] = expanded, fe
+                else:
+                    simplex[highest], f[highest] = reflected, fr
+            elif fr < f[second]:
+                simplex[highest], f[highest] = reflected, fr
+            else:
+                contracted = centroid + 0.5 * (simplex[highest] - centroid)
+                fc = cost(contracted[None])[0]
+                if fc < f[highest]:
+                    simplex[highest], f[highest] = contracted, fc
+                else:
+                    shrunk = [simplex[lowest] + 0.5 * (simplex[index] - simplex[lowest]) for index in range(4)]
+                    targets = [index for index in range(4) if index != lowest]
+                    values = cost(np.stack([shrunk[index] for index in targets]))
+                    for index, value in zip(targets, values):
+                        simplex[index], f[index] = shrunk[index], value
+            if np.max(np.abs(f - f[lowest])) < tol:
+                break
+        dev = self.device
+        return (torch.as_tensor(simplex[lowest].copy(), device=dev), torch.as_tensor(float(f[lowest]), dtype=torch.float64, device=dev),
+                iteration + 1)
+
+    def refine_nelder_mead(self, source_points, source_values, target_values, initial_angles, *,
+                           point_chunk: int = 1024, max_iter: int = 500, tol: float = 1.0e-4,
+                           simplex_step: float = 0.1):
+        inputs = self.prepare_cost_inputs(source_points, source_values, target_values)
+        return self.refine_nelder_mead_prepared(inputs, initial_angles, point_chunk=point_chunk, max_iter=max_iter,
+                                                tol=tol, simplex_step=simplex_step)
+
+    def search_rotation(self, source_points, source_values, target_values, *, point_chunk: int = 1024,
+                        refine: bool = True, max_iter: int = 500, tol: float = 1.0e-4, simplex_step: float = 0.1):
+        inputs = self.prepare_cost_inputs(source_points, source_values, target_values)
+        return self.search_rotation_prepared(inputs, point_chunk=point_chunk, refine=refine, max_iter=max_iter,
+                                             tol=tol, simplex_step=simplex_step)
+
+    def search_rotation_prepared(self, inputs: RotationCostInputs, *, point_chunk: int = 1024, refine: bool = True,
+                                 max_iter: int = 500, tol: float = 1.0e-4, simplex_step: float = 0.1):
+        """46 seeds, then optional refinement (reference 749-785)."""
+
+        seed_angle, seed_cost, seed_costs = self.coarse_seed_search_prepared(inputs, point_chunk=point_chunk)
+        if refine:
+            angle, cost, iterations = self.refine_nelder_mead_prepared(inputs, seed_angle, point_chunk=point_chunk,
+                                                                       max_iter=max_iter, tol=tol,
+                                                                       simplex_step=simplex_step)
+        else:
+            angle, cost, iterations = seed_angle.clone(), seed_cost.clone(), 0
+        return RotationSearchResult(seed_angle=seed_angle.clone(), seed_cost=seed_cost.clone(), seed_costs=seed_costs,
+                                    angle=angle, cost=cost, rotation_matrix=self.rotation_matrix(angle),
+                                    iterations=iterations)
+
+
+def batched_costs(indices, inputs, angle_sets, *, tile: int = 256, n_ctas: int = 0) -> list[torch.Tensor]:
+    """Costs of many candidate sets on many surfaces in ONE persistent launch.
+
+    ``indices[i]`` (a RotationGridIndexDevice), ``inputs[i]`` (its
+    RotationCostInputs) and ``angle_sets[i]`` ([C_i, 3] angles) describe
+    surface i; surfaces may differ in size and candidate count.  Returns one
+    float64 cost tensor per surface, identical to
+    ``indices[i].cost_batch_prepared(inputs[i], angle_sets[i])``.
+    """
+
+    n = len(indices)
+    if n == 0 or len(inputs) != n or len(angle_sets) != n:
+        raise ValueError("indices, inputs and angle_sets must be non-empty and of equal length")
+    dev = indices[0].device
+    mats = [torch.as_tensor(rotation_matrices_flat(np.asarray(a)), device=dev) for a in angle_sets]
+    counts = [int(m.shape[0]) for m in mats]
+    costs = torch.empty(sum(counts), dtype=torch.float64, device=dev)
+    surfaces = (_native.RotationSurface * n)()
+    for i, (index, inp, m) in enumerate(zip(indices, inputs, mats)):
+        surfaces[i] = _native.RotationSurface(
+            inp.source_points.data_ptr(), inp.source_values.data_ptr(), index.target_triangles.data_ptr(),
+            index.target_faces.data_ptr(), inp.target_values.data_ptr(), index.candidate_offsets.data_ptr(),
+            index.candidate_faces.data_ptr(), m.data_ptr(), int(inp.source_points.shape[0]), int(index.grid_size),
+            counts[i],
+        )
+    n_src = (ctypes.c_int * n)(*[int(inp.source_points.shape[0]) for inp in inputs])
+    n_cand = (ctypes.c_int * n)(*counts)
+    lib = _native.library()
+    need = lib.csg_rotation_scratch_bytes(n, ctypes.addressof(n_src), ctypes.addressof(n_cand), tile)
+    scratch = torch.empty(int(need), dtype=torch.uint8, device=dev)
+    stream = _native.stream_handle()
+    _native.check(lib.csg_rotation_cost_batch(n, ctypes.addressof(surfaces), costs.data_ptr(), tile, n_ctas,
+                                              scratch.data_ptr(), scratch.numel(), stream), "csg_rotation_cost_batch")
+    status = ctypes.c_int(0)
+    _native.check(lib.csg_rotation_status(scratch.data_ptr(), n, stream, ctypes.addressof(status)), "csg_rotation_status")
+    if status.value != 0:
+        raise RuntimeError("Rotation is not covered by target sphere candidate index")
+    return list(torch.split(costs, counts))

@@ -1,0 +1,172 @@
+"""Spherical resampling stencils (drop-in for the reference's surface_stencil).
+
+``SurfaceStencil`` reads the ``.stencil`` v1/v2 files written by the
+upstream helper (format of ``src/cat_surface_gpu/surface_stencil.py:16-17,
+128-191``): an 8 x int32 header (magic 0x46534354, version, points,
+triangles, sheet cells, nx, ny, source points), float64 sphere points, int32
+faces, int32 + float64 surface barycentrics, int32 + float64 sheet
+barycentrics and (v2) float32 unit-sphere points of the source mesh.
+``SurfaceStencilDevice`` holds the device copies and runs the feature
+operators on native kernels (``csrc/features.cu``).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from pathlib import Path
+import struct
+
+import numpy as np
+import torch
+
+from .device import resolve_device
+
+_HEADER = struct.Struct("<8i")
+_MAGIC = 0x46534354
+
+
+@dataclass(frozen=True)
+class SurfaceStencil:
+    """CPU indices, barycentric weights, topology, and unit-sphere points."""
+
+    sphere_points: np.ndarray
+    faces: np.ndarray
+    surface_indices: np.ndarray
+    surface_weights: np.ndarray
+    sheet_indices: np.ndarray
+    sheet_weights: np.ndarray
+    nx: int
+    ny: int
+    source_points: int
+    unit_sphere_points: np.ndarray | None = None
+
+    @classmethod
+    def from_file(cls, path) -> "SurfaceStencil":
+        """Read a versioned stencil (reference 128-191); ValueError on a bad file."""
+
+        with Path(path).open("rb") as stream:
+            header = stream.read(_HEADER.size)
+            if len(header) != _HEADER.size:
+                raise ValueError("Stencil file")
+            magic, version, n_points, n_tri, n_sheet, nx, ny, source_points = _HEADER.unpack(header)
+            if magic != _MAGIC or version not in (1, 2):
+                raise ValueError("Stencil file magic or")
+            sphere_points = np.fromfile(stream, dtype="<f8", count=3 * n_points)
+            faces = np.fromfile(stream, dtype="<i4", count=3 * n_tri)
+            surface_indices = np.fromfile(stream, dtype="<i4", count=3 * n_points)
+            surface_weights = np.fromfile(stream, dtype="<f8", count=3 * n_points)
+            sheet_indices = np.fromfile(stream, dtype="<i4", count=3 * n_sheet)
+            sheet_weights = np.fromfile(stream, dtype="<f8", count=3 * n_sheet)
+            unit = np.fromfile(stream, dtype="<f4", count=3 * source_points) if version == 2 else None
+        sizes = (sphere_points.size, faces.size, surface_indices.size, surface_weights.size, sheet_indices.size,
+                 sheet_weights.size)
+        expected = (3 * n_points, 3 * n_tri, 3 * n_points, 3 * n_points, 3 * n_sheet, 3 * n_sheet)
+        if sizes != expected:
+            raise ValueError("Stencil file length")
+        if unit is not None and unit.size != 3 * source_points:
+            raise ValueError("Stencil unit sphere length")
+        return cls(
+            sphere_points=sphere_points.reshape(n_points, 3),
+            faces=faces.reshape(n_tri, 3),
+            surface_indices=surface_indices.reshape(n_points, 3),
+            surface_weights=surface_weights.reshape(n_points, 3),
+            sheet_indices=sheet_indices.reshape(ny, nx, 3),
+            sheet_weights=sheet_weights.reshape(ny, nx, 3),
+            nx=nx,
+            ny=ny,
+            source_points=source_points,
+            unit_sphere_points=None if unit is None else unit.reshape(source_points, 3),
+        )
+
+    def to_file(self, path) -> None:
+        """Write the v2 (v1 without unit points) layout read by ``from_file``."""
+
+        version = 1 if self.unit_sphere_points is None else 2
+        with Path(path).open("wb") as stream:
+            stream.write(_HEADER.pack(_MAGIC, version, self.sphere_points.shape[0], self.faces.shape[0],
+                                      self.nx * self.ny, self.nx, self.ny, self.source_points))
+            for array, dtype in ((self.sphere_points, "<f8"), (self.faces, "<i4"), (self.surface_indices, "<i4"),
+                                 (self.surface_weights, "<f8"), (self.sheet_indices, "<i4"),
+                                 (self.sheet_weights, "<f8")):
+                np.ascontiguousarray(array, dtype=dtype).tofile(stream)
+            if self.unit_sphere_points is not None:
+                np.ascontiguousarray(self.unit_sphere_points, dtype="<f4").tofile(stream)
+
+    def to(self, device, *, geometry_dtype: torch.dtype = torch.float32,
+           weight_dtype: torch.dtype = torch.float64) -> "SurfaceStencilDevice":
+        """Upload the stencil and its topology tables to one CUDA device (reference 193-272)."""
+
+        from . import features
+
+        target = resolve_device(device)
+        return features.upload_stencil(self, target, geometry_dtype, weight_dtype)
+
+
+@dataclass
+class SurfaceStencilDevice:
+    """Device-resident stencil, neighbour CSR and per-device feature workspace."""
+
+    sphere_points: torch.Tensor
+    faces: torch.Tensor
+    surface_indices: torch.Tensor
+    surface_weights: torch.Tensor
+    sheet_indices: torch.Tensor
+    sheet_weights: torch.Tensor
+    nx: int
+    ny: int
+    source_points: int
+    unit_sphere_points: torch.Tensor | None = None
+    neighbour_offsets: torch.Tensor | None = None
+    neighbour_indices: torch.Tensor | None = None
+    max_degree: int = 0
+    _cache: dict = field(default_factory=dict, repr=False)
+
+    def resample_vertices(self, vertices):
+        from . import features
+
+        return features.resample_vertices(self, vertices)
+
+    def map_values_to_sheet(self, values):
+        from . import features
+
+        return features.map_values_to_sheet(self, values)
+
+    def smooth_geometry(self, vertices, fwhm: float):
+        from . import features
+
+        return features.smooth_geometry(self, vertices, fwhm)
+
+    def smooth_values(self, values, vertices, fwhm: float):
+        from . import features
+
+        return features.smooth_values(self, values, vertices, float(fwhm))
+
+    def smooth_values_many(self, values, vertices, fwhms):
+        from . import features
+
+        return features.smooth_values_many(self, values, vertices, tuple(float(f) for f in fwhms))
+
+    def vertex_normals(self, vertices):
+        from . import features
+
+        return features.vertex_normals(self, vertices)
+
+    def curvature_type5(self, vertices, fwhm: float):
+        from . import features
+
+        return features.curvature_type5(self, vertices, fwhm)
+
+    def curvature_type5_to_sheet_many(self, vertices, fwhms):
+        from . import features
+
+        return features.curvature_type5_to_sheet_many(self, vertices, tuple(float(f) for f in fwhms))
+
+    def curvature_type2(self, vertices, fwhm: float):
+        from . import features
+
+        return features.curvature_type2(self, vertices, fwhm)
+
+    def curvature_to_sheet(self, vertices, fwhm: float, *, curvtype: int = 5):
+        from . import features
+
+        return features.curvature_to_sheet(self, vertices, fwhm, curvtype)

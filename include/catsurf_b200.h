@@ -254,6 +254,109 @@ CSG_API int csg_apply_flow_to_sphere(int dtype, int n, const float *unit_points,
  * [n][3] out (src/cat_surface_gpu/gpu_pipeline.py:248-271). */
 CSG_API int csg_average_xz(int n, const double *x_surface, const double *z_surface, float *out, csg_stream_t stream);
 
+/* ------------------------------------------------------------------------
+ * SurfWarp: initial-rotation search (host grid index, device costs).
+ * ---------------------------------------------------------------------- */
+
+/* Uniform grid over [-1, 1]^3 of grid_size^3 cells; each triangle is listed,
+ * in face order, in every cell its bounding box (+/- margin cells) covers.
+ * Replaces RotationGridIndex.from_geometry
+ * (src/cat_surface_gpu/surface_rotation.py:58-120).  offsets
+ * [grid_size^3 + 1]; with cell_faces NULL only offsets and *count are
+ * produced (size query). */
+CSG_API int csg_rotation_grid_build(const double *points, int n_points, const int32_t *faces, int n_faces,
+                                    int grid_size, int margin, int32_t *offsets, int32_t *cell_faces,
+                                    long long capacity, long long *count);
+
+/* One surface of a batched cost evaluation (all device pointers). */
+typedef struct {
+    const float *src_points;     /* [n_src][3] source sphere points */
+    const double *src_values;    /* [n_src] source feature */
+    const float *triangles;      /* [n_tri][9] target triangle corners */
+    const int32_t *faces;        /* [n_tri][3] target faces */
+    const double *tgt_values;    /* target feature per target point */
+    const int32_t *grid_offsets; /* csg_rotation_grid_build offsets */
+    const int32_t *grid_faces;   /* csg_rotation_grid_build cell faces */
+    const float *matrices;       /* [n_candidates][9] column-major rotations */
+    int32_t n_src;
+    int32_t grid_size;
+    int32_t n_candidates;
+} csg_rotation_surface;
+
+CSG_API size_t csg_rotation_scratch_bytes(int n_surfaces, const int *n_src, const int *n_candidates, int tile);
+
+/* SSD cost of every candidate rotation of every surface in one persistent
+ * launch: closest target triangle of each rotated source point (plane
+ * projection with a 1e-3 inside tolerance, else nearest edge), barycentric
+ * resampling of the target feature, float64 sum of squared differences.
+ * costs: concatenated [n_candidates] per surface.  tile (128/256/512) is the
+ * number of source points per work item; n_ctas 0 = fill the GPU.
+ * Replaces RotationGridIndexDevice.cost_batch_prepared
+ * (src/cat_surface_gpu/surface_rotation.py:354-546).  A query point whose
+ * cell has no candidate triangle sets CSG_ERR_COVERAGE (read with
+ * csg_rotation_status). */
+CSG_API int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface *surfaces, double *costs, int tile,
+                                    int n_ctas, void *scratch, size_t scratch_bytes, csg_stream_t stream);
+
+/* Synchronously read the coverage status of the last csg_rotation_cost_batch
+ * that used this scratch (CSG_OK or CSG_ERR_COVERAGE). */
+CSG_API int csg_rotation_status(const void *scratch, int n_surfaces, csg_stream_t stream, int *status);
+
+/* ------------------------------------------------------------------------
+ * SurfWarp: stencil feature operators (device).
+ * Replace SurfaceStencilDevice's operators
+ * (src/cat_surface_gpu/surface_stencil.py:282-644).  Neighbour lists are the
+ * unique ascending 1-ring CSR of csg_mesh_neighbours; sums run in that order.
+ * ---------------------------------------------------------------------- */
+
+/* resample_vertices (282-306): out[i] = sum_k w[i][k] * vertices[indices[i][k]];
+ * CSG_DTYPE_F32 sums float32-rounded float64 products, CSG_DTYPE_F64 sums in
+ * float64. */
+CSG_API int csg_feature_resample(int dtype, int n_out, const int32_t *indices, const double *weights,
+                                 const void *vertices, void *out, csg_stream_t stream);
+
+/* map_values_to_sheet (308-317), float64. */
+CSG_API int csg_feature_sheet_map(int n_cells, const int32_t *indices, const double *weights, const double *values,
+                                  double *out, csg_stream_t stream);
+
+/* Scratch for the feature operators below. */
+CSG_API size_t csg_feature_scratch_bytes(int n_points, int n_faces, int n_slots, int series);
+
+/* Sum of the 3 n_faces edge lengths in float64 (for _edge_mean_distance, 347-356). */
+CSG_API int csg_feature_edge_sum(int dtype, int n_faces, const int32_t *faces, const void *vertices, double *out_sum,
+                                 void *scratch, size_t scratch_bytes, csg_stream_t stream);
+
+/* smooth_geometry (372-388): `iterations` Jacobi heat steps, float32 out. */
+CSG_API int csg_feature_smooth_geometry(int n_points, const int32_t *nbr_off, const int32_t *nbr, const float *vertices,
+                                        int iterations, float *out, void *scratch, size_t scratch_bytes,
+                                        csg_stream_t stream);
+
+/* smooth_values / smooth_values_many (390-476): `series` independent
+ * smoothings of one value field (<= 16), sigma and iteration count per series
+ * (host arrays); via_norm selects the single-FWHM distance form.
+ * out [series][n_points]. */
+CSG_API int csg_feature_smooth_values(int n_points, const int32_t *nbr_off, const int32_t *nbr, int n_slots,
+                                      int geometry_dtype, const void *geometry, const double *values, int series,
+                                      const double *sigmas, const int32_t *iterations, int via_norm, double *out,
+                                      void *scratch, size_t scratch_bytes, csg_stream_t stream);
+
+/* vertex_normals (478-505); inc = per-vertex (face << 2 | corner) sorted by
+ * (corner, face), inc_off [n_points + 1]. */
+CSG_API int csg_feature_vertex_normals(int n_points, const int32_t *faces, const int32_t *inc_off, const int32_t *inc,
+                                       const float *vertices, float *out, csg_stream_t stream);
+
+/* ((smoothed - geometry) . normals) in float32, as float64 (curvature type 5, 512-515). */
+CSG_API int csg_feature_normal_displacement(int n_points, const float *smoothed, const float *geometry,
+                                            const float *normals, double *out, csg_stream_t stream);
+
+/* curvature_type2 point values before smoothing (552-615), float64. */
+CSG_API int csg_feature_curvature2(int n_points, const int32_t *nbr_off, const int32_t *nbr, const float *vertices,
+                                   const float *normals, double *out, csg_stream_t stream);
+
+/* (v - min) / (max - min) per row of `series` rows of n values. */
+CSG_API int csg_feature_minmax(int n, int series, const double *values, double *out, void *scratch,
+                               size_t scratch_bytes, csg_stream_t stream);
+
 /* Synchronously read a persistent kernel's status word from its scratch. */
 CSG_API int csg_read_status(const void *scratch, csg_stream_t stream, int *status, int *where);
 

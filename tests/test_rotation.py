@@ -1,0 +1,145 @@
+"""Rotation search: oracle pinned to the reference's outputs; native kernel parity.
+
+``tests/golden/rotation_golden.npz`` holds the reference's own results
+(torch CPU path) on a seeded sphere: grid CSR, candidate costs for the 46
+seeds plus random angles, and the full seed + Nelder-Mead search.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN
+from oracle import rotation as orot
+
+R = np.load(GOLDEN / "rotation_golden.npz")
+GRID = int(R["grid_size"])
+
+
+def _oracle_cost(angles):
+    return orot.cost_batch(R["target_points"], R["target_faces"], R["target_values"], R["source_points"],
+                           R["source_values"], angles, grid=(R["grid_offsets"], R["grid_faces"]), grid_size=GRID)
+
+
+def test_oracle_matches_reference_costs_and_search():
+    off, flat = orot.build_grid(R["target_points"], R["target_faces"], GRID, 1)
+    np.testing.assert_array_equal(off, R["grid_offsets"])
+    np.testing.assert_array_equal(flat, R["grid_faces"])
+    costs = _oracle_cost(R["angles"])
+    np.testing.assert_allclose(costs, R["costs"], rtol=1e-6)
+    best = int(np.argmin(costs[:46]))
+    np.testing.assert_array_equal(orot.seed_angles()[best], R["seed_angle"])
+    angle, cost, iterations = orot.nelder_mead(_oracle_cost, orot.seed_angles()[best])
+    np.testing.assert_allclose(angle, R["angle"], atol=1e-9)
+    np.testing.assert_allclose(cost, float(R["cost"]), rtol=1e-5)
+    assert iterations == int(R["iterations"])
+
+
+def test_seed_grid_order_like_reference():
+    """Reference test_surface_rotation.py:138-146."""
+
+    from cat_surface_gpu_b200.surface_rotation import official_seed_grid_angles
+
+    angles = official_seed_grid_angles()
+    assert angles.shape == (46, 3)
+    np.testing.assert_array_equal(angles[0], (0.0, 0.0, 0.0))
+    np.testing.assert_array_equal(angles[1], (-0.6, -0.3, -0.3))
+    np.testing.assert_array_equal(angles[23], (0.0, 0.0, 0.0))
+    np.testing.assert_array_equal(angles[-1], (0.6, 0.3, 0.3))
+
+
+def test_native_grid_builder_matches_reference(native_library):
+    from cat_surface_gpu_b200.surface_rotation import RotationGridIndex
+
+    index = RotationGridIndex.from_geometry(R["target_points"], R["target_faces"], grid_size=GRID, margin=1,
+                                            include_dense_candidate_table=True)
+    np.testing.assert_array_equal(index.candidate_offsets, R["grid_offsets"])
+    np.testing.assert_array_equal(index.candidate_faces, R["grid_faces"])
+    assert index.max_candidates == int(np.diff(R["grid_offsets"]).max())
+    row = int(np.argmax(np.diff(R["grid_offsets"])))
+    width = int(np.diff(R["grid_offsets"])[row])
+    np.testing.assert_array_equal(index.candidate_table[row, :width],
+                                  R["grid_faces"][R["grid_offsets"][row]: R["grid_offsets"][row] + width])
+
+
+@pytest.fixture(scope="module")
+def device_index(native_library):
+    from cat_surface_gpu_b200.surface_rotation import RotationGridIndex
+
+    return RotationGridIndex.from_geometry(R["target_points"], R["target_faces"], grid_size=GRID, margin=1,
+                                           include_dense_candidate_table=False).to("cuda")
+
+
+@pytest.mark.gpu
+def test_costs_match_oracle_and_reference(device_index):
+    got = device_index.cost_batch(R["source_points"], R["source_values"], R["target_values"], R["angles"]).cpu().numpy()
+    np.testing.assert_allclose(got, _oracle_cost(R["angles"]), rtol=1e-12)
+    np.testing.assert_allclose(got, R["costs"], rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_rotate_points_identity_and_convention(device_index):
+    pts = torch.as_tensor(R["source_points"])
+    rotated = device_index.rotate_points(pts, torch.zeros((1, 3), dtype=torch.float64))
+    np.testing.assert_array_equal(rotated[0].cpu().numpy(), R["source_points"])
+    got = device_index.rotate_points(pts, R["angles"][:5]).cpu().numpy()
+    np.testing.assert_allclose(got, R["rotated"], rtol=0, atol=3e-7)
+
+
+@pytest.mark.gpu
+def test_search_matches_reference(device_index):
+    result = device_index.search_rotation(R["source_points"], R["source_values"], R["target_values"])
+    np.testing.assert_array_equal(result.seed_angle.cpu().numpy(), R["seed_angle"])
+    np.testing.assert_allclose(result.seed_costs.cpu().numpy(), R["seed_costs"], rtol=1e-6)
+    np.testing.assert_allclose(result.angle.cpu().numpy(), R["angle"], atol=1e-6)
+    np.testing.assert_allclose(float(result.cost), float(R["cost"]), rtol=1e-5)
+    assert result.iterations == int(R["iterations"])
+    np.testing.assert_allclose(result.rotation_matrix.cpu().numpy(), R["matrix"], atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_batched_surfaces_equal_single_surface_costs(native_library):
+    """Uneven surfaces and candidate counts in one persistent launch == per-surface launches."""
+
+    from cat_surface_gpu_b200 import synthetic
+    from cat_surface_gpu_b200.surface_rotation import RotationGridIndex, batched_costs
+
+    rng = np.random.default_rng(3)
+    indices, inputs, angle_sets = [], [], []
+    for n_sub, count in ((3, 7), (4, 130), (2, 33)):
+        tp, tf = synthetic.unit_icosphere(n_sub)
+        sp = tp + rng.normal(scale=0.02, size=tp.shape)
+        sp /= np.linalg.norm(sp, axis=1, keepdims=True)
+        index = RotationGridIndex.from_geometry(tp, tf, grid_size=24, margin=1,
+                                                include_dense_candidate_table=False).to("cuda")
+        indices.append(index)
+        inputs.append(index.prepare_cost_inputs(sp.astype(np.float32), np.sin(3 * sp[:, 0]), np.sin(3 * tp[:, 0])))
+        angle_sets.append(rng.uniform(-0.5, 0.5, size=(count, 3)))
+    together = batched_costs(indices, inputs, angle_sets)
+    for index, inp, angles, got in zip(indices, inputs, angle_sets, together):
+        alone = index.cost_batch_prepared(inp, angles)
+        np.testing.assert_array_equal(got.cpu().numpy(), alone.cpu().numpy())
+
+
+@pytest.mark.gpu
+def test_tetrahedron_known_answers(native_library):
+    """Reference test_surface_rotation.py:37-62 and 149-202: identity cost 0, first-minimum rules."""
+
+    from cat_surface_gpu_b200.surface_rotation import RotationGridIndex
+
+    points = np.asarray(((1.0, 0.0, 0.0), (-1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0)), dtype=np.float32)
+    faces = np.asarray(((0, 2, 3), (2, 1, 3), (1, 0, 3), (0, 1, 2)), dtype=np.int32)
+    index = RotationGridIndex.from_geometry(points, faces, grid_size=16, margin=16).to("cuda")
+    values = np.array([1.0, 2.0, 3.0, 4.0])
+    costs = index.cost_batch(points, values, values, np.zeros((1, 3)))
+    assert float(costs[0]) == 0.0
+    zeros = np.zeros(4)
+    best_angle, best_cost, seed_costs = index.coarse_seed_search(points, zeros, zeros)
+    assert seed_costs.shape == (46,)
+    np.testing.assert_array_equal(best_angle.cpu().numpy(), np.zeros(3))
+    assert float(best_cost) == 0.0
+    angle, cost, iterations = index.refine_nelder_mead(points, zeros, zeros, np.zeros(3))
+    np.testing.assert_array_equal(angle.cpu().numpy(), np.zeros(3))
+    assert float(cost) == 0.0 and iterations == 1
