@@ -79,6 +79,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_feature_normal_displacement": (_I, [_I, _P, _P, _P, _P, _P]),
     "csg_feature_curvature2": (_I, [_I, _P, _P, _P, _P, _P, _P]),
     "csg_feature_minmax": (_I, [_I, _I, _P, _P, _P, c_size_t, _P]),
+    "csg_stencil_build": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
     "csg_read_status": (_I, [_P, _P, _P, _P]),
 }
 

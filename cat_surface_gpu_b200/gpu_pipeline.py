@@ -1,0 +1,376 @@
+"""End-to-end CAT_SurfWarp-compatible registration on a B200 (drop-in for the reference's gpu_pipeline).
+
+``run_cat_surface_gpu_pipeline`` follows the reference's flow
+(``src/cat_surface_gpu/gpu_pipeline.py:468-1326``): stencils for both
+spheres, rotation features, 46-seed + Nelder-Mead rotation search, the
+rotated source stencil, ``runs`` DARTEL solves with the final warp applied
+between runs, the ``-avg`` pole-rotated solve and its blend, GIFTI output.
+
+Helpers: every stencil comes from ``stencil_builder`` -- a path to the
+reference's helper binary (as the reference runs it) or ``"native"`` (the
+host builder ``csg_stencil_build``).  Rotation features come from
+``rotation_values_path``, from the reference's helpers
+(``official-cpu`` / ``cuda-official-depth``), or from ``"native-curvature"``:
+the type-5 curvature of the resampled surfaces heat-smoothed with the
+reference's rotation FWHMs (15 source, 10 target) and min-max normalised.
+"""
+
+from __future__ import annotations
+
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass
+import math
+import os
+from pathlib import Path
+import subprocess
+import tempfile
+import time
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from .device import resolve_device
+from .gifti import GiftiMesh, read_gifti_mesh, write_gifti_mesh
+from .rotation_pipeline import RotationPipeline, read_rotation_values
+from .surface_stencil import SurfaceStencil, build_surface_stencil
+from .surface_warp import apply_flow_to_stenciled_sphere, average_xz_surfaces, solve_dartel_from_surfaces
+
+
+@dataclass(frozen=True)
+class CatSurfaceGpuResult:
+    """Final mesh data, rotation diagnostics, timings, and output path."""
+
+    vertices: np.ndarray
+    faces: np.ndarray
+    rotation_angle: np.ndarray
+    rotation_cost: float
+    timings: dict[str, float]
+    output_path: Path
+
+
+def _resolve_dartel_dtype(value) -> torch.dtype:
+    if isinstance(value, torch.dtype):
+        resolved = value
+    else:
+        mapping = {"float32": torch.float32, "fp32": torch.float32, "float64": torch.float64, "fp64": torch.float64}
+        try:
+            resolved = mapping[str(value).lower().replace("torch.", "")]
+        except KeyError as error:
+            raise ValueError("dartel_dtype must be float32/fp32 or float64/fp64") from error
+    if resolved not in {torch.float32, torch.float64}:
+        raise ValueError("dartel_dtype must be torch.float32 or torch.float64")
+    return resolved
+
+
+def _run_checked(command: Sequence[str], label: str, environment: dict | None = None) -> None:
+    completed = subprocess.run([str(item) for item in command], check=False, capture_output=True, text=True,
+                               env=environment)
+    if completed.returncode != 0:
+        raise RuntimeError(f"{label} failed with exit code {completed.returncode}\n"
+                           f"stdout:\n{completed.stdout.strip()[-1000:]}\nstderr:\n{completed.stderr.strip()[-2000:]}")
+
+
+def normalise_sphere(vertices: np.ndarray) -> np.ndarray:
+    """Centre on the vertex mean and project to unit length (reference 274-305).
+
+    The centre is the sequential float64 sum of the float32 coordinates, as in
+    the reference's per-vertex loop.
+    """
+
+    value = np.ascontiguousarray(np.asarray(vertices, dtype=np.float32))
+    if value.ndim != 2 or value.shape[1] != 3:
+        raise ValueError(f"Sphere vertices must have shape [n, 3], got {value.shape}")
+    centre = np.cumsum(value.astype(np.float64), axis=0)[-1]
+    centered = (value.astype(np.float64) - centre / value.shape[0]).astype(np.float32)
+    c = centered.astype(np.float64)
+    length = np.sqrt((c[:, 0] * c[:, 0] + c[:, 1] * c[:, 1]) + c[:, 2] * c[:, 2])
+    if not np.all(np.isfinite(length)) or np.any(length == 0.0):
+        raise ValueError("Sphere contains a vertex that cannot be normalized")
+    return np.ascontiguousarray((c * (1.0 / length)[:, None]).astype(np.float32))
+
+
+def rotation_matrix_from_angles(angles) -> torch.Tensor:
+    """float64 Rz (Ry Rx) as a 3x3 CPU tensor (reference 308-369).
+
+    Built with torch's float64 sin/cos and the same column-major product
+    order as the reference, so the matrix is bit-identical to it.
+    """
+
+    value = torch.as_tensor(np.asarray(angles, dtype=np.float64)).reshape(-1)
+    if value.numel() != 3:
+        raise ValueError("Rotation must contain exactly three angles")
+    ca = [torch.cos(angle) for angle in value.unbind()]
+    sa = [torch.sin(angle) for angle in value.unbind()]
+    one, zero = torch.ones((), dtype=torch.float64), torch.zeros((), dtype=torch.float64)
+    rx = (one, zero, zero, zero, ca[0], sa[0], zero, -sa[0], ca[0])
+    ry = (ca[1], zero, sa[1], zero, one, zero, -sa[1], zero, ca[1])
+    rz = (ca[2], sa[2], zero, -sa[2], ca[2], zero, zero, zero, one)
+
+    def product(left, right):
+        out = [None] * 9
+        for r in range(3):
+            for c in range(3):
+                out[r + 3 * c] = ((zero + left[r] * right[3 * c]) + left[r + 3] * right[1 + 3 * c]) \
+                    + left[r + 6] * right[2 + 3 * c]
+        return out
+
+    return torch.stack(product(rz, product(ry, rx))).reshape(3, 3)
+
+
+def rotate_vertices(vertices: np.ndarray, angles) -> np.ndarray:
+    """float32(vertices @ M^T) in float64 on the CPU, M = rotation_matrix_from_angles (reference 372-378)."""
+
+    sphere = torch.as_tensor(np.asarray(vertices), dtype=torch.float64)
+    rotated = sphere @ rotation_matrix_from_angles(angles).transpose(0, 1)
+    return np.ascontiguousarray(rotated.numpy(), dtype=np.float32)
+
+
+class _Stencils:
+    """Builds stencils with the native builder or a reference helper binary."""
+
+    def __init__(self, builder, threads: int, nx: int, ny: int, temp_dir: Path):
+        self.builder, self.threads, self.nx, self.ny, self.temp = builder, threads, nx, ny, temp_dir
+        self.count = 0
+
+    def build(self, sphere: GiftiMesh, surface_path: str | Path, *, normalize: bool,
+              sphere_path: str | Path | None = None) -> SurfaceStencil:
+        if self.builder in (None, "native"):
+            return build_surface_stencil(sphere.vertices, sphere.faces, nx=self.nx, ny=self.ny, normalize=normalize,
+                                         threads=self.threads)
+        self.count += 1
+        path = Path(sphere_path) if sphere_path is not None else self.temp / f"sphere-{self.count}.gii"
+        if sphere_path is None:
+            write_gifti_mesh(path, sphere)
+        output = self.temp / f"stencil-{self.count}.stencil"
+        options = ["--threads", str(self.threads), "--surface", str(surface_path)]
+        if not normalize:
+            options.insert(0, "--no-normalize")
+        _run_checked([self.builder, path, output, *options], "stencil builder")
+        return SurfaceStencil.from_file(output)
+
+
+def native_rotation_features(source_stencil, target_stencil, source_surface, target_surface, device,
+                             heat_fwhms=(15.0, 10.0)) -> tuple[np.ndarray, np.ndarray]:
+    """Type-5 curvature of the resampled surfaces at the rotation FWHMs, min-max normalised."""
+
+    out = []
+    for stencil, surface, fwhm in ((source_stencil, source_surface, heat_fwhms[0]),
+                                   (target_stencil, target_surface, heat_fwhms[1])):
+        st = stencil.to(device, geometry_dtype=torch.float32)
+        mapped = st.resample_vertices(torch.as_tensor(surface, dtype=torch.float32, device=device))
+        out.append(st.curvature_type5(mapped, float(fwhm)).cpu().numpy())
+    return out[0], out[1]
+
+
+def _official_rotation_features(probe, paths, target_stencil, source_stencil, device, temp: Path, raw_depth: bool):
+    output = temp / "rotation-values.bin"
+    environment = None
+    if raw_depth:
+        environment = os.environ.copy()
+        environment["CAT_SURFACE_GPU_ROTATION_RAW_DEPTH"] = "1"
+        environment["CAT_SURFACE_GPU_ROTATION_RAW_DEPTH_GEOMETRY"] = "1"
+    _run_checked([probe, *paths, output], "Rotation feature", environment)
+    source_values, target_values = read_rotation_values(output)
+    if not raw_depth:
+        return source_values, target_values
+    # reference rotation_feature.py:352-404: smooth raw depth on the helper's geometry (FWHM 50), min-max
+    values = []
+    for stencil, raw, side in ((source_stencil, source_values, "source"), (target_stencil, target_values, "target")):
+        raw_geo = Path(f"{output}.{side}.geometry").read_bytes()
+        count = int(np.frombuffer(raw_geo, dtype=np.int32, count=1)[0])
+        geometry = np.frombuffer(raw_geo, dtype=np.float64, count=3 * count, offset=4).reshape(count, 3).astype(np.float32)
+        st = stencil.to(device, geometry_dtype=torch.float32)
+        smoothed = st.smooth_values(torch.as_tensor(raw, device=device), torch.as_tensor(geometry, device=device), 50.0)
+        mn, mx = smoothed.amin(), smoothed.amax()
+        values.append(((smoothed - mn) / (mx - mn).clamp_min(torch.finfo(torch.float64).eps)).cpu().numpy())
+    return values[0], values[1]
+
+
+def run_cat_surface_gpu_pipeline(
+    source_surface_path, source_sphere_path, target_surface_path, target_sphere_path, output_path, *,
+    source_stencil_path=None, target_stencil_path=None, rotation_values_path=None, rotation_values_probe=None,
+    rotation_geometry_probe=None, rotation_depth_probe=None, stencil_builder="native", rotated_stencil_builder=None,
+    stencil_threads: int = 8, device="cuda", kernel: str = "triton", dartel_dtype=torch.float64,
+    squaring_kernel: str | None = None, steps: int = 2, runs: int = 1, avg: bool = False,
+    curvtypes: Sequence[int] = (5, 5, 2), fwhm: Sequence[float] = (5.0, 5.0 / 3.0, 5.0 / 9.0), loop: int = 6,
+    cycles: int = 3, nit: int = 3, its: int = 3, code: int = 1, point_chunk: int = 4096,
+    rotation_grid_size: int = 128, rotation_margin: int = 1, rotation_refine: bool = True,
+    rotation_max_iter: int = 500, rotation_tol: float = 1.0e-4, rotation_simplex_step: float = 0.1,
+    rotation_feature_backend: str = "auto", rotation_feature_solver: str = "colored-sor",
+    parallel_sides: bool = True, optimized_dartel: bool = True, cuda_graph: bool = True,
+    sheet_size: tuple[int, int] = (512, 256),
+) -> CatSurfaceGpuResult:
+    """Rotation, DARTEL runs, -avg blend and GIFTI output (reference 468-1326).
+
+    ``sheet_size`` is the DARTEL sheet (nx, ny) of natively built stencils;
+    helper-built stencils carry the helper's fixed 512 x 256.
+    """
+
+    if steps < 1 or steps > 3:
+        raise ValueError("steps must be between 1 and 3")
+    if runs < 1:
+        raise ValueError("runs must be positive")
+    if stencil_threads < 1 or stencil_threads > 256:
+        raise ValueError("stencil_threads must be between 1 and 256")
+    if len(curvtypes) < steps or len(fwhm) < steps:
+        raise ValueError("curvtypes and fwhm must contain at least 'steps' entries")
+    if rotation_max_iter < 1 or rotation_tol < 0.0 or rotation_simplex_step <= 0.0:
+        raise ValueError("rotation_max_iter, rotation_tol, and rotation_simplex_step must be positive")
+    backends = {"auto", "native-curvature", "cuda-official-depth", "official-cpu", "cuda", "cuda-official-geometry"}
+    if rotation_feature_backend not in backends:
+        raise ValueError(f"rotation_feature_backend must be one of {sorted(backends)}")
+    if rotation_feature_backend in {"cuda", "cuda-official-geometry"} and rotation_values_path is None:
+        raise NotImplementedError(f"rotation_feature_backend={rotation_feature_backend!r} needs the depth-potential "
+                                  "solver, which this package does not implement; use 'native-curvature', "
+                                  "'cuda-official-depth' or provide rotation_values_path")
+    if rotation_feature_backend == "auto":
+        rotation_feature_backend = "official-cpu" if rotation_values_probe is not None else "native-curvature"
+    solve_dtype = _resolve_dartel_dtype(dartel_dtype)
+    if device == "cpu" or str(device) == "cpu":
+        raise ValueError("The explicit GPU pipeline requires a CUDA device")
+    target_device = resolve_device(device)
+    if rotated_stencil_builder is None:
+        rotated_stencil_builder = stencil_builder
+    graph_requested = bool(cuda_graph and (runs + int(avg) >= 3))
+    timings: dict[str, float] = {}
+    total_start = time.perf_counter()
+    output = Path(output_path)
+    source_surface = read_gifti_mesh(source_surface_path)
+    source_sphere = read_gifti_mesh(source_sphere_path)
+    target_surface = read_gifti_mesh(target_surface_path)
+    target_sphere = read_gifti_mesh(target_sphere_path)
+    timings["input_read_seconds"] = time.perf_counter() - total_start
+    nx, ny = (int(v) for v in sheet_size)
+
+    with tempfile.TemporaryDirectory(prefix="cat_surface_b200_") as temp_name:
+        temp = Path(temp_name)
+        builder = _Stencils(stencil_builder, stencil_threads, nx, ny, temp)
+        rotated_builder = _Stencils(rotated_stencil_builder, stencil_threads, nx, ny, temp)
+        start = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=2) as pool:
+            src_future = pool.submit(
+                lambda: SurfaceStencil.from_file(source_stencil_path) if source_stencil_path else
+                builder.build(source_sphere, source_surface_path, normalize=True, sphere_path=source_sphere_path))
+            tgt_future = pool.submit(
+                lambda: SurfaceStencil.from_file(target_stencil_path) if target_stencil_path else
+                builder.build(target_sphere, target_surface_path, normalize=True, sphere_path=target_sphere_path))
+            source_stencil = src_future.result()
+            target_stencil = tgt_future.result()
+        timings["initial_stencil_seconds"] = time.perf_counter() - start
+
+        start = time.perf_counter()
+        if rotation_values_path is not None:
+            source_values, target_values = read_rotation_values(rotation_values_path)
+        elif rotation_feature_backend == "official-cpu":
+            if rotation_values_probe is None:
+                raise ValueError("official-cpu rotation features require rotation_values_probe")
+            source_values, target_values = _official_rotation_features(
+                rotation_values_probe, (source_surface_path, source_sphere_path, target_surface_path, target_sphere_path),
+                target_stencil, source_stencil, target_device, temp, raw_depth=False)
+        elif rotation_feature_backend == "cuda-official-depth":
+            if rotation_depth_probe is None:
+                raise ValueError("cuda-official-depth requires rotation_depth_probe")
+            source_values, target_values = _official_rotation_features(
+                rotation_depth_probe, (source_surface_path, source_sphere_path, target_surface_path, target_sphere_path),
+                target_stencil, source_stencil, target_device, temp, raw_depth=True)
+        else:
+            source_values, target_values = native_rotation_features(
+                source_stencil, target_stencil, source_surface.vertices, target_surface.vertices, target_device)
+        torch.cuda.synchronize(target_device)
+        timings["rotation_feature_seconds"] = time.perf_counter() - start
+
+        start = time.perf_counter()
+        rotation_pipeline = RotationPipeline.from_stencil(target_stencil, device=target_device,
+                                                          grid_size=rotation_grid_size, margin=rotation_margin)
+        torch.cuda.synchronize(target_device)
+        timings["rotation_index_upload_seconds"] = time.perf_counter() - start
+        start = time.perf_counter()
+        rotation = rotation_pipeline.search(source_stencil.sphere_points, source_values, target_values,
+                                            point_chunk=point_chunk, refine=rotation_refine,
+                                            max_iter=rotation_max_iter, tol=rotation_tol,
+                                            simplex_step=rotation_simplex_step)
+        torch.cuda.synchronize(target_device)
+        timings["rotation_search_seconds"] = time.perf_counter() - start
+
+        angle = rotation.angle.detach().cpu().numpy()
+        current_sphere = rotate_vertices(normalise_sphere(source_sphere.vertices), angle)
+        pole = np.asarray((0.0, np.pi / 2.0, 0.0))
+        avg_target_surface = rotate_vertices(target_surface.vertices, pole)
+        avg_target_sphere = rotate_vertices(normalise_sphere(target_sphere.vertices), pole)
+        start = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=2) as pool:
+            cur_future = pool.submit(rotated_builder.build, GiftiMesh(current_sphere, source_sphere.faces),
+                                     source_surface_path, normalize=False)
+            avg_future = pool.submit(rotated_builder.build, GiftiMesh(avg_target_sphere, target_sphere.faces),
+                                     target_surface_path, normalize=False) if avg else None
+            current_stencil = cur_future.result()
+            avg_target_stencil = avg_future.result() if avg_future is not None else None
+        timings["rotated_stencil_seconds"] = time.perf_counter() - start
+
+        target_dev = target_stencil.to(target_device)
+        current_dev = current_stencil.to(target_device)
+        source_surface_dev = torch.as_tensor(source_surface.vertices, dtype=torch.float32, device=target_device)
+        target_surface_dev = torch.as_tensor(target_surface.vertices, dtype=torch.float32, device=target_device)
+
+        def solve_one(src_vertices, tgt_vertices, src_stencil, tgt_stencil, solve_fwhm, solve_loop):
+            return solve_dartel_from_surfaces(src_vertices, tgt_vertices, src_stencil, tgt_stencil, fwhm=solve_fwhm,
+                                              curvtypes=tuple(curvtypes), n_steps=steps, loop=solve_loop,
+                                              cycles=cycles, nit=nit, its=its, code=code, kernel=kernel,
+                                              device=target_device, dtype=solve_dtype, squaring_kernel=squaring_kernel,
+                                              parallel_sides=parallel_sides, optimized=optimized_dartel,
+                                              cuda_graph=graph_requested)
+
+        dartel_start = time.perf_counter()
+        last_result = None
+        final_prewarp = None
+        avg_source_stencil = None
+        avg_source_sphere = None
+        avg_source_surface = None
+        for run_index in range(runs):
+            run_start = time.perf_counter()
+            base = float(fwhm[0])
+            run_fwhm = tuple(base / (3.0 ** (steps * (run_index + 1) + i)) for i in range(steps))
+            if avg and run_index == runs - 1:
+                final_prewarp = current_sphere.copy()
+                avg_source_surface = rotate_vertices(source_surface.vertices, pole)
+                avg_source_sphere = rotate_vertices(final_prewarp, pole)
+                avg_source_stencil = rotated_builder.build(GiftiMesh(avg_source_sphere, source_sphere.faces),
+                                                           source_surface_path, normalize=False)
+            solve = solve_one(source_surface_dev, target_surface_dev, current_dev, target_dev, run_fwhm, loop)
+            if not (avg and run_index == runs - 1):
+                current_sphere = apply_flow_to_stenciled_sphere(
+                    torch.as_tensor(current_sphere, dtype=torch.float32, device=target_device), solve.flow, current_dev, inverse=True,
+                    device=target_device, dtype=solve_dtype).cpu().numpy().astype(np.float32)
+            torch.cuda.synchronize(target_device)
+            timings[f"dartel_run_{run_index}_seconds"] = time.perf_counter() - run_start
+            last_result = solve
+            if run_index + 1 < runs:
+                current_stencil = rotated_builder.build(GiftiMesh(current_sphere, source_sphere.faces),
+                                                        source_surface_path, normalize=False)
+                current_dev = current_stencil.to(target_device)
+        if avg:
+            avg_fwhm = tuple(float(fwhm[0]) / (3.0 ** (steps * (runs + 1) + i)) for i in range(steps))
+            avg_start = time.perf_counter()
+            avg_source_dev = avg_source_stencil.to(target_device)
+            avg_result = solve_one(torch.as_tensor(avg_source_surface, dtype=torch.float32, device=target_device),
+                                   torch.as_tensor(avg_target_surface, dtype=torch.float32, device=target_device), avg_source_dev,
+                                   avg_target_stencil.to(target_device), avg_fwhm, loop)
+            main_warped = apply_flow_to_stenciled_sphere(torch.as_tensor(final_prewarp, dtype=torch.float32, device=target_device),
+                                                         last_result.flow, current_dev, inverse=True,
+                                                         device=target_device, dtype=solve_dtype)
+            avg_warped = apply_flow_to_stenciled_sphere(torch.as_tensor(avg_source_sphere, dtype=torch.float32, device=target_device),
+                                                        avg_result.flow, avg_source_dev, inverse=True,
+                                                        device=target_device, dtype=solve_dtype)
+            reverse = rotation_matrix_from_angles(-pole).to(device=target_device)
+            unrotated = avg_warped.to(torch.float64) @ reverse.transpose(0, 1)
+            combined = average_xz_surfaces(unrotated, main_warped, device=target_device)
+            current_sphere = combined.cpu().numpy().astype(np.float32)
+            timings["avg_dartel_seconds"] = time.perf_counter() - avg_start
+        timings["dartel_total_seconds"] = time.perf_counter() - dartel_start
+        final_mesh = GiftiMesh(current_sphere, source_sphere.faces)
+        write_gifti_mesh(output, final_mesh, reference_path=source_sphere_path)
+    timings["total_seconds"] = time.perf_counter() - total_start
+    return CatSurfaceGpuResult(vertices=final_mesh.vertices, faces=final_mesh.faces,
+                               rotation_angle=np.ascontiguousarray(angle, dtype=np.float64),
+                               rotation_cost=float(rotation.cost.detach().cpu()), timings=timings, output_path=output)

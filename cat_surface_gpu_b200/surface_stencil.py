@@ -170,3 +170,56 @@ class SurfaceStencilDevice:
         from . import features
 
         return features.curvature_to_sheet(self, vertices, fwhm, curvtype)
+
+
+_RESAMPLING_SPHERES: dict[int, tuple[np.ndarray, np.ndarray]] = {}
+
+
+def resampling_sphere(subdivisions: int = 6) -> tuple[np.ndarray, np.ndarray]:
+    """Unit icosphere used as the resampling sphere (6 subdivisions: 40,962 points / 81,920 triangles)."""
+
+    if subdivisions not in _RESAMPLING_SPHERES:
+        from .synthetic import unit_icosphere
+
+        points, faces = unit_icosphere(subdivisions)
+        _RESAMPLING_SPHERES[subdivisions] = (np.ascontiguousarray(points, dtype=np.float64),
+                                             np.ascontiguousarray(faces, dtype=np.int32))
+    return _RESAMPLING_SPHERES[subdivisions]
+
+
+def build_surface_stencil(sphere_vertices, sphere_faces, *, nx: int = 512, ny: int = 256, normalize: bool = True,
+                          subdivisions: int = 6, threads: int = 0) -> SurfaceStencil:
+    """Build a resampling stencil for a sphere mesh (native host builder, ``csg_stencil_build``).
+
+    Same contents as the reference's stencil helper (``--surface`` mode: the
+    surface shares the sphere's topology, so surface indices are sphere
+    vertex ids).  ``normalize=False`` matches the helper's
+    ``--no-normalize`` (for spheres that are already unit and centred).
+    """
+
+    from . import _native
+
+    sphere = np.ascontiguousarray(sphere_vertices, dtype=np.float32)
+    faces = np.ascontiguousarray(sphere_faces, dtype=np.int32)
+    if sphere.ndim != 2 or sphere.shape[1] != 3 or faces.ndim != 2 or faces.shape[1] != 3:
+        raise ValueError("sphere_vertices and sphere_faces must have shape [n, 3] and [m, 3]")
+    rpts, rfaces = resampling_sphere(subdivisions)
+    n = rpts.shape[0]
+    sphere_points = np.zeros((n, 3), dtype=np.float64)
+    surface_indices = np.zeros((n, 3), dtype=np.int32)
+    surface_weights = np.zeros((n, 3), dtype=np.float64)
+    sheet_indices = np.zeros((ny, nx, 3), dtype=np.int32)
+    sheet_weights = np.zeros((ny, nx, 3), dtype=np.float64)
+    unit = np.zeros(sphere.shape, dtype=np.float32)
+    _native.check(
+        _native.library().csg_stencil_build(
+            sphere.ctypes.data, sphere.shape[0], faces.ctypes.data, faces.shape[0], rpts.ctypes.data, n,
+            rfaces.ctypes.data, rfaces.shape[0], int(nx), int(ny), int(bool(normalize)), int(threads),
+            sphere_points.ctypes.data, surface_indices.ctypes.data, surface_weights.ctypes.data,
+            sheet_indices.ctypes.data, sheet_weights.ctypes.data, unit.ctypes.data,
+        ),
+        "csg_stencil_build",
+    )
+    return SurfaceStencil(sphere_points=sphere_points, faces=rfaces.copy(), surface_indices=surface_indices,
+                          surface_weights=surface_weights, sheet_indices=sheet_indices, sheet_weights=sheet_weights,
+                          nx=int(nx), ny=int(ny), source_points=int(sphere.shape[0]), unit_sphere_points=unit)

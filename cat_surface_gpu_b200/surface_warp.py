@@ -232,6 +232,53 @@ def solve_dartel_batch(source_maps, target_maps, *, loop: int = 6, lmreg: float 
     return solver.flows, solver.velocity, solver.metrics
 
 
+def solve_dartel_from_surfaces(source_vertices, target_vertices, source_stencil, target_stencil, *,
+                               fwhm: Sequence[float] = (5.0, 5.0 / 3.0, 5.0 / 9.0), curvtypes: Sequence[int] = (5, 5, 2),
+                               loop: int = 6, n_steps: int = 2, lmreg: float = 1e-3, cycles: int = 3, nit: int = 3,
+                               its: int = 3, code: int = 1, kernel: str = "auto", squaring_kernel: str | None = None,
+                               device="auto", dtype=torch.float64, parallel_sides: bool = True, optimized: bool = True,
+                               assume_initial_nonzero: bool = False, cuda_graph: bool = False) -> DartelSolveResult:
+    """Curvature sheets of both surfaces, then their DARTEL solve (reference 370-488)."""
+
+    if n_steps < 1 or n_steps > len(fwhm) or n_steps > len(curvtypes):
+        raise ValueError("n_steps must not exceed the lengths of fwhm and curvtypes")
+    if squaring_kernel not in {None, "auto", "torch", "triton"}:
+        raise ValueError("squaring_kernel must be None, 'auto', 'torch', or 'triton'")
+    dev = resolve_device(device)
+    src_st = source_stencil.to(dev, geometry_dtype=torch.float32) if hasattr(source_stencil, "from_file") else source_stencil
+    tgt_st = target_stencil.to(dev, geometry_dtype=torch.float32) if hasattr(target_stencil, "from_file") else target_stencil
+    source = torch.as_tensor(source_vertices, device=dev).to(torch.float32).contiguous()
+    target = torch.as_tensor(target_vertices, device=dev).to(torch.float32).contiguous()
+    types = tuple(int(item) for item in curvtypes[:n_steps])
+    if any(item not in (2, 5) for item in types):
+        raise NotImplementedError("The device surface backend supports only upstream curvtype 2 and 5")
+
+    def build_maps(stencil, mapped):
+        if n_steps > 1 and all(item == 5 for item in types):
+            return stencil.curvature_type5_to_sheet_many(mapped, tuple(float(item) for item in fwhm[:n_steps]))
+        return tuple(stencil.curvature_to_sheet(mapped, float(fwhm[i]), curvtype=types[i]) for i in range(n_steps))
+
+    if parallel_sides:
+        current = torch.cuda.current_stream(dev)
+        streams = (torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev))
+        results = []
+        for stream, stencil, surface in zip(streams, (src_st, tgt_st), (source, target)):
+            stream.wait_stream(current)
+            with torch.cuda.stream(stream):
+                results.append(build_maps(stencil, stencil.resample_vertices(surface)))
+        for stream in streams:
+            current.wait_stream(stream)
+        source_maps, target_maps = results
+    else:
+        source_maps = build_maps(src_st, src_st.resample_vertices(source))
+        target_maps = build_maps(tgt_st, tgt_st.resample_vertices(target))
+    stacked_source = torch.stack(source_maps, dim=0).to(dtype=dtype).contiguous()
+    stacked_target = torch.stack(target_maps, dim=0).to(dtype=dtype).contiguous()
+    return solve_dartel_maps(stacked_source, stacked_target, loop=loop, lmreg=lmreg, cycles=cycles, nit=nit, its=its,
+                             code=code, kernel=kernel, squaring_kernel=squaring_kernel, device=dev, dtype=dtype,
+                             optimized=optimized, assume_initial_nonzero=assume_initial_nonzero, cuda_graph=cuda_graph)
+
+
 def apply_flow_to_sphere(sphere_vertices, flow, *, unit_sphere_vertices=None, inverse: bool = True, device="auto",
                          dtype=torch.float64) -> torch.Tensor:
     """Warp sphere points by a solved flow (reference 500-584)."""

@@ -357,6 +357,23 @@ CSG_API int csg_feature_curvature2(int n_points, const int32_t *nbr_off, const i
 CSG_API int csg_feature_minmax(int n, int series, const double *values, double *out, void *scratch,
                                size_t scratch_bytes, csg_stream_t stream);
 
+/* ------------------------------------------------------------------------
+ * SurfWarp: resampling stencils (host, float64, threaded, deterministic).
+ * Replaces the reference's stencil helper
+ * (native/cat_surface_stencil_builder.c:172-464) with the same outputs:
+ * sphere points (the resampling sphere moved onto the input sphere),
+ * surface barycentrics of the resampling sphere scaled to 0.975 x the mean
+ * input radius, sheet barycentrics of the nx x ny cell centres on the
+ * unit-normalised sphere points, and unit-sphere points of the input
+ * vertices.  The resampling sphere (points + faces) is the caller's; closest
+ * points are exact (lowest triangle index on ties).  normalize centres the
+ * input on its vertex mean and projects it to unit length first. */
+CSG_API int csg_stencil_build(const float *sphere, int n_sphere, const int32_t *sphere_faces, int n_sphere_faces,
+                              const double *resampling_points, int n_points, const int32_t *resampling_faces,
+                              int n_faces, int nx, int ny, int normalize, int threads, double *sphere_points_out,
+                              int32_t *surface_indices_out, double *surface_weights_out, int32_t *sheet_indices_out,
+                              double *sheet_weights_out, float *unit_points_out);
+
 /* Synchronously read a persistent kernel's status word from its scratch. */
 CSG_API int csg_read_status(const void *scratch, csg_stream_t stream, int *status, int *where);
 

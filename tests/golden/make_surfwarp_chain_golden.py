@@ -1,0 +1,165 @@
+"""Generate an end-to-end SurfWarp golden by running the reference package on CPU.
+
+Development container only (imports ``cat_surface_gpu`` from the reference
+checkout).  Follows ``src/cat_surface_gpu/gpu_pipeline.py:468-1326`` step by
+step with the reference's own operators on the CPU: stencils (built by this
+package's native host builder, read back through the reference's reader),
+rotation features (type-5 curvature of the resampled surfaces at FWHM 15 /
+10, the "native-curvature" backend), the 46-seed + Nelder-Mead rotation
+search, ``runs`` DARTEL solves with the inverse warp between runs, the
+pole-rotated ``-avg`` solve and the blend.
+
+Inputs: two folded icospheres (10,242 vertices, subdivision 5) with shared
+folding plus a per-subject perturbation; the source sphere is the unit
+icosphere under a known rotation, scaled to radius 100.  Writes
+``surfwarp_chain_golden.npz`` (inputs, parameters, rotation features,
+rotation angle/cost, the rotated sphere, the sphere after run 0, the final
+sphere).
+
+Usage: ``python tests/golden/make_surfwarp_chain_golden.py``
+"""
+
+from __future__ import annotations
+
+import os
+from pathlib import Path
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+os.environ.setdefault("PYTHONDONTWRITEBYTECODE", "1")
+sys.dont_write_bytecode = True
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+sys.path.insert(0, "/root/reference/src")
+
+import torch  # noqa: E402
+
+from cat_surface_gpu.gpu_pipeline import (  # noqa: E402
+    _average_xz_surfaces, _normalise_sphere, _rotate_vertices, _rotation_matrix_from_angles)
+from cat_surface_gpu.rotation_pipeline import RotationPipeline  # noqa: E402
+from cat_surface_gpu.surface_stencil import SurfaceStencil as ReferenceStencil  # noqa: E402
+from cat_surface_gpu.surface_warp import apply_flow_to_stenciled_sphere, solve_dartel_from_surfaces  # noqa: E402
+
+from cat_surface_gpu_b200 import synthetic  # noqa: E402
+from cat_surface_gpu_b200.surface_stencil import build_surface_stencil  # noqa: E402
+
+PARAMS = dict(nx=128, ny=64, steps=2, runs=2, avg=True, loop=6, rotation_grid_size=128)
+CPU = torch.device("cpu")
+
+
+def chain_inputs(seed: int = 5):
+    """Source/target surfaces and spheres on one 10,242-vertex icosphere topology."""
+
+    rng = np.random.default_rng(seed)
+    points, faces = synthetic.unit_icosphere(5)
+    shared = synthetic.real_sph_harm_sum(points, range(3, 15), 0.08, rng)
+    target_r = 1.0 + shared + synthetic.real_sph_harm_sum(points, range(3, 10), 0.02, rng)
+    source_r = 1.0 + shared + synthetic.real_sph_harm_sum(points, range(3, 10), 0.02, rng)
+    angle = np.array([0.12, -0.08, 0.18])
+    c, s = np.cos(angle), np.sin(angle)
+    rx = np.array([[1, 0, 0], [0, c[0], -s[0]], [0, s[0], c[0]]])
+    ry = np.array([[c[1], 0, s[1]], [0, 1, 0], [-s[1], 0, c[1]]])
+    rz = np.array([[c[2], -s[2], 0], [s[2], c[2], 0], [0, 0, 1]])
+    rotated = points @ (rz @ ry @ rx).T
+    jitter = rng.normal(scale=2e-3, size=points.shape)
+    return dict(
+        faces=faces.astype(np.int32),
+        source_surface=(points * (60.0 * source_r)[:, None]).astype(np.float32),
+        target_surface=(points * (60.0 * target_r)[:, None]).astype(np.float32),
+        source_sphere=(100.0 * (rotated + jitter)).astype(np.float32),
+        target_sphere=(100.0 * (points + rng.normal(scale=2e-3, size=points.shape))).astype(np.float32),
+    )
+
+
+def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size):
+    faces = data["faces"]
+    temp = Path(tempfile.mkdtemp(prefix="chain_golden_"))
+    count = [0]
+
+    def stencil(sphere, normalize):
+        count[0] += 1
+        path = temp / f"s{count[0]}.stencil"
+        build_surface_stencil(sphere, faces, nx=nx, ny=ny, normalize=normalize).to_file(path)
+        return ReferenceStencil.from_file(path)
+
+    def on_cpu(st):
+        return st.to(CPU, geometry_dtype=torch.float32)
+
+    source_stencil = stencil(data["source_sphere"], True)
+    target_stencil = stencil(data["target_sphere"], True)
+    values = []
+    for st, surface, fwhm in ((source_stencil, data["source_surface"], 15.0),
+                              (target_stencil, data["target_surface"], 10.0)):
+        dev = on_cpu(st)
+        mapped = dev.resample_vertices(torch.as_tensor(surface))
+        values.append(dev.curvature_type5(mapped, fwhm).numpy())
+    pipeline = RotationPipeline.from_stencil(target_stencil, device=CPU, grid_size=rotation_grid_size, margin=1)
+    rotation = pipeline.search(source_stencil.sphere_points, values[0], values[1], point_chunk=4096)
+    angle = rotation.angle.detach().cpu().numpy()
+    current_sphere = _rotate_vertices(_normalise_sphere(data["source_sphere"]), angle)
+    rotated_initial = current_sphere.copy()
+    pole = np.asarray((0.0, np.pi / 2.0, 0.0), dtype=np.float64)
+    avg_target_surface = _rotate_vertices(data["target_surface"], pole)
+    avg_target_sphere = _rotate_vertices(_normalise_sphere(data["target_sphere"]), pole)
+    current_dev = on_cpu(stencil(current_sphere, False))
+    target_dev = on_cpu(target_stencil)
+    source_surface = torch.as_tensor(data["source_surface"])
+    target_surface = torch.as_tensor(data["target_surface"])
+
+    def solve(src, tgt, src_st, tgt_st, fwhm):
+        return solve_dartel_from_surfaces(src, tgt, src_st, tgt_st, fwhm=fwhm, curvtypes=(5, 5, 2), n_steps=steps,
+                                          loop=loop, kernel="torch", device=CPU, dtype=torch.float64,
+                                          parallel_sides=False)
+
+    after_run0 = None
+    final_prewarp = avg_source_sphere = avg_source_surface = avg_source_dev = None
+    last = None
+    for run_index in range(runs):
+        run_fwhm = tuple(5.0 / (3.0 ** (steps * (run_index + 1) + i)) for i in range(steps))
+        if avg and run_index == runs - 1:
+            final_prewarp = current_sphere.copy()
+            avg_source_surface = _rotate_vertices(data["source_surface"], pole)
+            avg_source_sphere = _rotate_vertices(final_prewarp, pole)
+            avg_source_dev = on_cpu(stencil(avg_source_sphere, False))
+        last = solve(source_surface, target_surface, current_dev, target_dev, run_fwhm)
+        if not (avg and run_index == runs - 1):
+            current_sphere = apply_flow_to_stenciled_sphere(torch.as_tensor(current_sphere), last.flow, current_dev,
+                                                            inverse=True, device=CPU,
+                                                            dtype=torch.float64).numpy().astype(np.float32)
+        if run_index == 0:
+            after_run0 = current_sphere.copy()
+        if run_index + 1 < runs:
+            current_dev = on_cpu(stencil(current_sphere, False))
+    if avg:
+        avg_fwhm = tuple(5.0 / (3.0 ** (steps * (runs + 1) + i)) for i in range(steps))
+        avg_result = solve(torch.as_tensor(avg_source_surface), torch.as_tensor(avg_target_surface), avg_source_dev,
+                           on_cpu(stencil(avg_target_sphere, False)), avg_fwhm)
+        main_warped = apply_flow_to_stenciled_sphere(torch.as_tensor(final_prewarp), last.flow, current_dev,
+                                                     inverse=True, device=CPU, dtype=torch.float64)
+        avg_warped = apply_flow_to_stenciled_sphere(torch.as_tensor(avg_source_sphere), avg_result.flow,
+                                                    avg_source_dev, inverse=True, device=CPU, dtype=torch.float64)
+        reverse = _rotation_matrix_from_angles(-pole)
+        unrotated = avg_warped.to(torch.float64) @ reverse.transpose(0, 1)
+        current_sphere = _average_xz_surfaces(unrotated, main_warped, device=CPU).numpy().astype(np.float32)
+    return dict(rotation_angle=angle.astype(np.float64), rotation_cost=float(rotation.cost),
+                source_values=values[0], target_values=values[1],
+                rotated_initial=rotated_initial, after_run0=after_run0, final_sphere=current_sphere)
+
+
+def main() -> int:
+    torch.set_num_threads(max(1, os.cpu_count() or 1))
+    data = chain_inputs()
+    started = time.perf_counter()
+    result = reference_chain(data, **PARAMS)
+    print(f"reference chain on CPU: {time.perf_counter() - started:.1f} s, angle {result['rotation_angle']}, "
+          f"cost {result['rotation_cost']:.6f}")
+    np.savez_compressed(HERE / "surfwarp_chain_golden.npz", **data, **result,
+                        **{f"param_{k}": np.asarray(v) for k, v in PARAMS.items()})
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,126 @@
+"""CPU tests of the SurfWarp pipeline's host logic: sphere normalisation and
+rotation (bit-exact against the reference chain golden), the native stencil
+builder (properties and file round trip), and the command-line front end."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+
+@pytest.fixture(scope="module")
+def chain():
+    return dict(np.load(GOLDEN / "surfwarp_chain_golden.npz"))
+
+
+def test_normalise_and_rotate_match_reference_chain(chain):
+    from cat_surface_gpu_b200.gpu_pipeline import normalise_sphere, rotate_vertices
+
+    rotated = rotate_vertices(normalise_sphere(chain["source_sphere"]), chain["rotation_angle"])
+    assert rotated.dtype == np.float32
+    assert np.array_equal(rotated, chain["rotated_initial"])
+
+
+def test_rotation_matrix_is_orthonormal_and_inverts():
+    from cat_surface_gpu_b200.gpu_pipeline import rotation_matrix_from_angles
+
+    pole = np.array([0.0, np.pi / 2.0, 0.0])
+    m = rotation_matrix_from_angles(pole).numpy()
+    assert np.allclose(m @ m.T, np.eye(3), atol=1e-15)
+    # the -avg pole rotation takes the x axis onto the -z axis
+    assert np.allclose(np.array([1.0, 0.0, 0.0]) @ m.T, [0.0, 0.0, -1.0], atol=1e-15)
+    assert np.allclose(rotation_matrix_from_angles(-pole).numpy() @ m, np.eye(3), atol=1e-15)
+
+
+def test_normalise_rejects_degenerate_sphere():
+    from cat_surface_gpu_b200.gpu_pipeline import normalise_sphere
+
+    points = np.array([[1.0, 0.0, 0.0], [-1.0, 0.0, 0.0], [0.0, 0.0, 0.0]], dtype=np.float32)
+    with pytest.raises(ValueError):
+        normalise_sphere(points)
+    with pytest.raises(ValueError):
+        normalise_sphere(np.zeros((4, 2), dtype=np.float32))
+
+
+@pytest.fixture(scope="module")
+def stencil(native_library, chain):
+    from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+    return build_surface_stencil(chain["target_sphere"], chain["faces"], nx=64, ny=32, normalize=True, threads=4)
+
+
+def test_stencil_builder_properties(stencil, chain):
+    n_source = chain["target_sphere"].shape[0]
+    assert stencil.sphere_points.shape == (40962, 3) and stencil.faces.shape == (81920, 3)
+    assert stencil.sheet_indices.shape == (32, 64, 3)
+    # surface barycentrics index the source mesh; sheet barycentrics index the resampling sphere
+    for idx, w, bound in ((stencil.surface_indices, stencil.surface_weights, n_source),
+                          (stencil.sheet_indices, stencil.sheet_weights, 40962)):
+        assert idx.min() >= 0 and idx.max() < bound
+        assert w.min() >= -1e-9
+        assert np.allclose(w.sum(axis=-1), 1.0, atol=1e-9)
+    unit = stencil.unit_sphere_points.astype(np.float64)
+    assert np.allclose(np.linalg.norm(unit, axis=1), 1.0, atol=1e-6)
+    # sphere points are closest points on the flat triangles of the unit input sphere
+    norms = np.linalg.norm(stencil.sphere_points, axis=1)
+    assert norms.max() <= 1.0 + 1e-12 and norms.min() > 0.999
+    # surface barycentrics sit on a triangle next to the resampling direction: the interpolated
+    # unit sphere deviates from it by less than one input edge
+    edges = unit[chain["faces"][:, 0]] - unit[chain["faces"][:, 1]]
+    edge_angle = float(np.mean(np.linalg.norm(edges, axis=1)))
+    recon = np.einsum("pk,pkc->pc", stencil.surface_weights, unit[stencil.surface_indices])
+    direction = stencil.sphere_points / norms[:, None]
+    cosine = np.einsum("pc,pc->p", recon / np.linalg.norm(recon, axis=1, keepdims=True), direction)
+    assert cosine.min() > np.cos(edge_angle)
+
+
+def test_stencil_builder_is_deterministic_across_threads(stencil, chain):
+    from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+    other = build_surface_stencil(chain["target_sphere"], chain["faces"], nx=64, ny=32, normalize=True, threads=1)
+    for name in ("sphere_points", "surface_indices", "surface_weights", "sheet_indices", "sheet_weights",
+                 "unit_sphere_points"):
+        assert np.array_equal(getattr(stencil, name), getattr(other, name)), name
+
+
+def test_stencil_file_round_trip(stencil, tmp_path):
+    from cat_surface_gpu_b200.surface_stencil import SurfaceStencil
+
+    path = tmp_path / "s.stencil"
+    stencil.to_file(path)
+    back = SurfaceStencil.from_file(path)
+    assert (back.nx, back.ny, back.source_points) == (stencil.nx, stencil.ny, stencil.source_points)
+    for name in ("sphere_points", "faces", "surface_indices", "surface_weights", "sheet_indices", "sheet_weights",
+                 "unit_sphere_points"):
+        assert np.array_equal(getattr(back, name), getattr(stencil, name)), name
+    path.write_bytes(path.read_bytes()[:100])
+    with pytest.raises(ValueError):
+        SurfaceStencil.from_file(path)
+
+
+def test_stencil_builder_rejects_bad_topology(native_library):
+    from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+    points = np.eye(3, dtype=np.float32)
+    with pytest.raises(ValueError):
+        build_surface_stencil(points, np.array([[0, 1, 7]], dtype=np.int32), nx=8, ny=4)
+
+
+def test_cli_dispatch_and_pipeline_argument_checks(tmp_path):
+    from cat_surface_gpu_b200 import cli
+    from cat_surface_gpu_b200.gpu_pipeline import run_cat_surface_gpu_pipeline
+
+    assert cli.main([]) == 2
+    with pytest.raises(SystemExit):
+        cli.surfwarp_main(["--help"])
+    paths = [tmp_path / f"{i}.gii" for i in range(5)]
+    with pytest.raises(ValueError):
+        run_cat_surface_gpu_pipeline(*paths, steps=4)
+    with pytest.raises(ValueError):
+        run_cat_surface_gpu_pipeline(*paths, runs=0)
+    with pytest.raises(ValueError):
+        run_cat_surface_gpu_pipeline(*paths, rotation_feature_backend="nope")
+    with pytest.raises(ValueError):
+        run_cat_surface_gpu_pipeline(*paths, device="cpu")
