@@ -1,23 +1,40 @@
 #!/usr/bin/env python3
-"""Benchmark of the CAT-Surface hot path on B200.
+"""Benchmark of the CAT-Surface hot path on B200: one hemisphere of Surf2Sphere + SurfWarp.
 
-Workload (one "step" = one hemisphere): CAT_Surf2Sphere's 4,999 ordered
-area-smoothing sweeps (projection every 1,000) on the 61,442-vertex /
-122,880-face folded Fibonacci-hull mesh -- the stage-5 prefix produced by the
-upstream binary, stored in ``tests/golden/surf2sphere_c2.npz`` -- followed by
-the ellipsoid-to-sphere step.  Inputs are synthetic and seeded.
+Step (one hemisphere; ``value``, seconds per hemisphere): CAT_Surf2Sphere's
+4,999 ordered area-smoothing sweeps (projection every 1,000) of the
+61,442-vertex / 122,880-face folded Fibonacci hull (the stage 1-5 output of
+the upstream binary, ``tests/golden/surf2sphere_c2.npz``), the
+ellipsoid-to-sphere step, then CAT_SurfWarp of that surface and sphere to a
+second, differently seeded 61,442-vertex hull (``surf2sphere_c3.npz``, with
+the binary's sphere): native stencils, type-5 curvature rotation features,
+46-seed + Nelder-Mead rotation search, two runs of two DARTEL steps on a
+256 x 128 sheet in float64 (the reference's default; a float32 DARTEL exceeds
+the 1e-3 vertex bound, its error and time are reported beside), the ``-avg``
+pole solve and the blend.  Inputs are
+synthetic and seeded.  The sweep input is resident in HBM when the step
+starts; SurfWarp's mesh inputs are host arrays (its stencil builder is host
+code).  Timed with CUDA events on the launching stream around the whole
+step, L2 flushed by a 256 MiB device write before every step, max over ranks.
 
-``value`` is device time per hemisphere with inputs resident in HBM (CUDA
-events on the launching stream, L2 flushed by a 256 MiB write between
-steps, max over ranks).  ``e2e`` is the same metric through the public API
-``run_areal_smoothing_cuda`` with host (NumPy) inputs and outputs, host<->device
-copies inside the timed region.  Multi-GPU runs are independent replicas (the
-sweeps are one sequential Gauss-Seidel chain per hemisphere); ``value`` is the
-whole-job seconds per hemisphere.
+``e2e``: the same hemisphere through the public API with host buffers and
+files -- ``run_areal_smoothing_cuda`` on NumPy input, the sphere written as
+GIFTI, ``run_cat_surface_gpu_pipeline`` on the four GIFTI files.
 
-``--impl reference`` times the reference's CPU algorithm for the path (the
-oracle's C restatement; the reference's own sweep code exists only as a
-prebuilt upstream binary) on the host, on rank 0 only.
+Also on the line: ``batched_rotation`` (8 surfaces of 40,962-163,842 points
+x 4,096 uniform quaternions x 2 features in one persistent launch vs one
+launch per surface) and ``batched_dartel`` (16 registrations x 2 step maps on
+256 x 128 float32 sheets in one graph-captured batched solve vs 16 graphed
+one-at-a-time solves).
+
+Multi-GPU runs are independent replicas (a hemisphere is one sequential
+Gauss-Seidel chain plus one Nelder-Mead chain); ``value`` is whole-job
+seconds per hemisphere.
+
+``--impl reference`` times the reference's CPU algorithm for the path on the
+host (the oracle's restatement, the reference's own code being a prebuilt
+binary plus the torch CPU path that does not travel): bounded samples of each
+stage, scaled to one hemisphere.
 """
 
 from __future__ import annotations
@@ -35,30 +52,34 @@ import time
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+GOLDEN = ROOT / "tests" / "golden"
 
 METRIC = "s/hemisphere Surf2Sphere+SurfWarp @ max vtx err≤1e-3; batched regs/s vs plain"
 UNIT = "s/hemisphere"
-WORKLOAD = "Surf2Sphere 4,999 ordered area-smoothing sweeps, 61,442 vertices / 122,880 faces (stage-5 prefix of the seeded folded hull)"
-REFERENCE_SAMPLE_SWEEPS = 400
-CPU_BASELINE_SAMPLE_SWEEPS = 2000
+WORKLOAD = ("Surf2Sphere (4,999 ordered sweeps, 61,442 v / 122,880 f folded hull) + SurfWarp steps=2 runs=2 -avg "
+            "to a second 61,442-v hull, 256x128 float64 DARTEL sheet")
+SWEEPS = 4999
+SHEET = (256, 128)
+CHAIN = dict(steps=2, runs=2, avg=True, loop=6, sheet_size=SHEET, rotation_feature_backend="native-curvature")
+# stage counts of one hemisphere, for scaling the CPU samples
+DARTEL_STEPS = (CHAIN["runs"] + int(CHAIN["avg"])) * CHAIN["steps"] * CHAIN["loop"] * 3
+FEATURE_SIDES = 2 + 2 * (CHAIN["runs"] + int(CHAIN["avg"]))
 
 
 def parse_args():
     parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=10)
+    parser.add_argument("--steps", type=int, default=5)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("native", "reference"), default="native")
-    parser.add_argument("--sweeps", type=int, default=4999, help="sweeps per hemisphere (default: the full 4,999)")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-batched", action="store_true", help="skip the batched rotation / DARTEL legs")
+    parser.add_argument("--no-e2e", action="store_true")
     return parser.parse_args()
 
 
 def dist_env():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
 class ClockSampler:
@@ -113,73 +134,318 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": sm_max, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def load_workload():
+def load_meshes():
     import numpy as np
 
-    data = np.load(ROOT / "tests" / "golden" / "surf2sphere_c2.npz")
+    c2 = np.load(GOLDEN / "surf2sphere_c2.npz")
+    c3 = np.load(GOLDEN / "surf2sphere_c3.npz")
+    gold = np.load(GOLDEN / "surfwarp_chain_hemisphere_golden.npz")
     return {
-        "faces": data["faces"].astype(np.int32),
-        "prefix": data["prefix"],
-        "final": data["final"],
-        "source_area": float(data["source_area"]),
-        "binary_seconds": float(data["cpu_seconds"]),
+        "faces": c2["faces"].astype(np.int32), "surface": c2["surface"], "prefix": c2["prefix"],
+        "binary_sphere": c2["final"], "source_area": float(c2["source_area"]),
+        "binary_seconds": float(c2["cpu_seconds"]),
+        "target_faces": c3["faces"].astype(np.int32), "target_surface": c3["surface"], "target_sphere": c3["final"],
+        "chain_final": gold["final_sphere"], "chain_cpu_seconds": float(gold["cpu_seconds"]),
+        "chain_cpu_threads": int(gold["cpu_threads"]),
+        "rotation_evaluations": int(gold["rotation_candidates_evaluated"]),
     }
 
 
-def algorithmic_bytes_per_sweep(n: int, f: int) -> int:
+def projection_radius(prefix) -> float:
+    import numpy as np
+
+    return float(np.sqrt(np.max(np.sum(prefix.astype(np.float64) ** 2, axis=1))))
+
+
+def areal_bytes_per_sweep(n: int, f: int) -> int:
     # positions read + written, faces, incident list, offsets (unique elements)
     return n * (12 + 12) + f * 12 + 3 * f * 4 + (n + 1) * 4
 
 
-def cpu_oracle_seconds(workload, sweeps: int) -> float:
+def error_stats(reference, candidate) -> dict:
     import numpy as np
 
-    from oracle import areal as oracle
+    d = np.linalg.norm(np.asarray(candidate, np.float64) - np.asarray(reference, np.float64), axis=1)
+    return {"max": float(d.max()), "mean": float(d.mean()), "p99": float(np.quantile(d, 0.99))}
 
-    prefix = workload["prefix"]
-    radius = float(np.sqrt(np.max(np.sum(prefix.astype(np.float64) ** 2, axis=1))))
+
+# ---------------------------------------------------------------------------------------------- CPU (oracle) leg
+
+
+def cpu_hemisphere_sample(meshes) -> dict:
+    """Bounded samples of every stage of the oracle port, scaled to one hemisphere (one host thread)."""
+
+    import numpy as np
+
+    from oracle import areal as oa, dartel as od, features as of, rotation as orot
+    from cat_surface_gpu_b200 import synthetic
+    from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+    out = {}
+    sweeps = 200
     start = time.perf_counter()
-    oracle.areal_sweeps(prefix, workload["faces"], iterations=sweeps + 1, project_every=1000, radius=radius)
-    return time.perf_counter() - start
+    oa.areal_sweeps(meshes["prefix"], meshes["faces"], iterations=sweeps + 1, project_every=1000,
+                    radius=projection_radius(meshes["prefix"]))
+    out["sweeps"] = (time.perf_counter() - start) * SWEEPS / sweeps
+    nx, ny = SHEET
+    src = synthetic.smooth_sheet(ny, nx, 1).astype(np.float64)
+    tgt = synthetic.smooth_sheet(ny, nx, 2).astype(np.float64)
+    vel = np.zeros((2, ny, nx), dtype=np.float64)
+    start = time.perf_counter()
+    for k in (0, 5):  # the squaring count runs 0..5 over the loop; sample both ends
+        vel, _ = od.dartel_step(src, tgt, vel, k)
+    out["dartel"] = (time.perf_counter() - start) / 2 * DARTEL_STEPS
+    stencil = build_surface_stencil(meshes["target_sphere"], meshes["target_faces"], nx=nx, ny=ny, threads=1)
+    start = time.perf_counter()
+    stencil = build_surface_stencil(meshes["target_sphere"], meshes["target_faces"], nx=nx, ny=ny, threads=1)
+    out["stencils"] = (time.perf_counter() - start) * (5 + int(CHAIN["runs"] > 1))
+    mapped = of.resample_vertices(meshes["target_surface"], stencil.surface_indices, stencil.surface_weights)
+    start = time.perf_counter()
+    of.curvature_type5_to_sheet_many(mapped, stencil.faces, (5.0 / 9.0, 5.0 / 27.0), stencil.sheet_indices,
+                                     stencil.sheet_weights)
+    out["features"] = (time.perf_counter() - start) * FEATURE_SIDES
+    values = of.curvature_type5(mapped, stencil.faces, 10.0)
+    grid = orot.build_grid(stencil.sphere_points, stencil.faces)
+    angles = np.random.default_rng(0).uniform(-0.3, 0.3, size=(2, 3))
+    start = time.perf_counter()
+    orot.cost_batch(stencil.sphere_points, stencil.faces, values, stencil.sphere_points.astype(np.float32), values,
+                    angles, grid=grid)
+    out["rotation"] = (time.perf_counter() - start) / 2 * meshes["rotation_evaluations"]
+    out["total"] = sum(out.values())
+    return out
+
+
+CPU_SAMPLE = ("200 of 4,999 sweeps (C port, 1 thread); 2 dartel_steps (k=0, 5) of the "
+              f"{DARTEL_STEPS} per hemisphere (NumPy port); 1 stencil build of 6; 1 type-5 curvature sheet pair of "
+              f"{FEATURE_SIDES}; 2 rotation candidates of the reference search's count; each scaled linearly")
 
 
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
-    workload = load_workload()
-    sample = min(REFERENCE_SAMPLE_SWEEPS, args.sweeps)
+    meshes = load_meshes()
     for _ in range(args.warmup):
-        cpu_oracle_seconds(workload, sample)
-    times = [cpu_oracle_seconds(workload, sample) * args.sweeps / sample for _ in range(args.steps)]
-    value = sum(times) / len(times)
+        cpu_hemisphere_sample(meshes)
+    samples = [cpu_hemisphere_sample(meshes) for _ in range(args.steps)]
+    value = statistics.mean(s["total"] for s in samples)
     line = {
-        "metric": METRIC,
-        "value": value,
-        "unit": UNIT,
-        "impl": "reference",
-        "n_gpus": args.gpus,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": value * 1e3,
-        "higher_is_better": False,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32+f64",
-        "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sweeps": args.sweeps},
-        "cpu_baseline": {
-            "value": value,
-            "unit": UNIT,
-            "cores": 1,
-            "kind": "port",
-            "sample": f"{sample} of {args.sweeps} sweeps per step, scaled linearly; sequential Gauss-Seidel "
-            "(the upstream algorithm is single-threaded)",
-        },
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sweeps": SWEEPS, "sheet": list(SHEET)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": CPU_SAMPLE,
+                         "stages_s": {k: v for k, v in samples[-1].items() if k != "total"}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_torch_cpu_chain_s": meshes["chain_cpu_seconds"],
+        "reference_binary_surf2sphere_s": meshes["binary_seconds"],
     }
     print(json.dumps(line))
     return 0
+
+
+# ---------------------------------------------------------------------------------------------- GPU legs
+
+
+class Hemisphere:
+    """Device-resident inputs of the hemisphere chain and its step."""
+
+    def __init__(self, meshes, device, dartel_dtype):
+        import torch
+
+        from cat_surface_gpu_b200 import surf2sphere
+        from cat_surface_gpu_b200.gifti import GiftiMesh
+
+        self.meshes, self.device, self.dartel_dtype = meshes, device, dartel_dtype
+        self.topology = surf2sphere.Surf2SphereTopology.from_mesh(GiftiMesh(meshes["prefix"], meshes["faces"]))
+        self.plan = self.topology.plan
+        self.plan_device = self.plan.to_device(device)
+        self.pristine = torch.from_numpy(meshes["prefix"]).to(device)
+        self.points = torch.empty_like(self.pristine)
+        self.radius = projection_radius(meshes["prefix"])
+        self.launch = surf2sphere.tuned_areal_launch(self.pristine, self.plan_device, self.plan, arithmetic="cat",
+                                                     radius=self.radius)
+        self.scratch = None
+        self.meshes_in = (GiftiMesh(meshes["surface"], meshes["faces"]),
+                          GiftiMesh(meshes["target_surface"], meshes["target_faces"]),
+                          GiftiMesh(meshes["target_sphere"], meshes["target_faces"]))
+
+    def step(self, dartel_dtype=None):
+        import torch
+
+        from cat_surface_gpu_b200 import surf2sphere
+        from cat_surface_gpu_b200.gifti import GiftiMesh
+        from cat_surface_gpu_b200.gpu_pipeline import register_meshes
+
+        stream = torch.cuda.current_stream()
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        self.points.copy_(self.pristine)
+        k0.record(stream)
+        self.scratch = surf2sphere.areal_sweeps_device(
+            self.points, self.plan_device, self.plan, iterations=SWEEPS + 1, project_every=1000, radius=self.radius,
+            arithmetic="cat", launch=self.launch, scratch=self.scratch)
+        k1.record(stream)
+        smoothed = self.points.cpu().numpy()
+        sphere = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(smoothed, self.meshes["source_area"])
+        surface, target_surface, target_sphere = self.meshes_in
+        final, angle, cost, timings = register_meshes(
+            surface, GiftiMesh(sphere, self.meshes["faces"]), target_surface, target_sphere, device=self.device,
+            dartel_dtype=dartel_dtype or self.dartel_dtype, stencil_threads=min(64, os.cpu_count() or 8), **CHAIN)
+        timings["sweeps_kernel_ms"] = k0, k1
+        return final, sphere, timings
+
+
+def hemisphere_e2e(meshes, device, dartel_dtype, workdir: Path) -> tuple[float, int, int]:
+    """One hemisphere through the public API with host buffers and GIFTI files; returns (s, h2d, d2h)."""
+
+    import torch
+
+    from cat_surface_gpu_b200 import surf2sphere
+    from cat_surface_gpu_b200.gifti import GiftiMesh, write_gifti_mesh
+    from cat_surface_gpu_b200.gpu_pipeline import run_cat_surface_gpu_pipeline
+
+    prefix, faces = meshes["prefix"], meshes["faces"]
+    torch.cuda.synchronize()
+    start = time.perf_counter()
+    topology = surf2sphere.Surf2SphereTopology.from_mesh(GiftiMesh(prefix, faces))
+    smoothed, _ = surf2sphere.run_areal_smoothing_cuda(prefix, faces, topology, iterations=SWEEPS + 1,
+                                                        project_every=1000, radius=projection_radius(prefix),
+                                                        device=device, launch="auto")
+    sphere = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(smoothed, meshes["source_area"])
+    write_gifti_mesh(workdir / "source_sphere.gii", GiftiMesh(sphere, faces))
+    result = run_cat_surface_gpu_pipeline(
+        workdir / "source_surface.gii", workdir / "source_sphere.gii", workdir / "target_surface.gii",
+        workdir / "target_sphere.gii", workdir / "registered.gii", device=device, dartel_dtype=dartel_dtype,
+        stencil_threads=min(64, os.cpu_count() or 8), **CHAIN)
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - start
+    plan = topology.plan
+    h2d = prefix.nbytes + sum(getattr(plan, n).nbytes for n in ("slot_off", "slot_tri", "order", "level_begin",
+                                                                  "level_end"))
+    h2d += meshes["surface"].nbytes + meshes["target_surface"].nbytes + sphere.nbytes + meshes["target_sphere"].nbytes
+    d2h = prefix.nbytes + result.vertices.nbytes
+    return seconds, int(h2d), int(d2h)
+
+
+def batched_rotation_leg(device) -> dict:
+    """8 surfaces x 4,096 quaternions x 2 features: one persistent launch vs one launch per surface."""
+
+    import numpy as np
+    import torch
+
+    from cat_surface_gpu_b200 import autotune, synthetic
+    from cat_surface_gpu_b200.surface_rotation import (RotationGridIndex, batched_costs, quaternion_matrices,
+                                                       uniform_quaternions)
+    from cat_surface_gpu_b200.surface_stencil import resampling_sphere
+
+    rng = np.random.default_rng(2024)
+    sizes = sorted(int(v) for v in rng.integers(40962, 163843, size=8))
+    tp, tf = resampling_sphere(6)
+    index = RotationGridIndex.from_geometry(tp, tf, grid_size=128, margin=1,
+                                            include_dense_candidate_table=False).to(device)
+
+    def features(points, seed):
+        # curvature proxy (-sum l(l+1) c Y) and depth proxy (max r - r) of a seeded radial fold, z-scored
+        r_rng, c_rng = np.random.default_rng(seed), np.random.default_rng(seed)
+        fold = synthetic.real_sph_harm_sum(points, range(8, 41), 0.15, r_rng)
+        curv = np.zeros(points.shape[0])
+        for degree in range(8, 41):
+            curv -= degree * (degree + 1) * synthetic.real_sph_harm_sum(points, range(degree, degree + 1), 0.15,
+                                                                        c_rng)
+        depth = fold.max() - fold
+        out = np.stack([curv, depth])
+        out = (out - out.mean(axis=1, keepdims=True)) / out.std(axis=1, keepdims=True)
+        return out.astype(np.float32).astype(np.float64)
+
+    target_values = features(tp, 7)
+    inputs, mats = [], []
+    for i, n in enumerate(sizes):
+        pts = synthetic.fibonacci_points(n, np.random.default_rng(100 + i)).astype(np.float32)
+        inputs.append(index.prepare_cost_inputs(pts, features(pts.astype(np.float64), 200 + i), target_values))
+        mats.append(quaternion_matrices(uniform_quaternions(4096, 300 + i)))
+    indices = [index] * len(sizes)
+    key = (tuple(sizes), 4096, 2)
+    shape = autotune.tune("rotation_cost", key, autotune.rotation_candidates(device),
+                          lambda s: batched_costs(indices, inputs, matrix_sets=mats, **s), repeats=1, warmup=1)
+
+    def batched():
+        return batched_costs(indices, inputs, matrix_sets=mats, **shape)
+
+    def plain():
+        return [batched_costs([index], [inp], matrix_sets=[m], **shape)[0] for inp, m in zip(inputs, mats)]
+
+    together = batched()
+    alone = plain()
+    identical = all(torch.equal(a, b) for a, b in zip(together, alone))
+    batched_ms = autotune.time_call(batched, repeats=3, warmup=1)
+    plain_ms = autotune.time_call(plain, repeats=3, warmup=1)
+    evaluations = 4096 * sum(sizes)
+    # algorithmic bytes per (candidate, point): point 12 + 2 source features 16 + 3 target ids 12
+    # + 3 x 2 target features 48 + 36 bytes per scanned candidate triangle (mean CSR width of the grid)
+    offsets = index.candidate_offsets.cpu().numpy().astype(np.int64)
+    width = np.diff(offsets)
+    mean_width = float(width[width > 0].mean())
+    bytes_per_eval = 12 + 16 + 12 + 48 + 36 * mean_width
+    return {
+        "surfaces": sizes, "candidates_per_surface": 4096, "features": 2, "autotuned_shape": shape,
+        "batched_ms": batched_ms, "plain_ms": plain_ms, "speedup_vs_plain": plain_ms / batched_ms,
+        "point_evaluations_per_s": evaluations / (batched_ms / 1e3), "costs_identical_to_plain": bool(identical),
+        "kernel_gbs_algorithmic": evaluations * bytes_per_eval / (batched_ms / 1e3) / 1e9,
+        "bytes_per_evaluation": bytes_per_eval, "mean_cell_width": mean_width,
+    }
+
+
+def batched_dartel_leg(device, repeats: int = 5) -> dict:
+    """16 registrations x 2 step maps (256 x 128 float32): one graphed batched solve vs 16 graphed solves."""
+
+    import numpy as np
+    import torch
+
+    from cat_surface_gpu_b200 import synthetic
+    from cat_surface_gpu_b200.surface_stencil import resampling_sphere
+    from cat_surface_gpu_b200.surface_warp import apply_flow_to_sphere, solve_dartel_maps, solve_dartel_registrations
+
+    nx, ny = SHEET
+    regs, steps = 16, 2
+    template = np.stack([synthetic.smooth_sheet(ny, nx, 5000 + s) for s in range(steps)])
+    src = np.stack([[synthetic.smooth_sheet(ny, nx, 6000 + 2 * r + s) for s in range(steps)] for r in range(regs)])
+    s_dev = torch.as_tensor(src, dtype=torch.float32, device=device)
+    t_dev = torch.as_tensor(np.broadcast_to(template, src.shape).copy(), dtype=torch.float32, device=device)
+    flows, _ = solve_dartel_registrations(s_dev, t_dev, dtype=torch.float32, cuda_graph=True)  # capture
+    plain_flows = [solve_dartel_maps(s_dev[r], t_dev[r], dtype=torch.float32, cuda_graph=True).flow
+                   for r in range(regs)]  # capture
+    torch.cuda.synchronize()
+    batch_lat, plain_lat = [], []
+    stream = torch.cuda.current_stream()
+    for _ in range(repeats):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        flows, _ = solve_dartel_registrations(s_dev, t_dev, dtype=torch.float32, cuda_graph=True)
+        e1.record(stream)
+        e1.synchronize()
+        batch_lat.append(e0.elapsed_time(e1))
+        events = [torch.cuda.Event(enable_timing=True) for _ in range(regs + 1)]
+        events[0].record(stream)
+        for r in range(regs):
+            plain_flows[r] = solve_dartel_maps(s_dev[r], t_dev[r], dtype=torch.float32, cuda_graph=True).flow
+            events[r + 1].record(stream)
+        events[-1].synchronize()
+        plain_lat.extend(events[r].elapsed_time(events[r + 1]) for r in range(regs))
+    unit = torch.as_tensor(resampling_sphere(5)[0], dtype=torch.float32, device=device)
+    errors = [float(torch.linalg.vector_norm(apply_flow_to_sphere(unit, flows[r], device=device)
+                                             - apply_flow_to_sphere(unit, plain_flows[r], device=device),
+                                             dim=1).max()) for r in range(regs)]
+    batch_s = statistics.mean(batch_lat) / 1e3
+    plain_s = sum(plain_lat) / repeats / 1e3
+    return {
+        "registrations": regs, "step_maps": steps, "sheet": [nx, ny], "dtype": "float32", "cuda_graphs": True,
+        "batched_regs_per_s": regs / batch_s, "plain_regs_per_s": regs / plain_s,
+        "speedup_vs_plain": plain_s / batch_s,
+        "batched_latency_ms": {"p50": float(np.percentile(batch_lat, 50)), "p99": float(np.percentile(batch_lat, 99))},
+        "plain_latency_ms": {"p50": float(np.percentile(plain_lat, 50)), "p99": float(np.percentile(plain_lat, 99))},
+        "max_vertex_error_vs_plain": max(errors),
+        "maps": "seeded smooth sheets standing in for the curvature maps of 16 uneven meshes",
+    }
 
 
 def run_native(args):
@@ -187,41 +453,19 @@ def run_native(args):
     import torch
     import torch.distributed as dist
 
-    from cat_surface_gpu_b200 import surf2sphere
-    from cat_surface_gpu_b200.gifti import GiftiMesh
-    from oracle import areal as oracle
+    from cat_surface_gpu_b200 import _native, surf2sphere
+    from cat_surface_gpu_b200.gifti import GiftiMesh, write_gifti_mesh
 
     world, rank, local = dist_env()
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
-    workload = load_workload()
-    prefix, faces = workload["prefix"], workload["faces"]
-    n, f = prefix.shape[0], faces.shape[0]
-    radius = float(np.sqrt(np.max(np.sum(prefix.astype(np.float64) ** 2, axis=1))))
-    iterations = args.sweeps + 1
-    topology = surf2sphere.Surf2SphereTopology.from_mesh(GiftiMesh(prefix, faces))
-    plan = topology.plan
-    plan_device = plan.to_device(device)
-    pristine = torch.from_numpy(prefix).to(device)
-    points = torch.empty_like(pristine)
+    meshes = load_meshes()
+    n, f = meshes["prefix"].shape[0], meshes["faces"].shape[0]
+    hemi = Hemisphere(meshes, device, torch.float64)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
     stream = torch.cuda.current_stream()
-    scratch = None
-
-    def step():
-        nonlocal scratch
-        points.copy_(pristine)
-        k0 = torch.cuda.Event(enable_timing=True)
-        k1 = torch.cuda.Event(enable_timing=True)
-        k0.record(stream)
-        scratch = surf2sphere.areal_sweeps_device(
-            points, plan_device, plan, iterations=iterations, project_every=1000, radius=radius, arithmetic="cat",
-            scratch=scratch,
-        )
-        k1.record(stream)
-        return k0, k1
 
     def barrier():
         if world > 1:
@@ -229,138 +473,119 @@ def run_native(args):
         torch.cuda.synchronize()
 
     for _ in range(args.warmup):
-        step()
+        hemi.step()
     barrier()
-    status, where = surf2sphere.read_status(scratch)
-    if status != 0:
-        raise RuntimeError(f"sweep kernel status {status} at {where}")
-
     sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
     if sampler:
         sampler.start()
-    step_ms, kernel_ms = [], []
-    launches = 0
-    for _ in range(args.steps):
-        flush.fill_(launches & 0xFF)
+    step_ms, kernel_ms, stage = [], [], []
+    final = sphere = None
+    launches_before = _native.kernel_launches()
+    for index in range(args.steps):
+        flush.fill_(index & 0xFF)
         barrier()
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
-        k0, k1 = step()
+        final, sphere, timings = hemi.step()
         s1.record(stream)
-        launches += 1
         torch.cuda.synchronize()
         step_ms.append(s0.elapsed_time(s1))
+        k0, k1 = timings.pop("sweeps_kernel_ms")
         kernel_ms.append(k0.elapsed_time(k1))
+        stage.append(timings)
     barrier()
+    launches = _native.kernel_launches() - launches_before
     clocks = sampler.stop() if sampler else None
-    status, where = surf2sphere.read_status(scratch)
+    status, where = surf2sphere.read_status(hemi.scratch)
     if status != 0:
         raise RuntimeError(f"sweep kernel status {status} at {where}")
-
     total_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device=device)
     if world > 1:
         dist.all_reduce(total_ms, op=dist.ReduceOp.MAX)
     total_s = float(total_ms.item()) / 1e3
     value = total_s / (args.steps * world)
 
-    # parity of the timed result against the upstream binary (not timed)
-    smoothed = points.cpu().numpy()
-    final = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(smoothed, workload["source_area"])
-    parity = oracle.error_stats(workload["final"], final) if args.sweeps == 4999 else None
+    # parity (untimed): the chain against the reference's CPU chain (float64 DARTEL, like the timed chain),
+    # the sweeps against the upstream binary, and a float32-DARTEL chain against the float64 one
+    parity = {"chain_vs_cpu_reference": error_stats(meshes["chain_final"], final),
+              "surf2sphere_vs_binary": error_stats(meshes["binary_sphere"], sphere)}
+    hemi.step(dartel_dtype=torch.float32)  # warm (graph capture for float32)
+    torch.cuda.synchronize()
+    f0 = time.perf_counter()
+    final32, _, timings32 = hemi.step(dartel_dtype=torch.float32)
+    torch.cuda.synchronize()
+    parity["chain_dartel_f32_vs_f64"] = error_stats(final, final32)
+    parity["chain_dartel_f32_seconds"] = time.perf_counter() - f0
 
-    # end to end through the public API (host inputs and outputs)
-    e2e_times = []
-    for index in range(max(1, args.steps // 2) + 1):
-        barrier()
-        start = time.perf_counter()
-        out, _ = surf2sphere.run_areal_smoothing_cuda(
-            prefix, faces, topology, iterations=iterations, project_every=1000, radius=radius, device=device
-        )
-        surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(out, workload["source_area"])
-        elapsed = time.perf_counter() - start
-        if index > 0:  # first call warms the host path
-            e2e_times.append(elapsed)
-    e2e_total = torch.tensor([sum(e2e_times)], dtype=torch.float64, device=device)
-    if world > 1:
-        dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
-    e2e_value = float(e2e_total.item()) / (len(e2e_times) * world)
-    h2d = prefix.nbytes + sum(getattr(plan, name).nbytes for name in ("slot_off", "slot_tri", "order", "level_begin", "level_end"))
-    d2h = prefix.nbytes + 12
+    e2e = None
+    if not args.no_e2e:
+        with tempfile.TemporaryDirectory(prefix="bench_e2e_") as tmp:
+            work = Path(tmp)
+            write_gifti_mesh(work / "source_surface.gii", GiftiMesh(meshes["surface"], meshes["faces"]))
+            write_gifti_mesh(work / "target_surface.gii", GiftiMesh(meshes["target_surface"], meshes["target_faces"]))
+            write_gifti_mesh(work / "target_sphere.gii", GiftiMesh(meshes["target_sphere"], meshes["target_faces"]))
+            hemisphere_e2e(meshes, device, torch.float64, work)  # first call warms the host paths
+            runs = [hemisphere_e2e(meshes, device, torch.float64, work) for _ in range(2)]
+        e2e_total = torch.tensor([sum(r[0] for r in runs)], dtype=torch.float64, device=device)
+        if world > 1:
+            dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
+        e2e = {"value": float(e2e_total.item()) / (len(runs) * world), "unit": UNIT,
+               "h2d_bytes_per_step": runs[0][1], "d2h_bytes_per_step": runs[0][2]}
+
+    batched = {}
+    if not args.no_batched:
+        batched["batched_rotation"] = batched_rotation_leg(device)
+        batched["batched_dartel"] = batched_dartel_leg(device)
 
     if rank == 0:
         kernel_s = statistics.mean(kernel_ms) / 1e3
-        algo = algorithmic_bytes_per_sweep(n, f) * args.sweeps
-        peaks = {}
-        peaks_path = ROOT / "MEASURED_PEAKS.json"
-        if peaks_path.exists():
-            peaks = json.loads(peaks_path.read_text())
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
         hbm = float(peaks.get("hbm_gbs", 6650.0))
-        achieved = algo / kernel_s / 1e9
-        steps_per_hemisphere = None
-        if plan is not None:
-            epochs = []
-            start_sweep = 1
-            while start_sweep <= args.sweeps:
-                end = min(args.sweeps, ((start_sweep - 1) // 1000 + 1) * 1000)
-                epochs.append(end - start_sweep + 1)
-                start_sweep = end + 1
-            steps_per_hemisphere = sum((s - 1) * plan.level_stride + plan.n_levels for s in epochs)
+        achieved = areal_bytes_per_sweep(n, f) * SWEEPS / kernel_s / 1e9
+        epochs, start = [], 1
+        while start <= SWEEPS:
+            end = min(SWEEPS, ((start - 1) // 1000 + 1) * 1000)
+            epochs.append(end - start + 1)
+            start = end + 1
+        wavefront_steps = sum((s - 1) * hemi.plan.level_stride + hemi.plan.n_levels for s in epochs)
+        stages = {k: statistics.mean(t[k] for t in stage) for k in stage[0] if isinstance(stage[0][k], float)}
+        stages["sweeps_kernel_s"] = kernel_s
         cpu_baseline = None
         if world == 1 and not args.no_cpu_baseline:
-            sample = min(CPU_BASELINE_SAMPLE_SWEEPS, args.sweeps)
-            seconds = cpu_oracle_seconds(workload, sample) * args.sweeps / sample
-            cpu_baseline = {
-                "value": seconds,
-                "unit": UNIT,
-                "cores": 1,
-                "kind": "port",
-                "sample": f"{sample} of {args.sweeps} sweeps of the same mesh, scaled linearly "
-                f"(upstream binary measured in the development container: {workload['binary_seconds']:.1f} s for stop_at=10 incl. stages 1-5)",
-            }
+            sample = cpu_hemisphere_sample(meshes)
+            cpu_baseline = {"value": sample["total"], "unit": UNIT, "cores": 1, "kind": "port", "sample": CPU_SAMPLE,
+                            "stages_s": {k: v for k, v in sample.items() if k != "total"},
+                            "reference_torch_cpu_chain_s": meshes["chain_cpu_seconds"],
+                            "reference_torch_cpu_threads": meshes["chain_cpu_threads"],
+                            "reference_binary_surf2sphere_s": meshes["binary_seconds"]}
         line = {
-            "metric": METRIC,
-            "value": value,
-            "unit": UNIT,
-            "n_gpus": world,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": total_s * 1e3 / args.steps,
-            "higher_is_better": False,
-            "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "f32+f64",
-            "data": "synthetic",
-            "config": {
-                "workload": WORKLOAD,
-                "n_vertices": n,
-                "n_faces": f,
-                "sweeps": args.sweeps,
-                "project_every": 1000,
-                "levels": plan.n_levels,
-                "wavefront_stride": plan.level_stride,
-                "wavefront_steps": steps_per_hemisphere,
-                "l2": "flushed between timed steps by a 256 MiB device write",
-                "parallelism": f"replicas x{world}",
-            },
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_vertices": n, "n_faces": f, "sweeps": SWEEPS, "project_every": 1000,
+                       "levels": hemi.plan.n_levels, "wavefront_stride": hemi.plan.level_stride,
+                       "wavefront_steps": wavefront_steps, "sheet": list(SHEET), "dartel_dtype": "float64",
+                       "surfwarp": {k: v for k, v in CHAIN.items() if k != "sheet_size"},
+                       "sweep_launch": hemi.launch,
+                       "l2": "flushed before every timed step by a 256 MiB device write",
+                       "parallelism": f"replicas x{world}"},
+            "stages_s": stages,
             "roofline": {
-                "bound": "hbm",
-                "achieved": achieved,
-                "peak": hbm,
-                "unit": "GB/s",
-                "frac": achieved / hbm,
-                "traffic": None,
-                "note": "algorithmic bytes = sweeps x (24 N + 24 F + 4 (N+1)); the sweep chain is barrier-latency bound "
-                "(working set is L2-resident), peak is the measured HBM copy bandwidth",
-                "kernel_ms": kernel_s * 1e3,
-                "us_per_wavefront_step": (kernel_s / steps_per_hemisphere * 1e6) if steps_per_hemisphere else None,
+                "kernel": "areal_sweeps (persistent wavefront)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                "note": "algorithmic bytes = 4,999 x (24 N + 24 F + 4 (N+1)); the sweep chain is barrier-latency "
+                        "bound (working set L2-resident); peak = measured HBM copy bandwidth",
+                "kernel_ms": kernel_s * 1e3, "us_per_wavefront_step": kernel_s / wavefront_steps * 1e6,
             },
             "cpu_baseline": cpu_baseline,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks,
-            "parity_vs_cpu_reference": parity,
-            "published_reference": {"value": 3.7084, "unit": "s", "what": "reference area smoothing only, RTX 2080 Ti, anatomical LH mesh (docs/BENCHMARKS.md:38)"},
+            "parity": parity,
+            **batched,
+            "published_reference": {"value": 3.7084 + 19.4, "unit": "s",
+                                    "what": "reference GPU area smoothing 3.71 s + SurfWarp 19.4 s on RTX 2080 Ti, "
+                                            "anatomical LH mesh (docs/BENCHMARKS.md)"},
         }
         print(json.dumps(line))
     if world > 1:

@@ -25,7 +25,8 @@ _EXPORTS = {
                           "run_rotation_pipeline_from_files"],
     "surface_warp": ["DartelSolveResult", "apply_flow_to_sphere", "apply_flow_to_stenciled_sphere",
                      "clear_dartel_cuda_graph_cache", "default_dartel_parameters", "prepare_dartel_cuda_graph",
-                     "solve_dartel_from_surfaces", "solve_dartel_maps", "solve_dartel_batch", "average_xz_surfaces"],
+                     "solve_dartel_from_surfaces", "solve_dartel_maps", "solve_dartel_batch", "solve_dartel_registrations",
+                     "average_xz_surfaces"],
     "gpu_pipeline": ["CatSurfaceGpuResult", "run_cat_surface_gpu_pipeline"],
     "gifti": ["GiftiMesh", "read_gifti_mesh", "write_gifti_mesh"],
     "surf2sphere": ["CatSurf2SphereGpuResult", "Surf2SphereTopology", "convert_ellipsoid_to_sphere_with_surface_area",

@@ -33,6 +33,7 @@ _I = c_int
 SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_last_error": (ctypes.c_char_p, []),
     "csg_abi_version": (_I, []),
+    "csg_kernel_launches": (ctypes.c_longlong, []),
     "csg_mesh_incidence": (_I, [_I, _P, _I, _P, _P]),
     "csg_mesh_neighbours": (_I, [_I, _P, _I, _P, _P, _I]),
     "csg_dependency_levels": (_I, [_I, _P, _P, _P]),
@@ -63,6 +64,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_dartel_fmg": (_I, [_I, _I, _I, _I, _P, _P, _P, _I, _I, _P, _I, _I, _P, c_size_t, _P]),
     "csg_dartel_expdef": (_I, [_I, _I, _I, _I, _P, _I, _P, _P, _P, c_size_t, _P]),
     "csg_dartel_sample": (_I, [_I, _I, _I, _P, _I, _P, _P, _P, _P]),
+    "csg_dartel_data_scratch_bytes": (c_size_t, [_I, _I, _I, _I, _I, _I]),
+    "csg_dartel_data_checkpoints": (_I, [_I, _I]),
+    "csg_dartel_data_forward": (_I, [_I, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P, _P, c_size_t, _P]),
+    "csg_dartel_data_backward": (_I, [_I, _I, _I, _I, _P, _P, _I, _I, _P, _P, _P, _P, c_size_t, _P]),
     "csg_apply_flow_to_sphere": (_I, [_I, _I, _P, _I, _I, _P, _I, _P, _P]),
     "csg_average_xz": (_I, [_I, _P, _P, _P, _P]),
     "csg_rotation_grid_build": (_I, [_P, _I, _P, _I, _I, _I, _P, _P, ctypes.c_longlong, _P]),
@@ -97,6 +102,8 @@ class RotationSurface(ctypes.Structure):
         ("n_src", ctypes.c_int32),
         ("grid_size", ctypes.c_int32),
         ("n_candidates", ctypes.c_int32),
+        ("n_features", ctypes.c_int32),
+        ("n_tgt_points", ctypes.c_int32),
     ]
 
 
@@ -178,3 +185,19 @@ def doubles(values) -> "ctypes.Array":
 
     values = [float(v) for v in values]
     return (ctypes.c_double * len(values))(*values)
+
+
+_GRAPH_REPLAYED_KERNELS = 0
+
+
+def note_graph_replay(kernels: int) -> None:
+    """Account the native kernels of one CUDA-graph replay (counted at capture)."""
+
+    global _GRAPH_REPLAYED_KERNELS
+    _GRAPH_REPLAYED_KERNELS += int(kernels)
+
+
+def kernel_launches() -> int:
+    """Native kernels launched in this process: direct launches plus kernels replayed from captured graphs."""
+
+    return int(library().csg_kernel_launches()) + _GRAPH_REPLAYED_KERNELS

@@ -394,6 +394,7 @@ int launch_variant(ArealParams params, int n_ctas, int threads, size_t smem, cud
     void* args[] = {&params};
     CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(n_ctas), dim3(threads), args,
                                                smem, stream));
+    csg::note_launch();
     return CSG_OK;
 }
 
@@ -504,6 +505,7 @@ int csg_selftest_barrier_timeout(void* scratch, size_t scratch_bytes, double tim
     void* args[] = {&ctl, &timeout_ns};
     CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(barrier_timeout_selftest_kernel), dim3(2),
                                                dim3(32), args, 0, s));
+    csg::note_launch();
     return CSG_OK;
 }
 

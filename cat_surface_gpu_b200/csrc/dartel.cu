@@ -642,13 +642,13 @@ struct Fmg {
         params_at(l, pr);
         const MemWeights w = mem_weights(pr);
         for (int it = 0; it < 2 * nit; ++it)
-            k_relax<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(buf.A[l], buf.B[l], buf.U[l], nx, ny,
-                                                                      it % 2 == 0 ? 1 : 0, T(w.w00), T(w.w01), T(w.w10));
+            (csg::note_launch(), k_relax<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(buf.A[l], buf.B[l], buf.U[l], nx, ny,
+                                                                      it % 2 == 0 ? 1 : 0, T(w.w00), T(w.w01), T(w.w10)));
     }
     void resize(const T* src, size_t from, T* dst, size_t to, int channels, bool accumulate) {
         const auto f = buf.specs[from], t = buf.specs[to];
-        k_resize<T><<<grid_for(t.first * t.second, batch * channels), kThreads, 0, s>>>(src, dst, f.first, f.second,
-                                                                                     t.first, t.second, accumulate);
+        (csg::note_launch(), k_resize<T><<<grid_for(t.first * t.second, batch * channels), kThreads, 0, s>>>(src, dst, f.first, f.second,
+                                                                                     t.first, t.second, accumulate));
     }
     void cycle(size_t start) {
         const size_t last = buf.specs.size() - 1;
@@ -657,8 +657,8 @@ struct Fmg {
             const int nx = buf.specs[l].first, ny = buf.specs[l].second;
             double pr[5];
             params_at(l, pr);
-            k_membrane_apply<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(buf.A[l], buf.U[l], buf.B[l], buf.R[l], nx,
-                                                                               ny, reg_weights(pr, 1));
+            (csg::note_launch(), k_membrane_apply<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(buf.A[l], buf.U[l], buf.B[l], buf.R[l], nx,
+                                                                               ny, reg_weights(pr, 1)));
             resize(buf.R[l], l, buf.B[l + 1], l + 1, 2, false);
             const size_t P1 = static_cast<size_t>(buf.specs[l + 1].first) * buf.specs[l + 1].second;
             cudaMemsetAsync(buf.U[l + 1], 0, 2 * P1 * batch * sizeof(T), s);
@@ -687,8 +687,8 @@ struct Fmg {
         }
         const size_t last = L - 1;
         const size_t Pl = static_cast<size_t>(buf.specs[last].first) * buf.specs[last].second;
-        k_point_solve<T><<<grid_for(static_cast<int>(Pl), batch), kThreads, 0, s>>>(
-            buf.A[last], last == 0 ? buf.B[0] : buf.B0[last], buf.U[last], static_cast<int>(Pl), T(base[4]));
+        (csg::note_launch(), k_point_solve<T><<<grid_for(static_cast<int>(Pl), batch), kThreads, 0, s>>>(
+            buf.A[last], last == 0 ? buf.B[0] : buf.B0[last], buf.U[last], static_cast<int>(Pl), T(base[4])));
         relax(last);
         for (size_t l = last; l-- > 0;) {
             resize(buf.U[l + 1], l + 1, buf.U[l], l, 2, false);
@@ -752,12 +752,12 @@ Squaring<T> run_squaring(T* rb[2], T* ha[2], T* maps[2], T* jacs[2], int k, bool
     const dim3 g = grid_for(nx * ny, batch);
     int cur = 0, other = 1, ba = 0;
     for (int step = 0; step < k; ++step) {
-        k_squaring<T><<<g, kThreads, 0, s>>>(rb[ba], ha[ba], maps[cur], jacs[cur], rb[1 - ba], ha[1 - ba], maps[other],
-                                             nx, ny);
+        (csg::note_launch(), k_squaring<T><<<g, kThreads, 0, s>>>(rb[ba], ha[ba], maps[cur], jacs[cur], rb[1 - ba], ha[1 - ba], maps[other],
+                                             nx, ny));
         ba = 1 - ba;
         if (save || step < k - 1) {
-            k_compose<T><<<g, kThreads, 0, s>>>(maps[cur], jacs[cur], maps[cur], jacs[cur], maps[other], jacs[other],
-                                                nx, ny);
+            (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(maps[cur], jacs[cur], maps[cur], jacs[cur], maps[other], jacs[other],
+                                                nx, ny));
             std::swap(cur, other);
         }
     }
@@ -777,26 +777,26 @@ int dartel_step_impl(StepBuffers<T>& W, const T* source, const T* target, T* vel
     const double scale = 1.0 / static_cast<double>(1LL << k);
     const size_t P = static_cast<size_t>(nx) * ny * batch;
     // expdef(v, k) with Jacobian
-    k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.map[0], W.jac[0], nx, ny, T(scale), T(scale * 0.5));
+    (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.map[0], W.jac[0], nx, ny, T(scale), T(scale * 0.5)));
     int cur = 0;
     for (int i = 0; i < k; ++i) {
-        k_compose<T><<<g, kThreads, 0, s>>>(W.map[cur], W.jac[cur], W.map[cur], W.jac[cur], W.map[1 - cur],
-                                            W.jac[1 - cur], nx, ny);
+        (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(W.map[cur], W.jac[cur], W.map[cur], W.jac[cur], W.map[1 - cur],
+                                            W.jac[1 - cur], nx, ny));
         cur = 1 - cur;
     }
     // forward objective with jac_div_smalldef(J, v, s)
-    k_objfun<T, true><<<g, kThreads, 0, s>>>(source, target, W.map[cur], W.jac[cur], velocity, nullptr, W.rhs_f[0],
-                                             W.hess_f[0], W.objf, nx, ny, T(scale * 0.5));
+    (csg::note_launch(), k_objfun<T, true><<<g, kThreads, 0, s>>>(source, target, W.map[cur], W.jac[cur], velocity, nullptr, W.rhs_f[0],
+                                             W.hess_f[0], W.objf, nx, ny, T(scale * 0.5)));
     // squaring of the forward terms from smalldef_jac(v, -s)
-    k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.smap[0], W.sjac[0], nx, ny, T(-scale), T(-scale * 0.5));
+    (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.smap[0], W.sjac[0], nx, ny, T(-scale), T(-scale * 0.5)));
     Squaring<T> fw = run_squaring<T>(W.rhs_f, W.hess_f, W.smap, W.sjac, k, code == 1, batch, nx, ny, s);
     T* initial = W.smap[0];
     T* rr = nullptr;
     T* hr = nullptr;
     if (code == 1) {
-        k_objfun<T, true><<<g, kThreads, 0, s>>>(target, source, W.smap[fw.cur_map], W.sjac[fw.cur_map], velocity,
-                                                 nullptr, W.rhs_r[0], W.hess_r[0], W.objr, nx, ny, T(-scale * 0.5));
-        k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.rmap[0], W.rjac[0], nx, ny, T(scale), T(scale * 0.5));
+        (csg::note_launch(), k_objfun<T, true><<<g, kThreads, 0, s>>>(target, source, W.smap[fw.cur_map], W.sjac[fw.cur_map], velocity,
+                                                 nullptr, W.rhs_r[0], W.hess_r[0], W.objr, nx, ny, T(-scale * 0.5)));
+        (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.rmap[0], W.rjac[0], nx, ny, T(scale), T(scale * 0.5)));
         Squaring<T> rv = run_squaring<T>(W.rhs_r, W.hess_r, W.rmap, W.rjac, k, false, batch, nx, ny, s);
         initial = W.rmap[0];
         rr = W.rhs_r[rv.cur_ba];
@@ -804,10 +804,10 @@ int dartel_step_impl(StepBuffers<T>& W, const T* source, const T* target, T* vel
     }
     const RegWeights rw = reg_weights(params, 1);
     T* rhs = W.rhs;
-    k_combine<T><<<g, kThreads, 0, s>>>(W.rhs_f[fw.cur_ba], rr, W.hess_f[fw.cur_ba], hr, velocity, rhs, W.hess, W.preg,
-                                        W.pnorm, nx, ny, T(scale), rw);
-    k_metrics<T><<<batch, 32, 0, s>>>(W.objf, code == 1 ? W.objr : nullptr, W.preg, W.pnorm, W.nblocks, metrics,
-                                      metric_stride);
+    (csg::note_launch(), k_combine<T><<<g, kThreads, 0, s>>>(W.rhs_f[fw.cur_ba], rr, W.hess_f[fw.cur_ba], hr, velocity, rhs, W.hess, W.preg,
+                                        W.pnorm, nx, ny, T(scale), rw));
+    (csg::note_launch(), k_metrics<T><<<batch, 32, 0, s>>>(W.objf, code == 1 ? W.objr : nullptr, W.preg, W.pnorm, W.nblocks, metrics,
+                                      metric_stride));
     // multigrid solve of (H + L) u = rhs from the scratch initial guess
     double solver[5] = {params[0], params[1], params[2], params[3], params[4] + lmreg};
     Fmg<T> fmg{W.fmg, batch, {solver[0], solver[1], solver[2], solver[3], solver[4]}, cycles, nit, s, nx, ny};
@@ -818,15 +818,15 @@ int dartel_step_impl(StepBuffers<T>& W, const T* source, const T* target, T* vel
     if (!assume_initial_nonzero) {
         int flag = 0;
         CSG_CUDA_CHECK(cudaMemsetAsync(W.fmg.flag, 0, sizeof(int), s));
-        k_any_nonzero<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(initial, 2 * P,
-                                                                                                     W.fmg.flag);
+        (csg::note_launch(), k_any_nonzero<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(initial, 2 * P,
+                                                                                                     W.fmg.flag));
         CSG_CUDA_CHECK(cudaMemcpyAsync(&flag, W.fmg.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
         CSG_CUDA_CHECK(cudaStreamSynchronize(s));
         coarse_init = flag == 0;
         if (coarse_init) CSG_CUDA_CHECK(cudaMemsetAsync(initial, 0, 2 * P * sizeof(T), s));
     }
     fmg.run(coarse_init);
-    k_sub<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(velocity, initial, 2 * P);
+    (csg::note_launch(), k_sub<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(velocity, initial, 2 * P));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -871,6 +871,200 @@ int check_grid(int dtype, int batch, int nx, int ny) {
     if (!check_dtype(dtype)) return csg::fail(CSG_ERR_ARG, "dartel: dtype must be CSG_DTYPE_F32 or CSG_DTYPE_F64");
     if (batch < 1 || nx < 1 || ny < 1) return csg::fail(CSG_ERR_ARG, "dartel: empty grid (%d x %d x %d)", batch, ny, nx);
     if (static_cast<long long>(nx) * ny > (1LL << 30)) return csg::fail(CSG_ERR_ARG, "dartel: grid too large");
+    return CSG_OK;
+}
+
+// ------------------------------------------------ data-term adjoint
+//
+// E_b(v) = 1/2 sum_x (S_b(phi_k(x)) - T_b(x))^2 with phi_0 = id + v / 2^k and
+// phi_{i+1} = phi_i o phi_i (the forward maps of expdef).  The adjoint runs
+// the same bilinear stencils backwards: the sample step gives
+// abar = r grad S(phi_k); each composition step C = F(A) with A = phi_i(x)
+// and F = phi_i splits abar into the position part J_F(A)^T abar (added at
+// x) and the value part (scattered to the four corner nodes with the
+// bilinear weights, atomically).  The period unwrap of the corner values is
+// a piecewise constant shift, so its derivative is the identity.
+
+// Residual of one sample step, its block objective partial and (when abar is
+// non-null) abar = r (dS/dX, dS/dY).
+template <typename T>
+__global__ void k_data_sample(const T* __restrict__ source, const T* __restrict__ target, const T* __restrict__ map,
+                              T* __restrict__ abar, T* __restrict__ partial, int nx, int ny) {
+    Pt p;
+    const bool ok = point(nx, ny, p);
+    T contrib = T(0);
+    if (ok) {
+        const int P = nx * ny;
+        const size_t o1 = static_cast<size_t>(p.b) * P;
+        const T* src = source + o1;
+        const T* M = map + 2 * o1;
+        const Stencil<T> st(M[p.i] - T(1), M[P + p.i] - T(1), nx, ny);
+        const T k22 = src[st.i22], k12 = src[st.i12], k21 = src[st.i21], k11 = src[st.i11];
+        const T sampled = (k22 * st.dx2 + k12 * st.dx1) * st.dy2 + (k21 * st.dx2 + k11 * st.dx1) * st.dy1;
+        const T r = sampled - target[o1 + p.i];
+        if (abar) {
+            const T ddx = (k11 - k21) * st.dy1 + (k12 - k22) * st.dy2;
+            const T ddy = (k11 * st.dx1 + k21 * st.dx2) - (k12 * st.dx1 + k22 * st.dx2);
+            abar[2 * o1 + p.i] = r * ddx;
+            abar[2 * o1 + P + p.i] = r * ddy;
+        }
+        contrib = r * r;
+    }
+    block_sum(contrib, partial);
+}
+
+// objective[b] = 1/2 sum of the block partials of batch b, in block order.
+template <typename T>
+__global__ void k_data_objective(const T* __restrict__ partial, int nblocks, int batch, T* __restrict__ objective) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    T total = T(0);
+    for (int i = 0; i < nblocks; ++i) total = total + partial[static_cast<size_t>(b) * nblocks + i];
+    objective[b] = total * T(0.5);
+}
+
+// pbar += adjoint of C = phi_i o phi_i at every x (pbar zeroed by the caller).
+template <typename T>
+__global__ void k_data_compose_adjoint(const T* __restrict__ f, const T* __restrict__ abar, T* __restrict__ pbar,
+                                       int nx, int ny) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const size_t o2 = static_cast<size_t>(p.b) * 2 * P;
+    const T* F = f + o2;
+    const Stencil<T> st(F[p.i] - T(1), F[P + p.i] - T(1), nx, ny);
+    T* out = pbar + o2;
+    T pos_x = T(0), pos_y = T(0);
+#pragma unroll
+    for (int ch = 0; ch < 2; ++ch) {
+        const T* fc = F + ch * P;
+        const T period = static_cast<T>(ch == 0 ? nx : ny);
+        const T c22 = fc[st.i22] - T(1);
+        const T c12 = unwrap(fc[st.i12] - T(1), c22, period);
+        const T c21 = unwrap(fc[st.i21] - T(1), c22, period);
+        const T c11 = unwrap(fc[st.i11] - T(1), c22, period);
+        const T a = abar[o2 + ch * P + p.i];
+        pos_x = pos_x + a * ((c12 - c22) * st.dy2 + (c11 - c21) * st.dy1);
+        pos_y = pos_y + a * ((c21 * st.dx2 + c11 * st.dx1) - (c22 * st.dx2 + c12 * st.dx1));
+        T* oc = out + ch * P;
+        atomicAdd(oc + st.i22, a * (st.dx2 * st.dy2));
+        atomicAdd(oc + st.i12, a * (st.dx1 * st.dy2));
+        atomicAdd(oc + st.i21, a * (st.dx2 * st.dy1));
+        atomicAdd(oc + st.i11, a * (st.dx1 * st.dy1));
+    }
+    atomicAdd(out + p.i, pos_x);
+    atomicAdd(out + P + p.i, pos_y);
+}
+
+// grad = scale_b * s * abar (phi_0 = id + s v).
+template <typename T>
+__global__ void k_data_velocity_grad(const T* __restrict__ abar, const T* __restrict__ grad_scale, T s,
+                                     T* __restrict__ grad, int nx, int ny) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const size_t o2 = static_cast<size_t>(p.b) * 2 * P;
+    const T g = grad_scale ? grad_scale[p.b] * s : s;
+    grad[o2 + p.i] = abar[o2 + p.i] * g;
+    grad[o2 + P + p.i] = abar[o2 + P + p.i] * g;
+}
+
+inline int data_checkpoints(int k, int every) { return k == 0 ? 1 : (k - 1) / every + 1; }
+
+inline size_t align_up(size_t bytes) { return (bytes + 255) & ~static_cast<size_t>(255); }
+
+template <typename T>
+size_t data_scratch(int batch, int nx, int ny, int k, int every) {
+    const size_t field = align_up(sizeof(T) * 2ULL * batch * nx * ny);
+    const size_t nblocks = (static_cast<size_t>(nx) * ny + kThreads - 1) / kThreads;
+    // forward ping-pong 2, backward segment `every`, abar + pbar, block partials
+    return field * (2 + static_cast<size_t>(every) + 2) + align_up(sizeof(T) * nblocks * batch) + 256;
+}
+
+template <typename T>
+struct DataScratch {
+    T* work[2];
+    T* seg;  // `every` maps
+    T* abar;
+    T* pbar;
+    T* partial;
+    size_t field_elems;
+};
+
+template <typename T>
+DataScratch<T> carve_data(void* scratch, int batch, int nx, int ny, int every) {
+    DataScratch<T> d{};
+    const size_t field = align_up(sizeof(T) * 2ULL * batch * nx * ny);
+    char* base = static_cast<char*>(scratch);
+    d.work[0] = reinterpret_cast<T*>(base);
+    d.work[1] = reinterpret_cast<T*>(base + field);
+    d.seg = reinterpret_cast<T*>(base + 2 * field);
+    d.abar = reinterpret_cast<T*>(base + (2 + static_cast<size_t>(every)) * field);
+    d.pbar = reinterpret_cast<T*>(base + (3 + static_cast<size_t>(every)) * field);
+    d.partial = reinterpret_cast<T*>(base + (4 + static_cast<size_t>(every)) * field);
+    d.field_elems = field / sizeof(T);
+    return d;
+}
+
+template <typename T>
+int data_forward_typed(int batch, int nx, int ny, const T* v, const T* source, const T* target, int k, int every,
+                       T* checkpoints, T* objective, void* scratch, size_t bytes, cudaStream_t s) {
+    if (bytes < data_scratch<T>(batch, nx, ny, k, every)) return csg::fail(CSG_ERR_ARG, "data term: scratch too small");
+    DataScratch<T> d = carve_data<T>(scratch, batch, nx, ny, every);
+    const size_t field = 2ULL * batch * nx * ny;
+    const dim3 g = grid_for(nx * ny, batch);
+    const T step = static_cast<T>(std::ldexp(1.0, -k));
+    (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(v, checkpoints, nullptr, nx, ny, step, T(0)));
+    const T* cur = checkpoints;
+    for (int i = 1; i <= k; ++i) {
+        T* dst = (i % every == 0 && i < k) ? checkpoints + field * (i / every) : d.work[i % 2];
+        (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(cur, nullptr, cur, nullptr, dst, nullptr, nx, ny));
+        cur = dst;
+    }
+    (csg::note_launch(), k_data_sample<T><<<g, kThreads, 0, s>>>(source, target, cur, nullptr, d.partial, nx, ny));
+    (csg::note_launch(), k_data_objective<T><<<(batch + 127) / 128, 128, 0, s>>>(d.partial, static_cast<int>(g.x), batch,
+                                                                               objective));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+template <typename T>
+int data_backward_typed(int batch, int nx, int ny, const T* source, const T* target, int k, int every,
+                        const T* checkpoints, const T* grad_scale, T* grad, void* scratch, size_t bytes,
+                        cudaStream_t s) {
+    if (bytes < data_scratch<T>(batch, nx, ny, k, every)) return csg::fail(CSG_ERR_ARG, "data term: scratch too small");
+    DataScratch<T> d = carve_data<T>(scratch, batch, nx, ny, every);
+    const size_t field = 2ULL * batch * nx * ny;
+    const dim3 g = grid_for(nx * ny, batch);
+    const int n_ckpt = data_checkpoints(k, every);
+    T* abar = d.abar;
+    T* pbar = d.pbar;
+    std::vector<const T*> maps(static_cast<size_t>(every) + 1);
+    for (int j = n_ckpt - 1; j >= 0; --j) {
+        const int first = j * every;
+        const int last = (j == n_ckpt - 1) ? k : (j + 1) * every - 1;  // maps this segment needs
+        maps[0] = checkpoints + field * j;
+        for (int i = first + 1; i <= last; ++i) {
+            T* dst = d.seg + d.field_elems * static_cast<size_t>(i - first - 1);
+            (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(maps[i - first - 1], nullptr, maps[i - first - 1],
+                                                                   nullptr, dst, nullptr, nx, ny));
+            maps[i - first] = dst;
+        }
+        if (j == n_ckpt - 1)
+            (csg::note_launch(), k_data_sample<T><<<g, kThreads, 0, s>>>(source, target, maps[k - first], abar,
+                                                                       d.partial, nx, ny));
+        const int top = (j == n_ckpt - 1) ? k - 1 : last;
+        for (int i = top; i >= first; --i) {
+            CSG_CUDA_CHECK(cudaMemsetAsync(pbar, 0, sizeof(T) * field, s));
+            (csg::note_launch(), k_data_compose_adjoint<T><<<g, kThreads, 0, s>>>(maps[i - first], abar, pbar, nx, ny));
+            T* t = abar;
+            abar = pbar;
+            pbar = t;
+        }
+    }
+    const T step = static_cast<T>(std::ldexp(1.0, -k));
+    (csg::note_launch(), k_data_velocity_grad<T><<<g, kThreads, 0, s>>>(abar, grad_scale, step, grad, nx, ny));
+    CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
 
@@ -948,8 +1142,8 @@ namespace {
 
 template <typename T>
 int smalldef_typed(int batch, int nx, int ny, const void* v, double scale, void* map, void* jac, cudaStream_t s) {
-    k_smalldef<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(static_cast<const T*>(v), static_cast<T*>(map),
-                                                                 static_cast<T*>(jac), nx, ny, T(scale), T(scale * 0.5));
+    (csg::note_launch(), k_smalldef<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(static_cast<const T*>(v), static_cast<T*>(map),
+                                                                 static_cast<T*>(jac), nx, ny, T(scale), T(scale * 0.5)));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -993,13 +1187,13 @@ int expdef_typed(int batch, int nx, int ny, const void* v, int k, void* map_out,
     const double scale = 1.0 / static_cast<double>(1LL << k);
     const dim3 g = grid_for(nx * ny, batch);
     const bool with_jac = jac_out != nullptr;
-    k_smalldef<T><<<g, kThreads, 0, s>>>(static_cast<const T*>(v), maps[0], with_jac ? jacs[0] : nullptr, nx, ny,
-                                         T(scale), T(scale * 0.5));
+    (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(static_cast<const T*>(v), maps[0], with_jac ? jacs[0] : nullptr, nx, ny,
+                                         T(scale), T(scale * 0.5)));
     int cur = 0;
     for (int i = 0; i < k; ++i) {
-        k_compose<T><<<g, kThreads, 0, s>>>(maps[cur], with_jac ? jacs[cur] : nullptr, maps[cur],
+        (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(maps[cur], with_jac ? jacs[cur] : nullptr, maps[cur],
                                             with_jac ? jacs[cur] : nullptr, maps[1 - cur],
-                                            with_jac ? jacs[1 - cur] : nullptr, nx, ny);
+                                            with_jac ? jacs[1 - cur] : nullptr, nx, ny));
         cur = 1 - cur;
     }
     CSG_CUDA_CHECK(cudaMemcpyAsync(map_out, maps[cur], 2 * P * sizeof(T), cudaMemcpyDeviceToDevice, s));
@@ -1022,8 +1216,8 @@ int fmg_typed(int batch, int nx, int ny, const void* hess, const void* rhs, cons
     if (has_initial && !assume_nonzero) {
         int flag = 0;
         CSG_CUDA_CHECK(cudaMemsetAsync(buf.flag, 0, sizeof(int), s));
-        k_any_nonzero<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(buf.U[0], 2 * P,
-                                                                                                     buf.flag);
+        (csg::note_launch(), k_any_nonzero<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(buf.U[0], 2 * P,
+                                                                                                     buf.flag));
         CSG_CUDA_CHECK(cudaMemcpyAsync(&flag, buf.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
         CSG_CUDA_CHECK(cudaStreamSynchronize(s));
         coarse_init = flag == 0;
@@ -1058,13 +1252,13 @@ int csg_dartel_compose(int dtype, int batch, int nx, int ny, const void* a, cons
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64)
-        k_compose<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(a), static_cast<const double*>(ja),
+        (csg::note_launch(), k_compose<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(a), static_cast<const double*>(ja),
                                                  static_cast<const double*>(b), static_cast<const double*>(jb),
-                                                 static_cast<double*>(c_out), static_cast<double*>(jc_out), nx, ny);
+                                                 static_cast<double*>(c_out), static_cast<double*>(jc_out), nx, ny));
     else
-        k_compose<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(a), static_cast<const float*>(ja),
+        (csg::note_launch(), k_compose<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(a), static_cast<const float*>(ja),
                                                 static_cast<const float*>(b), static_cast<const float*>(jb),
-                                                static_cast<float*>(c_out), static_cast<float*>(jc_out), nx, ny);
+                                                static_cast<float*>(c_out), static_cast<float*>(jc_out), nx, ny));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -1077,11 +1271,11 @@ int csg_dartel_jac_div(int dtype, int batch, int nx, int ny, const void* jac, co
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64)
-        k_jacdiv<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(jac), static_cast<const double*>(velocity),
-                                                static_cast<double*>(out), nx, ny, scale * 0.5);
+        (csg::note_launch(), k_jacdiv<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(jac), static_cast<const double*>(velocity),
+                                                static_cast<double*>(out), nx, ny, scale * 0.5));
     else
-        k_jacdiv<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(jac), static_cast<const float*>(velocity),
-                                               static_cast<float*>(out), nx, ny, static_cast<float>(scale * 0.5));
+        (csg::note_launch(), k_jacdiv<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(jac), static_cast<const float*>(velocity),
+                                               static_cast<float*>(out), nx, ny, static_cast<float>(scale * 0.5)));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -1099,19 +1293,19 @@ int csg_dartel_objfun(int dtype, int batch, int nx, int ny, const void* source, 
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64) {
-        k_objfun<double, false><<<g, kThreads, 0, s>>>(
+        (csg::note_launch(), k_objfun<double, false><<<g, kThreads, 0, s>>>(
             static_cast<const double*>(source), static_cast<const double*>(target), static_cast<const double*>(map),
             static_cast<const double*>(jac), nullptr, static_cast<const double*>(weights), static_cast<double*>(rhs_out),
-            static_cast<double*>(hess_out), static_cast<double*>(scratch), nx, ny, 0.0);
-        k_objective_out<double><<<batch, 32, 0, s>>>(static_cast<double*>(scratch), nblocks,
-                                                     static_cast<double*>(objective_out));
+            static_cast<double*>(hess_out), static_cast<double*>(scratch), nx, ny, 0.0));
+        (csg::note_launch(), k_objective_out<double><<<batch, 32, 0, s>>>(static_cast<double*>(scratch), nblocks,
+                                                     static_cast<double*>(objective_out)));
     } else {
-        k_objfun<float, false><<<g, kThreads, 0, s>>>(
+        (csg::note_launch(), k_objfun<float, false><<<g, kThreads, 0, s>>>(
             static_cast<const float*>(source), static_cast<const float*>(target), static_cast<const float*>(map),
             static_cast<const float*>(jac), nullptr, static_cast<const float*>(weights), static_cast<float*>(rhs_out),
-            static_cast<float*>(hess_out), static_cast<float*>(scratch), nx, ny, 0.0f);
-        k_objective_out<float><<<batch, 32, 0, s>>>(static_cast<float*>(scratch), nblocks,
-                                                    static_cast<float*>(objective_out));
+            static_cast<float*>(hess_out), static_cast<float*>(scratch), nx, ny, 0.0f));
+        (csg::note_launch(), k_objective_out<float><<<batch, 32, 0, s>>>(static_cast<float*>(scratch), nblocks,
+                                                    static_cast<float*>(objective_out)));
     }
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
@@ -1143,11 +1337,11 @@ int csg_dartel_regularization(int dtype, int batch, int nx, int ny, const void* 
     const RegWeights rw = reg_weights(params, rtype);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64)
-        k_regularise<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(velocity), static_cast<double*>(out), nx,
-                                                    ny, rtype, rw);
+        (csg::note_launch(), k_regularise<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(velocity), static_cast<double*>(out), nx,
+                                                    ny, rtype, rw));
     else
-        k_regularise<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(velocity), static_cast<float*>(out), nx, ny,
-                                                   rtype, rw);
+        (csg::note_launch(), k_regularise<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(velocity), static_cast<float*>(out), nx, ny,
+                                                   rtype, rw));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -1161,11 +1355,11 @@ int csg_dartel_membrane_apply(int dtype, int batch, int nx, int ny, const void* 
     const RegWeights rw = reg_weights(params, 1);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64)
-        k_membrane_apply<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(hess), static_cast<const double*>(field),
-                                                        nullptr, static_cast<double*>(out), nx, ny, rw);
+        (csg::note_launch(), k_membrane_apply<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(hess), static_cast<const double*>(field),
+                                                        nullptr, static_cast<double*>(out), nx, ny, rw));
     else
-        k_membrane_apply<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(hess), static_cast<const float*>(field),
-                                                       nullptr, static_cast<float*>(out), nx, ny, rw);
+        (csg::note_launch(), k_membrane_apply<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(hess), static_cast<const float*>(field),
+                                                       nullptr, static_cast<float*>(out), nx, ny, rw));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -1183,12 +1377,12 @@ int csg_dartel_relax(int dtype, int batch, int nx, int ny, const void* hess, con
     for (int it = 0; it < 2 * nit; ++it) {
         const int colour = it % 2 == 0 ? 1 : 0;
         if (dtype == CSG_DTYPE_F64)
-            k_relax<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(hess), static_cast<const double*>(rhs),
-                                                   static_cast<double*>(u), nx, ny, colour, w.w00, w.w01, w.w10);
+            (csg::note_launch(), k_relax<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(hess), static_cast<const double*>(rhs),
+                                                   static_cast<double*>(u), nx, ny, colour, w.w00, w.w01, w.w10));
         else
-            k_relax<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(hess), static_cast<const float*>(rhs),
+            (csg::note_launch(), k_relax<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(hess), static_cast<const float*>(rhs),
                                                   static_cast<float*>(u), nx, ny, colour, static_cast<float>(w.w00),
-                                                  static_cast<float>(w.w01), static_cast<float>(w.w10));
+                                                  static_cast<float>(w.w01), static_cast<float>(w.w10)));
     }
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
@@ -1201,11 +1395,11 @@ int csg_dartel_resize(int dtype, int fields, int src_nx, int src_ny, const void*
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const dim3 g = grid_for(dst_nx * dst_ny, fields);
     if (dtype == CSG_DTYPE_F64)
-        k_resize<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(src), static_cast<double*>(dst), src_nx,
-                                                src_ny, dst_nx, dst_ny, accumulate);
+        (csg::note_launch(), k_resize<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(src), static_cast<double*>(dst), src_nx,
+                                                src_ny, dst_nx, dst_ny, accumulate));
     else
-        k_resize<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(src), static_cast<float*>(dst), src_nx, src_ny,
-                                               dst_nx, dst_ny, accumulate);
+        (csg::note_launch(), k_resize<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(src), static_cast<float*>(dst), src_nx, src_ny,
+                                               dst_nx, dst_ny, accumulate));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -1237,6 +1431,57 @@ int csg_dartel_expdef(int dtype, int batch, int nx, int ny, const void* velocity
     if (dtype == CSG_DTYPE_F64)
         return expdef_typed<double>(batch, nx, ny, velocity, k, map_out, jac_out, scratch, scratch_bytes, s);
     return expdef_typed<float>(batch, nx, ny, velocity, k, map_out, jac_out, scratch, scratch_bytes, s);
+}
+
+size_t csg_dartel_data_scratch_bytes(int dtype, int batch, int nx, int ny, int k, int checkpoint_every) {
+    if (!check_dtype(dtype) || batch < 1 || nx < 1 || ny < 1 || k < 0 || k > 30 || checkpoint_every < 1) return 0;
+    return dtype == CSG_DTYPE_F64 ? data_scratch<double>(batch, nx, ny, k, checkpoint_every)
+                                  : data_scratch<float>(batch, nx, ny, k, checkpoint_every);
+}
+
+int csg_dartel_data_checkpoints(int k, int checkpoint_every) {
+    if (k < 0 || k > 30 || checkpoint_every < 1) return 0;
+    return data_checkpoints(k, checkpoint_every);
+}
+
+int csg_dartel_data_forward(int dtype, int batch, int nx, int ny, const void* velocity, const void* source,
+                            const void* target, int k, int checkpoint_every, void* checkpoints, void* objective,
+                            void* scratch, size_t scratch_bytes, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!velocity || !source || !target || !checkpoints || !objective || !scratch || k < 0 || k > 30 ||
+        checkpoint_every < 1)
+        return csg::fail(CSG_ERR_ARG, "data term forward: null pointer, bad k or checkpoint interval");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (dtype == CSG_DTYPE_F64)
+        return data_forward_typed<double>(batch, nx, ny, static_cast<const double*>(velocity),
+                                          static_cast<const double*>(source), static_cast<const double*>(target), k,
+                                          checkpoint_every, static_cast<double*>(checkpoints),
+                                          static_cast<double*>(objective), scratch, scratch_bytes, s);
+    return data_forward_typed<float>(batch, nx, ny, static_cast<const float*>(velocity),
+                                     static_cast<const float*>(source), static_cast<const float*>(target), k,
+                                     checkpoint_every, static_cast<float*>(checkpoints), static_cast<float*>(objective),
+                                     scratch, scratch_bytes, s);
+}
+
+int csg_dartel_data_backward(int dtype, int batch, int nx, int ny, const void* source, const void* target, int k,
+                             int checkpoint_every, const void* checkpoints, const void* grad_scale,
+                             void* grad_velocity, void* scratch, size_t scratch_bytes, csg_stream_t stream) {
+    int rc = check_grid(dtype, batch, nx, ny);
+    if (rc) return rc;
+    if (!source || !target || !checkpoints || !grad_velocity || !scratch || k < 0 || k > 30 || checkpoint_every < 1)
+        return csg::fail(CSG_ERR_ARG, "data term backward: null pointer, bad k or checkpoint interval");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (dtype == CSG_DTYPE_F64)
+        return data_backward_typed<double>(batch, nx, ny, static_cast<const double*>(source),
+                                           static_cast<const double*>(target), k, checkpoint_every,
+                                           static_cast<const double*>(checkpoints),
+                                           static_cast<const double*>(grad_scale), static_cast<double*>(grad_velocity),
+                                           scratch, scratch_bytes, s);
+    return data_backward_typed<float>(batch, nx, ny, static_cast<const float*>(source),
+                                      static_cast<const float*>(target), k, checkpoint_every,
+                                      static_cast<const float*>(checkpoints), static_cast<const float*>(grad_scale),
+                                      static_cast<float*>(grad_velocity), scratch, scratch_bytes, s);
 }
 
 }  // extern "C"

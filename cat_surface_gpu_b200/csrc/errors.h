@@ -8,6 +8,9 @@ namespace csg {
 extern thread_local std::string g_last_error;
 // Records a printf-style message and returns `code`.
 int fail(int code, const char* fmt, ...);
+// Counts one kernel launch (read with csg_kernel_launches()).  Launch sites
+// are written `(csg::note_launch(), kernel<<<...>>>(...))`.
+void note_launch();
 }  // namespace csg
 
 #define CSG_CUDA_CHECK(expr)                                                                                   \

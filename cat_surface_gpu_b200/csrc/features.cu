@@ -151,7 +151,10 @@ __global__ void k_heat_weights(const T* __restrict__ geometry, const int* __rest
 }
 
 // One smoothing iteration for every series still active (iteration < count).
-__global__ void k_smooth_values(const double* __restrict__ in, double* __restrict__ out,
+// Series s reads in[s * in_stride ...] (in_stride 0: every series starts from
+// the caller's single value array) and writes out[s * n ...]; `in` and `out`
+// never alias (Jacobi update).
+__global__ void k_smooth_values(const double* __restrict__ in, long long in_stride, double* __restrict__ out,
                                 const double* __restrict__ weights, const double* __restrict__ wsum,
                                 const int* __restrict__ off, const int* __restrict__ nbr, int n, SeriesParams sp,
                                 int iteration) {
@@ -159,15 +162,16 @@ __global__ void k_smooth_values(const double* __restrict__ in, double* __restric
     const int s = blockIdx.y;
     if (i >= n) return;
     const long long base = static_cast<long long>(s) * n;
+    const double* src = in + static_cast<long long>(s) * in_stride;
     if (iteration >= sp.count[s]) {
-        out[base + i] = in[base + i];
+        out[base + i] = src[i];
         return;
     }
     const int b = off[i], e = off[i + 1], slots = off[n];
     const double* w = weights + static_cast<long long>(s) * slots;
     double acc = 0.0;
-    for (int k = b; k < e; ++k) acc = acc + w[k] * in[base + nbr[k]];
-    out[base + i] = (in[base + i] + acc) / (1.0 + wsum[base + i]);
+    for (int k = b; k < e; ++k) acc = acc + w[k] * src[nbr[k]];
+    out[base + i] = (src[i] + acc) / (1.0 + wsum[base + i]);
 }
 
 // Angle-weighted vertex normals (478-505).  inc lists (face << 2 | corner) per
@@ -330,6 +334,12 @@ __global__ void k_minmax_apply(const double* __restrict__ v, int n, const double
     if (i < n) out[base + i] = (v[base + i] - lo) / (hi - lo);
 }
 
+// True when byte ranges [a, a + na) and [b, b + nb) intersect.
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+    const auto pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
+    return pa < pb + nb && pb < pa + na;
+}
+
 }  // namespace
 
 extern "C" {
@@ -342,11 +352,11 @@ int csg_feature_resample(int dtype, int n_out, const int32_t* indices, const dou
     if (n_out == 0) return CSG_OK;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     if (dtype == CSG_DTYPE_F32)
-        k_resample32<<<blocks_for(n_out), kThreads, 0, s>>>(static_cast<const float*>(vertices), indices, weights, n_out,
-                                                           static_cast<float*>(out));
+        (csg::note_launch(), k_resample32<<<blocks_for(n_out), kThreads, 0, s>>>(static_cast<const float*>(vertices), indices, weights, n_out,
+                                                           static_cast<float*>(out)));
     else
-        k_resample64<<<blocks_for(n_out), kThreads, 0, s>>>(static_cast<const double*>(vertices), indices, weights,
-                                                           n_out, static_cast<double*>(out));
+        (csg::note_launch(), k_resample64<<<blocks_for(n_out), kThreads, 0, s>>>(static_cast<const double*>(vertices), indices, weights,
+                                                           n_out, static_cast<double*>(out)));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -356,8 +366,8 @@ int csg_feature_sheet_map(int n_cells, const int32_t* indices, const double* wei
     if (n_cells < 0 || (n_cells > 0 && (!indices || !weights || !values || !out)))
         return csg::fail(CSG_ERR_ARG, "sheet map: bad arguments");
     if (n_cells == 0) return CSG_OK;
-    k_sheet<<<blocks_for(n_cells), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(values, indices, weights,
-                                                                                        n_cells, out);
+    (csg::note_launch(), k_sheet<<<blocks_for(n_cells), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(values, indices, weights,
+                                                                                        n_cells, out));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -383,10 +393,10 @@ int csg_feature_edge_sum(int dtype, int n_faces, const int32_t* faces, const voi
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     double* partial = static_cast<double*>(scratch);
     if (dtype == CSG_DTYPE_F32)
-        k_edge_sum<float><<<nb, kThreads, 0, s>>>(static_cast<const float*>(vertices), faces, n_faces, partial);
+        (csg::note_launch(), k_edge_sum<float><<<nb, kThreads, 0, s>>>(static_cast<const float*>(vertices), faces, n_faces, partial));
     else
-        k_edge_sum<double><<<nb, kThreads, 0, s>>>(static_cast<const double*>(vertices), faces, n_faces, partial);
-    k_sum_partials<<<1, 32, 0, s>>>(partial, static_cast<int>(nb), out_sum);
+        (csg::note_launch(), k_edge_sum<double><<<nb, kThreads, 0, s>>>(static_cast<const double*>(vertices), faces, n_faces, partial));
+    (csg::note_launch(), k_sum_partials<<<1, 32, 0, s>>>(partial, static_cast<int>(nb), out_sum));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -396,13 +406,15 @@ int csg_feature_smooth_geometry(int n_points, const int32_t* nbr_off, const int3
     if (n_points < 1 || !nbr_off || !nbr || !vertices || !out || iterations < 0 || !scratch)
         return csg::fail(CSG_ERR_ARG, "smooth geometry: bad arguments");
     if (scratch_bytes < 12ULL * n_points) return csg::fail(CSG_ERR_ARG, "smooth geometry: scratch too small");
+    if (overlaps(vertices, 12ULL * n_points, out, 12ULL * n_points))
+        return csg::fail(CSG_ERR_ARG, "smooth geometry: out must not overlap vertices");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     float* tmp = static_cast<float*>(scratch);
     // Ping-pong so that the last iteration lands in `out`.
     const float* src = vertices;
     for (int it = 0; it < iterations; ++it) {
         float* dst = ((iterations - 1 - it) % 2 == 0) ? out : tmp;
-        k_smooth_geometry<<<blocks_for(n_points), kThreads, 0, s>>>(src, dst, nbr_off, nbr, n_points);
+        (csg::note_launch(), k_smooth_geometry<<<blocks_for(n_points), kThreads, 0, s>>>(src, dst, nbr_off, nbr, n_points));
         src = dst;
     }
     if (iterations == 0) CSG_CUDA_CHECK(cudaMemcpyAsync(out, vertices, 12ULL * n_points, cudaMemcpyDeviceToDevice, s));
@@ -428,28 +440,33 @@ int csg_feature_smooth_values(int n_points, const int32_t* nbr_off, const int32_
     }
     const size_t need = 8ULL * series * (static_cast<size_t>(n_slots) + 2ULL * n_points) + 1024;
     if (scratch_bytes < need) return csg::fail(CSG_ERR_ARG, "smooth values: scratch too small");
+    if (overlaps(values, 8ULL * n_points, out, 8ULL * series * n_points))
+        return csg::fail(CSG_ERR_ARG, "smooth values: out must not overlap values");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     double* weights = static_cast<double*>(scratch);
     double* wsum = weights + static_cast<size_t>(series) * n_slots;
     double* tmp = wsum + static_cast<size_t>(series) * n_points;
     const dim3 grid(blocks_for(n_points), series);
     if (geometry_dtype == CSG_DTYPE_F32)
-        k_heat_weights<float><<<grid, kThreads, 0, s>>>(static_cast<const float*>(geometry), nbr_off, nbr, n_points, sp,
-                                                         series, via_norm, weights, wsum);
+        (csg::note_launch(), k_heat_weights<float><<<grid, kThreads, 0, s>>>(static_cast<const float*>(geometry), nbr_off, nbr, n_points, sp,
+                                                         series, via_norm, weights, wsum));
     else
-        k_heat_weights<double><<<grid, kThreads, 0, s>>>(static_cast<const double*>(geometry), nbr_off, nbr, n_points,
-                                                          sp, series, via_norm, weights, wsum);
-    for (int k = 0; k < series; ++k)
-        CSG_CUDA_CHECK(cudaMemcpyAsync(tmp + static_cast<size_t>(k) * n_points, values, 8ULL * n_points,
-                                       cudaMemcpyDeviceToDevice, s));
-    const double* src = tmp;
+        (csg::note_launch(), k_heat_weights<double><<<grid, kThreads, 0, s>>>(static_cast<const double*>(geometry), nbr_off, nbr, n_points,
+                                                          sp, series, via_norm, weights, wsum));
+    // Ping-pong between `out` and `tmp` so that the last iteration lands in `out`;
+    // the first iteration reads the caller's values directly.
+    const double* src = values;
+    long long stride = 0;
     for (int it = 0; it < max_it; ++it) {
         double* dst = ((max_it - 1 - it) % 2 == 0) ? out : tmp;
-        k_smooth_values<<<grid, kThreads, 0, s>>>(src, dst, weights, wsum, nbr_off, nbr, n_points, sp, it);
+        (csg::note_launch(), k_smooth_values<<<grid, kThreads, 0, s>>>(src, stride, dst, weights, wsum, nbr_off, nbr, n_points, sp, it));
         src = dst;
+        stride = n_points;
     }
     if (max_it == 0)
-        CSG_CUDA_CHECK(cudaMemcpyAsync(out, tmp, 8ULL * series * n_points, cudaMemcpyDeviceToDevice, s));
+        for (int k = 0; k < series; ++k)
+            CSG_CUDA_CHECK(cudaMemcpyAsync(out + static_cast<size_t>(k) * n_points, values, 8ULL * n_points,
+                                           cudaMemcpyDeviceToDevice, s));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -458,8 +475,8 @@ int csg_feature_vertex_normals(int n_points, const int32_t* faces, const int32_t
                                const float* vertices, float* out, csg_stream_t stream) {
     if (n_points < 1 || !faces || !inc_off || !inc || !vertices || !out)
         return csg::fail(CSG_ERR_ARG, "vertex normals: bad arguments");
-    k_vertex_normals<<<blocks_for(n_points), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        vertices, faces, inc_off, inc, n_points, out);
+    (csg::note_launch(), k_vertex_normals<<<blocks_for(n_points), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        vertices, faces, inc_off, inc, n_points, out));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -468,8 +485,8 @@ int csg_feature_normal_displacement(int n_points, const float* smoothed, const f
                                     double* out, csg_stream_t stream) {
     if (n_points < 1 || !smoothed || !geometry || !normals || !out)
         return csg::fail(CSG_ERR_ARG, "normal displacement: bad arguments");
-    k_normal_displacement<<<blocks_for(n_points), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        smoothed, geometry, normals, n_points, out);
+    (csg::note_launch(), k_normal_displacement<<<blocks_for(n_points), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        smoothed, geometry, normals, n_points, out));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -478,8 +495,8 @@ int csg_feature_curvature2(int n_points, const int32_t* nbr_off, const int32_t* 
                            const float* normals, double* out, csg_stream_t stream) {
     if (n_points < 1 || !nbr_off || !nbr || !vertices || !normals || !out)
         return csg::fail(CSG_ERR_ARG, "curvature type 2: bad arguments");
-    k_curvature2<<<blocks_for(n_points), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        vertices, normals, nbr_off, nbr, n_points, out);
+    (csg::note_launch(), k_curvature2<<<blocks_for(n_points), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        vertices, normals, nbr_off, nbr, n_points, out));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -491,8 +508,8 @@ int csg_feature_minmax(int n, int series, const double* values, double* out, voi
     if (scratch_bytes < 16ULL * nb * series) return csg::fail(CSG_ERR_ARG, "minmax: scratch too small");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     double* partial = static_cast<double*>(scratch);
-    k_minmax_partial<<<dim3(nb, series), kThreads, 0, s>>>(values, n, partial);
-    k_minmax_apply<<<dim3(nb, series), kThreads, 0, s>>>(values, n, partial, static_cast<int>(nb), out);
+    (csg::note_launch(), k_minmax_partial<<<dim3(nb, series), kThreads, 0, s>>>(values, n, partial));
+    (csg::note_launch(), k_minmax_apply<<<dim3(nb, series), kThreads, 0, s>>>(values, n, partial, static_cast<int>(nb), out));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }

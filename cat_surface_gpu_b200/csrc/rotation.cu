@@ -41,6 +41,8 @@ struct RotSurface {
     int n_src;
     int grid_size;
     int n_candidates;
+    int n_features;              // >= 1; values are feature-major
+    int n_tgt_points;            // feature stride of tgt_values
     int tiles;                   // ceil(n_src / tile)
     long long item_begin;        // first flat work item of this surface
 };
@@ -189,11 +191,14 @@ __global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __rest
                 float w[3];
                 barycentric(best_point, S.triangles + 9 * static_cast<long long>(best_face), w);
                 const int* fv = S.faces + 3 * static_cast<long long>(best_face);
-                const double sampled = (S.tgt_values[fv[0]] * static_cast<double>(w[0]) +
-                                        S.tgt_values[fv[1]] * static_cast<double>(w[1])) +
-                                       S.tgt_values[fv[2]] * static_cast<double>(w[2]);
-                const double diff = S.src_values[i] - sampled;
-                contrib = diff * diff;
+                for (int f = 0; f < S.n_features; ++f) {
+                    const double* tv = S.tgt_values + static_cast<long long>(f) * S.n_tgt_points;
+                    const double sampled = (tv[fv[0]] * static_cast<double>(w[0]) +
+                                            tv[fv[1]] * static_cast<double>(w[1])) +
+                                           tv[fv[2]] * static_cast<double>(w[2]);
+                    const double diff = S.src_values[static_cast<long long>(f) * S.n_src + i] - sampled;
+                    contrib = contrib + diff * diff;
+                }
             }
         }
         // fixed-order block reduction: warp tree, then warp 0 over warp sums
@@ -289,7 +294,8 @@ int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces
     for (int s = 0; s < n_surfaces; ++s) {
         const csg_rotation_surface& in = surfaces[s];
         if (!in.src_points || !in.src_values || !in.triangles || !in.faces || !in.tgt_values || !in.grid_offsets ||
-            !in.grid_faces || !in.matrices || in.n_src < 1 || in.n_candidates < 1 || in.grid_size < 4)
+            !in.grid_faces || !in.matrices || in.n_src < 1 || in.n_candidates < 1 || in.grid_size < 4 ||
+            in.n_features < 0 || (in.n_features > 1 && in.n_tgt_points < 1))
             return csg::fail(CSG_ERR_ARG, "rotation cost: surface %d is incomplete", s);
         ns[s] = in.n_src;
         nc[s] = in.n_candidates;
@@ -321,6 +327,8 @@ int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces
         r.n_src = in.n_src;
         r.grid_size = in.grid_size;
         r.n_candidates = in.n_candidates;
+        r.n_features = in.n_features > 1 ? in.n_features : 1;
+        r.n_tgt_points = in.n_features > 1 ? in.n_tgt_points : 0;
         r.tiles = (in.n_src + tile - 1) / tile;
         r.partials = reinterpret_cast<double*>(base + used);
         used += align256(sizeof(double) * static_cast<size_t>(r.tiles) * r.n_candidates);
@@ -340,11 +348,11 @@ int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces
     const long long want = n_ctas > 0 ? n_ctas : static_cast<long long>(sms) * (2048 / tile);
     const unsigned blocks = static_cast<unsigned>(std::min<long long>(std::max<long long>(1, want), items));
     switch (tile) {
-        case 128: k_rotation_cost<128><<<blocks, 128, 0, st>>>(d_surf, n_surfaces, items, d_err); break;
-        case 512: k_rotation_cost<512><<<blocks, 512, 0, st>>>(d_surf, n_surfaces, items, d_err); break;
-        default: k_rotation_cost<256><<<blocks, 256, 0, st>>>(d_surf, n_surfaces, items, d_err); break;
+        case 128: (csg::note_launch(), k_rotation_cost<128><<<blocks, 128, 0, st>>>(d_surf, n_surfaces, items, d_err)); break;
+        case 512: (csg::note_launch(), k_rotation_cost<512><<<blocks, 512, 0, st>>>(d_surf, n_surfaces, items, d_err)); break;
+        default: (csg::note_launch(), k_rotation_cost<256><<<blocks, 256, 0, st>>>(d_surf, n_surfaces, items, d_err)); break;
     }
-    k_rotation_finalize<<<dim3((max_c + 127) / 128, n_surfaces), 128, 0, st>>>(d_surf, n_surfaces, costs, d_off);
+    (csg::note_launch(), k_rotation_finalize<<<dim3((max_c + 127) / 128, n_surfaces), 128, 0, st>>>(d_surf, n_surfaces, costs, d_off));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }

@@ -1,5 +1,6 @@
 // Host-side mesh topology and wavefront planning for the ordered
 // Surf2Sphere sweeps.  Plain C++, no device memory; O(faces) everywhere.
+#include <atomic>
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
@@ -35,6 +36,9 @@ void incidence(int n, const int32_t* faces, int n_faces, int32_t* off, int32_t* 
 
 namespace csg {
 thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int fail(int code, const char* fmt, ...) {
     char buffer[1024];
@@ -52,6 +56,8 @@ extern "C" {
 const char* csg_last_error(void) { return csg::g_last_error.c_str(); }
 
 int csg_abi_version(void) { return 1; }
+
+long long csg_kernel_launches(void) { return csg::g_launches.load(std::memory_order_relaxed); }
 
 int csg_mesh_incidence(int n_vertices, const int32_t* faces, int n_faces, int32_t* inc_off, int32_t* inc_face) {
     int rc = check_faces(n_vertices, faces, n_faces);

@@ -151,13 +151,13 @@ int csg_dartel_sample(int dtype, int nx, int ny, const void* field, int n, const
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const unsigned blocks = (n + kThreads - 1) / kThreads;
     if (dtype == CSG_DTYPE_F64)
-        k_sample<double><<<blocks, kThreads, 0, s>>>(static_cast<const double*>(field), nx, ny, n,
+        (csg::note_launch(), k_sample<double><<<blocks, kThreads, 0, s>>>(static_cast<const double*>(field), nx, ny, n,
                                                      static_cast<const double*>(x), static_cast<const double*>(y),
-                                                     static_cast<double*>(out));
+                                                     static_cast<double*>(out)));
     else
-        k_sample<float><<<blocks, kThreads, 0, s>>>(static_cast<const float*>(field), nx, ny, n,
+        (csg::note_launch(), k_sample<float><<<blocks, kThreads, 0, s>>>(static_cast<const float*>(field), nx, ny, n,
                                                     static_cast<const float*>(x), static_cast<const float*>(y),
-                                                    static_cast<float*>(out));
+                                                    static_cast<float*>(out)));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -171,11 +171,11 @@ int csg_apply_flow_to_sphere(int dtype, int n, const float* unit_points, int nx,
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const unsigned blocks = (n + kThreads - 1) / kThreads;
     if (dtype == CSG_DTYPE_F64)
-        k_apply_flow<double><<<blocks, kThreads, 0, s>>>(unit_points, n, static_cast<const double*>(flow), nx, ny,
-                                                         inverse, static_cast<double*>(out));
+        (csg::note_launch(), k_apply_flow<double><<<blocks, kThreads, 0, s>>>(unit_points, n, static_cast<const double*>(flow), nx, ny,
+                                                         inverse, static_cast<double*>(out)));
     else
-        k_apply_flow<float><<<blocks, kThreads, 0, s>>>(unit_points, n, static_cast<const float*>(flow), nx, ny, inverse,
-                                                        static_cast<float*>(out));
+        (csg::note_launch(), k_apply_flow<float><<<blocks, kThreads, 0, s>>>(unit_points, n, static_cast<const float*>(flow), nx, ny, inverse,
+                                                        static_cast<float*>(out)));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -184,7 +184,7 @@ int csg_average_xz(int n, const double* x_surface, const double* z_surface, floa
     if (n < 0 || (n > 0 && (!x_surface || !z_surface || !out))) return csg::fail(CSG_ERR_ARG, "average_xz: bad arguments");
     if (n == 0) return CSG_OK;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    k_average_xz<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(x_surface, z_surface, n, out);
+    (csg::note_launch(), k_average_xz<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(x_surface, z_surface, n, out));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }

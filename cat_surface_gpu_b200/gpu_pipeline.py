@@ -179,7 +179,8 @@ def _official_rotation_features(probe, paths, target_stencil, source_stencil, de
     for stencil, raw, side in ((source_stencil, source_values, "source"), (target_stencil, target_values, "target")):
         raw_geo = Path(f"{output}.{side}.geometry").read_bytes()
         count = int(np.frombuffer(raw_geo, dtype=np.int32, count=1)[0])
-        geometry = np.frombuffer(raw_geo, dtype=np.float64, count=3 * count, offset=4).reshape(count, 3).astype(np.float32)
+        geometry = np.frombuffer(raw_geo, dtype=np.float64, count=3 * count, offset=4).reshape(count, 3)
+        geometry = geometry.astype(np.float32)
         st = stencil.to(device, geometry_dtype=torch.float32)
         smoothed = st.smooth_values(torch.as_tensor(raw, device=device), torch.as_tensor(geometry, device=device), 50.0)
         mn, mx = smoothed.amin(), smoothed.amax()
@@ -187,25 +188,14 @@ def _official_rotation_features(probe, paths, target_stencil, source_stencil, de
     return values[0], values[1]
 
 
-def run_cat_surface_gpu_pipeline(
-    source_surface_path, source_sphere_path, target_surface_path, target_sphere_path, output_path, *,
-    source_stencil_path=None, target_stencil_path=None, rotation_values_path=None, rotation_values_probe=None,
-    rotation_geometry_probe=None, rotation_depth_probe=None, stencil_builder="native", rotated_stencil_builder=None,
-    stencil_threads: int = 8, device="cuda", kernel: str = "triton", dartel_dtype=torch.float64,
-    squaring_kernel: str | None = None, steps: int = 2, runs: int = 1, avg: bool = False,
-    curvtypes: Sequence[int] = (5, 5, 2), fwhm: Sequence[float] = (5.0, 5.0 / 3.0, 5.0 / 9.0), loop: int = 6,
-    cycles: int = 3, nit: int = 3, its: int = 3, code: int = 1, point_chunk: int = 4096,
-    rotation_grid_size: int = 128, rotation_margin: int = 1, rotation_refine: bool = True,
-    rotation_max_iter: int = 500, rotation_tol: float = 1.0e-4, rotation_simplex_step: float = 0.1,
-    rotation_feature_backend: str = "auto", rotation_feature_solver: str = "colored-sor",
-    parallel_sides: bool = True, optimized_dartel: bool = True, cuda_graph: bool = True,
-    sheet_size: tuple[int, int] = (512, 256),
-) -> CatSurfaceGpuResult:
-    """Rotation, DARTEL runs, -avg blend and GIFTI output (reference 468-1326).
+_BACKENDS = {"auto", "native-curvature", "cuda-official-depth", "official-cpu", "cuda", "cuda-official-geometry"}
 
-    ``sheet_size`` is the DARTEL sheet (nx, ny) of natively built stencils;
-    helper-built stencils carry the helper's fixed 512 x 256.
-    """
+
+def _validate_options(*, steps=2, runs=1, stencil_threads=8, curvtypes=(5, 5, 2), fwhm=(5.0, 5.0 / 3.0, 5.0 / 9.0),
+                      rotation_max_iter=500, rotation_tol=1.0e-4, rotation_simplex_step=0.1,
+                      rotation_feature_backend="auto", has_values=False, dartel_dtype=torch.float64, device="cuda",
+                      **_unused) -> None:
+    """Argument checks of the reference pipeline (reference 514-560), before any file is read."""
 
     if steps < 1 or steps > 3:
         raise ValueError("steps must be between 1 and 3")
@@ -217,30 +207,94 @@ def run_cat_surface_gpu_pipeline(
         raise ValueError("curvtypes and fwhm must contain at least 'steps' entries")
     if rotation_max_iter < 1 or rotation_tol < 0.0 or rotation_simplex_step <= 0.0:
         raise ValueError("rotation_max_iter, rotation_tol, and rotation_simplex_step must be positive")
-    backends = {"auto", "native-curvature", "cuda-official-depth", "official-cpu", "cuda", "cuda-official-geometry"}
-    if rotation_feature_backend not in backends:
-        raise ValueError(f"rotation_feature_backend must be one of {sorted(backends)}")
-    if rotation_feature_backend in {"cuda", "cuda-official-geometry"} and rotation_values_path is None:
+    if rotation_feature_backend not in _BACKENDS:
+        raise ValueError(f"rotation_feature_backend must be one of {sorted(_BACKENDS)}")
+    if rotation_feature_backend in {"cuda", "cuda-official-geometry"} and not has_values:
         raise NotImplementedError(f"rotation_feature_backend={rotation_feature_backend!r} needs the depth-potential "
                                   "solver, which this package does not implement; use 'native-curvature', "
-                                  "'cuda-official-depth' or provide rotation_values_path")
+                                  "'cuda-official-depth' or provide rotation values")
+    _resolve_dartel_dtype(dartel_dtype)
+    if device == "cpu" or str(device) == "cpu":
+        raise ValueError("The explicit GPU pipeline requires a CUDA device")
+
+
+def run_cat_surface_gpu_pipeline(
+    source_surface_path, source_sphere_path, target_surface_path, target_sphere_path, output_path, *,
+    source_stencil_path=None, target_stencil_path=None, rotation_values_path=None, **options,
+) -> CatSurfaceGpuResult:
+    """Rotation, DARTEL runs, -avg blend and GIFTI output (reference 468-1326).
+
+    Reads the four GIFTI meshes, runs :func:`register_meshes` and writes the
+    registered sphere with the source sphere's topology and array intents.
+    ``options`` are :func:`register_meshes`'s keyword arguments.
+    """
+
+    _validate_options(has_values=rotation_values_path is not None, **options)
+    total_start = time.perf_counter()
+    meshes = [read_gifti_mesh(path) for path in (source_surface_path, source_sphere_path, target_surface_path,
+                                                 target_sphere_path)]
+    read_seconds = time.perf_counter() - total_start
+    stencils = {}
+    if source_stencil_path is not None:
+        stencils["source_stencil"] = SurfaceStencil.from_file(source_stencil_path)
+    if target_stencil_path is not None:
+        stencils["target_stencil"] = SurfaceStencil.from_file(target_stencil_path)
+    rotation_values = read_rotation_values(rotation_values_path) if rotation_values_path is not None else None
+    vertices, angle, cost, timings = register_meshes(
+        *meshes, paths=(source_surface_path, source_sphere_path, target_surface_path, target_sphere_path),
+        rotation_values=rotation_values, **stencils, **options)
+    timings["input_read_seconds"] = read_seconds
+    output = Path(output_path)
+    write_start = time.perf_counter()
+    final_mesh = GiftiMesh(vertices, meshes[1].faces)
+    write_gifti_mesh(output, final_mesh, reference_path=source_sphere_path)
+    timings["output_write_seconds"] = time.perf_counter() - write_start
+    timings["total_seconds"] = time.perf_counter() - total_start
+    return CatSurfaceGpuResult(vertices=final_mesh.vertices, faces=final_mesh.faces, rotation_angle=angle,
+                               rotation_cost=cost, timings=timings, output_path=output)
+
+
+def register_meshes(
+    source_surface: GiftiMesh, source_sphere: GiftiMesh, target_surface: GiftiMesh, target_sphere: GiftiMesh, *,
+    paths=None, source_stencil: SurfaceStencil | None = None, target_stencil: SurfaceStencil | None = None,
+    rotation_values=None, rotation_values_probe=None, rotation_geometry_probe=None, rotation_depth_probe=None,
+    stencil_builder="native", rotated_stencil_builder=None, stencil_threads: int = 8, device="cuda",
+    kernel: str = "triton", dartel_dtype=torch.float64, squaring_kernel: str | None = None, steps: int = 2,
+    runs: int = 1, avg: bool = False, curvtypes: Sequence[int] = (5, 5, 2),
+    fwhm: Sequence[float] = (5.0, 5.0 / 3.0, 5.0 / 9.0), loop: int = 6, cycles: int = 3, nit: int = 3, its: int = 3,
+    code: int = 1, point_chunk: int = 4096, rotation_grid_size: int = 128, rotation_margin: int = 1,
+    rotation_refine: bool = True, rotation_max_iter: int = 500, rotation_tol: float = 1.0e-4,
+    rotation_simplex_step: float = 0.1, rotation_feature_backend: str = "auto",
+    rotation_feature_solver: str = "colored-sor", parallel_sides: bool = True, optimized_dartel: bool = True,
+    cuda_graph: bool = True, sheet_size: tuple[int, int] = (512, 256),
+) -> tuple[np.ndarray, np.ndarray, float, dict[str, float]]:
+    """In-memory SurfWarp registration: returns (sphere vertices f32, angle, rotation cost, timings).
+
+    Same flow and options as :func:`run_cat_surface_gpu_pipeline`; ``paths``
+    (source surface, source sphere, target surface, target sphere files) are
+    needed only by the helper-binary stencil builders and feature probes.
+    ``sheet_size`` is the DARTEL sheet (nx, ny) of natively built stencils;
+    helper-built stencils carry the helper's fixed 512 x 256.
+    """
+
+    _validate_options(steps=steps, runs=runs, stencil_threads=stencil_threads, curvtypes=curvtypes, fwhm=fwhm,
+                      rotation_max_iter=rotation_max_iter, rotation_tol=rotation_tol,
+                      rotation_simplex_step=rotation_simplex_step, rotation_feature_backend=rotation_feature_backend,
+                      has_values=rotation_values is not None, dartel_dtype=dartel_dtype, device=device)
     if rotation_feature_backend == "auto":
         rotation_feature_backend = "official-cpu" if rotation_values_probe is not None else "native-curvature"
     solve_dtype = _resolve_dartel_dtype(dartel_dtype)
-    if device == "cpu" or str(device) == "cpu":
-        raise ValueError("The explicit GPU pipeline requires a CUDA device")
     target_device = resolve_device(device)
     if rotated_stencil_builder is None:
         rotated_stencil_builder = stencil_builder
     graph_requested = bool(cuda_graph and (runs + int(avg) >= 3))
+    uses_files = (stencil_builder not in (None, "native") or rotated_stencil_builder not in (None, "native")
+                  or (rotation_values is None and rotation_feature_backend in {"official-cpu", "cuda-official-depth"}))
+    if uses_files and paths is None:
+        raise ValueError("helper stencil builders and feature probes need the input file paths")
+    source_surface_path, source_sphere_path, target_surface_path, target_sphere_path = paths or (None,) * 4
     timings: dict[str, float] = {}
     total_start = time.perf_counter()
-    output = Path(output_path)
-    source_surface = read_gifti_mesh(source_surface_path)
-    source_sphere = read_gifti_mesh(source_sphere_path)
-    target_surface = read_gifti_mesh(target_surface_path)
-    target_sphere = read_gifti_mesh(target_sphere_path)
-    timings["input_read_seconds"] = time.perf_counter() - total_start
     nx, ny = (int(v) for v in sheet_size)
 
     with tempfile.TemporaryDirectory(prefix="cat_surface_b200_") as temp_name:
@@ -249,31 +303,27 @@ def run_cat_surface_gpu_pipeline(
         rotated_builder = _Stencils(rotated_stencil_builder, stencil_threads, nx, ny, temp)
         start = time.perf_counter()
         with ThreadPoolExecutor(max_workers=2) as pool:
-            src_future = pool.submit(
-                lambda: SurfaceStencil.from_file(source_stencil_path) if source_stencil_path else
-                builder.build(source_sphere, source_surface_path, normalize=True, sphere_path=source_sphere_path))
-            tgt_future = pool.submit(
-                lambda: SurfaceStencil.from_file(target_stencil_path) if target_stencil_path else
-                builder.build(target_sphere, target_surface_path, normalize=True, sphere_path=target_sphere_path))
-            source_stencil = src_future.result()
-            target_stencil = tgt_future.result()
+            src_future = None if source_stencil is not None else pool.submit(
+                builder.build, source_sphere, source_surface_path, normalize=True, sphere_path=source_sphere_path)
+            tgt_future = None if target_stencil is not None else pool.submit(
+                builder.build, target_sphere, target_surface_path, normalize=True, sphere_path=target_sphere_path)
+            source_stencil = source_stencil if src_future is None else src_future.result()
+            target_stencil = target_stencil if tgt_future is None else tgt_future.result()
         timings["initial_stencil_seconds"] = time.perf_counter() - start
 
         start = time.perf_counter()
-        if rotation_values_path is not None:
-            source_values, target_values = read_rotation_values(rotation_values_path)
+        if rotation_values is not None:
+            source_values, target_values = rotation_values
         elif rotation_feature_backend == "official-cpu":
             if rotation_values_probe is None:
                 raise ValueError("official-cpu rotation features require rotation_values_probe")
             source_values, target_values = _official_rotation_features(
-                rotation_values_probe, (source_surface_path, source_sphere_path, target_surface_path, target_sphere_path),
-                target_stencil, source_stencil, target_device, temp, raw_depth=False)
+                rotation_values_probe, paths, target_stencil, source_stencil, target_device, temp, raw_depth=False)
         elif rotation_feature_backend == "cuda-official-depth":
             if rotation_depth_probe is None:
                 raise ValueError("cuda-official-depth requires rotation_depth_probe")
             source_values, target_values = _official_rotation_features(
-                rotation_depth_probe, (source_surface_path, source_sphere_path, target_surface_path, target_sphere_path),
-                target_stencil, source_stencil, target_device, temp, raw_depth=True)
+                rotation_depth_probe, paths, target_stencil, source_stencil, target_device, temp, raw_depth=True)
         else:
             source_values, target_values = native_rotation_features(
                 source_stencil, target_stencil, source_surface.vertices, target_surface.vertices, target_device)
@@ -310,8 +360,12 @@ def run_cat_surface_gpu_pipeline(
 
         target_dev = target_stencil.to(target_device)
         current_dev = current_stencil.to(target_device)
-        source_surface_dev = torch.as_tensor(source_surface.vertices, dtype=torch.float32, device=target_device)
-        target_surface_dev = torch.as_tensor(target_surface.vertices, dtype=torch.float32, device=target_device)
+
+        def on_device(array):
+            return torch.as_tensor(np.ascontiguousarray(array), dtype=torch.float32, device=target_device)
+
+        source_surface_dev = on_device(source_surface.vertices)
+        target_surface_dev = on_device(target_surface.vertices)
 
         def solve_one(src_vertices, tgt_vertices, src_stencil, tgt_stencil, solve_fwhm, solve_loop):
             return solve_dartel_from_surfaces(src_vertices, tgt_vertices, src_stencil, tgt_stencil, fwhm=solve_fwhm,
@@ -340,8 +394,8 @@ def run_cat_surface_gpu_pipeline(
             solve = solve_one(source_surface_dev, target_surface_dev, current_dev, target_dev, run_fwhm, loop)
             if not (avg and run_index == runs - 1):
                 current_sphere = apply_flow_to_stenciled_sphere(
-                    torch.as_tensor(current_sphere, dtype=torch.float32, device=target_device), solve.flow, current_dev, inverse=True,
-                    device=target_device, dtype=solve_dtype).cpu().numpy().astype(np.float32)
+                    on_device(current_sphere), solve.flow, current_dev, inverse=True, device=target_device,
+                    dtype=solve_dtype).cpu().numpy().astype(np.float32)
             torch.cuda.synchronize(target_device)
             timings[f"dartel_run_{run_index}_seconds"] = time.perf_counter() - run_start
             last_result = solve
@@ -353,24 +407,18 @@ def run_cat_surface_gpu_pipeline(
             avg_fwhm = tuple(float(fwhm[0]) / (3.0 ** (steps * (runs + 1) + i)) for i in range(steps))
             avg_start = time.perf_counter()
             avg_source_dev = avg_source_stencil.to(target_device)
-            avg_result = solve_one(torch.as_tensor(avg_source_surface, dtype=torch.float32, device=target_device),
-                                   torch.as_tensor(avg_target_surface, dtype=torch.float32, device=target_device), avg_source_dev,
+            avg_result = solve_one(on_device(avg_source_surface), on_device(avg_target_surface), avg_source_dev,
                                    avg_target_stencil.to(target_device), avg_fwhm, loop)
-            main_warped = apply_flow_to_stenciled_sphere(torch.as_tensor(final_prewarp, dtype=torch.float32, device=target_device),
-                                                         last_result.flow, current_dev, inverse=True,
-                                                         device=target_device, dtype=solve_dtype)
-            avg_warped = apply_flow_to_stenciled_sphere(torch.as_tensor(avg_source_sphere, dtype=torch.float32, device=target_device),
-                                                        avg_result.flow, avg_source_dev, inverse=True,
-                                                        device=target_device, dtype=solve_dtype)
+            main_warped = apply_flow_to_stenciled_sphere(on_device(final_prewarp), last_result.flow, current_dev,
+                                                         inverse=True, device=target_device, dtype=solve_dtype)
+            avg_warped = apply_flow_to_stenciled_sphere(on_device(avg_source_sphere), avg_result.flow, avg_source_dev,
+                                                        inverse=True, device=target_device, dtype=solve_dtype)
             reverse = rotation_matrix_from_angles(-pole).to(device=target_device)
             unrotated = avg_warped.to(torch.float64) @ reverse.transpose(0, 1)
             combined = average_xz_surfaces(unrotated, main_warped, device=target_device)
             current_sphere = combined.cpu().numpy().astype(np.float32)
             timings["avg_dartel_seconds"] = time.perf_counter() - avg_start
         timings["dartel_total_seconds"] = time.perf_counter() - dartel_start
-        final_mesh = GiftiMesh(current_sphere, source_sphere.faces)
-        write_gifti_mesh(output, final_mesh, reference_path=source_sphere_path)
-    timings["total_seconds"] = time.perf_counter() - total_start
-    return CatSurfaceGpuResult(vertices=final_mesh.vertices, faces=final_mesh.faces,
-                               rotation_angle=np.ascontiguousarray(angle, dtype=np.float64),
-                               rotation_cost=float(rotation.cost.detach().cpu()), timings=timings, output_path=output)
+    timings["register_seconds"] = time.perf_counter() - total_start
+    return (np.ascontiguousarray(current_sphere, dtype=np.float32), np.ascontiguousarray(angle, dtype=np.float64),
+            float(rotation.cost.detach().cpu()), timings)

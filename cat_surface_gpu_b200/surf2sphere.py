@@ -226,7 +226,7 @@ def areal_sweeps_device(
     project_every: int,
     radius: float,
     arithmetic: str,
-    launch: dict | None = None,
+    launch: dict | str | None = None,
     timeout_s: float = 2.0,
     scratch: torch.Tensor | None = None,
     stream: torch.cuda.Stream | None = None,
@@ -244,7 +244,9 @@ def areal_sweeps_device(
     if scratch is None or scratch.numel() < need:
         scratch = torch.empty(need, dtype=torch.uint8, device=points.device)
     cfg = dict(DEFAULT_LAUNCH)
-    if launch:
+    if launch == "auto":
+        cfg.update(tuned_areal_launch(points, plan_device, plan, arithmetic=arithmetic, radius=radius))
+    elif launch:
         cfg.update(launch)
     _native.check(
         lib.csg_areal_sweeps(
@@ -258,6 +260,38 @@ def areal_sweeps_device(
         "csg_areal_sweeps",
     )
     return scratch
+
+
+def tuned_areal_launch(points: torch.Tensor, plan_device: dict[str, torch.Tensor], plan: SweepPlan, *,
+                       arithmetic: str, radius: float, sweeps: int = 200, force: bool = False) -> dict:
+    """Fastest launch shape of the sweep kernel for this mesh (autotuned once per mesh size and device).
+
+    Times :func:`cat_surface_gpu_b200.autotune.areal_candidates` on ``sweeps``
+    sweeps of a copy of ``points``; every shape gives bit-identical results
+    (the update order is fixed by the plan, not by the launch).
+    """
+
+    from . import autotune
+
+    key = (int(points.shape[0]), plan.n_levels, plan.level_stride, plan.max_degree, arithmetic, points.dtype)
+    if not force:
+        hit = autotune.cached("areal_sweeps", key, points.device)
+        if hit is not None:
+            return hit
+    work = torch.empty_like(points)
+    scratch = [None]
+
+    def run(shape):
+        work.copy_(points)
+        scratch[0] = areal_sweeps_device(work, plan_device, plan, iterations=sweeps + 1, project_every=1000,
+                                         radius=radius, arithmetic=arithmetic, launch=shape, scratch=scratch[0])
+
+    best = autotune.tune("areal_sweeps", key, autotune.areal_candidates(points.device), run, device=points.device,
+                         force=force)
+    status, where = read_status(scratch[0])
+    if status != 0:
+        raise RuntimeError(f"areal sweep kernel failed while tuning (status {status} at {where})")
+    return best
 
 
 def read_status(scratch: torch.Tensor) -> tuple[int, int]:
@@ -281,7 +315,7 @@ def run_areal_smoothing_cuda(
     schedule: str = "ordered",
     arithmetic: str = "cat",
     schedule_block_size: int | None = None,
-    launch: dict | None = None,
+    launch: dict | str | None = None,
 ) -> tuple[np.ndarray, dict[str, float]]:
     """Run every CAT area-smoothing sweep on CUDA in dependency order.
 
@@ -292,6 +326,8 @@ def run_areal_smoothing_cuda(
     the native sm_100a kernel.  Only the exact ``"ordered"`` schedule exists.
     ``dtype=float64`` runs float64 storage and arithmetic and, unlike the
     reference's float64 Triton path, applies the sphere projection.
+    ``launch`` is a launch shape dict, ``"auto"`` (autotuned once per mesh
+    size and device) or None (the default shape).
     """
 
     try:

@@ -142,6 +142,7 @@ class RotationCostInputs:
     source_points: torch.Tensor
     source_values: torch.Tensor
     target_values: torch.Tensor
+    n_features: int = 1
 
 
 @dataclass(frozen=True)
@@ -184,6 +185,7 @@ class _Costing:
             self.inputs.target_values.data_ptr(), self.index.candidate_offsets.data_ptr(),
             self.index.candidate_faces.data_ptr(), self.matrices.data_ptr(),
             int(self.inputs.source_points.shape[0]), int(self.index.grid_size), int(count),
+            int(self.inputs.n_features), int(self.index.target_points.shape[0]),
         )
         lib = _native.library()
         stream = _native.stream_handle()
@@ -243,16 +245,24 @@ class RotationGridIndexDevice:
         return torch.stack(cols, dim=-1)
 
     def prepare_cost_inputs(self, source_points, source_values, target_values) -> RotationCostInputs:
+        """Upload points and features once.  Values are [n] (one feature, the
+        reference's form) or [F, n] (F features; the cost sums all F SSDs)."""
+
         source = torch.as_tensor(source_points, dtype=torch.float32, device=self.device).contiguous()
-        sv = torch.as_tensor(source_values, dtype=torch.float64, device=self.device).reshape(-1).contiguous()
-        tv = torch.as_tensor(target_values, dtype=torch.float64, device=self.device).reshape(-1).contiguous()
+        sv = torch.as_tensor(source_values, dtype=torch.float64, device=self.device)
+        tv = torch.as_tensor(target_values, dtype=torch.float64, device=self.device)
         if source.ndim != 2 or source.shape[1] != 3:
             raise ValueError("source_points must have shape [n, 3]")
-        if sv.numel() != source.shape[0]:
+        features = int(sv.shape[0]) if sv.ndim == 2 else 1
+        if sv.ndim > 2 or tv.ndim > 2 or (tv.shape[0] if tv.ndim == 2 else 1) != features:
+            raise ValueError("source_values and target_values must both be [n] or both [F, n] with the same F")
+        sv = sv.reshape(-1).contiguous()
+        tv = tv.reshape(-1).contiguous()
+        if sv.numel() != features * source.shape[0]:
             raise ValueError("source_values length does not match source_points")
-        if tv.numel() != self.target_points.shape[0]:
+        if tv.numel() != features * self.target_points.shape[0]:
             raise ValueError("target_values length does not match the target sphere")
-        return RotationCostInputs(source_points=source, source_values=sv, target_values=tv)
+        return RotationCostInputs(source_points=source, source_values=sv, target_values=tv, n_features=features)
 
     def _costing(self, inputs: RotationCostInputs, capacity: int) -> _Costing:
         cache = self.__dict__.setdefault("_costing_cache", {})
@@ -380,21 +390,55 @@ class RotationGridIndexDevice:
                                     iterations=iterations)
 
 
-def batched_costs(indices, inputs, angle_sets, *, tile: int = 256, n_ctas: int = 0) -> list[torch.Tensor]:
+def quaternion_matrices(quaternions) -> np.ndarray:
+    """[C, 9] float32 rotation matrices (row-major R, q_rotated = R p) of unit quaternions (w, x, y, z)."""
+
+    q = np.asarray(quaternions, dtype=np.float64).reshape(-1, 4)
+    q = q / np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    r = np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                  2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                  2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], axis=1)
+    return np.ascontiguousarray(r, dtype=np.float32)
+
+
+def uniform_quaternions(count: int, seed: int) -> np.ndarray:
+    """Seeded uniform random unit quaternions (Shoemake's subgroup algorithm), [count, 4] as (w, x, y, z)."""
+
+    rng = np.random.default_rng(seed)
+    u1, u2, u3 = rng.random((3, int(count)))
+    a, b = np.sqrt(1.0 - u1), np.sqrt(u1)
+    return np.stack([b * np.cos(2 * np.pi * u3), a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2),
+                     b * np.sin(2 * np.pi * u3)], axis=1)
+
+
+def batched_costs(indices, inputs, angle_sets=None, *, matrix_sets=None, tile: int = 256,
+                  n_ctas: int = 0) -> list[torch.Tensor]:
     """Costs of many candidate sets on many surfaces in ONE persistent launch.
 
     ``indices[i]`` (a RotationGridIndexDevice), ``inputs[i]`` (its
-    RotationCostInputs) and ``angle_sets[i]`` ([C_i, 3] angles) describe
-    surface i; surfaces may differ in size and candidate count.  Returns one
-    float64 cost tensor per surface, identical to
+    RotationCostInputs) and ``angle_sets[i]`` ([C_i, 3] Euler angles) or
+    ``matrix_sets[i]`` ([C_i, 9] float32 matrices, e.g. from
+    :func:`quaternion_matrices`) describe surface i; surfaces may differ in
+    size, feature count and candidate count.  Returns one float64 cost tensor
+    per surface, identical to
     ``indices[i].cost_batch_prepared(inputs[i], angle_sets[i])``.
+    ``tile`` (128/256/512 source points per work item) is the launch shape
+    chosen by :mod:`cat_surface_gpu_b200.autotune`.
     """
 
     n = len(indices)
-    if n == 0 or len(inputs) != n or len(angle_sets) != n:
-        raise ValueError("indices, inputs and angle_sets must be non-empty and of equal length")
+    sets = angle_sets if matrix_sets is None else matrix_sets
+    if (angle_sets is None) == (matrix_sets is None):
+        raise ValueError("give exactly one of angle_sets and matrix_sets")
+    if n == 0 or len(inputs) != n or len(sets) != n:
+        raise ValueError("indices, inputs and candidate sets must be non-empty and of equal length")
     dev = indices[0].device
-    mats = [torch.as_tensor(rotation_matrices_flat(np.asarray(a)), device=dev) for a in angle_sets]
+    if matrix_sets is None:
+        mats = [torch.as_tensor(rotation_matrices_flat(np.asarray(a)), device=dev) for a in angle_sets]
+    else:
+        mats = [torch.as_tensor(np.asarray(m, dtype=np.float32).reshape(-1, 9), device=dev).contiguous()
+                for m in matrix_sets]
     counts = [int(m.shape[0]) for m in mats]
     costs = torch.empty(sum(counts), dtype=torch.float64, device=dev)
     surfaces = (_native.RotationSurface * n)()
@@ -403,7 +447,7 @@ def batched_costs(indices, inputs, angle_sets, *, tile: int = 256, n_ctas: int =
             inp.source_points.data_ptr(), inp.source_values.data_ptr(), index.target_triangles.data_ptr(),
             index.target_faces.data_ptr(), inp.target_values.data_ptr(), index.candidate_offsets.data_ptr(),
             index.candidate_faces.data_ptr(), m.data_ptr(), int(inp.source_points.shape[0]), int(index.grid_size),
-            counts[i],
+            counts[i], int(inp.n_features), int(index.target_points.shape[0]),
         )
     n_src = (ctypes.c_int * n)(*[int(inp.source_points.shape[0]) for inp in inputs])
     n_cand = (ctypes.c_int * n)(*counts)

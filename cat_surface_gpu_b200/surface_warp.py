@@ -66,9 +66,16 @@ class _Solver:
         self.expdef_scratch = _scratch(dtype, device, 1, nx, ny)
         self.flow = torch.empty((2, ny, nx), dtype=dtype, device=device)
         self.flows = torch.empty((batch, 2, ny, nx), dtype=dtype, device=device)
+        self.last_velocity = None
 
-    def launch(self, stream_handle: int, flows: str = "last") -> None:
-        """Enqueue the whole solve on a stream (no host synchronisation when `assume`)."""
+    def launch(self, stream_handle: int, flows: str = "last", steps_per_registration: int = 1) -> None:
+        """Enqueue the whole solve on a stream (no host synchronisation when `assume`).
+
+        flows: "last" -- exponential of the last map's velocity (one registration);
+        "all" -- of every map's velocity; "registrations" -- of the last map
+        of each run of ``steps_per_registration`` maps (many registrations).
+        Torch's current stream must be the stream of ``stream_handle``.
+        """
 
         lib = _native.library()
         self.velocity.zero_()
@@ -90,6 +97,19 @@ class _Solver:
                 ),
                 "csg_dartel_expdef",
             )
+        elif flows == "registrations":
+            steps = int(steps_per_registration)
+            count = self.batch // steps
+            if self.last_velocity is None:
+                self.last_velocity = torch.empty((count, 2, self.ny, self.nx), dtype=self.dtype, device=self.device)
+            self.last_velocity.copy_(self.velocity.view(count, steps, 2, self.ny, self.nx)[:, steps - 1])
+            _native.check(
+                lib.csg_dartel_expdef(
+                    _dtype_code(self.dtype), count, self.nx, self.ny, self.last_velocity.data_ptr(), 10,
+                    self.flows.data_ptr(), None, self.scratch.data_ptr(), self.scratch.numel(), stream_handle,
+                ),
+                "csg_dartel_expdef",
+            )
         else:
             _native.check(
                 lib.csg_dartel_expdef(
@@ -105,6 +125,11 @@ class _GraphEntry:
     graph: torch.cuda.CUDAGraph
     solver: _Solver
     capture_seconds: float
+    kernels: int = 0  # native kernels inside the graph
+
+    def replay(self) -> None:
+        self.graph.replay()
+        _native.note_graph_replay(self.kernels)
 
 
 _GRAPH_CACHE: dict[tuple, _GraphEntry] = {}
@@ -118,23 +143,27 @@ def _graph_key(source, target, *, loop, lmreg, cycles, nit, its, code, kernel, s
     )
 
 
-def _capture(source, target, *, loop, lmreg, cycles, nit, its, code, device) -> _GraphEntry:
-    steps, ny, nx = (int(v) for v in source.shape)
-    solver = _Solver(steps, ny, nx, source.dtype, device, loop, lmreg, cycles, nit, its, code, True)
-    solver.source.copy_(source)
-    solver.target.copy_(target)
+def _capture(source, target, *, loop, lmreg, cycles, nit, its, code, device, flows: str = "last",
+             steps_per_registration: int = 1) -> _GraphEntry:
+    batch = int(source.shape[0]) if flows != "registrations" else int(source.shape[0] * source.shape[1])
+    ny, nx = (int(v) for v in source.shape[-2:])
+    solver = _Solver(batch, ny, nx, source.dtype, device, loop, lmreg, cycles, nit, its, code, True)
+    solver.source.copy_(source.reshape(batch, ny, nx))
+    solver.target.copy_(target.reshape(batch, ny, nx))
     torch.cuda.synchronize(device)
     started = time.perf_counter()
     side = torch.cuda.Stream(device=device)
     side.wait_stream(torch.cuda.current_stream(device))
     with torch.cuda.stream(side):
-        solver.launch(_native.stream_handle(side))  # warm up outside capture
+        solver.launch(_native.stream_handle(side), flows, steps_per_registration)  # warm up outside capture
     torch.cuda.synchronize(device)
     graph = torch.cuda.CUDAGraph()
+    before = _native.library().csg_kernel_launches()
     with torch.cuda.graph(graph, stream=side):
-        solver.launch(_native.stream_handle(side))
+        solver.launch(_native.stream_handle(side), flows, steps_per_registration)
+    kernels = int(_native.library().csg_kernel_launches() - before)
     torch.cuda.synchronize(device)
-    return _GraphEntry(graph=graph, solver=solver, capture_seconds=time.perf_counter() - started)
+    return _GraphEntry(graph=graph, solver=solver, capture_seconds=time.perf_counter() - started, kernels=kernels)
 
 
 def prepare_dartel_cuda_graph(source_maps, target_maps, *, loop: int = 6, lmreg: float = 1e-3, cycles: int = 3,
@@ -198,7 +227,7 @@ def solve_dartel_maps(source_maps, target_maps, *, loop: int = 6, lmreg: float =
             _GRAPH_CACHE[key] = entry
         entry.solver.source.copy_(source)
         entry.solver.target.copy_(target)
-        entry.graph.replay()
+        entry.replay()
         s = entry.solver
         return DartelSolveResult(s.flow.clone(), s.source.clone(), s.target.clone(), s.metrics.clone())
     steps, ny, nx = (int(v) for v in source.shape)
@@ -230,6 +259,53 @@ def solve_dartel_batch(source_maps, target_maps, *, loop: int = 6, lmreg: float 
     solver.target.copy_(target)
     solver.launch(_native.stream_handle(), flows="all")
     return solver.flows, solver.velocity, solver.metrics
+
+
+def solve_dartel_registrations(source_maps, target_maps, *, loop: int = 6, lmreg: float = 1e-3, cycles: int = 3,
+                               nit: int = 3, its: int = 3, code: int = 1, device="auto", dtype=torch.float64,
+                               assume_initial_nonzero: bool = False, cuda_graph: bool = False):
+    """Many SurfWarp registrations' DARTEL solves as ONE batched solve.
+
+    ``source_maps`` / ``target_maps`` are ``[registrations, steps, ny, nx]``
+    (the step maps of each registration, as ``solve_dartel_maps`` takes them
+    one registration at a time).  All registrations x steps maps go through
+    one ``csg_dartel_solve`` launch sequence, then the exponential of each
+    registration's last-map velocity.  Returns ``(flows [R, 2, ny, nx],
+    metrics [R, steps, loop * its, 3])``; each flow equals
+    ``solve_dartel_maps(source_maps[r], target_maps[r], assume_initial_nonzero=...,
+    cuda_graph=...).flow``.  With ``cuda_graph`` the whole batched solve is
+    captured once per shape and replayed; like the reference's graph path it
+    then assumes a nonzero initial update in every multigrid solve.
+    """
+
+    dev = resolve_device(device)
+    source = _tensor(source_maps, dev, dtype)
+    target = _tensor(target_maps, dev, dtype)
+    if source.ndim != 4 or tuple(source.shape) != tuple(target.shape):
+        raise ValueError("source_maps and target_maps must have the same shape [registrations, steps, ny, nx]")
+    if loop <= 0 or cycles < 0 or nit < 0 or its < 0:
+        raise ValueError("loop must be positive; cycles, nit and its non-negative")
+    regs, steps, ny, nx = (int(v) for v in source.shape)
+    if cuda_graph:
+        key = ("registrations",) + _graph_key(source, target, loop=loop, lmreg=lmreg, cycles=cycles, nit=nit,
+                                              its=its, code=code, kernel="native", squaring_kernel=None,
+                                              optimized=True)
+        entry = _GRAPH_CACHE.get(key)
+        if entry is None:
+            entry = _capture(source, target, loop=loop, lmreg=lmreg, cycles=cycles, nit=nit, its=its, code=code,
+                             device=dev, flows="registrations", steps_per_registration=steps)
+            _GRAPH_CACHE[key] = entry
+        entry.solver.source.copy_(source.reshape(regs * steps, ny, nx))
+        entry.solver.target.copy_(target.reshape(regs * steps, ny, nx))
+        entry.replay()
+        solver = entry.solver
+        return solver.flows[:regs].clone(), solver.metrics.view(regs, steps, -1, 3).clone()
+    solver = _Solver(regs * steps, ny, nx, dtype, dev, loop, lmreg, cycles, nit, its, code,
+                     bool(assume_initial_nonzero))
+    solver.source.copy_(source.reshape(regs * steps, ny, nx))
+    solver.target.copy_(target.reshape(regs * steps, ny, nx))
+    solver.launch(_native.stream_handle(), "registrations", steps)
+    return solver.flows[:regs], solver.metrics.view(regs, steps, -1, 3)
 
 
 def solve_dartel_from_surfaces(source_vertices, target_vertices, source_stencil, target_stencil, *,

@@ -48,6 +48,10 @@ typedef struct CUstream_st *csg_stream_t;
 
 CSG_API const char *csg_last_error(void);
 CSG_API int csg_abi_version(void);
+/* Kernels this library has launched in this process (every entry point
+ * counts its own launches; launches replayed from a captured CUDA graph are
+ * not seen here). */
+CSG_API long long csg_kernel_launches(void);
 
 /* ------------------------------------------------------------------------
  * Surf2Sphere: mesh topology (host, no device memory).
@@ -156,6 +160,27 @@ CSG_API int csg_selftest_barrier_timeout(void *scratch, size_t scratch_bytes, do
  * reference's torch path operation by operation (one rounding each).
  * params are the five regulariser values (sx, sy, mu, lambda, identity).
  * ---------------------------------------------------------------------- */
+
+/* Data term E_b(v) = 1/2 sum_x (S_b(exp(v_b)(x)) - T_b(x))^2, exp(v) by k
+ * scaling-and-squaring compositions (expdef's maps), and its exact adjoint
+ * (no reference counterpart: the north-star's hand-written DARTEL adjoint;
+ * the reference's Gauss-Newton gradient of the same term is
+ * initialise_objfun + squaring_update, dartel_grid.py:723-914).
+ * Checkpoints: the forward keeps phi_0, phi_c, phi_2c, ... (c =
+ * checkpoint_every; csg_dartel_data_checkpoints maps of [batch][2][ny][nx]);
+ * the backward recomputes the maps between checkpoints.  objective [batch];
+ * grad_velocity [batch][2][ny][nx] = grad_scale[b] dE_b/dv_b (grad_scale a
+ * device array [batch] or NULL for 1).  The value scatter of each
+ * composition step uses atomic adds, so gradients agree across runs to
+ * rounding, not bit for bit. */
+CSG_API size_t csg_dartel_data_scratch_bytes(int dtype, int batch, int nx, int ny, int k, int checkpoint_every);
+CSG_API int csg_dartel_data_checkpoints(int k, int checkpoint_every);
+CSG_API int csg_dartel_data_forward(int dtype, int batch, int nx, int ny, const void *velocity, const void *source,
+                                    const void *target, int k, int checkpoint_every, void *checkpoints,
+                                    void *objective, void *scratch, size_t scratch_bytes, csg_stream_t stream);
+CSG_API int csg_dartel_data_backward(int dtype, int batch, int nx, int ny, const void *source, const void *target,
+                                     int k, int checkpoint_every, const void *checkpoints, const void *grad_scale,
+                                     void *grad_velocity, void *scratch, size_t scratch_bytes, csg_stream_t stream);
 
 /* Scratch for csg_dartel_solve / _step / _fmg / _expdef / _squaring / _objfun. */
 CSG_API size_t csg_dartel_scratch_bytes(int dtype, int batch, int nx, int ny);
@@ -268,19 +293,24 @@ CSG_API int csg_rotation_grid_build(const double *points, int n_points, const in
                                     int grid_size, int margin, int32_t *offsets, int32_t *cell_faces,
                                     long long capacity, long long *count);
 
-/* One surface of a batched cost evaluation (all device pointers). */
+/* One surface of a batched cost evaluation (all device pointers).  With
+ * n_features F > 1 the cost sums the squared differences of all F features
+ * (feature-major: src_values [F][n_src], tgt_values [F][n_tgt_points]);
+ * n_features 0 or 1 is the reference's single feature. */
 typedef struct {
     const float *src_points;     /* [n_src][3] source sphere points */
-    const double *src_values;    /* [n_src] source feature */
+    const double *src_values;    /* [n_features][n_src] source features */
     const float *triangles;      /* [n_tri][9] target triangle corners */
     const int32_t *faces;        /* [n_tri][3] target faces */
-    const double *tgt_values;    /* target feature per target point */
+    const double *tgt_values;    /* [n_features][n_tgt_points] target features */
     const int32_t *grid_offsets; /* csg_rotation_grid_build offsets */
     const int32_t *grid_faces;   /* csg_rotation_grid_build cell faces */
     const float *matrices;       /* [n_candidates][9] column-major rotations */
     int32_t n_src;
     int32_t grid_size;
     int32_t n_candidates;
+    int32_t n_features;          /* 0 or 1: one feature */
+    int32_t n_tgt_points;        /* feature stride of tgt_values (needed when n_features > 1) */
 } csg_rotation_surface;
 
 CSG_API size_t csg_rotation_scratch_bytes(int n_surfaces, const int *n_src, const int *n_candidates, int tile);
@@ -326,7 +356,7 @@ CSG_API size_t csg_feature_scratch_bytes(int n_points, int n_faces, int n_slots,
 CSG_API int csg_feature_edge_sum(int dtype, int n_faces, const int32_t *faces, const void *vertices, double *out_sum,
                                  void *scratch, size_t scratch_bytes, csg_stream_t stream);
 
-/* smooth_geometry (372-388): `iterations` Jacobi heat steps, float32 out. */
+/* smooth_geometry (372-388): `iterations` Jacobi heat steps, float32 out (must not overlap vertices). */
 CSG_API int csg_feature_smooth_geometry(int n_points, const int32_t *nbr_off, const int32_t *nbr, const float *vertices,
                                         int iterations, float *out, void *scratch, size_t scratch_bytes,
                                         csg_stream_t stream);
@@ -334,7 +364,7 @@ CSG_API int csg_feature_smooth_geometry(int n_points, const int32_t *nbr_off, co
 /* smooth_values / smooth_values_many (390-476): `series` independent
  * smoothings of one value field (<= 16), sigma and iteration count per series
  * (host arrays); via_norm selects the single-FWHM distance form.
- * out [series][n_points]. */
+ * out [series][n_points], which must not overlap values (CSG_ERR_ARG). */
 CSG_API int csg_feature_smooth_values(int n_points, const int32_t *nbr_off, const int32_t *nbr, int n_slots,
                                       int geometry_dtype, const void *geometry, const double *values, int series,
                                       const double *sigmas, const int32_t *iterations, int via_norm, double *out,

@@ -614,3 +614,71 @@ def average_xz_surfaces(x_surface, z_surface):
     avg = (wx[:, None] * xv + wz[:, None] * zv) / total[:, None]
     avg = avg / np.maximum(np.linalg.norm(avg, axis=-1, keepdims=True), np.finfo(np.float64).eps)
     return avg.astype(np.float32)
+
+
+# --------------------------------------------------------------------------- data-term adjoint
+
+
+def data_term(v, source, target, k):
+    """E(v) = 1/2 sum (S(exp(v)) - T)^2, exp = expdef's k squarings, S bilinear with the boundary rule.
+
+    Forward of the hand-written adjoint (no reference counterpart; the
+    sample is initialise_objfun's, dartel_grid.py:723-775)."""
+
+    ny, nx = source.shape
+    phi = expdef(v, k)
+    idx = interpolation_indices(phi[0] - v.dtype.type(1), phi[1] - v.dtype.type(1), nx, ny)
+    r = interpolate_channels(source[None], idx)[0] - target
+    return v.dtype.type(0.5) * np.sum(r * r)
+
+
+def data_term_gradient(v, source, target, k):
+    """Exact reverse-mode derivative dE/dv of :func:`data_term` (sequential scatter order)."""
+
+    ny, nx = source.shape
+    dt = v.dtype.type
+    s = dt(1.0 / 2 ** k)
+    maps = [identity_map(nx, ny, v.dtype) + v * s]
+    for _ in range(k):
+        maps.append(composition(maps[-1], maps[-1]))
+    phi = maps[-1]
+    x22, y22, x12, y12, x21, y21, x11, y11, dx1, dx2, dy1, dy2 = interpolation_indices(phi[0] - dt(1), phi[1] - dt(1),
+                                                                                        nx, ny)
+    k22, k12, k21, k11 = source[y22, x22], source[y12, x12], source[y21, x21], source[y11, x11]
+    r = ((k22 * dx2 + k12 * dx1) * dy2 + (k21 * dx2 + k11 * dx1) * dy1) - target
+    abar = np.stack((r * ((k11 - k21) * dy1 + (k12 - k22) * dy2),
+                     r * ((k11 * dx1 + k21 * dx2) - (k12 * dx1 + k22 * dx2))))
+    periods = np.array((nx, ny), dtype=v.dtype).reshape(2, 1, 1)
+    for i in reversed(range(k)):
+        f = maps[i]
+        x22, y22, x12, y12, x21, y21, x11, y11, dx1, dx2, dy1, dy2 = interpolation_indices(f[0] - dt(1), f[1] - dt(1),
+                                                                                            nx, ny)
+        cf = f - dt(1)
+        c22 = cf[:, y22, x22]
+        c12 = _unwrap(cf[:, y12, x12], c22, periods)
+        c21 = _unwrap(cf[:, y21, x21], c22, periods)
+        c11 = _unwrap(cf[:, y11, x11], c22, periods)
+        dcx = (c12 - c22) * dy2 + (c11 - c21) * dy1
+        dcy = (c21 * dx2 + c11 * dx1) - (c22 * dx2 + c12 * dx1)
+        pbar = np.zeros_like(f)
+        pbar[0] += abar[0] * dcx[0] + abar[1] * dcx[1]
+        pbar[1] += abar[0] * dcy[0] + abar[1] * dcy[1]
+        for ch in range(2):
+            for yy, xx, weight in ((y22, x22, dx2 * dy2), (y12, x12, dx1 * dy2), (y21, x21, dx2 * dy1),
+                                   (y11, x11, dx1 * dy1)):
+                np.add.at(pbar[ch], (yy, xx), abar[ch] * weight)
+        abar = pbar
+    return abar * s
+
+
+def gauss_newton_gradient(v, source, target, k):
+    """The reference's DARTEL gradient of the same term (code 0): initialise_objfun at exp(v)
+    pulled back by squaring_update, times 2^-k (dartel_grid.py:1420-1616 before the regulariser)."""
+
+    s = 1.0 / 2 ** k
+    t, jac = expdef(v, k, return_jacobian=True)
+    jac = jac_div_smalldef(jac, v, s)
+    _, rhs, hess = initialise_objfun(source, target, t, jac)
+    t2, j2 = smalldef_jac(v, -s)
+    rhs, _, _, _, _ = squaring_update(rhs, hess, t2, j2, k)
+    return rhs * v.dtype.type(s)

@@ -7,6 +7,7 @@ are committed so GPU tests never need the reference at run time.
 For each seeded synthetic mesh (``cat_surface_gpu_b200.synthetic``):
 
 * ``faces``       -- triangle array (int32; uint16 on disk when it fits)
+* ``surface``     -- the input surface (float32)
 * ``prefix``      -- the binary's stage 1-5 output (``CAT_Surf2Sphere in out 5 0``):
                      the input of the ordered sweeps
 * ``final``       -- the binary's full output (``CAT_Surf2Sphere in out 10 0``)
@@ -41,6 +42,8 @@ CASES = {
     "c1": lambda: synthetic.folded_icosphere(5, seed=1, radius_mm=60.0),
     # folded Fibonacci convex hull: 61,442 vertices / 122,880 faces, 70 mm
     "c2": lambda: synthetic.folded_hull(61442, seed=2, radius_mm=70.0),
+    # a second, differently seeded folded hull: the SurfWarp target of the chain workload
+    "c3": lambda: synthetic.folded_hull(61442, seed=3, radius_mm=70.0),
 }
 
 
@@ -71,6 +74,7 @@ def main() -> int:
         np.savez_compressed(
             HERE / f"surf2sphere_{name}.npz",
             faces=faces.astype(face_dtype),
+            surface=vertices.astype(np.float32),
             prefix=prefix.vertices.astype(np.float32),
             final=final.vertices.astype(np.float32),
             source_area=np.float64(surface_area(GiftiMesh(vertices, faces))),

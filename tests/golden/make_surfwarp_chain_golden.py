@@ -16,11 +16,20 @@ icosphere under a known rotation, scaled to radius 100.  Writes
 rotation angle/cost, the rotated sphere, the sphere after run 0, the final
 sphere).
 
-Usage: ``python tests/golden/make_surfwarp_chain_golden.py``
+``--workload hemisphere`` instead runs the 61,442-vertex hemisphere chain of
+the benchmark: source = the ``surf2sphere_c2`` surface with the upstream
+binary's sphere, target = the ``surf2sphere_c3`` surface and sphere, two runs
+of two steps on a 256 x 128 sheet with ``-avg``; it writes
+``surfwarp_chain_hemisphere_golden.npz`` (parameters, rotation angle/cost, the
+number of rotation candidates the search evaluated, the final sphere and the
+CPU wall time of the chain).
+
+Usage: ``python tests/golden/make_surfwarp_chain_golden.py [--workload small|hemisphere]``
 """
 
 from __future__ import annotations
 
+import argparse
 import os
 from pathlib import Path
 import sys
@@ -74,14 +83,16 @@ def chain_inputs(seed: int = 5):
     )
 
 
-def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size):
-    faces = data["faces"]
+def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size, target_faces=None):
+    source_faces = data["faces"]
+    target_faces = source_faces if target_faces is None else target_faces
     temp = Path(tempfile.mkdtemp(prefix="chain_golden_"))
     count = [0]
 
-    def stencil(sphere, normalize):
+    def stencil(sphere, normalize, faces=None):
         count[0] += 1
         path = temp / f"s{count[0]}.stencil"
+        faces = source_faces if faces is None else faces
         build_surface_stencil(sphere, faces, nx=nx, ny=ny, normalize=normalize).to_file(path)
         return ReferenceStencil.from_file(path)
 
@@ -89,7 +100,7 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size):
         return st.to(CPU, geometry_dtype=torch.float32)
 
     source_stencil = stencil(data["source_sphere"], True)
-    target_stencil = stencil(data["target_sphere"], True)
+    target_stencil = stencil(data["target_sphere"], True, target_faces)
     values = []
     for st, surface, fwhm in ((source_stencil, data["source_surface"], 15.0),
                               (target_stencil, data["target_surface"], 10.0)):
@@ -97,6 +108,14 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size):
         mapped = dev.resample_vertices(torch.as_tensor(surface))
         values.append(dev.curvature_type5(mapped, fwhm).numpy())
     pipeline = RotationPipeline.from_stencil(target_stencil, device=CPU, grid_size=rotation_grid_size, margin=1)
+    evaluated = [0]
+    plain_cost = pipeline.index.cost_batch_prepared
+
+    def counting_cost(inputs, angles, **kwargs):
+        evaluated[0] += int(torch.as_tensor(angles).reshape(-1, 3).shape[0])
+        return plain_cost(inputs, angles, **kwargs)
+
+    pipeline.index.cost_batch_prepared = counting_cost
     rotation = pipeline.search(source_stencil.sphere_points, values[0], values[1], point_chunk=4096)
     angle = rotation.angle.detach().cpu().numpy()
     current_sphere = _rotate_vertices(_normalise_sphere(data["source_sphere"]), angle)
@@ -136,7 +155,7 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size):
     if avg:
         avg_fwhm = tuple(5.0 / (3.0 ** (steps * (runs + 1) + i)) for i in range(steps))
         avg_result = solve(torch.as_tensor(avg_source_surface), torch.as_tensor(avg_target_surface), avg_source_dev,
-                           on_cpu(stencil(avg_target_sphere, False)), avg_fwhm)
+                           on_cpu(stencil(avg_target_sphere, False, target_faces)), avg_fwhm)
         main_warped = apply_flow_to_stenciled_sphere(torch.as_tensor(final_prewarp), last.flow, current_dev,
                                                      inverse=True, device=CPU, dtype=torch.float64)
         avg_warped = apply_flow_to_stenciled_sphere(torch.as_tensor(avg_source_sphere), avg_result.flow,
@@ -145,19 +164,50 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size):
         unrotated = avg_warped.to(torch.float64) @ reverse.transpose(0, 1)
         current_sphere = _average_xz_surfaces(unrotated, main_warped, device=CPU).numpy().astype(np.float32)
     return dict(rotation_angle=angle.astype(np.float64), rotation_cost=float(rotation.cost),
+                rotation_candidates_evaluated=np.int64(evaluated[0]),
                 source_values=values[0], target_values=values[1],
                 rotated_initial=rotated_initial, after_run0=after_run0, final_sphere=current_sphere)
 
 
+HEMISPHERE_PARAMS = dict(nx=256, ny=128, steps=2, runs=2, avg=True, loop=6, rotation_grid_size=128)
+
+
+def hemisphere_inputs():
+    """The benchmark's hemisphere pair: c2 (source) and c3 (target) with the upstream binary's spheres."""
+
+    return np.load(HERE / "surf2sphere_c2.npz"), np.load(HERE / "surf2sphere_c3.npz")
+
+
+def reference_hemisphere_chain():
+    source, target = hemisphere_inputs()
+    data = dict(faces=source["faces"].astype(np.int32), source_surface=source["surface"],
+                source_sphere=source["final"], target_surface=target["surface"], target_sphere=target["final"])
+    return data, target["faces"].astype(np.int32)
+
+
 def main() -> int:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--workload", choices=("small", "hemisphere"), default="small")
+    args = parser.parse_args()
     torch.set_num_threads(max(1, os.cpu_count() or 1))
-    data = chain_inputs()
-    started = time.perf_counter()
-    result = reference_chain(data, **PARAMS)
-    print(f"reference chain on CPU: {time.perf_counter() - started:.1f} s, angle {result['rotation_angle']}, "
+    if args.workload == "small":
+        data = chain_inputs()
+        started = time.perf_counter()
+        result = reference_chain(data, **PARAMS)
+        seconds = time.perf_counter() - started
+        np.savez_compressed(HERE / "surfwarp_chain_golden.npz", **data, **result,
+                            **{f"param_{k}": np.asarray(v) for k, v in PARAMS.items()})
+    else:
+        data, target_faces = reference_hemisphere_chain()
+        started = time.perf_counter()
+        result = reference_chain(data, target_faces=target_faces, **HEMISPHERE_PARAMS)
+        seconds = time.perf_counter() - started
+        keep = ("rotation_angle", "rotation_cost", "rotation_candidates_evaluated", "final_sphere")
+        np.savez_compressed(HERE / "surfwarp_chain_hemisphere_golden.npz", **{k: result[k] for k in keep},
+                            cpu_seconds=np.float64(seconds), cpu_threads=np.int64(torch.get_num_threads()),
+                            **{f"param_{k}": np.asarray(v) for k, v in HEMISPHERE_PARAMS.items()})
+    print(f"reference chain on CPU ({args.workload}): {seconds:.1f} s, angle {result['rotation_angle']}, "
           f"cost {result['rotation_cost']:.6f}")
-    np.savez_compressed(HERE / "surfwarp_chain_golden.npz", **data, **result,
-                        **{f"param_{k}": np.asarray(v) for k, v in PARAMS.items()})
     return 0
 
 

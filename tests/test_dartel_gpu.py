@@ -171,6 +171,24 @@ def test_batched_and_graph_solves_equal_single_solves(sw):
     np.testing.assert_array_equal(host(graphed2.flow), oracle_flow)
 
 
+def test_registration_batch_equals_one_at_a_time(sw):
+    """R registrations x 2 step maps in one batched solve == R solve_dartel_maps calls (eager and graphed)."""
+
+    from cat_surface_gpu_b200 import synthetic
+
+    ny, nx, regs, steps = 32, 64, 5, 2
+    src = np.stack([[synthetic.smooth_sheet(ny, nx, 100 + 2 * r + s) for s in range(steps)] for r in range(regs)])
+    tgt = np.stack([[synthetic.smooth_sheet(ny, nx, 300 + 2 * r + s) for s in range(steps)] for r in range(regs)])
+    s_dev, t_dev = torch.as_tensor(src).cuda(), torch.as_tensor(tgt).cuda()
+    for graph in (False, True):
+        flows, metrics = sw.solve_dartel_registrations(s_dev, t_dev, loop=3, its=2, cuda_graph=graph)
+        assert tuple(flows.shape) == (regs, 2, ny, nx) and tuple(metrics.shape) == (regs, steps, 6, 3)
+        for r in range(regs):
+            one = sw.solve_dartel_maps(s_dev[r], t_dev[r], loop=3, its=2, cuda_graph=graph)
+            np.testing.assert_array_equal(host(flows[r]), host(one.flow))
+            np.testing.assert_array_equal(host(metrics[r]), host(one.metrics))
+
+
 @pytest.mark.parametrize("tag", TAGS)
 def test_final_warp_and_average(sw, tag):
     flow = cuda(g(tag, "solve_flow"), tag)

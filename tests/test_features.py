@@ -104,3 +104,25 @@ def test_native_features_match_oracle_closely(device_stencil):
     got = host(st.smooth_values_many(torch.as_tensor(F["values"]).cuda(), torch.as_tensor(m).cuda(), (5.0,))[0])
     want = of.smooth_values_many(F["values"], m, F["faces"], (5.0,), tab)[0]
     np.testing.assert_allclose(got, want, rtol=0, atol=1e-14)
+
+
+@pytest.mark.gpu
+def test_smoothing_with_even_and_odd_iteration_counts(device_stencil):
+    """Jacobi smoothing never updates in place: both iteration parities match the oracle and repeat exactly."""
+
+    from cat_surface_gpu_b200 import features
+
+    st = device_stencil
+    m = F["resampled32"]
+    tab = _table()
+    mapped = torch.as_tensor(m).cuda()
+    values = torch.as_tensor(F["values"]).cuda()
+    parities = set()
+    for fwhm in (5.0, 10.0, 20.0, 30.0, 40.0):  # 1, 2, 7, 15 and 26 iterations
+        iterations, _ = features.heat_parameters(st, mapped, fwhm)
+        parities.add(iterations % 2)
+        first = host(st.smooth_values(values, mapped, fwhm))
+        np.testing.assert_array_equal(host(st.smooth_values(values, mapped, fwhm)), first)
+        want = of.smooth_values(F["values"], m, F["faces"], fwhm, tab)
+        np.testing.assert_allclose(first, want, rtol=0, atol=1e-13)
+    assert parities == {0, 1}

@@ -124,6 +124,39 @@ def test_batched_surfaces_equal_single_surface_costs(native_library):
 
 
 @pytest.mark.gpu
+def test_two_features_and_quaternion_candidates(native_library):
+    """F = 2 features sum both SSDs; quaternion matrices rotate like Euler matrices of the same rotation."""
+
+    from cat_surface_gpu_b200 import synthetic
+    from cat_surface_gpu_b200.surface_rotation import (RotationGridIndex, batched_costs, quaternion_matrices,
+                                                       rotation_matrices_flat, uniform_quaternions)
+
+    rng = np.random.default_rng(9)
+    tp, tf = synthetic.unit_icosphere(4)
+    sp = tp + rng.normal(scale=0.02, size=tp.shape)
+    sp = (sp / np.linalg.norm(sp, axis=1, keepdims=True)).astype(np.float32)
+    index = RotationGridIndex.from_geometry(tp, tf, grid_size=32, margin=1,
+                                            include_dense_candidate_table=False).to("cuda")
+    f_src = np.stack([np.sin(3 * sp[:, 0]), np.cos(2 * sp[:, 1] + sp[:, 2])])
+    f_tgt = np.stack([np.sin(3 * tp[:, 0]), np.cos(2 * tp[:, 1] + tp[:, 2])])
+    both = index.prepare_cost_inputs(sp, f_src, f_tgt)
+    one = [index.prepare_cost_inputs(sp, f_src[k], f_tgt[k]) for k in range(2)]
+    quats = uniform_quaternions(64, seed=4)
+    mats = quaternion_matrices(quats)
+    got = batched_costs([index], [both], matrix_sets=[mats])[0].cpu().numpy()
+    parts = [batched_costs([index], [inp], matrix_sets=[mats])[0].cpu().numpy() for inp in one]
+    np.testing.assert_allclose(got, parts[0] + parts[1], rtol=1e-12)
+    # matrices given directly reproduce the Euler-angle path bit for bit
+    angles = rng.uniform(-0.6, 0.6, size=(16, 3))
+    np.testing.assert_array_equal(batched_costs([index], [one[0]], matrix_sets=[rotation_matrices_flat(angles)])[0]
+                                  .cpu().numpy(), index.cost_batch_prepared(one[0], angles).cpu().numpy())
+    # a quaternion and its negative are the same rotation; rows of R are orthonormal
+    np.testing.assert_allclose(quaternion_matrices(-quats), mats, atol=1e-7)
+    r = mats.reshape(-1, 3, 3).astype(np.float64)
+    np.testing.assert_allclose(r @ r.transpose(0, 2, 1), np.broadcast_to(np.eye(3), r.shape), atol=1e-6)
+
+
+@pytest.mark.gpu
 def test_tetrahedron_known_answers(native_library):
     """Reference test_surface_rotation.py:37-62 and 149-202: identity cost 0, first-minimum rules."""
 
