@@ -75,6 +75,9 @@ def parse_args():
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-batched", action="store_true", help="skip the batched rotation / DARTEL legs")
     parser.add_argument("--no-e2e", action="store_true")
+    parser.add_argument("--profile", action="store_true",
+                        help="for profilers: --warmup then --steps hemispheres with the default sweep launch shape, "
+                             "no parity, e2e, CPU or batched legs; prints the step times only")
     return parser.parse_args()
 
 
@@ -250,7 +253,7 @@ def run_reference(args):
 class Hemisphere:
     """Device-resident inputs of the hemisphere chain and its step."""
 
-    def __init__(self, meshes, device, dartel_dtype):
+    def __init__(self, meshes, device, dartel_dtype, autotune_launch: bool = True):
         import torch
 
         from cat_surface_gpu_b200 import surf2sphere
@@ -264,7 +267,8 @@ class Hemisphere:
         self.points = torch.empty_like(self.pristine)
         self.radius = projection_radius(meshes["prefix"])
         self.launch = surf2sphere.tuned_areal_launch(self.pristine, self.plan_device, self.plan, arithmetic="cat",
-                                                     radius=self.radius)
+                                                     radius=self.radius) if autotune_launch else dict(
+            surf2sphere.DEFAULT_LAUNCH)
         self.scratch = None
         self.meshes_in = (GiftiMesh(meshes["surface"], meshes["faces"]),
                           GiftiMesh(meshes["target_surface"], meshes["target_faces"]),
@@ -463,7 +467,7 @@ def run_native(args):
     device = torch.device("cuda", local)
     meshes = load_meshes()
     n, f = meshes["prefix"].shape[0], meshes["faces"].shape[0]
-    hemi = Hemisphere(meshes, device, torch.float64)
+    hemi = Hemisphere(meshes, device, torch.float64, autotune_launch=not args.profile)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
     stream = torch.cuda.current_stream()
 
@@ -499,6 +503,13 @@ def run_native(args):
     status, where = surf2sphere.read_status(hemi.scratch)
     if status != 0:
         raise RuntimeError(f"sweep kernel status {status} at {where}")
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "step_ms": step_ms, "sweeps_kernel_ms": kernel_ms,
+                              "gpu_launches": launches}))
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     total_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device=device)
     if world > 1:
         dist.all_reduce(total_ms, op=dist.ReduceOp.MAX)

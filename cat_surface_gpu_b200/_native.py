@@ -34,6 +34,9 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_last_error": (ctypes.c_char_p, []),
     "csg_abi_version": (_I, []),
     "csg_kernel_launches": (ctypes.c_longlong, []),
+    "csg_preprocess_scratch_bytes": (c_size_t, [_I, _I]),
+    "csg_surf2sphere_preprocess": (_I, [_P, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, c_size_t, _I, _I,
+                                        _I, ctypes.c_double, _P]),
     "csg_mesh_incidence": (_I, [_I, _P, _I, _P, _P]),
     "csg_mesh_neighbours": (_I, [_I, _P, _I, _P, _P, _I]),
     "csg_dependency_levels": (_I, [_I, _P, _P, _P]),
@@ -72,6 +75,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_average_xz": (_I, [_I, _P, _P, _P, _P]),
     "csg_rotation_grid_build": (_I, [_P, _I, _P, _I, _I, _I, _P, _P, ctypes.c_longlong, _P]),
     "csg_rotation_scratch_bytes": (c_size_t, [_I, _P, _P, _I]),
+    "csg_rotation_grid_scratch_bytes": (c_size_t, [_I]),
+    "csg_rotation_grid_build_device": (_I, [_P, _I, _P, _I, _I, _I, _P, _P, ctypes.c_longlong, _P, _P, c_size_t, _P]),
     "csg_rotation_cost_batch": (_I, [_I, _P, _P, _I, _I, _P, c_size_t, _P]),
     "csg_rotation_status": (_I, [_P, _I, _P, _P]),
     "csg_feature_resample": (_I, [_I, _I, _P, _P, _P, _P, _P]),
@@ -85,6 +90,9 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_feature_curvature2": (_I, [_I, _P, _P, _P, _P, _P, _P]),
     "csg_feature_minmax": (_I, [_I, _I, _P, _P, _P, c_size_t, _P]),
     "csg_stencil_build": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "csg_stencil_scratch_bytes": (c_size_t, [_I, _I, _I, _I, _I, _I]),
+    "csg_stencil_build_device": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P,
+                                      c_size_t, _P]),
     "csg_read_status": (_I, [_P, _P, _P, _P]),
 }
 

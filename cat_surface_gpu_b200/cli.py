@@ -55,7 +55,8 @@ def surf2sphere_main(argv: list[str] | None = None) -> int:
     parser.add_argument("--areal-schedule", choices=("ordered", "color"), default="ordered")
     parser.add_argument("--areal-arithmetic", choices=("cat", "fp32"), default="cat")
     args = parser.parse_args(argv)
-    reference_cli = _binary("CAT_Surf2Sphere", args.reference_cli)
+    reference_cli = (_binary("CAT_Surf2Sphere", args.reference_cli) if args.preprocess_kernel == "cpu"
+                     else args.reference_cli)
     result = run_cat_surf2sphere_gpu(
         args.input_surface, args.output_surface, reference_cli=reference_cli, stop_at=args.stop_at,
         device=args.device, dtype=args.dtype, kernel=args.kernel, preprocess_kernel=args.preprocess_kernel,

@@ -237,8 +237,17 @@ __device__ __forceinline__ float dmul<float>(float a, float b) { return __fmul_r
 // One vertex update by a group of G lanes.  All 32 lanes of the warp must
 // call this together (warp shuffles); inactive groups pass v < 0.  `tri`
 // points at the vertex's incident-face slots (shared or global memory).
+//
+// float64 accumulation (CAT and FP64 modes): every lane computes one face's
+// area and area-weighted centre products and stages them in shared memory;
+// lanes 0, 1 and 2 of the group then each sum, in slot order, the area
+// total and one coordinate's weighted sum and divide it -- three dependent
+// chains and three divides in parallel instead of one lane doing all four
+// sums and three divides.  The arithmetic is unchanged: same products, same
+// order of additions.
 template <int MODE, int G, bool SMEM>
-__device__ __forceinline__ void update_vertex(const ArealParams& p, int v, const int4* tri, int deg) {
+__device__ __forceinline__ void update_vertex(const ArealParams& p, int v, const int4* tri, int deg,
+                                              double (*stage)[32]) {
     using T = Traits<MODE>;
     using Acc = typename T::Acc;
     const int lane = threadIdx.x & 31;
@@ -246,32 +255,81 @@ __device__ __forceinline__ void update_vertex(const ArealParams& p, int v, const
     const int gbase = lane & ~(G - 1);
     if (v < 0) deg = 0;
     const int wdeg = __reduce_max_sync(kFull, deg);
-    Acc total = 0, wx = 0, wy = 0, wz = 0;
-    for (int c0 = 0; c0 < wdeg; c0 += G) {
-        const int j = c0 + glane;
-        Acc fa = 0, fx = 0, fy = 0, fz = 0;
-        if (j < deg) {
-            const int4 t = SMEM ? tri[j] : __ldg(tri + j);
-            auto a = T::load(p.work, t.x);
-            auto b = T::load(p.work, t.y);
-            auto c = T::load(p.work, t.z);
-            T::face(a, b, c, fa, fx, fy, fz);
-        }
+    if constexpr (sizeof(Acc) == 8) {
+        double total = 0, wsum = 0;
+        const double* mine = stage[1 + (glane < 3 ? glane : 0)];
+        for (int c0 = 0; c0 < wdeg; c0 += G) {
+            const int j = c0 + glane;
+            double fa = 0, fx = 0, fy = 0, fz = 0;
+            if (j < deg) {
+                const int4 t = SMEM ? tri[j] : __ldg(tri + j);
+                auto a = T::load(p.work, t.x);
+                auto b = T::load(p.work, t.y);
+                auto c = T::load(p.work, t.z);
+                double mx, my, mz;
+                T::face(a, b, c, fa, mx, my, mz);
+                fx = __dmul_rn(fa, mx);
+                fy = __dmul_rn(fa, my);
+                fz = __dmul_rn(fa, mz);
+            }
+            stage[0][lane] = fa;
+            stage[1][lane] = fx;
+            stage[2][lane] = fy;
+            stage[3][lane] = fz;
+            __syncwarp();
+            if (glane < 3) {
+                const int n = min(G, deg - c0);
 #pragma unroll
-        for (int q = 0; q < G; ++q) {
-            const Acc a = __shfl_sync(kFull, fa, gbase + q);
-            const Acc x = __shfl_sync(kFull, fx, gbase + q);
-            const Acc y = __shfl_sync(kFull, fy, gbase + q);
-            const Acc z = __shfl_sync(kFull, fz, gbase + q);
-            if (c0 + q < deg) {  // slot order == ascending face id
-                total = dadd<Acc>(total, a);
-                wx = dadd<Acc>(wx, dmul<Acc>(a, x));
-                wy = dadd<Acc>(wy, dmul<Acc>(a, y));
-                wz = dadd<Acc>(wz, dmul<Acc>(a, z));
+                for (int q = 0; q < G; ++q) {
+                    if (q < n) {  // slot order == ascending face id
+                        total = __dadd_rn(total, stage[0][gbase + q]);
+                        wsum = __dadd_rn(wsum, mine[gbase + q]);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        const bool write = v >= 0 && total > 0.0;
+        const double safe = total > 1.0e-20 ? total : 1.0e-20;
+        const double comp = (glane < 3 && write) ? __ddiv_rn(wsum, safe) : 0.0;
+        if constexpr (MODE == CSG_ARITH_CAT) {
+            const float cf = __double2float_rn(comp);
+            const float cy = __shfl_sync(kFull, cf, gbase + 1);
+            const float cz = __shfl_sync(kFull, cf, gbase + 2);
+            if (write && glane == 0) __stcg(static_cast<float4*>(p.work) + v, make_float4(cf, cy, cz, 0.0f));
+        } else {
+            const double cy = __shfl_sync(kFull, comp, gbase + 1);
+            const double cz = __shfl_sync(kFull, comp, gbase + 2);
+            if (write && glane == 0) T::write(p.work, v, comp, cy, cz);
+        }
+    } else {
+        Acc total = 0, wx = 0, wy = 0, wz = 0;
+        for (int c0 = 0; c0 < wdeg; c0 += G) {
+            const int j = c0 + glane;
+            Acc fa = 0, fx = 0, fy = 0, fz = 0;
+            if (j < deg) {
+                const int4 t = SMEM ? tri[j] : __ldg(tri + j);
+                auto a = T::load(p.work, t.x);
+                auto b = T::load(p.work, t.y);
+                auto c = T::load(p.work, t.z);
+                T::face(a, b, c, fa, fx, fy, fz);
+            }
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                const Acc a = __shfl_sync(kFull, fa, gbase + q);
+                const Acc x = __shfl_sync(kFull, fx, gbase + q);
+                const Acc y = __shfl_sync(kFull, fy, gbase + q);
+                const Acc z = __shfl_sync(kFull, fz, gbase + q);
+                if (c0 + q < deg) {  // slot order == ascending face id
+                    total = dadd<Acc>(total, a);
+                    wx = dadd<Acc>(wx, dmul<Acc>(a, x));
+                    wy = dadd<Acc>(wy, dmul<Acc>(a, y));
+                    wz = dadd<Acc>(wz, dmul<Acc>(a, z));
+                }
             }
         }
+        if (v >= 0 && glane == 0 && total > Acc(0)) T::store(p.work, v, total, wx, wy, wz);
     }
-    if (v >= 0 && glane == 0 && total > Acc(0)) T::store(p.work, v, total, wx, wy, wz);
 }
 
 // Number of positions c, c + nc, c + 2 nc, ... that lie below `bound`.
@@ -286,6 +344,8 @@ template <int MODE, int G, bool SMEM>
 __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
     using T = Traits<MODE>;
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double stage_all[512 / 32][4][32];  // per-warp staging of face terms (float64 modes)
+    double (*stage)[32] = stage_all[threadIdx.x >> 5];
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthreads = gridDim.x * blockDim.x;
     const int c = blockIdx.x;
@@ -365,7 +425,7 @@ __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
                         tri = p.slot_tri + s0;
                     }
                 }
-                update_vertex<MODE, G, SMEM>(p, v, tri, deg);
+                update_vertex<MODE, G, SMEM>(p, v, tri, deg, stage);
             }
             if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
         }

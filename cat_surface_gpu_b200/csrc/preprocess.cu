@@ -1,0 +1,500 @@
+// CAT_Surf2Sphere stages 1-5 (low_smooth, inflate, very_inflate, high_smooth,
+// ellipsoid) on sm_100a.
+//
+// Semantics follow the reference's description of the upstream stages
+// (src/cat_surface_gpu/surf2sphere.py:283-397, 474-862): per stage, keep the
+// input as the reference geometry, centre on the vertex mean, then per cycle
+// `iterations - 1` distance-smoothing passes, the inflation scale, the
+// distortion selection and `finger_iterations - 1` passes over the selected
+// vertices.  The passes are Gauss-Seidel in vertex index order -- the order
+// the upstream binary uses (the reference's Triton path colours instead) --
+// so they run as one persistent cooperative wavefront kernel per group of
+// passes, with the same schedule as the area-smoothing sweeps (vertex v of
+// pass s at step s * D + level(v); the 1-ring is the dependency set of both).
+// The per-stage global steps (centre, extents, face/vertex areas, the
+// distortion selection, the inflation) are plain kernels between them.
+//
+// Arithmetic: float32 positions, float64 arithmetic (one rounding per
+// operation, --fmad=false).  Sums over all vertices or faces are blocked:
+// sequential within runs of kBlockSum elements, then sequential over the
+// runs, so results do not depend on the launch shape.
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "errors.h"
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBlockSum = 256;
+constexpr int kThreads = 256;
+
+struct StageSpec {
+    int cycles;
+    double strength;
+    int iterations;
+    double inflation;
+    double threshold;
+    double finger_strength;
+    int finger_iterations;
+};
+
+// surf2sphere.py:758-814
+constexpr StageSpec kStages[5] = {
+    {1, 0.2, 50, 1.0, 3.0, 1.0, 0},  {2, 1.0, 30, 1.4, 3.0, 1.0, 30}, {4, 1.0, 30, 1.1, 3.0, 1.0, 0},
+    {6, 1.0, 60, 1.6, 3.0, 1.0, 60}, {6, 1.0, 50, 1.4, 4.0, 1.0, 60},
+};
+
+// Stage statistics kept on the device: mean[3], lo[3], hi[3], extent[3],
+// reference surface, current surface.
+struct Stats {
+    double mean[3];
+    double lo[3];
+    double hi[3];
+    double extent[3];
+    double ref_surface;
+    double cur_surface;
+};
+
+__device__ __forceinline__ float4 ld4(const float4* p, int v) { return __ldcg(p + v); }
+
+// ---------------------------------------------------------------- passes
+
+struct PassParams {
+    float4* work;
+    const int* nb_off;
+    const int* nb;
+    const unsigned char* selected;  // nullable: every vertex
+    const int* order;
+    const int* level_begin;
+    const int* level_end;
+    csg::Control* ctl;
+    int n;
+    int n_levels;
+    int stride;
+    int passes;
+    double strength;
+    unsigned long long timeout_ns;
+};
+
+// One vertex of one pass by a group of G lanes: lane j computes neighbour
+// slots j, j + G, ... (L1 distance d, d q when d > 0), the terms are staged in
+// shared memory and lanes 0..2 sum them in slot order (total and one
+// coordinate each) and form that coordinate; lane 0 stores.
+template <int G>
+__device__ __forceinline__ void smooth_vertex(const PassParams& p, int v, double (*stage)[32]) {
+    const int lane = threadIdx.x & 31;
+    const int glane = lane & (G - 1);
+    const int gbase = lane & ~(G - 1);
+    int b = 0, deg = 0;
+    bool active = v >= 0;
+    if (active) {
+        b = __ldg(p.nb_off + v);
+        deg = __ldg(p.nb_off + v + 1) - b;
+        active = deg > 1 && (!p.selected || p.selected[v]);
+    }
+    if (!active) deg = 0;
+    const int wdeg = __reduce_max_sync(kFull, deg);
+    double o[3] = {0.0, 0.0, 0.0};
+    if (active) {
+        const float4 q = ld4(p.work, v);
+        o[0] = q.x;
+        o[1] = q.y;
+        o[2] = q.z;
+    }
+    double total = 0.0, wsum = 0.0;
+    const int comp = glane < 3 ? glane : 0;
+    for (int c0 = 0; c0 < wdeg; c0 += G) {
+        const int j = c0 + glane;
+        double d = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
+        if (j < deg) {
+            const float4 q = ld4(p.work, __ldg(p.nb + b + j));
+            const double qx = q.x, qy = q.y, qz = q.z;
+            d = __dadd_rn(__dadd_rn(fabs(__dsub_rn(qx, o[0])), fabs(__dsub_rn(qy, o[1]))), fabs(__dsub_rn(qz, o[2])));
+            if (d > 0.0) {
+                dx = __dmul_rn(d, qx);
+                dy = __dmul_rn(d, qy);
+                dz = __dmul_rn(d, qz);
+            }
+        }
+        stage[0][lane] = d;
+        stage[1][lane] = dx;
+        stage[2][lane] = dy;
+        stage[3][lane] = dz;
+        __syncwarp();
+        if (glane < 3) {
+            const int m = min(G, deg - c0);
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                if (q < m) {
+                    total = __dadd_rn(total, stage[0][gbase + q]);
+                    // the reference adds d q only for d > 0; the staged term is 0 otherwise
+                    if (stage[0][gbase + q] > 0.0) wsum = __dadd_rn(wsum, stage[1 + comp][gbase + q]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    const double inv = 1.0 - p.strength;
+    float c = 0.0f;
+    if (active && glane < 3) {
+        const double keep = __dmul_rn(o[comp], inv);
+        c = __double2float_rn(total > 0.0 ? __dadd_rn(keep, __dmul_rn(__ddiv_rn(wsum, total), p.strength)) : keep);
+    }
+    const float cy = __shfl_sync(kFull, c, gbase + 1);
+    const float cz = __shfl_sync(kFull, c, gbase + 2);
+    if (active && glane == 0) __stcg(p.work + v, make_float4(c, cy, cz, 0.0f));
+}
+
+__device__ __forceinline__ int owned_below(int bound, int c, int nc) { return bound > c ? (bound - c + nc - 1) / nc : 0; }
+
+// `passes` Gauss-Seidel passes as one wavefront (see the file comment).
+template <int G>
+__global__ void __launch_bounds__(512) smooth_passes_kernel(PassParams p) {
+    __shared__ double stage_all[512 / 32][4][32];
+    double (*stage)[32] = stage_all[threadIdx.x >> 5];
+    const int c = blockIdx.x, nc = gridDim.x;
+    const int groups = blockDim.x / G;
+    const int warp_first_group = (threadIdx.x >> 5) * (32 / G);
+    const int my_group = (threadIdx.x & 31) / G;
+    const int L = p.n_levels, D = p.stride;
+    unsigned int phase = 0;
+    int barrier_id = 0;
+    const int span = (p.passes - 1) * D;  // host guarantees span + L < 2^31
+    const int nsteps = span + L;
+    int r = 0;
+    for (int t = 0; t < nsteps; ++t, r = (r + 1 == D) ? 0 : r + 1) {
+        int lo = t - span;
+        if (lo < r) lo = r;
+        const int hi = t < L ? t : (L - 1) - ((L - 1 - r) % D + D) % D;
+        if (hi >= lo) {
+            const int i0 = owned_below(__ldg(p.level_begin + lo), c, nc);
+            const int i1 = owned_below(__ldg(p.level_end + hi), c, nc);
+            for (int base = i0 + warp_first_group; base < i1; base += groups) {
+                const int i = base + my_group;
+                const int v = i < i1 ? __ldg(p.order + c + i * nc) : -1;
+                smooth_vertex<G>(p, v, stage);
+            }
+        }
+        if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    }
+}
+
+// ---------------------------------------------------------------- per-stage steps
+
+__global__ void k_pack(const float* __restrict__ points, float4* __restrict__ work, int n) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) work[v] = make_float4(points[3 * v], points[3 * v + 1], points[3 * v + 2], 0.0f);
+}
+
+__global__ void k_unpack(const float4* __restrict__ work, float* __restrict__ points, int n) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const float4 q = work[v];
+    points[3 * v] = q.x;
+    points[3 * v + 1] = q.y;
+    points[3 * v + 2] = q.z;
+}
+
+// ref = work; per run of kBlockSum vertices: coordinate sums, min, max.
+__global__ void k_stage_partials(const float4* __restrict__ work, float4* __restrict__ ref, int n,
+                                 double* __restrict__ partial) {
+    const int run = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = run * kBlockSum;
+    if (b >= n) return;
+    double sum[3] = {0, 0, 0}, lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int v = b; v < n && v < b + kBlockSum; ++v) {
+        const float4 q = work[v];
+        ref[v] = q;
+        const double x[3] = {q.x, q.y, q.z};
+        for (int k = 0; k < 3; ++k) {
+            sum[k] = __dadd_rn(sum[k], x[k]);
+            lo[k] = fmin(lo[k], x[k]);
+            hi[k] = fmax(hi[k], x[k]);
+        }
+    }
+    double* out = partial + 9LL * run;
+    for (int k = 0; k < 3; ++k) {
+        out[k] = sum[k];
+        out[3 + k] = lo[k];
+        out[6 + k] = hi[k];
+    }
+}
+
+__global__ void k_stage_stats(const double* __restrict__ partial, int runs, int n, Stats* __restrict__ st) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int k = 0; k < 3; ++k) {
+        double sum = 0.0, lo = INFINITY, hi = -INFINITY;
+        for (int r = 0; r < runs; ++r) {
+            sum = __dadd_rn(sum, partial[9LL * r + k]);
+            lo = fmin(lo, partial[9LL * r + 3 + k]);
+            hi = fmax(hi, partial[9LL * r + 6 + k]);
+        }
+        st->mean[k] = __ddiv_rn(sum, static_cast<double>(n));
+        st->lo[k] = lo;
+        st->hi[k] = hi;
+        const double ext = __dsub_rn(hi, lo);
+        st->extent[k] = ext < 1.0e-20 ? 1.0e-20 : ext;
+    }
+}
+
+__global__ void k_center(float4* __restrict__ work, int n, const Stats* __restrict__ st) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const float4 q = work[v];
+    work[v] = make_float4(__double2float_rn(__dsub_rn(q.x, st->mean[0])), __double2float_rn(__dsub_rn(q.y, st->mean[1])),
+                          __double2float_rn(__dsub_rn(q.z, st->mean[2])), 0.0f);
+}
+
+__global__ void k_face_areas(const float4* __restrict__ pos, const int* __restrict__ faces, int nf,
+                             double* __restrict__ area) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const float4 a = pos[faces[3 * f]], b = pos[faces[3 * f + 1]], c = pos[faces[3 * f + 2]];
+    const double e0x = __dsub_rn(b.x, a.x), e0y = __dsub_rn(b.y, a.y), e0z = __dsub_rn(b.z, a.z);
+    const double e1x = __dsub_rn(c.x, a.x), e1y = __dsub_rn(c.y, a.y), e1z = __dsub_rn(c.z, a.z);
+    const double cx = __dsub_rn(__dmul_rn(e0y, e1z), __dmul_rn(e0z, e1y));
+    const double cy = __dsub_rn(__dmul_rn(e0z, e1x), __dmul_rn(e0x, e1z));
+    const double cz = __dsub_rn(__dmul_rn(e0x, e1y), __dmul_rn(e0y, e1x));
+    double s = __dmul_rn(0.5, __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(cx, cx), __dmul_rn(cy, cy)), __dmul_rn(cz, cz))));
+    if (isnan(s)) s = 0.0;
+    area[f] = s;
+}
+
+__global__ void k_run_sums(const double* __restrict__ x, int n, double* __restrict__ partial) {
+    const int run = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = run * kBlockSum;
+    if (b >= n) return;
+    double s = 0.0;
+    for (int i = b; i < n && i < b + kBlockSum; ++i) s = __dadd_rn(s, x[i]);
+    partial[run] = s;
+}
+
+__global__ void k_finish_sum(const double* __restrict__ partial, int runs, double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0.0;
+    for (int r = 0; r < runs; ++r) s = __dadd_rn(s, partial[r]);
+    *out = s;
+}
+
+// Vertex areas: a third of each incident face, in (corner, face) order
+// (inc = face << 2 | corner, sorted by corner then face).
+__global__ void k_vertex_areas(const double* __restrict__ area, const int* __restrict__ inc_off,
+                               const int* __restrict__ inc, int n, double* __restrict__ va) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    double s = 0.0;
+    for (int k = inc_off[v]; k < inc_off[v + 1]; ++k) s = __dadd_rn(s, __ddiv_rn(area[inc[k] >> 2], 3.0));
+    va[v] = s;
+}
+
+__global__ void k_inflate(float4* __restrict__ work, int n, const Stats* __restrict__ st, double delta) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const float4 q = work[v];
+    const double x = __ddiv_rn(q.x, st->extent[0]), y = __ddiv_rn(q.y, st->extent[1]), z = __ddiv_rn(q.z, st->extent[2]);
+    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+    const double scale = __dadd_rn(1.0, __dmul_rn(delta, __dsub_rn(1.0, r)));
+    work[v] = make_float4(__double2float_rn(__dmul_rn(q.x, scale)), __double2float_rn(__dmul_rn(q.y, scale)),
+                          __double2float_rn(__dmul_rn(q.z, scale)), 0.0f);
+}
+
+__device__ __forceinline__ double dist3(const float4& a, const float4& b) {
+    const double x = __dsub_rn(b.x, a.x), y = __dsub_rn(b.y, a.y), z = __dsub_rn(b.z, a.z);
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+}
+
+// Distortion measure per vertex (surf2sphere.py:573-629).
+__global__ void k_distortion(const float4* __restrict__ work, const float4* __restrict__ ref,
+                             const int* __restrict__ nb_off, const int* __restrict__ nb,
+                             const double* __restrict__ va_cur, const double* __restrict__ va_ref, int n,
+                             const Stats* __restrict__ st, double* __restrict__ comp) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const float4 pv = work[v], rv = ref[v];
+    double max_linear = 0.0;
+    for (int k = nb_off[v]; k < nb_off[v + 1]; ++k) {
+        const int u = nb[k];
+        const double rd = dist3(rv, ref[u]);
+        const double ratio = rd > 0.0 ? __ddiv_rn(dist3(pv, work[u]), rd) : 0.0;
+        if (ratio > max_linear) max_linear = ratio;
+    }
+    double area_ratio;
+    if (va_cur[v] > 0.0) area_ratio = __ddiv_rn(va_ref[v], va_cur[v]);
+    else area_ratio = va_ref[v] != 0.0 ? 10000.0 : 1.0;
+    if (area_ratio < 1.0e-8) area_ratio = 1.0e-8;
+    const double ref_surface = st->ref_surface > 1.0e-30 ? st->ref_surface : 1.0e-30;
+    comp[v] = __dmul_rn(__dmul_rn(max_linear, area_ratio), __ddiv_rn(st->cur_surface, ref_surface));
+}
+
+__global__ void k_select(const double* __restrict__ comp, const int* __restrict__ nb_off, const int* __restrict__ nb,
+                         int n, double threshold, unsigned char* __restrict__ selected) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    double s = comp[v];
+    for (int k = nb_off[v]; k < nb_off[v + 1]; ++k) s = __dadd_rn(s, comp[nb[k]]);
+    selected[v] = __ddiv_rn(s, static_cast<double>(nb_off[v + 1] - nb_off[v] + 1)) > threshold;
+}
+
+// ---------------------------------------------------------------- host side
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+struct Layout {
+    size_t ctl, work, ref, area, va_ref, va_cur, comp, sel, partial, stats, total;
+};
+
+Layout layout(int n, int nf) {
+    Layout L{};
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        const size_t here = at;
+        at += align256(bytes);
+        return here;
+    };
+    const size_t runs = (static_cast<size_t>(n > nf ? n : nf) + kBlockSum - 1) / kBlockSum;
+    L.ctl = take(sizeof(csg::Control));
+    L.work = take(16ULL * n);
+    L.ref = take(16ULL * n);
+    L.area = take(8ULL * nf);
+    L.va_ref = take(8ULL * n);
+    L.va_cur = take(8ULL * n);
+    L.comp = take(8ULL * n);
+    L.sel = take(static_cast<size_t>(n));
+    L.partial = take(8ULL * 9 * runs);
+    L.stats = take(sizeof(Stats));
+    L.total = at;
+    return L;
+}
+
+template <int G>
+int launch_passes(const PassParams& params, int n_ctas, int threads, cudaStream_t s) {
+    auto kernel = smooth_passes_kernel<G>;
+    int device = 0, sms = 0, per_sm = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+    if (n_ctas <= 0) n_ctas = sms;
+    if (per_sm < 1 || n_ctas > per_sm * sms)
+        return csg::fail(CSG_ERR_LAUNCH, "preprocess passes: %d CTAs x %d threads cannot be co-resident", n_ctas, threads);
+    PassParams p = params;
+    void* args[] = {&p};
+    CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(n_ctas), dim3(threads), args,
+                                               0, s));
+    csg::note_launch();
+    return CSG_OK;
+}
+
+int run_passes(PassParams p, int passes, double strength, const unsigned char* selected, int n_ctas, int threads,
+               int lanes, cudaStream_t s) {
+    if (passes <= 0) return CSG_OK;
+    p.passes = passes;
+    p.strength = strength;
+    p.selected = selected;
+    switch (lanes) {
+        case 4: return launch_passes<4>(p, n_ctas, threads, s);
+        case 16: return launch_passes<16>(p, n_ctas, threads, s);
+        default: return launch_passes<8>(p, n_ctas, threads, s);
+    }
+}
+
+inline unsigned blocks(long long n, int threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
+
+}  // namespace
+
+extern "C" {
+
+size_t csg_preprocess_scratch_bytes(int n_vertices, int n_faces) {
+    if (n_vertices < 4 || n_faces < 4) return 0;
+    return layout(n_vertices, n_faces).total;
+}
+
+int csg_surf2sphere_preprocess(float* points, int n, const int32_t* faces, int nf, const int32_t* nb_off,
+                               const int32_t* nb, const int32_t* inc_off, const int32_t* inc, const int32_t* order,
+                               const int32_t* level_begin, const int32_t* level_end, int n_levels, int level_stride,
+                               int stop_at, void* scratch, size_t scratch_bytes, int n_ctas, int threads_per_cta,
+                               int lanes_per_vertex, double timeout_s, csg_stream_t stream) {
+    if (!points || n < 4 || !faces || nf < 4 || !nb_off || !nb || !inc_off || !inc || !order || !level_begin ||
+        !level_end || n_levels < 1 || level_stride < 1 || stop_at < 1 || stop_at > 5 || !scratch)
+        return csg::fail(CSG_ERR_ARG, "preprocess: bad arguments (stop_at 1..5)");
+    if (threads_per_cta <= 0) threads_per_cta = 512;
+    if (threads_per_cta % 32 || threads_per_cta > 512) return csg::fail(CSG_ERR_ARG, "preprocess: threads 32..512, x32");
+    if (lanes_per_vertex <= 0) lanes_per_vertex = 8;
+    if (lanes_per_vertex != 4 && lanes_per_vertex != 8 && lanes_per_vertex != 16)
+        return csg::fail(CSG_ERR_ARG, "preprocess: lanes_per_vertex must be 4, 8 or 16");
+    if (timeout_s <= 0.0) timeout_s = 2.0;
+    const Layout L = layout(n, nf);
+    if (scratch_bytes < L.total) return csg::fail(CSG_ERR_ARG, "preprocess: scratch too small");
+    const double factor = nf > 350000 ? static_cast<double>(nf) / 350000.0 : 1.0;
+    // every pass group's span (passes - 1) * stride + levels must stay below 2^31 steps
+    if (std::nearbyint(factor * 60.0) * static_cast<double>(level_stride) + n_levels >= 2147483647.0)
+        return csg::fail(CSG_ERR_ARG, "preprocess: schedule too long");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    char* base = static_cast<char*>(scratch);
+    auto* ctl = reinterpret_cast<csg::Control*>(base + L.ctl);
+    auto* work = reinterpret_cast<float4*>(base + L.work);
+    auto* ref = reinterpret_cast<float4*>(base + L.ref);
+    auto* area = reinterpret_cast<double*>(base + L.area);
+    auto* va_ref = reinterpret_cast<double*>(base + L.va_ref);
+    auto* va_cur = reinterpret_cast<double*>(base + L.va_cur);
+    auto* comp = reinterpret_cast<double*>(base + L.comp);
+    auto* sel = reinterpret_cast<unsigned char*>(base + L.sel);
+    auto* partial = reinterpret_cast<double*>(base + L.partial);
+    auto* st = reinterpret_cast<Stats*>(base + L.stats);
+    CSG_CUDA_CHECK(cudaMemsetAsync(ctl, 0, sizeof(csg::Control), s));
+    (csg::note_launch(), k_pack<<<blocks(n, kThreads), kThreads, 0, s>>>(points, work, n));
+    PassParams pp{};
+    pp.work = work;
+    pp.nb_off = nb_off;
+    pp.nb = nb;
+    pp.order = order;
+    pp.level_begin = level_begin;
+    pp.level_end = level_end;
+    pp.ctl = ctl;
+    pp.n = n;
+    pp.n_levels = n_levels;
+    pp.stride = level_stride;
+    pp.timeout_ns = static_cast<unsigned long long>(timeout_s * 1e9);
+    const int vruns = (n + kBlockSum - 1) / kBlockSum, fruns = (nf + kBlockSum - 1) / kBlockSum;
+    for (int si = 0; si < stop_at; ++si) {
+        const StageSpec spec = kStages[si];
+        const int iterations = static_cast<int>(std::nearbyint(factor * spec.iterations));
+        const int finger = static_cast<int>(std::nearbyint(factor * spec.finger_iterations));
+        (csg::note_launch(), k_stage_partials<<<blocks(vruns, kThreads), kThreads, 0, s>>>(work, ref, n, partial));
+        (csg::note_launch(), k_stage_stats<<<1, 32, 0, s>>>(partial, vruns, n, st));
+        (csg::note_launch(), k_center<<<blocks(n, kThreads), kThreads, 0, s>>>(work, n, st));
+        (csg::note_launch(), k_face_areas<<<blocks(nf, kThreads), kThreads, 0, s>>>(ref, faces, nf, area));
+        (csg::note_launch(), k_run_sums<<<blocks(fruns, kThreads), kThreads, 0, s>>>(area, nf, partial));
+        (csg::note_launch(), k_finish_sum<<<1, 32, 0, s>>>(partial, fruns, &st->ref_surface));
+        (csg::note_launch(), k_vertex_areas<<<blocks(n, kThreads), kThreads, 0, s>>>(area, inc_off, inc, n, va_ref));
+        const double delta = spec.inflation - 1.0;
+        for (int cycle = 0; cycle < spec.cycles; ++cycle) {
+            int rc = run_passes(pp, iterations - 1, spec.strength, nullptr, n_ctas, threads_per_cta, lanes_per_vertex, s);
+            if (rc) return rc;
+            (csg::note_launch(), k_inflate<<<blocks(n, kThreads), kThreads, 0, s>>>(work, n, st, delta));
+            if (finger > 0) {
+                (csg::note_launch(), k_face_areas<<<blocks(nf, kThreads), kThreads, 0, s>>>(work, faces, nf, area));
+                (csg::note_launch(), k_run_sums<<<blocks(fruns, kThreads), kThreads, 0, s>>>(area, nf, partial));
+                (csg::note_launch(), k_finish_sum<<<1, 32, 0, s>>>(partial, fruns, &st->cur_surface));
+                (csg::note_launch(), k_vertex_areas<<<blocks(n, kThreads), kThreads, 0, s>>>(area, inc_off, inc, n,
+                                                                                         va_cur));
+                (csg::note_launch(), k_distortion<<<blocks(n, kThreads), kThreads, 0, s>>>(work, ref, nb_off, nb, va_cur,
+                                                                                       va_ref, n, st, comp));
+                (csg::note_launch(), k_select<<<blocks(n, kThreads), kThreads, 0, s>>>(comp, nb_off, nb, n,
+                                                                                   spec.threshold, sel));
+                rc = run_passes(pp, finger - 1, spec.finger_strength, sel, n_ctas, threads_per_cta, lanes_per_vertex,
+                                s);
+                if (rc) return rc;
+            }
+        }
+    }
+    (csg::note_launch(), k_unpack<<<blocks(n, kThreads), kThreads, 0, s>>>(work, points, n));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+}  // extern "C"

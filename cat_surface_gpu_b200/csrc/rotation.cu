@@ -229,6 +229,113 @@ __global__ void k_rotation_finalize(const RotSurface* __restrict__ surfaces, int
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
+// ---------------------------------------------------- device grid build
+// Same cells as csg_rotation_grid_build (bounding box of each triangle in
+// cells of size 2 / G over [-1, 1]^3, +/- margin, clamped); counts by
+// atomics, a two-level scan, an atomic fill, then every cell's list sorted
+// ascending so the candidate order (and the first-minimum rule) is the
+// host builder's.
+
+constexpr int kScan = 1024;
+
+__device__ __forceinline__ void face_cells(const double* pts, const int* faces, int f, int G, int margin, int lo[3],
+                                           int hi[3]) {
+    const double cell = 2.0 / static_cast<double>(G);
+    const int v0 = faces[3 * f], v1 = faces[3 * f + 1], v2 = faces[3 * f + 2];
+    for (int k = 0; k < 3; ++k) {
+        const double a = pts[3 * v0 + k], b = pts[3 * v1 + k], c = pts[3 * v2 + k];
+        const double mn = fmin(fmin(a, b), c), mx = fmax(fmax(a, b), c);
+        const long long l = static_cast<long long>(floor((mn + 1.0) / cell)) - margin;
+        const long long h = static_cast<long long>(floor((mx + 1.0) / cell)) + margin;
+        lo[k] = static_cast<int>(l < 0 ? 0 : (l > G - 1 ? G - 1 : l));
+        hi[k] = static_cast<int>(h < 0 ? 0 : (h > G - 1 ? G - 1 : h));
+    }
+}
+
+__global__ void k_rgrid_count(const double* __restrict__ pts, const int* __restrict__ faces, int n_faces, int G,
+                              int margin, int* __restrict__ counts) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_faces) return;
+    int lo[3], hi[3];
+    face_cells(pts, faces, f, G, margin, lo, hi);
+    for (int z = lo[2]; z <= hi[2]; ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+            for (int x = lo[0]; x <= hi[0]; ++x)
+                atomicAdd(counts + x + static_cast<long long>(G) * (y + static_cast<long long>(G) * z) + 1, 1);
+}
+
+__global__ void k_rgrid_scan_block(int* __restrict__ data, int n, int* __restrict__ sums) {
+    __shared__ int buf[kScan];
+    const int i = blockIdx.x * kScan + threadIdx.x;
+    buf[threadIdx.x] = i < n ? data[i] : 0;
+    __syncthreads();
+    for (int off = 1; off < kScan; off <<= 1) {
+        const int v = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
+        __syncthreads();
+        buf[threadIdx.x] += v;
+        __syncthreads();
+    }
+    if (i < n) data[i] = buf[threadIdx.x];
+    if (threadIdx.x == kScan - 1) sums[blockIdx.x] = buf[threadIdx.x];
+}
+
+__global__ void k_rgrid_scan_sums(int* __restrict__ sums, int nblocks) {
+    __shared__ int buf[kScan];
+    int carry = 0;
+    for (int base = 0; base < nblocks; base += kScan) {
+        const int i = base + threadIdx.x;
+        const int own = i < nblocks ? sums[i] : 0;
+        buf[threadIdx.x] = own;
+        __syncthreads();
+        for (int off = 1; off < kScan; off <<= 1) {
+            const int v = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
+            __syncthreads();
+            buf[threadIdx.x] += v;
+            __syncthreads();
+        }
+        if (i < nblocks) sums[i] = carry + buf[threadIdx.x] - own;
+        const int total = buf[kScan - 1];
+        __syncthreads();
+        carry += total;
+    }
+}
+
+__global__ void k_rgrid_scan_add(int* __restrict__ data, int n, const int* __restrict__ sums, int* __restrict__ cursor) {
+    const int i = blockIdx.x * kScan + threadIdx.x;
+    if (i >= n) return;
+    const int v = data[i] + sums[blockIdx.x];
+    data[i] = v;
+    if (cursor && i + 1 < n) cursor[i] = v;
+}
+
+__global__ void k_rgrid_fill(const double* __restrict__ pts, const int* __restrict__ faces, int n_faces, int G,
+                             int margin, int* __restrict__ cursor, int* __restrict__ cell_faces) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_faces) return;
+    int lo[3], hi[3];
+    face_cells(pts, faces, f, G, margin, lo, hi);
+    for (int z = lo[2]; z <= hi[2]; ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+            for (int x = lo[0]; x <= hi[0]; ++x)
+                cell_faces[atomicAdd(cursor + x + static_cast<long long>(G) * (y + static_cast<long long>(G) * z), 1)] = f;
+}
+
+// Insertion sort of each cell's (short) face list.
+__global__ void k_rgrid_sort(const int* __restrict__ offsets, long long n_cells, int* __restrict__ cell_faces) {
+    const long long c = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    const int b = offsets[c], e = offsets[c + 1];
+    for (int i = b + 1; i < e; ++i) {
+        const int key = cell_faces[i];
+        int j = i - 1;
+        while (j >= b && cell_faces[j] > key) {
+            cell_faces[j + 1] = cell_faces[j];
+            --j;
+        }
+        cell_faces[j + 1] = key;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -353,6 +460,48 @@ int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces
         default: (csg::note_launch(), k_rotation_cost<256><<<blocks, 256, 0, st>>>(d_surf, n_surfaces, items, d_err)); break;
     }
     (csg::note_launch(), k_rotation_finalize<<<dim3((max_c + 127) / 128, n_surfaces), 128, 0, st>>>(d_surf, n_surfaces, costs, d_off));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+size_t csg_rotation_grid_scratch_bytes(int grid_size) {
+    if (grid_size < 4 || static_cast<long long>(grid_size) * grid_size * grid_size >= (1LL << 31)) return 0;
+    const long long cells = static_cast<long long>(grid_size) * grid_size * grid_size;
+    return align256(sizeof(int) * static_cast<size_t>(cells)) + align256(sizeof(int) * ((cells + 1) / kScan + 2));
+}
+
+int csg_rotation_grid_build_device(const double* points, int n_points, const int32_t* faces, int n_faces,
+                                   int grid_size, int margin, int32_t* offsets, int32_t* cell_faces,
+                                   long long capacity, long long* count, void* scratch, size_t scratch_bytes,
+                                   csg_stream_t stream) {
+    if (!points || !faces || n_points < 1 || n_faces < 1 || grid_size < 4 || margin < 0 || !offsets || !count ||
+        !scratch)
+        return csg::fail(CSG_ERR_ARG, "rotation grid (device): bad arguments (grid_size >= 4, margin >= 0)");
+    if (scratch_bytes < csg_rotation_grid_scratch_bytes(grid_size))
+        return csg::fail(CSG_ERR_ARG, "rotation grid (device): scratch too small");
+    const int G = grid_size;
+    const long long cells = static_cast<long long>(G) * G * G;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    char* base = static_cast<char*>(scratch);
+    int* cursor = reinterpret_cast<int*>(base);
+    int* sums = reinterpret_cast<int*>(base + align256(sizeof(int) * static_cast<size_t>(cells)));
+    CSG_CUDA_CHECK(cudaMemsetAsync(offsets, 0, sizeof(int32_t) * static_cast<size_t>(cells + 1), st));
+    const unsigned fb = static_cast<unsigned>((n_faces + 255) / 256);
+    (csg::note_launch(), k_rgrid_count<<<fb, 256, 0, st>>>(points, faces, n_faces, G, margin, offsets));
+    const int n = static_cast<int>(cells + 1);
+    const int nblocks = (n + kScan - 1) / kScan;
+    (csg::note_launch(), k_rgrid_scan_block<<<nblocks, kScan, 0, st>>>(offsets, n, sums));
+    (csg::note_launch(), k_rgrid_scan_sums<<<1, kScan, 0, st>>>(sums, nblocks));
+    (csg::note_launch(), k_rgrid_scan_add<<<nblocks, kScan, 0, st>>>(offsets, n, sums, cursor));
+    int total = 0;
+    CSG_CUDA_CHECK(cudaMemcpyAsync(&total, offsets + cells, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CSG_CUDA_CHECK(cudaStreamSynchronize(st));
+    *count = total;
+    if (!cell_faces) return CSG_OK;  // size query
+    if (capacity < total) return csg::fail(CSG_ERR_ARG, "rotation grid (device): capacity %lld < %d", capacity, total);
+    (csg::note_launch(), k_rgrid_fill<<<fb, 256, 0, st>>>(points, faces, n_faces, G, margin, cursor, cell_faces));
+    (csg::note_launch(), k_rgrid_sort<<<static_cast<unsigned>((cells + 255) / 256), 256, 0, st>>>(offsets, cells,
+                                                                                                 cell_faces));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }

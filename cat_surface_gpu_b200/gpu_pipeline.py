@@ -127,17 +127,18 @@ def rotate_vertices(vertices: np.ndarray, angles) -> np.ndarray:
 
 
 class _Stencils:
-    """Builds stencils with the native builder or a reference helper binary."""
+    """Builds stencils with the native builder (on the GPU) or a reference helper binary."""
 
-    def __init__(self, builder, threads: int, nx: int, ny: int, temp_dir: Path):
+    def __init__(self, builder, threads: int, nx: int, ny: int, temp_dir: Path, device=None):
         self.builder, self.threads, self.nx, self.ny, self.temp = builder, threads, nx, ny, temp_dir
+        self.device = device
         self.count = 0
 
     def build(self, sphere: GiftiMesh, surface_path: str | Path, *, normalize: bool,
               sphere_path: str | Path | None = None) -> SurfaceStencil:
         if self.builder in (None, "native"):
             return build_surface_stencil(sphere.vertices, sphere.faces, nx=self.nx, ny=self.ny, normalize=normalize,
-                                         threads=self.threads)
+                                         threads=self.threads, device=self.device)
         self.count += 1
         path = Path(sphere_path) if sphere_path is not None else self.temp / f"sphere-{self.count}.gii"
         if sphere_path is None:
@@ -299,8 +300,8 @@ def register_meshes(
 
     with tempfile.TemporaryDirectory(prefix="cat_surface_b200_") as temp_name:
         temp = Path(temp_name)
-        builder = _Stencils(stencil_builder, stencil_threads, nx, ny, temp)
-        rotated_builder = _Stencils(rotated_stencil_builder, stencil_threads, nx, ny, temp)
+        builder = _Stencils(stencil_builder, stencil_threads, nx, ny, temp, target_device)
+        rotated_builder = _Stencils(rotated_stencil_builder, stencil_threads, nx, ny, temp, target_device)
         start = time.perf_counter()
         with ThreadPoolExecutor(max_workers=2) as pool:
             src_future = None if source_stencil is not None else pool.submit(

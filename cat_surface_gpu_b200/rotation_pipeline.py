@@ -7,7 +7,6 @@ index once, then seed search and Nelder-Mead on the device).
 
 from __future__ import annotations
 
-from dataclasses import dataclass
 from pathlib import Path
 
 import numpy as np
@@ -58,22 +57,34 @@ def read_rotation_points(path) -> np.ndarray:
     return np.ascontiguousarray(points.reshape(n_points, 3))
 
 
-@dataclass
 class RotationPipeline:
-    """A reusable target index plus CAT-compatible rotation search (reference 70-164)."""
+    """A reusable target index plus CAT-compatible rotation search (reference 70-164).
 
-    index_cpu: RotationGridIndex
-    index: RotationGridIndexDevice
+    ``from_stencil`` builds the candidate grid on the GPU; ``index_cpu`` (the
+    host copy the reference also keeps) is then built on first access.
+    """
+
+    def __init__(self, index_cpu: RotationGridIndex | None, index: RotationGridIndexDevice, geometry=None):
+        self._index_cpu, self.index, self._geometry = index_cpu, index, geometry
+
+    @property
+    def index_cpu(self) -> RotationGridIndex:
+        if self._index_cpu is None:
+            points, faces, grid_size, margin = self._geometry
+            self._index_cpu = RotationGridIndex.from_geometry(points, faces, grid_size=grid_size, margin=margin,
+                                                              include_dense_candidate_table=False)
+        return self._index_cpu
 
     @classmethod
     def from_stencil(cls, target_stencil: SurfaceStencil, *, device="auto", grid_size: int = 128, margin: int = 1,
                      candidate_table_dtype: torch.dtype = torch.int32, geometry_dtype: torch.dtype = torch.float32,
                      compressed_candidate_table: bool = True) -> "RotationPipeline":
         target = resolve_device(device)
-        index_cpu = RotationGridIndex.from_stencil(target_stencil, grid_size=grid_size, margin=margin,
-                                                   include_dense_candidate_table=False)
-        index = index_cpu.to(target, geometry_dtype=geometry_dtype, candidate_table_dtype=candidate_table_dtype)
-        return cls(index_cpu=index_cpu, index=index)
+        if geometry_dtype != torch.float32:
+            raise ValueError("the native rotation cost evaluates geometry in float32")
+        index = RotationGridIndexDevice.build(target_stencil.sphere_points, target_stencil.faces, device=target,
+                                              grid_size=grid_size, margin=margin)
+        return cls(None, index, (target_stencil.sphere_points, target_stencil.faces, grid_size, margin))
 
     @classmethod
     def from_index_cpu(cls, index_cpu: RotationGridIndex, *, device="auto",

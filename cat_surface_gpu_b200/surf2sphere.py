@@ -384,13 +384,81 @@ def run_areal_smoothing_cuda(
     }
 
 
-def run_surf2sphere_preprocess_cuda(*args, **kwargs):
-    """GPU stages 1-5 are not part of this package; the upstream binary runs them."""
+def run_surf2sphere_preprocess_cuda(
+    vertices: np.ndarray,
+    faces: np.ndarray,
+    topology: Surf2SphereTopology,
+    *,
+    stop_at: int = 5,
+    desired_surface_area: float,
+    device: str | torch.device = "cuda",
+    dtype: str | torch.dtype = torch.float32,
+    schedule_block_size: int | None = 131072,
+    launch: dict | None = None,
+    timeout_s: float = 2.0,
+) -> tuple[np.ndarray, dict[str, float]]:
+    """CAT_Surf2Sphere stages 1..stop_at on the GPU (reference ``surf2sphere.py:716-862``).
 
-    raise NotImplementedError(
-        "Surf2Sphere stages 1-5 on the GPU are not implemented; use preprocess_kernel='cpu' "
-        "(the upstream CAT_Surf2Sphere binary), as the reference does by default"
-    )
+    Same contract as the reference: returns ``(float32 [N, 3], timings)``,
+    and for ``stop_at >= 5`` the ellipsoid-to-sphere conversion to
+    ``desired_surface_area`` is applied.  The distance-smoothing passes run
+    in the upstream binary's vertex order (``csg_surf2sphere_preprocess``);
+    ``schedule_block_size`` (the reference's colour-group blocking) has no
+    meaning for that order and is accepted for compatibility.  Positions are
+    float32 with float64 arithmetic; ``dtype=float64`` is not offered.
+    """
+
+    try:
+        target = resolve_device(device)
+    except DeviceUnavailable as exc:
+        raise RuntimeError(f"CAT_Surf2Sphere CUDA backend: {exc}") from exc
+    if _resolve_dtype(dtype) != torch.float32:
+        raise ValueError("the GPU preprocess keeps float32 positions (float64 arithmetic)")
+    if stop_at < 1 or stop_at > 5:
+        raise ValueError("CUDA preprocessing stop_at must be between 1 and 5")
+    points_host = np.ascontiguousarray(np.asarray(vertices, dtype=np.float32))
+    tri = np.ascontiguousarray(faces, dtype=np.int32)
+    if points_host.ndim != 2 or points_host.shape[1] != 3 or tri.ndim != 2 or tri.shape[1] != 3:
+        raise ValueError("vertices and faces must have shape [n, 3] and [m, 3]")
+    n, nf = points_host.shape[0], tri.shape[0]
+    plan = topology.plan
+    if plan is None or plan.slot_off.shape[0] != n + 1:
+        plan = SweepPlan.build(tri, n)
+    from .features import _topology
+
+    cfg = {"n_ctas": 0, "threads_per_cta": 512, "lanes_per_vertex": 8}
+    if launch:
+        cfg.update(launch)
+    lib = _native.library()
+    timings: dict[str, float] = {}
+    with torch.no_grad(), torch.cuda.device(target):
+        start = time.perf_counter()
+        points = torch.from_numpy(points_host).to(target)
+        face_dev = torch.from_numpy(tri).to(target)
+        nb_off, nb, inc_off, inc, _ = _topology(tri, n, target)
+        plan_device = plan.to_device(target)
+        scratch = torch.empty(int(lib.csg_preprocess_scratch_bytes(n, nf)), dtype=torch.uint8, device=target)
+        torch.cuda.synchronize(target)
+        timings["preprocess_upload_seconds"] = time.perf_counter() - start
+        start = time.perf_counter()
+        _native.check(lib.csg_surf2sphere_preprocess(
+            _native.ptr(points), n, _native.ptr(face_dev), nf, _native.ptr(nb_off), _native.ptr(nb),
+            _native.ptr(inc_off), _native.ptr(inc), _native.ptr(plan_device["order"]),
+            _native.ptr(plan_device["level_begin"]), _native.ptr(plan_device["level_end"]), plan.n_levels,
+            plan.level_stride, int(stop_at), _native.ptr(scratch), scratch.numel(), int(cfg["n_ctas"]),
+            int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s), _native.stream_handle()),
+            "csg_surf2sphere_preprocess")
+        status, where = read_status(scratch)
+        if status != 0:
+            raise RuntimeError(f"CAT_Surf2Sphere preprocess kernel failed (status {status} at barrier {where})")
+        timings["preprocess_kernel_seconds"] = time.perf_counter() - start
+        result = points.cpu().numpy()
+    if stop_at >= 5:
+        start = time.perf_counter()
+        result = convert_ellipsoid_to_sphere_with_surface_area(result, desired_surface_area)
+        timings["ellipsoid_to_sphere_seconds"] = time.perf_counter() - start
+    timings["preprocess_total_seconds"] = sum(timings.values())
+    return np.ascontiguousarray(result, dtype=np.float32), timings
 
 
 def _run_reference(reference_cli: Path, input_path: Path, output_path: Path, stop_at: int) -> None:
@@ -408,7 +476,7 @@ def run_cat_surf2sphere_gpu(
     input_surface: str | Path,
     output_surface: str | Path,
     *,
-    reference_cli: str | Path,
+    reference_cli: str | Path | None = None,
     stop_at: int = 10,
     device: str | torch.device = "cuda",
     dtype: str | torch.dtype = torch.float32,
@@ -419,19 +487,52 @@ def run_cat_surf2sphere_gpu(
     areal_arithmetic: str = "cat",
     areal_block_size: int | None = None,
 ) -> CatSurf2SphereGpuResult:
-    """Upstream stages 1-5 on the CPU binary, sweeps on the GPU (reference 1107-1295)."""
+    """CAT_Surf2Sphere with the sweeps on the GPU (reference 1107-1295).
+
+    ``preprocess_kernel="cpu"`` (the reference's default) runs stages 1-5 on
+    the upstream binary ``reference_cli``; ``"triton"`` (the reference's name
+    for its GPU preprocess) runs them with the native kernels instead, so the
+    whole conversion stays on the GPU and no binary is needed.
+    """
 
     if stop_at < 1:
         raise ValueError("stop_at must be at least 1")
     if preprocess_kernel not in ("cpu", "triton"):
         raise ValueError(f"Unsupported CAT_Surf2Sphere preprocess kernel: {preprocess_kernel}")
-    if preprocess_kernel != "cpu":
-        run_surf2sphere_preprocess_cuda()
     input_path = Path(input_surface)
     output_path = Path(output_surface)
-    reference_path = Path(reference_cli)
+    reference_path = Path(reference_cli) if reference_cli is not None else None
     timings: dict[str, float] = {}
     total_start = time.perf_counter()
+    if preprocess_kernel != "cpu":
+        # every stage on the GPU (reference 1135-1213 with the native preprocess)
+        input_mesh = read_gifti_mesh(input_path)
+        topology_start = time.perf_counter()
+        topology = Surf2SphereTopology.from_mesh(input_mesh)
+        timings["topology_build_seconds"] = time.perf_counter() - topology_start
+        area = surface_area(input_mesh)
+        pre, pre_timings = run_surf2sphere_preprocess_cuda(
+            input_mesh.vertices, input_mesh.faces, topology, stop_at=min(stop_at, 5), desired_surface_area=area,
+            device=device, dtype=dtype, schedule_block_size=preprocess_block_size)
+        timings.update(pre_timings)
+        if stop_at > 5:
+            radius = float(np.sqrt(np.max(np.sum(pre.astype(np.float64) ** 2, axis=1))))
+            smoothed, smooth_timings = run_areal_smoothing_cuda(
+                pre, input_mesh.faces, topology, iterations=1000 * (stop_at - 5), project_every=1000, radius=radius,
+                device=device, dtype=dtype, kernel=kernel, schedule=areal_schedule, arithmetic=areal_arithmetic,
+                schedule_block_size=areal_block_size)
+            timings.update(smooth_timings)
+            conversion_start = time.perf_counter()
+            pre = convert_ellipsoid_to_sphere_with_surface_area(smoothed, area)
+            timings["ellipsoid_to_sphere_seconds"] = time.perf_counter() - conversion_start
+        write_start = time.perf_counter()
+        write_vertices_like(input_path, output_path, pre)
+        timings["output_write_seconds"] = time.perf_counter() - write_start
+        result_mesh = read_gifti_mesh(output_path)
+        timings["total_seconds"] = time.perf_counter() - total_start
+        return CatSurf2SphereGpuResult(result_mesh.vertices, result_mesh.faces, timings, output_path)
+    if reference_path is None:
+        raise ValueError("preprocess_kernel='cpu' runs stages 1-5 on the upstream binary: give reference_cli")
     if stop_at <= 5:
         start = time.perf_counter()
         _run_reference(reference_path, input_path, output_path, stop_at)

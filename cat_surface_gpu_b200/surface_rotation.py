@@ -218,6 +218,45 @@ class RotationGridIndexDevice:
     def device(self) -> torch.device:
         return self.target_points.device
 
+    @classmethod
+    def build(cls, points, faces, *, device, grid_size: int = 128, margin: int = 1) -> "RotationGridIndexDevice":
+        """Build the candidate grid directly on a CUDA device (``csg_rotation_grid_build_device``).
+
+        Same CSR (cells, face order) as ``RotationGridIndex.from_geometry(...).to(device)``.
+        """
+
+        target = resolve_device(device)
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        tri = np.ascontiguousarray(faces, dtype=np.int32)
+        if pts.ndim != 2 or pts.shape[1] != 3 or tri.ndim != 2 or tri.shape[1] != 3:
+            raise ValueError("points and faces must have shape [n, 3] and [m, 3]")
+        if grid_size < 4 or margin < 0:
+            raise ValueError("grid_size must be at least 4 and margin must be non-negative")
+        if tri.min(initial=0) < 0 or tri.max(initial=0) >= pts.shape[0]:
+            raise ValueError("faces reference a missing point")
+        lib = _native.library()
+        d_pts = torch.as_tensor(pts, device=target)
+        d_faces = torch.as_tensor(tri, device=target)
+        offsets = torch.empty(grid_size ** 3 + 1, dtype=torch.int32, device=target)
+        scratch = torch.empty(int(lib.csg_rotation_grid_scratch_bytes(grid_size)), dtype=torch.uint8, device=target)
+        count = ctypes.c_longlong(0)
+        stream = _native.stream_handle()
+        args = (d_pts.data_ptr(), pts.shape[0], d_faces.data_ptr(), tri.shape[0], grid_size, margin,
+                offsets.data_ptr())
+        _native.check(lib.csg_rotation_grid_build_device(*args, None, 0, ctypes.addressof(count), scratch.data_ptr(),
+                                                         scratch.numel(), stream), "csg_rotation_grid_build_device")
+        if count.value == 0:
+            raise ValueError("At least one triangle does not cover any spatial grid cell")
+        flat = torch.empty(count.value, dtype=torch.int32, device=target)
+        _native.check(lib.csg_rotation_grid_build_device(*args, flat.data_ptr(), count.value, ctypes.addressof(count),
+                                                         scratch.data_ptr(), scratch.numel(), stream),
+                      "csg_rotation_grid_build_device")
+        triangles = pts[tri.astype(np.int64)].astype(np.float32)
+        return cls(target_points=d_pts.to(torch.float32).contiguous(), target_faces=d_faces,
+                   target_triangles=torch.as_tensor(triangles, device=target).contiguous(),
+                   candidate_table=torch.empty(0, dtype=torch.int32, device=target), grid_size=int(grid_size),
+                   candidate_offsets=offsets, candidate_faces=flat)
+
     def _rotation_matrices(self, angles) -> torch.Tensor:
         a = torch.as_tensor(angles, dtype=torch.float64).detach().cpu().numpy()
         if a.ndim == 1:

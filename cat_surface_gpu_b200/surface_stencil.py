@@ -188,13 +188,16 @@ def resampling_sphere(subdivisions: int = 6) -> tuple[np.ndarray, np.ndarray]:
 
 
 def build_surface_stencil(sphere_vertices, sphere_faces, *, nx: int = 512, ny: int = 256, normalize: bool = True,
-                          subdivisions: int = 6, threads: int = 0) -> SurfaceStencil:
-    """Build a resampling stencil for a sphere mesh (native host builder, ``csg_stencil_build``).
+                          subdivisions: int = 6, threads: int = 0, device=None) -> SurfaceStencil:
+    """Build a resampling stencil for a sphere mesh.
 
     Same contents as the reference's stencil helper (``--surface`` mode: the
     surface shares the sphere's topology, so surface indices are sphere
     vertex ids).  ``normalize=False`` matches the helper's
     ``--no-normalize`` (for spheres that are already unit and centred).
+    With a CUDA ``device`` the closest-point queries run on that GPU
+    (``csg_stencil_build_device``); otherwise the threaded host builder
+    (``csg_stencil_build``).  Both give bit-identical stencils.
     """
 
     from . import _native
@@ -211,15 +214,23 @@ def build_surface_stencil(sphere_vertices, sphere_faces, *, nx: int = 512, ny: i
     sheet_indices = np.zeros((ny, nx, 3), dtype=np.int32)
     sheet_weights = np.zeros((ny, nx, 3), dtype=np.float64)
     unit = np.zeros(sphere.shape, dtype=np.float32)
-    _native.check(
-        _native.library().csg_stencil_build(
-            sphere.ctypes.data, sphere.shape[0], faces.ctypes.data, faces.shape[0], rpts.ctypes.data, n,
-            rfaces.ctypes.data, rfaces.shape[0], int(nx), int(ny), int(bool(normalize)), int(threads),
-            sphere_points.ctypes.data, surface_indices.ctypes.data, surface_weights.ctypes.data,
-            sheet_indices.ctypes.data, sheet_weights.ctypes.data, unit.ctypes.data,
-        ),
-        "csg_stencil_build",
-    )
+    lib = _native.library()
+    outputs = (sphere_points.ctypes.data, surface_indices.ctypes.data, surface_weights.ctypes.data,
+               sheet_indices.ctypes.data, sheet_weights.ctypes.data, unit.ctypes.data)
+    inputs = (sphere.ctypes.data, sphere.shape[0], faces.ctypes.data, faces.shape[0], rpts.ctypes.data, n,
+              rfaces.ctypes.data, rfaces.shape[0], int(nx), int(ny), int(bool(normalize)))
+    target = None if device is None else torch.device(device)
+    if target is not None and target.type == "cuda":
+        need = int(lib.csg_stencil_scratch_bytes(sphere.shape[0], faces.shape[0], n, rfaces.shape[0], int(nx),
+                                                 int(ny)))
+        if need == 0:
+            raise ValueError("stencil build: bad sizes")
+        with torch.cuda.device(target):
+            scratch = torch.empty(need, dtype=torch.uint8, device=target)
+            _native.check(lib.csg_stencil_build_device(*inputs, *outputs, scratch.data_ptr(), need,
+                                                       _native.stream_handle()), "csg_stencil_build_device")
+    else:
+        _native.check(lib.csg_stencil_build(*inputs, int(threads), *outputs), "csg_stencil_build")
     return SurfaceStencil(sphere_points=sphere_points, faces=rfaces.copy(), surface_indices=surface_indices,
                           surface_weights=surface_weights, sheet_indices=sheet_indices, sheet_weights=sheet_weights,
                           nx=int(nx), ny=int(ny), source_points=int(sphere.shape[0]), unit_sphere_points=unit)

@@ -152,6 +152,26 @@ CSG_API int csg_areal_sweeps_noalloc(void *points, int n_vertices, const int32_t
  * without faulting or hanging the GPU; the context stays usable. */
 CSG_API int csg_selftest_barrier_timeout(void *scratch, size_t scratch_bytes, double timeout_s, csg_stream_t stream);
 
+/* Surf2Sphere stages 1-5 (low_smooth, inflate, very_inflate, high_smooth,
+ * ellipsoid) in place on float32 points [n][3] (device), stages 1..stop_at.
+ * Replaces run_surf2sphere_preprocess_cuda
+ * (src/cat_surface_gpu/surf2sphere.py:716-862) without the final
+ * ellipsoid-to-sphere conversion (host).  Distance-smoothing passes run in
+ * vertex-index Gauss-Seidel order (the upstream binary's) as persistent
+ * wavefront launches over the sweep schedule (order, level ranges, stride of
+ * csg_areal_plan_build); nb_off/nb: unique ascending 1-ring; inc_off/inc:
+ * per-vertex incidences face << 2 | corner sorted by (corner, face).
+ * Float32 storage, float64 arithmetic.  Waits are bounded by timeout_s
+ * (status CSG_ERR_TIMEOUT in the scratch's control block, read with
+ * csg_read_status). */
+CSG_API size_t csg_preprocess_scratch_bytes(int n_vertices, int n_faces);
+CSG_API int csg_surf2sphere_preprocess(float *points, int n, const int32_t *faces, int n_faces,
+                                       const int32_t *nb_off, const int32_t *nb, const int32_t *inc_off,
+                                       const int32_t *inc, const int32_t *order, const int32_t *level_begin,
+                                       const int32_t *level_end, int n_levels, int level_stride, int stop_at,
+                                       void *scratch, size_t scratch_bytes, int n_ctas, int threads_per_cta,
+                                       int lanes_per_vertex, double timeout_s, csg_stream_t stream);
+
 /* ------------------------------------------------------------------------
  * SurfWarp: 2-D DARTEL on the lat-lon sheet (device, batched).
  * Fields are [batch][channels][ny][nx] of dtype CSG_DTYPE_F32 / _F64; maps
@@ -293,6 +313,18 @@ CSG_API int csg_rotation_grid_build(const double *points, int n_points, const in
                                     int grid_size, int margin, int32_t *offsets, int32_t *cell_faces,
                                     long long capacity, long long *count);
 
+/* The same grid built on the device (device points, faces, offsets and
+ * cell_faces; scratch of csg_rotation_grid_scratch_bytes()): counts, scan,
+ * fill and a per-cell sort, so every cell lists its faces in ascending order
+ * exactly as csg_rotation_grid_build does.  *count is read back (the call
+ * synchronises `stream`); with cell_faces NULL only offsets and *count are
+ * produced. */
+CSG_API size_t csg_rotation_grid_scratch_bytes(int grid_size);
+CSG_API int csg_rotation_grid_build_device(const double *points, int n_points, const int32_t *faces, int n_faces,
+                                           int grid_size, int margin, int32_t *offsets, int32_t *cell_faces,
+                                           long long capacity, long long *count, void *scratch, size_t scratch_bytes,
+                                           csg_stream_t stream);
+
 /* One surface of a batched cost evaluation (all device pointers).  With
  * n_features F > 1 the cost sums the squared differences of all F features
  * (feature-major: src_values [F][n_src], tgt_values [F][n_tgt_points]);
@@ -403,6 +435,22 @@ CSG_API int csg_stencil_build(const float *sphere, int n_sphere, const int32_t *
                               int n_faces, int nx, int ny, int normalize, int threads, double *sphere_points_out,
                               int32_t *surface_indices_out, double *surface_weights_out, int32_t *sheet_indices_out,
                               double *sheet_weights_out, float *unit_points_out);
+
+/* The same stencil built on the device (closest-point queries, grids and
+ * scans on the GPU; the input preparation and sheet directions on the host),
+ * bit-identical to csg_stencil_build.  Inputs and outputs are host arrays;
+ * scratch is device memory of csg_stencil_scratch_bytes(); the call
+ * synchronises `stream`.  CSG_ERR_UNSUPPORTED when a grid cell list would
+ * exceed its capacity (triangles far larger than the grid cells), which the
+ * host builder handles. */
+CSG_API size_t csg_stencil_scratch_bytes(int n_sphere, int n_sphere_faces, int n_points, int n_faces, int nx, int ny);
+CSG_API int csg_stencil_build_device(const float *sphere, int n_sphere, const int32_t *sphere_faces,
+                                     int n_sphere_faces, const double *resampling_points, int n_points,
+                                     const int32_t *resampling_faces, int n_faces, int nx, int ny, int normalize,
+                                     double *sphere_points_out, int32_t *surface_indices_out,
+                                     double *surface_weights_out, int32_t *sheet_indices_out,
+                                     double *sheet_weights_out, float *unit_points_out, void *scratch,
+                                     size_t scratch_bytes, csg_stream_t stream);
 
 /* Synchronously read a persistent kernel's status word from its scratch. */
 CSG_API int csg_read_status(const void *scratch, csg_stream_t stream, int *status, int *where);

@@ -157,6 +157,24 @@ def test_two_features_and_quaternion_candidates(native_library):
 
 
 @pytest.mark.gpu
+def test_device_grid_build_equals_host_build(native_library):
+    """The GPU candidate grid has the host builder's cells and per-cell face order."""
+
+    from cat_surface_gpu_b200.surface_rotation import RotationGridIndex, RotationGridIndexDevice
+    from cat_surface_gpu_b200.surface_stencil import resampling_sphere
+
+    rng = np.random.default_rng(5)
+    points, faces = resampling_sphere(6)
+    points = points + rng.normal(scale=1e-3, size=points.shape)
+    for grid_size, margin in ((128, 1), (37, 0), (16, 3)):
+        host = RotationGridIndex.from_geometry(points, faces, grid_size=grid_size, margin=margin,
+                                               include_dense_candidate_table=False)
+        dev = RotationGridIndexDevice.build(points, faces, device="cuda", grid_size=grid_size, margin=margin)
+        np.testing.assert_array_equal(dev.candidate_offsets.cpu().numpy(), host.candidate_offsets)
+        np.testing.assert_array_equal(dev.candidate_faces.cpu().numpy(), host.candidate_faces)
+
+
+@pytest.mark.gpu
 def test_tetrahedron_known_answers(native_library):
     """Reference test_surface_rotation.py:37-62 and 149-202: identity cost 0, first-minimum rules."""
 

@@ -65,3 +65,34 @@ def test_surfwarp_chain_matches_reference(native_library, chain, tmp_path):
     print(f"chain vertex error: max {error.max():.3e} mean {error.mean():.3e} p99 {np.quantile(error, 0.99):.3e}")
     assert error.max() <= 1e-3
     assert (tmp_path / "out.gii").exists()
+
+
+@pytest.mark.parametrize("normalize,size", [(True, (64, 32)), (False, (256, 128))])
+def test_device_stencil_builder_equals_host_builder(native_library, chain, normalize, size):
+    """The GPU stencil builder reproduces the host builder bit for bit."""
+
+    from cat_surface_gpu_b200.gpu_pipeline import normalise_sphere
+    from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+    nx, ny = size
+    sphere = chain["target_sphere"] if normalize else normalise_sphere(chain["source_sphere"])
+    host = build_surface_stencil(sphere, chain["faces"], nx=nx, ny=ny, normalize=normalize, threads=4)
+    dev = build_surface_stencil(sphere, chain["faces"], nx=nx, ny=ny, normalize=normalize, device="cuda:0")
+    for name in ("sphere_points", "surface_indices", "surface_weights", "sheet_indices", "sheet_weights",
+                 "unit_sphere_points"):
+        np.testing.assert_array_equal(getattr(dev, name), getattr(host, name), err_msg=name)
+
+
+def test_device_stencil_builder_on_hemisphere_mesh(native_library):
+    """61,442-vertex hull sphere (the benchmark's target): device == host."""
+
+    from conftest import GOLDEN
+    from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+    c3 = np.load(GOLDEN / "surf2sphere_c3.npz")
+    faces = c3["faces"].astype(np.int32)
+    host = build_surface_stencil(c3["final"], faces, nx=256, ny=128, threads=8)
+    dev = build_surface_stencil(c3["final"], faces, nx=256, ny=128, device="cuda:0")
+    for name in ("sphere_points", "surface_indices", "surface_weights", "sheet_indices", "sheet_weights",
+                 "unit_sphere_points"):
+        np.testing.assert_array_equal(getattr(dev, name), getattr(host, name), err_msg=name)
