@@ -1,25 +1,28 @@
 #!/usr/bin/env python3
 """Benchmark of the CAT-Surface hot path on B200: one hemisphere of Surf2Sphere + SurfWarp.
 
-Step (one hemisphere; ``value``, seconds per hemisphere): CAT_Surf2Sphere's
-4,999 ordered area-smoothing sweeps (projection every 1,000) of the
-61,442-vertex / 122,880-face folded Fibonacci hull (the stage 1-5 output of
-the upstream binary, ``tests/golden/surf2sphere_c2.npz``), the
-ellipsoid-to-sphere step, then CAT_SurfWarp of that surface and sphere to a
-second, differently seeded 61,442-vertex hull (``surf2sphere_c3.npz``, with
-the binary's sphere): native stencils, type-5 curvature rotation features,
-46-seed + Nelder-Mead rotation search, two runs of two DARTEL steps on a
-256 x 128 sheet in float64 (the reference's default; a float32 DARTEL exceeds
-the 1e-3 vertex bound, its error and time are reported beside), the ``-avg``
-pole solve and the blend.  Inputs are
-synthetic and seeded.  The sweep input is resident in HBM when the step
-starts; SurfWarp's mesh inputs are host arrays (its stencil builder is host
-code).  Timed with CUDA events on the launching stream around the whole
-step, L2 flushed by a 256 MiB device write before every step, max over ranks.
+Step (one hemisphere; ``value``, seconds per hemisphere): CAT_Surf2Sphere of
+the 61,442-vertex / 122,880-face folded Fibonacci hull
+(``tests/golden/surf2sphere_c2.npz``) -- stages 1-5 (smoothing, inflation,
+finger smoothing), the ellipsoid-to-sphere step, 4,999 ordered
+area-smoothing sweeps (projection every 1,000) and the final sphere scaling,
+all on the GPU -- then CAT_SurfWarp of that surface and sphere to a second,
+differently seeded 61,442-vertex hull (``surf2sphere_c3.npz``, with the
+upstream binary's sphere): native stencils, type-5 curvature rotation
+features, 46-seed + Nelder-Mead rotation search, two runs of two DARTEL steps
+on a 256 x 128 sheet in float64 (the reference's default; a float32 DARTEL
+exceeds the 1e-3 vertex bound, its error and time are reported beside), the
+``-avg`` pole solve and the blend.  Inputs are synthetic and seeded.  The
+input surface is resident in HBM when the step starts; the ellipsoid steps
+and SurfWarp's mesh inputs use host arrays (the reference computes them on
+the host too).  Timed with CUDA events on the launching stream around the
+whole step, L2 flushed by a 256 MiB device write before every step, max over
+ranks.
 
-``e2e``: the same hemisphere through the public API with host buffers and
-files -- ``run_areal_smoothing_cuda`` on NumPy input, the sphere written as
-GIFTI, ``run_cat_surface_gpu_pipeline`` on the four GIFTI files.
+``e2e``: the same hemisphere through the public API with files --
+``run_cat_surf2sphere_gpu`` (every stage on the GPU) from the surface GIFTI to
+the sphere GIFTI, then ``run_cat_surface_gpu_pipeline`` on the four GIFTI
+files.
 
 Also on the line: ``batched_rotation`` (8 surfaces of 40,962-163,842 points
 x 4,096 uniform quaternions x 2 features in one persistent launch vs one
@@ -56,7 +59,7 @@ GOLDEN = ROOT / "tests" / "golden"
 
 METRIC = "s/hemisphere Surf2Sphere+SurfWarp @ max vtx err≤1e-3; batched regs/s vs plain"
 UNIT = "s/hemisphere"
-WORKLOAD = ("Surf2Sphere (4,999 ordered sweeps, 61,442 v / 122,880 f folded hull) + SurfWarp steps=2 runs=2 -avg "
+WORKLOAD = ("Surf2Sphere (stages 1-5 + 4,999 ordered sweeps, 61,442 v / 122,880 f folded hull) + SurfWarp steps=2 runs=2 -avg "
             "to a second 61,442-v hull, 256x128 float64 DARTEL sheet")
 SWEEPS = 4999
 SHEET = (256, 128)
@@ -185,6 +188,11 @@ def cpu_hemisphere_sample(meshes) -> dict:
     from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
 
     out = {}
+    from oracle import preprocess as opre
+
+    start = time.perf_counter()
+    opre.preprocess(meshes["surface"], meshes["faces"], 5)
+    out["stages_1_5"] = time.perf_counter() - start
     sweeps = 200
     start = time.perf_counter()
     oa.areal_sweeps(meshes["prefix"], meshes["faces"], iterations=sweeps + 1, project_every=1000,
@@ -218,7 +226,7 @@ def cpu_hemisphere_sample(meshes) -> dict:
     return out
 
 
-CPU_SAMPLE = ("200 of 4,999 sweeps (C port, 1 thread); 2 dartel_steps (k=0, 5) of the "
+CPU_SAMPLE = ("stages 1-5 in full and 200 of 4,999 sweeps (C port, 1 thread); 2 dartel_steps (k=0, 5) of the "
               f"{DARTEL_STEPS} per hemisphere (NumPy port); 1 stencil build of 6; 1 type-5 curvature sheet pair of "
               f"{FEATURE_SIDES}; 2 rotation candidates of the reference search's count; each scaled linearly")
 
@@ -257,20 +265,25 @@ class Hemisphere:
         import torch
 
         from cat_surface_gpu_b200 import surf2sphere
+        from cat_surface_gpu_b200.features import _topology
         from cat_surface_gpu_b200.gifti import GiftiMesh
 
         self.meshes, self.device, self.dartel_dtype = meshes, device, dartel_dtype
-        self.topology = surf2sphere.Surf2SphereTopology.from_mesh(GiftiMesh(meshes["prefix"], meshes["faces"]))
+        faces = meshes["faces"]
+        self.topology = surf2sphere.Surf2SphereTopology.from_mesh(GiftiMesh(meshes["surface"], faces))
         self.plan = self.topology.plan
         self.plan_device = self.plan.to_device(device)
-        self.pristine = torch.from_numpy(meshes["prefix"]).to(device)
+        self.faces_device = torch.from_numpy(faces).to(device)
+        self.rings = _topology(faces, meshes["surface"].shape[0], device)[:4]
+        self.pristine = torch.from_numpy(meshes["surface"]).to(device)
         self.points = torch.empty_like(self.pristine)
-        self.radius = projection_radius(meshes["prefix"])
-        self.launch = surf2sphere.tuned_areal_launch(self.pristine, self.plan_device, self.plan, arithmetic="cat",
-                                                     radius=self.radius) if autotune_launch else dict(
-            surf2sphere.DEFAULT_LAUNCH)
+        prefix_radius = projection_radius(meshes["prefix"])
+        self.launch = surf2sphere.tuned_areal_launch(torch.from_numpy(meshes["prefix"]).to(device), self.plan_device,
+                                                     self.plan, arithmetic="cat", radius=prefix_radius) \
+            if autotune_launch else dict(surf2sphere.DEFAULT_LAUNCH)
         self.scratch = None
-        self.meshes_in = (GiftiMesh(meshes["surface"], meshes["faces"]),
+        self.pre_scratch = None
+        self.meshes_in = (GiftiMesh(meshes["surface"], faces),
                           GiftiMesh(meshes["target_surface"], meshes["target_faces"]),
                           GiftiMesh(meshes["target_sphere"], meshes["target_faces"]))
 
@@ -282,52 +295,67 @@ class Hemisphere:
         from cat_surface_gpu_b200.gpu_pipeline import register_meshes
 
         stream = torch.cuda.current_stream()
-        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        events = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        area = self.meshes["source_area"]
         self.points.copy_(self.pristine)
-        k0.record(stream)
+        events[0].record(stream)
+        self.pre_scratch = surf2sphere.preprocess_device(self.points, self.faces_device, self.rings, self.plan_device,
+                                                         self.plan, stop_at=5, scratch=self.pre_scratch)
+        events[1].record(stream)
+        prefix = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(self.points.cpu().numpy(), area)
+        radius = projection_radius(prefix)
+        self.points.copy_(torch.from_numpy(prefix))
+        events[2].record(stream)
         self.scratch = surf2sphere.areal_sweeps_device(
-            self.points, self.plan_device, self.plan, iterations=SWEEPS + 1, project_every=1000, radius=self.radius,
+            self.points, self.plan_device, self.plan, iterations=SWEEPS + 1, project_every=1000, radius=radius,
             arithmetic="cat", launch=self.launch, scratch=self.scratch)
-        k1.record(stream)
+        events[3].record(stream)
         smoothed = self.points.cpu().numpy()
-        sphere = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(smoothed, self.meshes["source_area"])
+        sphere = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(smoothed, area)
         surface, target_surface, target_sphere = self.meshes_in
         final, angle, cost, timings = register_meshes(
             surface, GiftiMesh(sphere, self.meshes["faces"]), target_surface, target_sphere, device=self.device,
             dartel_dtype=dartel_dtype or self.dartel_dtype, stencil_threads=min(64, os.cpu_count() or 8), **CHAIN)
-        timings["sweeps_kernel_ms"] = k0, k1
-        return final, sphere, timings
+        timings["events"] = events
+        return final, sphere, prefix, timings
+
+    def check_status(self):
+        from cat_surface_gpu_b200 import surf2sphere
+
+        for scratch, what in ((self.pre_scratch, "preprocess"), (self.scratch, "sweep")):
+            status, where = surf2sphere.read_status(scratch)
+            if status != 0:
+                raise RuntimeError(f"{what} kernel status {status} at {where}")
 
 
 def hemisphere_e2e(meshes, device, dartel_dtype, workdir: Path) -> tuple[float, int, int]:
-    """One hemisphere through the public API with host buffers and GIFTI files; returns (s, h2d, d2h)."""
+    """One hemisphere through the public API with host buffers and GIFTI files; returns (s, h2d, d2h).
+
+    ``run_cat_surf2sphere_gpu`` (every stage on the GPU) from the surface
+    file to the sphere file, then ``run_cat_surface_gpu_pipeline`` on the four
+    GIFTI files.
+    """
 
     import torch
 
-    from cat_surface_gpu_b200 import surf2sphere
-    from cat_surface_gpu_b200.gifti import GiftiMesh, write_gifti_mesh
     from cat_surface_gpu_b200.gpu_pipeline import run_cat_surface_gpu_pipeline
+    from cat_surface_gpu_b200.surf2sphere import run_cat_surf2sphere_gpu
 
-    prefix, faces = meshes["prefix"], meshes["faces"]
     torch.cuda.synchronize()
     start = time.perf_counter()
-    topology = surf2sphere.Surf2SphereTopology.from_mesh(GiftiMesh(prefix, faces))
-    smoothed, _ = surf2sphere.run_areal_smoothing_cuda(prefix, faces, topology, iterations=SWEEPS + 1,
-                                                        project_every=1000, radius=projection_radius(prefix),
-                                                        device=device, launch="auto")
-    sphere = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(smoothed, meshes["source_area"])
-    write_gifti_mesh(workdir / "source_sphere.gii", GiftiMesh(sphere, faces))
+    sphere = run_cat_surf2sphere_gpu(workdir / "source_surface.gii", workdir / "source_sphere.gii", stop_at=10,
+                                     preprocess_kernel="triton", device=device)
     result = run_cat_surface_gpu_pipeline(
         workdir / "source_surface.gii", workdir / "source_sphere.gii", workdir / "target_surface.gii",
         workdir / "target_sphere.gii", workdir / "registered.gii", device=device, dartel_dtype=dartel_dtype,
         stencil_threads=min(64, os.cpu_count() or 8), **CHAIN)
     torch.cuda.synchronize()
     seconds = time.perf_counter() - start
-    plan = topology.plan
-    h2d = prefix.nbytes + sum(getattr(plan, n).nbytes for n in ("slot_off", "slot_tri", "order", "level_begin",
-                                                                  "level_end"))
-    h2d += meshes["surface"].nbytes + meshes["target_surface"].nbytes + sphere.nbytes + meshes["target_sphere"].nbytes
-    d2h = prefix.nbytes + result.vertices.nbytes
+    surface = meshes["surface"]
+    # inputs copied to the device: the surface twice (Surf2Sphere, SurfWarp), the sphere, the target mesh
+    h2d = 2 * surface.nbytes + sphere.vertices.nbytes + meshes["target_surface"].nbytes + meshes["target_sphere"].nbytes
+    h2d += 2 * meshes["faces"].nbytes + meshes["target_faces"].nbytes
+    d2h = sphere.vertices.nbytes + result.vertices.nbytes
     return seconds, int(h2d), int(d2h)
 
 
@@ -479,34 +507,34 @@ def run_native(args):
     for _ in range(args.warmup):
         hemi.step()
     barrier()
+    hemi.check_status()
     sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
     if sampler:
         sampler.start()
-    step_ms, kernel_ms, stage = [], [], []
-    final = sphere = None
+    step_ms, kernel_ms, pre_ms, stage = [], [], [], []
+    final = sphere = prefix = None
     launches_before = _native.kernel_launches()
     for index in range(args.steps):
         flush.fill_(index & 0xFF)
         barrier()
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
-        final, sphere, timings = hemi.step()
+        final, sphere, prefix, timings = hemi.step()
         s1.record(stream)
         torch.cuda.synchronize()
         step_ms.append(s0.elapsed_time(s1))
-        k0, k1 = timings.pop("sweeps_kernel_ms")
-        kernel_ms.append(k0.elapsed_time(k1))
+        ev = timings.pop("events")
+        pre_ms.append(ev[0].elapsed_time(ev[1]))
+        kernel_ms.append(ev[2].elapsed_time(ev[3]))
         stage.append(timings)
     barrier()
     launches = _native.kernel_launches() - launches_before
     clocks = sampler.stop() if sampler else None
-    status, where = surf2sphere.read_status(hemi.scratch)
-    if status != 0:
-        raise RuntimeError(f"sweep kernel status {status} at {where}")
+    hemi.check_status()
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile": True, "step_ms": step_ms, "sweeps_kernel_ms": kernel_ms,
-                              "gpu_launches": launches}))
+                              "preprocess_ms": pre_ms, "gpu_launches": launches}))
         if world > 1:
             dist.destroy_process_group()
         return 0
@@ -519,11 +547,12 @@ def run_native(args):
     # parity (untimed): the chain against the reference's CPU chain (float64 DARTEL, like the timed chain),
     # the sweeps against the upstream binary, and a float32-DARTEL chain against the float64 one
     parity = {"chain_vs_cpu_reference": error_stats(meshes["chain_final"], final),
-              "surf2sphere_vs_binary": error_stats(meshes["binary_sphere"], sphere)}
+              "surf2sphere_vs_binary": error_stats(meshes["binary_sphere"], sphere),
+              "stages_1_5_vs_binary": error_stats(meshes["prefix"], prefix)}
     hemi.step(dartel_dtype=torch.float32)  # warm (graph capture for float32)
     torch.cuda.synchronize()
     f0 = time.perf_counter()
-    final32, _, timings32 = hemi.step(dartel_dtype=torch.float32)
+    final32, _, _, timings32 = hemi.step(dartel_dtype=torch.float32)
     torch.cuda.synchronize()
     parity["chain_dartel_f32_vs_f64"] = error_stats(final, final32)
     parity["chain_dartel_f32_seconds"] = time.perf_counter() - f0
@@ -561,6 +590,7 @@ def run_native(args):
         wavefront_steps = sum((s - 1) * hemi.plan.level_stride + hemi.plan.n_levels for s in epochs)
         stages = {k: statistics.mean(t[k] for t in stage) for k in stage[0] if isinstance(stage[0][k], float)}
         stages["sweeps_kernel_s"] = kernel_s
+        stages["preprocess_kernels_s"] = statistics.mean(pre_ms) / 1e3
         cpu_baseline = None
         if world == 1 and not args.no_cpu_baseline:
             sample = cpu_hemisphere_sample(meshes)

@@ -89,9 +89,9 @@ struct Traits<CSG_ARITH_CAT> {
         float cz = __fsub_rn(__fmul_rn(e0x, e1y), __fmul_rn(e0y, e1x));
         float sq = __fadd_rn(__fadd_rn(__fmul_rn(cx, cx), __fmul_rn(cy, cy)), __fmul_rn(cz, cz));
         area = __dmul_rn(0.5, __dsqrt_rn(static_cast<double>(sq)));
-        mx = __ddiv_rn(__dadd_rn(__dadd_rn((double)a.x, (double)b.x), (double)c.x), 3.0);
-        my = __ddiv_rn(__dadd_rn(__dadd_rn((double)a.y, (double)b.y), (double)c.y), 3.0);
-        mz = __ddiv_rn(__dadd_rn(__dadd_rn((double)a.z, (double)b.z), (double)c.z), 3.0);
+        mx = csg::div3_rn(__dadd_rn(__dadd_rn((double)a.x, (double)b.x), (double)c.x));
+        my = csg::div3_rn(__dadd_rn(__dadd_rn((double)a.y, (double)b.y), (double)c.y));
+        mz = csg::div3_rn(__dadd_rn(__dadd_rn((double)a.z, (double)b.z), (double)c.z));
         area = area > 0.0 ? area : 0.0;
         area = area < 1.0 ? area : 1.0;
     }
@@ -186,9 +186,9 @@ struct Traits<CSG_ARITH_FP64> {
         double cz = __dsub_rn(__dmul_rn(e0x, e1y), __dmul_rn(e0y, e1x));
         double sq = __dadd_rn(__dadd_rn(__dmul_rn(cx, cx), __dmul_rn(cy, cy)), __dmul_rn(cz, cz));
         area = __dmul_rn(0.5, __dsqrt_rn(sq));
-        mx = __ddiv_rn(__dadd_rn(__dadd_rn(a.x, b.x), c.x), 3.0);
-        my = __ddiv_rn(__dadd_rn(__dadd_rn(a.y, b.y), c.y), 3.0);
-        mz = __ddiv_rn(__dadd_rn(__dadd_rn(a.z, b.z), c.z), 3.0);
+        mx = csg::div3_rn(__dadd_rn(__dadd_rn(a.x, b.x), c.x));
+        my = csg::div3_rn(__dadd_rn(__dadd_rn(a.y, b.y), c.y));
+        mz = csg::div3_rn(__dadd_rn(__dadd_rn(a.z, b.z), c.z));
         area = area > 0.0 ? area : 0.0;
         area = area < 1.0 ? area : 1.0;
     }
@@ -486,6 +486,14 @@ size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
 // Barrier whose expected arrival count is one more than the grid holds: the
 // bounded wait must give up and record CSG_ERR_TIMEOUT.
+__global__ void k_div3_selftest(const double* __restrict__ x, long long n, double* __restrict__ a,
+                                double* __restrict__ b) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    a[i] = __ddiv_rn(x[i], 3.0);
+    b[i] = csg::div3_rn(x[i]);
+}
+
 __global__ void barrier_timeout_selftest_kernel(csg::Control* ctl, unsigned long long timeout_ns) {
     unsigned int phase = 1;
     csg::grid_barrier(ctl, phase, timeout_ns, 1);
@@ -553,6 +561,15 @@ int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, cons
         case CSG_ARITH_FP32: return dispatch_lanes<CSG_ARITH_FP32>(p, n_ctas, threads_per_cta, lanes_per_vertex, s);
         default: return dispatch_lanes<CSG_ARITH_FP64>(p, n_ctas, threads_per_cta, lanes_per_vertex, s);
     }
+}
+
+int csg_selftest_div3(const double* x, long long n, double* by_division, double* by_multiplies, csg_stream_t stream) {
+    if (!x || n < 0 || !by_division || !by_multiplies) return csg::fail(CSG_ERR_ARG, "div3 self-test: bad arguments");
+    if (n == 0) return CSG_OK;
+    (csg::note_launch(), k_div3_selftest<<<static_cast<unsigned>((n + 255) / 256), 256, 0,
+                                          reinterpret_cast<cudaStream_t>(stream)>>>(x, n, by_division, by_multiplies));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
 }
 
 int csg_selftest_barrier_timeout(void* scratch, size_t scratch_bytes, double timeout_s, csg_stream_t stream) {

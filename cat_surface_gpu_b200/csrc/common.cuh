@@ -12,6 +12,23 @@
 
 namespace csg {
 
+// Correctly rounded x / 3 for finite binary64 x with |x| >= 2^-1000 (far from
+// the subnormal range, where RN(x zl) loses the needed bits) with two
+// multiplies (Brisebarre, Muller and Raina, "Accelerating correctly rounded
+// floating-point division when the divisor is known in advance", IEEE TC
+// 53(8), 2004): q = RN(x zh + RN(x zl)) with zh = RN(1/3) and
+// zl = RN(1/3 - zh) = zh * 2^-54.  Why it is exact for the divisor 3: the
+// exact quotient x/3 = M 2^e / 3 sits at a multiple of a third of a unit in
+// the last place, so it is never closer than 1/6 ulp to a rounding midpoint,
+// while x zh + RN(x zl) is within ~2^-105 relative of x/3.  Equal to
+// __ddiv_rn(x, 3.0) bit for bit (csg_selftest_div3 and the sweep and
+// preprocess tests, which compare against the oracle's plain division).
+__device__ __forceinline__ double div3_rn(double x) {
+    const double zh = 0x1.5555555555555p-2;
+    const double zl = 0x1.5555555555555p-56;
+    return __fma_rn(x, zh, __dmul_rn(x, zl));
+}
+
 // Status word layout inside a kernel's control block (first 256 bytes of its
 // scratch).  word 0: barrier arrival counter; word 1: status (CSG_OK or a
 // negative CSG_ERR_*); word 2: index of the barrier/step that failed.

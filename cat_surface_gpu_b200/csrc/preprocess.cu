@@ -288,7 +288,7 @@ __global__ void k_vertex_areas(const double* __restrict__ area, const int* __res
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     double s = 0.0;
-    for (int k = inc_off[v]; k < inc_off[v + 1]; ++k) s = __dadd_rn(s, __ddiv_rn(area[inc[k] >> 2], 3.0));
+    for (int k = inc_off[v]; k < inc_off[v + 1]; ++k) s = __dadd_rn(s, csg::div3_rn(area[inc[k] >> 2]));
     va[v] = s;
 }
 

@@ -384,6 +384,44 @@ def run_areal_smoothing_cuda(
     }
 
 
+def preprocess_device(
+    points: torch.Tensor,
+    faces_device: torch.Tensor,
+    topology_device: tuple,
+    plan_device: dict[str, torch.Tensor],
+    plan: SweepPlan,
+    *,
+    stop_at: int = 5,
+    launch: dict | None = None,
+    timeout_s: float = 2.0,
+    scratch: torch.Tensor | None = None,
+) -> torch.Tensor:
+    """Stages 1..stop_at in place on a float32 device tensor (no host synchronisation, no ellipsoid step).
+
+    ``topology_device`` is ``(nb_off, nb, inc_off, inc)`` on the device (the
+    1-ring CSR and the corner-sorted incidences).  Returns the scratch tensor
+    whose first 256 bytes hold the status word (:func:`read_status`).
+    """
+
+    n, nf = int(points.shape[0]), int(faces_device.shape[0])
+    lib = _native.library()
+    need = int(lib.csg_preprocess_scratch_bytes(n, nf))
+    if scratch is None or scratch.numel() < need:
+        scratch = torch.empty(need, dtype=torch.uint8, device=points.device)
+    cfg = {"n_ctas": 0, "threads_per_cta": 512, "lanes_per_vertex": 8}
+    if launch:
+        cfg.update(launch)
+    nb_off, nb, inc_off, inc = topology_device[:4]
+    _native.check(lib.csg_surf2sphere_preprocess(
+        _native.ptr(points), n, _native.ptr(faces_device), nf, _native.ptr(nb_off), _native.ptr(nb),
+        _native.ptr(inc_off), _native.ptr(inc), _native.ptr(plan_device["order"]),
+        _native.ptr(plan_device["level_begin"]), _native.ptr(plan_device["level_end"]), plan.n_levels,
+        plan.level_stride, int(stop_at), _native.ptr(scratch), scratch.numel(), int(cfg["n_ctas"]),
+        int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s), _native.stream_handle()),
+        "csg_surf2sphere_preprocess")
+    return scratch
+
+
 def run_surf2sphere_preprocess_cuda(
     vertices: np.ndarray,
     faces: np.ndarray,
@@ -441,13 +479,8 @@ def run_surf2sphere_preprocess_cuda(
         torch.cuda.synchronize(target)
         timings["preprocess_upload_seconds"] = time.perf_counter() - start
         start = time.perf_counter()
-        _native.check(lib.csg_surf2sphere_preprocess(
-            _native.ptr(points), n, _native.ptr(face_dev), nf, _native.ptr(nb_off), _native.ptr(nb),
-            _native.ptr(inc_off), _native.ptr(inc), _native.ptr(plan_device["order"]),
-            _native.ptr(plan_device["level_begin"]), _native.ptr(plan_device["level_end"]), plan.n_levels,
-            plan.level_stride, int(stop_at), _native.ptr(scratch), scratch.numel(), int(cfg["n_ctas"]),
-            int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s), _native.stream_handle()),
-            "csg_surf2sphere_preprocess")
+        preprocess_device(points, face_dev, (nb_off, nb, inc_off, inc), plan_device, plan, stop_at=stop_at,
+                          launch=cfg, timeout_s=timeout_s, scratch=scratch)
         status, where = read_status(scratch)
         if status != 0:
             raise RuntimeError(f"CAT_Surf2Sphere preprocess kernel failed (status {status} at barrier {where})")

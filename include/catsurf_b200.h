@@ -150,6 +150,12 @@ CSG_API int csg_areal_sweeps_noalloc(void *points, int n_vertices, const int32_t
  * than the grid has; the wait gives up after timeout_s (<= 10 s) and records
  * CSG_ERR_TIMEOUT in scratch's status word.  Exercises the timeout path
  * without faulting or hanging the GPU; the context stays usable. */
+/* Self-test of the kernels' division by three (two multiplies, see
+ * csrc/common.cuh): writes __ddiv_rn(x, 3) and the fast form for n values so
+ * a test can compare them bit for bit.  No reference counterpart. */
+CSG_API int csg_selftest_div3(const double *x, long long n, double *by_division, double *by_multiplies,
+                              csg_stream_t stream);
+
 CSG_API int csg_selftest_barrier_timeout(void *scratch, size_t scratch_bytes, double timeout_s, csg_stream_t stream);
 
 /* Surf2Sphere stages 1-5 (low_smooth, inflate, very_inflate, high_smooth,

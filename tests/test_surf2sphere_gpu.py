@@ -179,3 +179,22 @@ def test_bounded_wait_reports_timeout_and_context_survives(s2s, native_library):
     f = np.asarray(((0, 1, 2), (0, 3, 1), (0, 2, 3), (1, 3, 2)), dtype=np.int32)
     out, _ = s2s.run_areal_smoothing_cuda(v, f, _topology(s2s, v, f), iterations=5, project_every=2, radius=1.0)
     np.testing.assert_array_equal(out, oracle.areal_sweeps(v, f, iterations=5, project_every=2, radius=1.0))
+
+
+@pytest.mark.gpu
+def test_division_by_three_is_correctly_rounded(native_library):
+    """The kernels' two-multiply x / 3 equals the IEEE division on 16M doubles across binades and edge cases."""
+
+    from cat_surface_gpu_b200 import _native
+
+    rng = np.random.default_rng(3)
+    mant = rng.random(1 << 24) + 1.0
+    expo = rng.integers(-1000, 1000, size=mant.size)
+    x = np.ldexp(mant, expo) * rng.choice([-1.0, 1.0], size=mant.size)
+    x[:8] = [0.0, -0.0, 1.0, 3.0, 6.0, 2.0 ** -1000, 1.7e308, np.nextafter(3.0, 0.0)]
+    xd = torch.as_tensor(x, device="cuda")
+    a, b = torch.empty_like(xd), torch.empty_like(xd)
+    _native.check(native_library.csg_selftest_div3(xd.data_ptr(), xd.numel(), a.data_ptr(), b.data_ptr(),
+                                                   _native.stream_handle()), "csg_selftest_div3")
+    assert torch.equal(a.view(torch.int64), b.view(torch.int64))
+    np.testing.assert_array_equal(a.cpu().numpy(), x / 3.0)
