@@ -392,6 +392,9 @@ int launch_passes(const PassParams& params, int n_ctas, int threads, cudaStream_
 int run_passes(PassParams p, int passes, double strength, const unsigned char* selected, int n_ctas, int threads,
                int lanes, cudaStream_t s) {
     if (passes <= 0) return CSG_OK;
+    // every launch counts its barrier arrivals from zero; the status word is
+    // kept, so a launch after a timed-out one leaves at its first barrier
+    CSG_CUDA_CHECK(cudaMemsetAsync(&p.ctl->arrivals, 0, sizeof(p.ctl->arrivals), s));
     p.passes = passes;
     p.strength = strength;
     p.selected = selected;
