@@ -81,7 +81,82 @@ def parse_args():
     parser.add_argument("--profile", action="store_true",
                         help="for profilers: --warmup then --steps hemispheres with the default sweep launch shape, "
                              "no parity, e2e, CPU or batched legs; prints the step times only")
+    parser.add_argument("--case", choices=("sweeps", "preprocess", "dartel", "rotation"),
+                        help="for kernel profilers: run one small case of one kernel family three times "
+                             "(the third run is the one to capture) and exit")
     return parser.parse_args()
+
+
+def run_case(name: str) -> int:
+    """Small single-kernel cases on cuda:0 for ncu captures (nothing is timed or printed but a summary)."""
+
+    import numpy as np
+    import torch
+
+    from cat_surface_gpu_b200 import surf2sphere, synthetic
+    from cat_surface_gpu_b200.gifti import GiftiMesh
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    meshes = load_meshes()
+    faces = meshes["faces"]
+    if name in ("sweeps", "preprocess"):
+        topology = surf2sphere.Surf2SphereTopology.from_mesh(GiftiMesh(meshes["surface"], faces))
+        plan = topology.plan
+        plan_device = plan.to_device(device)
+        scratch = None
+        if name == "sweeps":
+            # 200 of the 4,999 sweeps of the hemisphere mesh: one persistent launch
+            base = torch.from_numpy(meshes["prefix"]).to(device)
+            for _ in range(3):
+                pts = base.clone()
+                scratch = surf2sphere.areal_sweeps_device(pts, plan_device, plan, iterations=201, project_every=1000,
+                                                          radius=projection_radius(meshes["prefix"]),
+                                                          arithmetic="cat", scratch=scratch)
+        else:
+            # stage 1 of the hemisphere mesh: one persistent launch of 49 passes plus the stage statistics
+            from cat_surface_gpu_b200.features import _topology
+
+            rings = _topology(faces, meshes["surface"].shape[0], device)[:4]
+            faces_device = torch.from_numpy(faces).to(device)
+            base = torch.from_numpy(meshes["surface"]).to(device)
+            for _ in range(3):
+                pts = base.clone()
+                scratch = surf2sphere.preprocess_device(pts, faces_device, rings, plan_device, plan, stop_at=1,
+                                                        scratch=scratch)
+        torch.cuda.synchronize()
+        status, where = surf2sphere.read_status(scratch)
+        if status != 0:
+            raise RuntimeError(f"{name} kernel status {status} at {where}")
+    elif name == "dartel":
+        # four dartel_steps (k = 0..3, code 1) on two 256 x 128 float64 maps, batched
+        from cat_surface_gpu_b200.surface_warp import solve_dartel_maps
+
+        nx, ny = SHEET
+        src = torch.as_tensor(np.stack([synthetic.smooth_sheet(ny, nx, 1), synthetic.smooth_sheet(ny, nx, 2)]),
+                              device=device)
+        tgt = torch.as_tensor(np.stack([synthetic.smooth_sheet(ny, nx, 3), synthetic.smooth_sheet(ny, nx, 4)]),
+                              device=device)
+        for _ in range(3):
+            solve_dartel_maps(src, tgt, loop=4, its=1, device=device, dtype=torch.float64)
+        torch.cuda.synchronize()
+    else:
+        # 256 quaternion candidates on one 102,400-point surface against the resampling sphere
+        from cat_surface_gpu_b200.surface_rotation import (RotationGridIndexDevice, batched_costs,
+                                                           quaternion_matrices, uniform_quaternions)
+        from cat_surface_gpu_b200.surface_stencil import resampling_sphere
+
+        tp, tf = resampling_sphere(6)
+        index = RotationGridIndexDevice.build(tp, tf, device=device, grid_size=128, margin=1)
+        pts = synthetic.fibonacci_points(102400, np.random.default_rng(1)).astype(np.float32)
+        inputs = index.prepare_cost_inputs(pts, np.sin(3 * pts[:, 0]).astype(np.float64),
+                                           np.sin(3 * tp[:, 0]))
+        mats = quaternion_matrices(uniform_quaternions(256, 2))
+        for _ in range(3):
+            batched_costs([index], [inputs], matrix_sets=[mats])
+        torch.cuda.synchronize()
+    print(json.dumps({"case": name, "ok": True}))
+    return 0
 
 
 def dist_env():
@@ -637,6 +712,8 @@ def run_native(args):
 
 def main():
     args = parse_args()
+    if args.case:
+        return run_case(args.case)
     if args.impl == "reference":
         return run_reference(args)
     return run_native(args)
