@@ -1,5 +1,5 @@
 // Host-side mesh topology and wavefront planning for the ordered
-// Surf2Sphere sweeps.  Plain C++, no device memory; O(faces) everywhere.
+// Surf2Sphere sweeps.  Plain C++, no device memory.
 #include <atomic>
 #include <algorithm>
 #include <cstdint>
@@ -179,6 +179,73 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
                 int w = slot_tri[4 * s + k];
                 if (w > v) stride = std::max(stride, levels[w] - levels[v] + 1);
             }
+    // Tighten the stride.  Any integer schedule f with 1 <= f(w) - f(v) <= D - 1
+    // on every edge v < w runs vertex v of sweep s at step s D + f(v) with the
+    // sequential read versions (lower neighbours this sweep, higher ones the
+    // previous sweep).  The longest-path levels are one such f; the smallest
+    // feasible D comes from difference constraints: lower D while the
+    // relaxation f(w) >= f(v) + 1, f(v) >= f(w) - (D - 1) still converges
+    // (a non-converging relaxation means a positive cycle, or too slow a
+    // convergence to be worth it; both keep the last feasible D).
+    {
+        std::vector<int32_t> lo_off(n + 1, 0), hi_off(n + 1, 0);
+        std::vector<int32_t> lo_nb, hi_nb;
+        {
+            std::vector<std::vector<int32_t>> lower(n), higher(n);
+            for (int v = 0; v < n; ++v)
+                for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
+                    for (int k = 0; k < 3; ++k) {
+                        const int u = slot_tri[4 * s + k];
+                        if (u < v) lower[v].push_back(u);
+                        if (u > v) higher[v].push_back(u);
+                    }
+            for (int v = 0; v < n; ++v) {
+                std::sort(lower[v].begin(), lower[v].end());
+                lower[v].erase(std::unique(lower[v].begin(), lower[v].end()), lower[v].end());
+                std::sort(higher[v].begin(), higher[v].end());
+                higher[v].erase(std::unique(higher[v].begin(), higher[v].end()), higher[v].end());
+                lo_off[v + 1] = lo_off[v] + static_cast<int32_t>(lower[v].size());
+                hi_off[v + 1] = hi_off[v] + static_cast<int32_t>(higher[v].size());
+                lo_nb.insert(lo_nb.end(), lower[v].begin(), lower[v].end());
+                hi_nb.insert(hi_nb.end(), higher[v].begin(), higher[v].end());
+            }
+        }
+        std::vector<int32_t> best = levels, f;
+        int last_iterations = 64;
+        for (int trial = stride - 1; trial >= 2; --trial) {
+            f = best;
+            const int cap = std::min(4000, 4 * last_iterations + 64);
+            bool converged = false;
+            int it = 0;
+            for (; it < cap && !converged; ++it) {
+                bool changed = false;
+                for (int v = 0; v < n; ++v)  // f(v) >= f(u) + 1 for lower neighbours u
+                    for (int k = lo_off[v]; k < lo_off[v + 1]; ++k)
+                        if (f[v] < f[lo_nb[k]] + 1) {
+                            f[v] = f[lo_nb[k]] + 1;
+                            changed = true;
+                        }
+                for (int v = n - 1; v >= 0; --v)  // f(v) >= f(w) - (D - 1) for higher neighbours w
+                    for (int k = hi_off[v]; k < hi_off[v + 1]; ++k)
+                        if (f[v] < f[hi_nb[k]] - (trial - 1)) {
+                            f[v] = f[hi_nb[k]] - (trial - 1);
+                            changed = true;
+                        }
+                converged = !changed;
+            }
+            if (!converged) break;
+            const int32_t fmin = *std::min_element(f.begin(), f.end());
+            const int32_t fmax = *std::max_element(f.begin(), f.end());
+            if (fmax - fmin + 1 > n) break;  // level tables hold at most n levels
+            for (int v = 0; v < n; ++v) f[v] -= fmin;
+            best.swap(f);
+            stride = trial;
+            last_iterations = it;
+        }
+        levels.swap(best);
+        n_levels = 0;
+        for (int v = 0; v < n; ++v) n_levels = std::max(n_levels, levels[v] + 1);
+    }
     // order: by (level mod stride, level, id) -- counting sort on level.
     std::vector<int32_t> per_level(static_cast<size_t>(n_levels) + 1, 0);
     for (int v = 0; v < n; ++v) per_level[levels[v] + 1]++;

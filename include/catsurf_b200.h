@@ -80,10 +80,13 @@ CSG_API int csg_dependency_levels(int n_vertices, const int32_t *nbr_off, const 
 CSG_API int csg_greedy_colours(int n_vertices, const int32_t *nbr_off, const int32_t *nbr, int32_t *colours);
 
 /* Wavefront plan for the ordered sweeps (host).
- * Vertex v of sweep s runs at wavefront step s * level_stride + level(v);
- * level_stride = 1 + max over edges (v < w) of level(w) - level(v), which
- * keeps exactly the sequential Gauss-Seidel reads (lower neighbours of the
- * current sweep, higher neighbours of the previous one).
+ * Vertex v of sweep s runs at wavefront step s * level_stride + level(v),
+ * where level() is any integer schedule with 1 <= level(w) - level(v) <=
+ * level_stride - 1 on every edge v < w; that keeps exactly the sequential
+ * Gauss-Seidel reads (lower neighbours of the current sweep, higher
+ * neighbours of the previous one).  The builder starts from the longest-path
+ * levels and lowers the stride while difference-constraint relaxation still
+ * finds a schedule (61,442-vertex hull: stride 11 -> 6, so 45% fewer steps).
  * Outputs: slot_off [n+1]; slot_tri [3 * n_faces * 4] (per incident slot the
  * face's three vertex ids in face order plus the face id, int4-aligned);
  * order [n] (vertices sorted by (level mod stride, level, id));

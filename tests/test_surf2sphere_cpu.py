@@ -186,25 +186,31 @@ def test_wavefront_schedule_reads_sequential_versions(native_library, subdivisio
     assert updates == v.shape[0] * (iterations - 1)
 
 
-def test_plan_stride_bounds_level_gaps(native_library):
+def test_plan_schedule_is_a_valid_tight_potential(native_library):
+    """Plan groups f(v) satisfy 1 <= f(w) - f(v) <= stride - 1 on every edge v < w, with a stride no larger
+    than the longest-path levels give (6 instead of 11 on the 61,442-vertex hull)."""
+
     g = load_surf2sphere_golden("c2")
     from cat_surface_gpu_b200.surf2sphere import SweepPlan
 
-    plan = SweepPlan.build(g["faces"], g["prefix"].shape[0])
-    levels = oracle.dependency_levels(g["prefix"].shape[0], g["faces"])
-    assert plan.n_levels == levels.max() + 1
+    n = g["prefix"].shape[0]
     f = g["faces"]
-    gaps = []
-    for a, b in ((0, 1), (1, 2), (2, 0)):
-        lo = np.minimum(f[:, a], f[:, b])
-        hi = np.maximum(f[:, a], f[:, b])
-        gaps.append(levels[hi] - levels[lo])
-    assert plan.level_stride == max(1, int(np.max(np.concatenate(gaps))) + 1)
-    # every vertex appears once in `order`, grouped by level
-    np.testing.assert_array_equal(np.sort(plan.order), np.arange(g["prefix"].shape[0]))
+    plan = SweepPlan.build(f, n)
+    np.testing.assert_array_equal(np.sort(plan.order), np.arange(n))  # every vertex once
+    group = np.full(n, -1, dtype=np.int64)
     for level in range(plan.n_levels):
-        members = plan.order[plan.level_begin[level] : plan.level_end[level]]
-        assert (levels[members] == level).all()
+        group[plan.order[plan.level_begin[level] : plan.level_end[level]]] = level
+    assert (group >= 0).all()
+    edges = np.sort(np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]]), axis=1)
+    gap = group[edges[:, 1]] - group[edges[:, 0]]
+    assert gap.min() >= 1 and gap.max() <= plan.level_stride - 1
+    levels = oracle.dependency_levels(n, f)
+    longest_path_stride = int((levels[edges[:, 1]] - levels[edges[:, 0]]).max()) + 1
+    assert plan.level_stride <= longest_path_stride
+    assert (longest_path_stride, plan.level_stride) == (11, 6)
+    # groups of one residue class mod the stride are contiguous in `order`
+    residues = [group[plan.order[i]] % plan.level_stride for i in range(n)]
+    assert residues == sorted(residues)
 
 
 # --- the C ABI loads and exports every declared symbol ----------------------
