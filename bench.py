@@ -589,6 +589,8 @@ def run_native(args):
     step_ms, kernel_ms, pre_ms, stage = [], [], [], []
     final = sphere = prefix = None
     launches_before = _native.kernel_launches()
+    if args.profile:  # profilers can restrict a capture to this range (ncu --nvtx --nvtx-include "timed/")
+        torch.cuda.nvtx.range_push("timed")
     for index in range(args.steps):
         flush.fill_(index & 0xFF)
         barrier()
@@ -603,6 +605,8 @@ def run_native(args):
         kernel_ms.append(ev[2].elapsed_time(ev[3]))
         stage.append(timings)
     barrier()
+    if args.profile:
+        torch.cuda.nvtx.range_pop()
     launches = _native.kernel_launches() - launches_before
     clocks = sampler.stop() if sampler else None
     hemi.check_status()
