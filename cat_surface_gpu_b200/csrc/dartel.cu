@@ -16,6 +16,7 @@
 // 1420-1616), the membrane full multigrid (1211-1417) and the whole solve
 // (surface_warp.py:239-367) as launch sequences on one stream, so a caller
 // can capture a complete solve in one CUDA graph.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -413,10 +414,9 @@ __global__ void k_combine(const T* __restrict__ rf, const T* __restrict__ rr, co
 
 // (H + L_membrane) u (dartel_grid.py:1018-1070); with `b`, the residual b - (H + L) u.
 template <typename T>
-__global__ void k_membrane_apply(const T* __restrict__ hess, const T* __restrict__ u, const T* __restrict__ b,
-                                 T* __restrict__ out, int nx, int ny, RegWeights rw) {
-    Pt p;
-    if (!point(nx, ny, p)) return;
+__device__ __forceinline__ void membrane_apply_at(const T* __restrict__ hess, const T* __restrict__ u,
+                                                  const T* __restrict__ b, T* __restrict__ out, int nx, int ny,
+                                                  const RegWeights& rw, const Pt& p) {
     const int P = nx * ny;
     const size_t o1 = static_cast<size_t>(p.b) * P;
     const T* ux = u + 2 * o1;
@@ -436,16 +436,21 @@ __global__ void k_membrane_apply(const T* __restrict__ hess, const T* __restrict
     }
 }
 
+template <typename T>
+__global__ void k_membrane_apply(const T* __restrict__ hess, const T* __restrict__ u, const T* __restrict__ b,
+                                 T* __restrict__ out, int nx, int ny, RegWeights rw) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    membrane_apply_at(hess, u, b, out, nx, ny, rw, p);
+}
+
 // One red-black half sweep, in place (dartel_grid.py:1187-1208 /
 // dartel_triton.py:242-291): cells with ((x + y) & 1) == colour.  Exact for
 // even nx and for nx == 1, where every neighbour read is either of the other
 // colour or the cell itself.
 template <typename T>
-__global__ void k_relax(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u, int nx, int ny,
-                        int colour, T w00, T w01, T w10) {
-    Pt p;
-    if (!point(nx, ny, p)) return;
-    if (((p.x + p.y) & 1) != colour) return;
+__device__ __forceinline__ void relax_at(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u,
+                                         int nx, int ny, T w00, T w01, T w10, const Pt& p) {
     const int P = nx * ny;
     const size_t o1 = static_cast<size_t>(p.b) * P;
     T* ux = u + 2 * o1;
@@ -463,6 +468,15 @@ __global__ void k_relax(const T* __restrict__ hess, const T* __restrict__ b, T* 
     const T nyv = (-cr * rx + dxx * ry) / det;
     ux[p.i] = nxv;
     uy[p.i] = nyv;
+}
+
+template <typename T>
+__global__ void k_relax(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u, int nx, int ny,
+                        int colour, T w00, T w01, T w10) {
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    if (((p.x + p.y) & 1) != colour) return;
+    relax_at(hess, b, u, nx, ny, w00, w01, w10, p);
 }
 
 // Direct 2x2 point solve of the coarsest level (dartel_grid.py:1318-1334).
@@ -492,12 +506,10 @@ __device__ __forceinline__ T wt2(T d) {
 // x pass, per target point; `accumulate` adds into dst (prolongation,
 // dartel_grid.py:1380-1387).  Fields are [B * C][sny][snx] -> [B * C][tny][tnx].
 template <typename T>
-__global__ void k_resize(const T* __restrict__ src, T* __restrict__ dst, int snx, int sny, int tnx, int tny,
-                         int accumulate) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= tnx * tny) return;
+__device__ __forceinline__ void resize_at(const T* __restrict__ src, T* __restrict__ dst, int snx, int sny, int tnx,
+                                          int tny, int accumulate, int plane, int i) {
     const int x = i % tnx, y = i / tnx;
-    const T* f = src + static_cast<size_t>(blockIdx.y) * snx * sny;
+    const T* f = src + static_cast<size_t>(plane) * snx * sny;
     const T yl = (static_cast<T>(y) + T(0.5)) * static_cast<T>(sny) / static_cast<T>(tny) - T(0.5);
     const int yo = static_cast<int>(floor(yl + T(0.5)));
     const T yof = static_cast<T>(yo);
@@ -512,8 +524,94 @@ __global__ void k_resize(const T* __restrict__ src, T* __restrict__ dst, int snx
     const T ic = ywm * f[rm + cc] + yw * f[rc + cc] + ywp * f[rp + cc];
     const T ip = ywm * f[rm + cp] + yw * f[rc + cp] + ywp * f[rp + cp];
     const T r = xwm * im + xw * ic + xwp * ip;
-    T* o = dst + static_cast<size_t>(blockIdx.y) * tnx * tny;
+    T* o = dst + static_cast<size_t>(plane) * tnx * tny;
     o[i] = accumulate ? o[i] + r : r;
+}
+
+template <typename T>
+__global__ void k_resize(const T* __restrict__ src, T* __restrict__ dst, int snx, int sny, int tnx, int tny,
+                         int accumulate) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= tnx * tny) return;
+    resize_at(src, dst, snx, sny, tnx, tny, accumulate, static_cast<int>(blockIdx.y), i);
+}
+
+// ------------------------------------------------ fused coarse multigrid cycle
+//
+// The levels of a V-cycle at or below kCoarsePoints points per grid run as one
+// launch with one CTA per batch element: the same per-point operations as the
+// separate kernels (relax_at, membrane_apply_at, resize_at) in the same
+// order, phases separated by __syncthreads.  A coarse level's work is a few
+// thousand points, so one CTA covers it, and ~100 small launches per cycle
+// become one.
+
+constexpr int kCoarsePoints = 8192;
+constexpr int kMaxLevels = 16;
+constexpr int kCoarseThreads = 1024;
+
+template <typename T>
+struct CoarseLevel {
+    const T* A;  // Hessian [batch][3][ny][nx]
+    T* B;        // right-hand side [batch][2][ny][nx]
+    T* U;        // solution [batch][2][ny][nx]
+    T* R;        // residual [batch][2][ny][nx]
+    int nx, ny;
+    T w00, w01, w10;
+    RegWeights rw;
+};
+
+template <typename T>
+struct CoarseCycle {
+    CoarseLevel<T> lv[kMaxLevels];
+    int first, last, nit;
+};
+
+template <typename T>
+__device__ __forceinline__ void block_relax(const CoarseLevel<T>& L, int bi, int nit) {
+    const int P = L.nx * L.ny;
+    for (int it = 0; it < 2 * nit; ++it) {
+        const int colour = it % 2 == 0 ? 1 : 0;
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const Pt p{bi, i % L.nx, i / L.nx, i};
+            if (((p.x + p.y) & 1) == colour) relax_at(L.A, L.B, L.U, L.nx, L.ny, L.w00, L.w01, L.w10, p);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void block_resize(const T* src, int snx, int sny, T* dst, int tnx, int tny, int bi,
+                                             int accumulate) {
+    const int P = tnx * tny;
+    for (int j = threadIdx.x; j < 2 * P; j += blockDim.x)
+        resize_at(src, dst, snx, sny, tnx, tny, accumulate, 2 * bi + j / P, j % P);
+    __syncthreads();
+}
+
+// cycle(first) of Fmg (host side) restricted to levels first..last, for batch element blockIdx.x.
+template <typename T>
+__global__ void __launch_bounds__(kCoarseThreads) k_fmg_coarse_cycle(CoarseCycle<T> c) {
+    const int bi = blockIdx.x;
+    for (int l = c.first; l < c.last; ++l) {
+        const CoarseLevel<T>& L = c.lv[l];
+        block_relax(L, bi, c.nit);
+        const int P = L.nx * L.ny;
+        for (int i = threadIdx.x; i < P; i += blockDim.x)
+            membrane_apply_at(L.A, L.U, L.B, L.R, L.nx, L.ny, L.rw, Pt{bi, i % L.nx, i / L.nx, i});
+        __syncthreads();
+        const CoarseLevel<T>& N = c.lv[l + 1];
+        block_resize(L.R, L.nx, L.ny, N.B, N.nx, N.ny, bi, 0);
+        const int Pn = N.nx * N.ny;
+        for (int j = threadIdx.x; j < 2 * Pn; j += blockDim.x) N.U[2 * static_cast<size_t>(bi) * Pn + j] = T(0);
+        __syncthreads();
+    }
+    block_relax(c.lv[c.last], bi, c.nit);
+    for (int l = c.last; l-- > c.first;) {
+        const CoarseLevel<T>& L = c.lv[l];
+        const CoarseLevel<T>& N = c.lv[l + 1];
+        block_resize(N.U, N.nx, N.ny, L.U, L.nx, L.ny, bi, 1);
+        block_relax(L, bi, c.nit);
+    }
 }
 
 template <typename T>
@@ -650,8 +748,52 @@ struct Fmg {
         (csg::note_launch(), k_resize<T><<<grid_for(t.first * t.second, batch * channels), kThreads, 0, s>>>(src, dst, f.first, f.second,
                                                                                      t.first, t.second, accumulate));
     }
+    // First level of the fused coarse part: the finest level of at most
+    // kCoarsePoints points (the whole cycle when the finest level is small).
+    size_t coarse_first() const {
+        size_t l = 0;
+        while (l + 1 < buf.specs.size() &&
+               static_cast<long long>(buf.specs[l].first) * buf.specs[l].second > kCoarsePoints)
+            ++l;
+        return l;
+    }
+    void coarse_cycle(size_t first) {
+        const size_t last = buf.specs.size() - 1;
+        CoarseCycle<T> c{};
+        c.first = static_cast<int>(first);
+        c.last = static_cast<int>(last);
+        c.nit = nit;
+        for (size_t l = first; l <= last; ++l) {
+            double pr[5];
+            params_at(l, pr);
+            const MemWeights w = mem_weights(pr);
+            c.lv[l] = CoarseLevel<T>{buf.A[l], buf.B[l], buf.U[l], buf.R[l], buf.specs[l].first, buf.specs[l].second,
+                                     T(w.w00), T(w.w01), T(w.w10), reg_weights(pr, 1)};
+        }
+        (csg::note_launch(), k_fmg_coarse_cycle<T><<<batch, kCoarseThreads, 0, s>>>(c));
+    }
     void cycle(size_t start) {
         const size_t last = buf.specs.size() - 1;
+        const size_t fused = std::max(start, coarse_first());
+        if (buf.specs.size() <= static_cast<size_t>(kMaxLevels) && fused < last) {
+            for (size_t l = start; l < fused; ++l) {
+                relax(l);
+                const int nx = buf.specs[l].first, ny = buf.specs[l].second;
+                double pr[5];
+                params_at(l, pr);
+                (csg::note_launch(), k_membrane_apply<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(
+                    buf.A[l], buf.U[l], buf.B[l], buf.R[l], nx, ny, reg_weights(pr, 1)));
+                resize(buf.R[l], l, buf.B[l + 1], l + 1, 2, false);
+                const size_t P1 = static_cast<size_t>(buf.specs[l + 1].first) * buf.specs[l + 1].second;
+                cudaMemsetAsync(buf.U[l + 1], 0, 2 * P1 * batch * sizeof(T), s);
+            }
+            coarse_cycle(fused);
+            for (size_t l = fused; l-- > start;) {
+                resize(buf.U[l + 1], l + 1, buf.U[l], l, 2, true);
+                relax(l);
+            }
+            return;
+        }
         for (size_t l = start; l < last; ++l) {
             relax(l);
             const int nx = buf.specs[l].first, ny = buf.specs[l].second;
