@@ -117,7 +117,7 @@ def run_case(name: str) -> int:
             # stage 1 of the hemisphere mesh: one persistent launch of 49 passes plus the stage statistics
             from cat_surface_gpu_b200.features import _topology
 
-            rings = _topology(faces, meshes["surface"].shape[0], device)[:4]
+            rings = _topology(faces, meshes["surface"].shape[0], device)
             faces_device = torch.from_numpy(faces).to(device)
             base = torch.from_numpy(meshes["surface"]).to(device)
             for _ in range(3):
@@ -349,7 +349,7 @@ class Hemisphere:
         self.plan = self.topology.plan
         self.plan_device = self.plan.to_device(device)
         self.faces_device = torch.from_numpy(faces).to(device)
-        self.rings = _topology(faces, meshes["surface"].shape[0], device)[:4]
+        self.rings = _topology(faces, meshes["surface"].shape[0], device)
         self.pristine = torch.from_numpy(meshes["surface"]).to(device)
         self.points = torch.empty_like(self.pristine)
         prefix_radius = projection_radius(meshes["prefix"])
@@ -403,8 +403,8 @@ class Hemisphere:
                 raise RuntimeError(f"{what} kernel status {status} at {where}")
 
 
-def hemisphere_e2e(meshes, device, dartel_dtype, workdir: Path) -> tuple[float, int, int]:
-    """One hemisphere through the public API with host buffers and GIFTI files; returns (s, h2d, d2h).
+def hemisphere_e2e(meshes, device, dartel_dtype, workdir: Path) -> tuple[float, int, int, dict]:
+    """One hemisphere through the public API with host buffers and GIFTI files; returns (s, h2d, d2h, split).
 
     ``run_cat_surf2sphere_gpu`` (every stage on the GPU) from the surface
     file to the sphere file, then ``run_cat_surface_gpu_pipeline`` on the four
@@ -420,18 +420,23 @@ def hemisphere_e2e(meshes, device, dartel_dtype, workdir: Path) -> tuple[float, 
     start = time.perf_counter()
     sphere = run_cat_surf2sphere_gpu(workdir / "source_surface.gii", workdir / "source_sphere.gii", stop_at=10,
                                      preprocess_kernel="triton", device=device)
+    torch.cuda.synchronize()
+    split = time.perf_counter()
     result = run_cat_surface_gpu_pipeline(
         workdir / "source_surface.gii", workdir / "source_sphere.gii", workdir / "target_surface.gii",
         workdir / "target_sphere.gii", workdir / "registered.gii", device=device, dartel_dtype=dartel_dtype,
         stencil_threads=min(64, os.cpu_count() or 8), **CHAIN)
     torch.cuda.synchronize()
     seconds = time.perf_counter() - start
+    parts = {"surf2sphere_s": split - start, "surfwarp_s": seconds - (split - start)}
+    parts.update({f"surf2sphere.{k}": float(v) for k, v in sphere.timings.items()})
+    parts.update({f"surfwarp.{k}": float(v) for k, v in result.timings.items()})
     surface = meshes["surface"]
     # inputs copied to the device: the surface twice (Surf2Sphere, SurfWarp), the sphere, the target mesh
     h2d = 2 * surface.nbytes + sphere.vertices.nbytes + meshes["target_surface"].nbytes + meshes["target_sphere"].nbytes
     h2d += 2 * meshes["faces"].nbytes + meshes["target_faces"].nbytes
     d2h = sphere.vertices.nbytes + result.vertices.nbytes
-    return seconds, int(h2d), int(d2h)
+    return seconds, int(h2d), int(d2h), parts
 
 
 def batched_rotation_leg(device) -> dict:
@@ -649,7 +654,8 @@ def run_native(args):
         if world > 1:
             dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
         e2e = {"value": float(e2e_total.item()) / (len(runs) * world), "unit": UNIT,
-               "h2d_bytes_per_step": runs[0][1], "d2h_bytes_per_step": runs[0][2]}
+               "h2d_bytes_per_step": runs[0][1], "d2h_bytes_per_step": runs[0][2],
+               "split_s": {k: sum(r[3].get(k, 0.0) for r in runs) / len(runs) for k in runs[0][3]}}
 
     batched = {}
     if not args.no_batched:

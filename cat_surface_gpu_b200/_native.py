@@ -36,8 +36,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_kernel_launches": (ctypes.c_longlong, []),
     "csg_selftest_div3": (_I, [_P, ctypes.c_longlong, _P, _P, _P]),
     "csg_preprocess_scratch_bytes": (c_size_t, [_I, _I]),
-    "csg_surf2sphere_preprocess": (_I, [_P, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, c_size_t, _I, _I,
-                                        _I, ctypes.c_double, _P]),
+    "csg_surf2sphere_preprocess": (_I, [_P, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, c_size_t, _I,
+                                        _I, _I, ctypes.c_double, _P]),
     "csg_mesh_incidence": (_I, [_I, _P, _I, _P, _P]),
     "csg_mesh_neighbours": (_I, [_I, _P, _I, _P, _P, _I]),
     "csg_dependency_levels": (_I, [_I, _P, _P, _P]),

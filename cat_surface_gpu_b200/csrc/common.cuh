@@ -67,13 +67,16 @@ __device__ __forceinline__ void red_release_gpu_add(unsigned int* p, unsigned in
 // identically by every CTA.  Waits are bounded by `timeout_ns`; on timeout or
 // when another CTA has already reported an error the barrier returns true
 // and the caller must leave the kernel.  No trap, no unbounded spin.
+// Ordering: __syncthreads orders the CTA's writes before thread 0's arrival,
+// a release at gpu scope (cumulative, so it covers what thread 0 has
+// observed through the CTA barrier); the acquire poll and the closing
+// __syncthreads order the other CTAs' writes before this CTA's next reads.
 __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int& phase, unsigned long long timeout_ns,
                                              int where) {
     __shared__ int s_abort;
     __syncthreads();
     phase += gridDim.x;
     if (threadIdx.x == 0) {
-        __threadfence();
         red_release_gpu_add(&ctl->arrivals, 1u);
         int abort = 0;
         unsigned long long start = global_timer_ns();

@@ -8,11 +8,12 @@
 // distortion selection and `finger_iterations - 1` passes over the selected
 // vertices.  The passes are Gauss-Seidel in vertex index order -- the order
 // the upstream binary uses (the reference's Triton path colours instead) --
-// so they run as one persistent cooperative wavefront kernel per group of
-// passes, with the same schedule as the area-smoothing sweeps (vertex v of
-// pass s at step s * D + level(v); the 1-ring is the dependency set of both).
-// The per-stage global steps (centre, extents, face/vertex areas, the
-// distortion selection, the inflation) are plain kernels between them.
+// so they run as persistent cooperative wavefront kernels with the same
+// schedule as the area-smoothing sweeps (vertex v of pass s at step
+// s * D + level(v); the 1-ring is the dependency set of both).  The inflation
+// is a pointwise pass of the same wavefront.  The global steps (centre,
+// extents, face/vertex areas, the distortion selection) are plain kernels
+// between launches: 19 wavefront launches for stages 1-5.
 //
 // Arithmetic: float32 positions, float64 arithmetic (one rounding per
 // operation, --fmad=false).  Sums over all vertices or faces are blocked:
@@ -64,11 +65,27 @@ __device__ __forceinline__ float4 ld4(const float4* p, int v) { return __ldcg(p 
 
 // ---------------------------------------------------------------- passes
 
+// A launch runs a list of segments back to back: a run of smoothing passes
+// (over every vertex or over the selected ones) or one inflation pass.  The
+// inflation scale is pointwise with stage-fixed statistics, so it is a pass of
+// the same wavefront: vertex v is scaled after its own last smoothing pass and
+// before any neighbour's next pass reads it, which is the order a separate
+// kernel between two launches gives, without the pipeline drain in between.
+enum SegmentKind : int { kSmoothAll = 0, kSmoothSelected = 1, kInflate = 2 };
+constexpr int kMaxSegments = 8;
+
+struct Segment {
+    int first_pass;  // passes of earlier segments
+    int kind;
+    double value;  // smoothing strength, or the inflation's delta
+};
+
 struct PassParams {
     float4* work;
     const int* nb_off;
     const int* nb;
-    const unsigned char* selected;  // nullable: every vertex
+    const unsigned char* selected;
+    const Stats* st;
     const int* order;
     const int* level_begin;
     const int* level_end;
@@ -77,26 +94,37 @@ struct PassParams {
     int n_levels;
     int stride;
     int passes;
-    double strength;
+    int n_segments;
+    int max_degree;  // largest 1-ring (shared-memory variant)
+    int nloc_max;    // most vertices one CTA owns (shared-memory variant)
+    Segment seg[kMaxSegments];
     unsigned long long timeout_ns;
 };
 
-// One vertex of one pass by a group of G lanes: lane j computes neighbour
-// slots j, j + G, ... (L1 distance d, d q when d > 0), the terms are staged in
-// shared memory and lanes 0..2 sum them in slot order (total and one
-// coordinate each) and form that coordinate; lane 0 stores.
+__device__ __forceinline__ void inflate_vertex(float4* work, int v, const Stats* st, double delta) {
+    const float4 q = ld4(work, v);
+    const double x = __ddiv_rn(q.x, st->extent[0]), y = __ddiv_rn(q.y, st->extent[1]), z = __ddiv_rn(q.z, st->extent[2]);
+    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+    const double scale = __dadd_rn(1.0, __dmul_rn(delta, __dsub_rn(1.0, r)));
+    __stcg(work + v, make_float4(__double2float_rn(__dmul_rn(q.x, scale)), __double2float_rn(__dmul_rn(q.y, scale)),
+                                 __double2float_rn(__dmul_rn(q.z, scale)), 0.0f));
+}
+
+// One vertex of one pass of segment `sg` by a group of G lanes: lane j
+// computes neighbour slots j, j + G, ... (L1 distance d, d q when d > 0), the
+// terms are staged in shared memory and lanes 0..2 sum them in slot order
+// (total and one coordinate each) and form that coordinate; lane 0 stores.
+// An inflation segment scales the vertex by lane 0.  Groups of one warp may be
+// in different segments; every lane takes the warp-wide steps.
 template <int G>
-__device__ __forceinline__ void smooth_vertex(const PassParams& p, int v, double (*stage)[32]) {
+__device__ __forceinline__ void smooth_vertex(const PassParams& p, int v, const int* ring, int deg, int sg,
+                                              double (*stage)[32]) {
     const int lane = threadIdx.x & 31;
     const int glane = lane & (G - 1);
     const int gbase = lane & ~(G - 1);
-    int b = 0, deg = 0;
-    bool active = v >= 0;
-    if (active) {
-        b = __ldg(p.nb_off + v);
-        deg = __ldg(p.nb_off + v + 1) - b;
-        active = deg > 1 && (!p.selected || p.selected[v]);
-    }
+    const int kind = p.seg[sg].kind;
+    const double strength = p.seg[sg].value;
+    bool active = v >= 0 && kind != kInflate && deg > 1 && (kind == kSmoothAll || p.selected[v]);
     if (!active) deg = 0;
     const int wdeg = __reduce_max_sync(kFull, deg);
     double o[3] = {0.0, 0.0, 0.0};
@@ -112,7 +140,7 @@ __device__ __forceinline__ void smooth_vertex(const PassParams& p, int v, double
         const int j = c0 + glane;
         double d = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
         if (j < deg) {
-            const float4 q = ld4(p.work, __ldg(p.nb + b + j));
+            const float4 q = ld4(p.work, ring[j]);
             const double qx = q.x, qy = q.y, qz = q.z;
             d = __dadd_rn(__dadd_rn(fabs(__dsub_rn(qx, o[0])), fabs(__dsub_rn(qy, o[1]))), fabs(__dsub_rn(qz, o[2])));
             if (d > 0.0) {
@@ -139,22 +167,27 @@ __device__ __forceinline__ void smooth_vertex(const PassParams& p, int v, double
         }
         __syncwarp();
     }
-    const double inv = 1.0 - p.strength;
+    const double inv = 1.0 - strength;
     float c = 0.0f;
     if (active && glane < 3) {
         const double keep = __dmul_rn(o[comp], inv);
-        c = __double2float_rn(total > 0.0 ? __dadd_rn(keep, __dmul_rn(__ddiv_rn(wsum, total), p.strength)) : keep);
+        c = __double2float_rn(total > 0.0 ? __dadd_rn(keep, __dmul_rn(__ddiv_rn(wsum, total), strength)) : keep);
     }
     const float cy = __shfl_sync(kFull, c, gbase + 1);
     const float cz = __shfl_sync(kFull, c, gbase + 2);
     if (active && glane == 0) __stcg(p.work + v, make_float4(c, cy, cz, 0.0f));
+    if (kind == kInflate && v >= 0 && glane == 0) inflate_vertex(p.work, v, p.st, strength);
 }
 
 __device__ __forceinline__ int owned_below(int bound, int c, int nc) { return bound > c ? (bound - c + nc - 1) / nc : 0; }
 
-// `passes` Gauss-Seidel passes as one wavefront (see the file comment).
-template <int G>
+// `passes` passes (the segments' runs back to back) as one wavefront (see
+// the file comment).  CTA c owns order positions c, c + nc, ...  With SMEM the
+// CTA first copies its vertices' ids and 1-rings and its per-level owned
+// ranges into shared memory, so a step's only global loads are the positions.
+template <int G, bool SMEM>
 __global__ void __launch_bounds__(512) smooth_passes_kernel(PassParams p) {
+    extern __shared__ int smem[];
     __shared__ double stage_all[512 / 32][4][32];
     double (*stage)[32] = stage_all[threadIdx.x >> 5];
     const int c = blockIdx.x, nc = gridDim.x;
@@ -162,6 +195,35 @@ __global__ void __launch_bounds__(512) smooth_passes_kernel(PassParams p) {
     const int warp_first_group = (threadIdx.x >> 5) * (32 / G);
     const int my_group = (threadIdx.x & 31) / G;
     const int L = p.n_levels, D = p.stride;
+    // shared-memory image: rings [nloc_max][max_degree], ids, degrees, and the
+    // owned index range of every level
+    int* lring = smem;
+    int* lvid = lring + (SMEM ? p.nloc_max * p.max_degree : 0);
+    int* ldeg = lvid + p.nloc_max;
+    int* lbeg = ldeg + p.nloc_max;
+    int* lend = lbeg + L;
+    if (SMEM) {
+        const int nloc = owned_below(p.n, c, nc);
+        for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
+            const int v = __ldg(p.order + c + i * nc);
+            const int b = __ldg(p.nb_off + v);
+            int d = __ldg(p.nb_off + v + 1) - b;
+            if (d > p.max_degree) {
+                // a ring longer than the caller's max_degree: report it and
+                // keep the copy inside the image
+                if (atomicCAS(&p.ctl->status, CSG_OK, CSG_ERR_ARG) == CSG_OK) p.ctl->where = -1;
+                d = p.max_degree;
+            }
+            lvid[i] = v;
+            ldeg[i] = d;
+            for (int j = 0; j < d; ++j) lring[i * p.max_degree + j] = __ldg(p.nb + b + j);
+        }
+        for (int l = threadIdx.x; l < L; l += blockDim.x) {
+            lbeg[l] = owned_below(__ldg(p.level_begin + l), c, nc);
+            lend[l] = owned_below(__ldg(p.level_end + l), c, nc);
+        }
+        __syncthreads();
+    }
     unsigned int phase = 0;
     int barrier_id = 0;
     const int span = (p.passes - 1) * D;  // host guarantees span + L < 2^31
@@ -172,12 +234,41 @@ __global__ void __launch_bounds__(512) smooth_passes_kernel(PassParams p) {
         if (lo < r) lo = r;
         const int hi = t < L ? t : (L - 1) - ((L - 1 - r) % D + D) % D;
         if (hi >= lo) {
-            const int i0 = owned_below(__ldg(p.level_begin + lo), c, nc);
-            const int i1 = owned_below(__ldg(p.level_end + hi), c, nc);
+            const int i0 = SMEM ? lbeg[lo] : owned_below(__ldg(p.level_begin + lo), c, nc);
+            const int i1 = SMEM ? lend[hi] : owned_below(__ldg(p.level_end + hi), c, nc);
+            // Vertex v is in pass (t - level(v)) / D, so it has reached segment k
+            // when level(v) <= t - first_pass_k * D; the range is sorted by
+            // level, so that is every owned index below ib[k].
+            int ib[kMaxSegments];
+#pragma unroll
+            for (int k = 1; k < kMaxSegments; ++k) {
+                ib[k] = 0;
+                if (k < p.n_segments) {
+                    const int m = t - p.seg[k].first_pass * D;
+                    ib[k] = m < lo ? i0
+                                   : (m >= hi ? i1 : (SMEM ? lend[m] : owned_below(__ldg(p.level_end + m), c, nc)));
+                }
+            }
             for (int base = i0 + warp_first_group; base < i1; base += groups) {
                 const int i = base + my_group;
-                const int v = i < i1 ? __ldg(p.order + c + i * nc) : -1;
-                smooth_vertex<G>(p, v, stage);
+                int v = -1, deg = 0;
+                const int* ring = nullptr;
+                if (i < i1) {
+                    if (SMEM) {
+                        v = lvid[i];
+                        deg = ldeg[i];
+                        ring = lring + i * p.max_degree;
+                    } else {
+                        v = __ldg(p.order + c + i * nc);
+                        const int b = __ldg(p.nb_off + v);
+                        deg = __ldg(p.nb_off + v + 1) - b;
+                        ring = p.nb + b;
+                    }
+                }
+                int sg = 0;
+#pragma unroll
+                for (int k = 1; k < kMaxSegments; ++k) sg += i < ib[k];
+                smooth_vertex<G>(p, v, ring, deg, sg, stage);
             }
         }
         if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
@@ -292,17 +383,6 @@ __global__ void k_vertex_areas(const double* __restrict__ area, const int* __res
     va[v] = s;
 }
 
-__global__ void k_inflate(float4* __restrict__ work, int n, const Stats* __restrict__ st, double delta) {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const float4 q = work[v];
-    const double x = __ddiv_rn(q.x, st->extent[0]), y = __ddiv_rn(q.y, st->extent[1]), z = __ddiv_rn(q.z, st->extent[2]);
-    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
-    const double scale = __dadd_rn(1.0, __dmul_rn(delta, __dsub_rn(1.0, r)));
-    work[v] = make_float4(__double2float_rn(__dmul_rn(q.x, scale)), __double2float_rn(__dmul_rn(q.y, scale)),
-                          __double2float_rn(__dmul_rn(q.z, scale)), 0.0f);
-}
-
 __device__ __forceinline__ double dist3(const float4& a, const float4& b) {
     const double x = __dsub_rn(b.x, a.x), y = __dsub_rn(b.y, a.y), z = __dsub_rn(b.z, a.z);
     return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
@@ -371,39 +451,76 @@ Layout layout(int n, int nf) {
     return L;
 }
 
-template <int G>
-int launch_passes(const PassParams& params, int n_ctas, int threads, cudaStream_t s) {
-    auto kernel = smooth_passes_kernel<G>;
+constexpr size_t kMaxTopologySmem = 160 * 1024;
+
+template <int G, bool SMEM>
+int launch_variant(const PassParams& params, int n_ctas, int threads, size_t smem, cudaStream_t s) {
+    auto kernel = smooth_passes_kernel<G, SMEM>;
     int device = 0, sms = 0, per_sm = 0;
     CSG_CUDA_CHECK(cudaGetDevice(&device));
     CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
-    if (n_ctas <= 0) n_ctas = sms;
+    if (SMEM) CSG_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
     if (per_sm < 1 || n_ctas > per_sm * sms)
-        return csg::fail(CSG_ERR_LAUNCH, "preprocess passes: %d CTAs x %d threads cannot be co-resident", n_ctas, threads);
+        return csg::fail(CSG_ERR_LAUNCH, "preprocess passes: %d CTAs x %d threads (%zu B smem) cannot be co-resident",
+                         n_ctas, threads, smem);
     PassParams p = params;
     void* args[] = {&p};
     CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(n_ctas), dim3(threads), args,
-                                               0, s));
+                                               smem, s));
     csg::note_launch();
     return CSG_OK;
 }
 
-int run_passes(PassParams p, int passes, double strength, const unsigned char* selected, int n_ctas, int threads,
-               int lanes, cudaStream_t s) {
-    if (passes <= 0) return CSG_OK;
-    // every launch counts its barrier arrivals from zero; the status word is
-    // kept, so a launch after a timed-out one leaves at its first barrier
-    CSG_CUDA_CHECK(cudaMemsetAsync(&p.ctl->arrivals, 0, sizeof(p.ctl->arrivals), s));
-    p.passes = passes;
-    p.strength = strength;
-    p.selected = selected;
-    switch (lanes) {
-        case 4: return launch_passes<4>(p, n_ctas, threads, s);
-        case 16: return launch_passes<16>(p, n_ctas, threads, s);
-        default: return launch_passes<8>(p, n_ctas, threads, s);
-    }
+template <int G>
+int launch_passes(PassParams params, int n_ctas, int threads, cudaStream_t s) {
+    int device = 0, sms = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    if (n_ctas <= 0) n_ctas = sms;
+    params.nloc_max = (params.n + n_ctas - 1) / n_ctas;
+    const size_t smem = sizeof(int) * (static_cast<size_t>(params.nloc_max) * (params.max_degree + 2) +
+                                       2 * static_cast<size_t>(params.n_levels));
+    if (params.max_degree > 0 && smem <= kMaxTopologySmem) return launch_variant<G, true>(params, n_ctas, threads, smem, s);
+    return launch_variant<G, false>(params, n_ctas, threads, 0, s);
 }
+
+// The passes queued since the last launch, launched as one wavefront.
+struct PassQueue {
+    PassParams p;
+    int n_ctas, threads, lanes;
+    cudaStream_t s;
+
+    int add(int passes, int kind, double value) {
+        if (passes <= 0) return CSG_OK;
+        if (p.n_segments == kMaxSegments) {
+            const int rc = launch();
+            if (rc) return rc;
+        }
+        Segment& g = p.seg[p.n_segments++];
+        g.first_pass = p.passes;
+        g.kind = kind;
+        g.value = value;
+        p.passes += passes;
+        return CSG_OK;
+    }
+
+    int launch() {
+        if (p.passes <= 0) return CSG_OK;
+        // every launch counts its barrier arrivals from zero; the status word is
+        // kept, so a launch after a timed-out one leaves at its first barrier
+        CSG_CUDA_CHECK(cudaMemsetAsync(&p.ctl->arrivals, 0, sizeof(p.ctl->arrivals), s));
+        int rc;
+        switch (lanes) {
+            case 4: rc = launch_passes<4>(p, n_ctas, threads, s); break;
+            case 16: rc = launch_passes<16>(p, n_ctas, threads, s); break;
+            default: rc = launch_passes<8>(p, n_ctas, threads, s); break;
+        }
+        p.passes = 0;
+        p.n_segments = 0;
+        return rc;
+    }
+};
 
 inline unsigned blocks(long long n, int threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
 
@@ -419,10 +536,10 @@ size_t csg_preprocess_scratch_bytes(int n_vertices, int n_faces) {
 int csg_surf2sphere_preprocess(float* points, int n, const int32_t* faces, int nf, const int32_t* nb_off,
                                const int32_t* nb, const int32_t* inc_off, const int32_t* inc, const int32_t* order,
                                const int32_t* level_begin, const int32_t* level_end, int n_levels, int level_stride,
-                               int stop_at, void* scratch, size_t scratch_bytes, int n_ctas, int threads_per_cta,
-                               int lanes_per_vertex, double timeout_s, csg_stream_t stream) {
+                               int max_degree, int stop_at, void* scratch, size_t scratch_bytes, int n_ctas,
+                               int threads_per_cta, int lanes_per_vertex, double timeout_s, csg_stream_t stream) {
     if (!points || n < 4 || !faces || nf < 4 || !nb_off || !nb || !inc_off || !inc || !order || !level_begin ||
-        !level_end || n_levels < 1 || level_stride < 1 || stop_at < 1 || stop_at > 5 || !scratch)
+        !level_end || n_levels < 1 || level_stride < 1 || max_degree < 0 || stop_at < 1 || stop_at > 5 || !scratch)
         return csg::fail(CSG_ERR_ARG, "preprocess: bad arguments (stop_at 1..5)");
     if (threads_per_cta <= 0) threads_per_cta = 512;
     if (threads_per_cta % 32 || threads_per_cta > 512) return csg::fail(CSG_ERR_ARG, "preprocess: threads 32..512, x32");
@@ -433,8 +550,9 @@ int csg_surf2sphere_preprocess(float* points, int n, const int32_t* faces, int n
     const Layout L = layout(n, nf);
     if (scratch_bytes < L.total) return csg::fail(CSG_ERR_ARG, "preprocess: scratch too small");
     const double factor = nf > 350000 ? static_cast<double>(nf) / 350000.0 : 1.0;
-    // every pass group's span (passes - 1) * stride + levels must stay below 2^31 steps
-    if (std::nearbyint(factor * 60.0) * static_cast<double>(level_stride) + n_levels >= 2147483647.0)
+    // every launch's span (passes - 1) * stride + levels must stay below 2^31
+    // steps; a launch holds at most kMaxSegments segments of <= 60 factor passes
+    if (kMaxSegments * std::nearbyint(factor * 60.0) * static_cast<double>(level_stride) + n_levels >= 2147483647.0)
         return csg::fail(CSG_ERR_ARG, "preprocess: schedule too long");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     char* base = static_cast<char*>(scratch);
@@ -450,19 +568,29 @@ int csg_surf2sphere_preprocess(float* points, int n, const int32_t* faces, int n
     auto* st = reinterpret_cast<Stats*>(base + L.stats);
     CSG_CUDA_CHECK(cudaMemsetAsync(ctl, 0, sizeof(csg::Control), s));
     (csg::note_launch(), k_pack<<<blocks(n, kThreads), kThreads, 0, s>>>(points, work, n));
-    PassParams pp{};
-    pp.work = work;
-    pp.nb_off = nb_off;
-    pp.nb = nb;
-    pp.order = order;
-    pp.level_begin = level_begin;
-    pp.level_end = level_end;
-    pp.ctl = ctl;
-    pp.n = n;
-    pp.n_levels = n_levels;
-    pp.stride = level_stride;
-    pp.timeout_ns = static_cast<unsigned long long>(timeout_s * 1e9);
+    PassQueue q{};
+    q.p.work = work;
+    q.p.nb_off = nb_off;
+    q.p.nb = nb;
+    q.p.selected = sel;
+    q.p.st = st;
+    q.p.order = order;
+    q.p.level_begin = level_begin;
+    q.p.level_end = level_end;
+    q.p.ctl = ctl;
+    q.p.n = n;
+    q.p.n_levels = n_levels;
+    q.p.stride = level_stride;
+    q.p.max_degree = max_degree;
+    q.p.timeout_ns = static_cast<unsigned long long>(timeout_s * 1e9);
+    q.n_ctas = n_ctas;
+    q.threads = threads_per_cta;
+    q.lanes = lanes_per_vertex;
+    q.s = s;
     const int vruns = (n + kBlockSum - 1) / kBlockSum, fruns = (nf + kBlockSum - 1) / kBlockSum;
+    // One launch runs at most: the previous cycle's selected passes, this
+    // cycle's passes and the inflation.  Global steps (stage statistics, the
+    // distortion selection) end a launch.
     for (int si = 0; si < stop_at; ++si) {
         const StageSpec spec = kStages[si];
         const int iterations = static_cast<int>(std::nearbyint(factor * spec.iterations));
@@ -476,10 +604,12 @@ int csg_surf2sphere_preprocess(float* points, int n, const int32_t* faces, int n
         (csg::note_launch(), k_vertex_areas<<<blocks(n, kThreads), kThreads, 0, s>>>(area, inc_off, inc, n, va_ref));
         const double delta = spec.inflation - 1.0;
         for (int cycle = 0; cycle < spec.cycles; ++cycle) {
-            int rc = run_passes(pp, iterations - 1, spec.strength, nullptr, n_ctas, threads_per_cta, lanes_per_vertex, s);
+            int rc = q.add(iterations - 1, kSmoothAll, spec.strength);
+            if (!rc) rc = q.add(1, kInflate, delta);
             if (rc) return rc;
-            (csg::note_launch(), k_inflate<<<blocks(n, kThreads), kThreads, 0, s>>>(work, n, st, delta));
             if (finger > 0) {
+                rc = q.launch();
+                if (rc) return rc;
                 (csg::note_launch(), k_face_areas<<<blocks(nf, kThreads), kThreads, 0, s>>>(work, faces, nf, area));
                 (csg::note_launch(), k_run_sums<<<blocks(fruns, kThreads), kThreads, 0, s>>>(area, nf, partial));
                 (csg::note_launch(), k_finish_sum<<<1, 32, 0, s>>>(partial, fruns, &st->cur_surface));
@@ -489,11 +619,12 @@ int csg_surf2sphere_preprocess(float* points, int n, const int32_t* faces, int n
                                                                                        va_ref, n, st, comp));
                 (csg::note_launch(), k_select<<<blocks(n, kThreads), kThreads, 0, s>>>(comp, nb_off, nb, n,
                                                                                    spec.threshold, sel));
-                rc = run_passes(pp, finger - 1, spec.finger_strength, sel, n_ctas, threads_per_cta, lanes_per_vertex,
-                                s);
+                rc = q.add(finger - 1, kSmoothSelected, spec.finger_strength);
                 if (rc) return rc;
             }
         }
+        int rc = q.launch();
+        if (rc) return rc;
     }
     (csg::note_launch(), k_unpack<<<blocks(n, kThreads), kThreads, 0, s>>>(work, points, n));
     CSG_CUDA_CHECK(cudaGetLastError());

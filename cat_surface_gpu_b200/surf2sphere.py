@@ -398,9 +398,11 @@ def preprocess_device(
 ) -> torch.Tensor:
     """Stages 1..stop_at in place on a float32 device tensor (no host synchronisation, no ellipsoid step).
 
-    ``topology_device`` is ``(nb_off, nb, inc_off, inc)`` on the device (the
-    1-ring CSR and the corner-sorted incidences).  Returns the scratch tensor
-    whose first 256 bytes hold the status word (:func:`read_status`).
+    ``topology_device`` is ``(nb_off, nb, inc_off, inc[, max_degree])`` on
+    the device (the 1-ring CSR, the corner-sorted incidences and the largest
+    1-ring, which lets the kernel keep the rings in shared memory).  Returns
+    the scratch tensor whose first 256 bytes hold the status word
+    (:func:`read_status`).
     """
 
     n, nf = int(points.shape[0]), int(faces_device.shape[0])
@@ -412,11 +414,12 @@ def preprocess_device(
     if launch:
         cfg.update(launch)
     nb_off, nb, inc_off, inc = topology_device[:4]
+    max_degree = int(topology_device[4]) if len(topology_device) > 4 else 0
     _native.check(lib.csg_surf2sphere_preprocess(
         _native.ptr(points), n, _native.ptr(faces_device), nf, _native.ptr(nb_off), _native.ptr(nb),
         _native.ptr(inc_off), _native.ptr(inc), _native.ptr(plan_device["order"]),
         _native.ptr(plan_device["level_begin"]), _native.ptr(plan_device["level_end"]), plan.n_levels,
-        plan.level_stride, int(stop_at), _native.ptr(scratch), scratch.numel(), int(cfg["n_ctas"]),
+        plan.level_stride, max_degree, int(stop_at), _native.ptr(scratch), scratch.numel(), int(cfg["n_ctas"]),
         int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s), _native.stream_handle()),
         "csg_surf2sphere_preprocess")
     return scratch
@@ -473,13 +476,13 @@ def run_surf2sphere_preprocess_cuda(
         start = time.perf_counter()
         points = torch.from_numpy(points_host).to(target)
         face_dev = torch.from_numpy(tri).to(target)
-        nb_off, nb, inc_off, inc, _ = _topology(tri, n, target)
+        rings = _topology(tri, n, target)
         plan_device = plan.to_device(target)
         scratch = torch.empty(int(lib.csg_preprocess_scratch_bytes(n, nf)), dtype=torch.uint8, device=target)
         torch.cuda.synchronize(target)
         timings["preprocess_upload_seconds"] = time.perf_counter() - start
         start = time.perf_counter()
-        preprocess_device(points, face_dev, (nb_off, nb, inc_off, inc), plan_device, plan, stop_at=stop_at,
+        preprocess_device(points, face_dev, rings, plan_device, plan, stop_at=stop_at,
                           launch=cfg, timeout_s=timeout_s, scratch=scratch)
         status, where = read_status(scratch)
         if status != 0:

@@ -170,16 +170,22 @@ CSG_API int csg_selftest_barrier_timeout(void *scratch, size_t scratch_bytes, do
  * wavefront launches over the sweep schedule (order, level ranges, stride of
  * csg_areal_plan_build); nb_off/nb: unique ascending 1-ring; inc_off/inc:
  * per-vertex incidences face << 2 | corner sorted by (corner, face).
- * Float32 storage, float64 arithmetic.  Waits are bounded by timeout_s
- * (status CSG_ERR_TIMEOUT in the scratch's control block, read with
- * csg_read_status). */
+ * Float32 storage, float64 arithmetic.  The inflation is a pointwise pass of
+ * the same wavefront, so a launch ends only at a global step (stage
+ * statistics, distortion selection): 19 launches for stages 1-5.
+ * max_degree: the largest 1-ring (nb_off[v+1] - nb_off[v]); > 0 lets each
+ * CTA keep its vertices' rings in shared memory, 0 reads them from global
+ * memory.  A ring longer than max_degree sets status CSG_ERR_ARG.  Waits are
+ * bounded by timeout_s (status CSG_ERR_TIMEOUT in the scratch's control
+ * block, read with csg_read_status). */
 CSG_API size_t csg_preprocess_scratch_bytes(int n_vertices, int n_faces);
 CSG_API int csg_surf2sphere_preprocess(float *points, int n, const int32_t *faces, int n_faces,
                                        const int32_t *nb_off, const int32_t *nb, const int32_t *inc_off,
                                        const int32_t *inc, const int32_t *order, const int32_t *level_begin,
-                                       const int32_t *level_end, int n_levels, int level_stride, int stop_at,
-                                       void *scratch, size_t scratch_bytes, int n_ctas, int threads_per_cta,
-                                       int lanes_per_vertex, double timeout_s, csg_stream_t stream);
+                                       const int32_t *level_end, int n_levels, int level_stride, int max_degree,
+                                       int stop_at, void *scratch, size_t scratch_bytes, int n_ctas,
+                                       int threads_per_cta, int lanes_per_vertex, double timeout_s,
+                                       csg_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * SurfWarp: 2-D DARTEL on the lat-lon sheet (device, batched).

@@ -88,6 +88,36 @@ def test_gpu_preprocess_launch_shapes_agree(native_library):
 
 
 @pytest.mark.gpu
+def test_gpu_preprocess_shared_memory_rings_match_global_rings(native_library):
+    """Rings kept in shared memory (max_degree given) == rings read from global memory (max_degree 0);
+    a max_degree below the largest ring is reported as CSG_ERR_ARG in the status word."""
+
+    import torch
+
+    from cat_surface_gpu_b200 import surf2sphere
+    from cat_surface_gpu_b200.features import _topology
+    from cat_surface_gpu_b200.gifti import GiftiMesh
+
+    g = _golden("c1")
+    faces = g["faces"].astype(np.int32)
+    n = g["surface"].shape[0]
+    topology = surf2sphere.Surf2SphereTopology.from_mesh(GiftiMesh(g["surface"], faces))
+    plan = topology.plan
+    plan_device = plan.to_device("cuda:0")
+    rings = _topology(faces, n, torch.device("cuda:0"))
+    faces_device = torch.from_numpy(faces).to("cuda:0")
+    outs = []
+    for max_degree in (rings[4], 0, rings[4] - 1):
+        pts = torch.from_numpy(g["surface"]).to("cuda:0")
+        scratch = surf2sphere.preprocess_device(pts, faces_device, rings[:4] + (max_degree,), plan_device, plan,
+                                                stop_at=5)
+        outs.append((pts.cpu().numpy(), surf2sphere.read_status(scratch)[0]))
+    assert outs[0][1] == 0 and outs[1][1] == 0
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    assert outs[2][1] == -1  # CSG_ERR_ARG
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", ["c1", "c2"])
 def test_all_stages_on_gpu_match_binary(native_library, tmp_path, name):
     """Stages 1-5, 4,999 sweeps and the ellipsoid step on the GPU vs the upstream binary's stop_at=10 sphere."""
