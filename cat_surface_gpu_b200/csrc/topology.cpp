@@ -106,6 +106,39 @@ int csg_mesh_neighbours(int n_vertices, const int32_t* faces, int n_faces, int32
     return static_cast<int>(written);
 }
 
+int csg_colour_groups(int n_vertices, const int32_t* nbr_off, const int32_t* nbr, int32_t* colour_off,
+                      int32_t* members) {
+    if (n_vertices < 1 || !nbr_off || !nbr || !colour_off || !members) return csg::fail(CSG_ERR_ARG, "bad arguments");
+    // first fit in vertex order: the smallest colour no coloured neighbour has
+    std::vector<int32_t> colour(static_cast<size_t>(n_vertices), -1);
+    std::vector<int32_t> seen;  // seen[c] == v + 1: colour c is taken around v
+    int n_colours = 0;
+    for (int v = 0; v < n_vertices; ++v) {
+        const int b = nbr_off[v], e = nbr_off[v + 1];
+        if (b < 0 || e < b) return csg::fail(CSG_ERR_ARG, "neighbour offsets not ascending");
+        for (int k = b; k < e; ++k) {
+            const int w = nbr[k];
+            if (w < 0 || w >= n_vertices) return csg::fail(CSG_ERR_TOPOLOGY, "neighbour index out of range");
+            const int c = colour[w];
+            if (c >= 0) {
+                if (static_cast<size_t>(c) >= seen.size()) seen.resize(static_cast<size_t>(c) + 1, 0);
+                seen[c] = v + 1;
+            }
+        }
+        int c = 0;
+        while (static_cast<size_t>(c) < seen.size() && seen[c] == v + 1) ++c;
+        colour[v] = c;
+        if (c + 1 > n_colours) n_colours = c + 1;
+    }
+    // members by colour, ascending within each colour (counting sort)
+    std::fill(colour_off, colour_off + n_colours + 1, 0);
+    for (int v = 0; v < n_vertices; ++v) colour_off[colour[v] + 1]++;
+    for (int c = 0; c < n_colours; ++c) colour_off[c + 1] += colour_off[c];
+    std::vector<int32_t> fill(colour_off, colour_off + n_colours);
+    for (int v = 0; v < n_vertices; ++v) members[fill[colour[v]]++] = v;
+    return n_colours;
+}
+
 int csg_dependency_levels(int n_vertices, const int32_t* nbr_off, const int32_t* nbr, int32_t* levels) {
     if (n_vertices < 1 || !nbr_off || !levels) return csg::fail(CSG_ERR_ARG, "bad arguments");
     int count = 0;

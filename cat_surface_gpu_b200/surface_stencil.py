@@ -171,6 +171,13 @@ class SurfaceStencilDevice:
 
         return features.curvature_to_sheet(self, vertices, fwhm, curvtype)
 
+    def color_groups(self) -> tuple[torch.Tensor, ...]:
+        """Greedy first-fit colouring of the stencil mesh (reference 69-91, 333-347), one index tensor per colour."""
+
+        from .rotation_feature import _stencil_topology
+
+        return tuple(torch.as_tensor(g, device=self.faces.device) for g in _stencil_topology(self).groups)
+
 
 _RESAMPLING_SPHERES: dict[int, tuple[np.ndarray, np.ndarray]] = {}
 

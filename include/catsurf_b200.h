@@ -70,6 +70,15 @@ CSG_API int csg_mesh_incidence(int n_vertices, const int32_t *faces, int n_faces
 CSG_API int csg_mesh_neighbours(int n_vertices, const int32_t *faces, int n_faces, int32_t *nbr_off, int32_t *nbr,
                         int nbr_capacity);
 
+/* Greedy first-fit colouring in vertex order over a neighbour CSR: vertex v
+ * takes the smallest colour none of its already coloured neighbours has.
+ * Replaces _build_color_groups (src/cat_surface_gpu/surface_stencil.py:69-91).
+ * colour_off [n_vertices + 1] (first n_colours + 1 used), members
+ * [n_vertices] (each colour's vertices ascending).  Returns n_colours or a
+ * negative CSG_ERR_*. */
+CSG_API int csg_colour_groups(int n_vertices, const int32_t *nbr_off, const int32_t *nbr, int32_t *colour_off,
+                              int32_t *members);
+
 /* level(v) = 1 + max level of lower-index neighbours (0 if none).
  * Replaces _build_ordered_dependency_groups
  * (src/cat_surface_gpu/surface_stencil.py:94-109).  Returns the level count. */
@@ -186,6 +195,40 @@ CSG_API int csg_surf2sphere_preprocess(float *points, int n, const int32_t *face
                                        int stop_at, void *scratch, size_t scratch_bytes, int n_ctas,
                                        int threads_per_cta, int lanes_per_vertex, double timeout_s,
                                        csg_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * SurfWarp rotation feature: the depth potential (device, batched).
+ * Replaces compute_rotation_feature's solve (src/cat_surface_gpu/
+ * rotation_feature.py:37-317): stable normals, mixed Voronoi areas, the
+ * cotangent system (L + alpha A) u = (H - mean H) A with H the mean
+ * curvature, solved by coloured SOR (relaxation, max_iter sweeps) or
+ * Jacobi-preconditioned CG (max_iter, tolerance on |r| / |rhs|).
+ * geometry: device float32 [batch][n][3] (the smoothed coarse surfaces of one
+ * triangulation); faces [nf][3]; inc_off/inc: per-vertex incidences
+ * face << 2 | corner sorted by (corner, face) (csg_mesh_incidence order);
+ * max_incidences: the largest incidence count.  Rows sum in the order of the
+ * reference's CPU index_add_, so each row, normal, area and SOR sweep equals
+ * the reference's float64 CPU result; whole-vector sums are blocked (runs of
+ * 256, 32 lanes, pairwise) and do not depend on the launch shape.
+ * SOR needs the wavefront schedule of the colour-major order: relabel the
+ * vertices by (colour of csg_colour_groups, id), build csg_areal_plan_build's
+ * schedule on the relabelled faces, map its order back to the original ids.
+ * Outputs (device): values [batch][n] (the raw potential, before the
+ * reference's smoothing and min-max normalisation), iterations [batch],
+ * residual [batch] (|rhs - A u| / |rhs|); normals [batch][n][3] and areas
+ * [batch][n] when non-NULL.  alpha must be non-zero.  Waits are bounded by
+ * timeout_s (status in the scratch's control block, csg_read_status).
+ * ---------------------------------------------------------------------- */
+#define CSG_DEPTH_SOR 0
+#define CSG_DEPTH_PCG 1
+CSG_API size_t csg_depth_scratch_bytes(int n_vertices, int n_faces, int batch);
+CSG_API int csg_depth_potential(const float *geometry, int batch, int n, const int32_t *faces, int nf,
+                                const int32_t *inc_off, const int32_t *inc, int max_incidences, double alpha,
+                                int solver, int max_iter, double tolerance, double relaxation, const int32_t *order,
+                                const int32_t *level_begin, const int32_t *level_end, int n_levels,
+                                int level_stride, double *values, int32_t *iterations, double *residual,
+                                double *normals, double *areas, void *scratch, size_t scratch_bytes, int n_ctas,
+                                int threads_per_cta, int lanes_per_row, double timeout_s, csg_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * SurfWarp: 2-D DARTEL on the lat-lon sheet (device, batched).
