@@ -63,7 +63,8 @@ WORKLOAD = ("Surf2Sphere (stages 1-5 + 4,999 ordered sweeps, 61,442 v / 122,880 
             "to a second 61,442-v hull, 256x128 float64 DARTEL sheet")
 SWEEPS = 4999
 SHEET = (256, 128)
-CHAIN = dict(steps=2, runs=2, avg=True, loop=6, sheet_size=SHEET, rotation_feature_backend="native-curvature")
+CHAIN = dict(steps=2, runs=2, avg=True, loop=6, sheet_size=SHEET, rotation_feature_backend="cuda",
+             rotation_feature_solver="colored-sor")
 # stage counts of one hemisphere, for scaling the CPU samples
 DARTEL_STEPS = (CHAIN["runs"] + int(CHAIN["avg"])) * CHAIN["steps"] * CHAIN["loop"] * 3
 FEATURE_SIDES = 2 + 2 * (CHAIN["runs"] + int(CHAIN["avg"]))
@@ -258,7 +259,7 @@ def cpu_hemisphere_sample(meshes) -> dict:
 
     import numpy as np
 
-    from oracle import areal as oa, dartel as od, features as of, rotation as orot
+    from oracle import areal as oa, dartel as od, depth as odepth, features as of, rotation as orot
     from cat_surface_gpu_b200 import synthetic
     from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
 
@@ -290,6 +291,15 @@ def cpu_hemisphere_sample(meshes) -> dict:
     of.curvature_type5_to_sheet_many(mapped, stencil.faces, (5.0 / 9.0, 5.0 / 27.0), stencil.sheet_indices,
                                      stencil.sheet_weights)
     out["features"] = (time.perf_counter() - start) * FEATURE_SIDES
+    # depth-potential rotation features: per side the smoothing and the system, and 1,000 SOR sweeps
+    start = time.perf_counter()
+    smoothed = of.smooth_geometry(mapped, stencil.faces, 10.0)
+    system = odepth.System(smoothed, stencil.faces)
+    groups = odepth.colour_groups(stencil.faces, smoothed.shape[0])
+    setup = time.perf_counter() - start
+    start = time.perf_counter()
+    system.sor(groups, DEPTH_SAMPLE_SWEEPS)
+    out["rotation_features"] = 2 * setup + (time.perf_counter() - start) * 2 * DEPTH_SWEEPS / DEPTH_SAMPLE_SWEEPS
     values = of.curvature_type5(mapped, stencil.faces, 10.0)
     grid = orot.build_grid(stencil.sphere_points, stencil.faces)
     angles = np.random.default_rng(0).uniform(-0.3, 0.3, size=(2, 3))
@@ -301,9 +311,12 @@ def cpu_hemisphere_sample(meshes) -> dict:
     return out
 
 
+DEPTH_SWEEPS, DEPTH_SAMPLE_SWEEPS = 1000, 20
 CPU_SAMPLE = ("stages 1-5 in full and 200 of 4,999 sweeps (C port, 1 thread); 2 dartel_steps (k=0, 5) of the "
               f"{DARTEL_STEPS} per hemisphere (NumPy port); 1 stencil build of 6; 1 type-5 curvature sheet pair of "
-              f"{FEATURE_SIDES}; 2 rotation candidates of the reference search's count; each scaled linearly")
+              f"{FEATURE_SIDES}; depth features: 1 side's smoothing + system and {DEPTH_SAMPLE_SWEEPS} of "
+              f"{DEPTH_SWEEPS} SOR sweeps (C port) for 2 sides; 2 rotation candidates of the reference search's "
+              "count; each scaled linearly")
 
 
 def run_reference(args):

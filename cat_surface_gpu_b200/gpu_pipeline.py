@@ -9,10 +9,13 @@ between runs, the ``-avg`` pole-rotated solve and its blend, GIFTI output.
 Helpers: every stencil comes from ``stencil_builder`` -- a path to the
 reference's helper binary (as the reference runs it) or ``"native"`` (the
 host builder ``csg_stencil_build``).  Rotation features come from
-``rotation_values_path``, from the reference's helpers
-(``official-cpu`` / ``cuda-official-depth``), or from ``"native-curvature"``:
-the type-5 curvature of the resampled surfaces heat-smoothed with the
-reference's rotation FWHMs (15 source, 10 target) and min-max normalised.
+``rotation_values_path``; from the depth potential on the GPU (``"cuda"``, the
+reference's default that ``"auto"`` resolves to, or
+``"cuda-official-geometry"`` on the geometry helper's smoothed surfaces --
+``rotation_feature.py``); from the reference's helpers (``official-cpu`` /
+``cuda-official-depth``); or from ``"native-curvature"`` (an option of this
+package): the type-5 curvature of the resampled surfaces heat-smoothed with
+the rotation FWHMs (15 source, 10 target) and min-max normalised.
 """
 
 from __future__ import annotations
@@ -164,6 +167,51 @@ def native_rotation_features(source_stencil, target_stencil, source_surface, tar
     return out[0], out[1]
 
 
+def depth_rotation_features(source_stencil, target_stencil, source_surface, target_surface, device, *,
+                            solver: str = "colored-sor", smoothed_surfaces=None, depth_values=None,
+                            timings: dict | None = None):
+    """Depth-potential features of both sides (the reference's "cuda" backend, reference 836-893).
+
+    One batched solve for both sides on the stencils' shared triangulation;
+    returns the normalised device values (source, target).
+    """
+
+    from .rotation_feature import compute_rotation_features
+
+    stencils = [st.to(device, geometry_dtype=torch.float32) for st in (source_stencil, target_stencil)]
+    surfaces = [torch.as_tensor(np.asarray(v), dtype=torch.float32, device=device).contiguous()
+                for v in (source_surface, target_surface)]
+    results = compute_rotation_features(stencils, surfaces, heat_fwhms=(15.0, 10.0),
+                                        smoothed_surfaces=smoothed_surfaces, depth_values=depth_values, solver=solver)
+    if timings is not None:
+        for side, result in zip(("source", "target"), results):
+            timings[f"rotation_feature_{side}_iterations"] = float(result.iterations)
+            timings[f"rotation_feature_{side}_residual"] = float(result.relative_residual)
+    return results[0].values, results[1].values
+
+
+def _read_rotation_geometry(path) -> np.ndarray:
+    """``[i32 count, f64 xyz * count]`` coarse-feature geometry (reference 232-245)."""
+
+    raw = Path(path).read_bytes()
+    if len(raw) < 4:
+        raise ValueError(f"Coarse feature geometry file is too short: {path}")
+    count = int(np.frombuffer(raw, dtype=np.int32, count=1)[0])
+    if count <= 0 or len(raw) < 4 + 24 * count:
+        raise ValueError(f"Coarse feature geometry file has an invalid length: {path}")
+    return np.ascontiguousarray(np.frombuffer(raw, dtype=np.float64, count=3 * count, offset=4).reshape(count, 3),
+                                dtype=np.float32)
+
+
+def _probe_rotation_geometry(probe, surface_path, sphere_path, fwhm: float, output: Path) -> np.ndarray:
+    """Upstream coarse-feature geometry helper (reference 206-229)."""
+
+    _run_checked([probe, surface_path, sphere_path, str(float(fwhm)), output], "Upstream coarse feature geometry")
+    if not output.is_file() or output.stat().st_size < 4:
+        raise RuntimeError(f"Coarse feature geometry helper did not produce a valid file: {output}")
+    return _read_rotation_geometry(output)
+
+
 def _official_rotation_features(probe, paths, target_stencil, source_stencil, device, temp: Path, raw_depth: bool):
     output = temp / "rotation-values.bin"
     environment = None
@@ -190,12 +238,13 @@ def _official_rotation_features(probe, paths, target_stencil, source_stencil, de
 
 
 _BACKENDS = {"auto", "native-curvature", "cuda-official-depth", "official-cpu", "cuda", "cuda-official-geometry"}
+_SOLVERS = {"colored-sor", "pcg"}
 
 
 def _validate_options(*, steps=2, runs=1, stencil_threads=8, curvtypes=(5, 5, 2), fwhm=(5.0, 5.0 / 3.0, 5.0 / 9.0),
                       rotation_max_iter=500, rotation_tol=1.0e-4, rotation_simplex_step=0.1,
-                      rotation_feature_backend="auto", has_values=False, dartel_dtype=torch.float64, device="cuda",
-                      **_unused) -> None:
+                      rotation_feature_backend="auto", rotation_feature_solver="colored-sor", has_values=False,
+                      dartel_dtype=torch.float64, device="cuda", **_unused) -> None:
     """Argument checks of the reference pipeline (reference 514-560), before any file is read."""
 
     if steps < 1 or steps > 3:
@@ -210,10 +259,10 @@ def _validate_options(*, steps=2, runs=1, stencil_threads=8, curvtypes=(5, 5, 2)
         raise ValueError("rotation_max_iter, rotation_tol, and rotation_simplex_step must be positive")
     if rotation_feature_backend not in _BACKENDS:
         raise ValueError(f"rotation_feature_backend must be one of {sorted(_BACKENDS)}")
-    if rotation_feature_backend in {"cuda", "cuda-official-geometry"} and not has_values:
-        raise NotImplementedError(f"rotation_feature_backend={rotation_feature_backend!r} needs the depth-potential "
-                                  "solver, which this package does not implement; use 'native-curvature', "
-                                  "'cuda-official-depth' or provide rotation values")
+    if rotation_feature_solver not in _SOLVERS:
+        raise ValueError("rotation_feature_solver must be 'colored-sor' or 'pcg'")
+    if rotation_feature_backend in {"cuda-official-geometry", "cuda-official-depth"} and has_values:
+        raise ValueError("GPU official hybrid backend cannot rotation_values")
     _resolve_dartel_dtype(dartel_dtype)
     if device == "cpu" or str(device) == "cpu":
         raise ValueError("The explicit GPU pipeline requires a CUDA device")
@@ -281,16 +330,22 @@ def register_meshes(
     _validate_options(steps=steps, runs=runs, stencil_threads=stencil_threads, curvtypes=curvtypes, fwhm=fwhm,
                       rotation_max_iter=rotation_max_iter, rotation_tol=rotation_tol,
                       rotation_simplex_step=rotation_simplex_step, rotation_feature_backend=rotation_feature_backend,
-                      has_values=rotation_values is not None, dartel_dtype=dartel_dtype, device=device)
+                      rotation_feature_solver=rotation_feature_solver, has_values=rotation_values is not None,
+                      dartel_dtype=dartel_dtype, device=device)
     if rotation_feature_backend == "auto":
-        rotation_feature_backend = "official-cpu" if rotation_values_probe is not None else "native-curvature"
+        # the reference's resolution (reference 550-553)
+        rotation_feature_backend = "official-cpu" if rotation_values_probe is not None else "cuda"
+    if rotation_values is None and rotation_feature_backend == "cuda-official-geometry" \
+            and rotation_geometry_probe is None:
+        raise ValueError("cuda-official-geometry requires rotation_geometry_probe")
     solve_dtype = _resolve_dartel_dtype(dartel_dtype)
     target_device = resolve_device(device)
     if rotated_stencil_builder is None:
         rotated_stencil_builder = stencil_builder
     graph_requested = bool(cuda_graph and (runs + int(avg) >= 3))
     uses_files = (stencil_builder not in (None, "native") or rotated_stencil_builder not in (None, "native")
-                  or (rotation_values is None and rotation_feature_backend in {"official-cpu", "cuda-official-depth"}))
+                  or (rotation_values is None and rotation_feature_backend in {"official-cpu", "cuda-official-depth",
+                                                                                "cuda-official-geometry"}))
     if uses_files and paths is None:
         raise ValueError("helper stencil builders and feature probes need the input file paths")
     source_surface_path, source_sphere_path, target_surface_path, target_sphere_path = paths or (None,) * 4
@@ -325,9 +380,22 @@ def register_meshes(
                 raise ValueError("cuda-official-depth requires rotation_depth_probe")
             source_values, target_values = _official_rotation_features(
                 rotation_depth_probe, paths, target_stencil, source_stencil, target_device, temp, raw_depth=True)
-        else:
+        elif rotation_feature_backend == "cuda-official-geometry":
+            smoothed = tuple(_probe_rotation_geometry(rotation_geometry_probe, surface_path, sphere_path, fwhm,
+                                                      temp / f"rotation-geometry-{side}.bin")
+                             for side, surface_path, sphere_path, fwhm in (
+                                 ("source", source_surface_path, source_sphere_path, 15.0),
+                                 ("target", target_surface_path, target_sphere_path, 10.0)))
+            source_values, target_values = depth_rotation_features(
+                source_stencil, target_stencil, source_surface.vertices, target_surface.vertices, target_device,
+                solver=rotation_feature_solver, smoothed_surfaces=smoothed, timings=timings)
+        elif rotation_feature_backend == "native-curvature":
             source_values, target_values = native_rotation_features(
                 source_stencil, target_stencil, source_surface.vertices, target_surface.vertices, target_device)
+        else:
+            source_values, target_values = depth_rotation_features(
+                source_stencil, target_stencil, source_surface.vertices, target_surface.vertices, target_device,
+                solver=rotation_feature_solver, timings=timings)
         torch.cuda.synchronize(target_device)
         timings["rotation_feature_seconds"] = time.perf_counter() - start
 

@@ -4,15 +4,17 @@ Development container only (imports ``cat_surface_gpu`` from the reference
 checkout).  Follows ``src/cat_surface_gpu/gpu_pipeline.py:468-1326`` step by
 step with the reference's own operators on the CPU: stencils (built by this
 package's native host builder, read back through the reference's reader),
-rotation features (type-5 curvature of the resampled surfaces at FWHM 15 /
-10, the "native-curvature" backend), the 46-seed + Nelder-Mead rotation
-search, ``runs`` DARTEL solves with the inverse warp between runs, the
+rotation features (the reference's default "cuda" backend:
+``compute_rotation_features`` -- the depth potential by coloured SOR of the
+smoothed coarse surfaces at FWHM 15 / 10 -- run on the CPU), the 46-seed +
+Nelder-Mead rotation search, ``runs`` DARTEL solves with the inverse warp between runs, the
 pole-rotated ``-avg`` solve and the blend.
 
 Inputs: two folded icospheres (10,242 vertices, subdivision 5) with shared
 folding plus a per-subject perturbation; the source sphere is the unit
 icosphere under a known rotation, scaled to radius 100.  Writes
-``surfwarp_chain_golden.npz`` (inputs, parameters, rotation features,
+``surfwarp_chain_golden.npz`` (inputs, parameters, rotation features, the
+type-5 curvature features of this package's "native-curvature" option,
 rotation angle/cost, the rotated sphere, the sphere after run 0, the final
 sphere).
 
@@ -48,6 +50,7 @@ import torch  # noqa: E402
 
 from cat_surface_gpu.gpu_pipeline import (  # noqa: E402
     _average_xz_surfaces, _normalise_sphere, _rotate_vertices, _rotation_matrix_from_angles)
+from cat_surface_gpu.rotation_feature import compute_rotation_features  # noqa: E402
 from cat_surface_gpu.rotation_pipeline import RotationPipeline  # noqa: E402
 from cat_surface_gpu.surface_stencil import SurfaceStencil as ReferenceStencil  # noqa: E402
 from cat_surface_gpu.surface_warp import apply_flow_to_stenciled_sphere, solve_dartel_from_surfaces  # noqa: E402
@@ -101,12 +104,17 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size, ta
 
     source_stencil = stencil(data["source_sphere"], True)
     target_stencil = stencil(data["target_sphere"], True, target_faces)
-    values = []
+    curvature = []
     for st, surface, fwhm in ((source_stencil, data["source_surface"], 15.0),
                               (target_stencil, data["target_surface"], 10.0)):
         dev = on_cpu(st)
         mapped = dev.resample_vertices(torch.as_tensor(surface))
-        values.append(dev.curvature_type5(mapped, fwhm).numpy())
+        curvature.append(dev.curvature_type5(mapped, fwhm).numpy())
+    features = compute_rotation_features(
+        (on_cpu(source_stencil), on_cpu(target_stencil)),
+        (torch.as_tensor(data["source_surface"]), torch.as_tensor(data["target_surface"])), heat_fwhms=(15.0, 10.0),
+        solver="colored-sor")
+    values = [f.values.numpy() for f in features]
     pipeline = RotationPipeline.from_stencil(target_stencil, device=CPU, grid_size=rotation_grid_size, margin=1)
     evaluated = [0]
     plain_cost = pipeline.index.cost_batch_prepared
@@ -165,7 +173,8 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size, ta
         current_sphere = _average_xz_surfaces(unrotated, main_warped, device=CPU).numpy().astype(np.float32)
     return dict(rotation_angle=angle.astype(np.float64), rotation_cost=float(rotation.cost),
                 rotation_candidates_evaluated=np.int64(evaluated[0]),
-                source_values=values[0], target_values=values[1],
+                source_values=values[0], target_values=values[1], curv_source_values=curvature[0],
+                curv_target_values=curvature[1],
                 rotated_initial=rotated_initial, after_run0=after_run0, final_sphere=current_sphere)
 
 

@@ -2,7 +2,8 @@
 
 The golden (``tests/golden/make_surfwarp_chain_golden.py``) ran the reference
 package's operators on the CPU in the order of its ``run_cat_surface_gpu_pipeline``:
-native-builder stencils, type-5 curvature rotation features, the rotation
+native-builder stencils, the default ("cuda") rotation features -- the depth
+potential by coloured SOR, ``compute_rotation_features`` -- the rotation
 search, two DARTEL runs of two steps on a 128 x 64 sheet, the ``-avg`` solve
 and blend.  This runs ``run_cat_surface_gpu_pipeline`` on the same GIFTI
 inputs and bounds the final unit-sphere vertex error at 1e-3 (max), the
@@ -36,15 +37,23 @@ def _write_inputs(chain, directory):
 
 
 def test_rotation_features_match_reference(native_library, chain):
-    from cat_surface_gpu_b200.gpu_pipeline import native_rotation_features
+    """Depth-potential features (both sides in one batched solve) and the type-5 curvature option."""
+
+    from cat_surface_gpu_b200.gpu_pipeline import depth_rotation_features, native_rotation_features
     from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
 
     nx, ny = int(chain["param_nx"]), int(chain["param_ny"])
     stencils = [build_surface_stencil(chain[f"{side}_sphere"], chain["faces"], nx=nx, ny=ny, normalize=True)
                 for side in ("source", "target")]
+    timings = {}
+    values = depth_rotation_features(stencils[0], stencils[1], chain["source_surface"], chain["target_surface"],
+                                     torch.device("cuda:0"), timings=timings)
+    assert timings["rotation_feature_source_iterations"] == 1000.0
+    for got, want in zip(values, (chain["source_values"], chain["target_values"])):
+        np.testing.assert_allclose(got.cpu().numpy(), want, rtol=0, atol=1e-12)
     values = native_rotation_features(stencils[0], stencils[1], chain["source_surface"], chain["target_surface"],
                                       torch.device("cuda:0"))
-    for got, want in zip(values, (chain["source_values"], chain["target_values"])):
+    for got, want in zip(values, (chain["curv_source_values"], chain["curv_target_values"])):
         scale = float(np.abs(want).max())
         assert np.abs(got.astype(np.float64) - want).max() <= 1e-5 * scale
 
@@ -57,7 +66,7 @@ def test_surfwarp_chain_matches_reference(native_library, chain, tmp_path):
         paths["source_surface"], paths["source_sphere"], paths["target_surface"], paths["target_sphere"],
         tmp_path / "out.gii", device="cuda:0", steps=int(chain["param_steps"]), runs=int(chain["param_runs"]),
         avg=bool(chain["param_avg"]), loop=int(chain["param_loop"]),
-        rotation_grid_size=int(chain["param_rotation_grid_size"]), rotation_feature_backend="native-curvature",
+        rotation_grid_size=int(chain["param_rotation_grid_size"]),
         sheet_size=(int(chain["param_nx"]), int(chain["param_ny"])), stencil_threads=8,
     )
     assert np.abs(result.rotation_angle - chain["rotation_angle"]).max() <= 1e-4

@@ -124,3 +124,9 @@ def test_cli_dispatch_and_pipeline_argument_checks(tmp_path):
         run_cat_surface_gpu_pipeline(*paths, rotation_feature_backend="nope")
     with pytest.raises(ValueError):
         run_cat_surface_gpu_pipeline(*paths, device="cpu")
+    # reference 536-548: the solver name, and no provided values with the hybrid backends
+    with pytest.raises(ValueError):
+        run_cat_surface_gpu_pipeline(*paths, rotation_feature_solver="jacobi")
+    for backend in ("cuda-official-geometry", "cuda-official-depth"):
+        with pytest.raises(ValueError):
+            run_cat_surface_gpu_pipeline(*paths[:5], rotation_values_path=paths[0], rotation_feature_backend=backend)
