@@ -283,31 +283,36 @@ struct SorParams {
 
 __device__ __forceinline__ int owned_below(int bound, int c, int nc) { return bound > c ? (bound - c + nc - 1) / nc : 0; }
 
-// One row of one surface by a group of G lanes: lane j forms the products of
-// entries j, j + G, ...; lane 0 adds them in entry order (shuffles) and updates.
+// Row sum of one surface by a group of G lanes.  Lane j loads and multiplies
+// entries j, j + G, ..., j + (32 / G - 1) G of a block of 32 entries first (all
+// of a row's gathers in flight together), then the products are added in entry
+// order through shuffles; every lane of the group returns the sum.
 template <int G>
-__device__ __forceinline__ void sor_row(const SorParams& p, int b, int v, const int* rcol, const double* rval, int len) {
+__device__ __forceinline__ double sor_row_sum(const double* x, const int* rcol, const double* rval, int len) {
+    constexpr int kQ = 32 / G;
     const int lane = threadIdx.x & 31;
     const int glane = lane & (G - 1);
     const int gbase = lane & ~(G - 1);
-    const double* x = p.x + static_cast<long long>(b) * p.n;
     const int wlen = __reduce_max_sync(kFull, len);
     double s = 0.0;
-    for (int c0 = 0; c0 < wlen; c0 += G) {
-        const int j = c0 + glane;
-        double prod = 0.0;
-        if (j < len) prod = rval[j] * __ldcg(x + rcol[j]);
+    for (int base = 0; base < wlen; base += G * kQ) {
+        double prod[kQ];
 #pragma unroll
-        for (int q = 0; q < G; ++q) {
-            const double t = __shfl_sync(kFull, prod, gbase + q);
-            if (c0 + q < len) s = s + t;
+        for (int q = 0; q < kQ; ++q) {
+            const int j = base + q * G + glane;
+            prod[q] = j < len ? rval[j] * __ldcg(x + rcol[j]) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kQ; ++q) {
+            if (base + q * G >= wlen) break;  // warp-uniform
+#pragma unroll
+            for (int i = 0; i < G; ++i) {
+                const double t = __shfl_sync(kFull, prod[q], gbase + i);
+                if (base + q * G + i < len) s = s + t;
+            }
         }
     }
-    if (len > 0 && glane == 0) {
-        const long long at = static_cast<long long>(b) * p.n + v;
-        const double xv = __ldcg(p.x + at);
-        __stcg(p.x + at, xv + p.relaxation * (p.rhs[at] - s) / p.diag[at]);
-    }
+    return s;
 }
 
 template <int G, bool SMEM>
@@ -319,10 +324,16 @@ __global__ void __launch_bounds__(512) k_depth_sor(SorParams p) {
     const int warp_first_group = (threadIdx.x >> 5) * (32 / G);
     const int my_group = (threadIdx.x & 31) / G;
     const int L = p.n_levels, D = p.stride;
-    // shared-memory image: values [batch][nloc_max][max_row], columns
+    // shared-memory image: values [batch][nloc_max][max_row]; rhs, diagonal
+    // and current x of the owned vertices [batch][nloc_max] (x is written
+    // through to global memory for the other CTAs' gathers); columns
     // [nloc_max][max_row], vertex ids, row lengths, per-level owned ranges
+    const long long nb = static_cast<long long>(p.batch) * p.nloc_max;
     double* sval = reinterpret_cast<double*>(smem_raw);
-    int* scol = reinterpret_cast<int*>(sval + (SMEM ? static_cast<long long>(p.batch) * p.nloc_max * p.max_row : 0));
+    double* srhs = sval + (SMEM ? nb * p.max_row : 0);
+    double* sdiag = srhs + (SMEM ? nb : 0);
+    double* sx = sdiag + (SMEM ? nb : 0);
+    int* scol = reinterpret_cast<int*>(sx + (SMEM ? nb : 0));
     int* svid = scol + (SMEM ? p.nloc_max * p.max_row : 0);
     int* slen = svid + p.nloc_max;
     int* lbeg = slen + p.nloc_max;
@@ -340,9 +351,14 @@ __global__ void __launch_bounds__(512) k_depth_sor(SorParams p) {
             svid[i] = v;
             slen[i] = len;
             for (int j = 0; j < len; ++j) scol[i * p.max_row + j] = p.col[row + j];
-            for (int b = 0; b < p.batch; ++b)
-                for (int j = 0; j < len; ++j)
-                    sval[(static_cast<long long>(b) * p.nloc_max + i) * p.max_row + j] = p.val[b * p.nnz + row + j];
+            for (int b = 0; b < p.batch; ++b) {
+                const long long slot = static_cast<long long>(b) * p.nloc_max + i;
+                for (int j = 0; j < len; ++j) sval[slot * p.max_row + j] = p.val[b * p.nnz + row + j];
+                const long long at = static_cast<long long>(b) * p.n + v;
+                srhs[slot] = p.rhs[at];
+                sdiag[slot] = p.diag[at];
+                sx[slot] = p.x[at];
+            }
         }
         for (int l = threadIdx.x; l < L; l += blockDim.x) {
             lbeg[l] = owned_below(p.level_begin[l], c, nc);
@@ -366,25 +382,39 @@ __global__ void __launch_bounds__(512) k_depth_sor(SorParams p) {
             for (int base = warp_first_group; base < count * p.batch; base += groups) {
                 const int w = base + my_group;
                 int b = 0, i = -1, v = 0, len = 0;
+                long long slot = 0;
                 const int* rcol = nullptr;
                 const double* rval = nullptr;
+                double rhs = 0.0, diag = 1.0;
                 if (w < count * p.batch) {
                     b = w / count;
                     i = i0 + w % count;
+                    slot = static_cast<long long>(b) * p.nloc_max + i;
                     if (SMEM) {
                         v = svid[i];
                         len = slen[i];
                         rcol = scol + i * p.max_row;
-                        rval = sval + (static_cast<long long>(b) * p.nloc_max + i) * p.max_row;
+                        rval = sval + slot * p.max_row;
+                        rhs = srhs[slot];
+                        diag = sdiag[slot];
                     } else {
                         v = p.order[c + i * nc];
                         const long long row = 3LL * p.inc_off[v] + v;
                         len = 3 * (p.inc_off[v + 1] - p.inc_off[v]) + 1;
                         rcol = p.col + row;
                         rval = p.val + b * p.nnz + row;
+                        rhs = p.rhs[static_cast<long long>(b) * p.n + v];
+                        diag = p.diag[static_cast<long long>(b) * p.n + v];
                     }
                 }
-                sor_row<G>(p, b, v, rcol, rval, len);
+                const double sum = sor_row_sum<G>(p.x + static_cast<long long>(b) * p.n, rcol, rval, len);
+                if (len > 0 && (threadIdx.x & (G - 1)) == 0) {
+                    const long long at = static_cast<long long>(b) * p.n + v;
+                    const double xv = SMEM ? sx[slot] : __ldcg(p.x + at);
+                    const double nx = xv + p.relaxation * (rhs - sum) / diag;
+                    if (SMEM) sx[slot] = nx;
+                    __stcg(p.x + at, nx);
+                }
             }
         }
         if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
@@ -623,7 +653,7 @@ Layout layout(int n, int nf, int batch, long long nnz) {
 
 inline unsigned blocks(long long n, int threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
 
-constexpr size_t kMaxRowSmem = 160 * 1024;
+constexpr size_t kMaxRowSmem = 200 * 1024;
 
 template <int G, bool SMEM>
 int launch_sor(const SorParams& params, int n_ctas, int threads, size_t smem, cudaStream_t s) {
@@ -648,7 +678,7 @@ template <int G>
 int dispatch_sor(SorParams p, int n_ctas, int threads, cudaStream_t s) {
     p.nloc_max = (p.n + n_ctas - 1) / n_ctas;
     const size_t ints = static_cast<size_t>(p.nloc_max) * (p.max_row + 2) + 2 * static_cast<size_t>(p.n_levels);
-    const size_t smem = sizeof(double) * static_cast<size_t>(p.batch) * p.nloc_max * p.max_row + sizeof(int) * ints;
+    const size_t smem = sizeof(double) * static_cast<size_t>(p.batch) * p.nloc_max * (p.max_row + 3) + sizeof(int) * ints;
     if (p.max_row > 0 && smem <= kMaxRowSmem) return launch_sor<G, true>(p, n_ctas, threads, smem, s);
     p.max_row = 0;
     return launch_sor<G, false>(p, n_ctas, threads, 0, s);
@@ -685,7 +715,7 @@ int csg_depth_potential(const float* geometry, int batch, int n, const int32_t* 
         return csg::fail(CSG_ERR_ARG, "depth potential: schedule too long");
     if (threads_per_cta <= 0) threads_per_cta = 512;
     if (threads_per_cta % 32 || threads_per_cta > 512) return csg::fail(CSG_ERR_ARG, "depth potential: threads 32..512, x32");
-    if (lanes_per_row <= 0) lanes_per_row = 8;
+    if (lanes_per_row <= 0) lanes_per_row = 4;
     if (lanes_per_row != 4 && lanes_per_row != 8 && lanes_per_row != 16)
         return csg::fail(CSG_ERR_ARG, "depth potential: lanes_per_row must be 4, 8 or 16");
     if (timeout_s <= 0.0) timeout_s = 2.0;
@@ -751,9 +781,9 @@ int csg_depth_potential(const float* geometry, int batch, int n, const int32_t* 
             p.timeout_ns = timeout_ns;
             int rc;
             switch (lanes_per_row) {
-                case 4: rc = dispatch_sor<4>(p, n_ctas, threads_per_cta, s); break;
+                case 8: rc = dispatch_sor<8>(p, n_ctas, threads_per_cta, s); break;
                 case 16: rc = dispatch_sor<16>(p, n_ctas, threads_per_cta, s); break;
-                default: rc = dispatch_sor<8>(p, n_ctas, threads_per_cta, s); break;
+                default: rc = dispatch_sor<4>(p, n_ctas, threads_per_cta, s); break;
             }
             if (rc) return rc;
         }
