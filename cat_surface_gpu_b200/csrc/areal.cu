@@ -57,6 +57,7 @@ struct ArealParams {
     int nloc_max;  // vertices owned by one CTA (set at launch)
     int iterations;
     int project_every;
+    int allow_dataflow;  // float32 modes: published (value, version) words instead of per-step barriers
     double radius;
     unsigned long long timeout_ns;
 };
@@ -101,14 +102,16 @@ struct Traits<CSG_ARITH_CAT> {
                                __double2float_rn(__ddiv_rn(wz, safe)), 0.0f);
         __stcg(static_cast<float4*>(w) + v, q);
     }
-    static __device__ __forceinline__ void project(void* w, int v, double radius) {
-        float4 q = __ldcg(static_cast<float4*>(w) + v);
+    static __device__ __forceinline__ P3 project_p3(const P3& q, double radius) {
         float sq = __fadd_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.y, q.y)), __fmul_rn(q.z, q.z));
         double norm = __dsqrt_rn(static_cast<double>(sq));
         double scale = __ddiv_rn(radius, norm > 1.0e-20 ? norm : 1.0e-20);
-        q = make_float4(__double2float_rn(__dmul_rn((double)q.x, scale)), __double2float_rn(__dmul_rn((double)q.y, scale)),
-                        __double2float_rn(__dmul_rn((double)q.z, scale)), 0.0f);
-        __stcg(static_cast<float4*>(w) + v, q);
+        return {__double2float_rn(__dmul_rn((double)q.x, scale)), __double2float_rn(__dmul_rn((double)q.y, scale)),
+                __double2float_rn(__dmul_rn((double)q.z, scale))};
+    }
+    static __device__ __forceinline__ void project(void* w, int v, double radius) {
+        const P3 q = project_p3(load(w, v), radius);
+        __stcg(static_cast<float4*>(w) + v, make_float4(q.x, q.y, q.z, 0.0f));
     }
     static __device__ __forceinline__ void pack(const void* in, void* w, int v) {
         const float* p = static_cast<const float*>(in) + 3LL * v;
@@ -149,14 +152,16 @@ struct Traits<CSG_ARITH_FP32> {
         __stcg(static_cast<float4*>(w) + v,
                make_float4(__fdiv_rn(wx, safe), __fdiv_rn(wy, safe), __fdiv_rn(wz, safe), 0.0f));
     }
-    static __device__ __forceinline__ void project(void* w, int v, double radius) {
+    static __device__ __forceinline__ P3 project_p3(const P3& q, double radius) {
         const float r = static_cast<float>(radius);
-        float4 q = __ldcg(static_cast<float4*>(w) + v);
         float sq = __fadd_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.y, q.y)), __fmul_rn(q.z, q.z));
         float norm = __fsqrt_rn(sq);
         float scale = __fdiv_rn(r, norm > 1.0e-20f ? norm : 1.0e-20f);
-        __stcg(static_cast<float4*>(w) + v,
-               make_float4(__fmul_rn(q.x, scale), __fmul_rn(q.y, scale), __fmul_rn(q.z, scale), 0.0f));
+        return {__fmul_rn(q.x, scale), __fmul_rn(q.y, scale), __fmul_rn(q.z, scale)};
+    }
+    static __device__ __forceinline__ void project(void* w, int v, double radius) {
+        const P3 q = project_p3(load(w, v), radius);
+        __stcg(static_cast<float4*>(w) + v, make_float4(q.x, q.y, q.z, 0.0f));
     }
     static __device__ __forceinline__ void pack(const void* in, void* w, int v) { Traits<CSG_ARITH_CAT>::pack(in, w, v); }
     static __device__ __forceinline__ void unpack(const void* w, void* out, int v) {
@@ -438,6 +443,275 @@ __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
     for (int v = tid; v < p.n; v += nthreads) T::unpack(p.work, p.points, v);
 }
 
+// ---------------------------------------------------------------------------
+// Dataflow form of the sweeps (float32 storage modes).
+//
+// The grid barrier between wavefront steps is replaced by per-vertex versions.
+// Each coordinate of each vertex is published as one 8-byte word
+// (float32 bits | version << 32), version = the number of sweeps the vertex
+// has completed; 8-byte aligned accesses are single-copy atomic, so a word
+// read with a relaxed load carries a value and the version it belongs to.
+// Sweep s of vertex v needs lower-index neighbours at version s and
+// higher-index neighbours and v itself at version s - 1, and neither can be
+// further ahead: a lower neighbour u cannot finish sweep s + 1 before v
+// finishes sweep s (v > u is its higher neighbour), a higher neighbour w cannot
+// finish sweep s before v does.  So once every word shows its required version
+// the values are exactly the sequential Gauss-Seidel inputs, and the group
+// polls its faces' words until they do.  Each group walks the same wavefront
+// order as the barrier form (step t, then its share of the step's vertices),
+// which keeps progress guaranteed: the earliest unfinished update's inputs are
+// all finished.  Grid barriers remain around the projections only.
+// Every wait is bounded: on timeout (or another CTA's failure) the kernel
+// records the status and leaves.
+
+__device__ __forceinline__ unsigned long long ld_word(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_word(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long make_word(float x, unsigned int version) {
+    return (static_cast<unsigned long long>(version) << 32) | __float_as_uint(x);
+}
+__device__ __forceinline__ float word_value(unsigned long long w) { return __uint_as_float(static_cast<unsigned>(w)); }
+__device__ __forceinline__ unsigned int word_version(unsigned long long w) { return static_cast<unsigned>(w >> 32); }
+
+// words of vertex v: pub[4 v + k], k = 0, 1, 2 (coordinate k), 3 unused
+template <typename P3>
+__device__ __forceinline__ bool load_versioned(const unsigned long long* pub, int u, unsigned int need, P3& q) {
+    const unsigned long long* w = pub + 4LL * u;
+    const unsigned long long a = ld_word(w), b = ld_word(w + 1), c = ld_word(w + 2);
+    q = {word_value(a), word_value(b), word_value(c)};
+    return word_version(a) == need && word_version(b) == need && word_version(c) == need;
+}
+
+// Warp-uniform bounded-wait bookkeeping: lane 0 checks the clock and the status
+// every 64 polls; true means give up (status recorded).
+__device__ __forceinline__ bool wait_expired(const ArealParams& p, unsigned int& polls, unsigned long long& start) {
+    int expired = 0;
+    if ((threadIdx.x & 31) == 0 && ((++polls) & 63u) == 0u) {
+        const unsigned long long now = csg::global_timer_ns();
+        if (start == 0) start = now;
+        if (csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) expired = 1;
+        else if (now - start > p.timeout_ns) {
+            if (atomicCAS(&p.ctl->status, CSG_OK, CSG_ERR_TIMEOUT) == CSG_OK) p.ctl->where = -2;
+            expired = 1;
+        }
+    }
+    return __shfl_sync(kFull, expired, 0) != 0;
+}
+
+// One vertex update of sweep s by a group of G lanes (all 32 lanes call it;
+// inactive groups pass v < 0).  Same arithmetic and order as update_vertex;
+// lanes 0, 1, 2 publish coordinates 0, 1, 2.  Returns false to abort.
+template <int MODE, int G>
+__device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned long long* pub, int v, const int4* tri,
+                                                 int deg, unsigned int s, double (*stage)[32]) {
+    using T = Traits<MODE>;
+    using Acc = typename T::Acc;
+    using P3 = typename T::P3;
+    const int lane = threadIdx.x & 31;
+    const int glane = lane & (G - 1);
+    const int gbase = lane & ~(G - 1);
+    if (v < 0) deg = 0;
+    const int wdeg = __reduce_max_sync(kFull, deg);
+    const int chunks = wdeg > 0 ? (wdeg + G - 1) / G : 1;  // one pass at least: the own words
+    unsigned int polls = 0;
+    unsigned long long start = 0;
+    float own = 0.0f;  // coordinate glane of v (lanes 0..2), for a vertex that does not move
+    Acc total = 0, wx = 0, wy = 0, wz = 0;  // float path: lane 0 sums everything
+    double wsum = 0;                        // float64 path: lanes 0..2 sum one coordinate each
+    for (int ci = 0; ci < chunks; ++ci) {
+        const int c0 = ci * G;
+        const int j = c0 + glane;
+        const bool face = j < deg;
+        const int4 t = face ? tri[j] : make_int4(0, 0, 0, 0);
+        P3 a{}, b{}, c{};
+        while (true) {
+            bool ok = true;
+            if (face) {
+                ok = load_versioned(pub, t.x, t.x < v ? s : s - 1, a);
+                ok = load_versioned(pub, t.y, t.y < v ? s : s - 1, b) && ok;
+                ok = load_versioned(pub, t.z, t.z < v ? s : s - 1, c) && ok;
+            }
+            if (ci == 0 && v >= 0 && glane < 3) {
+                const unsigned long long w = ld_word(pub + 4LL * v + glane);
+                own = word_value(w);
+                ok = ok && word_version(w) == s - 1;
+            }
+            if (__all_sync(kFull, ok)) break;
+            if (wait_expired(p, polls, start)) return false;
+        }
+        if constexpr (sizeof(Acc) == 8) {
+            double fa = 0, fx = 0, fy = 0, fz = 0;
+            if (face) {
+                double mx, my, mz;
+                T::face(a, b, c, fa, mx, my, mz);
+                fx = __dmul_rn(fa, mx);
+                fy = __dmul_rn(fa, my);
+                fz = __dmul_rn(fa, mz);
+            }
+            stage[0][lane] = fa;
+            stage[1][lane] = fx;
+            stage[2][lane] = fy;
+            stage[3][lane] = fz;
+            __syncwarp();
+            if (glane < 3) {
+                const double* mine = stage[1 + glane];
+                const int n = min(G, deg - c0);
+#pragma unroll
+                for (int q = 0; q < G; ++q) {
+                    if (q < n) {  // slot order == ascending face id
+                        total = __dadd_rn(total, stage[0][gbase + q]);
+                        wsum = __dadd_rn(wsum, mine[gbase + q]);
+                    }
+                }
+            }
+            __syncwarp();
+        } else {
+            Acc fa = 0, fx = 0, fy = 0, fz = 0;
+            if (face) T::face(a, b, c, fa, fx, fy, fz);
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                const Acc aa = __shfl_sync(kFull, fa, gbase + q);
+                const Acc x = __shfl_sync(kFull, fx, gbase + q);
+                const Acc y = __shfl_sync(kFull, fy, gbase + q);
+                const Acc z = __shfl_sync(kFull, fz, gbase + q);
+                if (c0 + q < deg) {  // slot order == ascending face id
+                    total = dadd<Acc>(total, aa);
+                    wx = dadd<Acc>(wx, dmul<Acc>(aa, x));
+                    wy = dadd<Acc>(wy, dmul<Acc>(aa, y));
+                    wz = dadd<Acc>(wz, dmul<Acc>(aa, z));
+                }
+            }
+        }
+    }
+    float value = own;
+    if constexpr (sizeof(Acc) == 8) {
+        // total is summed by each of lanes 0..2 (same order, same value)
+        if (v >= 0 && glane < 3 && total > 0.0) {
+            const double safe = total > 1.0e-20 ? total : 1.0e-20;
+            value = __double2float_rn(__ddiv_rn(wsum, safe));
+        }
+    } else {
+        float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+        const bool moved = v >= 0 && glane == 0 && total > Acc(0);
+        if (moved) {
+            const float safe = total > 1.0e-20f ? total : 1.0e-20f;
+            nx = __fdiv_rn(wx, safe);
+            ny = __fdiv_rn(wy, safe);
+            nz = __fdiv_rn(wz, safe);
+        }
+        const int m = __shfl_sync(kFull, moved ? 1 : 0, gbase);
+        const float ny1 = __shfl_sync(kFull, ny, gbase);
+        const float nz2 = __shfl_sync(kFull, nz, gbase);
+        if (m) value = glane == 0 ? nx : (glane == 1 ? ny1 : nz2);
+    }
+    if (v >= 0 && glane < 3) st_word(pub + 4LL * v + glane, make_word(value, s));
+    return true;
+}
+
+template <int MODE, int G>
+__global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
+    using T = Traits<MODE>;
+    using P3 = typename T::P3;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double stage_all[512 / 32][4][32];
+    double (*stage)[32] = stage_all[threadIdx.x >> 5];
+    unsigned long long* pub = static_cast<unsigned long long*>(p.work);
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthreads = gridDim.x * blockDim.x;
+    const int c = blockIdx.x;
+    const int nc = gridDim.x;
+    const int groups = blockDim.x / G;
+    const int warp_first_group = (threadIdx.x >> 5) * (32 / G);
+    const int my_group = (threadIdx.x & 31) / G;
+    const int nloc = owned_below(p.n, c, nc);
+    const int L = p.n_levels;
+    const int D = p.stride;
+    // shared-memory image: face slots, ids, degrees and levels of the owned
+    // vertices, per-level owned ranges, per-residue top level
+    int4* ltri = reinterpret_cast<int4*>(smem);
+    int* lvid = reinterpret_cast<int*>(ltri + p.nloc_max * p.max_degree);
+    int* ldeg = lvid + p.nloc_max;
+    int* llev = ldeg + p.nloc_max;
+    int* lbeg = llev + p.nloc_max;
+    int* lend = lbeg + L;
+    int* hitop = lend + L;
+    unsigned int phase = 0;
+    int barrier_id = 0;
+    for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
+        const int v = __ldg(p.order + c + i * nc);
+        const int s0 = __ldg(p.slot_off + v);
+        const int d = __ldg(p.slot_off + v + 1) - s0;
+        lvid[i] = v;
+        ldeg[i] = d;
+        for (int j = 0; j < d; ++j) ltri[i * p.max_degree + j] = __ldg(p.slot_tri + s0 + j);
+    }
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+        const int b = owned_below(__ldg(p.level_begin + l), c, nc), e = owned_below(__ldg(p.level_end + l), c, nc);
+        lbeg[l] = b;
+        lend[l] = e;
+        for (int i = b; i < e; ++i) llev[i] = l;
+    }
+    for (int r = threadIdx.x; r < D; r += blockDim.x) hitop[r] = (L - 1) - ((L - 1 - r) % D + D) % D;
+    for (int v = tid; v < p.n; v += nthreads) {
+        const float* q = static_cast<const float*>(p.points) + 3LL * v;
+        for (int k = 0; k < 3; ++k) st_word(pub + 4LL * v + k, make_word(q[k], 0u));
+    }
+    if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+
+    const int last = p.iterations - 1;
+    for (int start = 1; start <= last;) {
+        int end = last;
+        if (p.project_every > 0) end = min(last, ((start - 1) / p.project_every + 1) * p.project_every);
+        const int S = end - start + 1;
+        const int span = (S - 1) * D;  // host guarantees span + L < 2^31
+        const int nsteps = span + L;
+        int r = 0;
+        for (int t = 0; t < nsteps; ++t, r = (r + 1 == D) ? 0 : r + 1) {
+            int lo = t - span;
+            if (lo < r) lo = r;
+            const int hi = t < L ? t : hitop[r];
+            if (hi < lo) continue;
+            const int i0 = lbeg[lo], i1 = lend[hi];
+            for (int base = i0 + warp_first_group; base < i1; base += groups) {
+                const int i = base + my_group;
+                int v = -1, deg = 0;
+                unsigned int sweep = 0;
+                const int4* tri = nullptr;
+                if (i < i1) {
+                    v = lvid[i];
+                    deg = ldeg[i];
+                    tri = ltri + i * p.max_degree;
+                    sweep = static_cast<unsigned int>(start + (t - llev[i]) / D);
+                }
+                if (!update_vertex_df<MODE, G>(p, pub, v, tri, deg, sweep, stage)) return;
+            }
+        }
+        if (p.project_every > 0 && end % p.project_every == 0) {
+            if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+            for (int v = tid; v < p.n; v += nthreads) {
+                P3 q;
+                load_versioned(pub, v, static_cast<unsigned int>(end), q);
+                q = T::project_p3(q, p.radius);
+                st_word(pub + 4LL * v, make_word(q.x, end));
+                st_word(pub + 4LL * v + 1, make_word(q.y, end));
+                st_word(pub + 4LL * v + 2, make_word(q.z, end));
+            }
+            if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+        }
+        start = end + 1;
+    }
+    if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    for (int v = tid; v < p.n; v += nthreads) {
+        float* q = static_cast<float*>(p.points) + 3LL * v;
+        for (int k = 0; k < 3; ++k) q[k] = word_value(ld_word(pub + 4LL * v + k));
+    }
+}
+
 constexpr size_t kMaxTopologySmem = 200 * 1024;
 
 template <int MODE, int G, bool SMEM>
@@ -459,12 +733,37 @@ int launch_variant(ArealParams params, int n_ctas, int threads, size_t smem, cud
 }
 
 template <int MODE, int G>
+int launch_dataflow(ArealParams params, int n_ctas, int threads, size_t smem, cudaStream_t stream) {
+    auto kernel = areal_dataflow_kernel<MODE, G>;
+    int device = 0, sms = 0, per_sm = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CSG_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    if (per_sm < 1 || n_ctas > per_sm * sms)
+        return csg::fail(CSG_ERR_LAUNCH, "areal sweeps: %d CTAs x %d threads (%zu B smem) cannot be co-resident (%d per SM, %d SMs)",
+                         n_ctas, threads, smem, per_sm, sms);
+    void* args[] = {&params};
+    CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(n_ctas), dim3(threads), args,
+                                               smem, stream));
+    csg::note_launch();
+    return CSG_OK;
+}
+
+template <int MODE, int G>
 int launch(ArealParams params, int n_ctas, int threads, cudaStream_t stream) {
     int device = 0, sms = 0;
     CSG_CUDA_CHECK(cudaGetDevice(&device));
     CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     if (n_ctas <= 0) n_ctas = sms;
     params.nloc_max = (params.n + n_ctas - 1) / n_ctas;
+    if constexpr (MODE != CSG_ARITH_FP64) {
+        if (params.allow_dataflow && params.max_degree > 0) {
+            const size_t smem = static_cast<size_t>(params.nloc_max) * (params.max_degree * sizeof(int4) + 3 * sizeof(int)) +
+                                sizeof(int) * (2 * static_cast<size_t>(params.n_levels) + params.stride);
+            if (smem <= kMaxTopologySmem) return launch_dataflow<MODE, G>(params, n_ctas, threads, smem, stream);
+        }
+    }
     const size_t smem = static_cast<size_t>(params.nloc_max) * (params.max_degree * sizeof(int4) + 2 * sizeof(int)) +
                         sizeof(int) * (2 * static_cast<size_t>(params.n_levels) + params.stride);
     if (params.max_degree > 0 && smem <= kMaxTopologySmem)
@@ -505,8 +804,9 @@ extern "C" {
 
 size_t csg_areal_scratch_bytes(int n_vertices, int arithmetic) {
     if (n_vertices < 1) return 0;
-    size_t per = arithmetic == CSG_ARITH_FP64 ? sizeof(D4) : sizeof(float4);
-    return sizeof(csg::Control) + align256(per * static_cast<size_t>(n_vertices));
+    // float64: a double4 working copy; float32 modes: four published 8-byte
+    // words per vertex (the dataflow form; the barrier form uses the first half)
+    return sizeof(csg::Control) + align256(32 * static_cast<size_t>(n_vertices));
 }
 
 int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, const int32_t* slot_tri,
@@ -553,6 +853,7 @@ int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, cons
     p.max_degree = max_degree;
     p.iterations = iterations;
     p.project_every = project_every;
+    p.allow_dataflow = 1;
     p.radius = radius;
     p.timeout_ns = static_cast<unsigned long long>(timeout_s * 1e9);
     CSG_CUDA_CHECK(cudaMemsetAsync(scratch, 0, sizeof(csg::Control), s));
@@ -656,7 +957,10 @@ extern "C" int csg_areal_sweeps_noalloc(void* points, int n_vertices, const int3
         return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): null pointer or empty mesh");
     if (arithmetic < CSG_ARITH_CAT || arithmetic > CSG_ARITH_FP64)
         return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): unknown arithmetic %d", arithmetic);
-    const size_t need = csg_areal_scratch_bytes(n_vertices, arithmetic);
+    // the barrier form: a float4 (float32 modes) or double4 working copy
+    const size_t need = sizeof(csg::Control) +
+                        align256((arithmetic == CSG_ARITH_FP64 ? sizeof(D4) : sizeof(float4)) *
+                                 static_cast<size_t>(n_vertices));
     if (need > kNoAllocBytes)
         return csg::fail(CSG_ERR_ARG,
                          "areal sweeps (no-alloc): %d vertices need %zu bytes of working memory, more than the "
