@@ -148,9 +148,9 @@ def areal_candidates(device=None) -> list[dict]:
 
     sms = sm_count(device)
     shapes = []
-    for threads in (256, 512):
+    for threads in (256, 384, 512):
         for lanes in (4, 8, 16):
-            for per_sm in (1, 2):
+            for per_sm in (1, 2, 3, 4):
                 if threads * per_sm > 1024:
                     continue
                 shapes.append({"n_ctas": sms * per_sm, "threads_per_cta": threads, "lanes_per_vertex": lanes})

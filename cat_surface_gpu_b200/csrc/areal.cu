@@ -503,46 +503,73 @@ __device__ __forceinline__ bool wait_expired(const ArealParams& p, unsigned int&
     return __shfl_sync(kFull, expired, 0) != 0;
 }
 
+// Ring of a vertex: itself, then the other vertices of its faces (at most
+// kRingMax); each face slot is coded as three ring indices (8 bits each).
+constexpr int kRingMax = 20;
+
 // One vertex update of sweep s by a group of G lanes (all 32 lanes call it;
-// inactive groups pass v < 0).  Same arithmetic and order as update_vertex;
-// lanes 0, 1, 2 publish coordinates 0, 1, 2.  Returns false to abort.
+// inactive groups pass v < 0).  The group first polls the words of the ring --
+// lane j loads members j, j + G, ... all at once, one round trip per poll --
+// and stages the positions in shared memory (`pos`, kRingMax entries per
+// group), then computes the faces exactly as update_vertex does (same
+// arithmetic, slot order).  Lanes 0, 1, 2 publish coordinates 0, 1, 2.
+// Returns false to abort.
 template <int MODE, int G>
-__device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned long long* pub, int v, const int4* tri,
-                                                 int deg, unsigned int s, double (*stage)[32]) {
+__device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned long long* pub, int v, const int* ring,
+                                                 int nring, const int* code, int deg, unsigned int s,
+                                                 double (*stage)[32], float3* pos) {
     using T = Traits<MODE>;
     using Acc = typename T::Acc;
     using P3 = typename T::P3;
+    constexpr int kQ = (kRingMax + G - 1) / G;
     const int lane = threadIdx.x & 31;
     const int glane = lane & (G - 1);
     const int gbase = lane & ~(G - 1);
-    if (v < 0) deg = 0;
-    const int wdeg = __reduce_max_sync(kFull, deg);
-    const int chunks = wdeg > 0 ? (wdeg + G - 1) / G : 1;  // one pass at least: the own words
+    if (v < 0) {
+        deg = 0;
+        nring = 0;
+    }
     unsigned int polls = 0;
     unsigned long long start = 0;
-    float own = 0.0f;  // coordinate glane of v (lanes 0..2), for a vertex that does not move
-    Acc total = 0, wx = 0, wy = 0, wz = 0;  // float path: lane 0 sums everything
+    int who[kQ];
+#pragma unroll
+    for (int q = 0; q < kQ; ++q) {
+        const int k = glane + q * G;
+        who[q] = k < nring ? ring[k] : -1;
+    }
+    while (true) {
+        unsigned long long w[kQ][3];
+#pragma unroll
+        for (int q = 0; q < kQ; ++q)
+            if (who[q] >= 0)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) w[q][k] = ld_word(pub + 4LL * who[q] + k);
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < kQ; ++q)
+            if (who[q] >= 0) {
+                const unsigned int need = who[q] < v ? s : s - 1;  // the vertex itself: s - 1
+                ok = ok && word_version(w[q][0]) == need && word_version(w[q][1]) == need &&
+                     word_version(w[q][2]) == need;
+                pos[glane + q * G] = make_float3(word_value(w[q][0]), word_value(w[q][1]), word_value(w[q][2]));
+            }
+        if (__all_sync(kFull, ok)) break;
+        if (wait_expired(p, polls, start)) return false;
+    }
+    __syncwarp();
+    const int wdeg = __reduce_max_sync(kFull, deg);
+    Acc total = 0, wx = 0, wy = 0, wz = 0;  // float path: every lane sums its group's faces
     double wsum = 0;                        // float64 path: lanes 0..2 sum one coordinate each
-    for (int ci = 0; ci < chunks; ++ci) {
-        const int c0 = ci * G;
+    for (int c0 = 0; c0 < wdeg; c0 += G) {
         const int j = c0 + glane;
         const bool face = j < deg;
-        const int4 t = face ? tri[j] : make_int4(0, 0, 0, 0);
         P3 a{}, b{}, c{};
-        while (true) {
-            bool ok = true;
-            if (face) {
-                ok = load_versioned(pub, t.x, t.x < v ? s : s - 1, a);
-                ok = load_versioned(pub, t.y, t.y < v ? s : s - 1, b) && ok;
-                ok = load_versioned(pub, t.z, t.z < v ? s : s - 1, c) && ok;
-            }
-            if (ci == 0 && v >= 0 && glane < 3) {
-                const unsigned long long w = ld_word(pub + 4LL * v + glane);
-                own = word_value(w);
-                ok = ok && word_version(w) == s - 1;
-            }
-            if (__all_sync(kFull, ok)) break;
-            if (wait_expired(p, polls, start)) return false;
+        if (face) {
+            const int cd = code[j];
+            const float3 pa = pos[cd & 255], pb = pos[(cd >> 8) & 255], pc = pos[(cd >> 16) & 255];
+            a = {pa.x, pa.y, pa.z};
+            b = {pb.x, pb.y, pb.z};
+            c = {pc.x, pc.y, pc.z};
         }
         if constexpr (sizeof(Acc) == 8) {
             double fa = 0, fx = 0, fy = 0, fz = 0;
@@ -588,7 +615,9 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
             }
         }
     }
-    float value = own;
+    // a vertex that does not move republishes its own position (ring member 0)
+    float value = 0.0f;
+    if (v >= 0 && glane < 3) value = glane == 0 ? pos[0].x : (glane == 1 ? pos[0].y : pos[0].z);
     if constexpr (sizeof(Acc) == 8) {
         // total is summed by each of lanes 0..2 (same order, same value)
         if (v >= 0 && glane < 3 && total > 0.0) {
@@ -609,6 +638,7 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
         const float nz2 = __shfl_sync(kFull, nz, gbase);
         if (m) value = glane == 0 ? nx : (glane == 1 ? ny1 : nz2);
     }
+    __syncwarp();  // every lane is done with `pos` before the next update overwrites it
     if (v >= 0 && glane < 3) st_word(pub + 4LL * v + glane, make_word(value, s));
     return true;
 }
@@ -631,10 +661,15 @@ __global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
     const int nloc = owned_below(p.n, c, nc);
     const int L = p.n_levels;
     const int D = p.stride;
-    // shared-memory image: face slots, ids, degrees and levels of the owned
-    // vertices, per-level owned ranges, per-residue top level
-    int4* ltri = reinterpret_cast<int4*>(smem);
-    int* lvid = reinterpret_cast<int*>(ltri + p.nloc_max * p.max_degree);
+    // shared-memory image: per warp, kRingMax staged positions per group; per
+    // owned vertex its ring, ring size, face codes, id, degree and level; per
+    // level the owned range; per residue the top level
+    float3* wpos = reinterpret_cast<float3*>(smem) + (threadIdx.x >> 5) * (32 / G) * kRingMax;
+    float3* pos = wpos + my_group * kRingMax;
+    int* lring = reinterpret_cast<int*>(reinterpret_cast<float3*>(smem) + (blockDim.x / 32) * (32 / G) * kRingMax);
+    int* lcode = lring + p.nloc_max * kRingMax;
+    int* lnring = lcode + p.nloc_max * p.max_degree;
+    int* lvid = lnring + p.nloc_max;
     int* ldeg = lvid + p.nloc_max;
     int* llev = ldeg + p.nloc_max;
     int* lbeg = llev + p.nloc_max;
@@ -646,9 +681,31 @@ __global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
         const int v = __ldg(p.order + c + i * nc);
         const int s0 = __ldg(p.slot_off + v);
         const int d = __ldg(p.slot_off + v + 1) - s0;
+        int* ring = lring + i * kRingMax;
+        int nr = 1;
+        ring[0] = v;
+        for (int j = 0; j < d; ++j) {
+            const int4 t = __ldg(p.slot_tri + s0 + j);
+            const int u[3] = {t.x, t.y, t.z};
+            int cd = 0;
+            for (int k = 0; k < 3; ++k) {
+                int at = 0;
+                while (at < nr && ring[at] != u[k]) ++at;
+                if (at == nr) {
+                    if (nr == kRingMax) {  // the host sized kRingMax from max_degree; report, stay inside
+                        if (atomicCAS(&p.ctl->status, CSG_OK, CSG_ERR_ARG) == CSG_OK) p.ctl->where = -1;
+                        at = 0;
+                    } else {
+                        ring[nr++] = u[k];
+                    }
+                }
+                cd |= at << (8 * k);
+            }
+            lcode[i * p.max_degree + j] = cd;
+        }
+        lnring[i] = nr;
         lvid[i] = v;
         ldeg[i] = d;
-        for (int j = 0; j < d; ++j) ltri[i * p.max_degree + j] = __ldg(p.slot_tri + s0 + j);
     }
     for (int l = threadIdx.x; l < L; l += blockDim.x) {
         const int b = owned_below(__ldg(p.level_begin + l), c, nc), e = owned_below(__ldg(p.level_end + l), c, nc);
@@ -662,6 +719,7 @@ __global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
         for (int k = 0; k < 3; ++k) st_word(pub + 4LL * v + k, make_word(q[k], 0u));
     }
     if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    if (csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) return;  // a ring overflow: same answer in every CTA
 
     const int last = p.iterations - 1;
     for (int start = 1; start <= last;) {
@@ -679,16 +737,19 @@ __global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
             const int i0 = lbeg[lo], i1 = lend[hi];
             for (int base = i0 + warp_first_group; base < i1; base += groups) {
                 const int i = base + my_group;
-                int v = -1, deg = 0;
+                int v = -1, deg = 0, nring = 0;
                 unsigned int sweep = 0;
-                const int4* tri = nullptr;
+                const int* ring = nullptr;
+                const int* code = nullptr;
                 if (i < i1) {
                     v = lvid[i];
                     deg = ldeg[i];
-                    tri = ltri + i * p.max_degree;
+                    nring = lnring[i];
+                    ring = lring + i * kRingMax;
+                    code = lcode + i * p.max_degree;
                     sweep = static_cast<unsigned int>(start + (t - llev[i]) / D);
                 }
-                if (!update_vertex_df<MODE, G>(p, pub, v, tri, deg, sweep, stage)) return;
+                if (!update_vertex_df<MODE, G>(p, pub, v, ring, nring, code, deg, sweep, stage, pos)) return;
             }
         }
         if (p.project_every > 0 && end % p.project_every == 0) {
@@ -758,8 +819,10 @@ int launch(ArealParams params, int n_ctas, int threads, cudaStream_t stream) {
     if (n_ctas <= 0) n_ctas = sms;
     params.nloc_max = (params.n + n_ctas - 1) / n_ctas;
     if constexpr (MODE != CSG_ARITH_FP64) {
-        if (params.allow_dataflow && params.max_degree > 0) {
-            const size_t smem = static_cast<size_t>(params.nloc_max) * (params.max_degree * sizeof(int4) + 3 * sizeof(int)) +
+        // a ring has at most 2 max_degree + 1 vertices
+        if (params.allow_dataflow && params.max_degree > 0 && 2 * params.max_degree + 1 <= kRingMax) {
+            const size_t smem = sizeof(float3) * (threads / 32) * (32 / G) * kRingMax +
+                                static_cast<size_t>(params.nloc_max) * sizeof(int) * (kRingMax + params.max_degree + 4) +
                                 sizeof(int) * (2 * static_cast<size_t>(params.n_levels) + params.stride);
             if (smem <= kMaxTopologySmem) return launch_dataflow<MODE, G>(params, n_ctas, threads, smem, stream);
         }
