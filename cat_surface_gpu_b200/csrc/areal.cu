@@ -464,19 +464,11 @@ __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
 // Every wait is bounded: on timeout (or another CTA's failure) the kernel
 // records the status and leaves.
 
-__device__ __forceinline__ unsigned long long ld_word(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_word(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ unsigned long long make_word(float x, unsigned int version) {
-    return (static_cast<unsigned long long>(version) << 32) | __float_as_uint(x);
-}
-__device__ __forceinline__ float word_value(unsigned long long w) { return __uint_as_float(static_cast<unsigned>(w)); }
-__device__ __forceinline__ unsigned int word_version(unsigned long long w) { return static_cast<unsigned>(w >> 32); }
+using csg::ld_word;
+using csg::make_word;
+using csg::st_word;
+using csg::word_value;
+using csg::word_version;
 
 // words of vertex v: pub[4 v + k], k = 0, 1, 2 (coordinate k), 3 unused
 template <typename P3>
@@ -487,20 +479,8 @@ __device__ __forceinline__ bool load_versioned(const unsigned long long* pub, in
     return word_version(a) == need && word_version(b) == need && word_version(c) == need;
 }
 
-// Warp-uniform bounded-wait bookkeeping: lane 0 checks the clock and the status
-// every 64 polls; true means give up (status recorded).
 __device__ __forceinline__ bool wait_expired(const ArealParams& p, unsigned int& polls, unsigned long long& start) {
-    int expired = 0;
-    if ((threadIdx.x & 31) == 0 && ((++polls) & 63u) == 0u) {
-        const unsigned long long now = csg::global_timer_ns();
-        if (start == 0) start = now;
-        if (csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) expired = 1;
-        else if (now - start > p.timeout_ns) {
-            if (atomicCAS(&p.ctl->status, CSG_OK, CSG_ERR_TIMEOUT) == CSG_OK) p.ctl->where = -2;
-            expired = 1;
-        }
-    }
-    return __shfl_sync(kFull, expired, 0) != 0;
+    return csg::warp_wait_expired(p.ctl, p.timeout_ns, polls, start);
 }
 
 // Ring of a vertex: itself, then the other vertices of its faces (at most

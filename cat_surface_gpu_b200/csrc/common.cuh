@@ -99,4 +99,41 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, unsigned int& phase, 
     return s_abort != 0;
 }
 
+// Versioned words of the dataflow kernels: a float32 value and the number of
+// updates it belongs to in one 8-byte word.  Aligned 8-byte accesses are
+// single-copy atomic, so a relaxed load returns a value together with its own
+// version and needs no acquire ordering.
+__device__ __forceinline__ unsigned long long ld_word(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_word(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long make_word(float x, unsigned int version) {
+    return (static_cast<unsigned long long>(version) << 32) | __float_as_uint(x);
+}
+__device__ __forceinline__ float word_value(unsigned long long w) { return __uint_as_float(static_cast<unsigned>(w)); }
+__device__ __forceinline__ unsigned int word_version(unsigned long long w) { return static_cast<unsigned>(w >> 32); }
+
+// Bounded wait of one warp in a dataflow kernel: lane 0 checks the clock and
+// the status word every 64 polls; true (the same in every lane) means give up
+// -- the status is CSG_ERR_TIMEOUT (recorded here) or another CTA's error.
+__device__ __forceinline__ bool warp_wait_expired(Control* ctl, unsigned long long timeout_ns, unsigned int& polls,
+                                                  unsigned long long& start) {
+    int expired = 0;
+    if ((threadIdx.x & 31) == 0 && ((++polls) & 63u) == 0u) {
+        const unsigned long long now = global_timer_ns();
+        if (start == 0) start = now;
+        if (ld_relaxed_gpu(&ctl->status) != CSG_OK) {
+            expired = 1;
+        } else if (now - start > timeout_ns) {
+            if (atomicCAS(&ctl->status, CSG_OK, CSG_ERR_TIMEOUT) == CSG_OK) ctl->where = -2;
+            expired = 1;
+        }
+    }
+    return __shfl_sync(0xffffffffu, expired, 0) != 0;
+}
+
 }  // namespace csg

@@ -82,6 +82,7 @@ struct Segment {
 
 struct PassParams {
     float4* work;
+    unsigned long long* pub;  // dataflow form: 4 versioned words per vertex
     const int* nb_off;
     const int* nb;
     const unsigned char* selected;
@@ -275,6 +276,219 @@ __global__ void __launch_bounds__(512) smooth_passes_kernel(PassParams p) {
     }
 }
 
+// ---------------------------------------------------------------- dataflow form
+//
+// The same passes without a grid barrier per wavefront step: each coordinate
+// is published as a versioned word (csg::make_word; version = passes the
+// vertex has completed in this launch).  Pass k of vertex v needs its
+// lower-index neighbours at version k + 1, its higher-index neighbours and
+// itself at version k, and none of them can be further ahead (a neighbour's
+// next pass needs v's pass k), so the words that show those versions hold
+// exactly the values the sequential order reads.  A group polls the ring (v
+// and its 1-ring, one round trip per poll), stages the positions in shared
+// memory and applies the segment's update; every vertex publishes every pass
+// (unchanged when it does not move).  Grid barriers remain at the start (the
+// words are written from `work`) and at the end (`work` is written back).
+
+constexpr int kPRing = 17;  // the vertex and at most 16 neighbours
+
+template <int G>
+__device__ __forceinline__ bool pass_vertex_df(const PassParams& p, int v, const int* ring, int nring, int sg,
+                                               unsigned int pass, double (*stage)[32], float3* pos) {
+    constexpr int kQ = (kPRing + G - 1) / G;
+    const int lane = threadIdx.x & 31;
+    const int glane = lane & (G - 1);
+    const int gbase = lane & ~(G - 1);
+    const int kind = p.seg[sg].kind;
+    const double strength = p.seg[sg].value;
+    if (v < 0) nring = 0;
+    unsigned int polls = 0;
+    unsigned long long start = 0;
+    int who[kQ];
+#pragma unroll
+    for (int q = 0; q < kQ; ++q) {
+        const int k = glane + q * G;
+        who[q] = k < nring ? ring[k] : -1;
+    }
+    while (true) {
+        unsigned long long w[kQ][3];
+#pragma unroll
+        for (int q = 0; q < kQ; ++q)
+            if (who[q] >= 0)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) w[q][k] = csg::ld_word(p.pub + 4LL * who[q] + k);
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < kQ; ++q)
+            if (who[q] >= 0) {
+                const unsigned int need = who[q] < v ? pass + 1 : pass;  // the vertex itself: pass
+                ok = ok && csg::word_version(w[q][0]) == need && csg::word_version(w[q][1]) == need &&
+                     csg::word_version(w[q][2]) == need;
+                pos[glane + q * G] = make_float3(csg::word_value(w[q][0]), csg::word_value(w[q][1]),
+                                                 csg::word_value(w[q][2]));
+            }
+        if (__all_sync(kFull, ok)) break;
+        if (csg::warp_wait_expired(p.ctl, p.timeout_ns, polls, start)) return false;
+    }
+    __syncwarp();
+    int deg = nring > 0 ? nring - 1 : 0;
+    const bool active = v >= 0 && kind != kInflate && deg > 1 && (kind == kSmoothAll || p.selected[v]);
+    if (!active) deg = 0;
+    const int wdeg = __reduce_max_sync(kFull, deg);
+    double o[3] = {0.0, 0.0, 0.0};
+    if (v >= 0) {
+        o[0] = pos[0].x;
+        o[1] = pos[0].y;
+        o[2] = pos[0].z;
+    }
+    double total = 0.0, wsum = 0.0;
+    const int comp = glane < 3 ? glane : 0;
+    for (int c0 = 0; c0 < wdeg; c0 += G) {
+        const int j = c0 + glane;
+        double d = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
+        if (j < deg) {
+            const float3 q = pos[1 + j];
+            const double qx = q.x, qy = q.y, qz = q.z;
+            d = __dadd_rn(__dadd_rn(fabs(__dsub_rn(qx, o[0])), fabs(__dsub_rn(qy, o[1]))), fabs(__dsub_rn(qz, o[2])));
+            if (d > 0.0) {
+                dx = __dmul_rn(d, qx);
+                dy = __dmul_rn(d, qy);
+                dz = __dmul_rn(d, qz);
+            }
+        }
+        stage[0][lane] = d;
+        stage[1][lane] = dx;
+        stage[2][lane] = dy;
+        stage[3][lane] = dz;
+        __syncwarp();
+        if (glane < 3) {
+            const int m = min(G, deg - c0);
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                if (q < m) {
+                    total = __dadd_rn(total, stage[0][gbase + q]);
+                    // the reference adds d q only for d > 0; the staged term is 0 otherwise
+                    if (stage[0][gbase + q] > 0.0) wsum = __dadd_rn(wsum, stage[1 + comp][gbase + q]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    float value = 0.0f;
+    if (v >= 0 && glane < 3) {
+        if (active) {
+            const double keep = __dmul_rn(o[comp], 1.0 - strength);
+            value = __double2float_rn(total > 0.0 ? __dadd_rn(keep, __dmul_rn(__ddiv_rn(wsum, total), strength)) : keep);
+        } else if (kind == kInflate) {
+            const Stats* st = p.st;
+            const double x = __ddiv_rn(o[0], st->extent[0]), y = __ddiv_rn(o[1], st->extent[1]),
+                         z = __ddiv_rn(o[2], st->extent[2]);
+            const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+            const double scale = __dadd_rn(1.0, __dmul_rn(strength, __dsub_rn(1.0, r)));
+            value = __double2float_rn(__dmul_rn(o[comp], scale));
+        } else {
+            value = static_cast<float>(o[comp]);
+        }
+    }
+    __syncwarp();  // every lane is done with `pos` before the next update overwrites it
+    if (v >= 0 && glane < 3) csg::st_word(p.pub + 4LL * v + glane, csg::make_word(value, pass + 1));
+    return true;
+}
+
+template <int G>
+__global__ void __launch_bounds__(512) smooth_passes_df(PassParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double stage_all[512 / 32][4][32];
+    double (*stage)[32] = stage_all[threadIdx.x >> 5];
+    const int c = blockIdx.x, nc = gridDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    const int groups = blockDim.x / G;
+    const int warp_first_group = (threadIdx.x >> 5) * (32 / G);
+    const int my_group = (threadIdx.x & 31) / G;
+    const int L = p.n_levels, D = p.stride;
+    // shared-memory image: per warp, kPRing staged positions per group; per
+    // owned vertex its ring (itself, then its 1-ring), ring size, id and level;
+    // per level the owned range
+    float3* pos = reinterpret_cast<float3*>(smem_raw) + ((threadIdx.x >> 5) * (32 / G) + my_group) * kPRing;
+    int* lring = reinterpret_cast<int*>(reinterpret_cast<float3*>(smem_raw) + (blockDim.x / G) * kPRing);
+    int* lnring = lring + p.nloc_max * kPRing;
+    int* lvid = lnring + p.nloc_max;
+    int* llev = lvid + p.nloc_max;
+    int* lbeg = llev + p.nloc_max;
+    int* lend = lbeg + L;
+    const int nloc = owned_below(p.n, c, nc);
+    for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
+        const int v = __ldg(p.order + c + i * nc);
+        const int b = __ldg(p.nb_off + v);
+        int d = __ldg(p.nb_off + v + 1) - b;
+        if (d > p.max_degree || d + 1 > kPRing) {  // a ring longer than the caller's max_degree: report it
+            if (atomicCAS(&p.ctl->status, CSG_OK, CSG_ERR_ARG) == CSG_OK) p.ctl->where = -1;
+            d = min(d, kPRing - 1);
+        }
+        int* ring = lring + i * kPRing;
+        ring[0] = v;
+        for (int j = 0; j < d; ++j) ring[1 + j] = __ldg(p.nb + b + j);
+        lnring[i] = d + 1;
+        lvid[i] = v;
+    }
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+        const int lb = owned_below(__ldg(p.level_begin + l), c, nc), le = owned_below(__ldg(p.level_end + l), c, nc);
+        lbeg[l] = lb;
+        lend[l] = le;
+        for (int i = lb; i < le; ++i) llev[i] = l;
+    }
+    for (int v = tid; v < p.n; v += nthreads) {
+        const float4 q = ld4(p.work, v);
+        csg::st_word(p.pub + 4LL * v, csg::make_word(q.x, 0u));
+        csg::st_word(p.pub + 4LL * v + 1, csg::make_word(q.y, 0u));
+        csg::st_word(p.pub + 4LL * v + 2, csg::make_word(q.z, 0u));
+    }
+    unsigned int phase = 0;
+    int barrier_id = 0;
+    if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    if (csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) return;  // a ring overflow: same answer in every CTA
+    const int span = (p.passes - 1) * D;  // host guarantees span + L < 2^31
+    const int nsteps = span + L;
+    int r = 0;
+    for (int t = 0; t < nsteps; ++t, r = (r + 1 == D) ? 0 : r + 1) {
+        int lo = t - span;
+        if (lo < r) lo = r;
+        const int hi = t < L ? t : (L - 1) - ((L - 1 - r) % D + D) % D;
+        if (hi < lo) continue;
+        const int i0 = lbeg[lo], i1 = lend[hi];
+        int ib[kMaxSegments];
+#pragma unroll
+        for (int k = 1; k < kMaxSegments; ++k) {
+            ib[k] = 0;
+            if (k < p.n_segments) {
+                const int m = t - p.seg[k].first_pass * D;
+                ib[k] = m < lo ? i0 : (m >= hi ? i1 : lend[m]);
+            }
+        }
+        for (int base = i0 + warp_first_group; base < i1; base += groups) {
+            const int i = base + my_group;
+            int v = -1, nring = 0, sg = 0;
+            unsigned int pass = 0;
+            const int* ring = nullptr;
+            if (i < i1) {
+                v = lvid[i];
+                nring = lnring[i];
+                ring = lring + i * kPRing;
+                pass = static_cast<unsigned int>((t - llev[i]) / D);
+#pragma unroll
+                for (int k = 1; k < kMaxSegments; ++k) sg += i < ib[k];
+            }
+            if (!pass_vertex_df<G>(p, v, ring, nring, sg, pass, stage, pos)) return;
+        }
+    }
+    if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    for (int v = tid; v < p.n; v += nthreads) {
+        const unsigned long long* w = p.pub + 4LL * v;
+        __stcg(p.work + v, make_float4(csg::word_value(csg::ld_word(w)), csg::word_value(csg::ld_word(w + 1)),
+                                       csg::word_value(csg::ld_word(w + 2)), 0.0f));
+    }
+}
+
 // ---------------------------------------------------------------- per-stage steps
 
 __global__ void k_pack(const float* __restrict__ points, float4* __restrict__ work, int n) {
@@ -425,7 +639,7 @@ __global__ void k_select(const double* __restrict__ comp, const int* __restrict_
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
 struct Layout {
-    size_t ctl, work, ref, area, va_ref, va_cur, comp, sel, partial, stats, total;
+    size_t ctl, work, pub, ref, area, va_ref, va_cur, comp, sel, partial, stats, total;
 };
 
 Layout layout(int n, int nf) {
@@ -439,6 +653,7 @@ Layout layout(int n, int nf) {
     const size_t runs = (static_cast<size_t>(n > nf ? n : nf) + kBlockSum - 1) / kBlockSum;
     L.ctl = take(sizeof(csg::Control));
     L.work = take(16ULL * n);
+    L.pub = take(32ULL * n);
     L.ref = take(16ULL * n);
     L.area = take(8ULL * nf);
     L.va_ref = take(8ULL * n);
@@ -473,12 +688,37 @@ int launch_variant(const PassParams& params, int n_ctas, int threads, size_t sme
 }
 
 template <int G>
+int launch_dataflow(const PassParams& params, int n_ctas, int threads, size_t smem, cudaStream_t s) {
+    auto kernel = smooth_passes_df<G>;
+    int device = 0, sms = 0, per_sm = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CSG_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    if (per_sm < 1 || n_ctas > per_sm * sms)
+        return csg::fail(CSG_ERR_LAUNCH, "preprocess passes: %d CTAs x %d threads (%zu B smem) cannot be co-resident",
+                         n_ctas, threads, smem);
+    PassParams p = params;
+    void* args[] = {&p};
+    CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(n_ctas), dim3(threads), args,
+                                               smem, s));
+    csg::note_launch();
+    return CSG_OK;
+}
+
+template <int G>
 int launch_passes(PassParams params, int n_ctas, int threads, cudaStream_t s) {
     int device = 0, sms = 0;
     CSG_CUDA_CHECK(cudaGetDevice(&device));
     CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     if (n_ctas <= 0) n_ctas = sms;
     params.nloc_max = (params.n + n_ctas - 1) / n_ctas;
+    if (params.max_degree > 0 && params.max_degree + 1 <= kPRing) {
+        const size_t smem = sizeof(float3) * (threads / G) * kPRing +
+                            sizeof(int) * (static_cast<size_t>(params.nloc_max) * (kPRing + 3) +
+                                           2 * static_cast<size_t>(params.n_levels));
+        if (smem <= kMaxTopologySmem) return launch_dataflow<G>(params, n_ctas, threads, smem, s);
+    }
     const size_t smem = sizeof(int) * (static_cast<size_t>(params.nloc_max) * (params.max_degree + 2) +
                                        2 * static_cast<size_t>(params.n_levels));
     if (params.max_degree > 0 && smem <= kMaxTopologySmem) return launch_variant<G, true>(params, n_ctas, threads, smem, s);
@@ -570,6 +810,7 @@ int csg_surf2sphere_preprocess(float* points, int n, const int32_t* faces, int n
     (csg::note_launch(), k_pack<<<blocks(n, kThreads), kThreads, 0, s>>>(points, work, n));
     PassQueue q{};
     q.p.work = work;
+    q.p.pub = reinterpret_cast<unsigned long long*>(base + L.pub);
     q.p.nb_off = nb_off;
     q.p.nb = nb;
     q.p.selected = sel;
