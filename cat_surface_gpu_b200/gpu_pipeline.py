@@ -37,7 +37,8 @@ from .device import resolve_device
 from .gifti import GiftiMesh, read_gifti_mesh, write_gifti_mesh
 from .rotation_pipeline import RotationPipeline, read_rotation_values
 from .surface_stencil import SurfaceStencil, build_surface_stencil
-from .surface_warp import apply_flow_to_stenciled_sphere, average_xz_surfaces, solve_dartel_from_surfaces
+from .surface_warp import (apply_flow_to_stenciled_sphere, average_xz_surfaces, solve_dartel_from_surfaces,
+                           solve_dartel_from_surfaces_many)
 
 
 @dataclass(frozen=True)
@@ -445,42 +446,48 @@ def register_meshes(
                                               cuda_graph=graph_requested)
 
         dartel_start = time.perf_counter()
-        last_result = None
+        last_flow = avg_flow = None
         final_prewarp = None
-        avg_source_stencil = None
+        avg_source_dev = None
         avg_source_sphere = None
-        avg_source_surface = None
+        avg_fwhm = tuple(float(fwhm[0]) / (3.0 ** (steps * (runs + 1) + i)) for i in range(steps))
         for run_index in range(runs):
             run_start = time.perf_counter()
             base = float(fwhm[0])
             run_fwhm = tuple(base / (3.0 ** (steps * (run_index + 1) + i)) for i in range(steps))
             if avg and run_index == runs - 1:
+                # the -avg solve starts from the same sphere as the last run and does not depend on its
+                # result (reference 1140-1177, 1229-1268): both registrations go through one batched
+                # solve, whose flows equal the two separate solves
                 final_prewarp = current_sphere.copy()
                 avg_source_surface = rotate_vertices(source_surface.vertices, pole)
                 avg_source_sphere = rotate_vertices(final_prewarp, pole)
                 avg_source_stencil = rotated_builder.build(GiftiMesh(avg_source_sphere, source_sphere.faces),
                                                            source_surface_path, normalize=False)
-            solve = solve_one(source_surface_dev, target_surface_dev, current_dev, target_dev, run_fwhm, loop)
-            if not (avg and run_index == runs - 1):
+                avg_source_dev = avg_source_stencil.to(target_device)
+                last_flow, avg_flow = solve_dartel_from_surfaces_many(
+                    [(source_surface_dev, target_surface_dev, current_dev, target_dev, run_fwhm),
+                     (on_device(avg_source_surface), on_device(avg_target_surface), avg_source_dev,
+                      avg_target_stencil.to(target_device), avg_fwhm)],
+                    curvtypes=tuple(curvtypes), loop=loop, n_steps=steps, cycles=cycles, nit=nit, its=its, code=code,
+                    device=target_device, dtype=solve_dtype, parallel_sides=parallel_sides, cuda_graph=graph_requested)
+            else:
+                last_flow = solve_one(source_surface_dev, target_surface_dev, current_dev, target_dev, run_fwhm,
+                                      loop).flow
                 current_sphere = apply_flow_to_stenciled_sphere(
-                    on_device(current_sphere), solve.flow, current_dev, inverse=True, device=target_device,
+                    on_device(current_sphere), last_flow, current_dev, inverse=True, device=target_device,
                     dtype=solve_dtype).cpu().numpy().astype(np.float32)
             torch.cuda.synchronize(target_device)
             timings[f"dartel_run_{run_index}_seconds"] = time.perf_counter() - run_start
-            last_result = solve
             if run_index + 1 < runs:
                 current_stencil = rotated_builder.build(GiftiMesh(current_sphere, source_sphere.faces),
                                                         source_surface_path, normalize=False)
                 current_dev = current_stencil.to(target_device)
         if avg:
-            avg_fwhm = tuple(float(fwhm[0]) / (3.0 ** (steps * (runs + 1) + i)) for i in range(steps))
             avg_start = time.perf_counter()
-            avg_source_dev = avg_source_stencil.to(target_device)
-            avg_result = solve_one(on_device(avg_source_surface), on_device(avg_target_surface), avg_source_dev,
-                                   avg_target_stencil.to(target_device), avg_fwhm, loop)
-            main_warped = apply_flow_to_stenciled_sphere(on_device(final_prewarp), last_result.flow, current_dev,
+            main_warped = apply_flow_to_stenciled_sphere(on_device(final_prewarp), last_flow, current_dev,
                                                          inverse=True, device=target_device, dtype=solve_dtype)
-            avg_warped = apply_flow_to_stenciled_sphere(on_device(avg_source_sphere), avg_result.flow, avg_source_dev,
+            avg_warped = apply_flow_to_stenciled_sphere(on_device(avg_source_sphere), avg_flow, avg_source_dev,
                                                         inverse=True, device=target_device, dtype=solve_dtype)
             reverse = rotation_matrix_from_angles(-pole).to(device=target_device)
             unrotated = avg_warped.to(torch.float64) @ reverse.transpose(0, 1)

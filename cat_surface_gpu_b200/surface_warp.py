@@ -308,19 +308,12 @@ def solve_dartel_registrations(source_maps, target_maps, *, loop: int = 6, lmreg
     return solver.flows[:regs], solver.metrics.view(regs, steps, -1, 3)
 
 
-def solve_dartel_from_surfaces(source_vertices, target_vertices, source_stencil, target_stencil, *,
-                               fwhm: Sequence[float] = (5.0, 5.0 / 3.0, 5.0 / 9.0), curvtypes: Sequence[int] = (5, 5, 2),
-                               loop: int = 6, n_steps: int = 2, lmreg: float = 1e-3, cycles: int = 3, nit: int = 3,
-                               its: int = 3, code: int = 1, kernel: str = "auto", squaring_kernel: str | None = None,
-                               device="auto", dtype=torch.float64, parallel_sides: bool = True, optimized: bool = True,
-                               assume_initial_nonzero: bool = False, cuda_graph: bool = False) -> DartelSolveResult:
-    """Curvature sheets of both surfaces, then their DARTEL solve (reference 370-488)."""
+def _surface_sheets(source_vertices, target_vertices, source_stencil, target_stencil, fwhm, curvtypes, n_steps, dev,
+                    dtype, parallel_sides):
+    """Curvature sheets [n_steps, ny, nx] of both surfaces (reference 370-470)."""
 
     if n_steps < 1 or n_steps > len(fwhm) or n_steps > len(curvtypes):
         raise ValueError("n_steps must not exceed the lengths of fwhm and curvtypes")
-    if squaring_kernel not in {None, "auto", "torch", "triton"}:
-        raise ValueError("squaring_kernel must be None, 'auto', 'torch', or 'triton'")
-    dev = resolve_device(device)
     src_st = source_stencil.to(dev, geometry_dtype=torch.float32) if hasattr(source_stencil, "from_file") else source_stencil
     tgt_st = target_stencil.to(dev, geometry_dtype=torch.float32) if hasattr(target_stencil, "from_file") else target_stencil
     source = torch.as_tensor(source_vertices, device=dev).to(torch.float32).contiguous()
@@ -348,11 +341,51 @@ def solve_dartel_from_surfaces(source_vertices, target_vertices, source_stencil,
     else:
         source_maps = build_maps(src_st, src_st.resample_vertices(source))
         target_maps = build_maps(tgt_st, tgt_st.resample_vertices(target))
-    stacked_source = torch.stack(source_maps, dim=0).to(dtype=dtype).contiguous()
-    stacked_target = torch.stack(target_maps, dim=0).to(dtype=dtype).contiguous()
+    return (torch.stack(source_maps, dim=0).to(dtype=dtype).contiguous(),
+            torch.stack(target_maps, dim=0).to(dtype=dtype).contiguous())
+
+
+def solve_dartel_from_surfaces(source_vertices, target_vertices, source_stencil, target_stencil, *,
+                               fwhm: Sequence[float] = (5.0, 5.0 / 3.0, 5.0 / 9.0), curvtypes: Sequence[int] = (5, 5, 2),
+                               loop: int = 6, n_steps: int = 2, lmreg: float = 1e-3, cycles: int = 3, nit: int = 3,
+                               its: int = 3, code: int = 1, kernel: str = "auto", squaring_kernel: str | None = None,
+                               device="auto", dtype=torch.float64, parallel_sides: bool = True, optimized: bool = True,
+                               assume_initial_nonzero: bool = False, cuda_graph: bool = False) -> DartelSolveResult:
+    """Curvature sheets of both surfaces, then their DARTEL solve (reference 370-488)."""
+
+    if squaring_kernel not in {None, "auto", "torch", "triton"}:
+        raise ValueError("squaring_kernel must be None, 'auto', 'torch', or 'triton'")
+    dev = resolve_device(device)
+    stacked_source, stacked_target = _surface_sheets(source_vertices, target_vertices, source_stencil, target_stencil,
+                                                     fwhm, curvtypes, n_steps, dev, dtype, parallel_sides)
     return solve_dartel_maps(stacked_source, stacked_target, loop=loop, lmreg=lmreg, cycles=cycles, nit=nit, its=its,
                              code=code, kernel=kernel, squaring_kernel=squaring_kernel, device=dev, dtype=dtype,
                              optimized=optimized, assume_initial_nonzero=assume_initial_nonzero, cuda_graph=cuda_graph)
+
+
+def solve_dartel_from_surfaces_many(problems, *, curvtypes: Sequence[int] = (5, 5, 2), loop: int = 6,
+                                    n_steps: int = 2, lmreg: float = 1e-3, cycles: int = 3, nit: int = 3, its: int = 3,
+                                    code: int = 1, device="auto", dtype=torch.float64, parallel_sides: bool = True,
+                                    assume_initial_nonzero: bool = False, cuda_graph: bool = False) -> list:
+    """Several independent surface registrations as ONE batched DARTEL solve.
+
+    ``problems`` holds ``(source_vertices, target_vertices, source_stencil,
+    target_stencil, fwhm)`` per registration (sheets of one size).  Returns
+    the flows ``[2, ny, nx]`` in order; each equals
+    ``solve_dartel_from_surfaces(...).flow`` of that registration with the
+    same ``assume_initial_nonzero`` / ``cuda_graph``.
+    """
+
+    dev = resolve_device(device)
+    sheets = [_surface_sheets(sv, tv, ss, ts, f, curvtypes, n_steps, dev, dtype, parallel_sides)
+              for sv, tv, ss, ts, f in problems]
+    if len({tuple(src.shape) for src, _ in sheets}) != 1:
+        raise ValueError("batched registrations need sheets of one size")
+    flows, _ = solve_dartel_registrations(torch.stack([src for src, _ in sheets]), torch.stack([tgt for _, tgt in sheets]),
+                                          loop=loop, lmreg=lmreg, cycles=cycles, nit=nit, its=its, code=code,
+                                          device=dev, dtype=dtype, assume_initial_nonzero=assume_initial_nonzero,
+                                          cuda_graph=cuda_graph)
+    return [flows[r] for r in range(len(problems))]
 
 
 def apply_flow_to_sphere(sphere_vertices, flow, *, unit_sphere_vertices=None, inverse: bool = True, device="auto",
