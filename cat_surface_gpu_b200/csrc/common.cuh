@@ -117,6 +117,19 @@ __device__ __forceinline__ unsigned long long make_word(float x, unsigned int ve
 __device__ __forceinline__ float word_value(unsigned long long w) { return __uint_as_float(static_cast<unsigned>(w)); }
 __device__ __forceinline__ unsigned int word_version(unsigned long long w) { return static_cast<unsigned>(w >> 32); }
 
+// Work distribution of a dataflow kernel with few items per step (the
+// coloured SOR): the items of successive wavefront steps are dealt to a CTA's
+// groups round-robin without restarting at group 0 each step: item k of a
+// step goes to group (rot + k) mod groups, rot = items dealt in earlier steps
+// mod groups.  Each group still takes its items in step order (progress is
+// guaranteed as in the step-by-step form), and groups without an item in this
+// step take the next steps' items, so several steps are in flight in a CTA.
+// Returns the first item index of this warp's first group (<= 0); the warp's
+// groups then take k = first + g + j * groups, valid while 0 <= k < count.
+__device__ __forceinline__ int dealt_first(int rot, int warp_first_group, int groups) {
+    return -(((rot - warp_first_group) % groups + groups) % groups);
+}
+
 // Bounded wait of one warp in a dataflow kernel: lane 0 checks the clock and
 // the status word every 64 polls; true (the same in every lane) means give up
 // -- the status is CSG_ERR_TIMEOUT (recorded here) or another CTA's error.

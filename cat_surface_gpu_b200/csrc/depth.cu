@@ -279,6 +279,8 @@ struct SorParams {
     int max_row, nloc_max;  // shared-memory image (0: rows read from global memory)
     double relaxation;
     unsigned long long timeout_ns;
+    unsigned long long* pub;  // dataflow form: x as versioned words, 2 per (surface, vertex)
+    int* level_of;            // dataflow form: the schedule level of every vertex
 };
 
 __device__ __forceinline__ int owned_below(int bound, int c, int nc) { return bound > c ? (bound - c + nc - 1) / nc : 0; }
@@ -419,6 +421,224 @@ __global__ void __launch_bounds__(512) k_depth_sor(SorParams p) {
         }
         if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
     }
+}
+
+// ---------------------------------------------------------------- SOR, dataflow form
+//
+// The sweeps without a grid barrier per step, as the Surf2Sphere dataflow
+// kernels do it: x[b][v] is published as two versioned words (the low and the
+// high 32 bits of the double, each with the number of sweeps completed).  In
+// colour-major Gauss-Seidel order a neighbour u comes before v exactly when
+// level(u) < level(v) (the schedule's potential grows along that order), so
+// sweep s of v needs earlier neighbours at version s and later neighbours and
+// v itself at version s - 1, and none can be further ahead.  A group polls the
+// row's distinct columns (its ring), stages their x in shared memory, forms
+// the row sum in entry order and publishes the update.
+
+constexpr int kSRing = 16;  // the vertex and at most 15 distinct neighbours
+
+__global__ void k_level_of(const int* __restrict__ order, const int* __restrict__ level_begin,
+                           const int* __restrict__ level_end, int* __restrict__ level_of) {
+    const int l = blockIdx.y;
+    for (int pos = level_begin[l] + blockIdx.x * blockDim.x + threadIdx.x; pos < level_end[l];
+         pos += gridDim.x * blockDim.x)
+        level_of[order[pos]] = l;
+}
+
+__device__ __forceinline__ double words_value(unsigned long long lo, unsigned long long hi) {
+    return __hiloint2double(static_cast<int>(static_cast<unsigned>(hi)), static_cast<int>(static_cast<unsigned>(lo)));
+}
+
+template <int G>
+__device__ __forceinline__ bool sor_row_df(const SorParams& p, int b, int v, const int* ring, int nring,
+                                           const unsigned char* code, const double* rval, int len, double rhs,
+                                           double diag, unsigned int s, double* ringx) {
+    constexpr int kQ = (kSRing + G - 1) / G;
+    constexpr int kE = 32 / G;  // entries per lane and block of 32
+    const int lane = threadIdx.x & 31;
+    const int glane = lane & (G - 1);
+    const int gbase = lane & ~(G - 1);
+    const unsigned long long* pub = p.pub + 2LL * p.n * b;
+    if (v < 0) {
+        nring = 0;
+        len = 0;
+    }
+    unsigned int polls = 0;
+    unsigned long long start = 0;
+    int who[kQ];
+    unsigned int need[kQ];
+#pragma unroll
+    for (int q = 0; q < kQ; ++q) {
+        const int k = glane + q * G;
+        who[q] = k < nring ? (ring[k] & 0x7fffffff) : -1;
+        need[q] = (k < nring && (ring[k] < 0)) ? s : s - 1;  // sign bit: the neighbour comes first
+    }
+    while (true) {
+        unsigned long long w[kQ][2];
+#pragma unroll
+        for (int q = 0; q < kQ; ++q)
+            if (who[q] >= 0) {
+                w[q][0] = csg::ld_word(pub + 2LL * who[q]);
+                w[q][1] = csg::ld_word(pub + 2LL * who[q] + 1);
+            }
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < kQ; ++q)
+            if (who[q] >= 0) {
+                ok = ok && csg::word_version(w[q][0]) == need[q] && csg::word_version(w[q][1]) == need[q];
+                ringx[glane + q * G] = words_value(w[q][0], w[q][1]);
+            }
+        if (__all_sync(kFull, ok)) break;
+        if (csg::warp_wait_expired(p.ctl, p.timeout_ns, polls, start)) return false;
+    }
+    __syncwarp();
+    const int wlen = __reduce_max_sync(kFull, len);
+    double sum = 0.0;
+    for (int base = 0; base < wlen; base += G * kE) {
+        double prod[kE];
+#pragma unroll
+        for (int q = 0; q < kE; ++q) {
+            const int j = base + q * G + glane;
+            prod[q] = j < len ? rval[j] * ringx[code[j]] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kE; ++q) {
+            if (base + q * G >= wlen) break;  // warp-uniform
+#pragma unroll
+            for (int i = 0; i < G; ++i) {
+                const double t = __shfl_sync(kFull, prod[q], gbase + i);
+                if (base + q * G + i < len) sum = sum + t;
+            }
+        }
+    }
+    const double xv = v >= 0 ? ringx[0] : 0.0;
+    __syncwarp();  // every lane is done with `ringx` before the next row overwrites it
+    if (v >= 0 && glane < 2) {
+        const double nx = xv + p.relaxation * (rhs - sum) / diag;
+        const unsigned int half = glane == 0 ? static_cast<unsigned>(__double2loint(nx))
+                                             : static_cast<unsigned>(__double2hiint(nx));
+        csg::st_word(p.pub + 2LL * p.n * b + 2LL * v + glane, csg::make_word(__uint_as_float(half), s));
+    }
+    return true;
+}
+
+template <int G>
+__global__ void __launch_bounds__(512) k_depth_sor_df(SorParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (failed(p.ctl)) return;  // set by an earlier kernel: the same for every CTA
+    const int c = blockIdx.x, nc = gridDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    const int groups = blockDim.x / G;
+    const int warp_first_group = (threadIdx.x >> 5) * (32 / G);
+    const int my_group = (threadIdx.x & 31) / G;
+    const int L = p.n_levels, D = p.stride;
+    // shared-memory image: per group kSRing staged x; values [batch][nloc][max_row];
+    // rhs and diagonal [batch][nloc]; rings [nloc][kSRing] (sign bit: the neighbour
+    // comes first); entry codes [nloc][max_row]; ids, ring sizes, row lengths,
+    // levels; per-level owned ranges
+    const long long nb = static_cast<long long>(p.batch) * p.nloc_max;
+    double* ringx = reinterpret_cast<double*>(smem_raw) + (threadIdx.x / G) * kSRing;
+    double* sval = reinterpret_cast<double*>(smem_raw) + (blockDim.x / G) * kSRing;
+    double* srhs = sval + nb * p.max_row;
+    double* sdiag = srhs + nb;
+    int* sring = reinterpret_cast<int*>(sdiag + nb);
+    int* svid = sring + p.nloc_max * kSRing;
+    int* snring = svid + p.nloc_max;
+    int* slen = snring + p.nloc_max;
+    int* slev = slen + p.nloc_max;
+    int* lbeg = slev + p.nloc_max;
+    int* lend = lbeg + L;
+    unsigned char* scode = reinterpret_cast<unsigned char*>(lend + L);
+    const int nloc = owned_below(p.n, c, nc);
+    for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
+        const int v = p.order[c + i * nc];
+        const long long row = 3LL * p.inc_off[v] + v;
+        int len = 3 * (p.inc_off[v + 1] - p.inc_off[v]) + 1;
+        bool bad = len > p.max_row;
+        if (bad) len = p.max_row;
+        const int lv = p.level_of[v];
+        int* ring = sring + i * kSRing;
+        int nr = 1;
+        ring[0] = v;
+        for (int j = 0; j < len; ++j) {
+            const int u = p.col[row + j];
+            int at = 0;
+            while (at < nr && (ring[at] & 0x7fffffff) != u) ++at;
+            if (at == nr) {
+                if (nr == kSRing) {
+                    bad = true;
+                    at = 0;
+                } else {
+                    ring[nr++] = p.level_of[u] < lv ? (u | static_cast<int>(0x80000000u)) : u;
+                }
+            }
+            scode[static_cast<long long>(i) * p.max_row + j] = static_cast<unsigned char>(at);
+        }
+        if (bad && atomicCAS(&p.ctl->status, CSG_OK, CSG_ERR_ARG) == CSG_OK) p.ctl->where = -1;
+        snring[i] = nr;
+        svid[i] = v;
+        slen[i] = len;
+        slev[i] = lv;
+        for (int b = 0; b < p.batch; ++b) {
+            const long long slot = static_cast<long long>(b) * p.nloc_max + i;
+            for (int j = 0; j < len; ++j) sval[slot * p.max_row + j] = p.val[b * p.nnz + row + j];
+            const long long at = static_cast<long long>(b) * p.n + v;
+            srhs[slot] = p.rhs[at];
+            sdiag[slot] = p.diag[at];
+        }
+    }
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+        lbeg[l] = owned_below(p.level_begin[l], c, nc);
+        lend[l] = owned_below(p.level_end[l], c, nc);
+    }
+    for (long long q = tid; q < static_cast<long long>(p.batch) * p.n; q += nthreads) {
+        const double x = p.x[q];
+        csg::st_word(p.pub + 2 * q, csg::make_word(__uint_as_float(static_cast<unsigned>(__double2loint(x))), 0u));
+        csg::st_word(p.pub + 2 * q + 1, csg::make_word(__uint_as_float(static_cast<unsigned>(__double2hiint(x))), 0u));
+    }
+    unsigned int phase = 0;
+    int barrier_id = 0;
+    if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    if (csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) return;  // an oversized row: same answer in every CTA
+    const int span = (p.sweeps - 1) * D;  // host guarantees span + L < 2^31
+    const int nsteps = span + L;
+    int r = 0, rot = 0;
+    for (int t = 0; t < nsteps; ++t, r = (r + 1 == D) ? 0 : r + 1) {
+        int lo = t - span;
+        if (lo < r) lo = r;
+        const int hi = t < L ? t : (L - 1) - ((L - 1 - r) % D + D) % D;
+        if (hi < lo) continue;
+        const int i0 = lbeg[lo], i1 = lend[hi];
+        const int count = i1 - i0;
+        for (int k0 = csg::dealt_first(rot, warp_first_group, groups); k0 < count * p.batch; k0 += groups) {
+            const int w = k0 + my_group;
+            int b = 0, i = 0, v = -1, nring = 0, len = 0;
+            unsigned int sweep = 0;
+            const int* ring = nullptr;
+            const unsigned char* code = nullptr;
+            const double* rval = nullptr;
+            double rhs = 0.0, diag = 1.0;
+            if (w >= 0 && w < count * p.batch) {
+                b = w / count;
+                i = i0 + w % count;
+                const long long slot = static_cast<long long>(b) * p.nloc_max + i;
+                v = svid[i];
+                nring = snring[i];
+                len = slen[i];
+                ring = sring + i * kSRing;
+                code = scode + static_cast<long long>(i) * p.max_row;
+                rval = sval + slot * p.max_row;
+                rhs = srhs[slot];
+                diag = sdiag[slot];
+                sweep = static_cast<unsigned int>(1 + (t - slev[i]) / D);
+            }
+            if (!sor_row_df<G>(p, b, v, ring, nring, code, rval, len, rhs, diag, sweep, ringx)) return;
+        }
+        rot = (rot + count * p.batch) % groups;
+    }
+    if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    for (long long q = tid; q < static_cast<long long>(p.batch) * p.n; q += nthreads)
+        p.x[q] = words_value(csg::ld_word(p.pub + 2 * q), csg::ld_word(p.pub + 2 * q + 1));
 }
 
 // residual terms (rhs - A x)^2 per vertex (also the matrix-vector product of CG's start)
@@ -620,7 +840,7 @@ __global__ void __launch_bounds__(512) k_depth_cg(CgParams p) {
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
 struct Layout {
-    size_t ctl, rec, col, val, areas, diag, mc, rhs, rhs_norm, runs, terms, r, z, pv, ap, total;
+    size_t ctl, rec, col, val, areas, diag, mc, rhs, rhs_norm, runs, terms, r, z, pv, ap, pub, level_of, total;
 };
 
 Layout layout(int n, int nf, int batch, long long nnz) {
@@ -647,6 +867,8 @@ Layout layout(int n, int nf, int batch, long long nnz) {
     L.z = take(8 * nb);
     L.pv = take(8 * nb);
     L.ap = take(8 * nb);
+    L.pub = take(16 * nb);
+    L.level_of = take(4 * static_cast<size_t>(n));
     L.total = at;
     return L;
 }
@@ -675,8 +897,35 @@ int launch_sor(const SorParams& params, int n_ctas, int threads, size_t smem, cu
 }
 
 template <int G>
+int launch_sor_df(const SorParams& params, int n_ctas, int threads, size_t smem, cudaStream_t s) {
+    auto kernel = k_depth_sor_df<G>;
+    int device = 0, sms = 0, per_sm = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CSG_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    if (per_sm < 1 || n_ctas > per_sm * sms)
+        return csg::fail(CSG_ERR_LAUNCH, "depth SOR: %d CTAs x %d threads (%zu B smem) cannot be co-resident", n_ctas,
+                         threads, smem);
+    SorParams p = params;
+    void* args[] = {&p};
+    CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(n_ctas), dim3(threads), args,
+                                               smem, s));
+    csg::note_launch();
+    return CSG_OK;
+}
+
+template <int G>
 int dispatch_sor(SorParams p, int n_ctas, int threads, cudaStream_t s) {
     p.nloc_max = (p.n + n_ctas - 1) / n_ctas;
+    // dataflow form: a row's distinct columns (at most 2 max_incidences + 1) fit the ring
+    if (p.pub && p.max_row > 0 && p.max_row <= 255 && 2 * ((p.max_row - 1) / 3) + 1 <= kSRing) {
+        const long long nb = static_cast<long long>(p.batch) * p.nloc_max;
+        const size_t smem = sizeof(double) * (static_cast<size_t>(threads / G) * kSRing + nb * (p.max_row + 2)) +
+                            sizeof(int) * (static_cast<size_t>(p.nloc_max) * (kSRing + 5) + 2 * static_cast<size_t>(p.n_levels)) +
+                            static_cast<size_t>(p.nloc_max) * p.max_row;
+        if (smem <= kMaxRowSmem) return launch_sor_df<G>(p, n_ctas, threads, smem, s);
+    }
     const size_t ints = static_cast<size_t>(p.nloc_max) * (p.max_row + 2) + 2 * static_cast<size_t>(p.n_levels);
     const size_t smem = sizeof(double) * static_cast<size_t>(p.batch) * p.nloc_max * (p.max_row + 3) + sizeof(int) * ints;
     if (p.max_row > 0 && smem <= kMaxRowSmem) return launch_sor<G, true>(p, n_ctas, threads, smem, s);
@@ -706,7 +955,8 @@ int csg_depth_potential(const float* geometry, int batch, int n, const int32_t* 
         return csg::fail(CSG_ERR_ARG, "depth potential: bad arguments");
     if (solver != CSG_DEPTH_SOR && solver != CSG_DEPTH_PCG)
         return csg::fail(CSG_ERR_ARG, "depth potential: solver must be CSG_DEPTH_SOR or CSG_DEPTH_PCG");
-    if (solver == CSG_DEPTH_SOR && (!order || !level_begin || !level_end || n_levels < 1 || level_stride < 1))
+    if (solver == CSG_DEPTH_SOR &&
+        (!order || !level_begin || !level_end || n_levels < 1 || n_levels > 65535 || level_stride < 1))
         return csg::fail(CSG_ERR_ARG, "depth potential: the SOR solver needs the colour-major wavefront schedule");
     if (solver == CSG_DEPTH_PCG && (max_iter < 1 || batch > kMaxCgBatch))
         return csg::fail(CSG_ERR_ARG, "depth potential: CG needs max_iter >= 1 and batch <= %d", kMaxCgBatch);
@@ -779,6 +1029,10 @@ int csg_depth_potential(const float* geometry, int batch, int n, const int32_t* 
             p.max_row = 3 * max_incidences + 1;
             p.relaxation = relaxation;
             p.timeout_ns = timeout_ns;
+            p.pub = reinterpret_cast<unsigned long long*>(base + L.pub);
+            p.level_of = reinterpret_cast<int*>(base + L.level_of);
+            (csg::note_launch(), k_level_of<<<dim3(blocks(n, kThreads) > 64 ? 64 : blocks(n, kThreads), n_levels),
+                                              kThreads, 0, s>>>(order, level_begin, level_end, p.level_of));
             int rc;
             switch (lanes_per_row) {
                 case 8: rc = dispatch_sor<8>(p, n_ctas, threads_per_cta, s); break;

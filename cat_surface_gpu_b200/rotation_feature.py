@@ -126,8 +126,8 @@ def depth_potential(geometries: torch.Tensor, topology: DepthTopology, *, solver
     areas = torch.empty((batch, topology.n), dtype=torch.float64, device=device) if with_geometry else None
     scratch = torch.empty(int(lib.csg_depth_scratch_bytes(topology.n, topology.nf, batch)), dtype=torch.uint8,
                           device=device)
-    # measured on the 40,962-point stencil sphere, two sides, 1,000 sweeps: 4 lanes x 512 threads 22.7 ms,
-    # 8 lanes 30.8 ms, 16 lanes 37.9 ms
+    # measured on the 40,962-point stencil sphere, two sides, 1,000 sweeps: 4 lanes x 512 threads 18.4 ms,
+    # 8 lanes 19.0 ms, 16 lanes 32.0 ms
     cfg = {"n_ctas": 0, "threads_per_cta": 512, "lanes_per_row": 4}
     if launch:
         cfg.update(launch)
