@@ -221,33 +221,35 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
     // (a non-converging relaxation means a positive cycle, or too slow a
     // convergence to be worth it; both keep the last feasible D).
     {
+        // unique lower and higher face neighbours of every vertex, as two CSR arrays
         std::vector<int32_t> lo_off(n + 1, 0), hi_off(n + 1, 0);
         std::vector<int32_t> lo_nb, hi_nb;
+        lo_nb.reserve(static_cast<size_t>(3) * n_faces);
+        hi_nb.reserve(static_cast<size_t>(3) * n_faces);
         {
-            std::vector<std::vector<int32_t>> lower(n), higher(n);
-            for (int v = 0; v < n; ++v)
-                for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
-                    for (int k = 0; k < 3; ++k) {
-                        const int u = slot_tri[4 * s + k];
-                        if (u < v) lower[v].push_back(u);
-                        if (u > v) higher[v].push_back(u);
-                    }
+            std::vector<int32_t> ring;
             for (int v = 0; v < n; ++v) {
-                std::sort(lower[v].begin(), lower[v].end());
-                lower[v].erase(std::unique(lower[v].begin(), lower[v].end()), lower[v].end());
-                std::sort(higher[v].begin(), higher[v].end());
-                higher[v].erase(std::unique(higher[v].begin(), higher[v].end()), higher[v].end());
-                lo_off[v + 1] = lo_off[v] + static_cast<int32_t>(lower[v].size());
-                hi_off[v + 1] = hi_off[v] + static_cast<int32_t>(higher[v].size());
-                lo_nb.insert(lo_nb.end(), lower[v].begin(), lower[v].end());
-                hi_nb.insert(hi_nb.end(), higher[v].begin(), higher[v].end());
+                ring.clear();
+                for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
+                    for (int k = 0; k < 3; ++k) ring.push_back(slot_tri[4 * s + k]);
+                std::sort(ring.begin(), ring.end());
+                ring.erase(std::unique(ring.begin(), ring.end()), ring.end());
+                for (int32_t u : ring) {
+                    if (u < v) lo_nb.push_back(u);
+                    if (u > v) hi_nb.push_back(u);
+                }
+                lo_off[v + 1] = static_cast<int32_t>(lo_nb.size());
+                hi_off[v + 1] = static_cast<int32_t>(hi_nb.size());
             }
         }
         std::vector<int32_t> best = levels, f;
         int last_iterations = 64;
         for (int trial = stride - 1; trial >= 2; --trial) {
             f = best;
-            const int cap = std::min(4000, 4 * last_iterations + 64);
+            // feasible strides converge in a few relaxation sweeps (3 to 10 on
+            // cortical hulls); a stride that needs many more than the last one
+            // is treated as infeasible -- only the schedule's length depends on it
+            const int cap = std::min(4000, 3 * last_iterations + 16);
             bool converged = false;
             int it = 0;
             for (; it < cap && !converged; ++it) {

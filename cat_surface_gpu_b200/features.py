@@ -31,11 +31,12 @@ def _topology(faces: np.ndarray, n_points: int, device: torch.device):
     count = _native.check(lib.csg_mesh_neighbours(n_points, f.ctypes.data, f.shape[0], off.ctypes.data,
                                                   nbr.ctypes.data, nbr.size), "csg_mesh_neighbours")
     nbr = nbr[: max(1, count)]
-    # per-vertex incidences sorted by (corner, face): the reference's three index_add_ passes
-    vertex = f.T.reshape(-1).astype(np.int64)
-    corner = np.repeat(np.arange(3), f.shape[0])
-    face = np.tile(np.arange(f.shape[0]), 3)
-    order = np.lexsort((face, corner, vertex))
+    # per-vertex incidences sorted by (corner, face): the reference's three index_add_ passes.
+    # The entries are laid out corner-major with faces ascending, so a stable sort by vertex keeps that order.
+    vertex = f.T.reshape(-1)
+    corner = np.repeat(np.arange(3, dtype=np.int32), f.shape[0])
+    face = np.tile(np.arange(f.shape[0], dtype=np.int32), 3)
+    order = np.argsort(vertex, kind="stable")
     inc = ((face[order] << 2) | corner[order]).astype(np.int32)
     inc_off = np.concatenate(([0], np.cumsum(np.bincount(vertex, minlength=n_points)))).astype(np.int32)
     tensors = tuple(torch.from_numpy(a).to(device) for a in (off, nbr, inc_off, inc))

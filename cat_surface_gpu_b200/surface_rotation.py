@@ -373,10 +373,14 @@ class RotationGridIndexDevice:
                     centroid += simplex[index]
             centroid /= 3.0
             reflected = centroid + (centroid - simplex[highest])
-            fr = cost(reflected[None])[0]
+            expanded = centroid + 2.0 * (reflected - centroid)
+            contracted = centroid + 0.5 * (simplex[highest] - centroid)
+            # The three trial points depend only on the simplex, and each cost is
+            # computed on its own (fixed summation order), so one launch evaluates
+            # all three; the branch below uses exactly the costs the reference's
+            # one-at-a-time evaluation would, and the same decisions follow.
+            fr, fe, fc = cost(np.stack((reflected, expanded, contracted)))
             if fr < f[lowest]:
-                expanded = centroid + 2.0 * (reflected - centroid)
-                fe = cost(expanded[None])[0]
                 if fe < fr:
                     simplex[highest], f[highest] = expanded, fe
                 else:
@@ -384,8 +388,6 @@ class RotationGridIndexDevice:
             elif fr < f[second]:
                 simplex[highest], f[highest] = reflected, fr
             else:
-                contracted = centroid + 0.5 * (simplex[highest] - centroid)
-                fc = cost(contracted[None])[0]
                 if fc < f[highest]:
                     simplex[highest], f[highest] = contracted, fc
                 else:
