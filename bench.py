@@ -365,10 +365,11 @@ class Hemisphere:
         self.rings = _topology(faces, meshes["surface"].shape[0], device)
         self.pristine = torch.from_numpy(meshes["surface"]).to(device)
         self.points = torch.empty_like(self.pristine)
+        self.prefix_copy = torch.empty_like(self.pristine)
         prefix_radius = projection_radius(meshes["prefix"])
         self.launch = surf2sphere.tuned_areal_launch(torch.from_numpy(meshes["prefix"]).to(device), self.plan_device,
                                                      self.plan, arithmetic="cat", radius=prefix_radius) \
-            if autotune_launch else dict(surf2sphere.DEFAULT_LAUNCH)
+            if autotune_launch else surf2sphere.sweep_launch_default(device)
         self.scratch = None
         self.pre_scratch = None
         self.meshes_in = (GiftiMesh(meshes["surface"], faces),
@@ -390,16 +391,16 @@ class Hemisphere:
         self.pre_scratch = surf2sphere.preprocess_device(self.points, self.faces_device, self.rings, self.plan_device,
                                                          self.plan, stop_at=5, scratch=self.pre_scratch)
         events[1].record(stream)
-        prefix = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(self.points.cpu().numpy(), area)
-        radius = projection_radius(prefix)
-        self.points.copy_(torch.from_numpy(prefix))
+        surf2sphere.ellipsoid_to_sphere_device(self.points, area)
+        self.prefix_copy.copy_(self.points)  # kept for the parity check against the binary's stage-5 output
+        radius = surf2sphere.projection_radius_device(self.points)
         events[2].record(stream)
         self.scratch = surf2sphere.areal_sweeps_device(
             self.points, self.plan_device, self.plan, iterations=SWEEPS + 1, project_every=1000, radius=radius,
             arithmetic="cat", launch=self.launch, scratch=self.scratch)
         events[3].record(stream)
-        smoothed = self.points.cpu().numpy()
-        sphere = surf2sphere.convert_ellipsoid_to_sphere_with_surface_area(smoothed, area)
+        sphere = surf2sphere.ellipsoid_to_sphere_device(self.points, area).cpu().numpy()
+        prefix = self.prefix_copy
         surface, target_surface, target_sphere = self.meshes_in
         final, angle, cost, timings = register_meshes(
             surface, GiftiMesh(sphere, self.meshes["faces"]), target_surface, target_sphere, device=self.device,
@@ -645,7 +646,7 @@ def run_native(args):
     # the sweeps against the upstream binary, and a float32-DARTEL chain against the float64 one
     parity = {"chain_vs_cpu_reference": error_stats(meshes["chain_final"], final),
               "surf2sphere_vs_binary": error_stats(meshes["binary_sphere"], sphere),
-              "stages_1_5_vs_binary": error_stats(meshes["prefix"], prefix)}
+              "stages_1_5_vs_binary": error_stats(meshes["prefix"], prefix.cpu().numpy())}
     hemi.step(dartel_dtype=torch.float32)  # warm (graph capture for float32)
     torch.cuda.synchronize()
     f0 = time.perf_counter()

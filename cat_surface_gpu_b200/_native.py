@@ -40,12 +40,14 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_preprocess_scratch_bytes": (c_size_t, [_I, _I]),
     "csg_surf2sphere_preprocess": (_I, [_P, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, c_size_t, _I,
                                         _I, _I, ctypes.c_double, _P]),
+    "csg_ellipsoid_to_sphere": (_I, [_P, _I, c_double, _P, c_size_t, _P]),
     "csg_depth_scratch_bytes": (c_size_t, [_I, _I, _I]),
     "csg_depth_potential": (_I, [_P, _I, _I, _P, _I, _P, _P, _I, c_double, _I, _I, c_double, c_double, _P, _P, _P, _I,
                                  _I, _P, _P, _P, _P, _P, _P, c_size_t, _I, _I, _I, c_double, _P]),
     "csg_mesh_incidence": (_I, [_I, _P, _I, _P, _P]),
     "csg_mesh_neighbours": (_I, [_I, _P, _I, _P, _P, _I]),
     "csg_colour_groups": (_I, [_I, _P, _P, _P, _P]),
+    "csg_normalise_sphere": (_I, [_I, _P, _P]),
     "csg_dependency_levels": (_I, [_I, _P, _P, _P]),
     "csg_greedy_colours": (_I, [_I, _P, _P, _P]),
     "csg_areal_plan_build": (_I, [_I, _P, _I, _P, _P, _P, _P, _P, _P]),

@@ -634,6 +634,62 @@ __global__ void k_select(const double* __restrict__ comp, const int* __restrict_
     selected[v] = __ddiv_rn(s, static_cast<double>(nb_off[v + 1] - nb_off[v] + 1)) > threshold;
 }
 
+// ---------------------------------------------------------------- ellipsoid to sphere
+
+// convert_ellipsoid_to_sphere_with_surface_area (surf2sphere.py:919-937) on the
+// device: float32 bounds, float32 half-axes (|lo| + |hi|) / 2 clamped to 1e-20,
+// then per vertex in float64 x / a, |x / a|, radius x / |x / a| / a, float32
+// store (a zero-length vertex becomes the origin).  Min and max are exact in
+// any order, so one CTA reduces them; the result equals the host arithmetic.
+__global__ void k_ellipsoid_bounds(const float* __restrict__ p, int n, float* __restrict__ axes) {
+    __shared__ float lo[3][32], hi[3][32];
+    float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int v = threadIdx.x; v < n; v += blockDim.x)
+        for (int k = 0; k < 3; ++k) {
+            const float x = p[3LL * v + k];
+            l[k] = fminf(l[k], x);
+            h[k] = fmaxf(h[k], x);
+        }
+    for (int k = 0; k < 3; ++k)
+        for (int off = 16; off >= 1; off >>= 1) {
+            l[k] = fminf(l[k], __shfl_xor_sync(kFull, l[k], off));
+            h[k] = fmaxf(h[k], __shfl_xor_sync(kFull, h[k], off));
+        }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int k = 0; k < 3; ++k) {
+            lo[k][warp] = l[k];
+            hi[k][warp] = h[k];
+        }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        const int k = threadIdx.x;
+        float a = INFINITY, b = -INFINITY;
+        for (int w = 0; w < (blockDim.x + 31) / 32; ++w) {
+            a = fminf(a, lo[k][w]);
+            b = fmaxf(b, hi[k][w]);
+        }
+        const float half = __fmul_rn(__fadd_rn(fabsf(a), fabsf(b)), 0.5f);
+        axes[k] = half < 1.0e-20f ? 1.0e-20f : half;
+    }
+}
+
+__global__ void k_ellipsoid_scale(float* __restrict__ p, int n, const float* __restrict__ axes, double radius) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    double x[3], s[3];
+    for (int k = 0; k < 3; ++k) {
+        x[k] = p[3LL * v + k];
+        s[k] = __ddiv_rn(x[k], static_cast<double>(axes[k]));
+    }
+    const double norm = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(s[0], s[0]), __dmul_rn(s[1], s[1])), __dmul_rn(s[2], s[2])));
+    for (int k = 0; k < 3; ++k) {
+        const double r = norm != 0.0 ? __ddiv_rn(__ddiv_rn(__dmul_rn(radius, x[k]), norm), static_cast<double>(axes[k]))
+                                     : 0.0;
+        p[3LL * v + k] = __double2float_rn(r);
+    }
+}
+
 // ---------------------------------------------------------------- host side
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
@@ -767,6 +823,18 @@ inline unsigned blocks(long long n, int threads) { return static_cast<unsigned>(
 }  // namespace
 
 extern "C" {
+
+int csg_ellipsoid_to_sphere(float* points, int n, double radius, void* scratch, size_t scratch_bytes,
+                            csg_stream_t stream) {
+    if (!points || n < 1 || !scratch || scratch_bytes < 16 || !(radius >= 0.0))
+        return csg::fail(CSG_ERR_ARG, "ellipsoid to sphere: bad arguments (16 bytes of scratch)");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    auto* axes = static_cast<float*>(scratch);
+    (csg::note_launch(), k_ellipsoid_bounds<<<1, 1024, 0, s>>>(points, n, axes));
+    (csg::note_launch(), k_ellipsoid_scale<<<blocks(n, kThreads), kThreads, 0, s>>>(points, n, axes, radius));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
 
 size_t csg_preprocess_scratch_bytes(int n_vertices, int n_faces) {
     if (n_vertices < 4 || n_faces < 4) return 0;

@@ -2,6 +2,7 @@
 // Surf2Sphere sweeps.  Plain C++, no device memory.
 #include <atomic>
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -137,6 +138,25 @@ int csg_colour_groups(int n_vertices, const int32_t* nbr_off, const int32_t* nbr
     std::vector<int32_t> fill(colour_off, colour_off + n_colours);
     for (int v = 0; v < n_vertices; ++v) members[fill[colour[v]]++] = v;
     return n_colours;
+}
+
+int csg_normalise_sphere(int n_vertices, const float* in, float* out) {
+    if (n_vertices < 1 || !in || !out) return csg::fail(CSG_ERR_ARG, "bad arguments");
+    // centre: the sequential float64 sum of the float32 coordinates, divided by n
+    double sum[3] = {0.0, 0.0, 0.0};
+    for (int v = 0; v < n_vertices; ++v)
+        for (int k = 0; k < 3; ++k) sum[k] = sum[k] + static_cast<double>(in[3LL * v + k]);
+    double centre[3];
+    for (int k = 0; k < 3; ++k) centre[k] = sum[k] / static_cast<double>(n_vertices);
+    for (int v = 0; v < n_vertices; ++v) {
+        double c[3];
+        for (int k = 0; k < 3; ++k) c[k] = static_cast<double>(static_cast<float>(static_cast<double>(in[3LL * v + k]) - centre[k]));
+        const double length = std::sqrt((c[0] * c[0] + c[1] * c[1]) + c[2] * c[2]);
+        if (!std::isfinite(length) || length == 0.0) return csg::fail(CSG_ERR_ARG, "sphere vertex %d cannot be normalised", v);
+        const double inv = 1.0 / length;
+        for (int k = 0; k < 3; ++k) out[3LL * v + k] = static_cast<float>(c[k] * inv);
+    }
+    return CSG_OK;
 }
 
 int csg_dependency_levels(int n_vertices, const int32_t* nbr_off, const int32_t* nbr, int32_t* levels) {

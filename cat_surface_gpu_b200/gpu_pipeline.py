@@ -33,6 +33,7 @@ from typing import Sequence
 import numpy as np
 import torch
 
+from . import _native
 from .device import resolve_device
 from .gifti import GiftiMesh, read_gifti_mesh, write_gifti_mesh
 from .rotation_pipeline import RotationPipeline, read_rotation_values
@@ -85,13 +86,11 @@ def normalise_sphere(vertices: np.ndarray) -> np.ndarray:
     value = np.ascontiguousarray(np.asarray(vertices, dtype=np.float32))
     if value.ndim != 2 or value.shape[1] != 3:
         raise ValueError(f"Sphere vertices must have shape [n, 3], got {value.shape}")
-    centre = np.cumsum(value.astype(np.float64), axis=0)[-1]
-    centered = (value.astype(np.float64) - centre / value.shape[0]).astype(np.float32)
-    c = centered.astype(np.float64)
-    length = np.sqrt((c[:, 0] * c[:, 0] + c[:, 1] * c[:, 1]) + c[:, 2] * c[:, 2])
-    if not np.all(np.isfinite(length)) or np.any(length == 0.0):
+    out = np.empty_like(value)
+    rc = _native.library().csg_normalise_sphere(value.shape[0], _native.ptr(value), _native.ptr(out))
+    if rc != 0:
         raise ValueError("Sphere contains a vertex that cannot be normalized")
-    return np.ascontiguousarray((c * (1.0 / length)[:, None]).astype(np.float32))
+    return out
 
 
 def rotation_matrix_from_angles(angles) -> torch.Tensor:

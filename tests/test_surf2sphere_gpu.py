@@ -198,3 +198,20 @@ def test_division_by_three_is_correctly_rounded(native_library):
                                                    _native.stream_handle()), "csg_selftest_div3")
     assert torch.equal(a.view(torch.int64), b.view(torch.int64))
     np.testing.assert_array_equal(a.cpu().numpy(), x / 3.0)
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_device_ellipsoid_step_and_radius_equal_host(s2s, name):
+    """csg_ellipsoid_to_sphere and the device projection radius equal the host NumPy arithmetic bit for bit."""
+
+    g = load_surf2sphere_golden(name)
+    area = float(g["source_area"])
+    for points in (g["prefix"], g["final"]):
+        want = s2s.convert_ellipsoid_to_sphere_with_surface_area(points, area)
+        dev = torch.from_numpy(np.ascontiguousarray(points, dtype=np.float32)).to("cuda:0")
+        got = s2s.ellipsoid_to_sphere_device(dev, area).cpu().numpy()
+        np.testing.assert_array_equal(got, want)
+        assert s2s.projection_radius_device(dev) == float(np.sqrt(np.max(np.sum(want.astype(np.float64) ** 2, axis=1))))
+    zeros = torch.zeros((5, 3), dtype=torch.float32, device="cuda:0")
+    np.testing.assert_array_equal(s2s.ellipsoid_to_sphere_device(zeros, 1.0).cpu().numpy(),
+                                  s2s.convert_ellipsoid_to_sphere_with_surface_area(np.zeros((5, 3), np.float32), 1.0))
