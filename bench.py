@@ -22,7 +22,7 @@ ranks.
 ``e2e``: the same hemisphere through the public API with files --
 ``run_cat_surf2sphere_gpu`` (every stage on the GPU) from the surface GIFTI to
 the sphere GIFTI, then ``run_cat_surface_gpu_pipeline`` on the four GIFTI
-files.
+files; two untimed calls, then the mean of three timed ones.
 
 Also on the line: ``batched_rotation`` (8 surfaces of 40,962-163,842 points
 x 4,096 uniform quaternions x 2 features in one persistent launch vs one
@@ -62,6 +62,9 @@ UNIT = "s/hemisphere"
 WORKLOAD = ("Surf2Sphere (stages 1-5 + 4,999 ordered sweeps, 61,442 v / 122,880 f folded hull) + SurfWarp steps=2 runs=2 -avg "
             "to a second 61,442-v hull, 256x128 float64 DARTEL sheet")
 SWEEPS = 4999
+# dram__bytes_read.sum + dram__bytes_write.sum of areal_dataflow_kernel<CAT, 8> over 200 sweeps of the
+# 61,442-vertex hull (9.1 MB + 0.85 MB; ncu summary in profiles/areal_dataflow_61k_hull_200sweeps.md)
+SWEEP_DRAM_BYTES = 9.95e6
 SHEET = (256, 128)
 CHAIN = dict(steps=2, runs=2, avg=True, loop=6, sheet_size=SHEET, rotation_feature_backend="cuda",
              rotation_feature_solver="colored-sor")
@@ -557,7 +560,7 @@ def batched_dartel_leg(device, repeats: int = 5) -> dict:
             events[r + 1].record(stream)
         events[-1].synchronize()
         plain_lat.extend(events[r].elapsed_time(events[r + 1]) for r in range(regs))
-    unit = torch.as_tensor(resampling_sphere(5)[0], dtype=torch.float32, device=device)
+    unit = torch.from_numpy(np.array(resampling_sphere(5)[0], dtype=np.float32)).to(device)
     errors = [float(torch.linalg.vector_norm(apply_flow_to_sphere(unit, flows[r], device=device)
                                              - apply_flow_to_sphere(unit, plain_flows[r], device=device),
                                              dim=1).max()) for r in range(regs)]
@@ -662,8 +665,9 @@ def run_native(args):
             write_gifti_mesh(work / "source_surface.gii", GiftiMesh(meshes["surface"], meshes["faces"]))
             write_gifti_mesh(work / "target_surface.gii", GiftiMesh(meshes["target_surface"], meshes["target_faces"]))
             write_gifti_mesh(work / "target_sphere.gii", GiftiMesh(meshes["target_sphere"], meshes["target_faces"]))
-            hemisphere_e2e(meshes, device, torch.float64, work)  # first call warms the host paths
-            runs = [hemisphere_e2e(meshes, device, torch.float64, work) for _ in range(2)]
+            for _ in range(2):  # warm-up: the host paths and the first page-locked allocations
+                hemisphere_e2e(meshes, device, torch.float64, work)
+            runs = [hemisphere_e2e(meshes, device, torch.float64, work) for _ in range(3)]
         e2e_total = torch.tensor([sum(r[0] for r in runs)], dtype=torch.float64, device=device)
         if world > 1:
             dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
@@ -680,6 +684,7 @@ def run_native(args):
         kernel_s = statistics.mean(kernel_ms) / 1e3
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
         hbm = float(peaks.get("hbm_gbs", 6650.0))
+        peak_source = "measured" if "hbm_gbs" in peaks else "fallback"
         achieved = areal_bytes_per_sweep(n, f) * SWEEPS / kernel_s / 1e9
         epochs, start = [], 1
         while start <= SWEEPS:
@@ -712,9 +717,12 @@ def run_native(args):
             "stages_s": stages,
             "roofline": {
                 "kernel": "areal_sweeps (persistent wavefront)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                "note": "algorithmic bytes = 4,999 x (24 N + 24 F + 4 (N+1)); the sweep chain is barrier-latency "
-                        "bound (working set L2-resident); peak = measured HBM copy bandwidth",
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": SWEEP_DRAM_BYTES, "peak_source": peak_source,
+                "note": "algorithmic bytes = 4,999 x (24 N + 24 F + 4 (N+1)); the sweep chain is bound by the "
+                        "latency of its dependency chain (working set L2-resident); peak = "
+                        f"{peak_source} HBM copy bandwidth; traffic = DRAM bytes of one ncu capture of a 200-sweep "
+                        "launch on the same mesh: the working set is read once per launch, so a 4,999-sweep "
+                        "launch moves the same bytes",
                 "kernel_ms": kernel_s * 1e3, "us_per_wavefront_step": kernel_s / wavefront_steps * 1e6,
             },
             "cpu_baseline": cpu_baseline,

@@ -22,7 +22,11 @@
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "../../include/catsurf_b200.h"
@@ -221,8 +225,30 @@ struct Prepared {
     std::vector<V3> pts;
     double radius = 0.0;
     std::vector<V3> unit;
-    std::vector<V3> sheet;
+    std::shared_ptr<const std::vector<V3>> sheet;  // shared by every build of one sheet size
 };
+
+// Unit directions of the nx x ny sheet cell centres (latitude v, longitude u).
+// They depend on the sheet size alone, so one table per size is kept for the
+// life of the process; builds running in parallel threads share it.
+std::shared_ptr<const std::vector<V3>> sheet_directions(int nx, int ny) {
+    static std::mutex lock;
+    static std::map<std::pair<int, int>, std::shared_ptr<const std::vector<V3>>> tables;
+    std::lock_guard<std::mutex> guard(lock);
+    auto& slot = tables[{nx, ny}];
+    if (!slot) {
+        const double pi = 3.141592653589793;
+        auto table = std::make_shared<std::vector<V3>>(static_cast<size_t>(nx) * ny);
+        for (int cellid = 0; cellid < nx * ny; ++cellid) {
+            const int x = cellid % nx, y = cellid / nx;
+            const double u = (x + 0.5) / nx, v = (y + 0.5) / ny;
+            (*table)[cellid] = {std::sin(v * pi) * std::cos(2.0 * pi * u), std::sin(v * pi) * std::sin(2.0 * pi * u),
+                                std::cos(v * pi)};
+        }
+        slot = std::move(table);
+    }
+    return slot;
+}
 
 int prepare(const float* sphere, int n_sphere, const int32_t* sphere_faces, int n_sphere_faces,
             const double* resampling_points, int n_points, const int32_t* resampling_faces, int n_faces, int nx, int ny,
@@ -259,14 +285,7 @@ int prepare(const float* sphere, int n_sphere, const int32_t* sphere_faces, int 
         V3 p{resampling_points[3 * i], resampling_points[3 * i + 1], resampling_points[3 * i + 2]};
         out.unit[i] = (1.0 / std::sqrt(dot(p, p))) * p;
     }
-    const double pi = 3.141592653589793;
-    out.sheet.assign(static_cast<size_t>(nx) * ny, V3{0, 0, 0});
-    for (int cellid = 0; cellid < nx * ny; ++cellid) {
-        const int x = cellid % nx, y = cellid / nx;
-        const double u = (x + 0.5) / nx, v = (y + 0.5) / ny;
-        out.sheet[cellid] = {std::sin(v * pi) * std::cos(2.0 * pi * u), std::sin(v * pi) * std::sin(2.0 * pi * u),
-                             std::cos(v * pi)};
-    }
+    out.sheet = sheet_directions(nx, ny);
     return CSG_OK;
 }
 
@@ -660,7 +679,7 @@ extern "C" int csg_stencil_build(const float* sphere, int n_sphere, const int32_
     gus.build(us, grid_resolution(n_faces));
     parallel_for(nx * ny, threads, [&](int cellid) {
         double w[3];
-        const int f = gus.closest(prep.sheet[cellid], w);
+        const int f = gus.closest((*prep.sheet)[cellid], w);
         if (f < 0) {
             failed = 1;
             return;
@@ -704,7 +723,7 @@ extern "C" int csg_stencil_build_device(const float* sphere, int n_sphere, const
     CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.in_faces, sphere_faces, 12ULL * n_sphere_faces, cudaMemcpyHostToDevice, s));
     CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.unit, prep.unit.data(), 24ULL * n_points, cudaMemcpyHostToDevice, s));
     CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.r_faces, resampling_faces, 12ULL * n_faces, cudaMemcpyHostToDevice, s));
-    CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.sheet, prep.sheet.data(), 24ULL * cells, cudaMemcpyHostToDevice, s));
+    CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.sheet, prep.sheet->data(), 24ULL * cells, cudaMemcpyHostToDevice, s));
     CSG_CUDA_CHECK(cudaMemsetAsync(base + L.flag, 0, sizeof(int), s));
     const int res_a = grid_resolution(n_sphere_faces), res_b = grid_resolution(n_faces);
     const double* in_pts = reinterpret_cast<const double*>(base + L.in_pts);

@@ -17,13 +17,29 @@ from . import _native
 from .surface_stencil import SurfaceStencil, SurfaceStencilDevice
 
 _TOPOLOGY_CACHE: dict[tuple, tuple[torch.Tensor, ...]] = {}
+_TOPOLOGY_BY_ID: dict[tuple, tuple] = {}
+_FACES_BY_ID: dict[tuple, tuple] = {}
+
+
+def _shared_faces(faces) -> bool:
+    """A read-only int32 face array (the shared resampling sphere): caches may key on its identity."""
+
+    return isinstance(faces, np.ndarray) and not faces.flags.writeable and faces.dtype == np.int32 \
+        and faces.flags.c_contiguous
 
 
 def _topology(faces: np.ndarray, n_points: int, device: torch.device):
+    ident = (id(faces), n_points, device.type, device.index) if _shared_faces(faces) else None
+    if ident is not None:
+        hit = _TOPOLOGY_BY_ID.get(ident)
+        if hit is not None and hit[0] is faces:
+            return hit[1]
     f = np.ascontiguousarray(faces, dtype=np.int32)
     key = (device.type, device.index, f.shape, n_points, f.tobytes())
     cached = _TOPOLOGY_CACHE.get(key)
     if cached is not None:
+        if ident is not None:
+            _TOPOLOGY_BY_ID[ident] = (faces, cached)
         return cached
     lib = _native.library()
     off = np.zeros(n_points + 1, dtype=np.int32)
@@ -43,7 +59,23 @@ def _topology(faces: np.ndarray, n_points: int, device: torch.device):
     max_degree = int(np.diff(off).max()) if n_points else 0
     cached = tensors + (max_degree,)
     _TOPOLOGY_CACHE[key] = cached
+    if ident is not None:
+        _TOPOLOGY_BY_ID[ident] = (faces, cached)
     return cached
+
+
+def _device_faces(faces, device: torch.device) -> torch.Tensor:
+    """Faces on the device; one shared read-only copy for the shared resampling faces."""
+
+    if _shared_faces(faces):
+        ident = (id(faces), device.type, device.index)
+        hit = _FACES_BY_ID.get(ident)
+        if hit is not None and hit[0] is faces:
+            return hit[1]
+        tensor = torch.from_numpy(faces.copy()).to(device)
+        _FACES_BY_ID[ident] = (faces, tensor)
+        return tensor
+    return torch.as_tensor(np.ascontiguousarray(faces, dtype=np.int32), device=device).contiguous()
 
 
 def upload_stencil(stencil: SurfaceStencil, device: torch.device, geometry_dtype: torch.dtype,
@@ -51,19 +83,35 @@ def upload_stencil(stencil: SurfaceStencil, device: torch.device, geometry_dtype
     if weight_dtype != torch.float64:
         raise ValueError("stencil weights are float64")
     off, nbr, inc_off, inc, max_degree = _topology(stencil.faces, stencil.sphere_points.shape[0], device)
+
+    pinned = getattr(stencil, "pinned", None)
+
+    def up(array, dtype):
+        # copy as stored and convert on the device (the same IEEE rounding as on the host)
+        array = np.asarray(array)
+        if pinned is not None and array.flags.c_contiguous:
+            offset = array.ctypes.data - pinned.data_ptr()
+            if 0 <= offset and offset + array.nbytes <= pinned.numel():
+                # a view of the page-locked block: an asynchronous copy that torch's pinned-memory
+                # cache tracks (the block is not reused before the copy has run)
+                source = pinned[offset: offset + array.nbytes].view(torch.from_numpy(array[:0]).dtype)
+                return source.reshape(array.shape).to(device, non_blocking=True).to(dtype).contiguous()
+        host = torch.from_numpy(np.ascontiguousarray(array, dtype=array.dtype.newbyteorder("=")))
+        return host.to(device).to(dtype).contiguous()
+
     st = SurfaceStencilDevice(
-        sphere_points=torch.as_tensor(stencil.sphere_points, dtype=geometry_dtype, device=device).contiguous(),
-        faces=torch.as_tensor(np.ascontiguousarray(stencil.faces, dtype=np.int32), device=device).contiguous(),
-        surface_indices=torch.as_tensor(np.ascontiguousarray(stencil.surface_indices, dtype=np.int32), device=device),
-        surface_weights=torch.as_tensor(stencil.surface_weights, dtype=torch.float64, device=device).contiguous(),
-        sheet_indices=torch.as_tensor(np.ascontiguousarray(stencil.sheet_indices, dtype=np.int32), device=device),
-        sheet_weights=torch.as_tensor(stencil.sheet_weights, dtype=torch.float64, device=device).contiguous(),
+        sphere_points=up(stencil.sphere_points, geometry_dtype),
+        faces=_device_faces(stencil.faces, device),
+        surface_indices=up(stencil.surface_indices, torch.int32),
+        surface_weights=up(stencil.surface_weights, torch.float64),
+        sheet_indices=up(stencil.sheet_indices, torch.int32),
+        sheet_weights=up(stencil.sheet_weights, torch.float64),
         nx=int(stencil.nx),
         ny=int(stencil.ny),
         source_points=int(stencil.source_points),
         unit_sphere_points=None
         if stencil.unit_sphere_points is None
-        else torch.as_tensor(stencil.unit_sphere_points, dtype=torch.float32, device=device).contiguous(),
+        else up(stencil.unit_sphere_points, torch.float32),
         neighbour_offsets=off,
         neighbour_indices=nbr,
         max_degree=max_degree,
@@ -114,8 +162,8 @@ def map_values_to_sheet(st: SurfaceStencilDevice, values) -> torch.Tensor:
     return out
 
 
-def heat_parameters(st: SurfaceStencilDevice, vertices: torch.Tensor, fwhm: float) -> tuple[int, float]:
-    """Iteration count and sigma of the iterative heat kernel (reference 359-369)."""
+def _edge_mean(st: SurfaceStencilDevice, vertices: torch.Tensor) -> float:
+    """Mean edge length of the stencil's faces on these vertices (reference 347-356); synchronises."""
 
     v = vertices.contiguous()
     dtype = _native.CSG_DTYPE_F32 if v.dtype == torch.float32 else _native.CSG_DTYPE_F64
@@ -124,11 +172,20 @@ def heat_parameters(st: SurfaceStencilDevice, vertices: torch.Tensor, fwhm: floa
     _native.check(_native.library().csg_feature_edge_sum(dtype, int(st.faces.shape[0]), st.faces.data_ptr(), v.data_ptr(),
                                                          total.data_ptr(), scratch.data_ptr(), scratch.numel(),
                                                          _stream()), "csg_feature_edge_sum")
-    edge_mean = float(total.item()) / (3.0 * int(st.faces.shape[0]))
+    return float(total.item()) / (3.0 * int(st.faces.shape[0]))
+
+
+def _heat_from_edge_mean(edge_mean: float, fwhm: float) -> tuple[int, float]:
     raw = float(fwhm) * float(fwhm) * 0.541011 / (edge_mean * edge_mean)
     iterations = max(1, int(math.ceil(raw)))
     sigma = float(fwhm) * 0.7355345 / float(iterations ** 0.5)
     return iterations, sigma
+
+
+def heat_parameters(st: SurfaceStencilDevice, vertices: torch.Tensor, fwhm: float) -> tuple[int, float]:
+    """Iteration count and sigma of the iterative heat kernel (reference 359-369)."""
+
+    return _heat_from_edge_mean(_edge_mean(st, vertices), fwhm)
 
 
 def smooth_geometry(st: SurfaceStencilDevice, vertices, fwhm: float) -> torch.Tensor:
@@ -152,7 +209,8 @@ def _smooth_series(st, values, geometry, fwhms, via_norm: bool) -> torch.Tensor:
         raise ValueError("vertices must have shape [sphere_points, 3]")
     if geom.dtype not in (torch.float32, torch.float64):
         geom = geom.to(torch.float64)
-    params = [heat_parameters(st, geom, f) for f in fwhms]
+    edge_mean = _edge_mean(st, geom)  # one reduction and one synchronisation for every FWHM of the series
+    params = [_heat_from_edge_mean(edge_mean, f) for f in fwhms]
     counts = ctypes_int_array([p[0] for p in params])
     sigmas = _native.doubles([p[1] for p in params])
     out = torch.empty((len(fwhms), n), dtype=torch.float64, device=base.device)

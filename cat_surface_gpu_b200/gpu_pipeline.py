@@ -103,22 +103,24 @@ def rotation_matrix_from_angles(angles) -> torch.Tensor:
     value = torch.as_tensor(np.asarray(angles, dtype=np.float64)).reshape(-1)
     if value.numel() != 3:
         raise ValueError("Rotation must contain exactly three angles")
-    ca = [torch.cos(angle) for angle in value.unbind()]
-    sa = [torch.sin(angle) for angle in value.unbind()]
-    one, zero = torch.ones((), dtype=torch.float64), torch.zeros((), dtype=torch.float64)
+    # torch's float64 sin/cos of each angle (as the reference takes them); the products are
+    # plain float64 multiplies and adds, one rounding each, so Python floats give the same bits
+    ca = [float(torch.cos(angle)) for angle in value.unbind()]
+    sa = [float(torch.sin(angle)) for angle in value.unbind()]
+    one, zero = 1.0, 0.0
     rx = (one, zero, zero, zero, ca[0], sa[0], zero, -sa[0], ca[0])
     ry = (ca[1], zero, sa[1], zero, one, zero, -sa[1], zero, ca[1])
     rz = (ca[2], sa[2], zero, -sa[2], ca[2], zero, zero, zero, one)
 
     def product(left, right):
-        out = [None] * 9
+        out = [0.0] * 9
         for r in range(3):
             for c in range(3):
                 out[r + 3 * c] = ((zero + left[r] * right[3 * c]) + left[r + 3] * right[1 + 3 * c]) \
                     + left[r + 6] * right[2 + 3 * c]
         return out
 
-    return torch.stack(product(rz, product(ry, rx))).reshape(3, 3)
+    return torch.tensor(product(rz, product(ry, rx)), dtype=torch.float64).reshape(3, 3)
 
 
 def rotate_vertices(vertices: np.ndarray, angles) -> np.ndarray:

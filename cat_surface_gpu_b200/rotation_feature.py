@@ -87,7 +87,7 @@ class DepthTopology:
         plan = SweepPlan.build(relabel[tri], n)
         order = perm[plan.order]
         topo = cls(
-            n=n, nf=int(tri.shape[0]), faces=torch.from_numpy(tri).to(device), inc_off=inc_off, inc=inc,
+            n=n, nf=int(tri.shape[0]), faces=torch.from_numpy(np.array(tri)).to(device), inc_off=inc_off, inc=inc,
             max_incidences=int(np.bincount(tri.reshape(-1), minlength=n).max()), groups=groups,
             order=torch.from_numpy(np.ascontiguousarray(order)).to(device),
             level_begin=torch.from_numpy(plan.level_begin).to(device),
@@ -151,11 +151,22 @@ def depth_potential(geometries: torch.Tensor, topology: DepthTopology, *, solver
     return values, its, res
 
 
+_TOPOLOGY_BY_FACES: dict[tuple, tuple] = {}
+
+
 def _stencil_topology(stencil) -> DepthTopology:
     cached = stencil._cache.get("depth_topology")
     if cached is None:
-        faces = stencil.faces.detach().cpu().numpy()
-        cached = DepthTopology.build(faces, int(stencil.sphere_points.shape[0]), stencil.faces.device)
+        # stencils of one resampling sphere share one device face tensor: look it up by identity
+        # before copying the faces back to hash them
+        ident = (id(stencil.faces), int(stencil.sphere_points.shape[0]))
+        hit = _TOPOLOGY_BY_FACES.get(ident)
+        if hit is not None and hit[0] is stencil.faces:
+            cached = hit[1]
+        else:
+            faces = stencil.faces.detach().cpu().numpy()
+            cached = DepthTopology.build(faces, int(stencil.sphere_points.shape[0]), stencil.faces.device)
+            _TOPOLOGY_BY_FACES[ident] = (stencil.faces, cached)
         stencil._cache["depth_topology"] = cached
     return cached
 

@@ -125,8 +125,8 @@ class RotationGridIndex:
             raise ValueError("RotationGridIndex is missing candidate index")
         triangles = self.points[self.faces.astype(np.int64)].astype(np.float32)
         return RotationGridIndexDevice(
-            target_points=torch.as_tensor(self.points, dtype=torch.float32, device=target).contiguous(),
-            target_faces=torch.as_tensor(self.faces, dtype=torch.int32, device=target).contiguous(),
+            target_points=torch.from_numpy(np.array(self.points, dtype=np.float32)).to(target),
+            target_faces=torch.from_numpy(np.array(self.faces, dtype=np.int32)).to(target),
             target_triangles=torch.as_tensor(triangles, device=target).contiguous(),
             candidate_table=torch.empty(0, dtype=candidate_table_dtype, device=target),
             grid_size=self.grid_size,
@@ -234,9 +234,11 @@ class RotationGridIndexDevice:
             raise ValueError("grid_size must be at least 4 and margin must be non-negative")
         if tri.min(initial=0) < 0 or tri.max(initial=0) >= pts.shape[0]:
             raise ValueError("faces reference a missing point")
+        from .features import _device_faces
+
         lib = _native.library()
-        d_pts = torch.as_tensor(pts, device=target)
-        d_faces = torch.as_tensor(tri, device=target)
+        d_pts = torch.from_numpy(pts).to(target)
+        d_faces = _device_faces(tri, target)
         offsets = torch.empty(grid_size ** 3 + 1, dtype=torch.int32, device=target)
         scratch = torch.empty(int(lib.csg_rotation_grid_scratch_bytes(grid_size)), dtype=torch.uint8, device=target)
         count = ctypes.c_longlong(0)
@@ -251,9 +253,10 @@ class RotationGridIndexDevice:
         _native.check(lib.csg_rotation_grid_build_device(*args, flat.data_ptr(), count.value, ctypes.addressof(count),
                                                          scratch.data_ptr(), scratch.numel(), stream),
                       "csg_rotation_grid_build_device")
-        triangles = pts[tri.astype(np.int64)].astype(np.float32)
+        # corner gather and float64 -> float32 rounding on the device (the same values as on the host)
+        triangles = d_pts[d_faces.long()].to(torch.float32).contiguous()
         return cls(target_points=d_pts.to(torch.float32).contiguous(), target_faces=d_faces,
-                   target_triangles=torch.as_tensor(triangles, device=target).contiguous(),
+                   target_triangles=triangles,
                    candidate_table=torch.empty(0, dtype=torch.int32, device=target), grid_size=int(grid_size),
                    candidate_offsets=offsets, candidate_faces=flat)
 

@@ -39,6 +39,9 @@ class SurfaceStencil:
     ny: int
     source_points: int
     unit_sphere_points: np.ndarray | None = None
+    # page-locked block holding the arrays above (a GPU-built stencil): uploads copy from views of
+    # it, so torch's pinned-memory cache keeps the block until those copies have run
+    pinned: torch.Tensor | None = field(default=None, repr=False, compare=False)
 
     @classmethod
     def from_file(cls, path) -> "SurfaceStencil":
@@ -189,8 +192,12 @@ def resampling_sphere(subdivisions: int = 6) -> tuple[np.ndarray, np.ndarray]:
         from .synthetic import unit_icosphere
 
         points, faces = unit_icosphere(subdivisions)
-        _RESAMPLING_SPHERES[subdivisions] = (np.ascontiguousarray(points, dtype=np.float64),
-                                             np.ascontiguousarray(faces, dtype=np.int32))
+        points = np.array(points, dtype=np.float64, order="C")
+        faces = np.array(faces, dtype=np.int32, order="C")
+        # shared by every stencil of this resolution (lookups key on the array itself): read-only
+        points.flags.writeable = False
+        faces.flags.writeable = False
+        _RESAMPLING_SPHERES[subdivisions] = (points, faces)
     return _RESAMPLING_SPHERES[subdivisions]
 
 
@@ -215,19 +222,31 @@ def build_surface_stencil(sphere_vertices, sphere_faces, *, nx: int = 512, ny: i
         raise ValueError("sphere_vertices and sphere_faces must have shape [n, 3] and [m, 3]")
     rpts, rfaces = resampling_sphere(subdivisions)
     n = rpts.shape[0]
-    sphere_points = np.zeros((n, 3), dtype=np.float64)
-    surface_indices = np.zeros((n, 3), dtype=np.int32)
-    surface_weights = np.zeros((n, 3), dtype=np.float64)
-    sheet_indices = np.zeros((ny, nx, 3), dtype=np.int32)
-    sheet_weights = np.zeros((ny, nx, 3), dtype=np.float64)
-    unit = np.zeros(sphere.shape, dtype=np.float32)
+    target = None if device is None else torch.device(device)
+    on_gpu = target is not None and target.type == "cuda"
+
+    shapes = (((n, 3), np.float64), ((n, 3), np.int32), ((n, 3), np.float64), ((ny, nx, 3), np.int32),
+              ((ny, nx, 3), np.float64), (tuple(sphere.shape), np.float32))
+    if on_gpu:
+        # a GPU build reads its results back into one page-locked block (the build writes every
+        # element), which the upload to the device (SurfaceStencil.to) then copies asynchronously
+        sizes = [(int(np.prod(shape)) * np.dtype(dt).itemsize + 7) // 8 * 8 for shape, dt in shapes]
+        pinned = torch.empty(sum(sizes), dtype=torch.uint8, pin_memory=True)
+        block = pinned.numpy()
+        arrays, offset = [], 0
+        for (shape, dt), size in zip(shapes, sizes):
+            arrays.append(block[offset: offset + int(np.prod(shape)) * np.dtype(dt).itemsize].view(dt).reshape(shape))
+            offset += size
+    else:
+        pinned = None
+        arrays = [np.zeros(shape, dtype=dt) for shape, dt in shapes]
+    sphere_points, surface_indices, surface_weights, sheet_indices, sheet_weights, unit = arrays
     lib = _native.library()
     outputs = (sphere_points.ctypes.data, surface_indices.ctypes.data, surface_weights.ctypes.data,
                sheet_indices.ctypes.data, sheet_weights.ctypes.data, unit.ctypes.data)
     inputs = (sphere.ctypes.data, sphere.shape[0], faces.ctypes.data, faces.shape[0], rpts.ctypes.data, n,
               rfaces.ctypes.data, rfaces.shape[0], int(nx), int(ny), int(bool(normalize)))
-    target = None if device is None else torch.device(device)
-    if target is not None and target.type == "cuda":
+    if on_gpu:
         need = int(lib.csg_stencil_scratch_bytes(sphere.shape[0], faces.shape[0], n, rfaces.shape[0], int(nx),
                                                  int(ny)))
         if need == 0:
@@ -238,6 +257,7 @@ def build_surface_stencil(sphere_vertices, sphere_faces, *, nx: int = 512, ny: i
                                                        _native.stream_handle()), "csg_stencil_build_device")
     else:
         _native.check(lib.csg_stencil_build(*inputs, int(threads), *outputs), "csg_stencil_build")
-    return SurfaceStencil(sphere_points=sphere_points, faces=rfaces.copy(), surface_indices=surface_indices,
+    return SurfaceStencil(sphere_points=sphere_points, faces=rfaces, surface_indices=surface_indices,
                           surface_weights=surface_weights, sheet_indices=sheet_indices, sheet_weights=sheet_weights,
-                          nx=int(nx), ny=int(ny), source_points=int(sphere.shape[0]), unit_sphere_points=unit)
+                          nx=int(nx), ny=int(ny), source_points=int(sphere.shape[0]), unit_sphere_points=unit,
+                          pinned=pinned)
