@@ -26,6 +26,7 @@
 
 #include "../../include/catsurf_b200.h"
 #include "errors.h"
+#include "pdl.cuh"
 
 namespace {
 
@@ -99,6 +100,7 @@ __device__ __forceinline__ int nb(int x, int y, int dx, int dy, int nx, int ny) 
 template <typename T>
 __global__ void k_smalldef(const T* __restrict__ v, T* __restrict__ map, T* __restrict__ jac, int nx, int ny, T s,
                            T hs) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     const int P = nx * ny;
@@ -124,6 +126,7 @@ __global__ void k_smalldef(const T* __restrict__ v, T* __restrict__ map, T* __re
 template <typename T>
 __global__ void k_compose(const T* __restrict__ a, const T* __restrict__ ja, const T* __restrict__ b,
                           const T* __restrict__ jb, T* __restrict__ c, T* __restrict__ jc, int nx, int ny) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     const int P = nx * ny;
@@ -179,6 +182,7 @@ __device__ __forceinline__ void jacdiv_at(const T* J, const T* vx, const T* vy, 
 template <typename T>
 __global__ void k_jacdiv(const T* __restrict__ jac, const T* __restrict__ v, T* __restrict__ out, int nx, int ny,
                          T hs) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     const int P = nx * ny;
@@ -209,6 +213,7 @@ template <typename T, bool JACDIV>
 __global__ void k_objfun(const T* __restrict__ source, const T* __restrict__ target, const T* __restrict__ map,
                          const T* __restrict__ jac, const T* __restrict__ v, const T* __restrict__ weights,
                          T* __restrict__ rhs, T* __restrict__ hess, T* __restrict__ partial, int nx, int ny, T hs) {
+    csg::pdl_begin();
     Pt p;
     const bool ok = point(nx, ny, p);
     T contrib = T(0);
@@ -253,6 +258,7 @@ template <typename T>
 __global__ void k_squaring(const T* __restrict__ b, const T* __restrict__ a, const T* __restrict__ map,
                            const T* __restrict__ jac, T* __restrict__ b_out, T* __restrict__ a_out,
                            T* __restrict__ inc, int nx, int ny) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     const int P = nx * ny;
@@ -368,6 +374,7 @@ __device__ __forceinline__ void regularise_at(const T* vx, const T* vy, const Pt
 
 template <typename T>
 __global__ void k_regularise(const T* __restrict__ v, T* __restrict__ out, int nx, int ny, int rtype, RegWeights rw) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     const int P = nx * ny;
@@ -387,6 +394,7 @@ template <typename T>
 __global__ void k_combine(const T* __restrict__ rf, const T* __restrict__ rr, const T* __restrict__ hf,
                           const T* __restrict__ hr, const T* __restrict__ v, T* __restrict__ rhs, T* __restrict__ hess,
                           T* __restrict__ partial_reg, T* __restrict__ partial_norm, int nx, int ny, T s, RegWeights rw) {
+    csg::pdl_begin();
     Pt p;
     const bool ok = point(nx, ny, p);
     T reg_dot = T(0), norm = T(0);
@@ -439,6 +447,7 @@ __device__ __forceinline__ void membrane_apply_at(const T* __restrict__ hess, co
 template <typename T>
 __global__ void k_membrane_apply(const T* __restrict__ hess, const T* __restrict__ u, const T* __restrict__ b,
                                  T* __restrict__ out, int nx, int ny, RegWeights rw) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     membrane_apply_at(hess, u, b, out, nx, ny, rw, p);
@@ -473,6 +482,7 @@ __device__ __forceinline__ void relax_at(const T* __restrict__ hess, const T* __
 template <typename T>
 __global__ void k_relax(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u, int nx, int ny,
                         int colour, T w00, T w01, T w10) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     if (((p.x + p.y) & 1) != colour) return;
@@ -482,6 +492,7 @@ __global__ void k_relax(const T* __restrict__ hess, const T* __restrict__ b, T* 
 // Direct 2x2 point solve of the coarsest level (dartel_grid.py:1318-1334).
 template <typename T>
 __global__ void k_point_solve(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u, int P, T id) {
+    csg::pdl_begin();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     const size_t o1 = static_cast<size_t>(blockIdx.y) * P;
@@ -531,6 +542,7 @@ __device__ __forceinline__ void resize_at(const T* __restrict__ src, T* __restri
 template <typename T>
 __global__ void k_resize(const T* __restrict__ src, T* __restrict__ dst, int snx, int sny, int tnx, int tny,
                          int accumulate) {
+    csg::pdl_begin();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= tnx * tny) return;
     resize_at(src, dst, snx, sny, tnx, tny, accumulate, static_cast<int>(blockIdx.y), i);
@@ -591,6 +603,7 @@ __device__ __forceinline__ void block_resize(const T* src, int snx, int sny, T* 
 // cycle(first) of Fmg (host side) restricted to levels first..last, for batch element blockIdx.x.
 template <typename T>
 __global__ void __launch_bounds__(kCoarseThreads) k_fmg_coarse_cycle(CoarseCycle<T> c) {
+    csg::pdl_begin();
     const int bi = blockIdx.x;
     for (int l = c.first; l < c.last; ++l) {
         const CoarseLevel<T>& L = c.lv[l];
@@ -616,12 +629,14 @@ __global__ void __launch_bounds__(kCoarseThreads) k_fmg_coarse_cycle(CoarseCycle
 
 template <typename T>
 __global__ void k_sub(T* __restrict__ v, const T* __restrict__ u, size_t n) {
+    csg::pdl_begin();
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n) v[i] = v[i] - u[i];
 }
 
 template <typename T>
 __global__ void k_any_nonzero(const T* __restrict__ u, size_t n, int* flag) {
+    csg::pdl_begin();
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n && u[i] != T(0)) atomicOr(flag, 1);
 }
@@ -631,6 +646,7 @@ __global__ void k_any_nonzero(const T* __restrict__ u, size_t n, int* flag) {
 template <typename T>
 __global__ void k_metrics(const T* __restrict__ obj_f, const T* __restrict__ obj_r, const T* __restrict__ reg,
                           const T* __restrict__ norm, int nblocks, T* __restrict__ metrics, int metric_stride) {
+    csg::pdl_begin();
     const int b = blockIdx.x;
     if (threadIdx.x != 0) return;
     T of = T(0), orv = T(0), rg = T(0), nm = T(0);
@@ -648,6 +664,7 @@ __global__ void k_metrics(const T* __restrict__ obj_f, const T* __restrict__ obj
 
 template <typename T>
 __global__ void k_objective_out(const T* __restrict__ partial, int nblocks, T* __restrict__ out) {
+    csg::pdl_begin();
     if (threadIdx.x != 0) return;
     T s = T(0);
     for (int k = 0; k < nblocks; ++k) s = s + partial[static_cast<size_t>(blockIdx.x) * nblocks + k];
@@ -740,12 +757,12 @@ struct Fmg {
         params_at(l, pr);
         const MemWeights w = mem_weights(pr);
         for (int it = 0; it < 2 * nit; ++it)
-            (csg::note_launch(), k_relax<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(buf.A[l], buf.B[l], buf.U[l], nx, ny,
+            (csg::note_launch(), csg::launch_pdl(k_relax<T>, grid_for(nx * ny, batch), kThreads, 0, s, buf.A[l], buf.B[l], buf.U[l], nx, ny,
                                                                       it % 2 == 0 ? 1 : 0, T(w.w00), T(w.w01), T(w.w10)));
     }
     void resize(const T* src, size_t from, T* dst, size_t to, int channels, bool accumulate) {
         const auto f = buf.specs[from], t = buf.specs[to];
-        (csg::note_launch(), k_resize<T><<<grid_for(t.first * t.second, batch * channels), kThreads, 0, s>>>(src, dst, f.first, f.second,
+        (csg::note_launch(), csg::launch_pdl(k_resize<T>, grid_for(t.first * t.second, batch * channels), kThreads, 0, s, src, dst, f.first, f.second,
                                                                                      t.first, t.second, accumulate));
     }
     // First level of the fused coarse part: the finest level of at most
@@ -770,7 +787,7 @@ struct Fmg {
             c.lv[l] = CoarseLevel<T>{buf.A[l], buf.B[l], buf.U[l], buf.R[l], buf.specs[l].first, buf.specs[l].second,
                                      T(w.w00), T(w.w01), T(w.w10), reg_weights(pr, 1)};
         }
-        (csg::note_launch(), k_fmg_coarse_cycle<T><<<batch, kCoarseThreads, 0, s>>>(c));
+        (csg::note_launch(), csg::launch_pdl(k_fmg_coarse_cycle<T>, batch, kCoarseThreads, 0, s, c));
     }
     void cycle(size_t start) {
         const size_t last = buf.specs.size() - 1;
@@ -781,7 +798,7 @@ struct Fmg {
                 const int nx = buf.specs[l].first, ny = buf.specs[l].second;
                 double pr[5];
                 params_at(l, pr);
-                (csg::note_launch(), k_membrane_apply<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(
+                (csg::note_launch(), csg::launch_pdl(k_membrane_apply<T>, grid_for(nx * ny, batch), kThreads, 0, s, 
                     buf.A[l], buf.U[l], buf.B[l], buf.R[l], nx, ny, reg_weights(pr, 1)));
                 resize(buf.R[l], l, buf.B[l + 1], l + 1, 2, false);
                 const size_t P1 = static_cast<size_t>(buf.specs[l + 1].first) * buf.specs[l + 1].second;
@@ -799,7 +816,7 @@ struct Fmg {
             const int nx = buf.specs[l].first, ny = buf.specs[l].second;
             double pr[5];
             params_at(l, pr);
-            (csg::note_launch(), k_membrane_apply<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(buf.A[l], buf.U[l], buf.B[l], buf.R[l], nx,
+            (csg::note_launch(), csg::launch_pdl(k_membrane_apply<T>, grid_for(nx * ny, batch), kThreads, 0, s, buf.A[l], buf.U[l], buf.B[l], buf.R[l], nx,
                                                                                ny, reg_weights(pr, 1)));
             resize(buf.R[l], l, buf.B[l + 1], l + 1, 2, false);
             const size_t P1 = static_cast<size_t>(buf.specs[l + 1].first) * buf.specs[l + 1].second;
@@ -829,7 +846,7 @@ struct Fmg {
         }
         const size_t last = L - 1;
         const size_t Pl = static_cast<size_t>(buf.specs[last].first) * buf.specs[last].second;
-        (csg::note_launch(), k_point_solve<T><<<grid_for(static_cast<int>(Pl), batch), kThreads, 0, s>>>(
+        (csg::note_launch(), csg::launch_pdl(k_point_solve<T>, grid_for(static_cast<int>(Pl), batch), kThreads, 0, s, 
             buf.A[last], last == 0 ? buf.B[0] : buf.B0[last], buf.U[last], static_cast<int>(Pl), T(base[4])));
         relax(last);
         for (size_t l = last; l-- > 0;) {
@@ -894,11 +911,11 @@ Squaring<T> run_squaring(T* rb[2], T* ha[2], T* maps[2], T* jacs[2], int k, bool
     const dim3 g = grid_for(nx * ny, batch);
     int cur = 0, other = 1, ba = 0;
     for (int step = 0; step < k; ++step) {
-        (csg::note_launch(), k_squaring<T><<<g, kThreads, 0, s>>>(rb[ba], ha[ba], maps[cur], jacs[cur], rb[1 - ba], ha[1 - ba], maps[other],
+        (csg::note_launch(), csg::launch_pdl(k_squaring<T>, g, kThreads, 0, s, rb[ba], ha[ba], maps[cur], jacs[cur], rb[1 - ba], ha[1 - ba], maps[other],
                                              nx, ny));
         ba = 1 - ba;
         if (save || step < k - 1) {
-            (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(maps[cur], jacs[cur], maps[cur], jacs[cur], maps[other], jacs[other],
+            (csg::note_launch(), csg::launch_pdl(k_compose<T>, g, kThreads, 0, s, maps[cur], jacs[cur], maps[cur], jacs[cur], maps[other], jacs[other],
                                                 nx, ny));
             std::swap(cur, other);
         }
@@ -919,26 +936,26 @@ int dartel_step_impl(StepBuffers<T>& W, const T* source, const T* target, T* vel
     const double scale = 1.0 / static_cast<double>(1LL << k);
     const size_t P = static_cast<size_t>(nx) * ny * batch;
     // expdef(v, k) with Jacobian
-    (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.map[0], W.jac[0], nx, ny, T(scale), T(scale * 0.5)));
+    (csg::note_launch(), csg::launch_pdl(k_smalldef<T>, g, kThreads, 0, s, velocity, W.map[0], W.jac[0], nx, ny, T(scale), T(scale * 0.5)));
     int cur = 0;
     for (int i = 0; i < k; ++i) {
-        (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(W.map[cur], W.jac[cur], W.map[cur], W.jac[cur], W.map[1 - cur],
+        (csg::note_launch(), csg::launch_pdl(k_compose<T>, g, kThreads, 0, s, W.map[cur], W.jac[cur], W.map[cur], W.jac[cur], W.map[1 - cur],
                                             W.jac[1 - cur], nx, ny));
         cur = 1 - cur;
     }
     // forward objective with jac_div_smalldef(J, v, s)
-    (csg::note_launch(), k_objfun<T, true><<<g, kThreads, 0, s>>>(source, target, W.map[cur], W.jac[cur], velocity, nullptr, W.rhs_f[0],
+    (csg::note_launch(), csg::launch_pdl(k_objfun<T, true>, g, kThreads, 0, s, source, target, W.map[cur], W.jac[cur], velocity, nullptr, W.rhs_f[0],
                                              W.hess_f[0], W.objf, nx, ny, T(scale * 0.5)));
     // squaring of the forward terms from smalldef_jac(v, -s)
-    (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.smap[0], W.sjac[0], nx, ny, T(-scale), T(-scale * 0.5)));
+    (csg::note_launch(), csg::launch_pdl(k_smalldef<T>, g, kThreads, 0, s, velocity, W.smap[0], W.sjac[0], nx, ny, T(-scale), T(-scale * 0.5)));
     Squaring<T> fw = run_squaring<T>(W.rhs_f, W.hess_f, W.smap, W.sjac, k, code == 1, batch, nx, ny, s);
     T* initial = W.smap[0];
     T* rr = nullptr;
     T* hr = nullptr;
     if (code == 1) {
-        (csg::note_launch(), k_objfun<T, true><<<g, kThreads, 0, s>>>(target, source, W.smap[fw.cur_map], W.sjac[fw.cur_map], velocity,
+        (csg::note_launch(), csg::launch_pdl(k_objfun<T, true>, g, kThreads, 0, s, target, source, W.smap[fw.cur_map], W.sjac[fw.cur_map], velocity,
                                                  nullptr, W.rhs_r[0], W.hess_r[0], W.objr, nx, ny, T(-scale * 0.5)));
-        (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(velocity, W.rmap[0], W.rjac[0], nx, ny, T(scale), T(scale * 0.5)));
+        (csg::note_launch(), csg::launch_pdl(k_smalldef<T>, g, kThreads, 0, s, velocity, W.rmap[0], W.rjac[0], nx, ny, T(scale), T(scale * 0.5)));
         Squaring<T> rv = run_squaring<T>(W.rhs_r, W.hess_r, W.rmap, W.rjac, k, false, batch, nx, ny, s);
         initial = W.rmap[0];
         rr = W.rhs_r[rv.cur_ba];
@@ -946,9 +963,9 @@ int dartel_step_impl(StepBuffers<T>& W, const T* source, const T* target, T* vel
     }
     const RegWeights rw = reg_weights(params, 1);
     T* rhs = W.rhs;
-    (csg::note_launch(), k_combine<T><<<g, kThreads, 0, s>>>(W.rhs_f[fw.cur_ba], rr, W.hess_f[fw.cur_ba], hr, velocity, rhs, W.hess, W.preg,
+    (csg::note_launch(), csg::launch_pdl(k_combine<T>, g, kThreads, 0, s, W.rhs_f[fw.cur_ba], rr, W.hess_f[fw.cur_ba], hr, velocity, rhs, W.hess, W.preg,
                                         W.pnorm, nx, ny, T(scale), rw));
-    (csg::note_launch(), k_metrics<T><<<batch, 32, 0, s>>>(W.objf, code == 1 ? W.objr : nullptr, W.preg, W.pnorm, W.nblocks, metrics,
+    (csg::note_launch(), csg::launch_pdl(k_metrics<T>, batch, 32, 0, s, W.objf, code == 1 ? W.objr : nullptr, W.preg, W.pnorm, W.nblocks, metrics,
                                       metric_stride));
     // multigrid solve of (H + L) u = rhs from the scratch initial guess
     double solver[5] = {params[0], params[1], params[2], params[3], params[4] + lmreg};
@@ -960,7 +977,7 @@ int dartel_step_impl(StepBuffers<T>& W, const T* source, const T* target, T* vel
     if (!assume_initial_nonzero) {
         int flag = 0;
         CSG_CUDA_CHECK(cudaMemsetAsync(W.fmg.flag, 0, sizeof(int), s));
-        (csg::note_launch(), k_any_nonzero<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(initial, 2 * P,
+        (csg::note_launch(), csg::launch_pdl(k_any_nonzero<T>, static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s, initial, 2 * P,
                                                                                                      W.fmg.flag));
         CSG_CUDA_CHECK(cudaMemcpyAsync(&flag, W.fmg.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
         CSG_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -968,7 +985,7 @@ int dartel_step_impl(StepBuffers<T>& W, const T* source, const T* target, T* vel
         if (coarse_init) CSG_CUDA_CHECK(cudaMemsetAsync(initial, 0, 2 * P * sizeof(T), s));
     }
     fmg.run(coarse_init);
-    (csg::note_launch(), k_sub<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(velocity, initial, 2 * P));
+    (csg::note_launch(), csg::launch_pdl(k_sub<T>, static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s, velocity, initial, 2 * P));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -1032,6 +1049,7 @@ int check_grid(int dtype, int batch, int nx, int ny) {
 template <typename T>
 __global__ void k_data_sample(const T* __restrict__ source, const T* __restrict__ target, const T* __restrict__ map,
                               T* __restrict__ abar, T* __restrict__ partial, int nx, int ny) {
+    csg::pdl_begin();
     Pt p;
     const bool ok = point(nx, ny, p);
     T contrib = T(0);
@@ -1058,6 +1076,7 @@ __global__ void k_data_sample(const T* __restrict__ source, const T* __restrict_
 // objective[b] = 1/2 sum of the block partials of batch b, in block order.
 template <typename T>
 __global__ void k_data_objective(const T* __restrict__ partial, int nblocks, int batch, T* __restrict__ objective) {
+    csg::pdl_begin();
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= batch) return;
     T total = T(0);
@@ -1069,6 +1088,7 @@ __global__ void k_data_objective(const T* __restrict__ partial, int nblocks, int
 template <typename T>
 __global__ void k_data_compose_adjoint(const T* __restrict__ f, const T* __restrict__ abar, T* __restrict__ pbar,
                                        int nx, int ny) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     const int P = nx * ny;
@@ -1102,6 +1122,7 @@ __global__ void k_data_compose_adjoint(const T* __restrict__ f, const T* __restr
 template <typename T>
 __global__ void k_data_velocity_grad(const T* __restrict__ abar, const T* __restrict__ grad_scale, T s,
                                      T* __restrict__ grad, int nx, int ny) {
+    csg::pdl_begin();
     Pt p;
     if (!point(nx, ny, p)) return;
     const int P = nx * ny;
@@ -1156,15 +1177,15 @@ int data_forward_typed(int batch, int nx, int ny, const T* v, const T* source, c
     const size_t field = 2ULL * batch * nx * ny;
     const dim3 g = grid_for(nx * ny, batch);
     const T step = static_cast<T>(std::ldexp(1.0, -k));
-    (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(v, checkpoints, nullptr, nx, ny, step, T(0)));
+    (csg::note_launch(), csg::launch_pdl(k_smalldef<T>, g, kThreads, 0, s, v, checkpoints, nullptr, nx, ny, step, T(0)));
     const T* cur = checkpoints;
     for (int i = 1; i <= k; ++i) {
         T* dst = (i % every == 0 && i < k) ? checkpoints + field * (i / every) : d.work[i % 2];
-        (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(cur, nullptr, cur, nullptr, dst, nullptr, nx, ny));
+        (csg::note_launch(), csg::launch_pdl(k_compose<T>, g, kThreads, 0, s, cur, nullptr, cur, nullptr, dst, nullptr, nx, ny));
         cur = dst;
     }
-    (csg::note_launch(), k_data_sample<T><<<g, kThreads, 0, s>>>(source, target, cur, nullptr, d.partial, nx, ny));
-    (csg::note_launch(), k_data_objective<T><<<(batch + 127) / 128, 128, 0, s>>>(d.partial, static_cast<int>(g.x), batch,
+    (csg::note_launch(), csg::launch_pdl(k_data_sample<T>, g, kThreads, 0, s, source, target, cur, nullptr, d.partial, nx, ny));
+    (csg::note_launch(), csg::launch_pdl(k_data_objective<T>, (batch + 127) / 128, 128, 0, s, d.partial, static_cast<int>(g.x), batch,
                                                                                objective));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
@@ -1188,24 +1209,24 @@ int data_backward_typed(int batch, int nx, int ny, const T* source, const T* tar
         maps[0] = checkpoints + field * j;
         for (int i = first + 1; i <= last; ++i) {
             T* dst = d.seg + d.field_elems * static_cast<size_t>(i - first - 1);
-            (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(maps[i - first - 1], nullptr, maps[i - first - 1],
+            (csg::note_launch(), csg::launch_pdl(k_compose<T>, g, kThreads, 0, s, maps[i - first - 1], nullptr, maps[i - first - 1],
                                                                    nullptr, dst, nullptr, nx, ny));
             maps[i - first] = dst;
         }
         if (j == n_ckpt - 1)
-            (csg::note_launch(), k_data_sample<T><<<g, kThreads, 0, s>>>(source, target, maps[k - first], abar,
+            (csg::note_launch(), csg::launch_pdl(k_data_sample<T>, g, kThreads, 0, s, source, target, maps[k - first], abar,
                                                                        d.partial, nx, ny));
         const int top = (j == n_ckpt - 1) ? k - 1 : last;
         for (int i = top; i >= first; --i) {
             CSG_CUDA_CHECK(cudaMemsetAsync(pbar, 0, sizeof(T) * field, s));
-            (csg::note_launch(), k_data_compose_adjoint<T><<<g, kThreads, 0, s>>>(maps[i - first], abar, pbar, nx, ny));
+            (csg::note_launch(), csg::launch_pdl(k_data_compose_adjoint<T>, g, kThreads, 0, s, maps[i - first], abar, pbar, nx, ny));
             T* t = abar;
             abar = pbar;
             pbar = t;
         }
     }
     const T step = static_cast<T>(std::ldexp(1.0, -k));
-    (csg::note_launch(), k_data_velocity_grad<T><<<g, kThreads, 0, s>>>(abar, grad_scale, step, grad, nx, ny));
+    (csg::note_launch(), csg::launch_pdl(k_data_velocity_grad<T>, g, kThreads, 0, s, abar, grad_scale, step, grad, nx, ny));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -1284,7 +1305,7 @@ namespace {
 
 template <typename T>
 int smalldef_typed(int batch, int nx, int ny, const void* v, double scale, void* map, void* jac, cudaStream_t s) {
-    (csg::note_launch(), k_smalldef<T><<<grid_for(nx * ny, batch), kThreads, 0, s>>>(static_cast<const T*>(v), static_cast<T*>(map),
+    (csg::note_launch(), csg::launch_pdl(k_smalldef<T>, grid_for(nx * ny, batch), kThreads, 0, s, static_cast<const T*>(v), static_cast<T*>(map),
                                                                  static_cast<T*>(jac), nx, ny, T(scale), T(scale * 0.5)));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
@@ -1329,11 +1350,11 @@ int expdef_typed(int batch, int nx, int ny, const void* v, int k, void* map_out,
     const double scale = 1.0 / static_cast<double>(1LL << k);
     const dim3 g = grid_for(nx * ny, batch);
     const bool with_jac = jac_out != nullptr;
-    (csg::note_launch(), k_smalldef<T><<<g, kThreads, 0, s>>>(static_cast<const T*>(v), maps[0], with_jac ? jacs[0] : nullptr, nx, ny,
+    (csg::note_launch(), csg::launch_pdl(k_smalldef<T>, g, kThreads, 0, s, static_cast<const T*>(v), maps[0], with_jac ? jacs[0] : nullptr, nx, ny,
                                          T(scale), T(scale * 0.5)));
     int cur = 0;
     for (int i = 0; i < k; ++i) {
-        (csg::note_launch(), k_compose<T><<<g, kThreads, 0, s>>>(maps[cur], with_jac ? jacs[cur] : nullptr, maps[cur],
+        (csg::note_launch(), csg::launch_pdl(k_compose<T>, g, kThreads, 0, s, maps[cur], with_jac ? jacs[cur] : nullptr, maps[cur],
                                             with_jac ? jacs[cur] : nullptr, maps[1 - cur],
                                             with_jac ? jacs[1 - cur] : nullptr, nx, ny));
         cur = 1 - cur;
@@ -1358,7 +1379,7 @@ int fmg_typed(int batch, int nx, int ny, const void* hess, const void* rhs, cons
     if (has_initial && !assume_nonzero) {
         int flag = 0;
         CSG_CUDA_CHECK(cudaMemsetAsync(buf.flag, 0, sizeof(int), s));
-        (csg::note_launch(), k_any_nonzero<T><<<static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s>>>(buf.U[0], 2 * P,
+        (csg::note_launch(), csg::launch_pdl(k_any_nonzero<T>, static_cast<unsigned>((2 * P + kThreads - 1) / kThreads), kThreads, 0, s, buf.U[0], 2 * P,
                                                                                                      buf.flag));
         CSG_CUDA_CHECK(cudaMemcpyAsync(&flag, buf.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
         CSG_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1394,11 +1415,11 @@ int csg_dartel_compose(int dtype, int batch, int nx, int ny, const void* a, cons
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64)
-        (csg::note_launch(), k_compose<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(a), static_cast<const double*>(ja),
+        (csg::note_launch(), csg::launch_pdl(k_compose<double>, g, kThreads, 0, s, static_cast<const double*>(a), static_cast<const double*>(ja),
                                                  static_cast<const double*>(b), static_cast<const double*>(jb),
                                                  static_cast<double*>(c_out), static_cast<double*>(jc_out), nx, ny));
     else
-        (csg::note_launch(), k_compose<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(a), static_cast<const float*>(ja),
+        (csg::note_launch(), csg::launch_pdl(k_compose<float>, g, kThreads, 0, s, static_cast<const float*>(a), static_cast<const float*>(ja),
                                                 static_cast<const float*>(b), static_cast<const float*>(jb),
                                                 static_cast<float*>(c_out), static_cast<float*>(jc_out), nx, ny));
     CSG_CUDA_CHECK(cudaGetLastError());
@@ -1413,10 +1434,10 @@ int csg_dartel_jac_div(int dtype, int batch, int nx, int ny, const void* jac, co
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64)
-        (csg::note_launch(), k_jacdiv<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(jac), static_cast<const double*>(velocity),
+        (csg::note_launch(), csg::launch_pdl(k_jacdiv<double>, g, kThreads, 0, s, static_cast<const double*>(jac), static_cast<const double*>(velocity),
                                                 static_cast<double*>(out), nx, ny, scale * 0.5));
     else
-        (csg::note_launch(), k_jacdiv<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(jac), static_cast<const float*>(velocity),
+        (csg::note_launch(), csg::launch_pdl(k_jacdiv<float>, g, kThreads, 0, s, static_cast<const float*>(jac), static_cast<const float*>(velocity),
                                                static_cast<float*>(out), nx, ny, static_cast<float>(scale * 0.5)));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
@@ -1435,18 +1456,18 @@ int csg_dartel_objfun(int dtype, int batch, int nx, int ny, const void* source, 
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64) {
-        (csg::note_launch(), k_objfun<double, false><<<g, kThreads, 0, s>>>(
+        (csg::note_launch(), csg::launch_pdl(k_objfun<double, false>, g, kThreads, 0, s, 
             static_cast<const double*>(source), static_cast<const double*>(target), static_cast<const double*>(map),
             static_cast<const double*>(jac), nullptr, static_cast<const double*>(weights), static_cast<double*>(rhs_out),
             static_cast<double*>(hess_out), static_cast<double*>(scratch), nx, ny, 0.0));
-        (csg::note_launch(), k_objective_out<double><<<batch, 32, 0, s>>>(static_cast<double*>(scratch), nblocks,
+        (csg::note_launch(), csg::launch_pdl(k_objective_out<double>, batch, 32, 0, s, static_cast<double*>(scratch), nblocks,
                                                      static_cast<double*>(objective_out)));
     } else {
-        (csg::note_launch(), k_objfun<float, false><<<g, kThreads, 0, s>>>(
+        (csg::note_launch(), csg::launch_pdl(k_objfun<float, false>, g, kThreads, 0, s, 
             static_cast<const float*>(source), static_cast<const float*>(target), static_cast<const float*>(map),
             static_cast<const float*>(jac), nullptr, static_cast<const float*>(weights), static_cast<float*>(rhs_out),
             static_cast<float*>(hess_out), static_cast<float*>(scratch), nx, ny, 0.0f));
-        (csg::note_launch(), k_objective_out<float><<<batch, 32, 0, s>>>(static_cast<float*>(scratch), nblocks,
+        (csg::note_launch(), csg::launch_pdl(k_objective_out<float>, batch, 32, 0, s, static_cast<float*>(scratch), nblocks,
                                                     static_cast<float*>(objective_out)));
     }
     CSG_CUDA_CHECK(cudaGetLastError());
@@ -1479,10 +1500,10 @@ int csg_dartel_regularization(int dtype, int batch, int nx, int ny, const void* 
     const RegWeights rw = reg_weights(params, rtype);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64)
-        (csg::note_launch(), k_regularise<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(velocity), static_cast<double*>(out), nx,
+        (csg::note_launch(), csg::launch_pdl(k_regularise<double>, g, kThreads, 0, s, static_cast<const double*>(velocity), static_cast<double*>(out), nx,
                                                     ny, rtype, rw));
     else
-        (csg::note_launch(), k_regularise<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(velocity), static_cast<float*>(out), nx, ny,
+        (csg::note_launch(), csg::launch_pdl(k_regularise<float>, g, kThreads, 0, s, static_cast<const float*>(velocity), static_cast<float*>(out), nx, ny,
                                                    rtype, rw));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
@@ -1497,10 +1518,10 @@ int csg_dartel_membrane_apply(int dtype, int batch, int nx, int ny, const void* 
     const RegWeights rw = reg_weights(params, 1);
     const dim3 g = grid_for(nx * ny, batch);
     if (dtype == CSG_DTYPE_F64)
-        (csg::note_launch(), k_membrane_apply<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(hess), static_cast<const double*>(field),
+        (csg::note_launch(), csg::launch_pdl(k_membrane_apply<double>, g, kThreads, 0, s, static_cast<const double*>(hess), static_cast<const double*>(field),
                                                         nullptr, static_cast<double*>(out), nx, ny, rw));
     else
-        (csg::note_launch(), k_membrane_apply<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(hess), static_cast<const float*>(field),
+        (csg::note_launch(), csg::launch_pdl(k_membrane_apply<float>, g, kThreads, 0, s, static_cast<const float*>(hess), static_cast<const float*>(field),
                                                        nullptr, static_cast<float*>(out), nx, ny, rw));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
@@ -1519,10 +1540,10 @@ int csg_dartel_relax(int dtype, int batch, int nx, int ny, const void* hess, con
     for (int it = 0; it < 2 * nit; ++it) {
         const int colour = it % 2 == 0 ? 1 : 0;
         if (dtype == CSG_DTYPE_F64)
-            (csg::note_launch(), k_relax<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(hess), static_cast<const double*>(rhs),
+            (csg::note_launch(), csg::launch_pdl(k_relax<double>, g, kThreads, 0, s, static_cast<const double*>(hess), static_cast<const double*>(rhs),
                                                    static_cast<double*>(u), nx, ny, colour, w.w00, w.w01, w.w10));
         else
-            (csg::note_launch(), k_relax<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(hess), static_cast<const float*>(rhs),
+            (csg::note_launch(), csg::launch_pdl(k_relax<float>, g, kThreads, 0, s, static_cast<const float*>(hess), static_cast<const float*>(rhs),
                                                   static_cast<float*>(u), nx, ny, colour, static_cast<float>(w.w00),
                                                   static_cast<float>(w.w01), static_cast<float>(w.w10)));
     }
@@ -1537,10 +1558,10 @@ int csg_dartel_resize(int dtype, int fields, int src_nx, int src_ny, const void*
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const dim3 g = grid_for(dst_nx * dst_ny, fields);
     if (dtype == CSG_DTYPE_F64)
-        (csg::note_launch(), k_resize<double><<<g, kThreads, 0, s>>>(static_cast<const double*>(src), static_cast<double*>(dst), src_nx,
+        (csg::note_launch(), csg::launch_pdl(k_resize<double>, g, kThreads, 0, s, static_cast<const double*>(src), static_cast<double*>(dst), src_nx,
                                                 src_ny, dst_nx, dst_ny, accumulate));
     else
-        (csg::note_launch(), k_resize<float><<<g, kThreads, 0, s>>>(static_cast<const float*>(src), static_cast<float*>(dst), src_nx, src_ny,
+        (csg::note_launch(), csg::launch_pdl(k_resize<float>, g, kThreads, 0, s, static_cast<const float*>(src), static_cast<float*>(dst), src_nx, src_ny,
                                                dst_nx, dst_ny, accumulate));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
