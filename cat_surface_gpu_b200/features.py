@@ -175,6 +175,29 @@ def _edge_mean(st: SurfaceStencilDevice, vertices: torch.Tensor) -> float:
     return float(total.item()) / (3.0 * int(st.faces.shape[0]))
 
 
+def edge_means(pairs) -> list[float]:
+    """Mean edge lengths of several (stencil, vertices) pairs with one synchronisation.
+
+    Equal to ``_edge_mean`` of each pair: the edge sums widen every coordinate
+    to float64, so a float32 geometry and its float64 copy give the same value.
+    """
+
+    totals = []
+    for st, vertices in pairs:
+        v = vertices.contiguous()
+        dtype = _native.CSG_DTYPE_F32 if v.dtype == torch.float32 else _native.CSG_DTYPE_F64
+        scratch = _scratch(st)
+        total = torch.empty(1, dtype=torch.float64, device=v.device)
+        _native.check(_native.library().csg_feature_edge_sum(dtype, int(st.faces.shape[0]), st.faces.data_ptr(),
+                                                             v.data_ptr(), total.data_ptr(), scratch.data_ptr(),
+                                                             scratch.numel(), _stream()), "csg_feature_edge_sum")
+        totals.append(total)
+    if not totals:
+        return []
+    values = torch.cat(totals).cpu().tolist()
+    return [float(t) / (3.0 * int(st.faces.shape[0])) for t, (st, _) in zip(values, pairs)]
+
+
 def _heat_from_edge_mean(edge_mean: float, fwhm: float) -> tuple[int, float]:
     raw = float(fwhm) * float(fwhm) * 0.541011 / (edge_mean * edge_mean)
     iterations = max(1, int(math.ceil(raw)))
@@ -188,9 +211,11 @@ def heat_parameters(st: SurfaceStencilDevice, vertices: torch.Tensor, fwhm: floa
     return _heat_from_edge_mean(_edge_mean(st, vertices), fwhm)
 
 
-def smooth_geometry(st: SurfaceStencilDevice, vertices, fwhm: float) -> torch.Tensor:
+def smooth_geometry(st: SurfaceStencilDevice, vertices, fwhm: float, edge_mean: float | None = None) -> torch.Tensor:
     value = torch.as_tensor(vertices, device=st.sphere_points.device).to(torch.float32).contiguous()
-    iterations, _ = heat_parameters(st, value, fwhm)
+    if edge_mean is None:
+        edge_mean = _edge_mean(st, value)
+    iterations, _ = _heat_from_edge_mean(edge_mean, fwhm)
     out = torch.empty_like(value)
     scratch = _scratch(st)
     _native.check(_native.library().csg_feature_smooth_geometry(
@@ -199,7 +224,7 @@ def smooth_geometry(st: SurfaceStencilDevice, vertices, fwhm: float) -> torch.Te
     return out
 
 
-def _smooth_series(st, values, geometry, fwhms, via_norm: bool) -> torch.Tensor:
+def _smooth_series(st, values, geometry, fwhms, via_norm: bool, edge_mean: float | None = None) -> torch.Tensor:
     n = int(st.sphere_points.shape[0])
     base = torch.as_tensor(values, device=st.sphere_points.device).to(torch.float64).reshape(-1).contiguous()
     if base.numel() != n:
@@ -209,7 +234,8 @@ def _smooth_series(st, values, geometry, fwhms, via_norm: bool) -> torch.Tensor:
         raise ValueError("vertices must have shape [sphere_points, 3]")
     if geom.dtype not in (torch.float32, torch.float64):
         geom = geom.to(torch.float64)
-    edge_mean = _edge_mean(st, geom)  # one reduction and one synchronisation for every FWHM of the series
+    if edge_mean is None:  # one reduction and one synchronisation for every FWHM of the series
+        edge_mean = _edge_mean(st, geom)
     params = [_heat_from_edge_mean(edge_mean, f) for f in fwhms]
     counts = ctypes_int_array([p[0] for p in params])
     sigmas = _native.doubles([p[1] for p in params])
@@ -269,8 +295,8 @@ def _minmax(st: SurfaceStencilDevice, values: torch.Tensor) -> torch.Tensor:
     return out
 
 
-def _type5_base(st: SurfaceStencilDevice, geometry: torch.Tensor) -> torch.Tensor:
-    smoothed = smooth_geometry(st, geometry, 50.0)
+def _type5_base(st: SurfaceStencilDevice, geometry: torch.Tensor, edge_mean: float | None = None) -> torch.Tensor:
+    smoothed = smooth_geometry(st, geometry, 50.0, edge_mean)
     normals = vertex_normals(st, smoothed)
     out = torch.empty(int(geometry.shape[0]), dtype=torch.float64, device=geometry.device)
     _native.check(_native.library().csg_feature_normal_displacement(int(geometry.shape[0]), smoothed.data_ptr(),
@@ -286,12 +312,19 @@ def curvature_type5(st: SurfaceStencilDevice, vertices, fwhm: float) -> torch.Te
     return _minmax(st, values)
 
 
-def curvature_type5_to_sheet_many(st: SurfaceStencilDevice, vertices, fwhms) -> tuple[torch.Tensor, ...]:
+def curvature_type5_to_sheet_many(st: SurfaceStencilDevice, vertices, fwhms,
+                                  edge_mean: float | None = None) -> tuple[torch.Tensor, ...]:
+    """Type-5 curvature sheets for several FWHMs; ``edge_mean`` (of ``vertices``, from
+    :func:`edge_means`) saves the synchronisation that computes it."""
+
     if not fwhms:
         return ()
     geometry = torch.as_tensor(vertices, device=st.sphere_points.device).to(torch.float32).contiguous()
-    base = _type5_base(st, geometry)
-    smoothed = _smooth_series(st, base, geometry.to(torch.float64), tuple(fwhms), False)
+    if edge_mean is None:
+        edge_mean = _edge_mean(st, geometry)
+    base = _type5_base(st, geometry, edge_mean)
+    # the same geometry in float64: the same edge mean
+    smoothed = _smooth_series(st, base, geometry.to(torch.float64), tuple(fwhms), False, edge_mean)
     normalised = _minmax(st, smoothed)
     maps = torch.stack([map_values_to_sheet(st, normalised[i]).reshape(-1) for i in range(len(fwhms))])
     maps = _minmax(st, maps)

@@ -182,10 +182,11 @@ def _smoothed_surface(stencil, surface_vertices, heat_fwhm, smoothed_surface):
     return smoothed
 
 
-def _finish(stencil, values, smoothed, iterations, residual) -> RotationFeatureResult:
-    from .features import _minmax
+def _finish(stencil, values, smoothed, iterations, residual, edge_mean: float | None = None) -> RotationFeatureResult:
+    from .features import _minmax, _smooth_series
 
-    smoothed_values = stencil.smooth_values(values, smoothed, 50.0)
+    # stencil.smooth_values(values, smoothed, 50.0); edge_mean (of `smoothed`) saves its synchronisation
+    smoothed_values = _smooth_series(stencil, values, smoothed, (50.0,), True, edge_mean)[0]
     return RotationFeatureResult(values=_minmax(stencil, smoothed_values).contiguous(), iterations=int(iterations),
                                  relative_residual=float(residual))
 
@@ -231,11 +232,22 @@ def compute_rotation_features(stencils: Sequence, surfaces: Sequence, *, heat_fw
         raise ValueError("depth_values length must match stencils")
     if solver not in {"colored-sor", "pcg"}:
         raise ValueError("rotation feature solver must be 'colored-sor' or 'pcg'")
-    smoothed = [_smoothed_surface(st, surf, float(fwhm), None if smoothed_surfaces is None else smoothed_surfaces[i])
-                for i, (st, surf, fwhm) in enumerate(zip(stencils, surfaces, heat_fwhms))]
+    from .features import edge_means, smooth_geometry
+
+    given = [None if smoothed_surfaces is None else smoothed_surfaces[i] for i in range(len(stencils))]
+    smoothed = [None if g is None else _smoothed_surface(st, None, 0.0, g) for st, g in zip(stencils, given)]
+    todo = [i for i, g in enumerate(given) if g is None]
+    if todo:
+        # stencil.smooth_geometry(stencil.resample_vertices(surface), fwhm) per side, with the
+        # sides' mean edge lengths read back together
+        mapped = {i: stencils[i].resample_vertices(surfaces[i]).to(torch.float32).contiguous() for i in todo}
+        means = edge_means([(stencils[i], mapped[i]) for i in todo])
+        for i, mean in zip(todo, means):
+            smoothed[i] = smooth_geometry(stencils[i], mapped[i], float(heat_fwhms[i]), mean)
+    finish_means = edge_means([(st, sm) for st, sm in zip(stencils, smoothed)])
     if depth_values is not None:
-        return tuple(_finish(st, _given_depth(st, dv), sm, 0, 0.0)
-                     for st, dv, sm in zip(stencils, depth_values, smoothed))
+        return tuple(_finish(st, _given_depth(st, dv), sm, 0, 0.0, mean)
+                     for st, dv, sm, mean in zip(stencils, depth_values, smoothed, finish_means))
     # group the sides by triangulation; each group is one batched solve
     topologies = [_stencil_topology(st) for st in stencils]
     results: list[RotationFeatureResult | None] = [None] * len(stencils)
@@ -247,5 +259,5 @@ def compute_rotation_features(stencils: Sequence, surfaces: Sequence, *, heat_fw
         values, its, res = depth_potential(torch.stack([smoothed[i] for i in group]), topo, solver=solver,
                                            alpha=depth_alpha, max_iter=max_iter, tolerance=tolerance)
         for k, i in enumerate(group):
-            results[i] = _finish(stencils[i], values[k], smoothed[i], its[k], res[k])
+            results[i] = _finish(stencils[i], values[k], smoothed[i], its[k], res[k], finish_means[i])
     return tuple(r for r in results if r is not None)

@@ -16,7 +16,7 @@ from typing import Sequence
 
 import torch
 
-from . import _native
+from . import _native, features
 from .dartel_grid import _addr, _dtype_code, _scratch, _tensor, expdef, resolve_device
 
 
@@ -322,25 +322,31 @@ def _surface_sheets(source_vertices, target_vertices, source_stencil, target_ste
     if any(item not in (2, 5) for item in types):
         raise NotImplementedError("The device surface backend supports only upstream curvtype 2 and 5")
 
-    def build_maps(stencil, mapped):
-        if n_steps > 1 and all(item == 5 for item in types):
-            return stencil.curvature_type5_to_sheet_many(mapped, tuple(float(item) for item in fwhm[:n_steps]))
+    many = n_steps > 1 and all(item == 5 for item in types)
+
+    def build_maps(stencil, mapped, edge_mean):
+        if many:
+            return features.curvature_type5_to_sheet_many(stencil, mapped, tuple(float(item) for item in fwhm[:n_steps]),
+                                                          edge_mean)
         return tuple(stencil.curvature_to_sheet(mapped, float(fwhm[i]), curvtype=types[i]) for i in range(n_steps))
 
+    mapped = [src_st.resample_vertices(source), tgt_st.resample_vertices(target)]
+    # the heat kernels' iteration counts come from each side's mean edge length: both read back at once
+    means = features.edge_means([(src_st, mapped[0]), (tgt_st, mapped[1])]) if many else [None, None]
     if parallel_sides:
         current = torch.cuda.current_stream(dev)
         streams = (torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev))
         results = []
-        for stream, stencil, surface in zip(streams, (src_st, tgt_st), (source, target)):
+        for stream, stencil, surface, mean in zip(streams, (src_st, tgt_st), mapped, means):
             stream.wait_stream(current)
             with torch.cuda.stream(stream):
-                results.append(build_maps(stencil, stencil.resample_vertices(surface)))
+                results.append(build_maps(stencil, surface, mean))
         for stream in streams:
             current.wait_stream(stream)
         source_maps, target_maps = results
     else:
-        source_maps = build_maps(src_st, src_st.resample_vertices(source))
-        target_maps = build_maps(tgt_st, tgt_st.resample_vertices(target))
+        source_maps = build_maps(src_st, mapped[0], means[0])
+        target_maps = build_maps(tgt_st, mapped[1], means[1])
     return (torch.stack(source_maps, dim=0).to(dtype=dtype).contiguous(),
             torch.stack(target_maps, dim=0).to(dtype=dtype).contiguous())
 
