@@ -126,3 +126,24 @@ def test_smoothing_with_even_and_odd_iteration_counts(device_stencil):
         want = of.smooth_values(F["values"], m, F["faces"], fwhm, tab)
         np.testing.assert_allclose(first, want, rtol=0, atol=1e-13)
     assert parities == {0, 1}
+
+
+@pytest.mark.gpu
+def test_edge_means_read_back_together_equal_single_reads(device_stencil):
+    """The batched edge-mean read-back equals one read per surface, and a float32 surface and
+    its float64 copy give the same mean (the sums widen float32 coordinates first)."""
+
+    from cat_surface_gpu_b200 import features
+
+    st = device_stencil
+    m32 = torch.as_tensor(F["resampled32"], device="cuda:0")
+    other = (m32 * 1.01).contiguous()
+    singles = [features._edge_mean(st, m32), features._edge_mean(st, other)]
+    together = features.edge_means([(st, m32), (st, other), (st, m32.to(torch.float64))])
+    assert together[:2] == singles
+    assert together[2] == singles[0]
+    # the sheets built with the shared mean equal the ones that compute it themselves
+    fw = (5.0, 5.0 / 3.0)
+    for a, b in zip(features.curvature_type5_to_sheet_many(st, m32, fw),
+                    features.curvature_type5_to_sheet_many(st, m32, fw, together[0])):
+        assert torch.equal(a, b)

@@ -34,6 +34,66 @@ def test_rotation_matrix_is_orthonormal_and_inverts():
     assert np.allclose(rotation_matrix_from_angles(-pole).numpy() @ m, np.eye(3), atol=1e-15)
 
 
+def _matrix_by_torch_ops(angles):
+    """Rz (Ry Rx) from 0-dim float64 torch operations, one per multiply and add (the reference's form)."""
+
+    import torch
+
+    value = torch.as_tensor(np.asarray(angles, dtype=np.float64)).reshape(-1)
+    ca = [torch.cos(a) for a in value.unbind()]
+    sa = [torch.sin(a) for a in value.unbind()]
+    one, zero = torch.ones((), dtype=torch.float64), torch.zeros((), dtype=torch.float64)
+    rx = (one, zero, zero, zero, ca[0], sa[0], zero, -sa[0], ca[0])
+    ry = (ca[1], zero, sa[1], zero, one, zero, -sa[1], zero, ca[1])
+    rz = (ca[2], sa[2], zero, -sa[2], ca[2], zero, zero, zero, one)
+
+    def product(left, right):
+        out = [None] * 9
+        for r in range(3):
+            for c in range(3):
+                out[r + 3 * c] = ((zero + left[r] * right[3 * c]) + left[r + 3] * right[1 + 3 * c]) \
+                    + left[r + 6] * right[2 + 3 * c]
+        return out
+
+    return torch.stack(product(rz, product(ry, rx))).reshape(3, 3).numpy()
+
+
+def test_rotation_matrix_bit_identical_to_torch_operations():
+    """The matrix is built from float64 Python products; every bit equals the 0-dim torch form."""
+
+    from cat_surface_gpu_b200.gpu_pipeline import rotation_matrix_from_angles
+
+    rng = np.random.default_rng(11)
+    cases = [rng.uniform(-4.0, 4.0, 3) for _ in range(400)]
+    cases += [np.zeros(3), np.array([0.0, np.pi / 2.0, 0.0]), np.array([-0.0, 0.0, -0.0]),
+              np.array([np.pi, -np.pi, 1e-300]), np.array([1e-8, -1e-12, 3e-5])]
+    for angles in cases:
+        got = rotation_matrix_from_angles(angles).numpy()
+        assert got.dtype == np.float64
+        np.testing.assert_array_equal(got.view(np.uint64), _matrix_by_torch_ops(angles).view(np.uint64))
+
+
+def test_shared_resampling_faces_hit_the_identity_cache(native_library):
+    """Stencils share one read-only face array; the identity lookup returns the bytes-keyed tables."""
+
+    import torch
+
+    from cat_surface_gpu_b200 import features
+    from cat_surface_gpu_b200.surface_stencil import resampling_sphere
+
+    points, faces = resampling_sphere(3)
+    assert not faces.flags.writeable and not points.flags.writeable
+    with pytest.raises(ValueError):
+        faces[0, 0] = 1
+    cpu = torch.device("cpu")
+    first = features._topology(faces, points.shape[0], cpu)
+    assert features._topology(faces, points.shape[0], cpu) is first
+    fresh = features._topology(np.array(faces), points.shape[0], cpu)  # a writable copy: the bytes key
+    for a, b in zip(first[:4], fresh[:4]):
+        assert torch.equal(a, b)
+    assert first[4] == fresh[4]
+
+
 def test_normalise_rejects_degenerate_sphere():
     from cat_surface_gpu_b200.gpu_pipeline import normalise_sphere
 
