@@ -247,13 +247,21 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
         lo_nb.reserve(static_cast<size_t>(3) * n_faces);
         hi_nb.reserve(static_cast<size_t>(3) * n_faces);
         {
-            std::vector<int32_t> ring;
+            // each face neighbour of v appears in two of its faces: a per-vertex stamp
+            // drops the repeats, and only the few unique neighbours are sorted
+            std::vector<int32_t> ring, stamp(n, -1);
             for (int v = 0; v < n; ++v) {
                 ring.clear();
+                stamp[v] = v;
                 for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
-                    for (int k = 0; k < 3; ++k) ring.push_back(slot_tri[4 * s + k]);
+                    for (int k = 0; k < 3; ++k) {
+                        const int32_t u = slot_tri[4 * s + k];
+                        if (stamp[u] != v) {
+                            stamp[u] = v;
+                            ring.push_back(u);
+                        }
+                    }
                 std::sort(ring.begin(), ring.end());
-                ring.erase(std::unique(ring.begin(), ring.end()), ring.end());
                 for (int32_t u : ring) {
                     if (u < v) lo_nb.push_back(u);
                     if (u > v) hi_nb.push_back(u);
@@ -273,19 +281,24 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
             bool converged = false;
             int it = 0;
             for (; it < cap && !converged; ++it) {
+                // In the forward pass no lower neighbour of v changes while v is
+                // processed (and no higher one in the backward pass), so taking the
+                // neighbours' maximum first raises f(v) exactly as one comparison per
+                // neighbour would, without a branch per constraint.
                 bool changed = false;
-                for (int v = 0; v < n; ++v)  // f(v) >= f(u) + 1 for lower neighbours u
-                    for (int k = lo_off[v]; k < lo_off[v + 1]; ++k)
-                        if (f[v] < f[lo_nb[k]] + 1) {
-                            f[v] = f[lo_nb[k]] + 1;
-                            changed = true;
-                        }
-                for (int v = n - 1; v >= 0; --v)  // f(v) >= f(w) - (D - 1) for higher neighbours w
-                    for (int k = hi_off[v]; k < hi_off[v + 1]; ++k)
-                        if (f[v] < f[hi_nb[k]] - (trial - 1)) {
-                            f[v] = f[hi_nb[k]] - (trial - 1);
-                            changed = true;
-                        }
+                int32_t* fv = f.data();
+                for (int v = 0; v < n; ++v) {  // f(v) >= f(u) + 1 for lower neighbours u
+                    int32_t need = fv[v];
+                    for (int k = lo_off[v]; k < lo_off[v + 1]; ++k) need = std::max(need, fv[lo_nb[k]] + 1);
+                    changed |= need != fv[v];
+                    fv[v] = need;
+                }
+                for (int v = n - 1; v >= 0; --v) {  // f(v) >= f(w) - (D - 1) for higher neighbours w
+                    int32_t need = fv[v];
+                    for (int k = hi_off[v]; k < hi_off[v + 1]; ++k) need = std::max(need, fv[hi_nb[k]] - (trial - 1));
+                    changed |= need != fv[v];
+                    fv[v] = need;
+                }
                 converged = !changed;
             }
             if (!converged) break;

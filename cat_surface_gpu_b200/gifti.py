@@ -15,8 +15,12 @@ which is what CAT-Surface's gifticlib produces and accepts.
 from __future__ import annotations
 
 import base64
+from collections import OrderedDict
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
+import os
 from pathlib import Path
+import threading
 import xml.etree.ElementTree as ET
 import zlib
 
@@ -45,6 +49,66 @@ class GiftiMesh:
     faces: np.ndarray
 
 
+# Deflate of large arrays runs in parallel chunks (as pigz does): each chunk is a raw
+# deflate stream ended by a sync flush (the last one by the final block), so their
+# concatenation behind a zlib header and the Adler-32 of the whole input is one valid
+# zlib stream that any inflater reads back as the same bytes.
+_CHUNK = 1 << 17
+_PARALLEL_MIN = 1 << 19
+_POOL: ThreadPoolExecutor | None = None
+_POOL_LOCK = threading.Lock()
+
+
+def _pool() -> ThreadPoolExecutor:
+    global _POOL
+    with _POOL_LOCK:
+        if _POOL is None:
+            _POOL = ThreadPoolExecutor(max_workers=max(2, min(16, os.cpu_count() or 2)),
+                                       thread_name_prefix="gifti-deflate")
+    return _POOL
+
+
+def _deflate(raw: bytes, level: int = 1) -> bytes:
+    if len(raw) < _PARALLEL_MIN:
+        return zlib.compress(raw, level)
+    chunks = [raw[i: i + _CHUNK] for i in range(0, len(raw), _CHUNK)]
+    last = len(chunks) - 1
+
+    def one(item):
+        index, chunk = item
+        stream = zlib.compressobj(level, zlib.DEFLATED, -15)
+        return stream.compress(chunk) + stream.flush(zlib.Z_FINISH if index == last else zlib.Z_SYNC_FLUSH)
+
+    body = b"".join(_pool().map(one, enumerate(chunks)))
+    header = bytes((0x78, 0x01 if level <= 1 else (0x5E if level <= 5 else (0x9C if level == 6 else 0xDA))))
+    return header + body + zlib.adler32(raw).to_bytes(4, "big")
+
+
+# Encoded payloads of the int32 arrays decoded most recently (face arrays): writing an
+# array with the same bytes reuses its payload instead of compressing it again.  Keyed
+# by (DataType, shape, CRC-32); a hit is confirmed by comparing the bytes themselves.
+_PAYLOADS: OrderedDict = OrderedDict()
+_PAYLOADS_MAX = 8
+_PAYLOADS_LOCK = threading.Lock()
+
+
+def _remember_payload(dtype_name: str, shape: tuple, raw: bytes, payload: str) -> None:
+    key = (dtype_name, shape, zlib.crc32(raw))
+    with _PAYLOADS_LOCK:
+        _PAYLOADS[key] = (raw, payload)
+        _PAYLOADS.move_to_end(key)
+        while len(_PAYLOADS) > _PAYLOADS_MAX:
+            _PAYLOADS.popitem(last=False)
+
+
+def _known_payload(dtype_name: str, shape: tuple, raw: bytes) -> str | None:
+    with _PAYLOADS_LOCK:
+        hit = _PAYLOADS.get((dtype_name, shape, zlib.crc32(raw)))
+    if hit is not None and hit[0] == raw:
+        return hit[1]
+    return None
+
+
 def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
     attrs = element.attrib
     dtype_name = attrs.get("DataType", "NIFTI_TYPE_FLOAT32")
@@ -63,9 +127,12 @@ def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
         values = np.array(text.split(), dtype=np.float64 if dtype.kind == "f" else np.int64)
         values = values.astype(dtype)
     elif encoding in ("Base64Binary", "GZipBase64Binary"):
-        raw = base64.b64decode("".join(text.split()))
+        payload = "".join(text.split())
+        raw = base64.b64decode(payload)
         if encoding == "GZipBase64Binary":
             raw = zlib.decompress(raw)
+            if dtype_name == "NIFTI_TYPE_INT32" and endian == "LittleEndian" and order == "C":
+                _remember_payload(dtype_name, shape, raw, payload)
         wire = dtype.newbyteorder("<" if endian == "LittleEndian" else ">")
         values = np.frombuffer(raw, dtype=wire).astype(dtype)
     else:
@@ -109,10 +176,13 @@ def read_gifti_mesh(path: str | Path) -> GiftiMesh:
     )
 
 
-def _encode_array(values: np.ndarray, intent: int, dtype_name: str) -> str:
-    # deflate level 1: on vertex and index arrays it packs as well as level 6 at a sixth of the time
-    raw = np.ascontiguousarray(values).astype(values.dtype.newbyteorder("<")).tobytes()
-    payload = base64.b64encode(zlib.compress(raw, 1)).decode("ascii")
+def _encode_array(values: np.ndarray, intent: int, dtype_name: str, payload: str | None = None) -> str:
+    if payload is None:
+        raw = np.ascontiguousarray(values).astype(values.dtype.newbyteorder("<")).tobytes()
+        payload = _known_payload(dtype_name, tuple(values.shape), raw) if dtype_name == "NIFTI_TYPE_INT32" else None
+        if payload is None:
+            # deflate level 1: on vertex and index arrays it packs as well as level 6 at a sixth of the time
+            payload = base64.b64encode(_deflate(raw, 1)).decode("ascii")
     dims = "".join(f' Dim{i}="{size}"' for i, size in enumerate(values.shape))
     intent_name = _INTENT_NAMES.get(intent, "NIFTI_INTENT_NONE")
     transform = ""
@@ -147,11 +217,41 @@ def write_gifti_mesh(
 
     intents = None
     if reference_path is not None:
-        intents = [intent for _, intent in read_gifti_arrays(reference_path)]
+        intents = [_INTENT_CODES.get(item.attrib.get("Intent", "NIFTI_INTENT_NONE"), 0)
+                   for item in _data_arrays(reference_path)]
     _write_mesh(path, mesh, intents)
 
 
-def _write_mesh(path, mesh: GiftiMesh, intents) -> None:
+def _data_arrays(path) -> list[ET.Element]:
+    """The DataArray elements of a GIFTI file, payloads not decoded."""
+
+    root = ET.parse(str(path)).getroot()
+    if root.tag != "GIFTI":
+        raise ValueError(f"Not a GIFTI file: {path}")
+    return root.findall("DataArray")
+
+
+def _shape(element: ET.Element) -> tuple[int, ...]:
+    attrs = element.attrib
+    return tuple(int(attrs[f"Dim{i}"]) for i in range(int(attrs.get("Dimensionality", "1"))))
+
+
+def _verbatim_faces(element: ET.Element) -> str | None:
+    """The payload of an [m, 3] int32 little-endian row-major gzip face array, as stored."""
+
+    attrs = element.attrib
+    shape = _shape(element)
+    if (attrs.get("DataType") == "NIFTI_TYPE_INT32" and attrs.get("Encoding") == "GZipBase64Binary"
+            and attrs.get("Endian", "LittleEndian") == "LittleEndian"
+            and attrs.get("ArrayIndexingOrder", "RowMajorOrder") == "RowMajorOrder"
+            and len(shape) == 2 and shape[1] == 3):
+        data = element.find("Data")
+        if data is not None and data.text:
+            return "".join(data.text.split())
+    return None
+
+
+def _write_mesh(path, mesh: GiftiMesh, intents, faces_payload: str | None = None) -> None:
     point_intent = _INTENT_CODES["NIFTI_INTENT_POINTSET"]
     triangle_intent = _INTENT_CODES["NIFTI_INTENT_TRIANGLE"]
     if intents is not None:
@@ -168,7 +268,7 @@ def _write_mesh(path, mesh: GiftiMesh, intents) -> None:
         '<!DOCTYPE GIFTI SYSTEM "http://www.nitrc.org/frs/download.php/115/gifti.dtd">\n'
         '<GIFTI Version="1.0" NumberOfDataArrays="2">\n<MetaData/>\n<LabelTable/>\n'
         + _encode_array(vertices, point_intent, "NIFTI_TYPE_FLOAT32")
-        + _encode_array(faces, triangle_intent, "NIFTI_TYPE_INT32")
+        + _encode_array(faces, triangle_intent, "NIFTI_TYPE_INT32", faces_payload)
         + "</GIFTI>\n"
     )
     output = Path(path)
@@ -184,11 +284,17 @@ def write_vertices_like(reference_path: str | Path, output_path: str | Path, ver
     ``reference_path`` unchanged, so triangle arrays are exact by construction.
     """
 
-    arrays = read_gifti_arrays(reference_path)
-    if len(arrays) < 2:
+    elements = _data_arrays(reference_path)
+    if len(elements) < 2:
         raise ValueError(f"GIFTI file must contain vertex and face arrays: {reference_path}")
     values = np.ascontiguousarray(vertices, dtype=np.float32)
-    if values.shape != arrays[0][0].shape:
-        raise ValueError(f"vertices shape {values.shape} does not match {arrays[0][0].shape}")
-    faces = np.ascontiguousarray(arrays[1][0], dtype=np.int32)
-    _write_mesh(output_path, GiftiMesh(values, faces), [intent for _, intent in arrays])
+    if values.shape != _shape(elements[0]):
+        raise ValueError(f"vertices shape {values.shape} does not match {_shape(elements[0])}")
+    intents = [_INTENT_CODES.get(item.attrib.get("Intent", "NIFTI_INTENT_NONE"), 0) for item in elements]
+    payload = _verbatim_faces(elements[1])
+    if payload is not None:
+        # the reference's own face payload, copied as stored: the same bytes without re-encoding
+        faces = np.empty(_shape(elements[1]), dtype=np.int32)
+    else:
+        faces = np.ascontiguousarray(_decode_array(elements[1])[0], dtype=np.int32)
+    _write_mesh(output_path, GiftiMesh(values, faces), intents, payload)

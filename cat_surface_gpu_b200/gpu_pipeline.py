@@ -283,8 +283,9 @@ def run_cat_surface_gpu_pipeline(
 
     _validate_options(has_values=rotation_values_path is not None, **options)
     total_start = time.perf_counter()
-    meshes = [read_gifti_mesh(path) for path in (source_surface_path, source_sphere_path, target_surface_path,
-                                                 target_sphere_path)]
+    with ThreadPoolExecutor(max_workers=4) as pool:  # the four decodes overlap where zlib releases the GIL
+        meshes = list(pool.map(read_gifti_mesh, (source_surface_path, source_sphere_path, target_surface_path,
+                                                 target_sphere_path)))
     read_seconds = time.perf_counter() - total_start
     stencils = {}
     if source_stencil_path is not None:

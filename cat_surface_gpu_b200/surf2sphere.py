@@ -163,6 +163,20 @@ class Surf2SphereTopology:
         )
 
 
+    @classmethod
+    def plan_only(cls, mesh: GiftiMesh) -> "Surf2SphereTopology":
+        """Only ``plan`` (the sweep schedule): the GPU path reads nothing else, so the
+        reference-compatible tables are left empty instead of being built."""
+
+        faces = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+        if faces.ndim != 2 or faces.shape[1] != 3:
+            raise ValueError(f"faces must have shape [m, 3], got {faces.shape}")
+        empty = np.zeros((0, 0), dtype=np.int64)
+        return cls(incident_faces=empty, incident_mask=empty.astype(bool), neighbours=empty,
+                   neighbour_mask=empty.astype(bool), color_groups=(), ordered_groups=(),
+                   plan=SweepPlan.build(faces, int(mesh.vertices.shape[0])))
+
+
 @dataclass(frozen=True)
 class CatSurf2SphereGpuResult:
     """Store the generated sphere path and synchronized stage timings."""
@@ -658,18 +672,20 @@ def run_cat_surf2sphere_gpu(
     if preprocess_kernel != "cpu":
         # every stage on the GPU (reference 1135-1213 with the native preprocess)
         input_mesh = read_gifti_mesh(input_path)
+        on_device = _resolve_dtype(dtype) == torch.float32 and stop_at > 5
         topology_start = time.perf_counter()
-        topology = Surf2SphereTopology.from_mesh(input_mesh)
+        topology = Surf2SphereTopology.plan_only(input_mesh) if on_device else Surf2SphereTopology.from_mesh(input_mesh)
         timings["topology_build_seconds"] = time.perf_counter() - topology_start
         area = surface_area(input_mesh)
-        if _resolve_dtype(dtype) == torch.float32 and stop_at > 5:
+        if on_device:
             pre = _surf2sphere_on_device(input_mesh, topology, area, stop_at, device, areal_arithmetic, timings)
             write_start = time.perf_counter()
             write_vertices_like(input_path, output_path, pre)
             timings["output_write_seconds"] = time.perf_counter() - write_start
-            result_mesh = read_gifti_mesh(output_path)
             timings["total_seconds"] = time.perf_counter() - total_start
-            return CatSurf2SphereGpuResult(result_mesh.vertices, result_mesh.faces, timings, output_path)
+            # the file holds exactly these arrays (float32 vertices, the input's faces)
+            return CatSurf2SphereGpuResult(np.ascontiguousarray(pre, dtype=np.float32), input_mesh.faces, timings,
+                                           output_path)
         pre, pre_timings = run_surf2sphere_preprocess_cuda(
             input_mesh.vertices, input_mesh.faces, topology, stop_at=min(stop_at, 5), desired_surface_area=area,
             device=device, dtype=dtype, schedule_block_size=preprocess_block_size)

@@ -239,6 +239,77 @@ def test_gifti_round_trip(tmp_path):
     np.testing.assert_array_equal(other.vertices, v * 2)
 
 
+def test_gifti_large_arrays_parallel_deflate_and_payload_reuse(tmp_path):
+    """Large arrays deflate in parallel chunks into one standard zlib stream; a face array
+    equal to one decoded before reuses its stored payload; any other array is encoded anew."""
+
+    import base64
+    import re
+    import zlib
+
+    from conftest import GOLDEN
+
+    from cat_surface_gpu_b200 import gifti
+    from cat_surface_gpu_b200.gifti import GiftiMesh, read_gifti_mesh, write_gifti_mesh, write_vertices_like
+
+    c = np.load(GOLDEN / "surf2sphere_c2.npz")
+    v, f = c["surface"].astype(np.float32), c["faces"].astype(np.int32)
+    for raw in (v.tobytes(), f.tobytes(), v[:5000].tobytes()):
+        z = gifti._deflate(raw, 1)
+        assert zlib.decompress(z) == raw
+        assert zlib.decompressobj().decompress(z) == raw
+    write_gifti_mesh(tmp_path / "a.gii", GiftiMesh(v, f))
+    a = read_gifti_mesh(tmp_path / "a.gii")
+    np.testing.assert_array_equal(a.vertices, v)
+    np.testing.assert_array_equal(a.faces, f)
+
+    def payloads(path):
+        return re.findall(r"<Data>([^<]*)</Data>", (tmp_path / path).read_text())
+
+    moved = (v * 1.5).astype(np.float32)
+    write_gifti_mesh(tmp_path / "b.gii", GiftiMesh(moved, a.faces.copy()), reference_path=tmp_path / "a.gii")
+    assert payloads("b.gii")[1] == payloads("a.gii")[1]  # the decoded face payload, reused
+    b = read_gifti_mesh(tmp_path / "b.gii")
+    np.testing.assert_array_equal(b.vertices, moved)
+    np.testing.assert_array_equal(b.faces, f)
+    changed = a.faces.copy()
+    changed[7] = changed[7][::-1]
+    write_gifti_mesh(tmp_path / "c.gii", GiftiMesh(moved, changed))
+    np.testing.assert_array_equal(read_gifti_mesh(tmp_path / "c.gii").faces, changed)
+    write_vertices_like(tmp_path / "a.gii", tmp_path / "d.gii", moved)
+    assert payloads("d.gii")[1] == payloads("a.gii")[1]  # copied from the reference as stored
+    np.testing.assert_array_equal(read_gifti_mesh(tmp_path / "d.gii").faces, f)
+    # a reference stored with another encoding: decoded and written anew
+    text = (tmp_path / "a.gii").read_text()
+    plain = base64.b64encode(f.astype("<i4").tobytes()).decode()
+    faces_start = text.index("<DataArray", text.index("</DataArray>"))
+    tail = text[faces_start:]
+    tail = tail.replace('Encoding="GZipBase64Binary"', 'Encoding="Base64Binary"', 1)
+    tail = re.sub(r"<Data>[^<]*</Data>", lambda _: f"<Data>{plain}</Data>", tail, count=1)
+    (tmp_path / "e.gii").write_text(text[:faces_start] + tail)
+    np.testing.assert_array_equal(read_gifti_mesh(tmp_path / "e.gii").faces, f)
+    write_vertices_like(tmp_path / "e.gii", tmp_path / "g.gii", moved)
+    g = read_gifti_mesh(tmp_path / "g.gii")
+    np.testing.assert_array_equal(g.faces, f)
+    np.testing.assert_array_equal(g.vertices, moved)
+    with pytest.raises(ValueError):
+        write_vertices_like(tmp_path / "a.gii", tmp_path / "h.gii", moved[:10])
+
+
+def test_plan_only_topology_has_the_same_plan(native_library):
+    from cat_surface_gpu_b200 import synthetic
+    from cat_surface_gpu_b200.gifti import GiftiMesh
+    from cat_surface_gpu_b200.surf2sphere import Surf2SphereTopology
+
+    pts, tri = synthetic.folded_icosphere(4, seed=5, radius_mm=50.0)
+    mesh = GiftiMesh(pts.astype(np.float32), tri.astype(np.int32))
+    full, light = Surf2SphereTopology.from_mesh(mesh), Surf2SphereTopology.plan_only(mesh)
+    for name in ("slot_off", "slot_tri", "order", "level_begin", "level_end"):
+        np.testing.assert_array_equal(getattr(light.plan, name), getattr(full.plan, name))
+    assert (light.plan.n_levels, light.plan.level_stride, light.plan.max_degree) == \
+        (full.plan.n_levels, full.plan.level_stride, full.plan.max_degree)
+
+
 def test_product_has_no_cpu_path():
     """Asking the product for a CPU device raises instead of falling back."""
 
