@@ -31,23 +31,28 @@ def official_seed_grid_angles() -> np.ndarray:
     return np.asarray(values, dtype=np.float64)
 
 
+_ROW0 = np.array([r for c in range(3) for r in range(3)])
+_ROW1 = _ROW0 + 3
+_ROW2 = _ROW0 + 6
+_COL0 = np.array([3 * c for c in range(3) for _ in range(3)])
+_COL1 = _COL0 + 1
+_COL2 = _COL0 + 2
+
+
 def rotation_matrices_flat(angles) -> np.ndarray:
     """Column-major flat float32 matrices Rz (Ry Rx) per angle row (reference 223-292)."""
 
     a = np.asarray(angles, dtype=np.float64).reshape(-1, 3).astype(np.float32)
     al, be, ga = a[:, 0], a[:, 1], a[:, 2]
     z, o = np.zeros_like(al), np.ones_like(al)
-    rx = np.stack((o, z, z, z, np.cos(al), np.sin(al), z, -np.sin(al), np.cos(al)), axis=1)
-    ry = np.stack((np.cos(be), z, np.sin(be), z, o, z, -np.sin(be), z, np.cos(be)), axis=1)
-    rz = np.stack((np.cos(ga), np.sin(ga), z, -np.sin(ga), np.cos(ga), z, z, z, o), axis=1)
-    first = np.empty_like(rx)
-    out = np.empty_like(rx)
-    for r in range(3):
-        for c in range(3):
-            first[:, r + 3 * c] = (ry[:, r] * rx[:, 3 * c] + ry[:, r + 3] * rx[:, 1 + 3 * c]) + ry[:, r + 6] * rx[:, 2 + 3 * c]
-    for r in range(3):
-        for c in range(3):
-            out[:, r + 3 * c] = (rz[:, r] * first[:, 3 * c] + rz[:, r + 3] * first[:, 1 + 3 * c]) + rz[:, r + 6] * first[:, 2 + 3 * c]
+    ca, sa, cb, sb, cg, sg = np.cos(al), np.sin(al), np.cos(be), np.sin(be), np.cos(ga), np.sin(ga)
+    rx = np.stack((o, z, z, z, ca, sa, z, -sa, ca), axis=1)
+    ry = np.stack((cb, z, sb, z, o, z, -sb, z, cb), axis=1)
+    rz = np.stack((cg, sg, z, -sg, cg, z, z, z, o), axis=1)
+    # entry r + 3 c of left @ right (column-major): (l[r] R[3c] + l[r+3] R[3c+1]) + l[r+6] R[3c+2],
+    # all nine entries at once -- the same float32 multiplies and adds per entry
+    first = (ry[:, _ROW0] * rx[:, _COL0] + ry[:, _ROW1] * rx[:, _COL1]) + ry[:, _ROW2] * rx[:, _COL2]
+    out = (rz[:, _ROW0] * first[:, _COL0] + rz[:, _ROW1] * first[:, _COL1]) + rz[:, _ROW2] * first[:, _COL2]
     return np.ascontiguousarray(out)
 
 
@@ -172,13 +177,20 @@ class _Costing:
         need = _native.library().csg_rotation_scratch_bytes(1, ctypes.addressof(n_src), ctypes.addressof(n_cand), tile)
         self.scratch = torch.empty(int(need), dtype=torch.uint8, device=dev)
         self.pinned = torch.empty(self.capacity, dtype=torch.float64, pin_memory=True)
+        self.staging = torch.empty((self.capacity, 9), dtype=torch.float32, pin_memory=True)
 
-    def evaluate(self, angles: np.ndarray) -> torch.Tensor:
+    def evaluate(self, angles: np.ndarray, *, host: bool = False):
+        """Costs of these candidates: a device tensor, or (``host``) a NumPy copy read back in the
+        same synchronisation as the coverage status."""
+
         mats = rotation_matrices_flat(angles)
         count = mats.shape[0]
         if count > self.capacity:
             raise ValueError("more candidates than this costing context holds")
-        self.matrices[:count].copy_(torch.from_numpy(mats), non_blocking=False)
+        # page-locked staging: an asynchronous upload (the previous call's status read has
+        # synchronised, so the staging rows are free)
+        self.staging[:count].copy_(torch.from_numpy(mats))
+        self.matrices[:count].copy_(self.staging[:count], non_blocking=True)
         surface = _native.RotationSurface(
             self.inputs.source_points.data_ptr(), self.inputs.source_values.data_ptr(),
             self.index.target_triangles.data_ptr(), self.index.target_faces.data_ptr(),
@@ -194,11 +206,15 @@ class _Costing:
                                         self.scratch.data_ptr(), self.scratch.numel(), stream),
             "csg_rotation_cost_batch",
         )
+        if host:
+            self.pinned[:count].copy_(self.costs[:count], non_blocking=True)
         status = ctypes.c_int(0)
         _native.check(lib.csg_rotation_status(self.scratch.data_ptr(), 1, stream, ctypes.addressof(status)),
                       "csg_rotation_status")
         if status.value != 0:
             raise RuntimeError("Rotation is not covered by target sphere candidate index")
+        if host:
+            return self.pinned[:count].numpy().copy()
         return self.costs[:count]
 
 
@@ -355,7 +371,7 @@ class RotationGridIndexDevice:
         costing = self._costing(inputs, 64)
 
         def cost(points: np.ndarray) -> np.ndarray:
-            return costing.evaluate(points).cpu().numpy()
+            return costing.evaluate(points, host=True)
 
         simplex = np.stack((seed, seed + (simplex_step, 0.0, 0.0), seed + (0.0, simplex_step, 0.0),
                             seed + (0.0, 0.0, simplex_step)))

@@ -72,6 +72,37 @@ def device_index(native_library):
                                            include_dense_candidate_table=False).to("cuda")
 
 
+
+def _matrices_per_entry(angles):
+    """Rz (Ry Rx) column-major float32, one numpy operation per matrix entry (the reference's form)."""
+
+    a = np.asarray(angles, dtype=np.float64).reshape(-1, 3).astype(np.float32)
+    al, be, ga = a[:, 0], a[:, 1], a[:, 2]
+    z, o = np.zeros_like(al), np.ones_like(al)
+    rx = np.stack((o, z, z, z, np.cos(al), np.sin(al), z, -np.sin(al), np.cos(al)), axis=1)
+    ry = np.stack((np.cos(be), z, np.sin(be), z, o, z, -np.sin(be), z, np.cos(be)), axis=1)
+    rz = np.stack((np.cos(ga), np.sin(ga), z, -np.sin(ga), np.cos(ga), z, z, z, o), axis=1)
+    first, out = np.empty_like(rx), np.empty_like(rx)
+    for r in range(3):
+        for c in range(3):
+            first[:, r + 3 * c] = (ry[:, r] * rx[:, 3 * c] + ry[:, r + 3] * rx[:, 1 + 3 * c]) + ry[:, r + 6] * rx[:, 2 + 3 * c]
+    for r in range(3):
+        for c in range(3):
+            out[:, r + 3 * c] = (rz[:, r] * first[:, 3 * c] + rz[:, r + 3] * first[:, 1 + 3 * c]) + rz[:, r + 6] * first[:, 2 + 3 * c]
+    return out
+
+
+def test_rotation_matrices_bit_identical_to_per_entry_form():
+    from cat_surface_gpu_b200.surface_rotation import official_seed_grid_angles, rotation_matrices_flat
+
+    rng = np.random.default_rng(7)
+    batches = [official_seed_grid_angles(), np.zeros((1, 3)), np.array([[0.0, np.pi / 2.0, -0.0]])]
+    batches += [rng.uniform(-7.0, 7.0, (n, 3)) for n in (1, 2, 3, 4, 5, 17, 64, 1000)]
+    for angles in batches:
+        got, want = rotation_matrices_flat(angles), _matrices_per_entry(angles)
+        assert got.dtype == np.float32 and got.shape == want.shape
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
 @pytest.mark.gpu
 def test_costs_match_oracle_and_reference(device_index):
     got = device_index.cost_batch(R["source_points"], R["source_values"], R["target_values"], R["angles"]).cpu().numpy()
