@@ -44,6 +44,7 @@ from __future__ import annotations
 
 import argparse
 from datetime import timedelta
+import gc
 import json
 import os
 from pathlib import Path
@@ -605,6 +606,10 @@ def run_native(args):
         hemi.step()
     barrier()
     hemi.check_status()
+    # Python's cyclic collector: a full collection over the ~170k objects of torch and the
+    # package pauses 50-100 ms in whichever step it lands; collect once and freeze what exists
+    gc.collect()
+    gc.freeze()
     sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
     if sampler:
         sampler.start()
@@ -713,6 +718,7 @@ def run_native(args):
                        "surfwarp": {k: v for k, v in CHAIN.items() if k != "sheet_size"},
                        "sweep_launch": hemi.launch,
                        "l2": "flushed before every timed step by a 256 MiB device write",
+                       "python_gc": "collected and frozen after the warm-up (gc.freeze)",
                        "parallelism": f"replicas x{world}"},
             "stages_s": stages,
             "roofline": {

@@ -16,6 +16,7 @@ Public names and signatures follow the reference module
 
 from __future__ import annotations
 
+from concurrent.futures import Future, ThreadPoolExecutor
 from dataclasses import dataclass, field
 import math
 from pathlib import Path
@@ -573,13 +574,15 @@ def run_surf2sphere_preprocess_cuda(
     return np.ascontiguousarray(result, dtype=np.float32), timings
 
 
-def _surf2sphere_on_device(mesh: GiftiMesh, topology: Surf2SphereTopology, area: float, stop_at: int, device,
-                           arithmetic: str, timings: dict) -> np.ndarray:
+def _surf2sphere_on_device(mesh: GiftiMesh, topology: "Surf2SphereTopology | Future", area: float, stop_at: int,
+                           device, arithmetic: str, timings: dict) -> np.ndarray:
     """Stages 1-5, the ellipsoid step, the sweeps and the final ellipsoid step without leaving the GPU.
 
     Same results as running :func:`run_surf2sphere_preprocess_cuda` and
     :func:`run_areal_smoothing_cuda` with the host conversions between them:
     the device conversion and projection radius use the host arithmetic.
+    ``topology`` may be a future of one (the plan still being built on
+    another thread); it is resolved once the upload and ring tables are done.
     """
 
     from .features import _topology
@@ -592,13 +595,15 @@ def _surf2sphere_on_device(mesh: GiftiMesh, topology: Surf2SphereTopology, area:
         raise RuntimeError(f"CAT_Surf2Sphere CUDA backend: {exc}") from exc
     tri = np.ascontiguousarray(mesh.faces, dtype=np.int32)
     n = int(mesh.vertices.shape[0])
-    plan = topology.plan
-    if plan is None or plan.slot_off.shape[0] != n + 1:
-        plan = SweepPlan.build(tri, n)
     with torch.no_grad(), torch.cuda.device(target):
         start = time.perf_counter()
         points = torch.from_numpy(np.ascontiguousarray(mesh.vertices, dtype=np.float32)).to(target)
         rings = _topology(tri, n, target)
+        if isinstance(topology, Future):  # the plan was being built while the lines above ran
+            topology = topology.result()
+        plan = topology.plan
+        if plan is None or plan.slot_off.shape[0] != n + 1:
+            plan = SweepPlan.build(tri, n)
         plan_device = plan.to_device(target)
         faces_device = torch.from_numpy(tri).to(target)
         timings["preprocess_upload_seconds"] = time.perf_counter() - start
@@ -673,12 +678,19 @@ def run_cat_surf2sphere_gpu(
         # every stage on the GPU (reference 1135-1213 with the native preprocess)
         input_mesh = read_gifti_mesh(input_path)
         on_device = _resolve_dtype(dtype) == torch.float32 and stop_at > 5
-        topology_start = time.perf_counter()
-        topology = Surf2SphereTopology.plan_only(input_mesh) if on_device else Surf2SphereTopology.from_mesh(input_mesh)
-        timings["topology_build_seconds"] = time.perf_counter() - topology_start
-        area = surface_area(input_mesh)
         if on_device:
-            pre = _surf2sphere_on_device(input_mesh, topology, area, stop_at, device, areal_arithmetic, timings)
+            # the host plan build (native code, the GIL released) runs beside the surface area,
+            # the upload and the ring tables; topology_build_seconds is its own duration
+            def timed_plan():
+                begin = time.perf_counter()
+                built = Surf2SphereTopology.plan_only(input_mesh)
+                timings["topology_build_seconds"] = time.perf_counter() - begin
+                return built
+
+            with ThreadPoolExecutor(max_workers=1) as pool:
+                future = pool.submit(timed_plan)
+                area = surface_area(input_mesh)
+                pre = _surf2sphere_on_device(input_mesh, future, area, stop_at, device, areal_arithmetic, timings)
             write_start = time.perf_counter()
             write_vertices_like(input_path, output_path, pre)
             timings["output_write_seconds"] = time.perf_counter() - write_start
@@ -686,6 +698,10 @@ def run_cat_surf2sphere_gpu(
             # the file holds exactly these arrays (float32 vertices, the input's faces)
             return CatSurf2SphereGpuResult(np.ascontiguousarray(pre, dtype=np.float32), input_mesh.faces, timings,
                                            output_path)
+        topology_start = time.perf_counter()
+        topology = Surf2SphereTopology.from_mesh(input_mesh)
+        timings["topology_build_seconds"] = time.perf_counter() - topology_start
+        area = surface_area(input_mesh)
         pre, pre_timings = run_surf2sphere_preprocess_cuda(
             input_mesh.vertices, input_mesh.faces, topology, stop_at=min(stop_at, 5), desired_surface_area=area,
             device=device, dtype=dtype, schedule_block_size=preprocess_block_size)
