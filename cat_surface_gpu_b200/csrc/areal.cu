@@ -846,7 +846,8 @@ __global__ void barrier_timeout_selftest_kernel(csg::Control* ctl, unsigned long
 extern "C" {
 
 size_t csg_areal_scratch_bytes(int n_vertices, int arithmetic) {
-    if (n_vertices < 1) return 0;
+    if (n_vertices < 1 || (arithmetic != CSG_ARITH_CAT && arithmetic != CSG_ARITH_FP32 && arithmetic != CSG_ARITH_FP64))
+        return 0;
     // float64: a double4 working copy; float32 modes: four published 8-byte
     // words per vertex (the dataflow form; the barrier form uses the first half)
     return sizeof(csg::Control) + align256(32 * static_cast<size_t>(n_vertices));

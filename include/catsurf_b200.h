@@ -134,6 +134,7 @@ CSG_API int csg_areal_plan_build(int n_vertices, const int32_t *faces, int n_fac
  * lanes_per_vertex of 0 pick defaults; timeout_s bounds every device wait.
  * The kernel's status lands in scratch; read it with csg_read_status.
  * ---------------------------------------------------------------------- */
+/* Scratch bytes for csg_areal_sweeps; 0 for n_vertices < 1 or an unknown arithmetic. */
 CSG_API size_t csg_areal_scratch_bytes(int n_vertices, int arithmetic);
 
 CSG_API int csg_areal_sweeps(void *points, int n_vertices, const int32_t *slot_off, const int32_t *slot_tri,
