@@ -257,7 +257,7 @@ CSG_API int csg_depth_potential(const float *geometry, int batch, int n, const i
 
 /* Data term E_b(v) = 1/2 sum_x (S_b(exp(v_b)(x)) - T_b(x))^2, exp(v) by k
  * scaling-and-squaring compositions (expdef's maps), and its exact adjoint
- * (no reference counterpart: the north-star's hand-written DARTEL adjoint;
+ * (no reference counterpart: a hand-written adjoint of DARTEL's data term;
  * the reference's Gauss-Newton gradient of the same term is
  * initialise_objfun + squaring_update, dartel_grid.py:723-914).
  * Checkpoints: the forward keeps phi_0, phi_c, phi_2c, ... (c =
