@@ -74,7 +74,7 @@ DARTEL_STEPS = (CHAIN["runs"] + int(CHAIN["avg"])) * CHAIN["steps"] * CHAIN["loo
 FEATURE_SIDES = 2 + 2 * (CHAIN["runs"] + int(CHAIN["avg"]))
 
 
-def parse_args():
+def parse_args(argv: list[str] | None = None):
     parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=5)
@@ -89,7 +89,7 @@ def parse_args():
     parser.add_argument("--case", choices=("sweeps", "preprocess", "dartel", "rotation"),
                         help="for kernel profilers: run one small case of one kernel family three times "
                              "(the third run is the one to capture) and exit")
-    return parser.parse_args()
+    return parser.parse_args(argv)
 
 
 def run_case(name: str) -> int:
@@ -166,6 +166,19 @@ def run_case(name: str) -> int:
 
 def dist_env():
     return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def job_seconds_per_unit(local_total_ms: float, units_per_rank: int, world: int, device) -> float:
+    """Seconds per unit for the whole job: the slowest rank's timed total (max over ranks)
+    divided by the units every rank processed (replicas: each rank runs its own units)."""
+
+    import torch
+    import torch.distributed as dist
+
+    total = torch.tensor([float(local_total_ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+    return float(total.item()) / 1e3 / (units_per_rank * world)
 
 
 class ClockSampler:
@@ -644,11 +657,8 @@ def run_native(args):
         if world > 1:
             dist.destroy_process_group()
         return 0
-    total_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device=device)
-    if world > 1:
-        dist.all_reduce(total_ms, op=dist.ReduceOp.MAX)
-    total_s = float(total_ms.item()) / 1e3
-    value = total_s / (args.steps * world)
+    value = job_seconds_per_unit(sum(step_ms), args.steps, world, device)
+    total_s = value * args.steps * world
 
     # parity (untimed): the chain against the reference's CPU chain (float64 DARTEL, like the timed chain),
     # the sweeps against the upstream binary, and a float32-DARTEL chain against the float64 one
@@ -673,10 +683,7 @@ def run_native(args):
             for _ in range(2):  # warm-up: the host paths and the first page-locked allocations
                 hemisphere_e2e(meshes, device, torch.float64, work)
             runs = [hemisphere_e2e(meshes, device, torch.float64, work) for _ in range(3)]
-        e2e_total = torch.tensor([sum(r[0] for r in runs)], dtype=torch.float64, device=device)
-        if world > 1:
-            dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
-        e2e = {"value": float(e2e_total.item()) / (len(runs) * world), "unit": UNIT,
+        e2e = {"value": job_seconds_per_unit(1e3 * sum(r[0] for r in runs), len(runs), world, device), "unit": UNIT,
                "h2d_bytes_per_step": runs[0][1], "d2h_bytes_per_step": runs[0][2],
                "split_s": {k: sum(r[3].get(k, 0.0) for r in runs) / len(runs) for k in runs[0][3]}}
 

@@ -1,0 +1,73 @@
+"""The bench's replica timing across ranks, on the CPU with two gloo ranks.
+
+Each rank of ``bench.py --gpus N`` runs its own hemispheres (replicas; the path
+has no exchange step).  The job's figure is the slowest rank's timed total over
+the hemispheres all ranks processed, the same on every rank; the reference arm
+runs on rank 0 alone.
+"""
+
+from __future__ import annotations
+
+import os
+import socket
+import sys
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from conftest import ROOT
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int, results) -> None:
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        assert bench.dist_env() == (world, rank, rank)
+        local_ms = [1200.0, 1500.0][rank]  # rank 1 is the slower replica
+        steps = 5
+        value = bench.job_seconds_per_unit(local_ms, steps, world, torch.device("cpu"))
+        results[rank] = value
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_two_gloo_ranks_agree_on_the_slowest_replica():
+    world = 2
+    manager = mp.Manager()
+    results = manager.dict()
+    mp.spawn(_rank_main, args=(world, _free_port(), results), nprocs=world, join=True)
+    expected = 1500.0 / 1e3 / (5 * world)  # max over ranks / hemispheres of the whole job
+    assert results[0] == pytest.approx(expected, rel=0, abs=1e-15)
+    assert results[1] == results[0]
+
+
+def test_single_process_needs_no_process_group():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    assert bench.job_seconds_per_unit(2000.0, 4, 1, torch.device("cpu")) == pytest.approx(0.5)
+
+
+def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("LOCAL_RANK", "1")
+    args = bench.parse_args(["--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"])
+    assert bench.run_reference(args) == 0  # returns before any work
+    assert capsys.readouterr().out == ""
