@@ -28,6 +28,15 @@ def _shared_faces(faces) -> bool:
         and faces.flags.c_contiguous
 
 
+def _stable_order(keys: np.ndarray, n_keys: int) -> np.ndarray:
+    """``np.argsort(keys, kind="stable")`` for keys in [0, n_keys): with 16-bit keys numpy's
+    stable sort is a radix sort, several times faster on meshes of up to 65,536 vertices."""
+
+    if n_keys <= 1 << 16:
+        return np.argsort(keys.astype(np.uint16), kind="stable")
+    return np.argsort(keys, kind="stable")
+
+
 def _topology(faces: np.ndarray, n_points: int, device: torch.device):
     ident = (id(faces), n_points, device.type, device.index) if _shared_faces(faces) else None
     if ident is not None:
@@ -52,7 +61,7 @@ def _topology(faces: np.ndarray, n_points: int, device: torch.device):
     vertex = f.T.reshape(-1)
     corner = np.repeat(np.arange(3, dtype=np.int32), f.shape[0])
     face = np.tile(np.arange(f.shape[0], dtype=np.int32), 3)
-    order = np.argsort(vertex, kind="stable")
+    order = _stable_order(vertex, n_points)
     inc = ((face[order] << 2) | corner[order]).astype(np.int32)
     inc_off = np.concatenate(([0], np.cumsum(np.bincount(vertex, minlength=n_points)))).astype(np.int32)
     tensors = tuple(torch.from_numpy(a).to(device) for a in (off, nbr, inc_off, inc))

@@ -190,3 +190,14 @@ def test_cli_dispatch_and_pipeline_argument_checks(tmp_path):
     for backend in ("cuda-official-geometry", "cuda-official-depth"):
         with pytest.raises(ValueError):
             run_cat_surface_gpu_pipeline(*paths[:5], rotation_values_path=paths[0], rotation_feature_backend=backend)
+
+
+def test_stable_order_equals_numpy_stable_argsort():
+    """The incidence tables' vertex order: 16-bit keys (a radix sort) where they fit, int32 beyond."""
+
+    from cat_surface_gpu_b200.features import _stable_order
+
+    rng = np.random.default_rng(4)
+    for n in (3, 1000, 1 << 16, (1 << 16) + 1, 200_000):
+        keys = rng.integers(0, n, 50_000).astype(np.int32)
+        np.testing.assert_array_equal(_stable_order(keys, n), np.argsort(keys, kind="stable"))
