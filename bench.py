@@ -336,6 +336,15 @@ CPU_SAMPLE = ("stages 1-5 in full and 200 of 4,999 sweeps (C port, 1 thread); 2 
               "count; each scaled linearly")
 
 
+def workload_config(meshes) -> dict:
+    """The keys that describe the benchmarked workload; both arms report them unchanged."""
+
+    return {"workload": WORKLOAD, "n_vertices": int(meshes["prefix"].shape[0]),
+            "n_faces": int(meshes["faces"].shape[0]), "sweeps": SWEEPS, "project_every": 1000,
+            "sheet": list(SHEET), "dartel_dtype": "float64",
+            "surfwarp": {k: v for k, v in CHAIN.items() if k != "sheet_size"}}
+
+
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -349,7 +358,7 @@ def run_reference(args):
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sweeps": SWEEPS, "sheet": list(SHEET)},
+        "config": {**workload_config(meshes), "parallelism": "one host thread (scalar port)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": CPU_SAMPLE,
                          "stages_s": {k: v for k, v in samples[-1].items() if k != "total"}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -719,10 +728,9 @@ def run_native(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_vertices": n, "n_faces": f, "sweeps": SWEEPS, "project_every": 1000,
+            "config": {**workload_config(meshes),
                        "levels": hemi.plan.n_levels, "wavefront_stride": hemi.plan.level_stride,
-                       "wavefront_steps": wavefront_steps, "sheet": list(SHEET), "dartel_dtype": "float64",
-                       "surfwarp": {k: v for k, v in CHAIN.items() if k != "sheet_size"},
+                       "wavefront_steps": wavefront_steps,
                        "sweep_launch": hemi.launch,
                        "l2": "flushed before every timed step by a 256 MiB device write",
                        "python_gc": "collected and frozen after the warm-up (gc.freeze)",

@@ -71,3 +71,32 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     args = bench.parse_args(["--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"])
     assert bench.run_reference(args) == 0  # returns before any work
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_line_follows_the_bench_contract(monkeypatch, capsys):
+    """The reference arm's JSON line: the native arm's metric, unit, direction and workload
+    config, a cpu_baseline describing the run, and an e2e entry with no device copies."""
+
+    import json
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    for name in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
+        monkeypatch.delenv(name, raising=False)
+    sample = {"total": 140.0, "stages_1_5": 1.5, "sweeps": 15.0}
+    monkeypatch.setattr(bench, "cpu_hemisphere_sample", lambda meshes: dict(sample))
+    args = bench.parse_args(["--impl", "reference", "--steps", "2", "--warmup", "1"])
+    assert bench.run_reference(args) == 0
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert (line["metric"], line["unit"], line["higher_is_better"]) == (bench.METRIC, bench.UNIT, False)
+    assert line["value"] == pytest.approx(140.0) and line["steps"] == 2 and line["warmup"] == 1
+    config = dict(line["config"])
+    assert config.pop("parallelism")
+    assert config == json.loads(json.dumps(bench.workload_config(bench.load_meshes())))
+    baseline = line["cpu_baseline"]
+    assert baseline["value"] == line["value"] and baseline["kind"] == "port" and baseline["cores"] == 1
+    assert baseline["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
