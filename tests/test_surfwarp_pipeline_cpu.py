@@ -201,3 +201,31 @@ def test_stable_order_equals_numpy_stable_argsort():
     for n in (3, 1000, 1 << 16, (1 << 16) + 1, 200_000):
         keys = rng.integers(0, n, 50_000).astype(np.int32)
         np.testing.assert_array_equal(_stable_order(keys, n), np.argsort(keys, kind="stable"))
+
+
+@pytest.mark.parametrize("thread_count", [0, -1, 257])
+def test_stencil_thread_count_rejects_invalid_values(thread_count, tmp_path):
+    """Reference test_gpu_pipeline.py:11-22: the check runs before any file is read."""
+
+    from cat_surface_gpu_b200.gpu_pipeline import run_cat_surface_gpu_pipeline
+
+    paths = [tmp_path / name for name in ("s.white.gii", "s.sphere.gii", "t.white.gii", "t.sphere.gii", "o.gii")]
+    with pytest.raises(ValueError, match="stencil_threads"):
+        run_cat_surface_gpu_pipeline(*paths, stencil_threads=thread_count)
+
+
+def test_synthetic_meshes_are_deterministic(tmp_path):
+    """The seeded synthetic meshes written as GIFTI twice give the same arrays."""
+
+    from cat_surface_gpu_b200 import synthetic
+    from cat_surface_gpu_b200.gifti import GiftiMesh, read_gifti_mesh, write_gifti_mesh
+
+    for seed in (1, 2):
+        first = synthetic.folded_icosphere(2, seed=seed)
+        second = synthetic.folded_icosphere(2, seed=seed)
+        write_gifti_mesh(tmp_path / f"a{seed}.gii", GiftiMesh(*first))
+        write_gifti_mesh(tmp_path / f"b{seed}.gii", GiftiMesh(*second))
+        a, b = read_gifti_mesh(tmp_path / f"a{seed}.gii"), read_gifti_mesh(tmp_path / f"b{seed}.gii")
+        np.testing.assert_array_equal(a.vertices, b.vertices)
+        np.testing.assert_array_equal(a.faces, b.faces)
+        assert a.faces.shape[1] == 3 and a.vertices.shape[1] == 3
