@@ -187,13 +187,42 @@ def ptr(tensor) -> int:
     return int(tensor.ctypes.data)
 
 
-def stream_handle(stream=None) -> int:
-    """cudaStream_t of the given (or current) torch CUDA stream."""
+def require_current_device(*operands) -> None:
+    """Raise ``ValueError`` unless every operand (tensor or device) is on the current CUDA device.
+
+    The native entry points launch on the CUDA runtime's current device, so a
+    device pointer from another GPU would be read through the wrong context.
+    """
 
     import torch
 
+    current = torch.cuda.current_device()
+    for operand in operands:
+        device = operand if isinstance(operand, torch.device) else getattr(operand, "device", None)
+        if device is None:
+            continue
+        if device.type != "cuda":
+            raise ValueError(f"native operands must be CUDA tensors, got one on {device}")
+        if device.index is not None and device.index != current:
+            raise ValueError(f"operand on cuda:{device.index} but the current device is cuda:{current}; "
+                             f"call under torch.cuda.device(cuda:{device.index})")
+
+
+def stream_handle(stream=None, *, like=None) -> int:
+    """cudaStream_t of the given (or the current device's current) torch CUDA stream.
+
+    ``like`` (a tensor, device or sequence of them) must be on the current
+    device; the stream must belong to it too.
+    """
+
+    import torch
+
+    if like is not None:
+        require_current_device(*(like if isinstance(like, (tuple, list)) else (like,)))
     if stream is None:
         stream = torch.cuda.current_stream()
+    else:
+        require_current_device(stream.device)
     return int(stream.cuda_stream)
 
 

@@ -14,7 +14,6 @@ import argparse
 import hashlib
 import json
 from pathlib import Path
-import shutil
 import sys
 import time
 
@@ -27,38 +26,37 @@ def _synchronize(device: torch.device) -> None:
         torch.cuda.synchronize(device)
 
 
-def _binary(name: str, explicit) -> str:
-    if explicit:
-        return str(explicit)
-    found = shutil.which(name)
-    if found is None:
-        raise SystemExit(f"{name} was not given and is not on PATH")
-    return found
-
-
 def surf2sphere_main(argv: list[str] | None = None) -> int:
-    """Upstream stages 1-5 on the CPU binary, all area-smoothing sweeps on the GPU (reference 35-94)."""
+    """Stages 1-5, the area-smoothing sweeps and the ellipsoid steps on the GPU (reference 35-94).
+
+    The reference's options are all parsed.  ``--preprocess-kernel cpu`` (the
+    reference ran stages 1-5 on its CPU binary) is rejected with a usage
+    error; ``--reference-cli`` is accepted and not used.
+    """
 
     from .surf2sphere import run_cat_surf2sphere_gpu
 
     parser = argparse.ArgumentParser(description="Run strict CAT_Surf2Sphere area smoothing on CUDA.")
-    parser.add_argument("--reference-cli", type=Path, help="CPU reference executable (default: CAT_Surf2Sphere on PATH)")
+    parser.add_argument("--reference-cli", type=Path,
+                        help="accepted for compatibility; not used (no CPU stage is run)")
     parser.add_argument("--input-surface", type=Path, required=True)
     parser.add_argument("--output-surface", type=Path, required=True)
     parser.add_argument("--stop-at", type=int, default=10)
     parser.add_argument("--device", default="cuda")
     parser.add_argument("--dtype", choices=("float32", "float64"), default="float32")
     parser.add_argument("--kernel", choices=("torch", "triton"), default="triton")
-    parser.add_argument("--preprocess-kernel", choices=("cpu", "triton"), default="cpu")
+    parser.add_argument("--preprocess-kernel", choices=("cpu", "triton"), default="triton",
+                        help="triton (default): stages 1-5 on the GPU; cpu is not supported")
     parser.add_argument("--preprocess-block-size", type=int, default=131072)
     parser.add_argument("--areal-block-size", type=int)
     parser.add_argument("--areal-schedule", choices=("ordered", "color"), default="ordered")
     parser.add_argument("--areal-arithmetic", choices=("cat", "fp32"), default="cat")
     args = parser.parse_args(argv)
-    reference_cli = (_binary("CAT_Surf2Sphere", args.reference_cli) if args.preprocess_kernel == "cpu"
-                     else args.reference_cli)
+    if args.preprocess_kernel == "cpu":
+        parser.error("--preprocess-kernel cpu ran stages 1-5 on the upstream CPU binary; this package runs them on "
+                     "the GPU (--preprocess-kernel triton, the default)")
     result = run_cat_surf2sphere_gpu(
-        args.input_surface, args.output_surface, reference_cli=reference_cli, stop_at=args.stop_at,
+        args.input_surface, args.output_surface, stop_at=args.stop_at,
         device=args.device, dtype=args.dtype, kernel=args.kernel, preprocess_kernel=args.preprocess_kernel,
         preprocess_block_size=args.preprocess_block_size, areal_schedule=args.areal_schedule,
         areal_arithmetic=args.areal_arithmetic, areal_block_size=args.areal_block_size,
@@ -66,7 +64,7 @@ def surf2sphere_main(argv: list[str] | None = None) -> int:
     print(json.dumps({
         "backend": f"surf2sphere_pre_{args.preprocess_kernel}_{args.areal_schedule}_wavefront_sm100a",
         "device": args.device, "dtype": args.dtype, "areal_arithmetic": args.areal_arithmetic,
-        "stop_at": args.stop_at, "reference_cli": str(reference_cli), "output_surface": str(result.output_path),
+        "stop_at": args.stop_at, "output_surface": str(result.output_path),
         "timings": result.timings,
     }, ensure_ascii=False, indent=2))
     return 0
@@ -94,7 +92,7 @@ def surfwarp_main(argv: list[str] | None = None) -> int:
                                  "official-cpu"))
     parser.add_argument("--rotation-feature-solver", choices=("colored-sor", "pcg"), default="colored-sor")
     parser.add_argument("--stencil-builder", default="native",
-                        help="'native' (default) or the path of the reference's stencil helper")
+                        help="'native' (default, the GPU builder); a path to the reference's helper is rejected")
     parser.add_argument("--rotated-stencil-builder")
     parser.add_argument("--stencil-threads", type=int, default=8)
     parser.add_argument("--sheet-size", type=int, nargs=2, default=(512, 256), metavar=("NX", "NY"))

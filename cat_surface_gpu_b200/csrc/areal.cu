@@ -376,7 +376,11 @@ __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
         for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
             const int v = __ldg(p.order + c + i * nc);
             const int s0 = __ldg(p.slot_off + v);
-            const int d = __ldg(p.slot_off + v + 1) - s0;
+            int d = __ldg(p.slot_off + v + 1) - s0;
+            if (d < 0 || d > p.max_degree) {  // plan and max_degree disagree: report, stay inside the image
+                if (atomicCAS(&p.ctl->status, CSG_OK, CSG_ERR_ARG) == CSG_OK) p.ctl->where = -3;
+                d = 0;
+            }
             lvid[i] = v;
             ldeg[i] = d;
             for (int j = 0; j < d; ++j) ltri[i * p.max_degree + j] = __ldg(p.slot_tri + s0 + j);
@@ -389,6 +393,7 @@ __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
     }
     for (int v = tid; v < p.n; v += nthreads) T::pack(p.points, p.work, v);
     if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    if (SMEM && csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) return;  // a degree over max_degree: every CTA sees it
 
     const int last = p.iterations - 1;
     for (int start = 1; start <= last;) {
@@ -660,7 +665,11 @@ __global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
     for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
         const int v = __ldg(p.order + c + i * nc);
         const int s0 = __ldg(p.slot_off + v);
-        const int d = __ldg(p.slot_off + v + 1) - s0;
+        int d = __ldg(p.slot_off + v + 1) - s0;
+        if (d < 0 || d > p.max_degree) {  // plan and max_degree disagree: report, stay inside the image
+            if (atomicCAS(&p.ctl->status, CSG_OK, CSG_ERR_ARG) == CSG_OK) p.ctl->where = -3;
+            d = 0;
+        }
         int* ring = lring + i * kRingMax;
         int nr = 1;
         ring[0] = v;
@@ -699,7 +708,8 @@ __global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
         for (int k = 0; k < 3; ++k) st_word(pub + 4LL * v + k, make_word(q[k], 0u));
     }
     if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
-    if (csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) return;  // a ring overflow: same answer in every CTA
+    // a ring overflow or a degree over max_degree: the same answer in every CTA
+    if (csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) return;
 
     const int last = p.iterations - 1;
     for (int start = 1; start <= last;) {
@@ -858,7 +868,7 @@ int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, cons
                      int level_stride, int max_degree, int iterations, int project_every, double radius, int arithmetic, void* scratch,
                      size_t scratch_bytes, int n_ctas, int threads_per_cta, int lanes_per_vertex, double timeout_s,
                      csg_stream_t stream) {
-    if (!points || n_vertices < 1 || !slot_off || !order || !level_begin || !level_end || !scratch)
+    if (!points || n_vertices < 1 || !slot_off || !slot_tri || !order || !level_begin || !level_end || !scratch)
         return csg::fail(CSG_ERR_ARG, "areal sweeps: null pointer or empty mesh");
     if (n_levels < 1 || n_levels > n_vertices || level_stride < 1 || iterations < 1 || project_every < 0 ||
         max_degree < 0)
@@ -970,7 +980,10 @@ constexpr int kNoAllocMaxDevices = 64;
 void* g_noalloc_address[kNoAllocMaxDevices] = {};
 
 // Device address of g_areal_noalloc_scratch on the current device, looked up
-// once per device (the name itself is only a host-side stand-in).
+// once per device (the name itself is only a host-side stand-in).  The cached
+// address belongs to the device's primary context: after cudaDeviceReset the
+// module may load elsewhere, so this entry point must not be used across a
+// device reset.
 int noalloc_scratch(void** out) {
     int device = 0;
     CSG_CUDA_CHECK(cudaGetDevice(&device));
@@ -997,7 +1010,7 @@ extern "C" int csg_areal_sweeps_noalloc(void* points, int n_vertices, const int3
                                         int project_every, double radius, int arithmetic, int n_ctas,
                                         int threads_per_cta, int lanes_per_vertex, double timeout_s,
                                         int* status_out, csg_stream_t stream) {
-    if (!points || n_vertices < 1 || !slot_off || !order || !level_begin || !level_end)
+    if (!points || n_vertices < 1 || !slot_off || !slot_tri || !order || !level_begin || !level_end)
         return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): null pointer or empty mesh");
     if (arithmetic < CSG_ARITH_CAT || arithmetic > CSG_ARITH_FP64)
         return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): unknown arithmetic %d", arithmetic);
@@ -1026,10 +1039,18 @@ extern "C" int csg_areal_sweeps_noalloc(void* points, int n_vertices, const int3
     if (threads_per_cta % 32 != 0 || threads_per_cta > 512)
         return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): threads_per_cta must be a multiple of 32 up to 512");
     if (timeout_s <= 0.0) timeout_s = 2.0;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (status_out != nullptr) {
+        // reading the status back waits for the kernel, which a stream being captured cannot do
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        CSG_CUDA_CHECK(cudaStreamIsCapturing(s, &capture));
+        if (capture != cudaStreamCaptureStatusNone)
+            return csg::fail(CSG_ERR_ARG, "areal sweeps (no-alloc): status_out must be NULL while the stream is "
+                                          "being captured");
+    }
     void* scratch = nullptr;
     int rc = noalloc_scratch(&scratch);
     if (rc) return rc;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     ArealParams p{};
     p.points = points;
     p.ctl = static_cast<csg::Control*>(scratch);

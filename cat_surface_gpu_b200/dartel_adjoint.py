@@ -67,13 +67,14 @@ class DartelDataTerm(torch.autograd.Function):
         count = int(lib.csg_dartel_data_checkpoints(int(k), int(checkpoint_every)))
         if count < 1:
             raise ValueError("k must be 0..30 and checkpoint_every >= 1")
-        checkpoints = torch.empty((count, batch, 2, ny, nx), dtype=v.dtype, device=v.device)
-        objective = torch.empty(batch, dtype=v.dtype, device=v.device)
-        scratch = _scratch(v.dtype, v.device, batch, nx, ny, int(k), int(checkpoint_every))
-        _native.check(lib.csg_dartel_data_forward(
-            _dtype_code(v.dtype), batch, nx, ny, v.data_ptr(), s.data_ptr(), t.data_ptr(), int(k),
-            int(checkpoint_every), checkpoints.data_ptr(), objective.data_ptr(), scratch.data_ptr(), scratch.numel(),
-            _native.stream_handle()), "csg_dartel_data_forward")
+        with torch.cuda.device(v.device):  # the native launch uses the current device
+            checkpoints = torch.empty((count, batch, 2, ny, nx), dtype=v.dtype, device=v.device)
+            objective = torch.empty(batch, dtype=v.dtype, device=v.device)
+            scratch = _scratch(v.dtype, v.device, batch, nx, ny, int(k), int(checkpoint_every))
+            _native.check(lib.csg_dartel_data_forward(
+                _dtype_code(v.dtype), batch, nx, ny, v.data_ptr(), s.data_ptr(), t.data_ptr(), int(k),
+                int(checkpoint_every), checkpoints.data_ptr(), objective.data_ptr(), scratch.data_ptr(),
+                scratch.numel(), _native.stream_handle(like=v)), "csg_dartel_data_forward")
         ctx.save_for_backward(checkpoints, s, t)
         ctx.k, ctx.every, ctx.squeeze = int(k), int(checkpoint_every), velocity.ndim == 3
         return objective if velocity.ndim == 4 else objective[0]
@@ -82,13 +83,14 @@ class DartelDataTerm(torch.autograd.Function):
     def backward(ctx, grad_objective):
         checkpoints, s, t = ctx.saved_tensors
         batch, ny, nx = (int(x) for x in s.shape)
-        scale = grad_objective.reshape(-1).to(s.dtype).contiguous()
-        grad = torch.empty((batch, 2, ny, nx), dtype=s.dtype, device=s.device)
-        scratch = _scratch(s.dtype, s.device, batch, nx, ny, ctx.k, ctx.every)
-        _native.check(_native.library().csg_dartel_data_backward(
-            _dtype_code(s.dtype), batch, nx, ny, s.data_ptr(), t.data_ptr(), ctx.k, ctx.every,
-            checkpoints.data_ptr(), scale.data_ptr(), grad.data_ptr(), scratch.data_ptr(), scratch.numel(),
-            _native.stream_handle()), "csg_dartel_data_backward")
+        with torch.cuda.device(s.device):  # the native launch uses the current device
+            scale = grad_objective.reshape(-1).to(device=s.device, dtype=s.dtype).contiguous()
+            grad = torch.empty((batch, 2, ny, nx), dtype=s.dtype, device=s.device)
+            scratch = _scratch(s.dtype, s.device, batch, nx, ny, ctx.k, ctx.every)
+            _native.check(_native.library().csg_dartel_data_backward(
+                _dtype_code(s.dtype), batch, nx, ny, s.data_ptr(), t.data_ptr(), ctx.k, ctx.every,
+                checkpoints.data_ptr(), scale.data_ptr(), grad.data_ptr(), scratch.data_ptr(), scratch.numel(),
+                _native.stream_handle(like=s)), "csg_dartel_data_backward")
         return (grad[0] if ctx.squeeze else grad), None, None, None, None
 
 

@@ -90,8 +90,10 @@ def _grid(value, spec: GridSpec, device, dtype, name: str, channels: int = 2) ->
     return tensor
 
 
-def _stream() -> int:
-    return _native.stream_handle()
+def _stream(operand: torch.Tensor) -> int:
+    """The current stream, after checking that ``operand`` lives on the current device."""
+
+    return _native.stream_handle(like=operand)
 
 
 def _call(name: str, *args) -> None:
@@ -150,7 +152,7 @@ def composition(a, b, *, device="auto", dtype=torch.float64, optimized: bool = T
     bt = _grid(b, spec, target, dtype, "B")
     out = torch.empty_like(at)
     _call("csg_dartel_compose", _dtype_code(dtype), 1, spec.nx, spec.ny, at.data_ptr(), None, bt.data_ptr(), None,
-          out.data_ptr(), None, _stream())
+          out.data_ptr(), None, _stream(out))
     return out
 
 
@@ -166,7 +168,7 @@ def composition_jacobian(a, ja, b, jb, *, device="auto", dtype=torch.float64, op
     out = torch.empty_like(at)
     jout = torch.empty_like(jat)
     _call("csg_dartel_compose", _dtype_code(dtype), 1, spec.nx, spec.ny, at.data_ptr(), jat.data_ptr(), bt.data_ptr(),
-          jbt.data_ptr(), out.data_ptr(), jout.data_ptr(), _stream())
+          jbt.data_ptr(), out.data_ptr(), jout.data_ptr(), _stream(jout))
     return out, jout
 
 
@@ -178,7 +180,7 @@ def jacobian_of_displacement(displacement, scale: float = 1.0, *, device="auto",
     v = _grid(displacement, spec, target, dtype, "displacement")
     jac = torch.empty((4, spec.ny, spec.nx), dtype=dtype, device=target)
     _call("csg_dartel_smalldef", _dtype_code(dtype), 1, spec.nx, spec.ny, v.data_ptr(), float(scale), None,
-          jac.data_ptr(), _stream())
+          jac.data_ptr(), _stream(jac))
     return jac
 
 
@@ -191,7 +193,7 @@ def smalldef_jac(displacement, scale: float, *, device="auto", dtype=torch.float
     out = torch.empty_like(v)
     jac = torch.empty((4, spec.ny, spec.nx), dtype=dtype, device=target)
     _call("csg_dartel_smalldef", _dtype_code(dtype), 1, spec.nx, spec.ny, v.data_ptr(), float(scale), out.data_ptr(),
-          jac.data_ptr(), _stream())
+          jac.data_ptr(), _stream(jac))
     return out, jac
 
 
@@ -204,7 +206,7 @@ def jac_div_smalldef(jacobian, displacement, scale: float, *, device="auto", dty
     jac = _grid(jacobian, spec, target, dtype, "jacobian", 4)
     out = torch.empty_like(jac)
     _call("csg_dartel_jac_div", _dtype_code(dtype), 1, spec.nx, spec.ny, jac.data_ptr(), v.data_ptr(), float(scale),
-          out.data_ptr(), _stream())
+          out.data_ptr(), _stream(out))
     return out
 
 
@@ -236,7 +238,7 @@ def initialise_objfun(source, target, transformation, jacobian, distortion=None,
     scratch = _scratch(dtype, dev, 1, spec.nx, spec.ny)
     _call("csg_dartel_objfun", _dtype_code(dtype), 1, spec.nx, spec.ny, src.data_ptr(), tgt.data_ptr(),
           tmap.data_ptr(), jac.data_ptr(), None if weights is None else weights.data_ptr(), rhs.data_ptr(),
-          hess.data_ptr(), objective.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream())
+          hess.data_ptr(), objective.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream(scratch))
     return objective[0], rhs, hess
 
 
@@ -262,7 +264,7 @@ def squaring_update(right_hand, hessian, transformation, jacobian, k: int, *, sa
     scratch = _scratch(dtype, dev, 1, spec.nx, spec.ny)
     _call("csg_dartel_squaring", _dtype_code(dtype), 1, spec.nx, spec.ny, rhs.data_ptr(), hess.data_ptr(),
           tmap.data_ptr(), jac.data_ptr(), int(k), int(bool(save_transformation)), b_out.data_ptr(), a_out.data_ptr(),
-          m_out.data_ptr(), j_out.data_ptr(), s_out.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream())
+          m_out.data_ptr(), j_out.data_ptr(), s_out.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream(scratch))
     result = (b_out, a_out, m_out, j_out)
     return result + (s_out,) if return_scratch else result
 
@@ -280,7 +282,7 @@ def regularization_operator(field, params: Sequence[float], rtype: int = 1, *, d
     out = torch.empty_like(v)
     p = _params(params)
     _call("csg_dartel_regularization", _dtype_code(dtype), 1, spec.nx, spec.ny, v.data_ptr(), _addr(p), int(rtype),
-          out.data_ptr(), _stream())
+          out.data_ptr(), _stream(out))
     return out
 
 
@@ -300,7 +302,7 @@ def apply_membrane_system(hessian, field, params: Sequence[float], *, kernel: st
     out = torch.empty_like(v)
     p = _params(params)
     _call("csg_dartel_membrane_apply", _dtype_code(dtype), 1, spec.nx, spec.ny, hess.data_ptr(), v.data_ptr(),
-          _addr(p), out.data_ptr(), _stream())
+          _addr(p), out.data_ptr(), _stream(out))
     return out
 
 
@@ -331,7 +333,7 @@ def relax_membrane(hessian, right_hand, params: Sequence[float], nit: int, initi
     u = torch.zeros_like(b) if initial is None else _grid(initial, spec, dev, dtype, "initial").clone()
     p = _params(params)
     _call("csg_dartel_relax", _dtype_code(dtype), 1, spec.nx, spec.ny, hess.data_ptr(), b.data_ptr(), _addr(p),
-          int(nit), u.data_ptr(), _stream())
+          int(nit), u.data_ptr(), _stream(u))
     return u
 
 
@@ -348,7 +350,7 @@ def resize_field(field, target: GridSpec, *, kernel: str = "auto", device="auto"
         raise ValueError(f"resize_field expects [channel, y, x], got {tuple(value.shape)}")
     out = torch.empty((value.shape[0], target.ny, target.nx), dtype=dtype, device=dev)
     _call("csg_dartel_resize", _dtype_code(dtype), int(value.shape[0]), int(value.shape[2]), int(value.shape[1]),
-          value.data_ptr(), target.nx, target.ny, out.data_ptr(), 0, _stream())
+          value.data_ptr(), target.nx, target.ny, out.data_ptr(), 0, _stream(out))
     return out
 
 
@@ -373,7 +375,7 @@ def fmg2_membrane(hessian, right_hand, params: Sequence[float], cycles: int = 3,
     scratch = _scratch(dtype, dev, 1, spec.nx, spec.ny)
     _call("csg_dartel_fmg", _dtype_code(dtype), 1, spec.nx, spec.ny, hess.data_ptr(), b.data_ptr(), _addr(p),
           int(cycles), int(nit), u.data_ptr(), int(initial is not None), int(bool(assume_initial_nonzero)),
-          scratch.data_ptr(), scratch.numel(), _stream())
+          scratch.data_ptr(), scratch.numel(), _stream(scratch))
     return u
 
 
@@ -414,7 +416,7 @@ def dartel_step(source, target, velocity, *, k: int, rtype: int = 1, params=(1.0
     scratch = _scratch(dtype, dev, 1, spec.nx, spec.ny)
     _call("csg_dartel_step", _dtype_code(dtype), 1, spec.nx, spec.ny, src.data_ptr(), tgt.data_ptr(), v.data_ptr(),
           metrics.data_ptr(), int(k), _addr(p), float(lmreg), int(cycles), int(nit), int(code),
-          int(bool(assume_initial_nonzero)), scratch.data_ptr(), scratch.numel(), _stream())
+          int(bool(assume_initial_nonzero)), scratch.data_ptr(), scratch.numel(), _stream(scratch))
     return v, metrics
 
 
@@ -431,7 +433,7 @@ def expdef(displacement, k: int, *, return_jacobian: bool = False, device="auto"
     jac = torch.empty((4, spec.ny, spec.nx), dtype=dtype, device=dev) if return_jacobian else None
     scratch = _scratch(dtype, dev, 1, spec.nx, spec.ny)
     _call("csg_dartel_expdef", _dtype_code(dtype), 1, spec.nx, spec.ny, v.data_ptr(), int(k), out.data_ptr(),
-          None if jac is None else jac.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream())
+          None if jac is None else jac.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream(scratch))
     return (out, jac) if return_jacobian else out
 
 
@@ -448,5 +450,5 @@ def sample_field(field, x, y, *, device="auto", dtype=torch.float64) -> torch.Te
         raise ValueError("sample_field x and y coordinates must have the same shape")
     out = torch.empty_like(xt)
     _call("csg_dartel_sample", _dtype_code(dtype), int(f.shape[1]), int(f.shape[0]), f.data_ptr(), xt.numel(),
-          xt.data_ptr(), yt.data_ptr(), out.data_ptr(), _stream())
+          xt.data_ptr(), yt.data_ptr(), out.data_ptr(), _stream(out))
     return out

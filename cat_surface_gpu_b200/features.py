@@ -129,8 +129,10 @@ def upload_stencil(stencil: SurfaceStencil, device: torch.device, geometry_dtype
     return st
 
 
-def _stream() -> int:
-    return _native.stream_handle()
+def _stream(operand: torch.Tensor) -> int:
+    """The current stream, after checking that ``operand`` lives on the current device."""
+
+    return _native.stream_handle(like=operand)
 
 
 def _scratch(st: SurfaceStencilDevice, series: int = 1) -> torch.Tensor:
@@ -156,7 +158,7 @@ def resample_vertices(st: SurfaceStencilDevice, vertices) -> torch.Tensor:
     dtype = _native.CSG_DTYPE_F32 if value.dtype == torch.float32 else _native.CSG_DTYPE_F64
     _native.check(_native.library().csg_feature_resample(dtype, int(out.shape[0]), st.surface_indices.data_ptr(),
                                                          st.surface_weights.data_ptr(), value.data_ptr(),
-                                                         out.data_ptr(), _stream()), "csg_feature_resample")
+                                                         out.data_ptr(), _stream(out)), "csg_feature_resample")
     return out
 
 
@@ -167,7 +169,7 @@ def map_values_to_sheet(st: SurfaceStencilDevice, values) -> torch.Tensor:
     out = torch.empty((st.ny, st.nx), dtype=torch.float64, device=value.device)
     _native.check(_native.library().csg_feature_sheet_map(st.nx * st.ny, st.sheet_indices.data_ptr(),
                                                           st.sheet_weights.data_ptr(), value.data_ptr(),
-                                                          out.data_ptr(), _stream()), "csg_feature_sheet_map")
+                                                          out.data_ptr(), _stream(out)), "csg_feature_sheet_map")
     return out
 
 
@@ -180,7 +182,7 @@ def _edge_mean(st: SurfaceStencilDevice, vertices: torch.Tensor) -> float:
     total = st._cache.setdefault("edge_sum", torch.empty(1, dtype=torch.float64, device=v.device))
     _native.check(_native.library().csg_feature_edge_sum(dtype, int(st.faces.shape[0]), st.faces.data_ptr(), v.data_ptr(),
                                                          total.data_ptr(), scratch.data_ptr(), scratch.numel(),
-                                                         _stream()), "csg_feature_edge_sum")
+                                                         _stream(scratch)), "csg_feature_edge_sum")
     return float(total.item()) / (3.0 * int(st.faces.shape[0]))
 
 
@@ -199,7 +201,7 @@ def edge_means(pairs) -> list[float]:
         total = torch.empty(1, dtype=torch.float64, device=v.device)
         _native.check(_native.library().csg_feature_edge_sum(dtype, int(st.faces.shape[0]), st.faces.data_ptr(),
                                                              v.data_ptr(), total.data_ptr(), scratch.data_ptr(),
-                                                             scratch.numel(), _stream()), "csg_feature_edge_sum")
+                                                             scratch.numel(), _stream(scratch)), "csg_feature_edge_sum")
         totals.append(total)
     if not totals:
         return []
@@ -229,7 +231,7 @@ def smooth_geometry(st: SurfaceStencilDevice, vertices, fwhm: float, edge_mean: 
     scratch = _scratch(st)
     _native.check(_native.library().csg_feature_smooth_geometry(
         int(value.shape[0]), st.neighbour_offsets.data_ptr(), st.neighbour_indices.data_ptr(), value.data_ptr(),
-        iterations, out.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream()), "csg_feature_smooth_geometry")
+        iterations, out.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream(scratch)), "csg_feature_smooth_geometry")
     return out
 
 
@@ -256,7 +258,7 @@ def _smooth_series(st, values, geometry, fwhms, via_norm: bool, edge_mean: float
     _native.check(_native.library().csg_feature_smooth_values(
         n, st.neighbour_offsets.data_ptr(), st.neighbour_indices.data_ptr(), int(st.neighbour_indices.numel()), dtype,
         geom.data_ptr(), base.data_ptr(), len(fwhms), ctypes.addressof(sigmas), ctypes.addressof(counts),
-        int(via_norm), out.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream()), "csg_feature_smooth_values")
+        int(via_norm), out.data_ptr(), scratch.data_ptr(), scratch.numel(), _stream(scratch)), "csg_feature_smooth_values")
     return out
 
 
@@ -289,7 +291,7 @@ def vertex_normals(st: SurfaceStencilDevice, vertices) -> torch.Tensor:
     out = torch.empty_like(geometry)
     _native.check(_native.library().csg_feature_vertex_normals(int(geometry.shape[0]), st.faces.data_ptr(),
                                                                inc_off.data_ptr(), inc.data_ptr(), geometry.data_ptr(),
-                                                               out.data_ptr(), _stream()), "csg_feature_vertex_normals")
+                                                               out.data_ptr(), _stream(out)), "csg_feature_vertex_normals")
     return out
 
 
@@ -300,7 +302,7 @@ def _minmax(st: SurfaceStencilDevice, values: torch.Tensor) -> torch.Tensor:
     out = torch.empty_like(v)
     scratch = _scratch(st, max(1, rows))
     _native.check(_native.library().csg_feature_minmax(n, rows, v.data_ptr(), out.data_ptr(), scratch.data_ptr(),
-                                                       scratch.numel(), _stream()), "csg_feature_minmax")
+                                                       scratch.numel(), _stream(scratch)), "csg_feature_minmax")
     return out
 
 
@@ -310,7 +312,7 @@ def _type5_base(st: SurfaceStencilDevice, geometry: torch.Tensor, edge_mean: flo
     out = torch.empty(int(geometry.shape[0]), dtype=torch.float64, device=geometry.device)
     _native.check(_native.library().csg_feature_normal_displacement(int(geometry.shape[0]), smoothed.data_ptr(),
                                                                     geometry.data_ptr(), normals.data_ptr(),
-                                                                    out.data_ptr(), _stream()),
+                                                                    out.data_ptr(), _stream(out)),
                   "csg_feature_normal_displacement")
     return out
 
@@ -346,7 +348,7 @@ def curvature_type2(st: SurfaceStencilDevice, vertices, fwhm: float) -> torch.Te
     values = torch.empty(int(geometry.shape[0]), dtype=torch.float64, device=geometry.device)
     _native.check(_native.library().csg_feature_curvature2(int(geometry.shape[0]), st.neighbour_offsets.data_ptr(),
                                                            st.neighbour_indices.data_ptr(), geometry.data_ptr(),
-                                                           normals.data_ptr(), values.data_ptr(), _stream()),
+                                                           normals.data_ptr(), values.data_ptr(), _stream(values)),
                   "csg_feature_curvature2")
     values = _smooth_series(st, values, geometry, (float(fwhm),), True)[0]
     return _minmax(st, values)

@@ -6,16 +6,19 @@ spheres, rotation features, 46-seed + Nelder-Mead rotation search, the
 rotated source stencil, ``runs`` DARTEL solves with the final warp applied
 between runs, the ``-avg`` pole-rotated solve and its blend, GIFTI output.
 
-Helpers: every stencil comes from ``stencil_builder`` -- a path to the
-reference's helper binary (as the reference runs it) or ``"native"`` (the
-host builder ``csg_stencil_build``).  Rotation features come from
+Every stencil is built by this package's GPU stencil builder
+(``stencil_builder="native"``).  Rotation features come from
 ``rotation_values_path``; from the depth potential on the GPU (``"cuda"``, the
-reference's default that ``"auto"`` resolves to, or
-``"cuda-official-geometry"`` on the geometry helper's smoothed surfaces --
-``rotation_feature.py``); from the reference's helpers (``official-cpu`` /
-``cuda-official-depth``); or from ``"native-curvature"`` (an option of this
-package): the type-5 curvature of the resampled surfaces heat-smoothed with
-the rotation FWHMs (15 source, 10 target) and min-max normalised.
+reference's default that ``"auto"`` resolves to -- ``rotation_feature.py``);
+or from ``"native-curvature"`` (an option of this package): the type-5
+curvature of the resampled surfaces heat-smoothed with the rotation FWHMs
+(15 source, 10 target) and min-max normalised.
+
+No process is spawned.  The reference's options that ran its helper
+binaries -- a stencil-builder path, the ``official-cpu``,
+``cuda-official-depth`` and ``cuda-official-geometry`` feature backends and
+the ``rotation_*_probe`` executables -- are parsed and rejected with
+``ValueError`` before any file is read.
 """
 
 from __future__ import annotations
@@ -23,10 +26,7 @@ from __future__ import annotations
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 import math
-import os
 from pathlib import Path
-import subprocess
-import tempfile
 import time
 from typing import Sequence
 
@@ -66,14 +66,6 @@ def _resolve_dartel_dtype(value) -> torch.dtype:
     if resolved not in {torch.float32, torch.float64}:
         raise ValueError("dartel_dtype must be torch.float32 or torch.float64")
     return resolved
-
-
-def _run_checked(command: Sequence[str], label: str, environment: dict | None = None) -> None:
-    completed = subprocess.run([str(item) for item in command], check=False, capture_output=True, text=True,
-                               env=environment)
-    if completed.returncode != 0:
-        raise RuntimeError(f"{label} failed with exit code {completed.returncode}\n"
-                           f"stdout:\n{completed.stdout.strip()[-1000:]}\nstderr:\n{completed.stderr.strip()[-2000:]}")
 
 
 def normalise_sphere(vertices: np.ndarray) -> np.ndarray:
@@ -132,28 +124,14 @@ def rotate_vertices(vertices: np.ndarray, angles) -> np.ndarray:
 
 
 class _Stencils:
-    """Builds stencils with the native builder (on the GPU) or a reference helper binary."""
+    """Builds stencils with the native builder on the pipeline's device."""
 
-    def __init__(self, builder, threads: int, nx: int, ny: int, temp_dir: Path, device=None):
-        self.builder, self.threads, self.nx, self.ny, self.temp = builder, threads, nx, ny, temp_dir
-        self.device = device
-        self.count = 0
+    def __init__(self, threads: int, nx: int, ny: int, device=None):
+        self.threads, self.nx, self.ny, self.device = threads, nx, ny, device
 
-    def build(self, sphere: GiftiMesh, surface_path: str | Path, *, normalize: bool,
-              sphere_path: str | Path | None = None) -> SurfaceStencil:
-        if self.builder in (None, "native"):
-            return build_surface_stencil(sphere.vertices, sphere.faces, nx=self.nx, ny=self.ny, normalize=normalize,
-                                         threads=self.threads, device=self.device)
-        self.count += 1
-        path = Path(sphere_path) if sphere_path is not None else self.temp / f"sphere-{self.count}.gii"
-        if sphere_path is None:
-            write_gifti_mesh(path, sphere)
-        output = self.temp / f"stencil-{self.count}.stencil"
-        options = ["--threads", str(self.threads), "--surface", str(surface_path)]
-        if not normalize:
-            options.insert(0, "--no-normalize")
-        _run_checked([self.builder, path, output, *options], "stencil builder")
-        return SurfaceStencil.from_file(output)
+    def build(self, sphere: GiftiMesh, *, normalize: bool) -> SurfaceStencil:
+        return build_surface_stencil(sphere.vertices, sphere.faces, nx=self.nx, ny=self.ny, normalize=normalize,
+                                     threads=self.threads, device=self.device)
 
 
 def native_rotation_features(source_stencil, target_stencil, source_surface, target_surface, device,
@@ -192,62 +170,24 @@ def depth_rotation_features(source_stencil, target_stencil, source_surface, targ
     return results[0].values, results[1].values
 
 
-def _read_rotation_geometry(path) -> np.ndarray:
-    """``[i32 count, f64 xyz * count]`` coarse-feature geometry (reference 232-245)."""
-
-    raw = Path(path).read_bytes()
-    if len(raw) < 4:
-        raise ValueError(f"Coarse feature geometry file is too short: {path}")
-    count = int(np.frombuffer(raw, dtype=np.int32, count=1)[0])
-    if count <= 0 or len(raw) < 4 + 24 * count:
-        raise ValueError(f"Coarse feature geometry file has an invalid length: {path}")
-    return np.ascontiguousarray(np.frombuffer(raw, dtype=np.float64, count=3 * count, offset=4).reshape(count, 3),
-                                dtype=np.float32)
-
-
-def _probe_rotation_geometry(probe, surface_path, sphere_path, fwhm: float, output: Path) -> np.ndarray:
-    """Upstream coarse-feature geometry helper (reference 206-229)."""
-
-    _run_checked([probe, surface_path, sphere_path, str(float(fwhm)), output], "Upstream coarse feature geometry")
-    if not output.is_file() or output.stat().st_size < 4:
-        raise RuntimeError(f"Coarse feature geometry helper did not produce a valid file: {output}")
-    return _read_rotation_geometry(output)
-
-
-def _official_rotation_features(probe, paths, target_stencil, source_stencil, device, temp: Path, raw_depth: bool):
-    output = temp / "rotation-values.bin"
-    environment = None
-    if raw_depth:
-        environment = os.environ.copy()
-        environment["CAT_SURFACE_GPU_ROTATION_RAW_DEPTH"] = "1"
-        environment["CAT_SURFACE_GPU_ROTATION_RAW_DEPTH_GEOMETRY"] = "1"
-    _run_checked([probe, *paths, output], "Rotation feature", environment)
-    source_values, target_values = read_rotation_values(output)
-    if not raw_depth:
-        return source_values, target_values
-    # reference rotation_feature.py:352-404: smooth raw depth on the helper's geometry (FWHM 50), min-max
-    values = []
-    for stencil, raw, side in ((source_stencil, source_values, "source"), (target_stencil, target_values, "target")):
-        raw_geo = Path(f"{output}.{side}.geometry").read_bytes()
-        count = int(np.frombuffer(raw_geo, dtype=np.int32, count=1)[0])
-        geometry = np.frombuffer(raw_geo, dtype=np.float64, count=3 * count, offset=4).reshape(count, 3)
-        geometry = geometry.astype(np.float32)
-        st = stencil.to(device, geometry_dtype=torch.float32)
-        smoothed = st.smooth_values(torch.as_tensor(raw, device=device), torch.as_tensor(geometry, device=device), 50.0)
-        mn, mx = smoothed.amin(), smoothed.amax()
-        values.append(((smoothed - mn) / (mx - mn).clamp_min(torch.finfo(torch.float64).eps)).cpu().numpy())
-    return values[0], values[1]
-
-
-_BACKENDS = {"auto", "native-curvature", "cuda-official-depth", "official-cpu", "cuda", "cuda-official-geometry"}
+_BACKENDS = {"auto", "native-curvature", "cuda"}
+# the reference's feature backends that run its helper binaries (reference 550-560, 836-893)
+_HELPER_BACKENDS = {"official-cpu", "cuda-official-depth", "cuda-official-geometry"}
 _SOLVERS = {"colored-sor", "pcg"}
 
 
 def _validate_options(*, steps=2, runs=1, stencil_threads=8, curvtypes=(5, 5, 2), fwhm=(5.0, 5.0 / 3.0, 5.0 / 9.0),
                       rotation_max_iter=500, rotation_tol=1.0e-4, rotation_simplex_step=0.1,
                       rotation_feature_backend="auto", rotation_feature_solver="colored-sor", has_values=False,
-                      dartel_dtype=torch.float64, device="cuda", **_unused) -> None:
-    """Argument checks of the reference pipeline (reference 514-560), before any file is read."""
+                      dartel_dtype=torch.float64, device="cuda", stencil_builder="native", rotated_stencil_builder=None,
+                      rotation_values_probe=None, rotation_geometry_probe=None, rotation_depth_probe=None,
+                      **_unused) -> None:
+    """Argument checks of the reference pipeline (reference 514-560), before any file is read.
+
+    Options that would run one of the reference's helper binaries raise
+    ``ValueError``: this package computes stencils and rotation features on
+    the GPU and spawns no process.
+    """
 
     if steps < 1 or steps > 3:
         raise ValueError("steps must be between 1 and 3")
@@ -259,12 +199,24 @@ def _validate_options(*, steps=2, runs=1, stencil_threads=8, curvtypes=(5, 5, 2)
         raise ValueError("curvtypes and fwhm must contain at least 'steps' entries")
     if rotation_max_iter < 1 or rotation_tol < 0.0 or rotation_simplex_step <= 0.0:
         raise ValueError("rotation_max_iter, rotation_tol, and rotation_simplex_step must be positive")
+    if rotation_feature_backend in _HELPER_BACKENDS:
+        raise ValueError(f"rotation_feature_backend={rotation_feature_backend!r} runs the reference's helper "
+                         "binaries; this package computes the rotation features on the GPU ('auto' or 'cuda', or "
+                         "'native-curvature')")
     if rotation_feature_backend not in _BACKENDS:
         raise ValueError(f"rotation_feature_backend must be one of {sorted(_BACKENDS)}")
+    for name, builder in (("stencil_builder", stencil_builder), ("rotated_stencil_builder", rotated_stencil_builder)):
+        if builder not in (None, "native"):
+            raise ValueError(f"{name}={builder!r}: the reference's stencil helper binary is not run; stencils are "
+                             "built on the GPU (stencil_builder='native')")
+    for name, probe in (("rotation_values_probe", rotation_values_probe),
+                        ("rotation_geometry_probe", rotation_geometry_probe),
+                        ("rotation_depth_probe", rotation_depth_probe)):
+        if probe is not None:
+            raise ValueError(f"{name}: the reference's feature helper binaries are not run; rotation features are "
+                             "computed on the GPU")
     if rotation_feature_solver not in _SOLVERS:
         raise ValueError("rotation_feature_solver must be 'colored-sor' or 'pcg'")
-    if rotation_feature_backend in {"cuda-official-geometry", "cuda-official-depth"} and has_values:
-        raise ValueError("GPU official hybrid backend cannot rotation_values")
     _resolve_dartel_dtype(dartel_dtype)
     if device == "cpu" or str(device) == "cpu":
         raise ValueError("The explicit GPU pipeline requires a CUDA device")
@@ -323,49 +275,39 @@ def register_meshes(
 ) -> tuple[np.ndarray, np.ndarray, float, dict[str, float]]:
     """In-memory SurfWarp registration: returns (sphere vertices f32, angle, rotation cost, timings).
 
-    Same flow and options as :func:`run_cat_surface_gpu_pipeline`; ``paths``
-    (source surface, source sphere, target surface, target sphere files) are
-    needed only by the helper-binary stencil builders and feature probes.
-    ``sheet_size`` is the DARTEL sheet (nx, ny) of natively built stencils;
-    helper-built stencils carry the helper's fixed 512 x 256.
+    Same flow and options as :func:`run_cat_surface_gpu_pipeline`.  ``paths``
+    (the four input files) is accepted for signature compatibility and not
+    used.  ``sheet_size`` is the DARTEL sheet (nx, ny) of the stencils built
+    here.  Every launch runs with ``device`` as the current CUDA device.
     """
 
     _validate_options(steps=steps, runs=runs, stencil_threads=stencil_threads, curvtypes=curvtypes, fwhm=fwhm,
                       rotation_max_iter=rotation_max_iter, rotation_tol=rotation_tol,
                       rotation_simplex_step=rotation_simplex_step, rotation_feature_backend=rotation_feature_backend,
                       rotation_feature_solver=rotation_feature_solver, has_values=rotation_values is not None,
-                      dartel_dtype=dartel_dtype, device=device)
+                      dartel_dtype=dartel_dtype, device=device, stencil_builder=stencil_builder,
+                      rotated_stencil_builder=rotated_stencil_builder, rotation_values_probe=rotation_values_probe,
+                      rotation_geometry_probe=rotation_geometry_probe, rotation_depth_probe=rotation_depth_probe)
     if rotation_feature_backend == "auto":
-        # the reference's resolution (reference 550-553)
-        rotation_feature_backend = "official-cpu" if rotation_values_probe is not None else "cuda"
-    if rotation_values is None and rotation_feature_backend == "cuda-official-geometry" \
-            and rotation_geometry_probe is None:
-        raise ValueError("cuda-official-geometry requires rotation_geometry_probe")
+        # the reference's resolution without a values probe (reference 550-553)
+        rotation_feature_backend = "cuda"
     solve_dtype = _resolve_dartel_dtype(dartel_dtype)
     target_device = resolve_device(device)
-    if rotated_stencil_builder is None:
-        rotated_stencil_builder = stencil_builder
     graph_requested = bool(cuda_graph and (runs + int(avg) >= 3))
-    uses_files = (stencil_builder not in (None, "native") or rotated_stencil_builder not in (None, "native")
-                  or (rotation_values is None and rotation_feature_backend in {"official-cpu", "cuda-official-depth",
-                                                                                "cuda-official-geometry"}))
-    if uses_files and paths is None:
-        raise ValueError("helper stencil builders and feature probes need the input file paths")
-    source_surface_path, source_sphere_path, target_surface_path, target_sphere_path = paths or (None,) * 4
     timings: dict[str, float] = {}
     total_start = time.perf_counter()
     nx, ny = (int(v) for v in sheet_size)
 
-    with tempfile.TemporaryDirectory(prefix="cat_surface_b200_") as temp_name:
-        temp = Path(temp_name)
-        builder = _Stencils(stencil_builder, stencil_threads, nx, ny, temp, target_device)
-        rotated_builder = _Stencils(rotated_stencil_builder, stencil_threads, nx, ny, temp, target_device)
+    # the native entry points launch on the current device: make it the pipeline's
+    with torch.cuda.device(target_device):
+        builder = _Stencils(stencil_threads, nx, ny, target_device)
+        rotated_builder = builder
         start = time.perf_counter()
         with ThreadPoolExecutor(max_workers=2) as pool:
-            src_future = None if source_stencil is not None else pool.submit(
-                builder.build, source_sphere, source_surface_path, normalize=True, sphere_path=source_sphere_path)
-            tgt_future = None if target_stencil is not None else pool.submit(
-                builder.build, target_sphere, target_surface_path, normalize=True, sphere_path=target_sphere_path)
+            src_future = None if source_stencil is not None else pool.submit(builder.build, source_sphere,
+                                                                             normalize=True)
+            tgt_future = None if target_stencil is not None else pool.submit(builder.build, target_sphere,
+                                                                             normalize=True)
             source_stencil = source_stencil if src_future is None else src_future.result()
             target_stencil = target_stencil if tgt_future is None else tgt_future.result()
         timings["initial_stencil_seconds"] = time.perf_counter() - start
@@ -373,25 +315,6 @@ def register_meshes(
         start = time.perf_counter()
         if rotation_values is not None:
             source_values, target_values = rotation_values
-        elif rotation_feature_backend == "official-cpu":
-            if rotation_values_probe is None:
-                raise ValueError("official-cpu rotation features require rotation_values_probe")
-            source_values, target_values = _official_rotation_features(
-                rotation_values_probe, paths, target_stencil, source_stencil, target_device, temp, raw_depth=False)
-        elif rotation_feature_backend == "cuda-official-depth":
-            if rotation_depth_probe is None:
-                raise ValueError("cuda-official-depth requires rotation_depth_probe")
-            source_values, target_values = _official_rotation_features(
-                rotation_depth_probe, paths, target_stencil, source_stencil, target_device, temp, raw_depth=True)
-        elif rotation_feature_backend == "cuda-official-geometry":
-            smoothed = tuple(_probe_rotation_geometry(rotation_geometry_probe, surface_path, sphere_path, fwhm,
-                                                      temp / f"rotation-geometry-{side}.bin")
-                             for side, surface_path, sphere_path, fwhm in (
-                                 ("source", source_surface_path, source_sphere_path, 15.0),
-                                 ("target", target_surface_path, target_sphere_path, 10.0)))
-            source_values, target_values = depth_rotation_features(
-                source_stencil, target_stencil, source_surface.vertices, target_surface.vertices, target_device,
-                solver=rotation_feature_solver, smoothed_surfaces=smoothed, timings=timings)
         elif rotation_feature_backend == "native-curvature":
             source_values, target_values = native_rotation_features(
                 source_stencil, target_stencil, source_surface.vertices, target_surface.vertices, target_device)
@@ -423,9 +346,9 @@ def register_meshes(
         start = time.perf_counter()
         with ThreadPoolExecutor(max_workers=2) as pool:
             cur_future = pool.submit(rotated_builder.build, GiftiMesh(current_sphere, source_sphere.faces),
-                                     source_surface_path, normalize=False)
+                                     normalize=False)
             avg_future = pool.submit(rotated_builder.build, GiftiMesh(avg_target_sphere, target_sphere.faces),
-                                     target_surface_path, normalize=False) if avg else None
+                                     normalize=False) if avg else None
             current_stencil = cur_future.result()
             avg_target_stencil = avg_future.result() if avg_future is not None else None
         timings["rotated_stencil_seconds"] = time.perf_counter() - start
@@ -465,7 +388,7 @@ def register_meshes(
                 avg_source_surface = rotate_vertices(source_surface.vertices, pole)
                 avg_source_sphere = rotate_vertices(final_prewarp, pole)
                 avg_source_stencil = rotated_builder.build(GiftiMesh(avg_source_sphere, source_sphere.faces),
-                                                           source_surface_path, normalize=False)
+                                                           normalize=False)
                 avg_source_dev = avg_source_stencil.to(target_device)
                 last_flow, avg_flow = solve_dartel_from_surfaces_many(
                     [(source_surface_dev, target_surface_dev, current_dev, target_dev, run_fwhm),
@@ -483,7 +406,7 @@ def register_meshes(
             timings[f"dartel_run_{run_index}_seconds"] = time.perf_counter() - run_start
             if run_index + 1 < runs:
                 current_stencil = rotated_builder.build(GiftiMesh(current_sphere, source_sphere.faces),
-                                                        source_surface_path, normalize=False)
+                                                        normalize=False)
                 current_dev = current_stencil.to(target_device)
         if avg:
             avg_start = time.perf_counter()

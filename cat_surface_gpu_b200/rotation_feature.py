@@ -140,7 +140,7 @@ def depth_potential(geometries: torch.Tensor, topology: DepthTopology, *, solver
         _native.ptr(iterations), _native.ptr(residual), _native.ptr(normals) if normals is not None else None,
         _native.ptr(areas) if areas is not None else None, _native.ptr(scratch), scratch.numel(),
         int(cfg["n_ctas"]), int(cfg["threads_per_cta"]), int(cfg["lanes_per_row"]), float(timeout_s),
-        _native.stream_handle()), "csg_depth_potential")
+        _native.stream_handle(like=scratch)), "csg_depth_potential")
     status = int(scratch[:8].cpu().view(torch.int32)[1])
     if status != 0:
         raise RuntimeError(f"depth potential kernel failed (status {status})")

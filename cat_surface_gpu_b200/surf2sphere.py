@@ -10,8 +10,8 @@ Public names and signatures follow the reference module
   Triton launch per dependency level per sweep.
 * ``convert_ellipsoid_to_sphere_with_surface_area`` (reference 919-937) and
   ``surface_area`` (reference 461-471) -- host NumPy, same arithmetic.
-* ``run_cat_surf2sphere_gpu`` (reference 1107-1295) -- upstream binary for
-  stages 1-5, then the GPU sweeps, then the ellipsoid-to-sphere step.
+* ``run_cat_surf2sphere_gpu`` (reference 1107-1295) -- stages 1-5, the
+  sweeps and the ellipsoid-to-sphere steps, all on the GPU.
 """
 
 from __future__ import annotations
@@ -20,8 +20,6 @@ from concurrent.futures import Future, ThreadPoolExecutor
 from dataclasses import dataclass, field
 import math
 from pathlib import Path
-import subprocess
-import tempfile
 import time
 
 import numpy as np
@@ -259,7 +257,7 @@ def ellipsoid_to_sphere_device(points: torch.Tensor, desired_surface_area: float
     scratch = torch.empty(16, dtype=torch.uint8, device=points.device)
     _native.check(_native.library().csg_ellipsoid_to_sphere(
         _native.ptr(points), int(points.shape[0]), float(radius), _native.ptr(scratch), scratch.numel(),
-        _native.stream_handle()), "csg_ellipsoid_to_sphere")
+        _native.stream_handle(like=points)), "csg_ellipsoid_to_sphere")
     return points
 
 
@@ -312,7 +310,7 @@ def areal_sweeps_device(
             _native.ptr(plan_device["level_end"]), plan.n_levels, plan.level_stride, plan.max_degree, int(iterations),
             int(project_every), float(radius), mode, _native.ptr(scratch), scratch.numel(),
             int(cfg["n_ctas"]), int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s),
-            _native.stream_handle(stream),
+            _native.stream_handle(stream, like=points),
         ),
         "csg_areal_sweeps",
     )
@@ -493,8 +491,8 @@ def preprocess_device(
         _native.ptr(inc_off), _native.ptr(inc), _native.ptr(plan_device["order"]),
         _native.ptr(plan_device["level_begin"]), _native.ptr(plan_device["level_end"]), plan.n_levels,
         plan.level_stride, max_degree, int(stop_at), _native.ptr(scratch), scratch.numel(), int(cfg["n_ctas"]),
-        int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s), _native.stream_handle()),
-        "csg_surf2sphere_preprocess")
+        int(cfg["threads_per_cta"]), int(cfg["lanes_per_vertex"]), float(timeout_s),
+        _native.stream_handle(like=points)), "csg_surf2sphere_preprocess")
     return scratch
 
 
@@ -631,17 +629,6 @@ def _surf2sphere_on_device(mesh: GiftiMesh, topology: "Surf2SphereTopology | Fut
     return np.ascontiguousarray(result, dtype=np.float32)
 
 
-def _run_reference(reference_cli: Path, input_path: Path, output_path: Path, stop_at: int) -> None:
-    completed = subprocess.run(
-        [str(reference_cli), str(input_path), str(output_path), str(stop_at), "0"],
-        check=False,
-        capture_output=True,
-        text=True,
-    )
-    if completed.returncode != 0:
-        raise RuntimeError("CAT_Surf2Sphere CPU preprocessing failed:\n" + completed.stderr[-4000:])
-
-
 def run_cat_surf2sphere_gpu(
     input_surface: str | Path,
     output_surface: str | Path,
@@ -651,120 +638,78 @@ def run_cat_surf2sphere_gpu(
     device: str | torch.device = "cuda",
     dtype: str | torch.dtype = torch.float32,
     kernel: str = "triton",
-    preprocess_kernel: str = "cpu",
+    preprocess_kernel: str = "triton",
     preprocess_block_size: int | None = 131072,
     areal_schedule: str = "ordered",
     areal_arithmetic: str = "cat",
     areal_block_size: int | None = None,
 ) -> CatSurf2SphereGpuResult:
-    """CAT_Surf2Sphere with the sweeps on the GPU (reference 1107-1295).
+    """CAT_Surf2Sphere with every stage on the GPU (reference 1107-1295).
 
-    ``preprocess_kernel="cpu"`` (the reference's default) runs stages 1-5 on
-    the upstream binary ``reference_cli``; ``"triton"`` (the reference's name
-    for its GPU preprocess) runs them with the native kernels instead, so the
-    whole conversion stays on the GPU and no binary is needed.
+    Stages 1-5, the ellipsoid step, the area-smoothing sweeps and the final
+    ellipsoid step run on the native kernels; no process is spawned.  The
+    reference's ``preprocess_kernel="cpu"`` ran stages 1-5 on the upstream
+    CPU binary ``reference_cli``; this package has no CPU path, so ``"cpu"``
+    raises ``ValueError``.  ``"triton"`` (the reference's name for its GPU
+    preprocess, the default here) selects the native stages.
+    ``reference_cli`` is accepted for signature compatibility and not used.
     """
 
     if stop_at < 1:
         raise ValueError("stop_at must be at least 1")
-    if preprocess_kernel not in ("cpu", "triton"):
+    if preprocess_kernel == "cpu":
+        raise ValueError("preprocess_kernel='cpu' ran CAT_Surf2Sphere stages 1-5 on the upstream CPU binary; this "
+                         "package runs every stage on the GPU: use preprocess_kernel='triton'")
+    if preprocess_kernel != "triton":
         raise ValueError(f"Unsupported CAT_Surf2Sphere preprocess kernel: {preprocess_kernel}")
     input_path = Path(input_surface)
     output_path = Path(output_surface)
-    reference_path = Path(reference_cli) if reference_cli is not None else None
     timings: dict[str, float] = {}
     total_start = time.perf_counter()
-    if preprocess_kernel != "cpu":
-        # every stage on the GPU (reference 1135-1213 with the native preprocess)
-        input_mesh = read_gifti_mesh(input_path)
-        on_device = _resolve_dtype(dtype) == torch.float32 and stop_at > 5
-        if on_device:
-            # the host plan build (native code, the GIL released) runs beside the surface area,
-            # the upload and the ring tables; topology_build_seconds is its own duration
-            def timed_plan():
-                begin = time.perf_counter()
-                built = Surf2SphereTopology.plan_only(input_mesh)
-                timings["topology_build_seconds"] = time.perf_counter() - begin
-                return built
+    # every stage on the GPU (reference 1135-1213 with the native preprocess)
+    input_mesh = read_gifti_mesh(input_path)
+    on_device = _resolve_dtype(dtype) == torch.float32 and stop_at > 5
+    if on_device:
+        # the host plan build (native code, the GIL released) runs beside the surface area,
+        # the upload and the ring tables; topology_build_seconds is its own duration
+        def timed_plan():
+            begin = time.perf_counter()
+            built = Surf2SphereTopology.plan_only(input_mesh)
+            timings["topology_build_seconds"] = time.perf_counter() - begin
+            return built
 
-            with ThreadPoolExecutor(max_workers=1) as pool:
-                future = pool.submit(timed_plan)
-                area = surface_area(input_mesh)
-                pre = _surf2sphere_on_device(input_mesh, future, area, stop_at, device, areal_arithmetic, timings)
-            write_start = time.perf_counter()
-            write_vertices_like(input_path, output_path, pre)
-            timings["output_write_seconds"] = time.perf_counter() - write_start
-            timings["total_seconds"] = time.perf_counter() - total_start
-            # the file holds exactly these arrays (float32 vertices, the input's faces)
-            return CatSurf2SphereGpuResult(np.ascontiguousarray(pre, dtype=np.float32), input_mesh.faces, timings,
-                                           output_path)
-        topology_start = time.perf_counter()
-        topology = Surf2SphereTopology.from_mesh(input_mesh)
-        timings["topology_build_seconds"] = time.perf_counter() - topology_start
-        area = surface_area(input_mesh)
-        pre, pre_timings = run_surf2sphere_preprocess_cuda(
-            input_mesh.vertices, input_mesh.faces, topology, stop_at=min(stop_at, 5), desired_surface_area=area,
-            device=device, dtype=dtype, schedule_block_size=preprocess_block_size)
-        timings.update(pre_timings)
-        if stop_at > 5:
-            radius = float(np.sqrt(np.max(np.sum(pre.astype(np.float64) ** 2, axis=1))))
-            smoothed, smooth_timings = run_areal_smoothing_cuda(
-                pre, input_mesh.faces, topology, iterations=1000 * (stop_at - 5), project_every=1000, radius=radius,
-                device=device, dtype=dtype, kernel=kernel, schedule=areal_schedule, arithmetic=areal_arithmetic,
-                schedule_block_size=areal_block_size)
-            timings.update(smooth_timings)
-            conversion_start = time.perf_counter()
-            pre = convert_ellipsoid_to_sphere_with_surface_area(smoothed, area)
-            timings["ellipsoid_to_sphere_seconds"] = time.perf_counter() - conversion_start
+        with ThreadPoolExecutor(max_workers=1) as pool:
+            future = pool.submit(timed_plan)
+            area = surface_area(input_mesh)
+            pre = _surf2sphere_on_device(input_mesh, future, area, stop_at, device, areal_arithmetic, timings)
         write_start = time.perf_counter()
         write_vertices_like(input_path, output_path, pre)
         timings["output_write_seconds"] = time.perf_counter() - write_start
-        result_mesh = read_gifti_mesh(output_path)
         timings["total_seconds"] = time.perf_counter() - total_start
-        return CatSurf2SphereGpuResult(result_mesh.vertices, result_mesh.faces, timings, output_path)
-    if reference_path is None:
-        raise ValueError("preprocess_kernel='cpu' runs stages 1-5 on the upstream binary: give reference_cli")
-    if stop_at <= 5:
-        start = time.perf_counter()
-        _run_reference(reference_path, input_path, output_path, stop_at)
-        timings["reference_prefix_seconds"] = time.perf_counter() - start
-        mesh = read_gifti_mesh(output_path)
-        timings["total_seconds"] = time.perf_counter() - total_start
-        return CatSurf2SphereGpuResult(mesh.vertices, mesh.faces, timings, output_path)
-
-    with tempfile.TemporaryDirectory(prefix="cat_surface_b200_surf2sphere_") as temp_dir:
-        prefix_path = Path(temp_dir) / "stage5.gii"
-        start = time.perf_counter()
-        _run_reference(reference_path, input_path, prefix_path, 5)
-        timings["reference_prefix_seconds"] = time.perf_counter() - start
-        prefix_mesh = read_gifti_mesh(prefix_path)
-        topology_start = time.perf_counter()
-        topology = Surf2SphereTopology.from_mesh(prefix_mesh)
-        timings["topology_build_seconds"] = time.perf_counter() - topology_start
-        radius = float(np.sqrt(np.max(np.sum(prefix_mesh.vertices.astype(np.float64) ** 2, axis=1))))
+        # the file holds exactly these arrays (float32 vertices, the input's faces)
+        return CatSurf2SphereGpuResult(np.ascontiguousarray(pre, dtype=np.float32), input_mesh.faces, timings,
+                                       output_path)
+    topology_start = time.perf_counter()
+    topology = Surf2SphereTopology.from_mesh(input_mesh)
+    timings["topology_build_seconds"] = time.perf_counter() - topology_start
+    area = surface_area(input_mesh)
+    pre, pre_timings = run_surf2sphere_preprocess_cuda(
+        input_mesh.vertices, input_mesh.faces, topology, stop_at=min(stop_at, 5), desired_surface_area=area,
+        device=device, dtype=dtype, schedule_block_size=preprocess_block_size)
+    timings.update(pre_timings)
+    if stop_at > 5:
+        radius = float(np.sqrt(np.max(np.sum(pre.astype(np.float64) ** 2, axis=1))))
         smoothed, smooth_timings = run_areal_smoothing_cuda(
-            prefix_mesh.vertices,
-            prefix_mesh.faces,
-            topology,
-            iterations=1000 * (stop_at - 5),
-            project_every=1000,
-            radius=radius,
-            device=device,
-            dtype=dtype,
-            kernel=kernel,
-            schedule=areal_schedule,
-            arithmetic=areal_arithmetic,
-            schedule_block_size=areal_block_size,
-        )
+            pre, input_mesh.faces, topology, iterations=1000 * (stop_at - 5), project_every=1000, radius=radius,
+            device=device, dtype=dtype, kernel=kernel, schedule=areal_schedule, arithmetic=areal_arithmetic,
+            schedule_block_size=areal_block_size)
         timings.update(smooth_timings)
         conversion_start = time.perf_counter()
-        converted = convert_ellipsoid_to_sphere_with_surface_area(
-            smoothed, surface_area(read_gifti_mesh(input_path))
-        )
+        pre = convert_ellipsoid_to_sphere_with_surface_area(smoothed, area)
         timings["ellipsoid_to_sphere_seconds"] = time.perf_counter() - conversion_start
-        write_start = time.perf_counter()
-        write_vertices_like(prefix_path, output_path, converted)
-        timings["output_write_seconds"] = time.perf_counter() - write_start
+    write_start = time.perf_counter()
+    write_vertices_like(input_path, output_path, pre)
+    timings["output_write_seconds"] = time.perf_counter() - write_start
     result_mesh = read_gifti_mesh(output_path)
     timings["total_seconds"] = time.perf_counter() - total_start
     return CatSurf2SphereGpuResult(result_mesh.vertices, result_mesh.faces, timings, output_path)

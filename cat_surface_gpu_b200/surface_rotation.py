@@ -200,7 +200,7 @@ class _Costing:
             int(self.inputs.n_features), int(self.index.target_points.shape[0]),
         )
         lib = _native.library()
-        stream = _native.stream_handle()
+        stream = _native.stream_handle(like=self.costs)
         _native.check(
             lib.csg_rotation_cost_batch(1, ctypes.addressof(surface), self.costs.data_ptr(), self.tile, 0,
                                         self.scratch.data_ptr(), self.scratch.numel(), stream),
@@ -258,7 +258,7 @@ class RotationGridIndexDevice:
         offsets = torch.empty(grid_size ** 3 + 1, dtype=torch.int32, device=target)
         scratch = torch.empty(int(lib.csg_rotation_grid_scratch_bytes(grid_size)), dtype=torch.uint8, device=target)
         count = ctypes.c_longlong(0)
-        stream = _native.stream_handle()
+        stream = _native.stream_handle(like=scratch)
         args = (d_pts.data_ptr(), pts.shape[0], d_faces.data_ptr(), tri.shape[0], grid_size, margin,
                 offsets.data_ptr())
         _native.check(lib.csg_rotation_grid_build_device(*args, None, 0, ctypes.addressof(count), scratch.data_ptr(),
@@ -514,7 +514,7 @@ def batched_costs(indices, inputs, angle_sets=None, *, matrix_sets=None, tile: i
     lib = _native.library()
     need = lib.csg_rotation_scratch_bytes(n, ctypes.addressof(n_src), ctypes.addressof(n_cand), tile)
     scratch = torch.empty(int(need), dtype=torch.uint8, device=dev)
-    stream = _native.stream_handle()
+    stream = _native.stream_handle(like=scratch)
     _native.check(lib.csg_rotation_cost_batch(n, ctypes.addressof(surfaces), costs.data_ptr(), tile, n_ctas,
                                               scratch.data_ptr(), scratch.numel(), stream), "csg_rotation_cost_batch")
     status = ctypes.c_int(0)

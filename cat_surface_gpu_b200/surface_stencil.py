@@ -254,7 +254,8 @@ def build_surface_stencil(sphere_vertices, sphere_faces, *, nx: int = 512, ny: i
         with torch.cuda.device(target):
             scratch = torch.empty(need, dtype=torch.uint8, device=target)
             _native.check(lib.csg_stencil_build_device(*inputs, *outputs, scratch.data_ptr(), need,
-                                                       _native.stream_handle()), "csg_stencil_build_device")
+                                                       _native.stream_handle(like=scratch)),
+                          "csg_stencil_build_device")
     else:
         _native.check(lib.csg_stencil_build(*inputs, int(threads), *outputs), "csg_stencil_build")
     return SurfaceStencil(sphere_points=sphere_points, faces=rfaces, surface_indices=surface_indices,

@@ -234,7 +234,7 @@ def solve_dartel_maps(source_maps, target_maps, *, loop: int = 6, lmreg: float =
     solver = _Solver(steps, ny, nx, dtype, dev, loop, lmreg, cycles, nit, its, code, assume_initial_nonzero)
     solver.source.copy_(source)
     solver.target.copy_(target)
-    solver.launch(_native.stream_handle())
+    solver.launch(_native.stream_handle(like=solver.source))
     return DartelSolveResult(solver.flow, source, target, solver.metrics)
 
 
@@ -257,7 +257,7 @@ def solve_dartel_batch(source_maps, target_maps, *, loop: int = 6, lmreg: float 
     solver = _Solver(batch, ny, nx, dtype, dev, loop, lmreg, cycles, nit, its, code, True)
     solver.source.copy_(source)
     solver.target.copy_(target)
-    solver.launch(_native.stream_handle(), flows="all")
+    solver.launch(_native.stream_handle(like=solver.source), flows="all")
     return solver.flows, solver.velocity, solver.metrics
 
 
@@ -304,7 +304,7 @@ def solve_dartel_registrations(source_maps, target_maps, *, loop: int = 6, lmreg
                      bool(assume_initial_nonzero))
     solver.source.copy_(source.reshape(regs * steps, ny, nx))
     solver.target.copy_(target.reshape(regs * steps, ny, nx))
-    solver.launch(_native.stream_handle(), "registrations", steps)
+    solver.launch(_native.stream_handle(like=solver.source), "registrations", steps)
     return solver.flows[:regs], solver.metrics.view(regs, steps, -1, 3)
 
 
@@ -418,7 +418,8 @@ def apply_flow_to_sphere(sphere_vertices, flow, *, unit_sphere_vertices=None, in
     _native.check(
         lib.csg_apply_flow_to_sphere(_dtype_code(dtype), int(points.shape[0]), points.data_ptr(),
                                      int(deformation.shape[2]), int(deformation.shape[1]), deformation.data_ptr(),
-                                     int(bool(inverse)), out.data_ptr(), _native.stream_handle()),
+                                     int(bool(inverse)), out.data_ptr(),
+                                     _native.stream_handle(like=out)),
         "csg_apply_flow_to_sphere",
     )
     return out
@@ -447,7 +448,7 @@ def average_xz_surfaces(x_surface, z_surface, *, device="auto") -> torch.Tensor:
     out = torch.empty(xv.shape, dtype=torch.float32, device=dev)
     _native.check(
         _native.library().csg_average_xz(int(xv.shape[0]), xv.data_ptr(), zv.data_ptr(), out.data_ptr(),
-                                         _native.stream_handle()),
+                                         _native.stream_handle(like=out)),
         "csg_average_xz",
     )
     return out

@@ -158,7 +158,10 @@ CSG_API int csg_areal_sweeps(void *points, int n_vertices, const int32_t *slot_o
  * All calls share the one array, so calls that overlap on the GPU (other
  * streams, other threads) race; serialise them.  With status_out non-NULL the
  * call waits for the kernel and reports its status word (also returned);
- * with NULL it returns once the work is enqueued. */
+ * with NULL it returns once the work is enqueued.  status_out must be NULL
+ * while `stream` is being captured (CSG_ERR_ARG otherwise, before any work).
+ * The array's address is looked up once per device, so the library must not
+ * be used across a cudaDeviceReset of that device. */
 CSG_API int csg_areal_sweeps_noalloc(void *points, int n_vertices, const int32_t *slot_off, const int32_t *slot_tri,
                                      const int32_t *order, const int32_t *level_begin, const int32_t *level_end,
                                      int n_levels, int level_stride, int max_degree, int iterations, int project_every,

@@ -33,24 +33,24 @@ def _plan(faces, n):
     return SweepPlan.build(faces, n)
 
 
-def _noalloc(lib, points, plan_device, plan, iterations, project_every, radius):
+def _noalloc(lib, points, plan_device, plan, iterations, project_every, radius, arithmetic=0):
     from cat_surface_gpu_b200 import _native
 
     status = ctypes.c_int(12345)
     rc = lib.csg_areal_sweeps_noalloc(
         points.data_ptr(), points.shape[0], plan_device["slot_off"].data_ptr(), plan_device["slot_tri"].data_ptr(),
         plan_device["order"].data_ptr(), plan_device["level_begin"].data_ptr(), plan_device["level_end"].data_ptr(),
-        plan.n_levels, plan.level_stride, plan.max_degree, iterations, project_every, radius, 0, 0, 0, 0, 2.0,
-        ctypes.addressof(status), _native.stream_handle(),
+        plan.n_levels, plan.level_stride, plan.max_degree, iterations, project_every, radius, arithmetic, 0, 0, 0,
+        2.0, ctypes.addressof(status), _native.stream_handle(),
     )
     return rc, status.value
 
 
-def _regular(points, plan_device, plan, iterations, project_every, radius):
+def _regular(points, plan_device, plan, iterations, project_every, radius, arithmetic="cat"):
     from cat_surface_gpu_b200 import surf2sphere
 
     scratch = surf2sphere.areal_sweeps_device(points, plan_device, plan, iterations=iterations,
-                                              project_every=project_every, radius=radius, arithmetic="cat")
+                                              project_every=project_every, radius=radius, arithmetic=arithmetic)
     torch.cuda.synchronize()
     assert surf2sphere.read_status(scratch) == (0, 0)
 
@@ -72,6 +72,25 @@ def test_noalloc_matches_regular_entry_point_on_two_calls(native_library):
         _regular(expected, plan_device, plan, iterations, project_every, radius)
         got = torch.from_numpy(np.ascontiguousarray(vertices, dtype=np.float32)).cuda()
         rc, status = _noalloc(native_library, got, plan_device, plan, iterations, project_every, radius)
+        assert rc == 0 and status == 0
+        np.testing.assert_array_equal(got.cpu().numpy(), expected.cpu().numpy())
+
+
+def test_noalloc_float64_matches_regular_entry_point(native_library):
+    """The float64 mode (a double4 working copy in the same array), twice in a row, bit for bit."""
+
+    from cat_surface_gpu_b200 import _native
+
+    g = load_surf2sphere_golden("c1")
+    plan = _plan(g["faces"], g["prefix"].shape[0])
+    plan_device = plan.to_device(torch.device("cuda"))
+    vertices = g["prefix"].astype(np.float64)
+    radius = float(np.sqrt(np.max(np.sum(vertices ** 2, axis=1))))
+    expected = torch.from_numpy(np.ascontiguousarray(vertices)).cuda()
+    _regular(expected, plan_device, plan, 1100, 1000, radius, arithmetic="fp64")
+    for _ in range(2):
+        got = torch.from_numpy(np.ascontiguousarray(vertices)).cuda()
+        rc, status = _noalloc(native_library, got, plan_device, plan, 1100, 1000, radius, _native.ARITH["fp64"])
         assert rc == 0 and status == 0
         np.testing.assert_array_equal(got.cpu().numpy(), expected.cpu().numpy())
 
