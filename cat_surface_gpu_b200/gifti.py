@@ -48,6 +48,32 @@ class GiftiMesh:
     vertices: np.ndarray
     faces: np.ndarray
 
+    def check(self, label: str = "mesh") -> "GiftiMesh":
+        """``ValueError`` unless the vertices are finite and every face index names a vertex.
+
+        The GPU kernels trust both, so a surface with NaN or infinite
+        coordinates, or faces outside ``[0, n)``, is refused on the host.
+        """
+
+        check_vertices(self.vertices, label)
+        faces = np.asarray(self.faces)
+        if faces.ndim != 2 or faces.shape[1] != 3:
+            raise ValueError(f"{label}: faces must have shape [m, 3], got {faces.shape}")
+        n = int(np.asarray(self.vertices).shape[0])
+        if faces.size and (int(faces.min()) < 0 or int(faces.max()) >= n):
+            raise ValueError(f"{label}: a face index lies outside [0, {n})")
+        return self
+
+
+def check_vertices(vertices, label: str = "vertices") -> None:
+    """``ValueError`` unless ``vertices`` is a non-empty ``[n, 3]`` array of finite numbers."""
+
+    values = np.asarray(vertices)
+    if values.ndim != 2 or values.shape[1] != 3 or values.shape[0] == 0:
+        raise ValueError(f"{label}: vertices must have shape [n, 3] with n > 0, got {values.shape}")
+    if not np.isfinite(values).all():
+        raise ValueError(f"{label}: vertices must be finite (NaN or infinite coordinates found)")
+
 
 # Deflate of large arrays runs in parallel chunks (as pigz does): each chunk is a raw
 # deflate stream ended by a sync flush (the last one by the final block), so their
@@ -145,12 +171,25 @@ def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
 
 
 def read_gifti_arrays(path: str | Path) -> list[tuple[np.ndarray, int]]:
-    """Return every data array of a GIFTI file with its NIfTI intent code."""
+    """Return every data array of a GIFTI file with its NIfTI intent code.
 
-    root = ET.parse(str(path)).getroot()
+    A file that is not well-formed XML, or whose array payload does not
+    decode (bad base64, a truncated or corrupt zlib stream, a size that
+    disagrees with the header), raises ``ValueError``.
+    """
+
+    try:
+        root = ET.parse(str(path)).getroot()
+    except ET.ParseError as error:
+        raise ValueError(f"Not a GIFTI file (XML: {error}): {path}") from error
     if root.tag != "GIFTI":
         raise ValueError(f"Not a GIFTI file: {path}")
-    return [_decode_array(item) for item in root.findall("DataArray")]
+    try:
+        return [_decode_array(item) for item in root.findall("DataArray")]
+    except (zlib.error, KeyError, TypeError) as error:
+        raise ValueError(f"Corrupt GIFTI data array ({error}): {path}") from error
+    except ValueError as error:
+        raise ValueError(f"Corrupt GIFTI data array ({error}): {path}") from error
 
 
 def read_gifti_mesh(path: str | Path) -> GiftiMesh:

@@ -291,6 +291,20 @@ def register_meshes(
     if rotation_feature_backend == "auto":
         # the reference's resolution without a values probe (reference 550-553)
         rotation_feature_backend = "cuda"
+    # the kernels trust the meshes: refuse bad ones before any launch
+    for label, surface, sphere in (("source", source_surface, source_sphere), ("target", target_surface, target_sphere)):
+        surface.check(f"{label} surface")
+        sphere.check(f"{label} sphere")
+        if surface.vertices.shape[0] != sphere.vertices.shape[0]:
+            raise ValueError(f"{label} surface has {surface.vertices.shape[0]} vertices but its sphere has "
+                             f"{sphere.vertices.shape[0]}")
+    for label, stencil in (("source", source_stencil), ("target", target_stencil)):
+        if stencil is not None:
+            stencil.validate()
+    if rotation_values is not None:
+        for label, values in zip(("source", "target"), rotation_values):
+            if not np.isfinite(np.asarray(values, dtype=np.float64)).all():
+                raise ValueError(f"{label} rotation values are not finite")
     solve_dtype = _resolve_dartel_dtype(dartel_dtype)
     target_device = resolve_device(device)
     graph_requested = bool(cuda_graph and (runs + int(avg) >= 3))

@@ -27,7 +27,7 @@ import torch
 
 from . import _native
 from .device import DeviceUnavailable, resolve_device
-from .gifti import GiftiMesh, read_gifti_mesh, write_vertices_like
+from .gifti import GiftiMesh, check_vertices, read_gifti_mesh, write_vertices_like
 
 
 @dataclass(frozen=True)
@@ -385,10 +385,6 @@ def run_areal_smoothing_cuda(
     size and device) or None (the default shape).
     """
 
-    try:
-        target = resolve_device(device)
-    except DeviceUnavailable as exc:
-        raise RuntimeError(f"CAT_Surf2Sphere CUDA backend: {exc}") from exc
     geometry_dtype = _resolve_dtype(dtype)
     if kernel not in ("torch", "triton", "cuda"):
         raise ValueError(f"Unsupported CAT_Surf2Sphere kernel: {kernel}")
@@ -405,6 +401,11 @@ def run_areal_smoothing_cuda(
     points_host = np.asarray(vertices)
     if points_host.ndim != 2 or points_host.shape[1] != 3:
         raise ValueError(f"vertices must have shape [n, 3], got {points_host.shape}")
+    check_vertices(points_host, "areal smoothing input")
+    try:
+        target = resolve_device(device)
+    except DeviceUnavailable as exc:
+        raise RuntimeError(f"CAT_Surf2Sphere CUDA backend: {exc}") from exc
     if geometry_dtype == torch.float64:
         mode = "fp64"
     else:
@@ -520,14 +521,15 @@ def run_surf2sphere_preprocess_cuda(
     float32 with float64 arithmetic; ``dtype=float64`` is not offered.
     """
 
-    try:
-        target = resolve_device(device)
-    except DeviceUnavailable as exc:
-        raise RuntimeError(f"CAT_Surf2Sphere CUDA backend: {exc}") from exc
     if _resolve_dtype(dtype) != torch.float32:
         raise ValueError("the GPU preprocess keeps float32 positions (float64 arithmetic)")
     if stop_at < 1 or stop_at > 5:
         raise ValueError("CUDA preprocessing stop_at must be between 1 and 5")
+    check_vertices(vertices, "CAT_Surf2Sphere input")
+    try:
+        target = resolve_device(device)
+    except DeviceUnavailable as exc:
+        raise RuntimeError(f"CAT_Surf2Sphere CUDA backend: {exc}") from exc
     points_host = np.ascontiguousarray(np.asarray(vertices, dtype=np.float32))
     tri = np.ascontiguousarray(faces, dtype=np.int32)
     if points_host.ndim != 2 or points_host.shape[1] != 3 or tri.ndim != 2 or tri.shape[1] != 3:
@@ -667,7 +669,7 @@ def run_cat_surf2sphere_gpu(
     timings: dict[str, float] = {}
     total_start = time.perf_counter()
     # every stage on the GPU (reference 1135-1213 with the native preprocess)
-    input_mesh = read_gifti_mesh(input_path)
+    input_mesh = read_gifti_mesh(input_path).check(str(input_path))
     on_device = _resolve_dtype(dtype) == torch.float32 and stop_at > 5
     if on_device:
         # the host plan build (native code, the GIL released) runs beside the surface area,

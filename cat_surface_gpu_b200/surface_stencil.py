@@ -54,6 +54,9 @@ class SurfaceStencil:
             magic, version, n_points, n_tri, n_sheet, nx, ny, source_points = _HEADER.unpack(header)
             if magic != _MAGIC or version not in (1, 2):
                 raise ValueError("Stencil file magic or")
+            if min(n_points, n_tri, n_sheet, nx, ny, source_points) < 0 or n_sheet != nx * ny:
+                raise ValueError(f"Stencil file header: points {n_points}, triangles {n_tri}, sheet {n_sheet} "
+                                 f"({nx} x {ny}), source points {source_points}")
             sphere_points = np.fromfile(stream, dtype="<f8", count=3 * n_points)
             faces = np.fromfile(stream, dtype="<i4", count=3 * n_tri)
             surface_indices = np.fromfile(stream, dtype="<i4", count=3 * n_points)
@@ -68,7 +71,7 @@ class SurfaceStencil:
             raise ValueError("Stencil file length")
         if unit is not None and unit.size != 3 * source_points:
             raise ValueError("Stencil unit sphere length")
-        return cls(
+        stencil = cls(
             sphere_points=sphere_points.reshape(n_points, 3),
             faces=faces.reshape(n_tri, 3),
             surface_indices=surface_indices.reshape(n_points, 3),
@@ -80,6 +83,27 @@ class SurfaceStencil:
             source_points=source_points,
             unit_sphere_points=None if unit is None else unit.reshape(source_points, 3),
         )
+        stencil.validate()
+        return stencil
+
+    def validate(self) -> None:
+        """``ValueError`` unless every index is in range and every value finite.
+
+        The device kernels gather with these indices, so a corrupt file must
+        be refused on the host: faces and sheet barycentrics index the sphere
+        points, surface barycentrics the source mesh's vertices.
+        """
+
+        n = int(self.sphere_points.shape[0])
+        checks = (("faces", self.faces, n), ("surface_indices", self.surface_indices, int(self.source_points)),
+                  ("sheet_indices", self.sheet_indices, n))
+        for name, indices, bound in checks:
+            if indices.size and (int(indices.min()) < 0 or int(indices.max()) >= bound):
+                raise ValueError(f"Stencil {name} outside [0, {bound})")
+        for name, values in (("sphere points", self.sphere_points), ("surface weights", self.surface_weights),
+                             ("sheet weights", self.sheet_weights), ("unit sphere points", self.unit_sphere_points)):
+            if values is not None and not np.isfinite(values).all():
+                raise ValueError(f"Stencil {name} are not finite")
 
     def to_file(self, path) -> None:
         """Write the v2 (v1 without unit points) layout read by ``from_file``."""
