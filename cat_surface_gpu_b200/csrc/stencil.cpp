@@ -1,22 +1,36 @@
 // Spherical resampling stencils (host C++, float64, deterministic, threaded).
 //
 // Builds the same stencil the reference's helper writes
-// (native/cat_surface_stencil_builder.c:172-464 in the reference project):
-//   * sphere points: the resampling sphere's points moved onto the input
-//     sphere (closest point on the input's triangles);
-//   * surface barycentrics: for every resampling-sphere point scaled to
-//     0.975 x the mean input radius, the closest input triangle and the
-//     barycentric weights of the closest point -- indices refer to the
-//     surface (same topology as the sphere);
+// (native/cat_surface_stencil_builder.c:107-170, 355-464 in the reference
+// project):
+//   * the input sphere is centred on its vertex mean and unit-normalised
+//     (unless `normalize` is 0); the resampling sphere's unit directions are
+//     placed at centre + r u with centre = per-axis (min + max) of those
+//     points and r = 0.975 x their mean length, as the helper places its
+//     tetrahedral sphere (:406-421);
+//   * surface barycentrics: for every placed resampling point, the input
+//     triangle the helper's closest-polygon rule picks and the barycentric
+//     weights of the picked point -- indices refer to the surface (same
+//     topology as the sphere);
+//   * sphere points: the input sphere interpolated with those weights (the
+//     helper's resampled sphere, :424);
 //   * sheet barycentrics: for every sheet cell centre (u, v) =
 //     ((x + 0.5) / nx, (y + 0.5) / ny) mapped to the unit point
-//     (sin(pi v) cos(2 pi u), sin(pi v) sin(2 pi u), cos(pi v)), the closest
-//     triangle of the unit-normalised sphere points;
+//     (sin(pi v) cos(2 pi u), sin(pi v) sin(2 pi u), cos(pi v)), the picked
+//     triangle of the unit-normalised sphere points (:138-170);
 //   * unit-sphere points of the input vertices.
-// The resampling sphere (points + faces) is supplied by the caller.  Closest
-// points are exact: a uniform grid over the target triangles is searched in
-// growing shells of cells until no unvisited cell can hold a closer point;
-// ties keep the lowest triangle index.
+// The resampling sphere (points + faces) is supplied by the caller.
+//
+// The closest-polygon rule is the one the reference restates for its
+// rotation search (src/cat_surface_gpu/surface_rotation.py:354-425): project
+// the query onto each triangle's plane; if the projection's parametric
+// coordinates lie inside the triangle with a 1e-3 tolerance the candidate
+// distance is the plane distance, otherwise it is the distance to the nearer
+// of the two edges at the triangle's nearest vertex; the smallest candidate
+// distance wins, ties to the lowest triangle index; the weights are those of
+// the winning point (:335-352).  The search over a uniform grid of the
+// triangles is exhaustive in effect: shells of cells are visited until no
+// unvisited cell can hold a triangle whose candidate distance is smaller.
 #include <algorithm>
 #include <array>
 #include <atomic>
@@ -42,61 +56,86 @@ __host__ __device__ inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b
 __host__ __device__ inline V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
 __host__ __device__ inline double dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
 
-// Closest point of p on triangle abc with its barycentric weights (Voronoi
-// region classification of the point against the triangle's features;
-// Ericson, Real-Time Collision Detection, 5.1.5).
-// Shared by the host builder and the device kernels (one IEEE rounding per
-// operation on both: no contraction on either side).
-__host__ __device__ double closest_on_triangle(V3 p, V3 a, V3 b, V3 c, double w[3]) {
-    const V3 ab = b - a, ac = c - a, ap = p - a;
-    const double d1 = dot(ab, ap), d2 = dot(ac, ap);
-    V3 q;
-    if (d1 <= 0.0 && d2 <= 0.0) {
-        w[0] = 1; w[1] = 0; w[2] = 0;
-        q = a;
-    } else {
-        const V3 bp = p - b;
-        const double d3 = dot(ab, bp), d4 = dot(ac, bp);
-        if (d3 >= 0.0 && d4 <= d3) {
-            w[0] = 0; w[1] = 1; w[2] = 0;
-            q = b;
-        } else {
-            const double vc = d1 * d4 - d3 * d2;
-            if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
-                const double t = d1 / (d1 - d3);
-                w[0] = 1 - t; w[1] = t; w[2] = 0;
-                q = a + t * ab;
-            } else {
-                const V3 cp = p - c;
-                const double d5 = dot(ab, cp), d6 = dot(ac, cp);
-                if (d6 >= 0.0 && d5 <= d6) {
-                    w[0] = 0; w[1] = 0; w[2] = 1;
-                    q = c;
-                } else {
-                    const double vb = d5 * d2 - d1 * d6;
-                    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
-                        const double t = d2 / (d2 - d6);
-                        w[0] = 1 - t; w[1] = 0; w[2] = t;
-                        q = a + t * ac;
-                    } else {
-                        const double va = d3 * d6 - d5 * d4;
-                        if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
-                            const double t = (d4 - d3) / ((d4 - d3) + (d5 - d6));
-                            w[0] = 0; w[1] = 1 - t; w[2] = t;
-                            q = b + t * (c - b);
-                        } else {
-                            const double den = 1.0 / ((va + vb) + vc);
-                            const double v = vb * den, u = vc * den;
-                            w[0] = 1.0 - v - u; w[1] = v; w[2] = u;
-                            q = (a + v * ab) + u * ac;
-                        }
-                    }
-                }
-            }
-        }
-    }
+__host__ __device__ inline V3 cross(V3 a, V3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Nearest point to p on segment [first, second] and its squared distance.
+__host__ __device__ inline double segment_point(V3 p, V3 first, V3 second, V3& q) {
+    const V3 dir = second - first, off = p - first;
+    const double den = dot(dir, dir);
+    double alpha = den != 0.0 ? dot(off, dir) / den : 0.0;
+    alpha = alpha < 0.0 ? 0.0 : (alpha > 1.0 ? 1.0 : alpha);
+    q = first + alpha * dir;
     const V3 d = p - q;
     return dot(d, d);
+}
+
+// Candidate distance of p to triangle abc under the closest-polygon rule
+// (plane projection inside with a 1e-3 parametric tolerance, else the nearer
+// edge at the nearest vertex) and the candidate point.  Shared by the host
+// builder and the device kernels (one IEEE rounding per operation on both:
+// no contraction on either side).
+__host__ __device__ double locate_on_triangle(V3 p, V3 a, V3 b, V3 c, V3& point) {
+    const V3 ea = b - a, eb = c - a;
+    const V3 n = cross(ea, eb);
+    const double nsq = dot(n, n);
+    const double t = nsq != 0.0 ? dot(a - p, n) / nsq : 0.0;
+    const V3 proj = p + t * n;
+    const V3 po = proj - a;
+    const double xx = dot(ea, ea), xy = dot(ea, eb), xv = dot(ea, po), yy = dot(eb, eb), yv = dot(eb, po);
+    const double den = xx * yy - xy * xy;
+    const double xpos = den != 0.0 ? (xv * yy - yv * xy) / den : 0.0;
+    const double ypos = den != 0.0 ? (yv * xx - xv * xy) / den : 0.0;
+    const double tol = 1.0e-3, top = 1.0 + tol;
+    const double sum = xpos + ypos;
+    if (den != 0.0 && xpos >= -tol && xpos <= top && ypos >= -tol && ypos <= top && sum >= -tol && sum <= top) {
+        point = proj;
+        return t * t * nsq;
+    }
+    const V3 v[3] = {a, b, c};
+    double vd[3];
+    for (int k = 0; k < 3; ++k) {
+        const V3 d = p - v[k];
+        vd[k] = dot(d, d);
+    }
+    int cv = 0;
+    if (vd[1] < vd[cv]) cv = 1;
+    if (vd[2] < vd[cv]) cv = 2;
+    V3 q1, q2;
+    const double d1 = segment_point(p, v[(cv + 2) % 3], v[cv], q1);
+    const double d2 = segment_point(p, v[cv], v[(cv + 1) % 3], q2);
+    if (d1 < d2) {
+        point = q1;
+        return d1;
+    }
+    point = q2;
+    return d2;
+}
+
+// Barycentric weights of p in triangle abc: for each vertex, the offset of
+// p from the opposite edge along the in-plane normal of that edge, over the
+// vertex's own offset (the reference's three-cross-product form).
+__host__ __device__ void point_weights(V3 p, V3 a, V3 b, V3 c, double w[3]) {
+    const V3 t[3] = {a, b, c};
+    for (int k = 0; k < 3; ++k) {
+        const V3 first = t[(k + 1) % 3], second = t[(k + 2) % 3], third = t[k];
+        const V3 po = p - first, hz = second - first, up = third - first;
+        const V3 vert = cross(cross(hz, up), hz);
+        w[k] = dot(po, vert) / dot(up, vert);
+    }
+}
+
+// Upper bound on how far a point the rule accepts as inside (within the
+// tolerance) can lie from its triangle: 3e-3 of the longest edge, doubled.
+double tolerance_reach(const std::vector<V3>& pts, const int32_t* faces, int n_faces) {
+    double longest = 0.0;
+    for (int f = 0; f < n_faces; ++f)
+        for (int k = 0; k < 3; ++k) {
+            const V3 d = pts[faces[3 * f + k]] - pts[faces[3 * f + (k + 1) % 3]];
+            longest = std::max(longest, std::sqrt(dot(d, d)));
+        }
+    return 6.0e-3 * longest;
 }
 
 struct Mesh {
@@ -110,12 +149,14 @@ struct Mesh {
 struct Grid {
     V3 lo{}, cell{};
     int n = 1;
+    double slack = 0.0;  // tolerance_reach of the mesh
     std::vector<int> off, tri;
     const Mesh* mesh = nullptr;
 
     void build(const Mesh& m, int resolution) {
         mesh = &m;
         n = resolution;
+        slack = tolerance_reach(m.pts, m.faces, m.n_faces);
         V3 hi{-1e300, -1e300, -1e300};
         lo = {1e300, 1e300, 1e300};
         for (const V3& p : m.pts) {
@@ -156,17 +197,19 @@ struct Grid {
     }
     size_t id(int x, int y, int z) const { return (static_cast<size_t>(z) * n + y) * n + x; }
 
-    // Exact closest triangle (lowest index on ties) and barycentric weights.
-    int closest(V3 p, double w[3]) const {
+    // The triangle the closest-polygon rule picks (lowest index on ties) and
+    // the weights of its candidate point.  A triangle in a cell at Chebyshev
+    // distance >= r lies at least (r - 1) * cmin away, so its candidate
+    // distance is at least ((r - 1) * cmin - slack)^2.
+    int locate(V3 p, double w[3]) const {
         const int cx = index(p.x, lo.x, cell.x), cy = index(p.y, lo.y, cell.y), cz = index(p.z, lo.z, cell.z);
         double best = INFINITY;
         int best_f = -1;
-        double bw[3] = {1, 0, 0};
+        V3 bq{0, 0, 0};
         const double cmin = std::min({cell.x, cell.y, cell.z});
         for (int r = 0; r < n; ++r) {
-            // cells at Chebyshev distance >= r from the query cell are at least (r - 1) * cmin away
             if (best_f >= 0) {
-                const double reach = (r - 1) * cmin;
+                const double reach = (r - 1) * cmin - slack;
                 if (reach > 0 && reach * reach > best) break;
             }
             for (int z = cz - r; z <= cz + r; ++z) {
@@ -179,25 +222,23 @@ struct Grid {
                         const size_t c = id(x, y, z);
                         for (int k = off[c]; k < off[c + 1]; ++k) {
                             const int f = tri[k];
-                            double ww[3];
-                            const double d = closest_on_triangle(p, mesh->pts[mesh->faces[3 * f]],
-                                                                 mesh->pts[mesh->faces[3 * f + 1]],
-                                                                 mesh->pts[mesh->faces[3 * f + 2]], ww);
+                            V3 q;
+                            const double d = locate_on_triangle(p, mesh->pts[mesh->faces[3 * f]],
+                                                                mesh->pts[mesh->faces[3 * f + 1]],
+                                                                mesh->pts[mesh->faces[3 * f + 2]], q);
                             if (d < best || (d == best && f < best_f)) {
                                 best = d;
                                 best_f = f;
-                                bw[0] = ww[0];
-                                bw[1] = ww[1];
-                                bw[2] = ww[2];
+                                bq = q;
                             }
                         }
                     }
                 }
             }
         }
-        w[0] = bw[0];
-        w[1] = bw[1];
-        w[2] = bw[2];
+        if (best_f >= 0)
+            point_weights(bq, mesh->pts[mesh->faces[3 * best_f]], mesh->pts[mesh->faces[3 * best_f + 1]],
+                          mesh->pts[mesh->faces[3 * best_f + 2]], w);
         return best_f;
     }
 };
@@ -224,7 +265,9 @@ int grid_resolution(int n_faces) {
 struct Prepared {
     std::vector<V3> pts;
     double radius = 0.0;
+    V3 centre{0, 0, 0};       // per-axis (min + max) of pts: where the resampling sphere is placed
     std::vector<V3> unit;
+    std::vector<V3> placed;   // centre + radius * unit
     std::shared_ptr<const std::vector<V3>> sheet;  // shared by every build of one sheet size
 };
 
@@ -280,10 +323,18 @@ int prepare(const float* sphere, int n_sphere, const int32_t* sphere_faces, int 
         radius += std::sqrt(dot(out.pts[i], out.pts[i]));
     }
     out.radius = 0.975 * radius / n_sphere;
+    V3 lo = out.pts[0], hi = out.pts[0];
+    for (const V3& p : out.pts) {
+        lo = {std::min(lo.x, p.x), std::min(lo.y, p.y), std::min(lo.z, p.z)};
+        hi = {std::max(hi.x, p.x), std::max(hi.y, p.y), std::max(hi.z, p.z)};
+    }
+    out.centre = lo + hi;
     out.unit.assign(n_points, V3{0, 0, 0});
+    out.placed.assign(n_points, V3{0, 0, 0});
     for (int i = 0; i < n_points; ++i) {
         V3 p{resampling_points[3 * i], resampling_points[3 * i + 1], resampling_points[3 * i + 2]};
         out.unit[i] = (1.0 / std::sqrt(dot(p, p))) * p;
+        out.placed[i] = out.centre + out.radius * out.unit[i];
     }
     out.sheet = sheet_directions(nx, ny);
     return CSG_OK;
@@ -301,12 +352,12 @@ void write_unit_points(const Prepared& prep, float* unit_points_out) {
 
 // ------------------------------------------------------------ device builder
 //
-// The same exact closest-point queries on the GPU: one thread per query,
-// the host's shell search over a uniform grid (built on the device: bounding
-// box by min/max reduction, per-cell counts by atomics, a two-level scan, and
-// an atomic fill whose in-cell order does not matter because the search is
-// exact and breaks ties by the lowest triangle index).  Results are
-// bit-identical to the host builder.
+// The same closest-polygon queries on the GPU: one thread per query, the
+// host's shell search over a uniform grid (built on the device: bounding box
+// by min/max reduction, per-cell counts by atomics, a two-level scan, and an
+// atomic fill whose in-cell order does not matter because the search visits
+// every triangle that can win and breaks ties by the lowest triangle index).
+// Results are bit-identical to the host builder.
 
 constexpr int kScanBlock = 1024;
 
@@ -314,6 +365,7 @@ struct GridParams {
     double lo[3];
     double cell[3];
     double cmin;
+    double slack;  // an upper bound on the mesh's tolerance_reach
 };
 
 __device__ __forceinline__ int cell_index(double v, double o, double c, int n) {
@@ -326,7 +378,8 @@ __device__ __forceinline__ V3 load_point(const double* pts, int i) {
 }
 
 // Bounding box of the points padded like Grid::build, then the cell sizes.
-__global__ void k_grid_box(const double* __restrict__ pts, int n_pts, int res, GridParams* __restrict__ gp) {
+__global__ void k_grid_box(const double* __restrict__ pts, int n_pts, int res, double slack,
+                           GridParams* __restrict__ gp) {
     __shared__ double lo_s[3][kScanBlock], hi_s[3][kScanBlock];
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int i = threadIdx.x; i < n_pts; i += blockDim.x)
@@ -356,6 +409,7 @@ __global__ void k_grid_box(const double* __restrict__ pts, int n_pts, int res, G
             gp->cell[k] = ((hi_s[k][0] + pad) - gp->lo[k]) / res;
         }
         gp->cmin = fmin(fmin(gp->cell[0], gp->cell[1]), gp->cell[2]);
+        gp->slack = slack;
     }
 }
 
@@ -459,18 +513,19 @@ struct DevMesh {
     int res;
 };
 
-// Grid::closest on the device: exact closest triangle, lowest index on ties.
-__device__ int closest_device(const DevMesh& m, V3 p, double w[3]) {
+// Grid::locate on the device: the triangle the closest-polygon rule picks
+// (lowest index on ties) and the weights of its candidate point.
+__device__ int locate_device(const DevMesh& m, V3 p, double w[3]) {
     const GridParams g = *m.gp;
     const int n = m.res;
     const int cx = cell_index(p.x, g.lo[0], g.cell[0], n), cy = cell_index(p.y, g.lo[1], g.cell[1], n),
               cz = cell_index(p.z, g.lo[2], g.cell[2], n);
     double best = INFINITY;
     int best_f = -1;
-    double bw[3] = {1, 0, 0};
+    V3 bq{0, 0, 0};
     for (int r = 0; r < n; ++r) {
         if (best_f >= 0) {
-            const double reach = (r - 1) * g.cmin;
+            const double reach = (r - 1) * g.cmin - g.slack;
             if (reach > 0 && reach * reach > best) break;
         }
         for (int z = cz - r; z <= cz + r; ++z) {
@@ -484,41 +539,37 @@ __device__ int closest_device(const DevMesh& m, V3 p, double w[3]) {
                     const int k1 = __ldg(m.off + c + 1);
                     for (int k = __ldg(m.off + c); k < k1; ++k) {
                         const int f = __ldg(m.tri + k);
-                        double ww[3];
-                        const double d = closest_on_triangle(p, load_point(m.pts, __ldg(m.faces + 3 * f)),
-                                                             load_point(m.pts, __ldg(m.faces + 3 * f + 1)),
-                                                             load_point(m.pts, __ldg(m.faces + 3 * f + 2)), ww);
+                        V3 q;
+                        const double d = locate_on_triangle(p, load_point(m.pts, __ldg(m.faces + 3 * f)),
+                                                            load_point(m.pts, __ldg(m.faces + 3 * f + 1)),
+                                                            load_point(m.pts, __ldg(m.faces + 3 * f + 2)), q);
                         if (d < best || (d == best && f < best_f)) {
                             best = d;
                             best_f = f;
-                            bw[0] = ww[0];
-                            bw[1] = ww[1];
-                            bw[2] = ww[2];
+                            bq = q;
                         }
                     }
                 }
             }
         }
     }
-    w[0] = bw[0];
-    w[1] = bw[1];
-    w[2] = bw[2];
+    if (best_f >= 0)
+        point_weights(bq, load_point(m.pts, __ldg(m.faces + 3 * best_f)),
+                      load_point(m.pts, __ldg(m.faces + 3 * best_f + 1)),
+                      load_point(m.pts, __ldg(m.faces + 3 * best_f + 2)), w);
     return best_f;
 }
 
 // flag: 1 = a grid overflowed its capacity, 2 = a query found no triangle
 // (non-finite input); later kernels skip their work once it is set.
-__global__ void k_stencil_points(DevMesh in, const double* __restrict__ unit, int n_points, double radius,
-                                 int* __restrict__ flag, double* __restrict__ sphere_points,
-                                 double* __restrict__ unit_sphere, int* __restrict__ sidx, double* __restrict__ sw) {
+__global__ void k_stencil_points(DevMesh in, const double* __restrict__ placed, int n_points, int* __restrict__ flag,
+                                 double* __restrict__ sphere_points, double* __restrict__ unit_sphere,
+                                 int* __restrict__ sidx, double* __restrict__ sw) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_points || *flag) return;
-    const V3 u = load_point(unit, i);
     double w[3];
-    const int f = closest_device(in, u, w);
-    double w2[3];
-    const int f2 = closest_device(in, radius * u, w2);
-    if (f < 0 || f2 < 0) {
+    const int f = locate_device(in, load_point(placed, i), w);
+    if (f < 0) {
         atomicExch(flag, 2);
         return;
     }
@@ -532,8 +583,8 @@ __global__ void k_stencil_points(DevMesh in, const double* __restrict__ unit, in
     unit_sphere[3 * i + 1] = un.y;
     unit_sphere[3 * i + 2] = un.z;
     for (int k = 0; k < 3; ++k) {
-        sidx[3 * i + k] = in.faces[3 * f2 + k];
-        sw[3 * i + k] = w2[k];
+        sidx[3 * i + k] = t[k];
+        sw[3 * i + k] = w[k];
     }
 }
 
@@ -542,7 +593,7 @@ __global__ void k_stencil_sheet(DevMesh us, const double* __restrict__ sheet, in
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_cells || *flag) return;
     double w[3];
-    const int f = closest_device(us, load_point(sheet, i), w);
+    const int f = locate_device(us, load_point(sheet, i), w);
     if (f < 0) {
         atomicExch(flag, 2);
         return;
@@ -602,14 +653,14 @@ DeviceLayout layout(int n_sphere, int n_sphere_faces, int n_points, int n_faces,
 }
 
 int build_grid_device(char* base, const double* pts, int n_pts, const int* faces, int n_faces, int res,
-                      size_t gp_at, size_t off_at, size_t cur_at, size_t tri_at, long long cap, size_t sums_at,
-                      size_t flag_at, cudaStream_t s) {
+                      double slack, size_t gp_at, size_t off_at, size_t cur_at, size_t tri_at, long long cap,
+                      size_t sums_at, size_t flag_at, cudaStream_t s) {
     const size_t cells = static_cast<size_t>(res) * res * res;
     GridParams* gp = reinterpret_cast<GridParams*>(base + gp_at);
     int* off = reinterpret_cast<int*>(base + off_at);
     int* cur = reinterpret_cast<int*>(base + cur_at);
     int* sums = reinterpret_cast<int*>(base + sums_at);
-    (csg::note_launch(), k_grid_box<<<1, kScanBlock, 0, s>>>(pts, n_pts, res, gp));
+    (csg::note_launch(), k_grid_box<<<1, kScanBlock, 0, s>>>(pts, n_pts, res, slack, gp));
     CSG_CUDA_CHECK(cudaMemsetAsync(off, 0, 4 * (cells + 1), s));
     const unsigned fb = static_cast<unsigned>((n_faces + 255) / 256);
     (csg::note_launch(), k_grid_count<<<fb, 256, 0, s>>>(pts, faces, n_faces, gp, res, off));
@@ -643,10 +694,10 @@ extern "C" int csg_stencil_build(const float* sphere, int n_sphere, const int32_
     Mesh in{prep.pts, sphere_faces, n_sphere_faces};
     Grid gin;
     gin.build(in, grid_resolution(n_sphere_faces));
-    // sphere points: resampling-sphere directions moved onto the input sphere
+    // surface barycentrics of each placed resampling point, and the input sphere interpolated there
     parallel_for(n_points, threads, [&](int i) {
         double w[3];
-        const int f = gin.closest(prep.unit[i], w);
+        const int f = gin.locate(prep.placed[i], w);
         if (f < 0) {
             failed = 1;
             return;
@@ -656,16 +707,9 @@ extern "C" int csg_stencil_build(const float* sphere, int n_sphere, const int32_
         sphere_points_out[3 * i] = q.x;
         sphere_points_out[3 * i + 1] = q.y;
         sphere_points_out[3 * i + 2] = q.z;
-        // surface barycentrics of the resampling point at 0.975 x the mean radius
-        double w2[3];
-        const int f2 = gin.closest(prep.radius * prep.unit[i], w2);
-        if (f2 < 0) {
-            failed = 1;
-            return;
-        }
         for (int k = 0; k < 3; ++k) {
-            surface_indices_out[3 * i + k] = sphere_faces[3 * f2 + k];
-            surface_weights_out[3 * i + k] = w2[k];
+            surface_indices_out[3 * i + k] = t[k];
+            surface_weights_out[3 * i + k] = w[k];
         }
     });
     // sheet: cell centres on the unit-normalised sphere points
@@ -679,7 +723,7 @@ extern "C" int csg_stencil_build(const float* sphere, int n_sphere, const int32_
     gus.build(us, grid_resolution(n_faces));
     parallel_for(nx * ny, threads, [&](int cellid) {
         double w[3];
-        const int f = gus.closest((*prep.sheet)[cellid], w);
+        const int f = gus.locate((*prep.sheet)[cellid], w);
         if (f < 0) {
             failed = 1;
             return;
@@ -721,7 +765,7 @@ extern "C" int csg_stencil_build_device(const float* sphere, int n_sphere, const
     const int cells = nx * ny;
     CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.in_pts, prep.pts.data(), 24ULL * n_sphere, cudaMemcpyHostToDevice, s));
     CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.in_faces, sphere_faces, 12ULL * n_sphere_faces, cudaMemcpyHostToDevice, s));
-    CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.unit, prep.unit.data(), 24ULL * n_points, cudaMemcpyHostToDevice, s));
+    CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.unit, prep.placed.data(), 24ULL * n_points, cudaMemcpyHostToDevice, s));
     CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.r_faces, resampling_faces, 12ULL * n_faces, cudaMemcpyHostToDevice, s));
     CSG_CUDA_CHECK(cudaMemcpyAsync(base + L.sheet, prep.sheet->data(), 24ULL * cells, cudaMemcpyHostToDevice, s));
     CSG_CUDA_CHECK(cudaMemsetAsync(base + L.flag, 0, sizeof(int), s));
@@ -730,7 +774,10 @@ extern "C" int csg_stencil_build_device(const float* sphere, int n_sphere, const
     const int* in_faces = reinterpret_cast<const int*>(base + L.in_faces);
     const int* r_faces = reinterpret_cast<const int*>(base + L.r_faces);
     int* flag = reinterpret_cast<int*>(base + L.flag);
-    rc = build_grid_device(base, in_pts, n_sphere, in_faces, n_sphere_faces, res_a, L.gp_a, L.off_a, L.cur_a, L.tri_a,
+    // the sheet mesh (the unit-normalised sphere points) is built on the device: bound its tolerance
+    // reach by four times that of the unit resampling directions it stays close to
+    rc = build_grid_device(base, in_pts, n_sphere, in_faces, n_sphere_faces, res_a,
+                           tolerance_reach(prep.pts, sphere_faces, n_sphere_faces), L.gp_a, L.off_a, L.cur_a, L.tri_a,
                            L.cap_a, L.sums, L.flag, s);
     if (rc) return rc;
     DevMesh in{in_pts, in_faces, reinterpret_cast<const int*>(base + L.off_a),
@@ -739,10 +786,11 @@ extern "C" int csg_stencil_build_device(const float* sphere, int n_sphere, const
     double* us = reinterpret_cast<double*>(base + L.us);
     CSG_CUDA_CHECK(cudaMemsetAsync(us, 0, 24ULL * n_points, s));
     (csg::note_launch(), k_stencil_points<<<(n_points + 127) / 128, 128, 0, s>>>(
-        in, reinterpret_cast<const double*>(base + L.unit), n_points, prep.radius, flag, sp, us,
+        in, reinterpret_cast<const double*>(base + L.unit), n_points, flag, sp, us,
         reinterpret_cast<int*>(base + L.sidx), reinterpret_cast<double*>(base + L.sw)));
-    rc = build_grid_device(base, us, n_points, r_faces, n_faces, res_b, L.gp_b, L.off_b, L.cur_b, L.tri_b, L.cap_b,
-                           L.sums, L.flag, s);
+    rc = build_grid_device(base, us, n_points, r_faces, n_faces, res_b,
+                           4.0 * tolerance_reach(prep.unit, resampling_faces, n_faces), L.gp_b, L.off_b, L.cur_b,
+                           L.tri_b, L.cap_b, L.sums, L.flag, s);
     if (rc) return rc;
     DevMesh um{us, r_faces, reinterpret_cast<const int*>(base + L.off_b), reinterpret_cast<const int*>(base + L.tri_b),
                reinterpret_cast<const GridParams*>(base + L.gp_b), res_b};

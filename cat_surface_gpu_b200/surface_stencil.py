@@ -208,14 +208,63 @@ class SurfaceStencilDevice:
 
 _RESAMPLING_SPHERES: dict[int, tuple[np.ndarray, np.ndarray]] = {}
 
+# The base icosahedron of the resampling sphere, in the vertex and face order
+# of the upstream tetrahedral sphere the stencil helper builds
+# (create_tetrahedral_sphere, called at native/cat_surface_stencil_builder.c:
+# 406-421): vertices (+-a, +-b, 0), (0, +-a, +-b), (+-b, 0, +-a) with
+# a = phi / sqrt(1 + phi^2), b = 1 / sqrt(1 + phi^2) (phi the golden ratio).
+# The order of vertices and faces is the helper's, read off the face list of
+# its stencil files; the subdivision below then reproduces that face list
+# exactly, so stencils index the same resampling points as the helper's.
+_ICOSA_A = 0.85065080835203993  # phi / sqrt(1 + phi^2)
+_ICOSA_B = 0.52573111211913359  # 1 / sqrt(1 + phi^2)
+_ICOSA_SIGNS = ((1, 1, 0), (1, -1, 0), (-1, 1, 0), (-1, -1, 0), (0, 1, 1), (0, 1, -1), (0, -1, 1), (0, -1, -1),
+                (1, 0, 1), (-1, 0, 1), (1, 0, -1), (-1, 0, -1))
+_ICOSA_FACES = ((2, 11, 3), (2, 5, 11), (11, 5, 10), (5, 0, 10), (0, 5, 4), (4, 5, 2), (4, 2, 9), (9, 2, 3),
+                (9, 3, 6), (9, 6, 8), (4, 9, 8), (4, 8, 0), (0, 8, 1), (1, 8, 6), (1, 6, 7), (7, 6, 3),
+                (11, 7, 3), (11, 10, 7), (10, 1, 7), (10, 0, 1))
+
+
+def tetrahedral_sphere(subdivisions: int = 6) -> tuple[np.ndarray, np.ndarray]:
+    """Unit sphere of 20 * 4^subdivisions triangles in the upstream tetrahedral-sphere order.
+
+    Each level splits every triangle (a, b, c), in face order, into
+    (a, ab, ca), (ab, b, bc), (ca, ab, bc), (ca, bc, c); a new edge midpoint
+    takes the next vertex number the first time its edge is met (edges
+    visited ab, bc, ca) and is the normalised sum of its end points.  Six
+    levels give the helper's 40,962 points and 81,920 faces.
+    """
+
+    if subdivisions < 0:
+        raise ValueError("subdivisions must be non-negative")
+    a, b = _ICOSA_A, _ICOSA_B
+    points = np.array([(sx * a, sy * b, 0.0) if i < 4 else (0.0, sy * a, sz * b) if i < 8 else (sx * b, 0.0, sz * a)
+                       for i, (sx, sy, sz) in enumerate(_ICOSA_SIGNS)], dtype=np.float64)
+    faces = np.array(_ICOSA_FACES, dtype=np.int64)
+    for _ in range(int(subdivisions)):
+        nf = faces.shape[0]
+        ends = np.stack((faces, np.roll(faces, -1, axis=1)), axis=2).reshape(3 * nf, 2)  # ab, bc, ca per face
+        keys = np.sort(ends, axis=1)
+        unique, first, inverse = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+        rank = np.empty(unique.shape[0], dtype=np.int64)
+        rank[np.argsort(first, kind="stable")] = np.arange(unique.shape[0])
+        mids = points.shape[0] + rank[inverse.reshape(-1)].reshape(nf, 3)
+        summed = points[unique[:, 0]] + points[unique[:, 1]]
+        new_points = np.empty_like(summed)
+        new_points[rank] = summed / np.sqrt((summed * summed).sum(axis=1, keepdims=True))
+        ab, bc, ca = mids[:, 0], mids[:, 1], mids[:, 2]
+        fa, fb, fc = faces[:, 0], faces[:, 1], faces[:, 2]
+        faces = np.stack((np.stack((fa, ab, ca), 1), np.stack((ab, fb, bc), 1), np.stack((ca, ab, bc), 1),
+                          np.stack((ca, bc, fc), 1)), axis=1).reshape(4 * nf, 3)
+        points = np.concatenate((points, new_points), axis=0)
+    return points, faces.astype(np.int32)
+
 
 def resampling_sphere(subdivisions: int = 6) -> tuple[np.ndarray, np.ndarray]:
-    """Unit icosphere used as the resampling sphere (6 subdivisions: 40,962 points / 81,920 triangles)."""
+    """The stencil helper's resampling sphere: :func:`tetrahedral_sphere` (6: 40,962 points / 81,920 triangles)."""
 
     if subdivisions not in _RESAMPLING_SPHERES:
-        from .synthetic import unit_icosphere
-
-        points, faces = unit_icosphere(subdivisions)
+        points, faces = tetrahedral_sphere(subdivisions)
         points = np.array(points, dtype=np.float64, order="C")
         faces = np.array(faces, dtype=np.int32, order="C")
         # shared by every stencil of this resolution (lookups key on the array itself): read-only
@@ -229,13 +278,18 @@ def build_surface_stencil(sphere_vertices, sphere_faces, *, nx: int = 512, ny: i
                           subdivisions: int = 6, threads: int = 0, device=None) -> SurfaceStencil:
     """Build a resampling stencil for a sphere mesh.
 
-    Same contents as the reference's stencil helper (``--surface`` mode: the
-    surface shares the sphere's topology, so surface indices are sphere
-    vertex ids).  ``normalize=False`` matches the helper's
-    ``--no-normalize`` (for spheres that are already unit and centred).
-    With a CUDA ``device`` the closest-point queries run on that GPU
-    (``csg_stencil_build_device``); otherwise the threaded host builder
-    (``csg_stencil_build``).  Both give bit-identical stencils.
+    The reference's stencil helper (``native/cat_surface_stencil_builder.c``;
+    ``--surface`` mode: the surface shares the sphere's topology, so surface
+    indices are sphere vertex ids), restated in float64: the helper's
+    tetrahedral resampling sphere placed at the per-axis (min + max) centre
+    with 0.975 x the mean radius, its closest-polygon rule, the resampled
+    sphere and the sheet of the cell centres.  It equals the helper's files
+    up to the helper's own float32 rounding (``tests/test_stencil_helper.py``)
+    and writes any sheet size, not only the helper's 512 x 256.
+    ``normalize=False`` matches the helper's ``--no-normalize`` (for spheres
+    that are already unit and centred).  With a CUDA ``device`` the queries
+    run on that GPU (``csg_stencil_build_device``); otherwise the threaded
+    host builder (``csg_stencil_build``).  Both give bit-identical stencils.
     """
 
     from . import _native

@@ -499,13 +499,17 @@ CSG_API int csg_feature_minmax(int n, int series, const double *values, double *
 /* ------------------------------------------------------------------------
  * SurfWarp: resampling stencils (host, float64, threaded, deterministic).
  * Replaces the reference's stencil helper
- * (native/cat_surface_stencil_builder.c:172-464) with the same outputs:
- * sphere points (the resampling sphere moved onto the input sphere),
- * surface barycentrics of the resampling sphere scaled to 0.975 x the mean
- * input radius, sheet barycentrics of the nx x ny cell centres on the
- * unit-normalised sphere points, and unit-sphere points of the input
- * vertices.  The resampling sphere (points + faces) is the caller's; closest
- * points are exact (lowest triangle index on ties).  normalize centres the
+ * (native/cat_surface_stencil_builder.c:107-170, 355-464) with the same
+ * outputs: the resampling sphere's unit directions placed at
+ * centre + r u (centre = per-axis min + max of the input points, r = 0.975 x
+ * their mean length); surface barycentrics of each placed point under the
+ * helper's closest-polygon rule (plane projection accepted within a 1e-3
+ * parametric tolerance, else the nearer edge at the triangle's nearest
+ * vertex; smallest candidate distance, lowest triangle index on ties); the
+ * sphere points (the input interpolated there); sheet barycentrics of the
+ * nx x ny cell centres on the unit-normalised sphere points; unit-sphere
+ * points of the input vertices.  The resampling sphere (points + faces) is
+ * the caller's (the helper's is 81,920 triangles).  normalize centres the
  * input on its vertex mean and projects it to unit length first. */
 CSG_API int csg_stencil_build(const float *sphere, int n_sphere, const int32_t *sphere_faces, int n_sphere_faces,
                               const double *resampling_points, int n_points, const int32_t *resampling_faces,

@@ -25,7 +25,10 @@ os.environ.setdefault("PYTHONDONTWRITEBYTECODE", "1")
 sys.dont_write_bytecode = True
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
-sys.path.insert(0, "/root/reference/src")
+sys.path.insert(0, str(HERE))
+from _reference import use_reference_package  # noqa: E402
+
+use_reference_package()
 
 import torch  # noqa: E402
 

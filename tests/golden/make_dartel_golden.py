@@ -1,7 +1,7 @@
 """Generate DARTEL / warp golden vectors by running the reference package on CPU.
 
 Runs in the development container only: it imports ``cat_surface_gpu`` from
-the reference checkout (``/root/reference/src``) and evaluates its torch CPU
+the reference checkout (``$CAT_SURFACE_REFERENCE/src``) and evaluates its torch CPU
 path on seeded small grids.  The committed ``dartel_golden.npz`` holds every
 input and output, so tests never need the reference at run time.
 
@@ -18,8 +18,10 @@ import numpy as np
 
 os.environ.setdefault("PYTHONDONTWRITEBYTECODE", "1")
 sys.dont_write_bytecode = True
-REFERENCE_SRC = Path("/root/reference/src")
-sys.path.insert(0, str(REFERENCE_SRC))
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+from _reference import use_reference_package  # noqa: E402
+
+REFERENCE_SRC = use_reference_package()
 
 import torch  # noqa: E402
 

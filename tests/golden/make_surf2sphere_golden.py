@@ -35,7 +35,10 @@ from cat_surface_gpu_b200 import synthetic  # noqa: E402
 from cat_surface_gpu_b200.gifti import GiftiMesh, read_gifti_mesh, write_gifti_mesh  # noqa: E402
 from cat_surface_gpu_b200.surf2sphere import surface_area  # noqa: E402
 
-BINARY = Path("/root/reference/bin/linux-x86_64/CAT_Surf2Sphere")
+sys.path.insert(0, str(HERE))
+from _reference import reference_binary  # noqa: E402
+
+BINARY = reference_binary("CAT_Surf2Sphere")
 
 CASES = {
     # folded icosphere, subdivision 5: 10,242 vertices / 20,480 faces, 60 mm

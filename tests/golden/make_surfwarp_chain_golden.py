@@ -2,8 +2,12 @@
 
 Development container only (imports ``cat_surface_gpu`` from the reference
 checkout).  Follows ``src/cat_surface_gpu/gpu_pipeline.py:468-1326`` step by
-step with the reference's own operators on the CPU: stencils (built by this
-package's native host builder, read back through the reference's reader),
+step with the reference's own operators on the CPU: stencils written by the
+reference's own helper (``bin/linux-x86_64/cat_surface_stencil_builder``,
+executed; read back through the reference's reader -- the helper's sheet is
+fixed at 512 x 256, so for other sheet sizes the sheet part is the oracle's
+restatement of the helper's sheet, ``oracle/stencil.py``, pinned to the helper
+by ``tests/test_stencil_helper.py``),
 rotation features (the reference's default "cuda" backend:
 ``compute_rotation_features`` -- the depth potential by coloured SOR of the
 smoothed coarse surfaces at FWHM 15 / 10 -- run on the CPU), the 46-seed +
@@ -16,7 +20,8 @@ icosphere under a known rotation, scaled to radius 100.  Writes
 ``surfwarp_chain_golden.npz`` (inputs, parameters, rotation features, the
 type-5 curvature features of this package's "native-curvature" option,
 rotation angle/cost, the rotated sphere, the sphere after run 0, the final
-sphere).
+sphere; and both feature kinds recomputed by the reference on this package's
+own stencils of the two spheres, ``builder_*``).
 
 ``--workload hemisphere`` instead runs the 61,442-vertex hemisphere chain of
 the benchmark: source = the ``surf2sphere_c2`` surface with the upstream
@@ -32,8 +37,10 @@ Usage: ``python tests/golden/make_surfwarp_chain_golden.py [--workload small|hem
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import os
 from pathlib import Path
+import subprocess
 import sys
 import tempfile
 import time
@@ -44,7 +51,11 @@ os.environ.setdefault("PYTHONDONTWRITEBYTECODE", "1")
 sys.dont_write_bytecode = True
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
-sys.path.insert(0, "/root/reference/src")
+sys.path.insert(0, str(HERE))
+from _reference import reference_binary, use_reference_package  # noqa: E402
+
+use_reference_package()
+HELPER = reference_binary("cat_surface_stencil_builder")
 
 import torch  # noqa: E402
 
@@ -56,7 +67,9 @@ from cat_surface_gpu.surface_stencil import SurfaceStencil as ReferenceStencil  
 from cat_surface_gpu.surface_warp import apply_flow_to_stenciled_sphere, solve_dartel_from_surfaces  # noqa: E402
 
 from cat_surface_gpu_b200 import synthetic  # noqa: E402
-from cat_surface_gpu_b200.surface_stencil import build_surface_stencil  # noqa: E402
+from cat_surface_gpu_b200.gifti import GiftiMesh, write_gifti_mesh  # noqa: E402
+from cat_surface_gpu_b200.surface_stencil import SurfaceStencil  # noqa: E402
+from oracle import stencil as oracle_stencil  # noqa: E402
 
 PARAMS = dict(nx=128, ny=64, steps=2, runs=2, avg=True, loop=6, rotation_grid_size=128)
 CPU = torch.device("cpu")
@@ -93,10 +106,21 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size, ta
     count = [0]
 
     def stencil(sphere, normalize, faces=None):
+        """The helper's stencil of this sphere (the reference pipeline's call, gpu_pipeline.py:144-166)."""
+
         count[0] += 1
-        path = temp / f"s{count[0]}.stencil"
+        mesh_path, path = temp / f"s{count[0]}.gii", temp / f"s{count[0]}.stencil"
         faces = source_faces if faces is None else faces
-        build_surface_stencil(sphere, faces, nx=nx, ny=ny, normalize=normalize).to_file(path)
+        write_gifti_mesh(mesh_path, GiftiMesh(np.asarray(sphere, dtype=np.float32), faces))
+        command = [str(HELPER), str(mesh_path), str(path), "--threads", "8"]
+        if not normalize:
+            command.insert(3, "--no-normalize")
+        subprocess.run(command, check=True, capture_output=True)
+        if (nx, ny) != (512, 256):
+            written = SurfaceStencil.from_file(path)
+            sheet_indices, sheet_weights = oracle_stencil.sheet_stencil(written.sphere_points, written.faces, nx, ny)
+            dataclasses.replace(written, sheet_indices=sheet_indices, sheet_weights=sheet_weights, nx=nx,
+                                ny=ny).to_file(path)
         return ReferenceStencil.from_file(path)
 
     def on_cpu(st):
@@ -178,6 +202,30 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size, ta
                 rotated_initial=rotated_initial, after_run0=after_run0, final_sphere=current_sphere)
 
 
+def builder_features(data, nx, ny):
+    """The reference's rotation and curvature features on this package's own stencils of the two spheres.
+
+    Pins the feature operators on identical inputs (the chain itself uses the
+    helper's stencils, which this package's builder matches to the helper's
+    float32 rounding only).
+    """
+
+    from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+    temp = Path(tempfile.mkdtemp(prefix="chain_builder_"))
+    stencils = []
+    for side in ("source", "target"):
+        build_surface_stencil(data[f"{side}_sphere"], data["faces"], nx=nx, ny=ny, normalize=True).to_file(
+            temp / f"{side}.stencil")
+        stencils.append(ReferenceStencil.from_file(temp / f"{side}.stencil").to(CPU, geometry_dtype=torch.float32))
+    surfaces = (torch.as_tensor(data["source_surface"]), torch.as_tensor(data["target_surface"]))
+    features = compute_rotation_features(tuple(stencils), surfaces, heat_fwhms=(15.0, 10.0), solver="colored-sor")
+    curvature = [st.curvature_type5(st.resample_vertices(surface), fwhm).numpy()
+                 for st, surface, fwhm in zip(stencils, surfaces, (15.0, 10.0))]
+    return dict(builder_source_values=features[0].values.numpy(), builder_target_values=features[1].values.numpy(),
+                builder_curv_source_values=curvature[0], builder_curv_target_values=curvature[1])
+
+
 HEMISPHERE_PARAMS = dict(nx=256, ny=128, steps=2, runs=2, avg=True, loop=6, rotation_grid_size=128)
 
 
@@ -204,6 +252,7 @@ def main() -> int:
         started = time.perf_counter()
         result = reference_chain(data, **PARAMS)
         seconds = time.perf_counter() - started
+        result.update(builder_features(data, PARAMS["nx"], PARAMS["ny"]))
         np.savez_compressed(HERE / "surfwarp_chain_golden.npz", **data, **result,
                             **{f"param_{k}": np.asarray(v) for k, v in PARAMS.items()})
     else:

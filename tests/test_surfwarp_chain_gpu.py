@@ -2,12 +2,15 @@
 
 The golden (``tests/golden/make_surfwarp_chain_golden.py``) ran the reference
 package's operators on the CPU in the order of its ``run_cat_surface_gpu_pipeline``:
-native-builder stencils, the default ("cuda") rotation features -- the depth
-potential by coloured SOR, ``compute_rotation_features`` -- the rotation
-search, two DARTEL runs of two steps on a 128 x 64 sheet, the ``-avg`` solve
-and blend.  This runs ``run_cat_surface_gpu_pipeline`` on the same GIFTI
-inputs and bounds the final unit-sphere vertex error at 1e-3 (max), the
-accuracy the Surf2Sphere+SurfWarp chain is quoted at.
+stencils from the reference's own stencil helper (its 128 x 64 sheet from the
+oracle's restatement of the helper's sheet), the default ("cuda") rotation
+features -- the depth potential by coloured SOR, ``compute_rotation_features``
+-- the rotation search, two DARTEL runs of two steps, the ``-avg`` solve and
+blend.  This runs ``run_cat_surface_gpu_pipeline`` (its own GPU-built
+stencils) on the same GIFTI inputs and bounds the final unit-sphere vertex
+error at 1e-3 (max), the accuracy the Surf2Sphere+SurfWarp chain is quoted
+at.  The feature operators are pinned on identical stencils: the golden
+also holds the reference's features on this package's stencils.
 """
 
 from __future__ import annotations
@@ -49,11 +52,11 @@ def test_rotation_features_match_reference(native_library, chain):
     values = depth_rotation_features(stencils[0], stencils[1], chain["source_surface"], chain["target_surface"],
                                      torch.device("cuda:0"), timings=timings)
     assert timings["rotation_feature_source_iterations"] == 1000.0
-    for got, want in zip(values, (chain["source_values"], chain["target_values"])):
+    for got, want in zip(values, (chain["builder_source_values"], chain["builder_target_values"])):
         np.testing.assert_allclose(got.cpu().numpy(), want, rtol=0, atol=1e-12)
     values = native_rotation_features(stencils[0], stencils[1], chain["source_surface"], chain["target_surface"],
                                       torch.device("cuda:0"))
-    for got, want in zip(values, (chain["curv_source_values"], chain["curv_target_values"])):
+    for got, want in zip(values, (chain["builder_curv_source_values"], chain["builder_curv_target_values"])):
         scale = float(np.abs(want).max())
         assert np.abs(got.astype(np.float64) - want).max() <= 1e-5 * scale
 

@@ -119,7 +119,8 @@ def test_stencil_builder_properties(stencil, chain):
     for idx, w, bound in ((stencil.surface_indices, stencil.surface_weights, n_source),
                           (stencil.sheet_indices, stencil.sheet_weights, 40962)):
         assert idx.min() >= 0 and idx.max() < bound
-        assert w.min() >= -1e-9
+        # the closest-polygon rule accepts plane projections up to 1e-3 outside a triangle
+        assert w.min() >= -1.1e-3
         assert np.allclose(w.sum(axis=-1), 1.0, atol=1e-9)
     unit = stencil.unit_sphere_points.astype(np.float64)
     assert np.allclose(np.linalg.norm(unit, axis=1), 1.0, atol=1e-6)
