@@ -17,6 +17,7 @@
 // (surface_warp.py:239-367) as launch sequences on one stream, so a caller
 // can capture a complete solve in one CUDA graph.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -627,6 +628,296 @@ __global__ void __launch_bounds__(kCoarseThreads) k_fmg_coarse_cycle(CoarseCycle
     }
 }
 
+// ------------------------------------------------ fused fine-level V-cycle legs
+//
+// On the fine levels (above kCoarsePoints points) one V-cycle leg used to be
+// 2 nit red-black half-sweep launches plus a residual and a restriction
+// launch going down, and a prolongation plus 2 nit half-sweeps going up.
+// Here each leg of each level is one launch: a CTA copies its tile of the
+// level and a halo into shared memory, runs all the leg's steps there and
+// writes back its tile.  A red-black half-sweep reads only neighbours one
+// step away, so after k half-sweeps the values are exact everywhere at
+// least k cells inside the copied region (the true y edges reflect onto
+// copied rows and x is periodic, so only the region's cut edges shrink);
+// with a halo of 2 nit + 2 the tile and one ring round it hold exact
+// residuals for the restriction taps.  Every point sees the same operands in
+// the same order as in the separate kernels (relax_at, membrane_apply_at,
+// resize_at), so results are bit-identical; halo points are recomputed by
+// neighbouring tiles instead of exchanged.
+
+constexpr int kTileX = 32, kTileY = 16;
+
+struct TileGeom {
+    int x0, x1, y0, y1;  // the tile's interior (global, half-open)
+    int gx0, wx;         // copied columns: gx0 .. gx0 + wx - 1 (unwrapped), or all nx when full_x
+    int gy0, wy;         // copied rows (clipped to the grid)
+    bool full_x;
+};
+
+__device__ __forceinline__ TileGeom tile_geom(int nx, int ny, int halo) {
+    const int tiles_x = (nx + kTileX - 1) / kTileX;
+    TileGeom g;
+    const int tx = static_cast<int>(blockIdx.x) % tiles_x, ty = static_cast<int>(blockIdx.x) / tiles_x;
+    g.x0 = tx * kTileX;
+    g.x1 = min(nx, g.x0 + kTileX);
+    g.y0 = ty * kTileY;
+    g.y1 = min(ny, g.y0 + kTileY);
+    g.full_x = (g.x1 - g.x0) + 2 * halo >= nx;
+    g.gx0 = g.full_x ? 0 : g.x0 - halo;
+    g.wx = g.full_x ? nx : (g.x1 - g.x0) + 2 * halo;
+    g.gy0 = max(0, g.y0 - halo);
+    g.wy = min(ny, g.y1 + halo) - g.gy0;
+    return g;
+}
+
+// Image coordinates of the x neighbour of image column ix (dx = -1 / +1).
+__device__ __forceinline__ int image_x(const TileGeom& g, int ix, int dx, int nx) {
+    return g.full_x ? wrap_x(ix + dx, nx) : ix + dx;
+}
+// Image row of the y neighbour of global row gy (reflected at the grid edges).
+__device__ __forceinline__ int image_y(const TileGeom& g, int gy, int dy, int ny) {
+    return reflect_y(gy + dy, ny) - g.gy0;
+}
+// Whether image point (ix, iy) is exact after `k` steps that each read one cell away.
+__device__ __forceinline__ bool image_valid(const TileGeom& g, int ix, int iy, int k, int ny) {
+    if (!g.full_x && (ix < k || ix >= g.wx - k)) return false;
+    if (g.gy0 > 0 && iy < k) return false;
+    if (g.gy0 + g.wy < ny && iy >= g.wy - k) return false;
+    return true;
+}
+
+template <typename T>
+struct FineImage {
+    T* a;  // [3][wy][wx]
+    T* b;  // [2][wy][wx]
+    T* u;  // [2][wy][wx]
+    int n;  // wx * wy
+};
+
+// Copy A, B and U of batch element bi over the tile's region into shared memory.
+template <typename T>
+__device__ void load_image(const T* __restrict__ A, const T* __restrict__ B, const T* __restrict__ U,
+                           const TileGeom& g, int nx, int ny, int bi, FineImage<T>& im) {
+    const int P = nx * ny;
+    const size_t o1 = static_cast<size_t>(bi) * P;
+    for (int q = threadIdx.x; q < im.n; q += blockDim.x) {
+        const int ix = q % g.wx, iy = q / g.wx;
+        const int gi = (g.gy0 + iy) * nx + wrap_x(g.gx0 + ix, nx);
+        for (int c = 0; c < 3; ++c) im.a[c * im.n + q] = A[3 * o1 + c * P + gi];
+        for (int c = 0; c < 2; ++c) {
+            im.b[c * im.n + q] = B[2 * o1 + c * P + gi];
+            im.u[c * im.n + q] = U[2 * o1 + c * P + gi];
+        }
+    }
+}
+
+// relax_at on the image: one half-sweep of `colour` over the points exact after `k` steps.
+template <typename T>
+__device__ void image_half_sweep(FineImage<T>& im, const TileGeom& g, int nx, int ny, int colour, int k, T w00, T w01,
+                                 T w10) {
+    for (int q = threadIdx.x; q < im.n; q += blockDim.x) {
+        const int ix = q % g.wx, iy = q / g.wx;
+        const int gx = g.gx0 + ix, gy = g.gy0 + iy;
+        if (((gx + gy) & 1) != colour || !image_valid(g, ix, iy, k, ny)) continue;
+        T* ux = im.u;
+        T* uy = im.u + im.n;
+        const int xm = iy * g.wx + image_x(g, ix, -1, nx), xp = iy * g.wx + image_x(g, ix, 1, nx);
+        const int ym = image_y(g, gy, -1, ny) * g.wx + ix, yp = image_y(g, gy, 1, ny) * g.wx + ix;
+        const T rx = im.b[q] - w01 * (ux[ym] + ux[yp]) - w10 * (ux[xm] + ux[xp]);
+        const T ry = im.b[im.n + q] - w01 * (uy[ym] + uy[yp]) - w10 * (uy[xm] + uy[xp]);
+        const T dxx = im.a[q] + w00;
+        const T dyy = im.a[im.n + q] + w00;
+        const T cr = im.a[2 * im.n + q];
+        const T det = dxx * dyy * T(1.0000000001) - cr * cr;
+        const T nxv = (dyy * rx - cr * ry) / det;
+        const T nyv = (-cr * rx + dxx * ry) / det;
+        ux[q] = nxv;
+        uy[q] = nyv;
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ void image_relax(FineImage<T>& im, const TileGeom& g, int nx, int ny, int nit, T w00, T w01, T w10) {
+    for (int it = 0; it < 2 * nit; ++it) image_half_sweep(im, g, nx, ny, it % 2 == 0 ? 1 : 0, it + 1, w00, w01, w10);
+}
+
+template <typename T>
+__device__ void store_tile(const FineImage<T>& im, const TileGeom& g, int nx, int ny, int bi, T* __restrict__ U) {
+    const int P = nx * ny;
+    const size_t o1 = static_cast<size_t>(bi) * P;
+    const int tw = g.x1 - g.x0, th = g.y1 - g.y0;
+    for (int q = threadIdx.x; q < tw * th; q += blockDim.x) {
+        const int gx = g.x0 + q % tw, gy = g.y0 + q / tw;
+        const int iq = (gy - g.gy0) * g.wx + (g.full_x ? gx : gx - g.gx0);
+        U[2 * o1 + gy * nx + gx] = im.u[iq];
+        U[2 * o1 + P + gy * nx + gx] = im.u[im.n + iq];
+    }
+}
+
+// A leg reads the level's solution from Uin and writes its tiles to Uout, a
+// different buffer: tiles of one launch read each other's halos, so none may
+// overwrite what another still reads (down: U -> the level's R buffer; up:
+// R -> U).
+template <typename T>
+struct FineLeg {
+    const T* A;    // this level's Hessian [batch][3][ny][nx]
+    const T* B;    // right-hand side [batch][2][ny][nx]
+    const T* Uin;  // solution before the leg [batch][2][ny][nx]
+    T* Uout;       // solution after the leg
+    int nx, ny;
+    T w00, w01, w10;
+    RegWeights rw;
+    T* nB;  // down: the next coarser level's right-hand side (restricted residual)
+    T* nU;  // down: the next coarser level's solution (zeroed); up: the coarser solution to prolongate
+    int cnx, cny;
+    int nit;
+};
+
+// Down leg of level l: 2 nit half-sweeps, the residual b - (H + L) u and its
+// restriction to level l + 1, whose solution is zeroed.  Halo 2 nit + 2.
+template <typename T>
+__global__ void __launch_bounds__(256) k_vcycle_down(FineLeg<T> L) {
+    csg::pdl_begin();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int bi = blockIdx.y;
+    const TileGeom g = tile_geom(L.nx, L.ny, 2 * L.nit + 2);
+    FineImage<T> im;
+    im.n = g.wx * g.wy;
+    im.a = reinterpret_cast<T*>(smem_raw);
+    im.b = im.a + 3 * im.n;
+    im.u = im.b + 2 * im.n;
+    T* r = im.u + 2 * im.n;  // residual [2][wy][wx]
+    load_image(L.A, L.B, L.Uin, g, L.nx, L.ny, bi, im);
+    __syncthreads();
+    image_relax(im, g, L.nx, L.ny, L.nit, L.w00, L.w01, L.w10);
+    // residual (membrane_apply_at on the image) where it is exact
+    const int kr = 2 * L.nit + 1;
+    const T w00 = T(L.rw.w[0]), w01 = T(L.rw.w[1]), w10 = T(L.rw.w[2]);
+    for (int q = threadIdx.x; q < im.n; q += blockDim.x) {
+        const int ix = q % g.wx, iy = q / g.wx;
+        if (!image_valid(g, ix, iy, kr, L.ny)) continue;
+        const int gy = g.gy0 + iy;
+        const int xm = iy * g.wx + image_x(g, ix, -1, L.nx), xp = iy * g.wx + image_x(g, ix, 1, L.nx);
+        const int ym = image_y(g, gy, -1, L.ny) * g.wx + ix, yp = image_y(g, gy, 1, L.ny) * g.wx + ix;
+        T reg[2];
+        for (int c = 0; c < 2; ++c) {
+            const T* f = im.u + c * im.n;
+            reg[c] = w00 * f[q] + w01 * (f[ym] + f[yp]) + w10 * (f[xm] + f[xp]);
+        }
+        const T u0 = im.u[q], u1 = im.u[im.n + q];
+        const T a0 = reg[0] + im.a[q] * u0 + im.a[2 * im.n + q] * u1;
+        const T a1 = reg[1] + im.a[2 * im.n + q] * u0 + im.a[im.n + q] * u1;
+        r[q] = im.b[q] - a0;
+        r[im.n + q] = im.b[im.n + q] - a1;
+    }
+    __syncthreads();
+    store_tile(im, g, L.nx, L.ny, bi, L.Uout);
+    // restriction (resize_at) of the residual to the coarse points whose centre tap lies in this tile
+    const int snx = L.nx, sny = L.ny, tnx = L.cnx, tny = L.cny;
+    const int X0 = max(0, (g.x0 - 2) * tnx / snx - 1), X1 = min(tnx, (g.x1 + 2) * tnx / snx + 2);
+    const int Y0 = max(0, (g.y0 - 2) * tny / sny - 1), Y1 = min(tny, (g.y1 + 2) * tny / sny + 2);
+    const int cw = X1 - X0, ch = Y1 - Y0;
+    const size_t cP = static_cast<size_t>(tnx) * tny;
+    for (int q = threadIdx.x; q < cw * ch; q += blockDim.x) {
+        const int X = X0 + q % cw, Y = Y0 + q / cw;
+        const T yl = (static_cast<T>(Y) + T(0.5)) * static_cast<T>(sny) / static_cast<T>(tny) - T(0.5);
+        const int yo = static_cast<int>(floor(yl + T(0.5)));
+        const T xl = (static_cast<T>(X) + T(0.5)) * static_cast<T>(snx) / static_cast<T>(tnx) - T(0.5);
+        const int xo = static_cast<int>(floor(xl + T(0.5)));
+        const int oy = reflect_y(yo, sny), ox = wrap_x(xo, snx);
+        if (oy < g.y0 || oy >= g.y1 || ox < g.x0 || ox >= g.x1) continue;  // another tile's coarse point
+        const T yof = static_cast<T>(yo);
+        const T yw = wt2(yof - yl), ywm = wt2(yof - T(1) - yl), ywp = wt2(yof + T(1) - yl);
+        const T xof = static_cast<T>(xo);
+        const T xw = wt2(xof - xl), xwm = wt2(xof - T(1) - xl), xwp = wt2(xof + T(1) - xl);
+        const int rm = (reflect_y(yo - 1, sny) - g.gy0) * g.wx, rc = (reflect_y(yo, sny) - g.gy0) * g.wx,
+                  rp = (reflect_y(yo + 1, sny) - g.gy0) * g.wx;
+        auto col = [&](int x) { return g.full_x ? wrap_x(x, snx) : wrap_x(x - g.gx0, snx); };
+        const int cm = col(xo - 1), cc = col(xo), cp = col(xo + 1);
+        for (int c = 0; c < 2; ++c) {
+            const T* f = r + c * im.n;
+            const T vm = ywm * f[rm + cm] + yw * f[rc + cm] + ywp * f[rp + cm];
+            const T vc = ywm * f[rm + cc] + yw * f[rc + cc] + ywp * f[rp + cc];
+            const T vp = ywm * f[rm + cp] + yw * f[rc + cp] + ywp * f[rp + cp];
+            const size_t o = (2 * static_cast<size_t>(bi) + c) * cP + static_cast<size_t>(Y) * tnx + X;
+            L.nB[o] = xwm * vm + xw * vc + xwp * vp;
+            L.nU[o] = T(0);
+        }
+    }
+}
+
+// Up leg of level l: u += prolongation of the coarser solution (resize_at,
+// accumulate), then 2 nit half-sweeps.  Halo 2 nit.
+template <typename T>
+__global__ void __launch_bounds__(256) k_vcycle_up(FineLeg<T> L) {
+    csg::pdl_begin();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int bi = blockIdx.y;
+    const TileGeom g = tile_geom(L.nx, L.ny, 2 * L.nit);
+    FineImage<T> im;
+    im.n = g.wx * g.wy;
+    im.a = reinterpret_cast<T*>(smem_raw);
+    im.b = im.a + 3 * im.n;
+    im.u = im.b + 2 * im.n;
+    load_image(L.A, L.B, L.Uin, g, L.nx, L.ny, bi, im);
+    for (int q = threadIdx.x; q < im.n; q += blockDim.x) {
+        const int ix = q % g.wx, iy = q / g.wx;
+        const int i = (g.gy0 + iy) * L.nx + wrap_x(g.gx0 + ix, L.nx);
+        for (int c = 0; c < 2; ++c) {
+            const int plane = 2 * bi + c;
+            const T* src = L.nU + static_cast<size_t>(plane) * L.cnx * L.cny;
+            const int x = i % L.nx, y = i / L.nx;
+            const T yl = (static_cast<T>(y) + T(0.5)) * static_cast<T>(L.cny) / static_cast<T>(L.ny) - T(0.5);
+            const int yo = static_cast<int>(floor(yl + T(0.5)));
+            const T yof = static_cast<T>(yo);
+            const T yw = wt2(yof - yl), ywm = wt2(yof - T(1) - yl), ywp = wt2(yof + T(1) - yl);
+            const int rm = reflect_y(yo - 1, L.cny) * L.cnx, rc = reflect_y(yo, L.cny) * L.cnx,
+                      rp = reflect_y(yo + 1, L.cny) * L.cnx;
+            const T xl = (static_cast<T>(x) + T(0.5)) * static_cast<T>(L.cnx) / static_cast<T>(L.nx) - T(0.5);
+            const int xo = static_cast<int>(floor(xl + T(0.5)));
+            const T xof = static_cast<T>(xo);
+            const T xw = wt2(xof - xl), xwm = wt2(xof - T(1) - xl), xwp = wt2(xof + T(1) - xl);
+            const int cm = wrap_x(xo - 1, L.cnx), cc = wrap_x(xo, L.cnx), cp = wrap_x(xo + 1, L.cnx);
+            const T vm = ywm * src[rm + cm] + yw * src[rc + cm] + ywp * src[rp + cm];
+            const T vc = ywm * src[rm + cc] + yw * src[rc + cc] + ywp * src[rp + cc];
+            const T vp = ywm * src[rm + cp] + yw * src[rc + cp] + ywp * src[rp + cp];
+            const T v = xwm * vm + xw * vc + xwp * vp;
+            im.u[c * im.n + q] = im.u[c * im.n + q] + v;
+        }
+    }
+    __syncthreads();
+    image_relax(im, g, L.nx, L.ny, L.nit, L.w00, L.w01, L.w10);
+    store_tile(im, g, L.nx, L.ny, bi, L.Uout);
+}
+
+// Shared memory of one leg launch: A, B, U (+ the residual going down) over the largest tile region.
+template <typename T>
+size_t leg_smem(int nx, int ny, int halo, bool down) {
+    const int tw = std::min(kTileX, nx), th = std::min(kTileY, ny);
+    const int wx = tw + 2 * halo >= nx ? nx : tw + 2 * halo;
+    const int wy = std::min(ny, th + 2 * halo);
+    return static_cast<size_t>(wx) * wy * (down ? 9 : 7) * sizeof(T);
+}
+
+constexpr size_t kLegSmemMax = 200 * 1024;
+
+// Opt the leg kernels in to more than 48 KB of dynamic shared memory, once per
+// type and device (the first solve on a device runs eagerly, before any capture).
+template <typename T>
+void allow_leg_smem() {
+    static std::atomic<unsigned long long> done{0};
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return;
+    const unsigned long long bit = 1ULL << device;
+    if (done.load() & bit) return;
+    cudaFuncSetAttribute(reinterpret_cast<const void*>(k_vcycle_down<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kLegSmemMax));
+    cudaFuncSetAttribute(reinterpret_cast<const void*>(k_vcycle_up<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kLegSmemMax));
+    done.fetch_or(bit);
+}
+
 template <typename T>
 __global__ void k_sub(T* __restrict__ v, const T* __restrict__ u, size_t n) {
     csg::pdl_begin();
@@ -789,9 +1080,62 @@ struct Fmg {
         }
         (csg::note_launch(), csg::launch_pdl(k_fmg_coarse_cycle<T>, batch, kCoarseThreads, 0, s, c));
     }
+    // One launch per fine leg (k_vcycle_down / k_vcycle_up) when every fine
+    // level has an even x size and the tile regions fit in shared memory.
+    bool legs_fit(size_t start, size_t fused) const {
+        for (size_t l = start; l < fused; ++l) {
+            const int nx = buf.specs[l].first, ny = buf.specs[l].second;
+            if (nx % 2 != 0 || leg_smem<T>(nx, ny, 2 * nit + 2, true) > kLegSmemMax) return false;
+        }
+        return true;
+    }
+    FineLeg<T> leg(size_t l, const T* uin, T* uout) const {
+        double pr[5];
+        params_at(l, pr);
+        const MemWeights w = mem_weights(pr);
+        FineLeg<T> g{};
+        g.A = buf.A[l];
+        g.B = buf.B[l];
+        g.Uin = uin;
+        g.Uout = uout;
+        g.nx = buf.specs[l].first;
+        g.ny = buf.specs[l].second;
+        g.w00 = T(w.w00);
+        g.w01 = T(w.w01);
+        g.w10 = T(w.w10);
+        g.rw = reg_weights(pr, 1);
+        g.nB = buf.B[l + 1];
+        g.nU = buf.U[l + 1];
+        g.cnx = buf.specs[l + 1].first;
+        g.cny = buf.specs[l + 1].second;
+        g.nit = nit;
+        return g;
+    }
+    dim3 leg_grid(size_t l) const {
+        const int nx = buf.specs[l].first, ny = buf.specs[l].second;
+        return dim3(static_cast<unsigned>(((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY)),
+                    static_cast<unsigned>(batch));
+    }
     void cycle(size_t start) {
         const size_t last = buf.specs.size() - 1;
         const size_t fused = std::max(start, coarse_first());
+        if (buf.specs.size() <= static_cast<size_t>(kMaxLevels) && fused < last && legs_fit(start, fused)) {
+            allow_leg_smem<T>();
+            // down: relax, residual, restriction (relaxed solution in R[l]); up: prolongation, relax (back in U[l])
+            for (size_t l = start; l < fused; ++l) {
+                const int nx = buf.specs[l].first, ny = buf.specs[l].second;
+                (csg::note_launch(), csg::launch_pdl(k_vcycle_down<T>, leg_grid(l), 256,
+                                                     leg_smem<T>(nx, ny, 2 * nit + 2, true), s,
+                                                     leg(l, buf.U[l], buf.R[l])));
+            }
+            coarse_cycle(fused);
+            for (size_t l = fused; l-- > start;) {
+                const int nx = buf.specs[l].first, ny = buf.specs[l].second;
+                (csg::note_launch(), csg::launch_pdl(k_vcycle_up<T>, leg_grid(l), 256, leg_smem<T>(nx, ny, 2 * nit, false),
+                                                     s, leg(l, buf.R[l], buf.U[l])));
+            }
+            return;
+        }
         if (buf.specs.size() <= static_cast<size_t>(kMaxLevels) && fused < last) {
             for (size_t l = start; l < fused; ++l) {
                 relax(l);

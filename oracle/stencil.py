@@ -110,10 +110,9 @@ def locate(points: np.ndarray, faces: np.ndarray, queries: np.ndarray):
     edges = points[faces] - points[np.roll(faces, -1, axis=1)]
     longest = float(np.sqrt(_dot(edges, edges)).max())
     reach = longest + 6.0e-3 * longest
-    incident = [[] for _ in range(points.shape[0])]
-    for f, tri in enumerate(faces):
-        for v in tri:
-            incident[v].append(f)
+    corner_faces = np.argsort(faces.ravel(), kind="stable") // 3  # faces grouped by vertex
+    ends = np.cumsum(np.bincount(faces.ravel(), minlength=points.shape[0]))
+    incident = np.split(corner_faces, ends[:-1])
     tree = cKDTree(points)
     nearest, _ = tree.query(queries)
     face_out = np.empty(queries.shape[0], dtype=np.int64)
@@ -136,6 +135,45 @@ def locate(points: np.ndarray, faces: np.ndarray, queries: np.ndarray):
         face_out[start:start + 4096] = f
         w_out[start:start + 4096] = weights(pt[rows, best], t[:, 0], t[:, 1], t[:, 2])
     return face_out, w_out
+
+
+def tetrahedral_sphere(levels: int = 6):
+    """The helper's resampling sphere (its tetrahedral sphere of 20 * 4^levels triangles).
+
+    An icosahedron with vertices (+-a, +-b, 0), (0, +-a, +-b), (+-b, 0, +-a),
+    a = phi / sqrt(1 + phi^2), b = 1 / sqrt(1 + phi^2), in the helper's vertex
+    and face order, split 1-to-4 per level: each face (p, q, r) in order gives
+    (p, pq, rp), (pq, q, qr), (rp, pq, qr), (rp, qr, r), an edge midpoint is
+    numbered when its edge is first met (edges pq, qr, rp) and is the
+    normalised sum of its ends.  One edge at a time, with a dictionary.
+    """
+
+    phi = (1.0 + math.sqrt(5.0)) / 2.0
+    a, b = phi / math.sqrt(1.0 + phi * phi), 1.0 / math.sqrt(1.0 + phi * phi)
+    signs = [(1, 1), (1, -1), (-1, 1), (-1, -1)]
+    points = [(sa * a, sb * b, 0.0) for sa, sb in signs] + [(0.0, sa * a, sb * b) for sa, sb in signs] + \
+        [(sa * b, 0.0, sb * a) for sa, sb in ((1, 1), (-1, 1), (1, -1), (-1, -1))]
+    faces = [(2, 11, 3), (2, 5, 11), (11, 5, 10), (5, 0, 10), (0, 5, 4), (4, 5, 2), (4, 2, 9), (9, 2, 3),
+             (9, 3, 6), (9, 6, 8), (4, 9, 8), (4, 8, 0), (0, 8, 1), (1, 8, 6), (1, 6, 7), (7, 6, 3),
+             (11, 7, 3), (11, 10, 7), (10, 1, 7), (10, 0, 1)]
+    points = [np.array(pt) for pt in points]
+    for _ in range(levels):
+        middle = {}
+
+        def mid(i, j):
+            key = (min(i, j), max(i, j))
+            if key not in middle:
+                m = points[i] + points[j]
+                middle[key] = len(points)
+                points.append(m / math.sqrt(float(m @ m)))
+            return middle[key]
+
+        split = []
+        for p_, q_, r_ in faces:
+            pq, qr, rp = mid(p_, q_), mid(q_, r_), mid(r_, p_)
+            split += [(p_, pq, rp), (pq, q_, qr), (rp, pq, qr), (rp, qr, r_)]
+        faces = split
+    return np.array(points), np.array(faces, dtype=np.int32)
 
 
 def _unit(p):
@@ -165,8 +203,12 @@ def sheet_directions(nx: int, ny: int) -> np.ndarray:
     return out
 
 
-def surface_stencil(sphere, sphere_faces, resampling_points, normalize: bool = True):
-    """(sphere points, surface indices, surface weights, normalised input points) of the helper."""
+def surface_stencil(sphere, sphere_faces, resampling_points, normalize: bool = True, rows=None):
+    """(sphere points, surface indices, surface weights, normalised input points) of the helper.
+
+    With ``rows`` only those resampling points are located (the placement
+    still uses every input point).
+    """
 
     p = np.asarray(sphere, dtype=np.float32).astype(np.float64)
     faces = np.asarray(sphere_faces, dtype=np.int64)
@@ -175,6 +217,8 @@ def surface_stencil(sphere, sphere_faces, resampling_points, normalize: bool = T
     radius = 0.975 * _sequential_sum(np.sqrt(_dot(p, p))) / p.shape[0]
     centre = p.min(axis=0) + p.max(axis=0)
     u = _unit(np.asarray(resampling_points, dtype=np.float64))
+    if rows is not None:
+        u = u[np.asarray(rows)]
     face, w = locate(p, faces, centre + radius * u)
     tri = faces[face]
     resampled = (w[:, 0:1] * p[tri[:, 0]] + w[:, 1:2] * p[tri[:, 1]]) + w[:, 2:3] * p[tri[:, 2]]

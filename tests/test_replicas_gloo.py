@@ -84,19 +84,35 @@ def test_reference_arm_line_follows_the_bench_contract(monkeypatch, capsys):
 
     for name in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
         monkeypatch.delenv(name, raising=False)
-    sample = {"total": 140.0, "stages_1_5": 1.5, "sweeps": 15.0}
-    monkeypatch.setattr(bench, "cpu_hemisphere_sample", lambda meshes: dict(sample))
+    stages = {"stages_1_5": {"measured_s": 1.5, "fraction": 1.0, "scaled_s": 1.5},
+              "sweeps": {"measured_s": 1.5, "fraction": 0.1, "scaled_s": 15.0}}
+
+    class FakeSampler:
+        cores = 3
+
+        def __init__(self, meshes):
+            pass
+
+        def sample(self):
+            return {"total": 140.0, "measured_s": 3.0, "stages": stages}
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(bench, "CpuSampler", FakeSampler)
     args = bench.parse_args(["--impl", "reference", "--steps", "2", "--warmup", "1"])
     assert bench.run_reference(args) == 0
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert line["impl"] == "reference"
     assert (line["metric"], line["unit"], line["higher_is_better"]) == (bench.METRIC, bench.UNIT, False)
     assert line["value"] == pytest.approx(140.0) and line["steps"] == 2 and line["warmup"] == 1
+    # a step is the measured sample: the driver's wall clock covers steps x ms_per_step
+    assert line["ms_per_step"] == pytest.approx(3000.0) and line["extrapolated"] is True
     config = dict(line["config"])
     assert config.pop("parallelism")
     assert config == json.loads(json.dumps(bench.workload_config(bench.load_meshes())))
     baseline = line["cpu_baseline"]
-    assert baseline["value"] == line["value"] and baseline["kind"] == "port" and baseline["cores"] == 1
-    assert baseline["sample"]
+    assert baseline["value"] == line["value"] and baseline["kind"] == "port" and baseline["cores"] == 3
+    assert baseline["sample"] and baseline["stages_s"] == stages
     assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}

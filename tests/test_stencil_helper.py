@@ -81,6 +81,11 @@ def test_resampling_sphere_is_the_helpers_tetrahedral_sphere(golden):
     for name in CASES:
         assert digest == str(golden[f"{name}_faces_sha256"])
     assert np.allclose(np.linalg.norm(points, axis=1), 1.0, atol=1e-15)
+    # the oracle's own construction (edge by edge) gives the same sphere
+    from oracle import stencil as ost
+
+    opoints, ofaces = ost.tetrahedral_sphere(6)
+    assert np.array_equal(ofaces, faces) and np.abs(opoints - points).max() <= 1e-15
 
 
 @pytest.mark.parametrize("name", CASES)
