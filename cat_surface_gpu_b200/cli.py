@@ -118,6 +118,9 @@ def surfwarp_main(argv: list[str] | None = None) -> int:
     parser.add_argument("--rotation-max-iter", type=int, default=500)
     parser.add_argument("--rotation-tol", type=float, default=1.0e-4)
     parser.add_argument("--rotation-simplex-step", type=float, default=0.1)
+    parser.add_argument("--rotation-search", choices=("nelder-mead", "euler-grid"), default="nelder-mead",
+                        help="nelder-mead: the reference's 46 seeds + Nelder-Mead; euler-grid: 10 then 2 degree "
+                             "Euler grids on z-scored curvature and depth")
     args = parser.parse_args(argv)
     result = run_cat_surface_gpu_pipeline(
         args.source_surface, args.source_sphere, args.target_surface, args.target_sphere, args.output,
@@ -133,7 +136,7 @@ def surfwarp_main(argv: list[str] | None = None) -> int:
         rotation_refine=not args.no_rotation_refine, rotation_max_iter=args.rotation_max_iter,
         rotation_tol=args.rotation_tol, rotation_simplex_step=args.rotation_simplex_step,
         parallel_sides=args.parallel_sides, optimized_dartel=args.optimized_dartel, cuda_graph=args.cuda_graph,
-        sheet_size=tuple(args.sheet_size),
+        sheet_size=tuple(args.sheet_size), rotation_search=args.rotation_search,
     )
     device = torch.device(args.device)
     print(json.dumps({

@@ -174,6 +174,7 @@ _BACKENDS = {"auto", "native-curvature", "cuda"}
 # the reference's feature backends that run its helper binaries (reference 550-560, 836-893)
 _HELPER_BACKENDS = {"official-cpu", "cuda-official-depth", "cuda-official-geometry"}
 _SOLVERS = {"colored-sor", "pcg"}
+_SEARCHES = {"nelder-mead", "euler-grid"}
 
 
 def _validate_options(*, steps=2, runs=1, stencil_threads=8, curvtypes=(5, 5, 2), fwhm=(5.0, 5.0 / 3.0, 5.0 / 9.0),
@@ -181,7 +182,7 @@ def _validate_options(*, steps=2, runs=1, stencil_threads=8, curvtypes=(5, 5, 2)
                       rotation_feature_backend="auto", rotation_feature_solver="colored-sor", has_values=False,
                       dartel_dtype=torch.float64, device="cuda", stencil_builder="native", rotated_stencil_builder=None,
                       rotation_values_probe=None, rotation_geometry_probe=None, rotation_depth_probe=None,
-                      **_unused) -> None:
+                      rotation_search="nelder-mead", **_unused) -> None:
     """Argument checks of the reference pipeline (reference 514-560), before any file is read.
 
     Options that would run one of the reference's helper binaries raise
@@ -217,6 +218,10 @@ def _validate_options(*, steps=2, runs=1, stencil_threads=8, curvtypes=(5, 5, 2)
                              "computed on the GPU")
     if rotation_feature_solver not in _SOLVERS:
         raise ValueError("rotation_feature_solver must be 'colored-sor' or 'pcg'")
+    if rotation_search not in _SEARCHES:
+        raise ValueError(f"rotation_search must be one of {sorted(_SEARCHES)}")
+    if rotation_search == "euler-grid" and has_values:
+        raise ValueError("rotation_search='euler-grid' computes its own two features; rotation values are not used")
     _resolve_dartel_dtype(dartel_dtype)
     if device == "cpu" or str(device) == "cpu":
         raise ValueError("The explicit GPU pipeline requires a CUDA device")
@@ -271,7 +276,7 @@ def register_meshes(
     rotation_refine: bool = True, rotation_max_iter: int = 500, rotation_tol: float = 1.0e-4,
     rotation_simplex_step: float = 0.1, rotation_feature_backend: str = "auto",
     rotation_feature_solver: str = "colored-sor", parallel_sides: bool = True, optimized_dartel: bool = True,
-    cuda_graph: bool = True, sheet_size: tuple[int, int] = (512, 256),
+    cuda_graph: bool = True, sheet_size: tuple[int, int] = (512, 256), rotation_search: str = "nelder-mead",
 ) -> tuple[np.ndarray, np.ndarray, float, dict[str, float]]:
     """In-memory SurfWarp registration: returns (sphere vertices f32, angle, rotation cost, timings).
 
@@ -279,6 +284,11 @@ def register_meshes(
     (the four input files) is accepted for signature compatibility and not
     used.  ``sheet_size`` is the DARTEL sheet (nx, ny) of the stencils built
     here.  Every launch runs with ``device`` as the current CUDA device.
+    ``rotation_search`` is the reference's 46 seeds + Nelder-Mead
+    (``"nelder-mead"``, default) or ``"euler-grid"``: all of SO(3) on a 10
+    degree Euler grid, then a 2 degree grid round the best, on two features
+    per side -- the type-5 curvature (FWHM 15 / 10) and the depth potential,
+    each z-scored and rounded to float32.
     """
 
     _validate_options(steps=steps, runs=runs, stencil_threads=stencil_threads, curvtypes=curvtypes, fwhm=fwhm,
@@ -286,6 +296,7 @@ def register_meshes(
                       rotation_simplex_step=rotation_simplex_step, rotation_feature_backend=rotation_feature_backend,
                       rotation_feature_solver=rotation_feature_solver, has_values=rotation_values is not None,
                       dartel_dtype=dartel_dtype, device=device, stencil_builder=stencil_builder,
+                      rotation_search=rotation_search,
                       rotated_stencil_builder=rotated_stencil_builder, rotation_values_probe=rotation_values_probe,
                       rotation_geometry_probe=rotation_geometry_probe, rotation_depth_probe=rotation_depth_probe)
     if rotation_feature_backend == "auto":
@@ -327,7 +338,17 @@ def register_meshes(
         timings["initial_stencil_seconds"] = time.perf_counter() - start
 
         start = time.perf_counter()
-        if rotation_values is not None:
+        if rotation_search == "euler-grid":
+            from .surface_rotation import zscore
+
+            curvature = native_rotation_features(source_stencil, target_stencil, source_surface.vertices,
+                                                 target_surface.vertices, target_device)
+            depth = depth_rotation_features(source_stencil, target_stencil, source_surface.vertices,
+                                            target_surface.vertices, target_device, solver=rotation_feature_solver,
+                                            timings=timings)
+            source_values = zscore(np.stack([np.asarray(curvature[0]), depth[0].cpu().numpy()]))
+            target_values = zscore(np.stack([np.asarray(curvature[1]), depth[1].cpu().numpy()]))
+        elif rotation_values is not None:
             source_values, target_values = rotation_values
         elif rotation_feature_backend == "native-curvature":
             source_values, target_values = native_rotation_features(
@@ -345,10 +366,13 @@ def register_meshes(
         torch.cuda.synchronize(target_device)
         timings["rotation_index_upload_seconds"] = time.perf_counter() - start
         start = time.perf_counter()
-        rotation = rotation_pipeline.search(source_stencil.sphere_points, source_values, target_values,
-                                            point_chunk=point_chunk, refine=rotation_refine,
-                                            max_iter=rotation_max_iter, tol=rotation_tol,
-                                            simplex_step=rotation_simplex_step)
+        if rotation_search == "euler-grid":
+            rotation = rotation_pipeline.search_euler_grid(source_stencil.sphere_points, source_values, target_values)
+        else:
+            rotation = rotation_pipeline.search(source_stencil.sphere_points, source_values, target_values,
+                                                point_chunk=point_chunk, refine=rotation_refine,
+                                                max_iter=rotation_max_iter, tol=rotation_tol,
+                                                simplex_step=rotation_simplex_step)
         torch.cuda.synchronize(target_device)
         timings["rotation_search_seconds"] = time.perf_counter() - start
 

@@ -107,6 +107,15 @@ class RotationPipeline:
         return self.index.search_rotation_prepared(inputs, point_chunk=point_chunk, refine=refine, max_iter=max_iter,
                                                    tol=tol, simplex_step=simplex_step)
 
+    def search_euler_grid(self, source_points, source_values, target_values, *, coarse_step_deg: float = 10.0,
+                          fine_step_deg: float = 2.0, fine_half_width_deg: float = 10.0) -> RotationSearchResult:
+        """The 10-degree then 2-degree Euler-grid search (values [n] or [F, n])."""
+
+        inputs = self.prepare_inputs(source_points, source_values, target_values)
+        return self.index.euler_grid_search_prepared(inputs, coarse_step_deg=coarse_step_deg,
+                                                     fine_step_deg=fine_step_deg,
+                                                     fine_half_width_deg=fine_half_width_deg)
+
 
 def run_rotation_pipeline(target_stencil, source_points, source_values, target_values, *, device="auto",
                           grid_size: int = 128, margin: int = 1, candidate_table_dtype=torch.int32,

@@ -31,6 +31,42 @@ def official_seed_grid_angles() -> np.ndarray:
     return np.asarray(values, dtype=np.float64)
 
 
+def euler_grid_angles(step_deg: float, center=None, half_width_deg: float | None = None) -> np.ndarray:
+    """Euler-angle candidates [C, 3] (radians) on a regular grid, x slowest, z fastest.
+
+    Without ``center``: all of SO(3) -- x and z over [-180, 180), y over
+    [-90, 90] -- every ``step_deg`` degrees.  With ``center`` (radians) and
+    ``half_width_deg``: ``center + k * step`` for every k with
+    |k * step| <= half_width on each axis.  The search takes the first
+    minimum in this order.
+    """
+
+    step = float(step_deg)
+    if step <= 0:
+        raise ValueError("step_deg must be positive")
+    if center is None:
+        ax = np.arange(-180.0, 180.0 - 1e-9, step)
+        ay = np.arange(-90.0, 90.0 + 1e-9, step)
+        axes = [np.deg2rad(ax), np.deg2rad(ay), np.deg2rad(ax)]
+    else:
+        if half_width_deg is None or half_width_deg < 0:
+            raise ValueError("a centred grid needs a non-negative half_width_deg")
+        k = np.arange(-np.floor(half_width_deg / step + 1e-9), np.floor(half_width_deg / step + 1e-9) + 1)
+        c = np.asarray(center, dtype=np.float64).reshape(3)
+        axes = [c[i] + np.deg2rad(k * step) for i in range(3)]
+    grid = np.meshgrid(*axes, indexing="ij")
+    return np.stack([g.ravel() for g in grid], axis=1)
+
+
+def zscore(values) -> np.ndarray:
+    """(v - mean) / std per feature row (population std), rounded to float32 and widened back."""
+
+    v = np.asarray(values, dtype=np.float64)
+    mean = v.mean(axis=-1, keepdims=True)
+    std = v.std(axis=-1, keepdims=True)
+    return ((v - mean) / np.where(std > 0, std, 1.0)).astype(np.float32).astype(np.float64)
+
+
 _ROW0 = np.array([r for c in range(3) for r in range(3)])
 _ROW1 = _ROW0 + 3
 _ROW2 = _ROW0 + 6
@@ -427,6 +463,28 @@ class RotationGridIndexDevice:
         inputs = self.prepare_cost_inputs(source_points, source_values, target_values)
         return self.refine_nelder_mead_prepared(inputs, initial_angles, point_chunk=point_chunk, max_iter=max_iter,
                                                 tol=tol, simplex_step=simplex_step)
+
+    def euler_grid_search_prepared(self, inputs: RotationCostInputs, *, coarse_step_deg: float = 10.0,
+                                   fine_step_deg: float = 2.0, fine_half_width_deg: float = 10.0):
+        """Two-level Euler-grid search: all of SO(3) every ``coarse_step_deg``, then
+        every ``fine_step_deg`` within +-``fine_half_width_deg`` of the coarse best.
+
+        The rotation search of the 10-degree-then-2-degree configuration
+        (an alternative to the reference's 46 seeds + Nelder-Mead); each
+        level is one batched cost launch; first minimum in grid order.
+        """
+
+        coarse = torch.as_tensor(euler_grid_angles(coarse_step_deg), dtype=torch.float64)
+        coarse_costs = self.cost_batch_prepared(inputs, coarse)
+        best = int(torch.argmin(coarse_costs))
+        fine = torch.as_tensor(euler_grid_angles(fine_step_deg, coarse[best].numpy(), fine_half_width_deg),
+                               dtype=torch.float64)
+        fine_costs = self.cost_batch_prepared(inputs, fine)
+        pick = int(torch.argmin(fine_costs))
+        angle = fine[pick].to(self.device)
+        return RotationSearchResult(seed_angle=coarse[best].to(self.device), seed_cost=coarse_costs[best].clone(),
+                                    seed_costs=coarse_costs, angle=angle, cost=fine_costs[pick].clone(),
+                                    rotation_matrix=self.rotation_matrix(angle), iterations=0)
 
     def search_rotation(self, source_points, source_values, target_values, *, point_chunk: int = 1024,
                         refine: bool = True, max_iter: int = 500, tol: float = 1.0e-4, simplex_step: float = 0.1):
