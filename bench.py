@@ -684,6 +684,144 @@ def batched_dartel_leg(device, repeats: int = 5) -> dict:
     }
 
 
+def _registration_subject(spec):
+    """Worker of the registration leg: one subject mesh and its sphere (spawned process)."""
+
+    from cat_surface_gpu_b200 import synthetic
+
+    return synthetic.folded_hull_and_sphere(*spec)
+
+
+def batched_registration_leg(device, repeats: int = 3) -> dict:
+    """16 subject meshes (folded hulls of 40,962-163,842 vertices) registered to one 61,442-vertex template.
+
+    A registration: the curvature sheets of both surfaces on their stencils,
+    one DARTEL run of two steps (256 x 128, float64, graph-captured solve)
+    and the inverse warp of the subject's sphere; each subject's stencil is
+    built once beforehand (``prep_s``), as a serving system builds it when a
+    subject arrives.  Batched: all 16 through one batched solve; plain: one
+    registration at a time.  The first two subjects are compared with the
+    reference's CPU registration (``registration_golden.npz``).  The
+    checkpointed adjoint (k = 7) of the DARTEL data term is timed on the
+    registrations' step maps: one batched gradient of all 16 vs one at a time.
+    """
+
+    import multiprocessing
+
+    import numpy as np
+    import torch
+
+    from cat_surface_gpu_b200 import synthetic
+    from cat_surface_gpu_b200.dartel_adjoint import dartel_data_term
+    from cat_surface_gpu_b200.gpu_pipeline import normalise_sphere
+    from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+    from cat_surface_gpu_b200.surface_warp import (_surface_sheets, apply_flow_to_stenciled_sphere,
+                                                   solve_dartel_from_surfaces, solve_dartel_from_surfaces_many)
+
+    specs = synthetic.registration_subjects()
+    with multiprocessing.get_context("spawn").Pool(min(len(specs), max(1, os.cpu_count() or 1))) as pool:
+        subjects = pool.map(_registration_subject, specs)
+    target = np.load(GOLDEN / "surf2sphere_c3.npz")
+    nx, ny = SHEET
+    steps, loop = 2, 6
+    fwhm = tuple(5.0 / (3.0 ** (steps + i)) for i in range(steps))
+    tgt_stencil = build_surface_stencil(target["final"], target["faces"], nx=nx, ny=ny, device=device).to(device)
+    tgt_surface = torch.as_tensor(target["surface"], device=device)
+    start = time.perf_counter()
+    prepared = []
+    for vertices, faces, sphere in subjects:
+        current = normalise_sphere(sphere)
+        stencil = build_surface_stencil(current, faces, nx=nx, ny=ny, normalize=False, device=device).to(device)
+        prepared.append((torch.as_tensor(vertices, device=device), stencil, torch.as_tensor(current, device=device)))
+    torch.cuda.synchronize(device)
+    prep_s = time.perf_counter() - start
+
+    def batched():
+        flows = solve_dartel_from_surfaces_many([(v, tgt_surface, st, tgt_stencil, fwhm) for v, st, _ in prepared],
+                                                curvtypes=(5, 5, 2), n_steps=steps, loop=loop, device=device,
+                                                dtype=torch.float64, cuda_graph=True)
+        return [apply_flow_to_stenciled_sphere(cur, f, st, inverse=True, device=device, dtype=torch.float64)
+                for (_, st, cur), f in zip(prepared, flows)]
+
+    def plain(r):
+        v, st, cur = prepared[r]
+        flow = solve_dartel_from_surfaces(v, tgt_surface, st, tgt_stencil, fwhm=fwhm, curvtypes=(5, 5, 2),
+                                          n_steps=steps, loop=loop, device=device, dtype=torch.float64,
+                                          cuda_graph=True).flow
+        return apply_flow_to_stenciled_sphere(cur, flow, st, inverse=True, device=device, dtype=torch.float64)
+
+    warped = batched()  # capture the batched graph
+    alone = [plain(r) for r in range(len(prepared))]  # capture the single-registration graph
+    torch.cuda.synchronize(device)
+    stream = torch.cuda.current_stream(device)
+    batch_ms, plain_ms = [], []
+    for _ in range(repeats):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        warped = batched()
+        e1.record(stream)
+        e1.synchronize()
+        batch_ms.append(e0.elapsed_time(e1))
+        events = [torch.cuda.Event(enable_timing=True) for _ in range(len(prepared) + 1)]
+        events[0].record(stream)
+        for r in range(len(prepared)):
+            alone[r] = plain(r)
+            events[r + 1].record(stream)
+        events[-1].synchronize()
+        plain_ms.extend(events[r].elapsed_time(events[r + 1]) for r in range(len(prepared)))
+    regs = len(prepared)
+    batch_s = statistics.mean(batch_ms) / 1e3
+    plain_s = sum(plain_ms) / repeats / 1e3
+    golden = np.load(GOLDEN / "registration_golden.npz")
+    vs_cpu = [error_stats(golden[f"warped_{k}"], warped[k].cpu().numpy()) for k in range(2)]
+    vs_plain = max(float(torch.linalg.vector_norm(a - b, dim=1).max()) for a, b in zip(warped, alone))
+
+    # checkpointed adjoint of the data term on the registrations' step maps
+    sheets = [_surface_sheets(v, tgt_surface, st, tgt_stencil, fwhm, (5, 5, 2), steps, device, torch.float64, True)
+              for v, st, _ in prepared]
+    src = torch.cat([a for a, _ in sheets]).contiguous()
+    tgt = torch.cat([b for _, b in sheets]).contiguous()
+    gen = torch.Generator(device=device).manual_seed(9)
+    velocity = (0.3 * torch.randn((src.shape[0], 2, ny, nx), generator=gen, device=device, dtype=torch.float64))
+
+    def gradient(v, s, t):
+        v = v.detach().requires_grad_(True)
+        dartel_data_term(v, s, t, k=7).sum().backward()
+        return v.grad
+
+    for _ in range(2):
+        gradient(velocity, src, tgt)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    together = gradient(velocity, src, tgt)
+    e1.record(stream)
+    e1.synchronize()
+    adjoint_batched_ms = e0.elapsed_time(e1)
+    e0.record(stream)
+    single = [gradient(velocity[i:i + steps], src[i:i + steps], tgt[i:i + steps]) for i in range(0, src.shape[0], steps)]
+    e1.record(stream)
+    e1.synchronize()
+    adjoint_plain_ms = e0.elapsed_time(e1)
+    adjoint_identical = bool(torch.equal(together, torch.cat(single)))
+    return {
+        "registrations": regs, "subject_vertices": [n for n, _ in specs], "template_vertices": int(
+            target["surface"].shape[0]), "sheet": [nx, ny], "dtype": "float64", "steps": steps, "loop": loop,
+        "cuda_graphs": True, "prep_s": prep_s,
+        "batched_regs_per_s": regs / batch_s, "plain_regs_per_s": regs / plain_s,
+        "speedup_vs_plain": plain_s / batch_s,
+        "batched_latency_ms": {"p50": float(np.percentile(batch_ms, 50)), "p99": float(np.percentile(batch_ms, 99))},
+        "plain_latency_ms": {"p50": float(np.percentile(plain_ms, 50)), "p99": float(np.percentile(plain_ms, 99))},
+        "vertex_error_vs_cpu_reference": {f"subject_{k}": vs_cpu[k] for k in range(2)},
+        "max_vertex_error_vs_plain": vs_plain,
+        "adjoint": {"k": 7, "maps": int(src.shape[0]), "batched_ms": adjoint_batched_ms,
+                    "one_registration_at_a_time_ms": adjoint_plain_ms,
+                    "batched_gradients_per_s": regs / (adjoint_batched_ms / 1e3),
+                    "plain_gradients_per_s": regs / (adjoint_plain_ms / 1e3),
+                    "identical_to_one_at_a_time": adjoint_identical},
+    }
+
+
 def run_native(args):
     import numpy as np
     import torch
@@ -784,6 +922,7 @@ def run_native(args):
     if not args.no_batched:
         batched["batched_rotation"] = batched_rotation_leg(device)
         batched["batched_dartel"] = batched_dartel_leg(device)
+        batched["batched_registration"] = batched_registration_leg(device)
 
     if rank == 0:
         kernel_s = statistics.mean(kernel_ms) / 1e3

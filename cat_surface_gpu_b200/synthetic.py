@@ -184,6 +184,34 @@ def folded_hull(n_vertices: int = 61442, seed: int = 0, radius_mm: float = 70.0)
     return (points * (r * radius_mm)[:, None]).astype(np.float32), faces
 
 
+def folded_hull_and_sphere(n_vertices: int, seed: int, radius_mm: float = 70.0):
+    """:func:`folded_hull` and its spherical parametrisation (the unfolded points at 100 mm).
+
+    The fold is radial, so the hull's own unit points map the folded surface
+    to the sphere: (vertices float32 [n, 3], faces int32 [m, 3], sphere
+    float32 [n, 3]).
+    """
+
+    rng = np.random.default_rng(seed)
+    points = fibonacci_points(int(n_vertices), rng)
+    faces = hull_faces(points)
+    r = np.exp(real_sph_harm_sum(points, range(8, 41), 0.15, rng))
+    return ((points * (r * radius_mm)[:, None]).astype(np.float32), faces,
+            (100.0 * points).astype(np.float32))
+
+
+def registration_subjects(count: int = 16, seed: int = 5005) -> list[tuple[int, int]]:
+    """(vertex count, seed) of the subjects of the batched registration workload.
+
+    Vertex counts are drawn uniformly from 40,962..163,842 (sorted); each
+    subject is ``folded_hull_and_sphere(n, seed)``.
+    """
+
+    rng = np.random.default_rng(seed)
+    sizes = sorted(int(v) for v in rng.integers(40962, 163843, size=int(count)))
+    return [(n, 700 + i) for i, n in enumerate(sizes)]
+
+
 def smooth_sheet(ny: int, nx: int, seed: int, n_modes: int = 12) -> np.ndarray:
     """A smooth, periodic-in-x feature sheet in [0, 1] (synthetic DARTEL input)."""
 
