@@ -564,7 +564,14 @@ def hemisphere_e2e(meshes, device, dartel_dtype, workdir: Path) -> tuple[float, 
 
 
 def batched_rotation_leg(device) -> dict:
-    """8 surfaces x 4,096 quaternions x 2 features: one persistent launch vs one launch per surface."""
+    """8 surfaces x 4,096 quaternions x 2 features in one persistent launch.
+
+    Compared with one launch per surface and with one launch per (surface,
+    candidate) -- the one-candidate-at-a-time form ("plain"), timed on 32
+    candidates per surface and scaled.  Source points are the surfaces'
+    unit-sphere vertex directions (the jittered Fibonacci points their folded
+    hulls are built on); the cost reads only points and features, not faces.
+    """
 
     import numpy as np
     import torch
@@ -607,14 +614,25 @@ def batched_rotation_leg(device) -> dict:
     def batched():
         return batched_costs(indices, inputs, matrix_sets=mats, **shape)
 
-    def plain():
+    def per_surface():
         return [batched_costs([index], [inp], matrix_sets=[m], **shape)[0] for inp, m in zip(inputs, mats)]
 
+    # one launch per (surface, candidate): how a one-candidate-at-a-time search costs them;
+    # timed on the first 32 candidates of every surface and scaled to 4,096
+    sample = 32
+
+    def per_candidate():
+        return [[batched_costs([index], [inp], matrix_sets=[m[c:c + 1]], **shape)[0] for c in range(sample)]
+                for inp, m in zip(inputs, mats)]
+
     together = batched()
-    alone = plain()
-    identical = all(torch.equal(a, b) for a, b in zip(together, alone))
+    alone = per_surface()
+    single = per_candidate()
+    identical = all(torch.equal(a, b) for a, b in zip(together, alone)) and all(
+        torch.equal(a[:sample], torch.cat(b)) for a, b in zip(together, single))
     batched_ms = autotune.time_call(batched, repeats=3, warmup=1)
-    plain_ms = autotune.time_call(plain, repeats=3, warmup=1)
+    plain_ms = autotune.time_call(per_surface, repeats=3, warmup=1)
+    candidate_ms = autotune.time_call(per_candidate, repeats=2, warmup=1) * 4096 / sample
     evaluations = 4096 * sum(sizes)
     # algorithmic bytes per (candidate, point): point 12 + 2 source features 16 + 3 target ids 12
     # + 3 x 2 target features 48 + 36 bytes per scanned candidate triangle (mean CSR width of the grid)
@@ -624,7 +642,9 @@ def batched_rotation_leg(device) -> dict:
     bytes_per_eval = 12 + 16 + 12 + 48 + 36 * mean_width
     return {
         "surfaces": sizes, "candidates_per_surface": 4096, "features": 2, "autotuned_shape": shape,
-        "batched_ms": batched_ms, "plain_ms": plain_ms, "speedup_vs_plain": plain_ms / batched_ms,
+        "batched_ms": batched_ms, "per_surface_ms": plain_ms, "speedup_vs_per_surface": plain_ms / batched_ms,
+        "one_candidate_per_launch_ms": candidate_ms, "one_candidate_per_launch_sample": sample,
+        "speedup_vs_plain": candidate_ms / batched_ms,
         "point_evaluations_per_s": evaluations / (batched_ms / 1e3), "costs_identical_to_plain": bool(identical),
         "kernel_gbs_algorithmic": evaluations * bytes_per_eval / (batched_ms / 1e3) / 1e9,
         "bytes_per_evaluation": bytes_per_eval, "mean_cell_width": mean_width,
