@@ -181,6 +181,38 @@ def job_seconds_per_unit(local_total_ms: float, units_per_rank: int, world: int,
     return float(total.item()) / 1e3 / (units_per_rank * world)
 
 
+def shard_by_cost(costs, world: int, rank: int) -> list[int]:
+    """Indices of the units rank ``rank`` of ``world`` processes in a batched leg.
+
+    Units are independent (surfaces, registrations), so a leg shards with no
+    exchange step: largest estimated cost first, dealt in snake order
+    (ranks 0 .. world-1, then world-1 .. 0, ...) so the ranks' totals stay
+    close; each rank's indices in ascending order.
+    """
+
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    mine = []
+    for k, i in enumerate(order):
+        slot = k % (2 * world)
+        if (slot if slot < world else 2 * world - 1 - slot) == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
+def job_throughput(local_units: float, local_ms: float, world: int, device) -> tuple[float, float]:
+    """(units of the whole job, the slowest rank's milliseconds): throughput = units / max time."""
+
+    import torch
+    import torch.distributed as dist
+
+    units = torch.tensor([float(local_units)], dtype=torch.float64, device=device)
+    ms = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(units, op=dist.ReduceOp.SUM)
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    return float(units.item()), float(ms.item())
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling while the timed region runs."""
 
@@ -563,7 +595,7 @@ def hemisphere_e2e(meshes, device, dartel_dtype, workdir: Path) -> tuple[float, 
     return seconds, int(h2d), int(d2h), parts
 
 
-def batched_rotation_leg(device) -> dict:
+def batched_rotation_leg(device, world: int = 1, rank: int = 0) -> dict:
     """8 surfaces x 4,096 quaternions x 2 features in one persistent launch.
 
     Compared with one launch per surface and with one launch per (surface,
@@ -582,7 +614,9 @@ def batched_rotation_leg(device) -> dict:
     from cat_surface_gpu_b200.surface_stencil import resampling_sphere
 
     rng = np.random.default_rng(2024)
-    sizes = sorted(int(v) for v in rng.integers(40962, 163843, size=8))
+    all_sizes = sorted(int(v) for v in rng.integers(40962, 163843, size=8))
+    mine = shard_by_cost(all_sizes, world, rank)
+    sizes = [all_sizes[i] for i in mine]
     tp, tf = resampling_sphere(6)
     index = RotationGridIndex.from_geometry(tp, tf, grid_size=128, margin=1,
                                             include_dense_candidate_table=False).to(device)
@@ -602,7 +636,7 @@ def batched_rotation_leg(device) -> dict:
 
     target_values = features(tp, 7)
     inputs, mats = [], []
-    for i, n in enumerate(sizes):
+    for i, n in zip(mine, sizes):
         pts = synthetic.fibonacci_points(n, np.random.default_rng(100 + i)).astype(np.float32)
         inputs.append(index.prepare_cost_inputs(pts, features(pts.astype(np.float64), 200 + i), target_values))
         mats.append(quaternion_matrices(uniform_quaternions(4096, 300 + i)))
@@ -633,7 +667,7 @@ def batched_rotation_leg(device) -> dict:
     batched_ms = autotune.time_call(batched, repeats=3, warmup=1)
     plain_ms = autotune.time_call(per_surface, repeats=3, warmup=1)
     candidate_ms = autotune.time_call(per_candidate, repeats=2, warmup=1) * 4096 / sample
-    evaluations = 4096 * sum(sizes)
+    evaluations, job_ms = job_throughput(4096 * sum(sizes), batched_ms, world, device)
     # algorithmic bytes per (candidate, point): point 12 + 2 source features 16 + 3 target ids 12
     # + 3 x 2 target features 48 + 36 bytes per scanned candidate triangle (mean CSR width of the grid)
     offsets = index.candidate_offsets.cpu().numpy().astype(np.int64)
@@ -641,12 +675,13 @@ def batched_rotation_leg(device) -> dict:
     mean_width = float(width[width > 0].mean())
     bytes_per_eval = 12 + 16 + 12 + 48 + 36 * mean_width
     return {
-        "surfaces": sizes, "candidates_per_surface": 4096, "features": 2, "autotuned_shape": shape,
+        "surfaces": all_sizes, "ranks": world, "surfaces_on_rank0": sizes if rank == 0 else None,
+        "candidates_per_surface": 4096, "features": 2, "autotuned_shape": shape,
         "batched_ms": batched_ms, "per_surface_ms": plain_ms, "speedup_vs_per_surface": plain_ms / batched_ms,
         "one_candidate_per_launch_ms": candidate_ms, "one_candidate_per_launch_sample": sample,
         "speedup_vs_plain": candidate_ms / batched_ms,
-        "point_evaluations_per_s": evaluations / (batched_ms / 1e3), "costs_identical_to_plain": bool(identical),
-        "kernel_gbs_algorithmic": evaluations * bytes_per_eval / (batched_ms / 1e3) / 1e9,
+        "point_evaluations_per_s": evaluations / (job_ms / 1e3), "costs_identical_to_plain": bool(identical),
+        "kernel_gbs_algorithmic": evaluations * bytes_per_eval / (job_ms / 1e3) / 1e9 / world,
         "bytes_per_evaluation": bytes_per_eval, "mean_cell_width": mean_width,
     }
 
@@ -712,7 +747,7 @@ def _registration_subject(spec):
     return synthetic.folded_hull_and_sphere(*spec)
 
 
-def batched_registration_leg(device, repeats: int = 3) -> dict:
+def batched_registration_leg(device, repeats: int = 3, world: int = 1, rank: int = 0) -> dict:
     """16 subject meshes (folded hulls of 40,962-163,842 vertices) registered to one 61,442-vertex template.
 
     A registration: the curvature sheets of both surfaces on their stencils,
@@ -738,7 +773,9 @@ def batched_registration_leg(device, repeats: int = 3) -> dict:
     from cat_surface_gpu_b200.surface_warp import (_surface_sheets, apply_flow_to_stenciled_sphere,
                                                    solve_dartel_from_surfaces, solve_dartel_from_surfaces_many)
 
-    specs = synthetic.registration_subjects()
+    all_specs = synthetic.registration_subjects()
+    mine = shard_by_cost([n for n, _ in all_specs], world, rank)
+    specs = [all_specs[i] for i in mine]
     with multiprocessing.get_context("spawn").Pool(min(len(specs), max(1, os.cpu_count() or 1))) as pool:
         subjects = pool.map(_registration_subject, specs)
     target = np.load(GOLDEN / "surf2sphere_c3.npz")
@@ -789,11 +826,13 @@ def batched_registration_leg(device, repeats: int = 3) -> dict:
             events[r + 1].record(stream)
         events[-1].synchronize()
         plain_ms.extend(events[r].elapsed_time(events[r + 1]) for r in range(len(prepared)))
-    regs = len(prepared)
-    batch_s = statistics.mean(batch_ms) / 1e3
-    plain_s = sum(plain_ms) / repeats / 1e3
+    regs, job_batch_ms = job_throughput(len(prepared), statistics.mean(batch_ms), world, device)
+    _, job_plain_ms = job_throughput(0, sum(plain_ms) / repeats, world, device)
+    batch_s, plain_s = job_batch_ms / 1e3, job_plain_ms / 1e3
     golden = np.load(GOLDEN / "registration_golden.npz")
-    vs_cpu = [error_stats(golden[f"warped_{k}"], warped[k].cpu().numpy()) for k in range(2)]
+    # the golden's two subjects are the two smallest; check the ones this rank registered
+    vs_cpu = {f"subject_{k}": error_stats(golden[f"warped_{k}"], warped[mine.index(k)].cpu().numpy())
+              for k in range(2) if k in mine}
     vs_plain = max(float(torch.linalg.vector_norm(a - b, dim=1).max()) for a, b in zip(warped, alone))
 
     # checkpointed adjoint of the data term on the registrations' step maps
@@ -825,19 +864,20 @@ def batched_registration_leg(device, repeats: int = 3) -> dict:
     adjoint_plain_ms = e0.elapsed_time(e1)
     adjoint_identical = bool(torch.equal(together, torch.cat(single)))
     return {
-        "registrations": regs, "subject_vertices": [n for n, _ in specs], "template_vertices": int(
+        "registrations": int(regs), "ranks": world, "subject_vertices": [n for n, _ in all_specs],
+        "template_vertices": int(
             target["surface"].shape[0]), "sheet": [nx, ny], "dtype": "float64", "steps": steps, "loop": loop,
         "cuda_graphs": True, "prep_s": prep_s,
         "batched_regs_per_s": regs / batch_s, "plain_regs_per_s": regs / plain_s,
         "speedup_vs_plain": plain_s / batch_s,
         "batched_latency_ms": {"p50": float(np.percentile(batch_ms, 50)), "p99": float(np.percentile(batch_ms, 99))},
         "plain_latency_ms": {"p50": float(np.percentile(plain_ms, 50)), "p99": float(np.percentile(plain_ms, 99))},
-        "vertex_error_vs_cpu_reference": {f"subject_{k}": vs_cpu[k] for k in range(2)},
+        "vertex_error_vs_cpu_reference": vs_cpu,
         "max_vertex_error_vs_plain": vs_plain,
         "adjoint": {"k": 7, "maps": int(src.shape[0]), "batched_ms": adjoint_batched_ms,
                     "one_registration_at_a_time_ms": adjoint_plain_ms,
-                    "batched_gradients_per_s": regs / (adjoint_batched_ms / 1e3),
-                    "plain_gradients_per_s": regs / (adjoint_plain_ms / 1e3),
+                    "batched_gradients_per_s": len(prepared) / (adjoint_batched_ms / 1e3),
+                    "plain_gradients_per_s": len(prepared) / (adjoint_plain_ms / 1e3),
                     "identical_to_one_at_a_time": adjoint_identical},
     }
 
@@ -940,9 +980,9 @@ def run_native(args):
 
     batched = {}
     if not args.no_batched:
-        batched["batched_rotation"] = batched_rotation_leg(device)
+        batched["batched_rotation"] = batched_rotation_leg(device, world, rank)
         batched["batched_dartel"] = batched_dartel_leg(device)
-        batched["batched_registration"] = batched_registration_leg(device)
+        batched["batched_registration"] = batched_registration_leg(device, world=world, rank=rank)
 
     if rank == 0:
         kernel_s = statistics.mean(kernel_ms) / 1e3
@@ -987,7 +1027,9 @@ def run_native(args):
             "stages_s": stages,
             "roofline": {
                 "kernel": "areal_sweeps (persistent wavefront)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": SWEEP_DRAM_BYTES, "peak_source": peak_source,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": SWEEP_DRAM_BYTES,
+                "traffic_source": "ncu capture of a 200-sweep launch on the same mesh (not scaled: the working set "
+                                  "is read once per launch)", "peak_source": peak_source,
                 "note": "algorithmic bytes = 4,999 x (24 N + 24 F + 4 (N+1)); the sweep chain is bound by the "
                         "latency of its dependency chain (working set L2-resident); peak = "
                         f"{peak_source} HBM copy bandwidth; traffic = DRAM bytes of one ncu capture of a 200-sweep "

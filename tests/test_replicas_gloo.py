@@ -116,3 +116,41 @@ def test_reference_arm_line_follows_the_bench_contract(monkeypatch, capsys):
     assert baseline["sample"] and baseline["stages_s"] == stages
     assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_batched_legs_shard_units_by_cost():
+    """Every unit goes to exactly one rank; the ranks' total costs stay close."""
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    costs = [55679, 68864, 72655, 74933, 81661, 93349, 103165, 106130, 106236, 111415, 112878, 122399, 135336,
+             141626, 150137, 152628]
+    assert bench.shard_by_cost(costs, 1, 0) == list(range(16))
+    for world in (2, 3, 4, 8):
+        shards = [bench.shard_by_cost(costs, world, r) for r in range(world)]
+        assert sorted(i for s in shards for i in s) == list(range(16))
+        totals = [sum(costs[i] for i in s) for s in shards]
+        assert max(totals) - min(totals) <= max(costs)
+
+
+def _throughput_main(rank: int, world: int, port: int, results) -> None:
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        results[rank] = bench.job_throughput([7.0, 9.0][rank], [100.0, 250.0][rank], world, torch.device("cpu"))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_batched_leg_throughput_is_all_units_over_the_slowest_rank():
+    world = 2
+    manager = mp.Manager()
+    results = manager.dict()
+    mp.spawn(_throughput_main, args=(world, _free_port(), results), nprocs=world, join=True)
+    assert results[0] == results[1] == (16.0, 250.0)
