@@ -918,6 +918,32 @@ void allow_leg_smem() {
     done.fetch_or(bit);
 }
 
+// The restriction chain of a level-l field to every coarser level at or below
+// kChainPoints points per grid, in one launch with one CTA per batch element:
+// the same resize_at per point as separate k_resize launches, level after
+// level, with __syncthreads between levels.
+constexpr int kChainPoints = 2048;
+
+template <typename T>
+struct ResizeChain {
+    T* field[kMaxLevels];  // [batch * channels][ny][nx] per level
+    int nx[kMaxLevels], ny[kMaxLevels];
+    int first, last, channels;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kCoarseThreads) k_resize_chain(ResizeChain<T> c) {
+    csg::pdl_begin();
+    const int bi = blockIdx.x;
+    for (int l = c.first; l <= c.last; ++l) {
+        const int P = c.nx[l] * c.ny[l];
+        for (int j = threadIdx.x; j < c.channels * P; j += blockDim.x)
+            resize_at(c.field[l - 1], c.field[l], c.nx[l - 1], c.ny[l - 1], c.nx[l], c.ny[l], 0,
+                      c.channels * bi + j / P, j % P);
+        __syncthreads();
+    }
+}
+
 template <typename T>
 __global__ void k_sub(T* __restrict__ v, const T* __restrict__ u, size_t n) {
     csg::pdl_begin();
@@ -1174,19 +1200,43 @@ struct Fmg {
     }
     // Solves into buf.U[0]; U[0] must already hold the initial guess (or
     // zeros when `coarse_init`).  hess / rhs are level-0 A / B.
+    // A[l] = resize(A[l - 1]) for every level: separate launches down to
+    // kChainPoints points per grid, then the rest in one k_resize_chain launch.
+    void restrict_hessians() {
+        const size_t L = buf.specs.size();
+        size_t l = 1;
+        for (; l < L && static_cast<long long>(buf.specs[l].first) * buf.specs[l].second > kChainPoints; ++l)
+            resize(buf.A[l - 1], l - 1, buf.A[l], l, 3, false);
+        if (l >= L) return;
+        if (L > static_cast<size_t>(kMaxLevels)) {
+            for (; l < L; ++l) resize(buf.A[l - 1], l - 1, buf.A[l], l, 3, false);
+            return;
+        }
+        ResizeChain<T> c{};
+        for (size_t k = 0; k < L; ++k) {
+            c.field[k] = buf.A[k];
+            c.nx[k] = buf.specs[k].first;
+            c.ny[k] = buf.specs[k].second;
+        }
+        c.first = static_cast<int>(l);
+        c.last = static_cast<int>(L - 1);
+        c.channels = 3;
+        (csg::note_launch(), csg::launch_pdl(k_resize_chain<T>, batch, kCoarseThreads, 0, s, c));
+    }
     void run(bool coarse_init) {
         const size_t L = buf.specs.size();
-        for (size_t l = 1; l < L; ++l) resize(buf.A[l - 1], l - 1, buf.A[l], l, 3, false);
-        if (coarse_init)
-            for (size_t l = 1; l < L; ++l) resize(l == 1 ? buf.B[0] : buf.B0[l - 1], l - 1, buf.B0[l], l, 2, false);
+        restrict_hessians();
+        if (!coarse_init) {
+            // every V-cycle writes each coarser level's right-hand side and zeroes its
+            // solution before reading them, so the warm start needs no clearing
+            for (int c = 0; c < cycles; ++c) cycle(0);
+            return;
+        }
+        for (size_t l = 1; l < L; ++l) resize(l == 1 ? buf.B[0] : buf.B0[l - 1], l - 1, buf.B0[l], l, 2, false);
         for (size_t l = 1; l < L; ++l) {
             const size_t P = static_cast<size_t>(buf.specs[l].first) * buf.specs[l].second;
             cudaMemsetAsync(buf.B[l], 0, 2 * P * batch * sizeof(T), s);
             cudaMemsetAsync(buf.U[l], 0, 2 * P * batch * sizeof(T), s);
-        }
-        if (!coarse_init) {
-            for (int c = 0; c < cycles; ++c) cycle(0);
-            return;
         }
         const size_t last = L - 1;
         const size_t Pl = static_cast<size_t>(buf.specs[last].first) * buf.specs[last].second;

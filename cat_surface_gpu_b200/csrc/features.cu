@@ -8,8 +8,11 @@
 // neighbour table; normal accumulation per vertex runs corner 0 over all
 // faces, then corner 1, then corner 2, each in face order -- the reference's
 // three index_add_ calls.  Compiled with --fmad=false; acos / exp are CUDA's.
-// Iterative smoothers launch one kernel per iteration on the caller's stream
-// (no host synchronisation inside), ping-ponging between two buffers.
+// Iterative smoothers run all their Jacobi iterations in one cooperative
+// launch on the caller's stream (no host synchronisation inside): the grid
+// strides over the points, a bounded grid barrier separates iterations, and
+// the values ping-pong between two buffers.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -17,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/catsurf_b200.h"
+#include "common.cuh"
 #include "errors.h"
 
 namespace {
@@ -101,18 +105,31 @@ __global__ void k_sum_partials(const double* __restrict__ partial, int n, double
     out[0] = s;
 }
 
-// One smooth_geometry iteration (372-388): float32 positions, float64 sums.
-__global__ void k_smooth_geometry(const float* __restrict__ in, float* __restrict__ out, const int* __restrict__ off,
-                                  const int* __restrict__ nbr, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int b = off[i], e = off[i + 1];
-    const double den = 1.0 + static_cast<double>(e - b) / 3.0;
-    for (int c = 0; c < 3; ++c) {
-        double s = 0.0;
-        for (int k = b; k < e; ++k) s = s + static_cast<double>(in[3 * nbr[k] + c]);
-        const double num = static_cast<double>(in[3 * i + c]) + s / 3.0;
-        out[3 * i + c] = static_cast<float>(num / den);
+// smooth_geometry (372-388), every iteration in one cooperative launch:
+// float32 positions, float64 sums.  Iteration it reads `in` (it == 0) or the
+// previous destination and writes `out` when an even number of iterations
+// remain after it, else `tmp`, so the last lands in `out`; a grid barrier
+// between iterations.
+__global__ void k_smooth_geometry_all(const float* __restrict__ in, float* __restrict__ out, float* __restrict__ tmp,
+                                      const int* __restrict__ off, const int* __restrict__ nbr, int n, int iterations,
+                                      csg::Control* ctl, unsigned long long timeout_ns) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    unsigned int phase = 0;
+    const float* src = in;
+    for (int it = 0; it < iterations; ++it) {
+        float* dst = ((iterations - 1 - it) % 2 == 0) ? out : tmp;
+        for (int i = tid; i < n; i += nthreads) {
+            const int b = off[i], e = off[i + 1];
+            const double den = 1.0 + static_cast<double>(e - b) / 3.0;
+            for (int c = 0; c < 3; ++c) {
+                double sum = 0.0;
+                for (int k = b; k < e; ++k) sum = sum + static_cast<double>(src[3 * nbr[k] + c]);
+                const double num = static_cast<double>(src[3 * i + c]) + sum / 3.0;
+                dst[3 * i + c] = static_cast<float>(num / den);
+            }
+        }
+        if (it + 1 < iterations && csg::grid_barrier(ctl, phase, timeout_ns, it)) return;
+        src = dst;
     }
 }
 
@@ -150,29 +167,58 @@ __global__ void k_heat_weights(const T* __restrict__ geometry, const int* __rest
     wsum[static_cast<long long>(s) * n + i] = total;
 }
 
-// One smoothing iteration for every series still active (iteration < count).
-// Series s reads in[s * in_stride ...] (in_stride 0: every series starts from
-// the caller's single value array) and writes out[s * n ...]; `in` and `out`
-// never alias (Jacobi update).
-__global__ void k_smooth_values(const double* __restrict__ in, long long in_stride, double* __restrict__ out,
-                                const double* __restrict__ weights, const double* __restrict__ wsum,
-                                const int* __restrict__ off, const int* __restrict__ nbr, int n, SeriesParams sp,
-                                int iteration) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = blockIdx.y;
-    if (i >= n) return;
-    const long long base = static_cast<long long>(s) * n;
-    const double* src = in + static_cast<long long>(s) * in_stride;
-    if (iteration >= sp.count[s]) {
-        out[base + i] = src[i];
-        return;
+// smooth_values (390-476), every iteration of every series in one cooperative
+// launch.  Series s reads in[s * stride ...] (stride 0 in the first iteration:
+// every series starts from the caller's single value array) and writes
+// out[s * n ...]; `in` and `out` never alias (Jacobi update); a series whose
+// iteration count is reached copies its values through; a grid barrier
+// between iterations.
+__global__ void k_smooth_values_all(const double* __restrict__ in, double* __restrict__ out,
+                                    double* __restrict__ tmp, const double* __restrict__ weights,
+                                    const double* __restrict__ wsum, const int* __restrict__ off,
+                                    const int* __restrict__ nbr, int n, int series, SeriesParams sp, int max_it,
+                                    csg::Control* ctl, unsigned long long timeout_ns) {
+    const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long long nthreads = static_cast<long long>(gridDim.x) * blockDim.x;
+    const int slots = off[n];
+    unsigned int phase = 0;
+    const double* src = in;
+    long long stride = 0;
+    for (int it = 0; it < max_it; ++it) {
+        double* dst = ((max_it - 1 - it) % 2 == 0) ? out : tmp;
+        for (long long q = tid; q < static_cast<long long>(series) * n; q += nthreads) {
+            const int s = static_cast<int>(q / n), i = static_cast<int>(q - static_cast<long long>(s) * n);
+            const long long base = static_cast<long long>(s) * n;
+            const double* from = src + static_cast<long long>(s) * stride;
+            if (it >= sp.count[s]) {
+                dst[base + i] = from[i];
+                continue;
+            }
+            const int b = off[i], e = off[i + 1];
+            const double* w = weights + static_cast<long long>(s) * slots;
+            double acc = 0.0;
+            for (int k = b; k < e; ++k) acc = acc + w[k] * from[nbr[k]];
+            dst[base + i] = (from[i] + acc) / (1.0 + wsum[base + i]);
+        }
+        if (it + 1 < max_it && csg::grid_barrier(ctl, phase, timeout_ns, it)) return;
+        src = dst;
+        stride = n;
     }
-    const int b = off[i], e = off[i + 1], slots = off[n];
-    const double* w = weights + static_cast<long long>(s) * slots;
-    double acc = 0.0;
-    for (int k = b; k < e; ++k) acc = acc + w[k] * src[nbr[k]];
-    out[base + i] = (src[i] + acc) / (1.0 + wsum[base + i]);
 }
+
+// Grid of a cooperative launch of `kernel`: as many kThreads-blocks as `work`
+// needs, at most as many as the device holds at once.
+int cooperative_grid(const void* kernel, long long work, unsigned* grid) {
+    int device = 0, sms = 0, per_sm = 0;
+    CSG_CUDA_CHECK(cudaGetDevice(&device));
+    CSG_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CSG_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
+    const long long resident = static_cast<long long>(sms) * (per_sm > 0 ? per_sm : 1);
+    *grid = static_cast<unsigned>(std::max(1LL, std::min(resident, (work + kThreads - 1) / kThreads)));
+    return CSG_OK;
+}
+
+size_t align_up_256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
 // Angle-weighted vertex normals (478-505).  inc lists (face << 2 | corner) per
 // vertex sorted by (corner, face).
@@ -405,19 +451,30 @@ int csg_feature_smooth_geometry(int n_points, const int32_t* nbr_off, const int3
                                 int iterations, float* out, void* scratch, size_t scratch_bytes, csg_stream_t stream) {
     if (n_points < 1 || !nbr_off || !nbr || !vertices || !out || iterations < 0 || !scratch)
         return csg::fail(CSG_ERR_ARG, "smooth geometry: bad arguments");
-    if (scratch_bytes < 12ULL * n_points) return csg::fail(CSG_ERR_ARG, "smooth geometry: scratch too small");
+    const size_t control_at = align_up_256(12ULL * n_points);
+    if (scratch_bytes < control_at + sizeof(csg::Control))
+        return csg::fail(CSG_ERR_ARG, "smooth geometry: scratch too small");
     if (overlaps(vertices, 12ULL * n_points, out, 12ULL * n_points))
         return csg::fail(CSG_ERR_ARG, "smooth geometry: out must not overlap vertices");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     float* tmp = static_cast<float*>(scratch);
-    // Ping-pong so that the last iteration lands in `out`.
-    const float* src = vertices;
-    for (int it = 0; it < iterations; ++it) {
-        float* dst = ((iterations - 1 - it) % 2 == 0) ? out : tmp;
-        (csg::note_launch(), k_smooth_geometry<<<blocks_for(n_points), kThreads, 0, s>>>(src, dst, nbr_off, nbr, n_points));
-        src = dst;
+    if (iterations == 0) {
+        CSG_CUDA_CHECK(cudaMemcpyAsync(out, vertices, 12ULL * n_points, cudaMemcpyDeviceToDevice, s));
+        return CSG_OK;
     }
-    if (iterations == 0) CSG_CUDA_CHECK(cudaMemcpyAsync(out, vertices, 12ULL * n_points, cudaMemcpyDeviceToDevice, s));
+    // Ping-pong so that the last iteration lands in `out`; one cooperative launch.
+    csg::Control* ctl = reinterpret_cast<csg::Control*>(static_cast<char*>(scratch) + control_at);
+    CSG_CUDA_CHECK(cudaMemsetAsync(ctl, 0, sizeof(csg::Control), s));
+    unsigned grid = 1;
+    int rc = cooperative_grid(reinterpret_cast<const void*>(k_smooth_geometry_all), n_points, &grid);
+    if (rc) return rc;
+    unsigned long long timeout_ns = 2000000000ULL;
+    const float* in = vertices;
+    void* args[] = {&in, &out, &tmp, const_cast<int32_t**>(&nbr_off), const_cast<int32_t**>(&nbr), &n_points,
+                    &iterations, &ctl, &timeout_ns};
+    CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_smooth_geometry_all), dim3(grid),
+                                               dim3(kThreads), args, 0, s));
+    csg::note_launch();
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -454,14 +511,22 @@ int csg_feature_smooth_values(int n_points, const int32_t* nbr_off, const int32_
         (csg::note_launch(), k_heat_weights<double><<<grid, kThreads, 0, s>>>(static_cast<const double*>(geometry), nbr_off, nbr, n_points,
                                                           sp, series, via_norm, weights, wsum));
     // Ping-pong between `out` and `tmp` so that the last iteration lands in `out`;
-    // the first iteration reads the caller's values directly.
-    const double* src = values;
-    long long stride = 0;
-    for (int it = 0; it < max_it; ++it) {
-        double* dst = ((max_it - 1 - it) % 2 == 0) ? out : tmp;
-        (csg::note_launch(), k_smooth_values<<<grid, kThreads, 0, s>>>(src, stride, dst, weights, wsum, nbr_off, nbr, n_points, sp, it));
-        src = dst;
-        stride = n_points;
+    // the first iteration reads the caller's values directly; one cooperative launch.
+    if (max_it > 0) {
+        csg::Control* ctl = reinterpret_cast<csg::Control*>(
+            static_cast<char*>(scratch) + align_up_256(8ULL * series * (static_cast<size_t>(n_slots) + 2ULL * n_points)));
+        CSG_CUDA_CHECK(cudaMemsetAsync(ctl, 0, sizeof(csg::Control), s));
+        unsigned cgrid = 1;
+        int rc = cooperative_grid(reinterpret_cast<const void*>(k_smooth_values_all),
+                                  static_cast<long long>(series) * n_points, &cgrid);
+        if (rc) return rc;
+        unsigned long long timeout_ns = 2000000000ULL;
+        const double* in = values;
+        void* args[] = {&in, &out, &tmp, &weights, &wsum, const_cast<int32_t**>(&nbr_off), const_cast<int32_t**>(&nbr),
+                        &n_points, &series, &sp, &max_it, &ctl, &timeout_ns};
+        CSG_CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_smooth_values_all), dim3(cgrid),
+                                                   dim3(kThreads), args, 0, s));
+        csg::note_launch();
     }
     if (max_it == 0)
         for (int k = 0; k < series; ++k)

@@ -210,6 +210,8 @@ def edge_means(pairs) -> list[float]:
 
 
 def _heat_from_edge_mean(edge_mean: float, fwhm: float) -> tuple[int, float]:
+    if not (math.isfinite(edge_mean) and edge_mean > 0.0):
+        raise ValueError(f"heat kernel: the mean edge length is {edge_mean} (a collapsed or non-finite surface)")
     raw = float(fwhm) * float(fwhm) * 0.541011 / (edge_mean * edge_mean)
     iterations = max(1, int(math.ceil(raw)))
     sigma = float(fwhm) * 0.7355345 / float(iterations ** 0.5)

@@ -70,11 +70,11 @@ def no_spawn(monkeypatch):
     return calls
 
 
-def _write_mesh(path: Path, seed: int) -> None:
+def _write_mesh(path: Path, seed: int, subdivisions: int = 3) -> None:
     from cat_surface_gpu_b200 import synthetic
     from cat_surface_gpu_b200.gifti import GiftiMesh, write_gifti_mesh
 
-    vertices, faces = synthetic.folded_icosphere(3, seed=seed)
+    vertices, faces = synthetic.folded_icosphere(subdivisions, seed=seed)
     write_gifti_mesh(path, GiftiMesh(vertices, faces))
 
 
@@ -136,8 +136,9 @@ def test_default_cli_calls_run_on_the_gpu_without_spawning(native_library, tmp_p
     from cat_surface_gpu_b200.cli import surf2sphere_main, surfwarp_main
     from cat_surface_gpu_b200.gifti import read_gifti_mesh
 
+    # 10,242-vertex folded icospheres: CAT_Surf2Sphere's stages 1-4 shrink much coarser meshes to a point
     for seed, name in ((3, "a"), (4, "b")):
-        _write_mesh(tmp_path / f"{name}.gii", seed)
+        _write_mesh(tmp_path / f"{name}.gii", seed, subdivisions=5)
         assert surf2sphere_main(["--input-surface", str(tmp_path / f"{name}.gii"), "--output-surface",
                                  str(tmp_path / f"{name}.sphere.gii"), "--device", "cuda:0"]) == 0
         sphere = read_gifti_mesh(tmp_path / f"{name}.sphere.gii").vertices.astype(np.float64)
