@@ -87,6 +87,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_rotation_grid_scratch_bytes": (c_size_t, [_I]),
     "csg_rotation_grid_build_device": (_I, [_P, _I, _P, _I, _I, _I, _P, _P, ctypes.c_longlong, _P, _P, c_size_t, _P]),
     "csg_rotation_cost_batch": (_I, [_I, _P, _P, _I, _I, _P, c_size_t, _P]),
+    "csg_rotation_triangle_records": (_I, [_P, _I, _P, _P]),
     "csg_rotation_status": (_I, [_P, _I, _P, _P]),
     "csg_feature_resample": (_I, [_I, _I, _P, _P, _P, _P, _P]),
     "csg_feature_sheet_map": (_I, [_I, _P, _P, _P, _P, _P]),
@@ -121,6 +122,7 @@ class RotationSurface(ctypes.Structure):
         ("n_candidates", ctypes.c_int32),
         ("n_features", ctypes.c_int32),
         ("n_tgt_points", ctypes.c_int32),
+        ("records", c_void_p),
     ]
 
 

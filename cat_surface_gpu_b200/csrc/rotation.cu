@@ -37,6 +37,7 @@ struct RotSurface {
     const int* grid_offsets;     // [G^3 + 1]
     const int* grid_faces;       // CSR faces
     const float* matrices;       // [n_candidates][9] column-major
+    const float* records;        // [n_tri][16] triangle records or null
     double* partials;            // [n_candidates][tiles]
     int n_src;
     int grid_size;
@@ -121,6 +122,74 @@ __device__ __forceinline__ float candidate(const float* q, const float* t, float
     return first ? d1 : d2;
 }
 
+// The same candidate from a precomputed triangle record (corners, n, n.n,
+// ea.ea, ea.eb, eb.eb; see csg_rotation_triangle_records): four 16-byte loads
+// instead of nine scalar ones, and the cross and dot products of the corners
+// read instead of formed.  Every value is the one candidate() forms, so the
+// result is the same bit for bit.
+__device__ __forceinline__ float candidate_record(const float* q, const float* rec, float* point) {
+    const float4* r4 = reinterpret_cast<const float4*>(rec);
+    const float4 r0 = __ldg(r4), r1 = __ldg(r4 + 1), r2 = __ldg(r4 + 2), r3 = __ldg(r4 + 3);
+    const float t[9] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x};
+    const float n[3] = {r2.y, r2.z, r2.w};
+    const float nsq = r3.x, xx = r3.y, xy = r3.z, yy = r3.w;
+    const float* p0 = t;
+    float ea[3], eb[3], off[3];
+    sub3(t + 3, p0, ea);
+    sub3(t + 6, p0, eb);
+    sub3(p0, q, off);
+    const float plane_t = nsq != 0.0f ? dot3(off, n) / nsq : 0.0f;
+    float proj[3], po[3];
+    for (int k = 0; k < 3; ++k) proj[k] = q[k] + plane_t * n[k];
+    sub3(proj, p0, po);
+    const float xv = dot3(ea, po), yv = dot3(eb, po);
+    const float den = xx * yy - xy * xy;
+    const float xpos = den != 0.0f ? (xv * yy - yv * xy) / den : 0.0f;
+    const float ypos = den != 0.0f ? (yv * xx - xv * xy) / den : 0.0f;
+    const float lo = -1.0e-3f, hi = static_cast<float>(1.0 + 1.0e-3);
+    const float s = xpos + ypos;
+    const bool inside = den != 0.0f && xpos >= lo && xpos <= hi && ypos >= lo && ypos <= hi && s >= lo && s <= hi;
+    if (inside) {
+        for (int k = 0; k < 3; ++k) point[k] = proj[k];
+        return plane_t * plane_t * nsq;
+    }
+    float d[3][3];
+    float vd[3];
+    for (int v = 0; v < 3; ++v) {
+        sub3(q, t + 3 * v, d[v]);
+        vd[v] = dot3(d[v], d[v]);
+    }
+    int cv = 0;  // first minimum
+    if (vd[1] < vd[cv]) cv = 1;
+    if (vd[2] < vd[cv]) cv = 2;
+    const float* closest = t + 3 * cv;
+    const float* prev = t + 3 * ((cv + 2) % 3);
+    const float* next = t + 3 * ((cv + 1) % 3);
+    float c1[3], c2[3];
+    const float d1 = segment(q, prev, closest, c1);
+    const float d2 = segment(q, closest, next, c2);
+    const bool first = d1 < d2;
+    for (int k = 0; k < 3; ++k) point[k] = first ? c1[k] : c2[k];
+    return first ? d1 : d2;
+}
+
+__global__ void k_triangle_records(const float* __restrict__ tri, int n, float* __restrict__ rec) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    const float* t = tri + 9LL * f;
+    float ea[3], eb[3], nv[3];
+    sub3(t + 3, t, ea);
+    sub3(t + 6, t, eb);
+    cross3(ea, eb, nv);
+    float* r = rec + 16LL * f;
+    for (int k = 0; k < 9; ++k) r[k] = t[k];
+    for (int k = 0; k < 3; ++k) r[9 + k] = nv[k];
+    r[12] = dot3(nv, nv);
+    r[13] = dot3(ea, ea);
+    r[14] = dot3(ea, eb);
+    r[15] = dot3(eb, eb);
+}
+
 // Barycentric weights of `point` in triangle t (surface_rotation.py:335-352).
 __device__ __forceinline__ void barycentric(const float* point, const float* t, float w[3]) {
     const int order[3][3] = {{1, 2, 0}, {2, 0, 1}, {0, 1, 2}};
@@ -175,7 +244,8 @@ __global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __rest
                 for (int k = begin; k < end; ++k) {
                     const int f = S.grid_faces[k];
                     float point[3];
-                    const float d = candidate(q, S.triangles + 9 * static_cast<long long>(f), point);
+                    const float d = S.records ? candidate_record(q, S.records + 16 * static_cast<long long>(f), point)
+                                              : candidate(q, S.triangles + 9 * static_cast<long long>(f), point);
                     if (d < best) {
                         best = d;
                         best_face = f;
@@ -404,6 +474,8 @@ int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces
             !in.grid_faces || !in.matrices || in.n_src < 1 || in.n_candidates < 1 || in.grid_size < 4 ||
             in.n_features < 0 || (in.n_features > 1 && in.n_tgt_points < 1))
             return csg::fail(CSG_ERR_ARG, "rotation cost: surface %d is incomplete", s);
+        if (reinterpret_cast<uintptr_t>(in.records) % 16 != 0)
+            return csg::fail(CSG_ERR_ARG, "rotation cost: surface %d's triangle records are not 16-byte aligned", s);
         ns[s] = in.n_src;
         nc[s] = in.n_candidates;
     }
@@ -431,6 +503,7 @@ int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces
         r.grid_offsets = in.grid_offsets;
         r.grid_faces = in.grid_faces;
         r.matrices = in.matrices;
+        r.records = in.records;
         r.n_src = in.n_src;
         r.grid_size = in.grid_size;
         r.n_candidates = in.n_candidates;
@@ -502,6 +575,16 @@ int csg_rotation_grid_build_device(const double* points, int n_points, const int
     (csg::note_launch(), k_rgrid_fill<<<fb, 256, 0, st>>>(points, faces, n_faces, G, margin, cursor, cell_faces));
     (csg::note_launch(), k_rgrid_sort<<<static_cast<unsigned>((cells + 255) / 256), 256, 0, st>>>(offsets, cells,
                                                                                                  cell_faces));
+    CSG_CUDA_CHECK(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_rotation_triangle_records(const float* triangles, int n_tri, float* records, csg_stream_t stream) {
+    if (!triangles || !records || n_tri < 1) return csg::fail(CSG_ERR_ARG, "triangle records: bad arguments");
+    if (reinterpret_cast<uintptr_t>(records) % 16 != 0)
+        return csg::fail(CSG_ERR_ARG, "triangle records: records must be 16-byte aligned");
+    (csg::note_launch(), k_triangle_records<<<static_cast<unsigned>((n_tri + 255) / 256), 256, 0,
+                                              reinterpret_cast<cudaStream_t>(stream)>>>(triangles, n_tri, records));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }

@@ -234,6 +234,7 @@ class _Costing:
             self.index.candidate_faces.data_ptr(), self.matrices.data_ptr(),
             int(self.inputs.source_points.shape[0]), int(self.index.grid_size), int(count),
             int(self.inputs.n_features), int(self.index.target_points.shape[0]),
+            self.index.target_records.data_ptr(),
         )
         lib = _native.library()
         stream = _native.stream_handle(like=self.costs)
@@ -269,6 +270,20 @@ class RotationGridIndexDevice:
     @property
     def device(self) -> torch.device:
         return self.target_points.device
+
+    @property
+    def target_records(self) -> torch.Tensor:
+        """[n_tri, 16] float32 per-triangle terms of the closest-polygon test (built once, on the device)."""
+
+        records = self.__dict__.get("_records")
+        if records is None:
+            tri = self.target_triangles.reshape(-1, 9).contiguous()
+            records = torch.empty((tri.shape[0], 16), dtype=torch.float32, device=self.device)
+            _native.check(_native.library().csg_rotation_triangle_records(
+                tri.data_ptr(), int(tri.shape[0]), records.data_ptr(), _native.stream_handle(like=records)),
+                "csg_rotation_triangle_records")
+            self.__dict__["_records"] = records
+        return records
 
     @classmethod
     def build(cls, points, faces, *, device, grid_size: int = 128, margin: int = 1) -> "RotationGridIndexDevice":
@@ -565,7 +580,7 @@ def batched_costs(indices, inputs, angle_sets=None, *, matrix_sets=None, tile: i
             inp.source_points.data_ptr(), inp.source_values.data_ptr(), index.target_triangles.data_ptr(),
             index.target_faces.data_ptr(), inp.target_values.data_ptr(), index.candidate_offsets.data_ptr(),
             index.candidate_faces.data_ptr(), m.data_ptr(), int(inp.source_points.shape[0]), int(index.grid_size),
-            counts[i], int(inp.n_features), int(index.target_points.shape[0]),
+            counts[i], int(inp.n_features), int(index.target_points.shape[0]), index.target_records.data_ptr(),
         )
     n_src = (ctypes.c_int * n)(*[int(inp.source_points.shape[0]) for inp in inputs])
     n_cand = (ctypes.c_int * n)(*counts)

@@ -225,3 +225,44 @@ def test_tetrahedron_known_answers(native_library):
     angle, cost, iterations = index.refine_nelder_mead(points, zeros, zeros, np.zeros(3))
     np.testing.assert_array_equal(angle.cpu().numpy(), np.zeros(3))
     assert float(cost) == 0.0 and iterations == 1
+
+
+@pytest.mark.gpu
+def test_triangle_records_give_the_same_costs(native_library):
+    """Costs with precomputed triangle records equal costs formed per query, bit for bit."""
+
+    import ctypes
+
+    import torch
+
+    from cat_surface_gpu_b200 import _native
+    from cat_surface_gpu_b200.surface_rotation import RotationGridIndexDevice, rotation_matrices_flat
+    from cat_surface_gpu_b200.surface_stencil import resampling_sphere
+
+    rng = np.random.default_rng(12)
+    tp, tf = resampling_sphere(5)
+    index = RotationGridIndexDevice.build(tp, tf, device="cuda:0", grid_size=64, margin=1)
+    src = rng.normal(size=(20000, 3))
+    src = (src / np.linalg.norm(src, axis=1, keepdims=True)).astype(np.float32)
+    inputs = index.prepare_cost_inputs(src, np.sin(4 * src[:, 0]).astype(np.float64), np.sin(4 * tp[:, 0]))
+    mats = torch.as_tensor(rotation_matrices_flat(rng.uniform(-1, 1, size=(24, 3))), device="cuda:0")
+    lib = _native.library()
+    out = []
+    for records in (None, index.target_records.data_ptr()):
+        surface = _native.RotationSurface(
+            inputs.source_points.data_ptr(), inputs.source_values.data_ptr(), index.target_triangles.data_ptr(),
+            index.target_faces.data_ptr(), inputs.target_values.data_ptr(), index.candidate_offsets.data_ptr(),
+            index.candidate_faces.data_ptr(), mats.data_ptr(), src.shape[0], index.grid_size, 24, 1,
+            int(index.target_points.shape[0]), records)
+        n_src, n_cand = (ctypes.c_int * 1)(src.shape[0]), (ctypes.c_int * 1)(24)
+        need = lib.csg_rotation_scratch_bytes(1, ctypes.addressof(n_src), ctypes.addressof(n_cand), 256)
+        scratch = torch.empty(int(need), dtype=torch.uint8, device="cuda:0")
+        costs = torch.empty(24, dtype=torch.float64, device="cuda:0")
+        _native.check(lib.csg_rotation_cost_batch(1, ctypes.addressof(surface), costs.data_ptr(), 256, 0,
+                                                  scratch.data_ptr(), scratch.numel(),
+                                                  _native.stream_handle(like=costs)), "csg_rotation_cost_batch")
+        out.append(costs.cpu().numpy())
+    assert np.array_equal(out[0], out[1])
+    records = index.target_records.cpu().numpy()
+    tri = index.target_triangles.reshape(-1, 9).cpu().numpy()
+    assert np.array_equal(records[:, :9], tri)
