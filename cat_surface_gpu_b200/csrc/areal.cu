@@ -484,13 +484,16 @@ __device__ __forceinline__ bool load_versioned(const unsigned long long* pub, in
     return word_version(a) == need && word_version(b) == need && word_version(c) == need;
 }
 
+__device__ __forceinline__ bool wait_expired(const ArealParams& p, unsigned int& polls, unsigned long long& start) {
+    return csg::warp_wait_expired(p.ctl, p.timeout_ns, polls, start);
+}
 
 // Ring of a vertex: itself, then the other vertices of its faces (at most
 // kRingMax); each face slot is coded as three ring indices (8 bits each).
 constexpr int kRingMax = 20;
 
-// One vertex update of sweep s by a group of G lanes (every lane of the group
-// calls it; an inactive group passes v < 0).  The group first polls the words of the ring --
+// One vertex update of sweep s by a group of G lanes (all 32 lanes call it;
+// inactive groups pass v < 0).  The group first polls the words of the ring --
 // lane j loads members j, j + G, ... all at once, one round trip per poll --
 // and stages the positions in shared memory (`pos`, kRingMax entries per
 // group), then computes the faces exactly as update_vertex does (same
@@ -507,10 +510,6 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
     const int lane = threadIdx.x & 31;
     const int glane = lane & (G - 1);
     const int gbase = lane & ~(G - 1);
-    // every collective below is scoped to this group's lanes: the groups of a
-    // warp poll, compute and publish independently, so a group whose ring is
-    // ready does not wait for the warp's other vertices
-    const unsigned gmask = (G == 32 ? kFull : ((1u << G) - 1u)) << gbase;
     if (v < 0) {
         deg = 0;
         nring = 0;
@@ -539,11 +538,11 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
                      word_version(w[q][2]) == need;
                 pos[glane + q * G] = make_float3(word_value(w[q][0]), word_value(w[q][1]), word_value(w[q][2]));
             }
-        if (__all_sync(gmask, ok)) break;
-        if (csg::group_wait_expired(p.ctl, p.timeout_ns, polls, start, gmask, gbase)) return false;
+        if (__all_sync(kFull, ok)) break;
+        if (wait_expired(p, polls, start)) return false;
     }
-    __syncwarp(gmask);
-    const int wdeg = __reduce_max_sync(gmask, deg);
+    __syncwarp();
+    const int wdeg = __reduce_max_sync(kFull, deg);
     Acc total = 0, wx = 0, wy = 0, wz = 0;  // float path: every lane sums its group's faces
     double wsum = 0;                        // float64 path: lanes 0..2 sum one coordinate each
     for (int c0 = 0; c0 < wdeg; c0 += G) {
@@ -570,7 +569,7 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
             stage[1][lane] = fx;
             stage[2][lane] = fy;
             stage[3][lane] = fz;
-            __syncwarp(gmask);
+            __syncwarp();
             if (glane < 3) {
                 const double* mine = stage[1 + glane];
                 const int n = min(G, deg - c0);
@@ -582,16 +581,16 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
                     }
                 }
             }
-            __syncwarp(gmask);
+            __syncwarp();
         } else {
             Acc fa = 0, fx = 0, fy = 0, fz = 0;
             if (face) T::face(a, b, c, fa, fx, fy, fz);
 #pragma unroll
             for (int q = 0; q < G; ++q) {
-                const Acc aa = __shfl_sync(gmask, fa, gbase + q);
-                const Acc x = __shfl_sync(gmask, fx, gbase + q);
-                const Acc y = __shfl_sync(gmask, fy, gbase + q);
-                const Acc z = __shfl_sync(gmask, fz, gbase + q);
+                const Acc aa = __shfl_sync(kFull, fa, gbase + q);
+                const Acc x = __shfl_sync(kFull, fx, gbase + q);
+                const Acc y = __shfl_sync(kFull, fy, gbase + q);
+                const Acc z = __shfl_sync(kFull, fz, gbase + q);
                 if (c0 + q < deg) {  // slot order == ascending face id
                     total = dadd<Acc>(total, aa);
                     wx = dadd<Acc>(wx, dmul<Acc>(aa, x));
@@ -619,12 +618,12 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
             ny = __fdiv_rn(wy, safe);
             nz = __fdiv_rn(wz, safe);
         }
-        const int m = __shfl_sync(gmask, moved ? 1 : 0, gbase);
-        const float ny1 = __shfl_sync(gmask, ny, gbase);
-        const float nz2 = __shfl_sync(gmask, nz, gbase);
+        const int m = __shfl_sync(kFull, moved ? 1 : 0, gbase);
+        const float ny1 = __shfl_sync(kFull, ny, gbase);
+        const float nz2 = __shfl_sync(kFull, nz, gbase);
         if (m) value = glane == 0 ? nx : (glane == 1 ? ny1 : nz2);
     }
-    __syncwarp(gmask);  // every lane is done with `pos` before the next update overwrites it
+    __syncwarp();  // every lane is done with `pos` before the next update overwrites it
     if (v >= 0 && glane < 3) st_word(pub + 4LL * v + glane, make_word(value, s));
     return true;
 }

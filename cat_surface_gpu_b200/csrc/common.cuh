@@ -149,24 +149,4 @@ __device__ __forceinline__ bool warp_wait_expired(Control* ctl, unsigned long lo
     return __shfl_sync(0xffffffffu, expired, 0) != 0;
 }
 
-// The same bounded wait for one group of lanes of a warp (mask `group`,
-// first lane `leader`): the leader checks the clock and the status word every
-// 64 polls and the answer is shared within the group only, so the warp's
-// other groups keep their own pace.
-__device__ __forceinline__ bool group_wait_expired(Control* ctl, unsigned long long timeout_ns, unsigned int& polls,
-                                                   unsigned long long& start, unsigned group, int leader) {
-    int expired = 0;
-    if ((threadIdx.x & 31) == leader && ((++polls) & 63u) == 0u) {
-        const unsigned long long now = global_timer_ns();
-        if (start == 0) start = now;
-        if (ld_relaxed_gpu(&ctl->status) != CSG_OK) {
-            expired = 1;
-        } else if (now - start > timeout_ns) {
-            if (atomicCAS(&ctl->status, CSG_OK, CSG_ERR_TIMEOUT) == CSG_OK) ctl->where = -2;
-            expired = 1;
-        }
-    }
-    return __shfl_sync(group, expired, leader) != 0;
-}
-
 }  // namespace csg

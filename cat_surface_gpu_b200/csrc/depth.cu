@@ -458,8 +458,6 @@ __device__ __forceinline__ bool sor_row_df(const SorParams& p, int b, int v, con
     const int lane = threadIdx.x & 31;
     const int glane = lane & (G - 1);
     const int gbase = lane & ~(G - 1);
-    // collectives scoped to this group's lanes: the warp's groups progress independently
-    const unsigned gmask = (G == 32 ? kFull : ((1u << G) - 1u)) << gbase;
     const unsigned long long* pub = p.pub + 2LL * p.n * b;
     if (v < 0) {
         nring = 0;
@@ -490,11 +488,11 @@ __device__ __forceinline__ bool sor_row_df(const SorParams& p, int b, int v, con
                 ok = ok && csg::word_version(w[q][0]) == need[q] && csg::word_version(w[q][1]) == need[q];
                 ringx[glane + q * G] = words_value(w[q][0], w[q][1]);
             }
-        if (__all_sync(gmask, ok)) break;
-        if (csg::group_wait_expired(p.ctl, p.timeout_ns, polls, start, gmask, gbase)) return false;
+        if (__all_sync(kFull, ok)) break;
+        if (csg::warp_wait_expired(p.ctl, p.timeout_ns, polls, start)) return false;
     }
-    __syncwarp(gmask);
-    const int wlen = __reduce_max_sync(gmask, len);
+    __syncwarp();
+    const int wlen = __reduce_max_sync(kFull, len);
     double sum = 0.0;
     for (int base = 0; base < wlen; base += G * kE) {
         double prod[kE];
@@ -505,16 +503,16 @@ __device__ __forceinline__ bool sor_row_df(const SorParams& p, int b, int v, con
         }
 #pragma unroll
         for (int q = 0; q < kE; ++q) {
-            if (base + q * G >= wlen) break;  // group-uniform
+            if (base + q * G >= wlen) break;  // warp-uniform
 #pragma unroll
             for (int i = 0; i < G; ++i) {
-                const double t = __shfl_sync(gmask, prod[q], gbase + i);
+                const double t = __shfl_sync(kFull, prod[q], gbase + i);
                 if (base + q * G + i < len) sum = sum + t;
             }
         }
     }
     const double xv = v >= 0 ? ringx[0] : 0.0;
-    __syncwarp(gmask);  // every lane is done with `ringx` before the next row overwrites it
+    __syncwarp();  // every lane is done with `ringx` before the next row overwrites it
     if (v >= 0 && glane < 2) {
         const double nx = xv + p.relaxation * (rhs - sum) / diag;
         const unsigned int half = glane == 0 ? static_cast<unsigned>(__double2loint(nx))

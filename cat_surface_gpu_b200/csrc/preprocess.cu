@@ -299,8 +299,6 @@ __device__ __forceinline__ bool pass_vertex_df(const PassParams& p, int v, const
     const int lane = threadIdx.x & 31;
     const int glane = lane & (G - 1);
     const int gbase = lane & ~(G - 1);
-    // collectives scoped to this group's lanes: the warp's groups progress independently
-    const unsigned gmask = (G == 32 ? kFull : ((1u << G) - 1u)) << gbase;
     const int kind = p.seg[sg].kind;
     const double strength = p.seg[sg].value;
     if (v < 0) nring = 0;
@@ -329,14 +327,14 @@ __device__ __forceinline__ bool pass_vertex_df(const PassParams& p, int v, const
                 pos[glane + q * G] = make_float3(csg::word_value(w[q][0]), csg::word_value(w[q][1]),
                                                  csg::word_value(w[q][2]));
             }
-        if (__all_sync(gmask, ok)) break;
-        if (csg::group_wait_expired(p.ctl, p.timeout_ns, polls, start, gmask, gbase)) return false;
+        if (__all_sync(kFull, ok)) break;
+        if (csg::warp_wait_expired(p.ctl, p.timeout_ns, polls, start)) return false;
     }
-    __syncwarp(gmask);
+    __syncwarp();
     int deg = nring > 0 ? nring - 1 : 0;
     const bool active = v >= 0 && kind != kInflate && deg > 1 && (kind == kSmoothAll || p.selected[v]);
     if (!active) deg = 0;
-    const int wdeg = __reduce_max_sync(gmask, deg);
+    const int wdeg = __reduce_max_sync(kFull, deg);
     double o[3] = {0.0, 0.0, 0.0};
     if (v >= 0) {
         o[0] = pos[0].x;
@@ -362,7 +360,7 @@ __device__ __forceinline__ bool pass_vertex_df(const PassParams& p, int v, const
         stage[1][lane] = dx;
         stage[2][lane] = dy;
         stage[3][lane] = dz;
-        __syncwarp(gmask);
+        __syncwarp();
         if (glane < 3) {
             const int m = min(G, deg - c0);
 #pragma unroll
@@ -374,7 +372,7 @@ __device__ __forceinline__ bool pass_vertex_df(const PassParams& p, int v, const
                 }
             }
         }
-        __syncwarp(gmask);
+        __syncwarp();
     }
     float value = 0.0f;
     if (v >= 0 && glane < 3) {
@@ -392,7 +390,7 @@ __device__ __forceinline__ bool pass_vertex_df(const PassParams& p, int v, const
             value = static_cast<float>(o[comp]);
         }
     }
-    __syncwarp(gmask);  // every lane is done with `pos` before the next update overwrites it
+    __syncwarp();  // every lane is done with `pos` before the next update overwrites it
     if (v >= 0 && glane < 3) csg::st_word(p.pub + 4LL * v + glane, csg::make_word(value, pass + 1));
     return true;
 }
