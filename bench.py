@@ -1046,7 +1046,10 @@ def run_native(args):
                                 "reference_binary_surf2sphere_s": meshes["binary_seconds"]}}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": False,
+            "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps,
+            "step_ms_each": [round(ms, 3) for ms in step_ms],
+            "dartel_s_each": [round(t.get("dartel_total_seconds", 0.0), 4) for t in stage],
+            "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {**workload_config(meshes),
                        "levels": hemi.plan.n_levels, "wavefront_stride": hemi.plan.level_stride,
