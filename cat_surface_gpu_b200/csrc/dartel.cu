@@ -123,18 +123,15 @@ __global__ void k_smalldef(const T* __restrict__ v, T* __restrict__ map, T* __re
     }
 }
 
-// (c, jc) = (b o a, J_b(a) . J_a) (dartel_grid.py:407-507); jac pointers may be null.
+// (c, jc) = (b o a, J_b(a) . J_a) (dartel_grid.py:407-507) at point p, with the
+// stencil of a at p; jac pointers may be null.
 template <typename T>
-__global__ void k_compose(const T* __restrict__ a, const T* __restrict__ ja, const T* __restrict__ b,
-                          const T* __restrict__ jb, T* __restrict__ c, T* __restrict__ jc, int nx, int ny) {
-    csg::pdl_begin();
-    Pt p;
-    if (!point(nx, ny, p)) return;
+__device__ __forceinline__ void compose_at(const Stencil<T>& st, const T* __restrict__ a, const T* __restrict__ ja,
+                                           const T* __restrict__ b, const T* __restrict__ jb, T* __restrict__ c,
+                                           T* __restrict__ jc, int nx, int ny, const Pt& p) {
     const int P = nx * ny;
     const size_t o2 = static_cast<size_t>(p.b) * 2 * P, o4 = static_cast<size_t>(p.b) * 4 * P;
-    const T* A = a + o2;
     const T* Bm = b + o2;
-    const Stencil<T> st(A[p.i] - T(1), A[P + p.i] - T(1), nx, ny);
     T* C = c + o2;
 #pragma unroll
     for (int ch = 0; ch < 2; ++ch) {
@@ -158,6 +155,18 @@ __global__ void k_compose(const T* __restrict__ a, const T* __restrict__ ja, con
         J[2 * P + p.i] = jb00 * ja2 + jb10 * ja3;
         J[3 * P + p.i] = jb01 * ja2 + jb11 * ja3;
     }
+}
+
+template <typename T>
+__global__ void k_compose(const T* __restrict__ a, const T* __restrict__ ja, const T* __restrict__ b,
+                          const T* __restrict__ jb, T* __restrict__ c, T* __restrict__ jc, int nx, int ny) {
+    csg::pdl_begin();
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const T* A = a + static_cast<size_t>(p.b) * 2 * P;
+    const Stencil<T> st(A[p.i] - T(1), A[P + p.i] - T(1), nx, ny);
+    compose_at(st, a, ja, b, jb, c, jc, nx, ny, p);
 }
 
 // jac_div_smalldef (dartel_grid.py:678-720) at one point.
@@ -253,22 +262,19 @@ __global__ void k_objfun(const T* __restrict__ source, const T* __restrict__ tar
 }
 
 // One scaling-and-squaring increment (dartel_grid.py:832-893; the fused
-// form of dartel_triton.py:345-477): b_out = b + inc_b, a_out = a + inc_a,
-// inc = inc_b.  Out of place (the gathers read b and a at other points).
+// form of dartel_triton.py:345-477) at point p: b_out = b + inc_b, a_out = a +
+// inc_a, inc = inc_b (inc may be null).  Out of place (the gathers read b and
+// a at other points).  st is the stencil of map at p.
 template <typename T>
-__global__ void k_squaring(const T* __restrict__ b, const T* __restrict__ a, const T* __restrict__ map,
-                           const T* __restrict__ jac, T* __restrict__ b_out, T* __restrict__ a_out,
-                           T* __restrict__ inc, int nx, int ny) {
-    csg::pdl_begin();
-    Pt p;
-    if (!point(nx, ny, p)) return;
+__device__ __forceinline__ void squaring_at(const Stencil<T>& st, const T* __restrict__ b, const T* __restrict__ a,
+                                            const T* __restrict__ map, const T* __restrict__ jac,
+                                            T* __restrict__ b_out, T* __restrict__ a_out, T* __restrict__ inc,
+                                            int nx, int ny, const Pt& p) {
     const int P = nx * ny;
     const size_t o1 = static_cast<size_t>(p.b) * P;
-    const T* M = map + 2 * o1;
     const T* J = jac + 4 * o1;
     const T* Bv = b + 2 * o1;
     const T* Av = a + 3 * o1;
-    const Stencil<T> st(M[p.i] - T(1), M[P + p.i] - T(1), nx, ny);
     const T j00 = J[p.i], j10 = J[P + p.i], j01 = J[2 * P + p.i], j11 = J[3 * P + p.i];
     const T det = j00 * j11 - j01 * j10;
     const T sbx = st.interp(Bv), sby = st.interp(Bv + P);
@@ -289,9 +295,43 @@ __global__ void k_squaring(const T* __restrict__ b, const T* __restrict__ a, con
     AO[p.i] = Av[p.i] + ia00;
     AO[P + p.i] = Av[P + p.i] + ia11;
     AO[2 * P + p.i] = Av[2 * P + p.i] + ia01;
-    T* I = inc + 2 * o1;
-    I[p.i] = ibx;
-    I[P + p.i] = iby;
+    if (inc) {
+        T* I = inc + 2 * o1;
+        I[p.i] = ibx;
+        I[P + p.i] = iby;
+    }
+}
+
+template <typename T>
+__global__ void k_squaring(const T* __restrict__ b, const T* __restrict__ a, const T* __restrict__ map,
+                           const T* __restrict__ jac, T* __restrict__ b_out, T* __restrict__ a_out,
+                           T* __restrict__ inc, int nx, int ny) {
+    csg::pdl_begin();
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const T* M = map + static_cast<size_t>(p.b) * 2 * P;
+    const Stencil<T> st(M[p.i] - T(1), M[P + p.i] - T(1), nx, ny);
+    squaring_at(st, b, a, map, jac, b_out, a_out, inc, nx, ny, p);
+}
+
+// One squaring step followed by the composition of the map with itself, in one
+// pass: (b, a) advance as in k_squaring and (map_out, jac_out) = (map o map,
+// J(map) . J).  Both read the same map at the same stencil and neither reads
+// what the other writes, so the pass equals the two launches; the increment
+// k_squaring would store in map_out is overwritten by the composed map there.
+template <typename T>
+__global__ void k_squaring_compose(const T* __restrict__ b, const T* __restrict__ a, const T* __restrict__ map,
+                                   const T* __restrict__ jac, T* __restrict__ b_out, T* __restrict__ a_out,
+                                   T* __restrict__ map_out, T* __restrict__ jac_out, int nx, int ny) {
+    csg::pdl_begin();
+    Pt p;
+    if (!point(nx, ny, p)) return;
+    const int P = nx * ny;
+    const T* M = map + static_cast<size_t>(p.b) * 2 * P;
+    const Stencil<T> st(M[p.i] - T(1), M[P + p.i] - T(1), nx, ny);
+    squaring_at(st, b, a, map, jac, b_out, a_out, static_cast<T*>(nullptr), nx, ny, p);
+    compose_at(st, map, jac, map, jac, map_out, jac_out, nx, ny, p);
 }
 
 // regularization_operator weights (dartel_grid.py:937-1015), host-computed
@@ -556,11 +596,16 @@ __global__ void k_resize(const T* __restrict__ src, T* __restrict__ dst, int snx
 // separate kernels (relax_at, membrane_apply_at, resize_at) in the same
 // order, phases separated by __syncthreads.  A coarse level's work is a few
 // thousand points, so one CTA covers it, and ~100 small launches per cycle
-// become one.
+// become one.  Every level's Hessian, right-hand side, solution and residual
+// live in shared memory for the whole cycle (at most ~1,100 points over all
+// levels, 9 words each): the CTA reads the Hessians and the first level's
+// right-hand side and solution once, and writes back the first level's
+// solution, the only field read after the cycle.
 
 constexpr int kCoarsePoints = 512;  // measured: 512 beats 0, 2048 and 8192 at 256 x 128
 constexpr int kMaxLevels = 16;
 constexpr int kCoarseThreads = 1024;
+constexpr int kCoarseCycleThreads = 512;
 
 template <typename T>
 struct CoarseLevel {
@@ -571,6 +616,7 @@ struct CoarseLevel {
     int nx, ny;
     T w00, w01, w10;
     RegWeights rw;
+    int off;  // offset of the level's [A 3 | B 2 | U 2 | R 2] x nx x ny block in shared memory (elements)
 };
 
 template <typename T>
@@ -601,31 +647,71 @@ __device__ __forceinline__ void block_resize(const T* src, int snx, int sny, T* 
     __syncthreads();
 }
 
+// The shared-memory image of level L (one batch element, batch index 0).
+template <typename T>
+__device__ __forceinline__ CoarseLevel<T> shared_level(const CoarseLevel<T>& L, T* base) {
+    CoarseLevel<T> S = L;
+    const int P = L.nx * L.ny;
+    T* a = base + L.off;
+    S.A = a;
+    S.B = a + 3 * P;
+    S.U = a + 5 * P;
+    S.R = a + 7 * P;
+    return S;
+}
+
 // cycle(first) of Fmg (host side) restricted to levels first..last, for batch element blockIdx.x.
 template <typename T>
-__global__ void __launch_bounds__(kCoarseThreads) k_fmg_coarse_cycle(CoarseCycle<T> c) {
+__global__ void __launch_bounds__(kCoarseCycleThreads) k_fmg_coarse_cycle(CoarseCycle<T> c) {
     csg::pdl_begin();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* base = reinterpret_cast<T*>(smem_raw);
     const int bi = blockIdx.x;
-    for (int l = c.first; l < c.last; ++l) {
+    for (int l = c.first; l <= c.last; ++l) {
         const CoarseLevel<T>& L = c.lv[l];
-        block_relax(L, bi, c.nit);
+        const CoarseLevel<T> S = shared_level(L, base);
+        const int P = L.nx * L.ny;
+        for (int j = threadIdx.x; j < 3 * P; j += blockDim.x)
+            const_cast<T*>(S.A)[j] = L.A[3 * static_cast<size_t>(bi) * P + j];
+        if (l == c.first)
+            for (int j = threadIdx.x; j < 2 * P; j += blockDim.x) {
+                S.B[j] = L.B[2 * static_cast<size_t>(bi) * P + j];
+                S.U[j] = L.U[2 * static_cast<size_t>(bi) * P + j];
+            }
+    }
+    __syncthreads();
+    for (int l = c.first; l < c.last; ++l) {
+        const CoarseLevel<T> L = shared_level(c.lv[l], base);
+        block_relax(L, 0, c.nit);
         const int P = L.nx * L.ny;
         for (int i = threadIdx.x; i < P; i += blockDim.x)
-            membrane_apply_at(L.A, L.U, L.B, L.R, L.nx, L.ny, L.rw, Pt{bi, i % L.nx, i / L.nx, i});
+            membrane_apply_at(L.A, L.U, L.B, L.R, L.nx, L.ny, L.rw, Pt{0, i % L.nx, i / L.nx, i});
         __syncthreads();
-        const CoarseLevel<T>& N = c.lv[l + 1];
-        block_resize(L.R, L.nx, L.ny, N.B, N.nx, N.ny, bi, 0);
+        const CoarseLevel<T> N = shared_level(c.lv[l + 1], base);
+        block_resize(L.R, L.nx, L.ny, N.B, N.nx, N.ny, 0, 0);
         const int Pn = N.nx * N.ny;
-        for (int j = threadIdx.x; j < 2 * Pn; j += blockDim.x) N.U[2 * static_cast<size_t>(bi) * Pn + j] = T(0);
+        for (int j = threadIdx.x; j < 2 * Pn; j += blockDim.x) N.U[j] = T(0);
         __syncthreads();
     }
-    block_relax(c.lv[c.last], bi, c.nit);
+    block_relax(shared_level(c.lv[c.last], base), 0, c.nit);
     for (int l = c.last; l-- > c.first;) {
-        const CoarseLevel<T>& L = c.lv[l];
-        const CoarseLevel<T>& N = c.lv[l + 1];
-        block_resize(N.U, N.nx, N.ny, L.U, L.nx, L.ny, bi, 1);
-        block_relax(L, bi, c.nit);
+        const CoarseLevel<T> L = shared_level(c.lv[l], base);
+        const CoarseLevel<T> N = shared_level(c.lv[l + 1], base);
+        block_resize(N.U, N.nx, N.ny, L.U, L.nx, L.ny, 0, 1);
+        block_relax(L, 0, c.nit);
     }
+    const CoarseLevel<T>& F = c.lv[c.first];
+    const int P = F.nx * F.ny;
+    const T* su = base + F.off + 5 * P;
+    for (int j = threadIdx.x; j < 2 * P; j += blockDim.x) F.U[2 * static_cast<size_t>(bi) * P + j] = su[j];
+}
+
+// Shared memory of the coarse cycle over levels first..last (specs: (nx, ny) per level).
+template <typename T>
+size_t coarse_cycle_smem(const std::vector<std::pair<int, int>>& specs, size_t first) {
+    size_t words = 0;
+    for (size_t l = first; l < specs.size(); ++l) words += 9 * static_cast<size_t>(specs[l].first) * specs[l].second;
+    return words * sizeof(T);
 }
 
 // ------------------------------------------------ fused fine-level V-cycle legs
@@ -678,13 +764,6 @@ __device__ __forceinline__ int image_x(const TileGeom& g, int ix, int dx, int nx
 __device__ __forceinline__ int image_y(const TileGeom& g, int gy, int dy, int ny) {
     return reflect_y(gy + dy, ny) - g.gy0;
 }
-// Whether image point (ix, iy) is exact after `k` steps that each read one cell away.
-__device__ __forceinline__ bool image_valid(const TileGeom& g, int ix, int iy, int k, int ny) {
-    if (!g.full_x && (ix < k || ix >= g.wx - k)) return false;
-    if (g.gy0 > 0 && iy < k) return false;
-    if (g.gy0 + g.wy < ny && iy >= g.wy - k) return false;
-    return true;
-}
 
 template <typename T>
 struct FineImage {
@@ -711,20 +790,69 @@ __device__ void load_image(const T* __restrict__ A, const T* __restrict__ B, con
     }
 }
 
-// relax_at on the image: one half-sweep of `colour` over the points exact after `k` steps.
-template <typename T>
-__device__ void image_half_sweep(FineImage<T>& im, const TileGeom& g, int nx, int ny, int colour, int k, T w00, T w01,
-                                 T w10) {
-    for (int q = threadIdx.x; q < im.n; q += blockDim.x) {
-        const int ix = q % g.wx, iy = q / g.wx;
-        const int gx = g.gx0 + ix, gy = g.gy0 + iy;
-        if (((gx + gy) & 1) != colour || !image_valid(g, ix, iy, k, ny)) continue;
-        T* ux = im.u;
-        T* uy = im.u + im.n;
-        const int xm = iy * g.wx + image_x(g, ix, -1, nx), xp = iy * g.wx + image_x(g, ix, 1, nx);
-        const int ym = image_y(g, gy, -1, ny) * g.wx + ix, yp = image_y(g, gy, 1, ny) * g.wx + ix;
-        const T rx = im.b[q] - w01 * (ux[ym] + ux[yp]) - w10 * (ux[xm] + ux[xp]);
-        const T ry = im.b[im.n + q] - w01 * (uy[ym] + uy[yp]) - w10 * (uy[xm] + uy[xp]);
+// The points of one colour a thread owns in a leg: the r-th point of that
+// colour in row-major image order for r = threadIdx.x + j * blockDim.x (an
+// image row has an even width, so it holds wx / 2 points of each colour).
+// Each carries its image index, its neighbours' image indices and its depth,
+// the number of steps (each reading one cell away) after which it is still
+// exact: its distance to the nearest cut edge of the region (x edges unless
+// the region spans the periodic x range, y edges inside the grid); all are
+// formed once per leg instead of once per half-sweep.
+constexpr int kLegPts = 3;
+constexpr int kLegThreads = 256;
+
+struct LegPoint {
+    int q;  // image index, -1 for an empty slot
+    int depth;
+    int xm, xp, ym, yp;
+};
+
+__device__ __forceinline__ LegPoint leg_point(const TileGeom& g, int nx, int ny, int colour, int r) {
+    LegPoint p{-1, 0, 0, 0, 0, 0};
+    const int half = g.wx >> 1;
+    if (r >= half * g.wy) return p;
+    const int iy = r / half;
+    const int ix = 2 * (r - iy * half) + ((colour - g.gx0 - g.gy0 - iy) & 1);
+    p.q = iy * g.wx + ix;
+    int d = 1 << 30;
+    if (!g.full_x) d = min(d, min(ix, g.wx - 1 - ix));
+    if (g.gy0 > 0) d = min(d, iy);
+    if (g.gy0 + g.wy < ny) d = min(d, g.wy - 1 - iy);
+    p.depth = d;
+    if (d >= 1) {  // every neighbour lies inside the image
+        const int gy = g.gy0 + iy;
+        p.xm = iy * g.wx + image_x(g, ix, -1, nx);
+        p.xp = iy * g.wx + image_x(g, ix, 1, nx);
+        p.ym = image_y(g, gy, -1, ny) * g.wx + ix;
+        p.yp = image_y(g, gy, 1, ny) * g.wx + ix;
+    }
+    return p;
+}
+
+struct LegPoints {
+    LegPoint c[2][kLegPts];  // by colour
+};
+
+__device__ __forceinline__ void own_points(const TileGeom& g, int nx, int ny, LegPoints& own) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int j = 0; j < kLegPts; ++j) own.c[c][j] = leg_point(g, nx, ny, c, threadIdx.x + j * blockDim.x);
+}
+
+// relax_at on the image: one half-sweep of `colour` over the owned points exact after `k` steps.
+template <int COLOUR, typename T>
+__device__ __forceinline__ void image_half_sweep(FineImage<T>& im, const LegPoints& own, int k, T w00, T w01,
+                                                 T w10) {
+    T* ux = im.u;
+    T* uy = im.u + im.n;
+#pragma unroll
+    for (int j = 0; j < kLegPts; ++j) {
+        const LegPoint& p = own.c[COLOUR][j];
+        if (p.q < 0 || p.depth < k) continue;
+        const int q = p.q;
+        const T rx = im.b[q] - w01 * (ux[p.ym] + ux[p.yp]) - w10 * (ux[p.xm] + ux[p.xp]);
+        const T ry = im.b[im.n + q] - w01 * (uy[p.ym] + uy[p.yp]) - w10 * (uy[p.xm] + uy[p.xp]);
         const T dxx = im.a[q] + w00;
         const T dyy = im.a[im.n + q] + w00;
         const T cr = im.a[2 * im.n + q];
@@ -737,9 +865,13 @@ __device__ void image_half_sweep(FineImage<T>& im, const TileGeom& g, int nx, in
     __syncthreads();
 }
 
+// 2 nit half-sweeps, colour 1 first (the order of the separate relax launches).
 template <typename T>
-__device__ void image_relax(FineImage<T>& im, const TileGeom& g, int nx, int ny, int nit, T w00, T w01, T w10) {
-    for (int it = 0; it < 2 * nit; ++it) image_half_sweep(im, g, nx, ny, it % 2 == 0 ? 1 : 0, it + 1, w00, w01, w10);
+__device__ void image_relax(FineImage<T>& im, const LegPoints& own, int nit, T w00, T w01, T w10) {
+    for (int it = 0; it < nit; ++it) {
+        image_half_sweep<1>(im, own, 2 * it + 1, w00, w01, w10);
+        image_half_sweep<0>(im, own, 2 * it + 2, w00, w01, w10);
+    }
 }
 
 template <typename T>
@@ -777,7 +909,7 @@ struct FineLeg {
 // Down leg of level l: 2 nit half-sweeps, the residual b - (H + L) u and its
 // restriction to level l + 1, whose solution is zeroed.  Halo 2 nit + 2.
 template <typename T>
-__global__ void __launch_bounds__(256) k_vcycle_down(FineLeg<T> L) {
+__global__ void __launch_bounds__(kLegThreads) k_vcycle_down(FineLeg<T> L) {
     csg::pdl_begin();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int bi = blockIdx.y;
@@ -788,29 +920,32 @@ __global__ void __launch_bounds__(256) k_vcycle_down(FineLeg<T> L) {
     im.b = im.a + 3 * im.n;
     im.u = im.b + 2 * im.n;
     T* r = im.u + 2 * im.n;  // residual [2][wy][wx]
+    LegPoints own;
+    own_points(g, L.nx, L.ny, own);
     load_image(L.A, L.B, L.Uin, g, L.nx, L.ny, bi, im);
     __syncthreads();
-    image_relax(im, g, L.nx, L.ny, L.nit, L.w00, L.w01, L.w10);
+    image_relax(im, own, L.nit, L.w00, L.w01, L.w10);
     // residual (membrane_apply_at on the image) where it is exact
     const int kr = 2 * L.nit + 1;
     const T w00 = T(L.rw.w[0]), w01 = T(L.rw.w[1]), w10 = T(L.rw.w[2]);
-    for (int q = threadIdx.x; q < im.n; q += blockDim.x) {
-        const int ix = q % g.wx, iy = q / g.wx;
-        if (!image_valid(g, ix, iy, kr, L.ny)) continue;
-        const int gy = g.gy0 + iy;
-        const int xm = iy * g.wx + image_x(g, ix, -1, L.nx), xp = iy * g.wx + image_x(g, ix, 1, L.nx);
-        const int ym = image_y(g, gy, -1, L.ny) * g.wx + ix, yp = image_y(g, gy, 1, L.ny) * g.wx + ix;
-        T reg[2];
-        for (int c = 0; c < 2; ++c) {
-            const T* f = im.u + c * im.n;
-            reg[c] = w00 * f[q] + w01 * (f[ym] + f[yp]) + w10 * (f[xm] + f[xp]);
+#pragma unroll
+    for (int colour = 0; colour < 2; ++colour)
+#pragma unroll
+        for (int j = 0; j < kLegPts; ++j) {
+            const LegPoint& p = own.c[colour][j];
+            if (p.q < 0 || p.depth < kr) continue;
+            const int q = p.q;
+            T reg[2];
+            for (int c = 0; c < 2; ++c) {
+                const T* f = im.u + c * im.n;
+                reg[c] = w00 * f[q] + w01 * (f[p.ym] + f[p.yp]) + w10 * (f[p.xm] + f[p.xp]);
+            }
+            const T u0 = im.u[q], u1 = im.u[im.n + q];
+            const T a0 = reg[0] + im.a[q] * u0 + im.a[2 * im.n + q] * u1;
+            const T a1 = reg[1] + im.a[2 * im.n + q] * u0 + im.a[im.n + q] * u1;
+            r[q] = im.b[q] - a0;
+            r[im.n + q] = im.b[im.n + q] - a1;
         }
-        const T u0 = im.u[q], u1 = im.u[im.n + q];
-        const T a0 = reg[0] + im.a[q] * u0 + im.a[2 * im.n + q] * u1;
-        const T a1 = reg[1] + im.a[2 * im.n + q] * u0 + im.a[im.n + q] * u1;
-        r[q] = im.b[q] - a0;
-        r[im.n + q] = im.b[im.n + q] - a1;
-    }
     __syncthreads();
     store_tile(im, g, L.nx, L.ny, bi, L.Uout);
     // restriction (resize_at) of the residual to the coarse points whose centre tap lies in this tile
@@ -850,7 +985,7 @@ __global__ void __launch_bounds__(256) k_vcycle_down(FineLeg<T> L) {
 // Up leg of level l: u += prolongation of the coarser solution (resize_at,
 // accumulate), then 2 nit half-sweeps.  Halo 2 nit.
 template <typename T>
-__global__ void __launch_bounds__(256) k_vcycle_up(FineLeg<T> L) {
+__global__ void __launch_bounds__(kLegThreads) k_vcycle_up(FineLeg<T> L) {
     csg::pdl_begin();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int bi = blockIdx.y;
@@ -860,25 +995,26 @@ __global__ void __launch_bounds__(256) k_vcycle_up(FineLeg<T> L) {
     im.a = reinterpret_cast<T*>(smem_raw);
     im.b = im.a + 3 * im.n;
     im.u = im.b + 2 * im.n;
+    LegPoints own;
+    own_points(g, L.nx, L.ny, own);
     load_image(L.A, L.B, L.Uin, g, L.nx, L.ny, bi, im);
     for (int q = threadIdx.x; q < im.n; q += blockDim.x) {
         const int ix = q % g.wx, iy = q / g.wx;
-        const int i = (g.gy0 + iy) * L.nx + wrap_x(g.gx0 + ix, L.nx);
+        const int x = wrap_x(g.gx0 + ix, L.nx), y = g.gy0 + iy;
+        // resize_at's taps and weights for this point (the same for both channels)
+        const T yl = (static_cast<T>(y) + T(0.5)) * static_cast<T>(L.cny) / static_cast<T>(L.ny) - T(0.5);
+        const int yo = static_cast<int>(floor(yl + T(0.5)));
+        const T yof = static_cast<T>(yo);
+        const T yw = wt2(yof - yl), ywm = wt2(yof - T(1) - yl), ywp = wt2(yof + T(1) - yl);
+        const int rm = reflect_y(yo - 1, L.cny) * L.cnx, rc = reflect_y(yo, L.cny) * L.cnx,
+                  rp = reflect_y(yo + 1, L.cny) * L.cnx;
+        const T xl = (static_cast<T>(x) + T(0.5)) * static_cast<T>(L.cnx) / static_cast<T>(L.nx) - T(0.5);
+        const int xo = static_cast<int>(floor(xl + T(0.5)));
+        const T xof = static_cast<T>(xo);
+        const T xw = wt2(xof - xl), xwm = wt2(xof - T(1) - xl), xwp = wt2(xof + T(1) - xl);
+        const int cm = wrap_x(xo - 1, L.cnx), cc = wrap_x(xo, L.cnx), cp = wrap_x(xo + 1, L.cnx);
         for (int c = 0; c < 2; ++c) {
-            const int plane = 2 * bi + c;
-            const T* src = L.nU + static_cast<size_t>(plane) * L.cnx * L.cny;
-            const int x = i % L.nx, y = i / L.nx;
-            const T yl = (static_cast<T>(y) + T(0.5)) * static_cast<T>(L.cny) / static_cast<T>(L.ny) - T(0.5);
-            const int yo = static_cast<int>(floor(yl + T(0.5)));
-            const T yof = static_cast<T>(yo);
-            const T yw = wt2(yof - yl), ywm = wt2(yof - T(1) - yl), ywp = wt2(yof + T(1) - yl);
-            const int rm = reflect_y(yo - 1, L.cny) * L.cnx, rc = reflect_y(yo, L.cny) * L.cnx,
-                      rp = reflect_y(yo + 1, L.cny) * L.cnx;
-            const T xl = (static_cast<T>(x) + T(0.5)) * static_cast<T>(L.cnx) / static_cast<T>(L.nx) - T(0.5);
-            const int xo = static_cast<int>(floor(xl + T(0.5)));
-            const T xof = static_cast<T>(xo);
-            const T xw = wt2(xof - xl), xwm = wt2(xof - T(1) - xl), xwp = wt2(xof + T(1) - xl);
-            const int cm = wrap_x(xo - 1, L.cnx), cc = wrap_x(xo, L.cnx), cp = wrap_x(xo + 1, L.cnx);
+            const T* src = L.nU + static_cast<size_t>(2 * bi + c) * L.cnx * L.cny;
             const T vm = ywm * src[rm + cm] + yw * src[rc + cm] + ywp * src[rp + cm];
             const T vc = ywm * src[rm + cc] + yw * src[rc + cc] + ywp * src[rp + cc];
             const T vp = ywm * src[rm + cp] + yw * src[rc + cp] + ywp * src[rp + cp];
@@ -887,25 +1023,77 @@ __global__ void __launch_bounds__(256) k_vcycle_up(FineLeg<T> L) {
         }
     }
     __syncthreads();
-    image_relax(im, g, L.nx, L.ny, L.nit, L.w00, L.w01, L.w10);
+    image_relax(im, own, L.nit, L.w00, L.w01, L.w10);
     store_tile(im, g, L.nx, L.ny, bi, L.Uout);
+}
+
+// Points of the largest tile region of a level (tile plus halo, clipped to the grid).
+inline size_t leg_points(int nx, int ny, int halo) {
+    const int tw = std::min(kTileX, nx), th = std::min(kTileY, ny);
+    const int wx = tw + 2 * halo >= nx ? nx : tw + 2 * halo;
+    const int wy = std::min(ny, th + 2 * halo);
+    return static_cast<size_t>(wx) * wy;
 }
 
 // Shared memory of one leg launch: A, B, U (+ the residual going down) over the largest tile region.
 template <typename T>
 size_t leg_smem(int nx, int ny, int halo, bool down) {
-    const int tw = std::min(kTileX, nx), th = std::min(kTileY, ny);
-    const int wx = tw + 2 * halo >= nx ? nx : tw + 2 * halo;
-    const int wy = std::min(ny, th + 2 * halo);
-    return static_cast<size_t>(wx) * wy * (down ? 9 : 7) * sizeof(T);
+    return leg_points(nx, ny, halo) * (down ? 9 : 7) * sizeof(T);
 }
 
 constexpr size_t kLegSmemMax = 200 * 1024;
 
-// Opt the leg kernels in to more than 48 KB of dynamic shared memory, once per
-// type and device (the first solve on a device runs eagerly, before any capture).
+// The restriction chain of a level-l field to every coarser level at or below
+// kChainPoints points per grid, in one launch with one CTA per batch element:
+// the same resize_at per point as separate k_resize launches, level after
+// level, with __syncthreads between levels.  Each restricted level is kept in
+// shared memory (at most ~2,800 points x channels over all levels) as the
+// source of the next one, and written to its field.
+constexpr int kChainPoints = 2048;
+
 template <typename T>
-void allow_leg_smem() {
+struct ResizeChain {
+    T* field[kMaxLevels];  // [batch * channels][ny][nx] per level
+    int nx[kMaxLevels], ny[kMaxLevels];
+    int off[kMaxLevels];   // offset of level l's [channels][ny][nx] image in shared memory (elements)
+    int first, last, channels;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kCoarseThreads) k_resize_chain(ResizeChain<T> c) {
+    csg::pdl_begin();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* base = reinterpret_cast<T*>(smem_raw);
+    const int bi = blockIdx.x;
+    for (int l = c.first; l <= c.last; ++l) {
+        const int P = c.nx[l] * c.ny[l];
+        const size_t plane0 = static_cast<size_t>(c.channels) * bi;
+        T* image = base + c.off[l];
+        T* out = c.field[l] + plane0 * P;
+        for (int j = threadIdx.x; j < c.channels * P; j += blockDim.x) {
+            if (l == c.first)  // the source level lives in global memory
+                resize_at(c.field[l - 1], c.field[l], c.nx[l - 1], c.ny[l - 1], c.nx[l], c.ny[l], 0,
+                          static_cast<int>(plane0) + j / P, j % P);
+            else
+                resize_at(static_cast<const T*>(base + c.off[l - 1]), out, c.nx[l - 1], c.ny[l - 1], c.nx[l],
+                          c.ny[l], 0, j / P, j % P);
+            image[j] = out[j];
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+size_t resize_chain_smem(const ResizeChain<T>& c) {
+    size_t words = 0;
+    for (int l = c.first; l <= c.last; ++l) words += static_cast<size_t>(c.channels) * c.nx[l] * c.ny[l];
+    return words * sizeof(T);
+}
+
+// Opt the leg, coarse-cycle and chain kernels in to more than 48 KB of dynamic
+// shared memory, once per type and device (the first solve on a device runs eagerly, before any capture).
+template <typename T>
+void allow_big_smem() {
     static std::atomic<unsigned long long> done{0};
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return;
@@ -915,33 +1103,11 @@ void allow_leg_smem() {
                          static_cast<int>(kLegSmemMax));
     cudaFuncSetAttribute(reinterpret_cast<const void*>(k_vcycle_up<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(kLegSmemMax));
+    cudaFuncSetAttribute(reinterpret_cast<const void*>(k_fmg_coarse_cycle<T>),
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kLegSmemMax));
+    cudaFuncSetAttribute(reinterpret_cast<const void*>(k_resize_chain<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kLegSmemMax));
     done.fetch_or(bit);
-}
-
-// The restriction chain of a level-l field to every coarser level at or below
-// kChainPoints points per grid, in one launch with one CTA per batch element:
-// the same resize_at per point as separate k_resize launches, level after
-// level, with __syncthreads between levels.
-constexpr int kChainPoints = 2048;
-
-template <typename T>
-struct ResizeChain {
-    T* field[kMaxLevels];  // [batch * channels][ny][nx] per level
-    int nx[kMaxLevels], ny[kMaxLevels];
-    int first, last, channels;
-};
-
-template <typename T>
-__global__ void __launch_bounds__(kCoarseThreads) k_resize_chain(ResizeChain<T> c) {
-    csg::pdl_begin();
-    const int bi = blockIdx.x;
-    for (int l = c.first; l <= c.last; ++l) {
-        const int P = c.nx[l] * c.ny[l];
-        for (int j = threadIdx.x; j < c.channels * P; j += blockDim.x)
-            resize_at(c.field[l - 1], c.field[l], c.nx[l - 1], c.ny[l - 1], c.nx[l], c.ny[l], 0,
-                      c.channels * bi + j / P, j % P);
-        __syncthreads();
-    }
 }
 
 template <typename T>
@@ -1097,21 +1263,27 @@ struct Fmg {
         c.first = static_cast<int>(first);
         c.last = static_cast<int>(last);
         c.nit = nit;
+        int off = 0;
         for (size_t l = first; l <= last; ++l) {
             double pr[5];
             params_at(l, pr);
             const MemWeights w = mem_weights(pr);
             c.lv[l] = CoarseLevel<T>{buf.A[l], buf.B[l], buf.U[l], buf.R[l], buf.specs[l].first, buf.specs[l].second,
-                                     T(w.w00), T(w.w01), T(w.w10), reg_weights(pr, 1)};
+                                     T(w.w00), T(w.w01), T(w.w10), reg_weights(pr, 1), off};
+            off += 9 * buf.specs[l].first * buf.specs[l].second;
         }
-        (csg::note_launch(), csg::launch_pdl(k_fmg_coarse_cycle<T>, batch, kCoarseThreads, 0, s, c));
+        allow_big_smem<T>();
+        (csg::note_launch(), csg::launch_pdl(k_fmg_coarse_cycle<T>, batch, kCoarseCycleThreads,
+                                             coarse_cycle_smem<T>(buf.specs, first), s, c));
     }
     // One launch per fine leg (k_vcycle_down / k_vcycle_up) when every fine
     // level has an even x size and the tile regions fit in shared memory.
     bool legs_fit(size_t start, size_t fused) const {
         for (size_t l = start; l < fused; ++l) {
             const int nx = buf.specs[l].first, ny = buf.specs[l].second;
-            if (nx % 2 != 0 || leg_smem<T>(nx, ny, 2 * nit + 2, true) > kLegSmemMax) return false;
+            if (nx % 2 != 0 || leg_smem<T>(nx, ny, 2 * nit + 2, true) > kLegSmemMax ||
+                leg_points(nx, ny, 2 * nit + 2) > static_cast<size_t>(2 * kLegPts * kLegThreads))
+                return false;
         }
         return true;
     }
@@ -1146,18 +1318,18 @@ struct Fmg {
         const size_t last = buf.specs.size() - 1;
         const size_t fused = std::max(start, coarse_first());
         if (buf.specs.size() <= static_cast<size_t>(kMaxLevels) && fused < last && legs_fit(start, fused)) {
-            allow_leg_smem<T>();
+            allow_big_smem<T>();
             // down: relax, residual, restriction (relaxed solution in R[l]); up: prolongation, relax (back in U[l])
             for (size_t l = start; l < fused; ++l) {
                 const int nx = buf.specs[l].first, ny = buf.specs[l].second;
-                (csg::note_launch(), csg::launch_pdl(k_vcycle_down<T>, leg_grid(l), 256,
+                (csg::note_launch(), csg::launch_pdl(k_vcycle_down<T>, leg_grid(l), kLegThreads,
                                                      leg_smem<T>(nx, ny, 2 * nit + 2, true), s,
                                                      leg(l, buf.U[l], buf.R[l])));
             }
             coarse_cycle(fused);
             for (size_t l = fused; l-- > start;) {
                 const int nx = buf.specs[l].first, ny = buf.specs[l].second;
-                (csg::note_launch(), csg::launch_pdl(k_vcycle_up<T>, leg_grid(l), 256, leg_smem<T>(nx, ny, 2 * nit, false),
+                (csg::note_launch(), csg::launch_pdl(k_vcycle_up<T>, leg_grid(l), kLegThreads, leg_smem<T>(nx, ny, 2 * nit, false),
                                                      s, leg(l, buf.R[l], buf.U[l])));
             }
             return;
@@ -1221,7 +1393,12 @@ struct Fmg {
         c.first = static_cast<int>(l);
         c.last = static_cast<int>(L - 1);
         c.channels = 3;
-        (csg::note_launch(), csg::launch_pdl(k_resize_chain<T>, batch, kCoarseThreads, 0, s, c));
+        for (int k = c.first, off = 0; k <= c.last; ++k) {
+            c.off[k] = off;
+            off += c.channels * c.nx[k] * c.ny[k];
+        }
+        allow_big_smem<T>();
+        (csg::note_launch(), csg::launch_pdl(k_resize_chain<T>, batch, kCoarseThreads, resize_chain_smem(c), s, c));
     }
     void run(bool coarse_init) {
         const size_t L = buf.specs.size();
@@ -1305,14 +1482,15 @@ Squaring<T> run_squaring(T* rb[2], T* ha[2], T* maps[2], T* jacs[2], int k, bool
     const dim3 g = grid_for(nx * ny, batch);
     int cur = 0, other = 1, ba = 0;
     for (int step = 0; step < k; ++step) {
-        (csg::note_launch(), csg::launch_pdl(k_squaring<T>, g, kThreads, 0, s, rb[ba], ha[ba], maps[cur], jacs[cur], rb[1 - ba], ha[1 - ba], maps[other],
-                                             nx, ny));
-        ba = 1 - ba;
         if (save || step < k - 1) {
-            (csg::note_launch(), csg::launch_pdl(k_compose<T>, g, kThreads, 0, s, maps[cur], jacs[cur], maps[cur], jacs[cur], maps[other], jacs[other],
-                                                nx, ny));
+            (csg::note_launch(), csg::launch_pdl(k_squaring_compose<T>, g, kThreads, 0, s, rb[ba], ha[ba], maps[cur],
+                                                 jacs[cur], rb[1 - ba], ha[1 - ba], maps[other], jacs[other], nx, ny));
             std::swap(cur, other);
+        } else {
+            (csg::note_launch(), csg::launch_pdl(k_squaring<T>, g, kThreads, 0, s, rb[ba], ha[ba], maps[cur], jacs[cur],
+                                                 rb[1 - ba], ha[1 - ba], maps[other], nx, ny));
         }
+        ba = 1 - ba;
     }
     if (save && cur != 0) {
         const size_t P = static_cast<size_t>(nx) * ny * batch;
