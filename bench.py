@@ -266,6 +266,15 @@ class ClockSampler:
             )
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # nvidia-smi's start-up (driver and NVML initialisation) stalled this process's CUDA
+        # calls for hundreds of milliseconds when it overlapped the first timed steps; the timed
+        # region starts once the sampler has written its first sample
+        deadline = time.perf_counter() + 10.0
+        while time.perf_counter() < deadline and self.proc.poll() is None:
+            if Path(self.file.name).stat().st_size > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -1021,12 +1030,8 @@ def run_native(args):
         hbm = float(peaks.get("hbm_gbs", 6650.0))
         peak_source = "measured" if "hbm_gbs" in peaks else "fallback"
         achieved = areal_bytes_per_sweep(n, f) * SWEEPS / kernel_s / 1e9
-        epochs, start = [], 1
-        while start <= SWEEPS:
-            end = min(SWEEPS, ((start - 1) // 1000 + 1) * 1000)
-            epochs.append(end - start + 1)
-            start = end + 1
-        wavefront_steps = sum((s - 1) * hemi.plan.level_stride + hemi.plan.n_levels for s in epochs)
+        # one wavefront runs every sweep (the projections ride in it)
+        wavefront_steps = (SWEEPS - 1) * hemi.plan.level_stride + hemi.plan.n_levels
         stages = {k: statistics.mean(t[k] for t in stage) for k in stage[0] if isinstance(stage[0][k], float)}
         stages["sweeps_kernel_s"] = kernel_s
         stages["preprocess_kernels_s"] = statistics.mean(pre_ms) / 1e3

@@ -465,7 +465,10 @@ __global__ void __launch_bounds__(512) areal_sweeps_kernel(ArealParams p) {
 // polls its faces' words until they do.  Each group walks the same wavefront
 // order as the barrier form (step t, then its share of the step's vertices),
 // which keeps progress guaranteed: the earliest unfinished update's inputs are
-// all finished.  Grid barriers remain around the projections only.
+// all finished.  The projections ride in the wavefront too (a second array
+// of projected words, written as each epoch's last sweep is published), so
+// one wavefront runs every sweep and grid barriers remain only at the start
+// and the end.
 // Every wait is bounded: on timeout (or another CTA's failure) the kernel
 // records the status and leaves.
 
@@ -500,8 +503,9 @@ constexpr int kRingMax = 20;
 // arithmetic, slot order).  Lanes 0, 1, 2 publish coordinates 0, 1, 2.
 // Returns false to abort.
 template <int MODE, int G>
-__device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned long long* pub, int v, const int* ring,
-                                                 int nring, const int* code, int deg, unsigned int s,
+__device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned long long* pub,
+                                                 const unsigned long long* prev, unsigned long long* proj_out, int v,
+                                                 const int* ring, int nring, const int* code, int deg, unsigned int s,
                                                  double (*stage)[32], float3* pos) {
     using T = Traits<MODE>;
     using Acc = typename T::Acc;
@@ -528,7 +532,7 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
         for (int q = 0; q < kQ; ++q)
             if (who[q] >= 0)
 #pragma unroll
-                for (int k = 0; k < 3; ++k) w[q][k] = ld_word(pub + 4LL * who[q] + k);
+                for (int k = 0; k < 3; ++k) w[q][k] = ld_word((who[q] < v ? pub : prev) + 4LL * who[q] + k);
         bool ok = true;
 #pragma unroll
         for (int q = 0; q < kQ; ++q)
@@ -625,6 +629,16 @@ __device__ __forceinline__ bool update_vertex_df(const ArealParams& p, unsigned 
     }
     __syncwarp();  // every lane is done with `pos` before the next update overwrites it
     if (v >= 0 && glane < 3) st_word(pub + 4LL * v + glane, make_word(value, s));
+    if (__any_sync(kFull, proj_out != nullptr && v >= 0)) {
+        // sweep s ends a projection epoch: publish the projected point too (T::project_p3 of
+        // the float32 values just published, as the separate projection pass computed it)
+        const float px = __shfl_sync(kFull, value, gbase), py = __shfl_sync(kFull, value, gbase + 1),
+                    pz = __shfl_sync(kFull, value, gbase + 2);
+        if (proj_out != nullptr && v >= 0 && glane < 3) {
+            const P3 q = T::project_p3(P3{px, py, pz}, p.radius);
+            st_word(proj_out + 4LL * v + glane, make_word(glane == 0 ? q.x : (glane == 1 ? q.y : q.z), s));
+        }
+    }
     return true;
 }
 
@@ -706,17 +720,24 @@ __global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
     for (int v = tid; v < p.n; v += nthreads) {
         const float* q = static_cast<const float*>(p.points) + 3LL * v;
         for (int k = 0; k < 3; ++k) st_word(pub + 4LL * v + k, make_word(q[k], 0u));
+        // projected words start at version 0, below any epoch's end: a word left
+        // from an earlier call on the same scratch never satisfies a poll
+        for (int k = 0; k < 3; ++k) st_word(pub + 4LL * p.n + 4LL * v + k, make_word(0.0f, 0u));
     }
     if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
     // a ring overflow or a degree over max_degree: the same answer in every CTA
     if (csg::ld_relaxed_gpu(&p.ctl->status) != CSG_OK) return;
 
+    // One wavefront over every sweep.  The projection after sweep b (b a multiple of
+    // project_every) is applied by each vertex's group as it publishes sweep b, into
+    // the second word array `proj`; the updates of sweep b + 1 read their
+    // previous-sweep members (higher neighbours and the vertex itself) from there,
+    // the updates of sweep b read the unprojected words.  The wavefront therefore
+    // never drains at a projection.
     const int last = p.iterations - 1;
-    for (int start = 1; start <= last;) {
-        int end = last;
-        if (p.project_every > 0) end = min(last, ((start - 1) / p.project_every + 1) * p.project_every);
-        const int S = end - start + 1;
-        const int span = (S - 1) * D;  // host guarantees span + L < 2^31
+    unsigned long long* proj = pub + 4LL * p.n;
+    if (last >= 1) {
+        const int span = (last - 1) * D;  // host guarantees span + L < 2^31
         const int nsteps = span + L;
         int r = 0;
         for (int t = 0; t < nsteps; ++t, r = (r + 1 == D) ? 0 : r + 1) {
@@ -737,29 +758,22 @@ __global__ void __launch_bounds__(512) areal_dataflow_kernel(ArealParams p) {
                     nring = lnring[i];
                     ring = lring + i * kRingMax;
                     code = lcode + i * p.max_degree;
-                    sweep = static_cast<unsigned int>(start + (t - llev[i]) / D);
+                    sweep = static_cast<unsigned int>(1 + (t - llev[i]) / D);
                 }
-                if (!update_vertex_df<MODE, G>(p, pub, v, ring, nring, code, deg, sweep, stage, pos)) return;
+                const bool after = p.project_every > 0 && sweep > 1 && (sweep - 1) % p.project_every == 0;
+                const bool at = p.project_every > 0 && sweep > 0 && sweep % p.project_every == 0;
+                if (!update_vertex_df<MODE, G>(p, pub, after ? proj : pub, at ? proj : nullptr, v, ring, nring, code,
+                                               deg, sweep, stage, pos))
+                    return;
             }
         }
-        if (p.project_every > 0 && end % p.project_every == 0) {
-            if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
-            for (int v = tid; v < p.n; v += nthreads) {
-                P3 q;
-                load_versioned(pub, v, static_cast<unsigned int>(end), q);
-                q = T::project_p3(q, p.radius);
-                st_word(pub + 4LL * v, make_word(q.x, end));
-                st_word(pub + 4LL * v + 1, make_word(q.y, end));
-                st_word(pub + 4LL * v + 2, make_word(q.z, end));
-            }
-            if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
-        }
-        start = end + 1;
     }
     if (csg::grid_barrier(p.ctl, phase, p.timeout_ns, barrier_id++)) return;
+    const unsigned long long* result =
+        (p.project_every > 0 && last >= 1 && last % p.project_every == 0) ? proj : pub;
     for (int v = tid; v < p.n; v += nthreads) {
         float* q = static_cast<float*>(p.points) + 3LL * v;
-        for (int k = 0; k < 3; ++k) q[k] = word_value(ld_word(pub + 4LL * v + k));
+        for (int k = 0; k < 3; ++k) q[k] = word_value(ld_word(result + 4LL * v + k));
     }
 }
 
@@ -859,8 +873,9 @@ size_t csg_areal_scratch_bytes(int n_vertices, int arithmetic) {
     if (n_vertices < 1 || (arithmetic != CSG_ARITH_CAT && arithmetic != CSG_ARITH_FP32 && arithmetic != CSG_ARITH_FP64))
         return 0;
     // float64: a double4 working copy; float32 modes: four published 8-byte
-    // words per vertex (the dataflow form; the barrier form uses the first half)
-    return sizeof(csg::Control) + align256(32 * static_cast<size_t>(n_vertices));
+    // words per vertex and four projected ones (the dataflow form; the barrier
+    // form uses the first 16 bytes per vertex)
+    return sizeof(csg::Control) + align256(64 * static_cast<size_t>(n_vertices));
 }
 
 int csg_areal_sweeps(void* points, int n_vertices, const int32_t* slot_off, const int32_t* slot_tri,
