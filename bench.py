@@ -315,6 +315,7 @@ def load_meshes():
         "binary_seconds": float(c2["cpu_seconds"]),
         "target_faces": c3["faces"].astype(np.int32), "target_surface": c3["surface"], "target_sphere": c3["final"],
         "chain_final": gold["final_sphere"], "chain_cpu_seconds": float(gold["cpu_seconds"]),
+        "chain_final_builder": gold["builder_final_sphere"] if "builder_final_sphere" in gold.files else None,
         "chain_cpu_threads": int(gold["cpu_threads"]),
         "rotation_evaluations": int(gold["rotation_candidates_evaluated"]),
     }
@@ -994,6 +995,9 @@ def run_native(args):
     # parity (untimed): the chain against the reference's CPU chain (float64 DARTEL, like the timed chain),
     # the sweeps against the upstream binary, and a float32-DARTEL chain against the float64 one
     parity = {"chain_vs_cpu_reference": error_stats(meshes["chain_final"], final),
+              # the reference's CPU chain on this package's stencils instead of its helper's float32 ones
+              "chain_vs_cpu_reference_same_stencils": (error_stats(meshes["chain_final_builder"], final)
+                                                       if meshes["chain_final_builder"] is not None else None),
               "surf2sphere_vs_binary": error_stats(meshes["binary_sphere"], sphere),
               "stages_1_5_vs_binary": error_stats(meshes["prefix"], prefix.cpu().numpy())}
     hemi.step(dartel_dtype=torch.float32)  # warm (graph capture for float32)

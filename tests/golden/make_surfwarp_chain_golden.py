@@ -29,7 +29,9 @@ binary's sphere, target = the ``surf2sphere_c3`` surface and sphere, two runs
 of two steps on a 256 x 128 sheet with ``-avg``; it writes
 ``surfwarp_chain_hemisphere_golden.npz`` (parameters, rotation angle/cost, the
 number of rotation candidates the search evaluated, the final sphere and the
-CPU wall time of the chain).
+CPU wall time of the chain), plus the same chain run on this package's host
+stencil builder instead of the helper (``builder_rotation_angle``,
+``builder_final_sphere``).
 
 Usage: ``python tests/golden/make_surfwarp_chain_golden.py [--workload small|hemisphere]``
 """
@@ -99,7 +101,7 @@ def chain_inputs(seed: int = 5):
     )
 
 
-def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size, target_faces=None):
+def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size, target_faces=None, stencils="helper"):
     source_faces = data["faces"]
     target_faces = source_faces if target_faces is None else target_faces
     temp = Path(tempfile.mkdtemp(prefix="chain_golden_"))
@@ -111,6 +113,12 @@ def reference_chain(data, nx, ny, steps, runs, avg, loop, rotation_grid_size, ta
         count[0] += 1
         mesh_path, path = temp / f"s{count[0]}.gii", temp / f"s{count[0]}.stencil"
         faces = source_faces if faces is None else faces
+        if stencils == "builder":  # this package's host builder, read back through the reference's reader
+            from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+            build_surface_stencil(np.asarray(sphere, dtype=np.float32), np.asarray(faces, dtype=np.int32), nx=nx,
+                                  ny=ny, normalize=normalize, threads=8).to_file(path)
+            return ReferenceStencil.from_file(path)
         write_gifti_mesh(mesh_path, GiftiMesh(np.asarray(sphere, dtype=np.float32), faces))
         command = [str(HELPER), str(mesh_path), str(path), "--threads", "8"]
         if not normalize:
@@ -261,7 +269,11 @@ def main() -> int:
         result = reference_chain(data, target_faces=target_faces, **HEMISPHERE_PARAMS)
         seconds = time.perf_counter() - started
         keep = ("rotation_angle", "rotation_cost", "rotation_candidates_evaluated", "final_sphere")
+        # the same chain on this package's stencils: separates the chain's arithmetic from its
+        # sensitivity to the helper's float32 stencil rounding
+        builder = reference_chain(data, target_faces=target_faces, stencils="builder", **HEMISPHERE_PARAMS)
         np.savez_compressed(HERE / "surfwarp_chain_hemisphere_golden.npz", **{k: result[k] for k in keep},
+                            **{f"builder_{k}": builder[k] for k in ("rotation_angle", "final_sphere")},
                             cpu_seconds=np.float64(seconds), cpu_threads=np.int64(torch.get_num_threads()),
                             **{f"param_{k}": np.asarray(v) for k, v in HEMISPHERE_PARAMS.items()})
     print(f"reference chain on CPU ({args.workload}): {seconds:.1f} s, angle {result['rotation_angle']}, "
