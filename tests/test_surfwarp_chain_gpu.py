@@ -111,3 +111,37 @@ def test_device_stencil_builder_on_hemisphere_mesh(native_library):
     for name in ("sphere_points", "surface_indices", "surface_weights", "sheet_indices", "sheet_weights",
                  "unit_sphere_points"):
         np.testing.assert_array_equal(getattr(dev, name), getattr(host, name), err_msg=name)
+
+
+def test_hemisphere_chain_matches_reference_on_the_same_stencils(native_library):
+    """The benchmark's hemisphere (61,442-vertex hulls c2 -> c3, 256 x 128, steps 2, runs 2, -avg).
+
+    The golden holds the reference's CPU chain twice: on its helper's float32
+    stencils and on this package's host stencils.  The two reference results
+    differ by up to ~9e-3 (the stencils' rounding moves the rotation pick by
+    ~4e-5 rad and the registration carries that), so the GPU chain is held to
+    1e-3 against the reference run on the same stencils, and to the helper
+    chain's own spread against the other.
+    """
+
+    from cat_surface_gpu_b200.gifti import GiftiMesh
+    from cat_surface_gpu_b200.gpu_pipeline import register_meshes
+
+    source, target = (np.load(GOLDEN / f"surf2sphere_{name}.npz") for name in ("c2", "c3"))
+    gold = np.load(GOLDEN / "surfwarp_chain_hemisphere_golden.npz")
+    faces, target_faces = source["faces"].astype(np.int32), target["faces"].astype(np.int32)
+    final, angle, _, _ = register_meshes(
+        GiftiMesh(source["surface"], faces), GiftiMesh(source["final"], faces),
+        GiftiMesh(target["surface"], target_faces), GiftiMesh(target["final"], target_faces), device="cuda:0",
+        steps=2, runs=2, avg=True, loop=6, sheet_size=(256, 128), rotation_feature_backend="cuda",
+        rotation_feature_solver="colored-sor")
+    final = np.asarray(final, dtype=np.float64)
+    same = np.linalg.norm(final - gold["builder_final_sphere"], axis=1)
+    helper = np.linalg.norm(final - gold["final_sphere"], axis=1)
+    spread = np.linalg.norm(gold["builder_final_sphere"] - gold["final_sphere"], axis=1)
+    print(f"hemisphere chain error: same stencils max {same.max():.3g}, helper stencils max {helper.max():.3g} "
+          f"(reference spread {spread.max():.3g})")
+    assert np.abs(angle - gold["builder_rotation_angle"]).max() <= 1e-5
+    assert same.max() <= 1e-3
+    assert helper.max() <= 1.5 * spread.max()
+    torch.cuda.synchronize()
