@@ -275,9 +275,11 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
         for (int trial = stride - 1; trial >= 2; --trial) {
             f = best;
             // feasible strides converge in a few relaxation sweeps (3 to 10 on
-            // cortical hulls); a stride that needs many more than the last one
-            // is treated as infeasible -- only the schedule's length depends on it
-            const int cap = std::min(4000, 3 * last_iterations + 16);
+            // cortical hulls, each at most 5 more than the stride before it); a
+            // stride that needs 8 more than the last one is treated as infeasible
+            // -- only the schedule's length depends on it, and the infeasible
+            // trial, which runs to the cap, is most of the planning time
+            const int cap = std::min(4000, last_iterations + 8);
             bool converged = false;
             int it = 0;
             for (; it < cap && !converged; ++it) {

@@ -94,9 +94,11 @@ def _pool() -> ThreadPoolExecutor:
     return _POOL
 
 
-def _deflate(raw: bytes, level: int = 1) -> bytes:
+def _deflate(raw: bytes, level: int = 1) -> tuple[bytes, list[int] | None]:
+    """zlib stream of ``raw`` and, when it was deflated in chunks, the chunks' compressed lengths."""
+
     if len(raw) < _PARALLEL_MIN:
-        return zlib.compress(raw, level)
+        return zlib.compress(raw, level), None
     chunks = [raw[i: i + _CHUNK] for i in range(0, len(raw), _CHUNK)]
     last = len(chunks) - 1
 
@@ -105,9 +107,67 @@ def _deflate(raw: bytes, level: int = 1) -> bytes:
         stream = zlib.compressobj(level, zlib.DEFLATED, -15)
         return stream.compress(chunk) + stream.flush(zlib.Z_FINISH if index == last else zlib.Z_SYNC_FLUSH)
 
-    body = b"".join(_pool().map(one, enumerate(chunks)))
+    parts = list(_pool().map(one, enumerate(chunks)))
     header = bytes((0x78, 0x01 if level <= 1 else (0x5E if level <= 5 else (0x9C if level == 6 else 0xDA))))
-    return header + body + zlib.adler32(raw).to_bytes(4, "big")
+    return header + b"".join(parts) + zlib.adler32(raw).to_bytes(4, "big"), [len(part) for part in parts]
+
+
+# The chunk index of a payload deflated here rides in the array's MetaData, so a reader
+# can inflate the chunks in parallel: each is an independent raw deflate stream.  Other
+# readers ignore the entry and inflate the one zlib stream as usual.
+_CHUNK_KEY = "DeflateChunkLengths"
+
+
+def _chunk_metadata(lengths: list[int] | None) -> str:
+    if not lengths:
+        return "<MetaData/>\n"
+    value = f"{_CHUNK}:" + ",".join(str(n) for n in lengths)
+    return f"<MetaData><MD><Name><![CDATA[{_CHUNK_KEY}]]></Name><Value><![CDATA[{value}]]></Value></MD></MetaData>\n"
+
+
+def _chunk_lengths(element: ET.Element) -> list[int] | None:
+    meta = element.find("MetaData")
+    if meta is None:
+        return None
+    for md in meta.findall("MD"):
+        name, value = md.find("Name"), md.find("Value")
+        if name is not None and (name.text or "").strip() == _CHUNK_KEY and value is not None and value.text:
+            size, _, lengths = value.text.strip().partition(":")
+            try:
+                if int(size) != _CHUNK:
+                    return None
+                return [int(n) for n in lengths.split(",")]
+            except ValueError:
+                return None
+    return None
+
+
+def _inflate(raw: bytes, lengths: list[int] | None) -> bytes:
+    """zlib.decompress(raw), with the chunks of a chunk-indexed stream inflated in parallel.
+
+    The result is checked against the stream's Adler-32 like zlib's own; a
+    stream whose index does not fit it is inflated as one stream.
+    """
+
+    body = len(raw) - 6
+    if not lengths or len(lengths) < 2 or body < 0 or sum(lengths) != body or (raw[0] * 256 + raw[1]) % 31 != 0:
+        return zlib.decompress(raw)
+    starts = [2]
+    for n in lengths[:-1]:
+        starts.append(starts[-1] + n)
+    last = len(lengths) - 1
+
+    def one(index):
+        stream = zlib.decompressobj(-15)
+        out = stream.decompress(raw[starts[index]: starts[index] + lengths[index]])
+        if stream.eof != (index == last) or stream.unused_data:
+            raise zlib.error("chunk boundaries do not match the deflate stream")
+        return out
+
+    out = b"".join(_pool().map(one, range(len(lengths))))
+    if zlib.adler32(out) != int.from_bytes(raw[-4:], "big"):
+        raise zlib.error("incorrect data check")
+    return out
 
 
 # Encoded payloads of the int32 arrays decoded most recently (face arrays): writing an
@@ -118,20 +178,20 @@ _PAYLOADS_MAX = 8
 _PAYLOADS_LOCK = threading.Lock()
 
 
-def _remember_payload(dtype_name: str, shape: tuple, raw: bytes, payload: str) -> None:
+def _remember_payload(dtype_name: str, shape: tuple, raw: bytes, payload: str, lengths: list[int] | None) -> None:
     key = (dtype_name, shape, zlib.crc32(raw))
     with _PAYLOADS_LOCK:
-        _PAYLOADS[key] = (raw, payload)
+        _PAYLOADS[key] = (raw, payload, lengths)
         _PAYLOADS.move_to_end(key)
         while len(_PAYLOADS) > _PAYLOADS_MAX:
             _PAYLOADS.popitem(last=False)
 
 
-def _known_payload(dtype_name: str, shape: tuple, raw: bytes) -> str | None:
+def _known_payload(dtype_name: str, shape: tuple, raw: bytes) -> tuple[str, list[int] | None] | None:
     with _PAYLOADS_LOCK:
         hit = _PAYLOADS.get((dtype_name, shape, zlib.crc32(raw)))
     if hit is not None and hit[0] == raw:
-        return hit[1]
+        return hit[1], hit[2]
     return None
 
 
@@ -156,9 +216,10 @@ def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
         payload = "".join(text.split())
         raw = base64.b64decode(payload)
         if encoding == "GZipBase64Binary":
-            raw = zlib.decompress(raw)
+            lengths = _chunk_lengths(element)
+            raw = _inflate(raw, lengths)
             if dtype_name == "NIFTI_TYPE_INT32" and endian == "LittleEndian" and order == "C":
-                _remember_payload(dtype_name, shape, raw, payload)
+                _remember_payload(dtype_name, shape, raw, payload, lengths)
         wire = dtype.newbyteorder("<" if endian == "LittleEndian" else ">")
         values = np.frombuffer(raw, dtype=wire).astype(dtype)
     else:
@@ -215,13 +276,18 @@ def read_gifti_mesh(path: str | Path) -> GiftiMesh:
     )
 
 
-def _encode_array(values: np.ndarray, intent: int, dtype_name: str, payload: str | None = None) -> str:
-    if payload is None:
+def _encode_array(values: np.ndarray, intent: int, dtype_name: str,
+                  stored: tuple[str, list[int] | None] | None = None) -> str:
+    """One DataArray; ``stored`` is a (payload, chunk lengths) pair to write as it is."""
+
+    if stored is None:
         raw = np.ascontiguousarray(values).astype(values.dtype.newbyteorder("<")).tobytes()
-        payload = _known_payload(dtype_name, tuple(values.shape), raw) if dtype_name == "NIFTI_TYPE_INT32" else None
-        if payload is None:
+        stored = _known_payload(dtype_name, tuple(values.shape), raw) if dtype_name == "NIFTI_TYPE_INT32" else None
+        if stored is None:
             # deflate level 1: on vertex and index arrays it packs as well as level 6 at a sixth of the time
-            payload = base64.b64encode(_deflate(raw, 1)).decode("ascii")
+            compressed, lengths = _deflate(raw, 1)
+            stored = base64.b64encode(compressed).decode("ascii"), lengths
+    payload, lengths = stored
     dims = "".join(f' Dim{i}="{size}"' for i, size in enumerate(values.shape))
     intent_name = _INTENT_NAMES.get(intent, "NIFTI_INTENT_NONE")
     transform = ""
@@ -237,7 +303,7 @@ def _encode_array(values: np.ndarray, intent: int, dtype_name: str, payload: str
         f'<DataArray Intent="{intent_name}" DataType="{dtype_name}" '
         f'ArrayIndexingOrder="RowMajorOrder" Dimensionality="{values.ndim}"{dims} '
         'Encoding="GZipBase64Binary" Endian="LittleEndian" ExternalFileName="" ExternalFileOffset="">\n'
-        "<MetaData/>\n"
+        + _chunk_metadata(lengths) +
         f"{transform}<Data>{payload}</Data>\n</DataArray>\n"
     )
 
@@ -275,8 +341,8 @@ def _shape(element: ET.Element) -> tuple[int, ...]:
     return tuple(int(attrs[f"Dim{i}"]) for i in range(int(attrs.get("Dimensionality", "1"))))
 
 
-def _verbatim_faces(element: ET.Element) -> str | None:
-    """The payload of an [m, 3] int32 little-endian row-major gzip face array, as stored."""
+def _verbatim_faces(element: ET.Element) -> tuple[str, list[int] | None] | None:
+    """The payload (and chunk index) of an [m, 3] int32 little-endian row-major gzip face array, as stored."""
 
     attrs = element.attrib
     shape = _shape(element)
@@ -286,11 +352,11 @@ def _verbatim_faces(element: ET.Element) -> str | None:
             and len(shape) == 2 and shape[1] == 3):
         data = element.find("Data")
         if data is not None and data.text:
-            return "".join(data.text.split())
+            return "".join(data.text.split()), _chunk_lengths(element)
     return None
 
 
-def _write_mesh(path, mesh: GiftiMesh, intents, faces_payload: str | None = None) -> None:
+def _write_mesh(path, mesh: GiftiMesh, intents, faces_payload: tuple[str, list[int] | None] | None = None) -> None:
     point_intent = _INTENT_CODES["NIFTI_INTENT_POINTSET"]
     triangle_intent = _INTENT_CODES["NIFTI_INTENT_TRIANGLE"]
     if intents is not None:
