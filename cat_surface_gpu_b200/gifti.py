@@ -213,7 +213,7 @@ def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
         values = np.array(text.split(), dtype=np.float64 if dtype.kind == "f" else np.int64)
         values = values.astype(dtype)
     elif encoding in ("Base64Binary", "GZipBase64Binary"):
-        payload = "".join(text.split())
+        payload = "".join(text.split()) if any(c in text for c in " \t\r\n") else text
         raw = base64.b64decode(payload)
         if encoding == "GZipBase64Binary":
             lengths = _chunk_lengths(element)
@@ -231,6 +231,47 @@ def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
     return np.ascontiguousarray(values.reshape(shape, order=order)), intent
 
 
+_BASE64_BYTES = frozenset(b"ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/=")
+
+
+def _parse_root(data: bytes) -> ET.Element:
+    """The GIFTI document's element tree, its encoded payloads cut out before parsing.
+
+    Every ``<Data>`` payload that is plain base64 text (no markup, entities or
+    CDATA) is replaced by a placeholder, the rest of the document -- a few
+    kilobytes -- is parsed by ElementTree (so the document is still checked
+    for well-formedness), and the payloads are put back as the Data texts.
+    Parsing the megabytes of payload text was most of a mesh read.
+    """
+
+    pieces, payloads, at = [], [], 0
+    while True:
+        start = data.find(b"<Data>", at)
+        if start < 0:
+            break
+        end = data.find(b"</Data>", start + 6)
+        if end < 0:
+            break
+        payload = data[start + 6:end]
+        if len(payload) < 4096 or not _BASE64_BYTES.issuperset(payload.translate(None, b" \t\r\n")[:4096]) \
+                or b"<" in payload or b"&" in payload:
+            pieces.append(data[at:end])
+            at = end
+            continue
+        pieces.append(data[at:start + 6])
+        pieces.append(b"@%d@" % len(payloads))
+        payloads.append(payload)
+        at = end
+    pieces.append(data[at:])
+    root = ET.fromstring(b"".join(pieces))
+    if payloads:
+        for element in root.iter("Data"):
+            text = element.text or ""
+            if text.startswith("@") and text.endswith("@") and text[1:-1].isdigit():
+                element.text = payloads[int(text[1:-1])].decode("ascii")
+    return root
+
+
 def read_gifti_arrays(path: str | Path) -> list[tuple[np.ndarray, int]]:
     """Return every data array of a GIFTI file with its NIfTI intent code.
 
@@ -240,7 +281,7 @@ def read_gifti_arrays(path: str | Path) -> list[tuple[np.ndarray, int]]:
     """
 
     try:
-        root = ET.parse(str(path)).getroot()
+        root = _parse_root(Path(path).read_bytes())
     except ET.ParseError as error:
         raise ValueError(f"Not a GIFTI file (XML: {error}): {path}") from error
     if root.tag != "GIFTI":
@@ -330,7 +371,7 @@ def write_gifti_mesh(
 def _data_arrays(path) -> list[ET.Element]:
     """The DataArray elements of a GIFTI file, payloads not decoded."""
 
-    root = ET.parse(str(path)).getroot()
+    root = _parse_root(Path(path).read_bytes())
     if root.tag != "GIFTI":
         raise ValueError(f"Not a GIFTI file: {path}")
     return root.findall("DataArray")

@@ -326,3 +326,27 @@ def test_product_has_no_cpu_path():
 
     with pytest.raises(DeviceUnavailable):
         resolve_device("cpu")
+
+
+def test_gifti_reader_handles_wrapped_and_marked_up_payloads(tmp_path):
+    """The reader parses the document without its payloads; payloads other writers wrap in
+    lines or CDATA, and short ones, take the full parse and decode to the same arrays."""
+
+    import re
+
+    from cat_surface_gpu_b200.gifti import GiftiMesh, read_gifti_mesh, write_gifti_mesh
+
+    from cat_surface_gpu_b200 import synthetic
+
+    vertices, faces = synthetic.folded_icosphere(3, seed=11)
+    write_gifti_mesh(tmp_path / "a.gii", GiftiMesh(vertices, faces))
+    text = (tmp_path / "a.gii").read_text()
+    wrapped = re.sub(r"<Data>([^<]*)</Data>",
+                     lambda m: "<Data>" + "\n".join(m.group(1)[i:i + 76] for i in range(0, len(m.group(1)), 76))
+                     + "\n</Data>", text)
+    cdata = re.sub(r"<Data>([^<]*)</Data>", lambda m: "<Data><![CDATA[" + m.group(1) + "]]></Data>", text)
+    for name, body in (("wrapped.gii", wrapped), ("cdata.gii", cdata)):
+        (tmp_path / name).write_text(body)
+        mesh = read_gifti_mesh(tmp_path / name)
+        np.testing.assert_array_equal(mesh.vertices, np.asarray(vertices, dtype=np.float32))
+        np.testing.assert_array_equal(mesh.faces, np.asarray(faces, dtype=np.int32))
