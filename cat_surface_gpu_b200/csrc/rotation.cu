@@ -37,7 +37,7 @@ struct RotSurface {
     const int* grid_offsets;     // [G^3 + 1]
     const int* grid_faces;       // CSR faces
     const float* matrices;       // [n_candidates][9] column-major
-    const float* records;        // [n_tri][16] triangle records or null
+    const float* records;        // [n_tri][kRecordFloats] triangle records or null
     double* partials;            // [n_candidates][tiles]
     int n_src;
     int grid_size;
@@ -173,6 +173,11 @@ __device__ __forceinline__ float candidate_record(const float* q, const float* r
     return first ? d1 : d2;
 }
 
+// Per-triangle record (kRecordFloats floats): corners, normal, n.n and the edge Gram
+// terms (the float32 values candidate() forms), then a bounding sphere: centre and a
+// radius that also covers the closest-polygon test's 1e-3 parametric tolerance.
+constexpr int kRecordFloats = 20;
+
 __global__ void k_triangle_records(const float* __restrict__ tri, int n, float* __restrict__ rec) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= n) return;
@@ -181,13 +186,39 @@ __global__ void k_triangle_records(const float* __restrict__ tri, int n, float* 
     sub3(t + 3, t, ea);
     sub3(t + 6, t, eb);
     cross3(ea, eb, nv);
-    float* r = rec + 16LL * f;
+    float* r = rec + static_cast<long long>(kRecordFloats) * f;
     for (int k = 0; k < 9; ++k) r[k] = t[k];
     for (int k = 0; k < 3; ++k) r[9 + k] = nv[k];
     r[12] = dot3(nv, nv);
     r[13] = dot3(ea, ea);
     r[14] = dot3(ea, eb);
     r[15] = dot3(eb, eb);
+    double c[3], radius = 0.0, edge = 0.0;
+    for (int k = 0; k < 3; ++k) c[k] = (static_cast<double>(t[k]) + t[3 + k] + t[6 + k]) / 3.0;
+    for (int v = 0; v < 3; ++v) {
+        double dc = 0.0, de = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            const double a = t[3 * v + k] - c[k], b = t[3 * ((v + 1) % 3) + k] - static_cast<double>(t[3 * v + k]);
+            dc += a * a;
+            de += b * b;
+        }
+        radius = fmax(radius, sqrt(dc));
+        edge = fmax(edge, sqrt(de));
+    }
+    // a point accepted by the tolerant test lies within 1e-3 of the triangle in parametric
+    // coordinates, i.e. within 2e-3 x the longest edge of it
+    for (int k = 0; k < 3; ++k) r[16 + k] = static_cast<float>(c[k]);
+    const double scale = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    r[19] = static_cast<float>((radius + 4.0e-3 * edge) * 1.001 + 1.0e-6 * scale);
+}
+
+// Lower bound of the distance from q to every point the test can return for a record's
+// triangle (0 when q is inside the bounding sphere).
+__device__ __forceinline__ float record_reach(const float* q, const float* rec) {
+    const float4 b = __ldg(reinterpret_cast<const float4*>(rec) + 4);
+    const float dx = q[0] - b.x, dy = q[1] - b.y, dz = q[2] - b.z;
+    const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+    return dist > b.w ? dist - b.w : 0.0f;
 }
 
 // Barycentric weights of `point` in triangle t (surface_rotation.py:335-352).
@@ -241,10 +272,36 @@ __global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __rest
                 float best = INFINITY;
                 int best_face = -1;
                 float best_point[3] = {0.0f, 0.0f, 0.0f};
+                // With records: the candidate of least reach gives a distance d0 that the first
+                // minimum cannot exceed, and a candidate whose reach is clearly above sqrt(d0)
+                // cannot be it, so the ordered scan skips it; every other candidate is tested
+                // in cell order exactly as without the bound.
+                float limit = INFINITY;
+                if (S.records) {
+                    float least = INFINITY;
+                    int pick = -1;
+                    for (int k = begin; k < end; ++k) {
+                        const float reach = record_reach(q, S.records + kRecordFloats * static_cast<long long>(S.grid_faces[k]));
+                        if (reach < least) {
+                            least = reach;
+                            pick = S.grid_faces[k];
+                        }
+                    }
+                    if (pick >= 0) {
+                        float point[3];
+                        const float d0 = candidate_record(q, S.records + kRecordFloats * static_cast<long long>(pick), point);
+                        // margins far above float32 rounding of the distances, relative to the
+                        // coordinates' scale
+                        const float scale = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                        if (d0 >= 0.0f && d0 < INFINITY) limit = sqrtf(d0) * 1.0001f + 1.0e-6f * scale;
+                    }
+                }
                 for (int k = begin; k < end; ++k) {
                     const int f = S.grid_faces[k];
                     float point[3];
-                    const float d = S.records ? candidate_record(q, S.records + 16 * static_cast<long long>(f), point)
+                    if (S.records && record_reach(q, S.records + kRecordFloats * static_cast<long long>(f)) > limit)
+                        continue;
+                    const float d = S.records ? candidate_record(q, S.records + kRecordFloats * static_cast<long long>(f), point)
                                               : candidate(q, S.triangles + 9 * static_cast<long long>(f), point);
                     if (d < best) {
                         best = d;

@@ -56,7 +56,7 @@ extern "C" {
 
 const char* csg_last_error(void) { return csg::g_last_error.c_str(); }
 
-int csg_abi_version(void) { return 2; }
+int csg_abi_version(void) { return 3; }
 
 long long csg_kernel_launches(void) { return csg::g_launches.load(std::memory_order_relaxed); }
 

@@ -273,12 +273,12 @@ class RotationGridIndexDevice:
 
     @property
     def target_records(self) -> torch.Tensor:
-        """[n_tri, 16] float32 per-triangle terms of the closest-polygon test (built once, on the device)."""
+        """[n_tri, 20] float32 per-triangle terms of the closest-polygon test and a bounding sphere (built once, on the device)."""
 
         records = self.__dict__.get("_records")
         if records is None:
             tri = self.target_triangles.reshape(-1, 9).contiguous()
-            records = torch.empty((tri.shape[0], 16), dtype=torch.float32, device=self.device)
+            records = torch.empty((tri.shape[0], 20), dtype=torch.float32, device=self.device)
             _native.check(_native.library().csg_rotation_triangle_records(
                 tri.data_ptr(), int(tri.shape[0]), records.data_ptr(), _native.stream_handle(like=records)),
                 "csg_rotation_triangle_records")

@@ -420,17 +420,22 @@ typedef struct {
     int32_t n_candidates;
     int32_t n_features;          /* 0 or 1: one feature */
     int32_t n_tgt_points;        /* feature stride of tgt_values (needed when n_features > 1) */
-    const float *records;        /* optional [n_tri][16] csg_rotation_triangle_records of `triangles`
-                                    (16-byte aligned); NULL: the same terms are formed per query */
+    const float *records;        /* optional [n_tri][20] csg_rotation_triangle_records of `triangles`
+                                    (16-byte aligned); NULL: the same terms are formed per query and
+                                    every candidate of the cell is tested */
 } csg_rotation_surface;
 
 /* Per-triangle terms of the closest-polygon test, once per target sphere
- * (ABI version 2): record t = corners p0, p1, p2 (9 floats), n = (p1 - p0) x
+ * (ABI version 3): record t = corners p0, p1, p2 (9 floats), n = (p1 - p0) x
  * (p2 - p0) (3), n.n, |p1 - p0|^2, (p1 - p0).(p2 - p0), |p2 - p0|^2 -- the
  * float32 values the cost kernel would otherwise form for every query and
- * triangle, with the same operations, so costs are identical either way.
- * triangles: device [n_tri][9]; records: device [n_tri][16], 16-byte
- * aligned.  No reference counterpart (the reference forms them per query). */
+ * triangle, with the same operations -- then a bounding sphere (centre 3,
+ * radius 1) that covers every point the tolerant test can return.  With
+ * records the kernel tests first the candidate nearest by its sphere and skips
+ * every candidate whose sphere lies clearly farther than that distance: none
+ * of those can be the first minimum, so the costs are identical either way.
+ * triangles: device [n_tri][9]; records: device [n_tri][20], 16-byte
+ * aligned.  No reference counterpart (the reference tests every candidate). */
 CSG_API int csg_rotation_triangle_records(const float *triangles, int n_tri, float *records, csg_stream_t stream);
 
 CSG_API size_t csg_rotation_scratch_bytes(int n_surfaces, const int *n_src, const int *n_candidates, int tile);
