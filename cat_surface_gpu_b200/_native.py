@@ -88,6 +88,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_rotation_grid_build_device": (_I, [_P, _I, _P, _I, _I, _I, _P, _P, ctypes.c_longlong, _P, _P, c_size_t, _P]),
     "csg_rotation_cost_batch": (_I, [_I, _P, _P, _I, _I, _P, c_size_t, _P]),
     "csg_rotation_triangle_records": (_I, [_P, _I, _P, _P]),
+    "csg_rotation_status_offset": (c_size_t, [_I]),
     "csg_rotation_status": (_I, [_P, _I, _P, _P]),
     "csg_feature_resample": (_I, [_I, _I, _P, _P, _P, _P, _P]),
     "csg_feature_sheet_map": (_I, [_I, _P, _P, _P, _P, _P]),

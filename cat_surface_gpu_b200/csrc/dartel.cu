@@ -462,6 +462,33 @@ __global__ void k_combine(const T* __restrict__ rf, const T* __restrict__ rr, co
 }
 
 // (H + L_membrane) u (dartel_grid.py:1018-1070); with `b`, the residual b - (H + L) u.
+// Flat offsets of a point's four neighbours under the boundary rule.
+struct Nbr4 {
+    int xm, xp, ym, yp;
+};
+
+__device__ __forceinline__ Nbr4 neighbours(int x, int y, int nx, int ny) {
+    return {nb(x, y, -1, 0, nx, ny), nb(x, y, 1, 0, nx, ny), nb(x, y, 0, -1, nx, ny), nb(x, y, 0, 1, nx, ny)};
+}
+
+// membrane_apply_at (rtype 1) with the neighbour offsets given, for one batch element's fields.
+template <typename T>
+__device__ __forceinline__ void membrane_core(const T* __restrict__ H, const T* __restrict__ ux,
+                                              const T* __restrict__ b, T* __restrict__ o, int P, int i, const Nbr4& n,
+                                              const RegWeights& rw) {
+    const T w00 = T(rw.w[0]), w01 = T(rw.w[1]), w10 = T(rw.w[2]);
+    T reg[2];
+    for (int c = 0; c < 2; ++c) {
+        const T* f = ux + c * P;
+        reg[c] = w00 * f[i] + w01 * (f[n.ym] + f[n.yp]) + w10 * (f[n.xm] + f[n.xp]);
+    }
+    const T u0 = ux[i], u1 = ux[P + i];
+    const T a0 = reg[0] + H[i] * u0 + H[2 * P + i] * u1;
+    const T a1 = reg[1] + H[2 * P + i] * u0 + H[P + i] * u1;
+    o[i] = b[i] - a0;
+    o[P + i] = b[P + i] - a1;
+}
+
 template <typename T>
 __device__ __forceinline__ void membrane_apply_at(const T* __restrict__ hess, const T* __restrict__ u,
                                                   const T* __restrict__ b, T* __restrict__ out, int nx, int ny,
@@ -498,26 +525,30 @@ __global__ void k_membrane_apply(const T* __restrict__ hess, const T* __restrict
 // dartel_triton.py:242-291): cells with ((x + y) & 1) == colour.  Exact for
 // even nx and for nx == 1, where every neighbour read is either of the other
 // colour or the cell itself.
+// relax_at with the neighbour offsets given (o1: the batch element's point offset).
+template <typename T>
+__device__ __forceinline__ void relax_core(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u,
+                                           int P, size_t o1, int i, const Nbr4& n, T w00, T w01, T w10) {
+    T* ux = u + 2 * o1;
+    T* uy = ux + P;
+    const T rx = b[2 * o1 + i] - w01 * (ux[n.ym] + ux[n.yp]) - w10 * (ux[n.xm] + ux[n.xp]);
+    const T ry = b[2 * o1 + P + i] - w01 * (uy[n.ym] + uy[n.yp]) - w10 * (uy[n.xm] + uy[n.xp]);
+    const T* H = hess + 3 * o1;
+    const T dxx = H[i] + w00;
+    const T dyy = H[P + i] + w00;
+    const T cr = H[2 * P + i];
+    const T det = dxx * dyy * T(1.0000000001) - cr * cr;
+    const T nxv = (dyy * rx - cr * ry) / det;
+    const T nyv = (-cr * rx + dxx * ry) / det;
+    ux[i] = nxv;
+    uy[i] = nyv;
+}
+
 template <typename T>
 __device__ __forceinline__ void relax_at(const T* __restrict__ hess, const T* __restrict__ b, T* __restrict__ u,
                                          int nx, int ny, T w00, T w01, T w10, const Pt& p) {
     const int P = nx * ny;
-    const size_t o1 = static_cast<size_t>(p.b) * P;
-    T* ux = u + 2 * o1;
-    T* uy = ux + P;
-    const int xm = nb(p.x, p.y, -1, 0, nx, ny), xp = nb(p.x, p.y, 1, 0, nx, ny);
-    const int ym = nb(p.x, p.y, 0, -1, nx, ny), yp = nb(p.x, p.y, 0, 1, nx, ny);
-    const T rx = b[2 * o1 + p.i] - w01 * (ux[ym] + ux[yp]) - w10 * (ux[xm] + ux[xp]);
-    const T ry = b[2 * o1 + P + p.i] - w01 * (uy[ym] + uy[yp]) - w10 * (uy[xm] + uy[xp]);
-    const T* H = hess + 3 * o1;
-    const T dxx = H[p.i] + w00;
-    const T dyy = H[P + p.i] + w00;
-    const T cr = H[2 * P + p.i];
-    const T det = dxx * dyy * T(1.0000000001) - cr * cr;
-    const T nxv = (dyy * rx - cr * ry) / det;
-    const T nyv = (-cr * rx + dxx * ry) / det;
-    ux[p.i] = nxv;
-    uy[p.i] = nyv;
+    relax_core(hess, b, u, P, static_cast<size_t>(p.b) * P, p.i, neighbours(p.x, p.y, nx, ny), w00, w01, w10);
 }
 
 template <typename T>
@@ -554,6 +585,54 @@ __device__ __forceinline__ T wt2(T d) {
     return a < T(0.5) ? inner : (a < T(1.5) ? outer : T(0));
 }
 
+// Taps of resize_at along one axis for target index t: the three source offsets
+// (rows: reflected and scaled by the source row length; columns: periodic) and the
+// quadratic B-spline weights, formed as resize_at forms them.
+template <typename T>
+struct AxisTaps {
+    int o[3];  // minus, centre, plus
+    T w[3];
+};
+
+template <typename T>
+__device__ __forceinline__ AxisTaps<T> row_taps(int y, int sny, int tny, int snx) {
+    const T yl = (static_cast<T>(y) + T(0.5)) * static_cast<T>(sny) / static_cast<T>(tny) - T(0.5);
+    const int yo = static_cast<int>(floor(yl + T(0.5)));
+    const T yof = static_cast<T>(yo);
+    AxisTaps<T> a;
+    a.w[1] = wt2(yof - yl);
+    a.w[0] = wt2(yof - T(1) - yl);
+    a.w[2] = wt2(yof + T(1) - yl);
+    a.o[0] = reflect_y(yo - 1, sny) * snx;
+    a.o[1] = reflect_y(yo, sny) * snx;
+    a.o[2] = reflect_y(yo + 1, sny) * snx;
+    return a;
+}
+
+template <typename T>
+__device__ __forceinline__ AxisTaps<T> col_taps(int x, int snx, int tnx) {
+    const T xl = (static_cast<T>(x) + T(0.5)) * static_cast<T>(snx) / static_cast<T>(tnx) - T(0.5);
+    const int xo = static_cast<int>(floor(xl + T(0.5)));
+    const T xof = static_cast<T>(xo);
+    AxisTaps<T> a;
+    a.w[1] = wt2(xof - xl);
+    a.w[0] = wt2(xof - T(1) - xl);
+    a.w[2] = wt2(xof + T(1) - xl);
+    a.o[0] = wrap_x(xo - 1, snx);
+    a.o[1] = wrap_x(xo, snx);
+    a.o[2] = wrap_x(xo + 1, snx);
+    return a;
+}
+
+// One target value of the separable resize from its row and column taps (f: the source plane).
+template <typename T>
+__device__ __forceinline__ T resize_value(const T* __restrict__ f, const AxisTaps<T>& r, const AxisTaps<T>& c) {
+    const T im = r.w[0] * f[r.o[0] + c.o[0]] + r.w[1] * f[r.o[1] + c.o[0]] + r.w[2] * f[r.o[2] + c.o[0]];
+    const T ic = r.w[0] * f[r.o[0] + c.o[1]] + r.w[1] * f[r.o[1] + c.o[1]] + r.w[2] * f[r.o[2] + c.o[1]];
+    const T ip = r.w[0] * f[r.o[0] + c.o[2]] + r.w[1] * f[r.o[1] + c.o[2]] + r.w[2] * f[r.o[2] + c.o[2]];
+    return c.w[0] * im + c.w[1] * ic + c.w[2] * ip;
+}
+
 // Separable quadratic B-spline resize (dartel_grid.py:239-305), y pass then
 // x pass, per target point; `accumulate` adds into dst (prolongation,
 // dartel_grid.py:1380-1387).  Fields are [B * C][sny][snx] -> [B * C][tny][tnx].
@@ -562,20 +641,7 @@ __device__ __forceinline__ void resize_at(const T* __restrict__ src, T* __restri
                                           int tny, int accumulate, int plane, int i) {
     const int x = i % tnx, y = i / tnx;
     const T* f = src + static_cast<size_t>(plane) * snx * sny;
-    const T yl = (static_cast<T>(y) + T(0.5)) * static_cast<T>(sny) / static_cast<T>(tny) - T(0.5);
-    const int yo = static_cast<int>(floor(yl + T(0.5)));
-    const T yof = static_cast<T>(yo);
-    const T yw = wt2(yof - yl), ywm = wt2(yof - T(1) - yl), ywp = wt2(yof + T(1) - yl);
-    const int rm = reflect_y(yo - 1, sny) * snx, rc = reflect_y(yo, sny) * snx, rp = reflect_y(yo + 1, sny) * snx;
-    const T xl = (static_cast<T>(x) + T(0.5)) * static_cast<T>(snx) / static_cast<T>(tnx) - T(0.5);
-    const int xo = static_cast<int>(floor(xl + T(0.5)));
-    const T xof = static_cast<T>(xo);
-    const T xw = wt2(xof - xl), xwm = wt2(xof - T(1) - xl), xwp = wt2(xof + T(1) - xl);
-    const int cm = wrap_x(xo - 1, snx), cc = wrap_x(xo, snx), cp = wrap_x(xo + 1, snx);
-    const T im = ywm * f[rm + cm] + yw * f[rc + cm] + ywp * f[rp + cm];
-    const T ic = ywm * f[rm + cc] + yw * f[rc + cc] + ywp * f[rp + cc];
-    const T ip = ywm * f[rm + cp] + yw * f[rc + cp] + ywp * f[rp + cp];
-    const T r = xwm * im + xw * ic + xwp * ip;
+    const T r = resize_value(f, row_taps<T>(y, sny, tny, snx), col_taps<T>(x, snx, tnx));
     T* o = dst + static_cast<size_t>(plane) * tnx * tny;
     o[i] = accumulate ? o[i] + r : r;
 }
@@ -600,7 +666,11 @@ __global__ void k_resize(const T* __restrict__ src, T* __restrict__ dst, int snx
 // live in shared memory for the whole cycle (at most ~1,100 points over all
 // levels, 9 words each): the CTA reads the Hessians and the first level's
 // right-hand side and solution once, and writes back the first level's
-// solution, the only field read after the cycle.
+// solution, the only field read after the cycle.  Each point's neighbour
+// offsets and each level pair's resize taps (per target row and column) are
+// tabled once per launch, so the ~90 barrier-separated phases do no index or
+// weight arithmetic (the values are the ones relax_at, membrane_apply_at and
+// resize_at form).
 
 constexpr int kCoarsePoints = 512;  // measured: 512 beats 0, 2048 and 8192 at 256 x 128
 constexpr int kMaxLevels = 16;
@@ -625,25 +695,17 @@ struct CoarseCycle {
     int first, last, nit;
 };
 
+// Resize of one batch element's two planes with the target rows' and columns' taps tabled.
 template <typename T>
-__device__ __forceinline__ void block_relax(const CoarseLevel<T>& L, int bi, int nit) {
-    const int P = L.nx * L.ny;
-    for (int it = 0; it < 2 * nit; ++it) {
-        const int colour = it % 2 == 0 ? 1 : 0;
-        for (int i = threadIdx.x; i < P; i += blockDim.x) {
-            const Pt p{bi, i % L.nx, i / L.nx, i};
-            if (((p.x + p.y) & 1) == colour) relax_at(L.A, L.B, L.U, L.nx, L.ny, L.w00, L.w01, L.w10, p);
-        }
-        __syncthreads();
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ void block_resize(const T* src, int snx, int sny, T* dst, int tnx, int tny, int bi,
-                                             int accumulate) {
+__device__ __forceinline__ void taps_resize(const T* src, int snx, int sny, T* dst, int tnx, int tny,
+                                            const AxisTaps<T>* rows, const AxisTaps<T>* cols, int accumulate) {
     const int P = tnx * tny;
-    for (int j = threadIdx.x; j < 2 * P; j += blockDim.x)
-        resize_at(src, dst, snx, sny, tnx, tny, accumulate, 2 * bi + j / P, j % P);
+    for (int j = threadIdx.x; j < 2 * P; j += blockDim.x) {
+        const int c = j >= P ? 1 : 0, i = j - c * P;
+        const T r = resize_value(src + static_cast<size_t>(c) * snx * sny, rows[i / tnx], cols[i % tnx]);
+        T* o = dst + static_cast<size_t>(c) * P;
+        o[i] = accumulate ? o[i] + r : r;
+    }
     __syncthreads();
 }
 
@@ -660,6 +722,21 @@ __device__ __forceinline__ CoarseLevel<T> shared_level(const CoarseLevel<T>& L, 
     return S;
 }
 
+// Red-black relaxation of a shared-memory level with tabled neighbour offsets.
+template <typename T>
+__device__ __forceinline__ void table_relax(const CoarseLevel<T>& L, const int4* tab, int nit) {
+    const int P = L.nx * L.ny;
+    for (int it = 0; it < 2 * nit; ++it) {
+        const int colour = it % 2 == 0 ? 1 : 0;
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const int4 t = tab[i];
+            if (((i % L.nx + i / L.nx) & 1) == colour)
+                relax_core(L.A, L.B, L.U, P, 0, i, Nbr4{t.x, t.y, t.z, t.w}, L.w00, L.w01, L.w10);
+        }
+        __syncthreads();
+    }
+}
+
 // cycle(first) of Fmg (host side) restricted to levels first..last, for batch element blockIdx.x.
 template <typename T>
 __global__ void __launch_bounds__(kCoarseCycleThreads) k_fmg_coarse_cycle(CoarseCycle<T> c) {
@@ -667,7 +744,13 @@ __global__ void __launch_bounds__(kCoarseCycleThreads) k_fmg_coarse_cycle(Coarse
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* base = reinterpret_cast<T*>(smem_raw);
     const int bi = blockIdx.x;
+    int words = 0;
     for (int l = c.first; l <= c.last; ++l) {
+        words += 9 * c.lv[l].nx * c.lv[l].ny;
+    }
+    // neighbour offsets of every point of every level, after the fields (16-byte aligned)
+    int4* table = reinterpret_cast<int4*>(smem_raw + ((static_cast<size_t>(words) * sizeof(T) + 15) & ~size_t(15)));
+    for (int l = c.first, toff = 0; l <= c.last; ++l) {
         const CoarseLevel<T>& L = c.lv[l];
         const CoarseLevel<T> S = shared_level(L, base);
         const int P = L.nx * L.ny;
@@ -678,27 +761,68 @@ __global__ void __launch_bounds__(kCoarseCycleThreads) k_fmg_coarse_cycle(Coarse
                 S.B[j] = L.B[2 * static_cast<size_t>(bi) * P + j];
                 S.U[j] = L.U[2 * static_cast<size_t>(bi) * P + j];
             }
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const Nbr4 n = neighbours(i % L.nx, i / L.nx, L.nx, L.ny);
+            table[toff + i] = make_int4(n.xm, n.xp, n.ym, n.yp);
+        }
+        toff += P;
+    }
+    __syncthreads();
+    int toff = 0;
+    int level_toff[kMaxLevels];
+    for (int l = c.first; l <= c.last; ++l) {
+        level_toff[l] = toff;
+        toff += c.lv[l].nx * c.lv[l].ny;
+    }
+    // resize taps per level pair: restriction rows/columns of level l + 1, prolongation rows/columns of l
+    AxisTaps<T>* taps = reinterpret_cast<AxisTaps<T>*>(table + toff);
+    int down_rows[kMaxLevels], down_cols[kMaxLevels], up_rows[kMaxLevels], up_cols[kMaxLevels];
+    {
+        int at = 0;
+        for (int l = c.first; l < c.last; ++l) {
+            const CoarseLevel<T>& L = c.lv[l];
+            const CoarseLevel<T>& N = c.lv[l + 1];
+            down_rows[l] = at;
+            at += N.ny;
+            down_cols[l] = at;
+            at += N.nx;
+            up_rows[l] = at;
+            at += L.ny;
+            up_cols[l] = at;
+            at += L.nx;
+            for (int k = threadIdx.x; k < N.ny + N.nx + L.ny + L.nx; k += blockDim.x) {
+                AxisTaps<T> t;
+                if (k < N.ny) t = row_taps<T>(k, L.ny, N.ny, L.nx);
+                else if (k < N.ny + N.nx) t = col_taps<T>(k - N.ny, L.nx, N.nx);
+                else if (k < N.ny + N.nx + L.ny) t = row_taps<T>(k - N.ny - N.nx, N.ny, L.ny, N.nx);
+                else t = col_taps<T>(k - N.ny - N.nx - L.ny, N.nx, L.nx);
+                taps[down_rows[l] + k] = t;
+            }
+        }
     }
     __syncthreads();
     for (int l = c.first; l < c.last; ++l) {
         const CoarseLevel<T> L = shared_level(c.lv[l], base);
-        block_relax(L, 0, c.nit);
+        const int4* tab = table + level_toff[l];
+        table_relax(L, tab, c.nit);
         const int P = L.nx * L.ny;
-        for (int i = threadIdx.x; i < P; i += blockDim.x)
-            membrane_apply_at(L.A, L.U, L.B, L.R, L.nx, L.ny, L.rw, Pt{0, i % L.nx, i / L.nx, i});
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const int4 t = tab[i];
+            membrane_core(L.A, L.U, L.B, L.R, P, i, Nbr4{t.x, t.y, t.z, t.w}, L.rw);
+        }
         __syncthreads();
         const CoarseLevel<T> N = shared_level(c.lv[l + 1], base);
-        block_resize(L.R, L.nx, L.ny, N.B, N.nx, N.ny, 0, 0);
+        taps_resize(L.R, L.nx, L.ny, N.B, N.nx, N.ny, taps + down_rows[l], taps + down_cols[l], 0);
         const int Pn = N.nx * N.ny;
         for (int j = threadIdx.x; j < 2 * Pn; j += blockDim.x) N.U[j] = T(0);
         __syncthreads();
     }
-    block_relax(shared_level(c.lv[c.last], base), 0, c.nit);
+    table_relax(shared_level(c.lv[c.last], base), table + level_toff[c.last], c.nit);
     for (int l = c.last; l-- > c.first;) {
         const CoarseLevel<T> L = shared_level(c.lv[l], base);
         const CoarseLevel<T> N = shared_level(c.lv[l + 1], base);
-        block_resize(N.U, N.nx, N.ny, L.U, L.nx, L.ny, 0, 1);
-        block_relax(L, 0, c.nit);
+        taps_resize(N.U, N.nx, N.ny, L.U, L.nx, L.ny, taps + up_rows[l], taps + up_cols[l], 1);
+        table_relax(L, table + level_toff[l], c.nit);
     }
     const CoarseLevel<T>& F = c.lv[c.first];
     const int P = F.nx * F.ny;
@@ -709,9 +833,15 @@ __global__ void __launch_bounds__(kCoarseCycleThreads) k_fmg_coarse_cycle(Coarse
 // Shared memory of the coarse cycle over levels first..last (specs: (nx, ny) per level).
 template <typename T>
 size_t coarse_cycle_smem(const std::vector<std::pair<int, int>>& specs, size_t first) {
-    size_t words = 0;
-    for (size_t l = first; l < specs.size(); ++l) words += 9 * static_cast<size_t>(specs[l].first) * specs[l].second;
-    return words * sizeof(T);
+    size_t words = 0, points = 0;
+    for (size_t l = first; l < specs.size(); ++l) {
+        words += 9 * static_cast<size_t>(specs[l].first) * specs[l].second;
+        points += static_cast<size_t>(specs[l].first) * specs[l].second;
+    }
+    size_t taps = 0;
+    for (size_t l = first; l + 1 < specs.size(); ++l)
+        taps += static_cast<size_t>(specs[l].first + specs[l].second + specs[l + 1].first + specs[l + 1].second);
+    return ((words * sizeof(T) + 15) & ~size_t(15)) + points * sizeof(int4) + taps * sizeof(AxisTaps<T>);
 }
 
 // ------------------------------------------------ fused fine-level V-cycle legs
@@ -798,8 +928,10 @@ __device__ void load_image(const T* __restrict__ A, const T* __restrict__ B, con
 // exact: its distance to the nearest cut edge of the region (x edges unless
 // the region spans the periodic x range, y edges inside the grid); all are
 // formed once per leg instead of once per half-sweep.
-constexpr int kLegPts = 3;
-constexpr int kLegThreads = 256;
+// measured on 2 maps x 256 x 128 float64: 512 threads with two points of each colour
+// solve in 8.27 ms against 9.08 ms for 256 threads with three
+constexpr int kLegPts = 2;
+constexpr int kLegThreads = 512;
 
 struct LegPoint {
     int q;  // image index, -1 for an empty slot
@@ -1055,9 +1187,9 @@ constexpr long long leg_max_ctas() {
 // kChainPoints points per grid, in one launch with one CTA per batch element:
 // the same resize_at per point as separate k_resize launches, level after
 // level, with __syncthreads between levels.  Each restricted level is kept in
-// shared memory (at most ~2,800 points x channels over all levels) as the
+// shared memory (at most ~700 points x channels over all levels) as the
 // source of the next one, and written to its field.
-constexpr int kChainPoints = 2048;
+constexpr int kChainPoints = 512;  // measured: 512 beats 2,048 (7.96 vs 8.14 ms per 256 x 128 solve) and matches 128
 
 template <typename T>
 struct ResizeChain {
@@ -1073,29 +1205,48 @@ __global__ void __launch_bounds__(kCoarseThreads) k_resize_chain(ResizeChain<T> 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* base = reinterpret_cast<T*>(smem_raw);
     const int bi = blockIdx.x;
+    // every level's row and column taps first (after the level images), then the levels
+    int words = 0, ntaps = 0;
     for (int l = c.first; l <= c.last; ++l) {
+        words += c.channels * c.nx[l] * c.ny[l];
+        ntaps += c.nx[l] + c.ny[l];
+    }
+    AxisTaps<T>* taps = reinterpret_cast<AxisTaps<T>*>(smem_raw + ((static_cast<size_t>(words) * sizeof(T) + 15) & ~size_t(15)));
+    for (int l = c.first, at = 0; l <= c.last; ++l) {
+        for (int k = threadIdx.x; k < c.ny[l] + c.nx[l]; k += blockDim.x)
+            taps[at + k] = k < c.ny[l] ? row_taps<T>(k, c.ny[l - 1], c.ny[l], c.nx[l - 1])
+                                       : col_taps<T>(k - c.ny[l], c.nx[l - 1], c.nx[l]);
+        at += c.ny[l] + c.nx[l];
+    }
+    __syncthreads();
+    for (int l = c.first, at = 0; l <= c.last; ++l) {
         const int P = c.nx[l] * c.ny[l];
         const size_t plane0 = static_cast<size_t>(c.channels) * bi;
         T* image = base + c.off[l];
         T* out = c.field[l] + plane0 * P;
+        const T* src = l == c.first ? c.field[l - 1] + plane0 * c.nx[l - 1] * c.ny[l - 1] : base + c.off[l - 1];
+        const AxisTaps<T>* rows = taps + at;
+        const AxisTaps<T>* cols = rows + c.ny[l];
         for (int j = threadIdx.x; j < c.channels * P; j += blockDim.x) {
-            if (l == c.first)  // the source level lives in global memory
-                resize_at(c.field[l - 1], c.field[l], c.nx[l - 1], c.ny[l - 1], c.nx[l], c.ny[l], 0,
-                          static_cast<int>(plane0) + j / P, j % P);
-            else
-                resize_at(static_cast<const T*>(base + c.off[l - 1]), out, c.nx[l - 1], c.ny[l - 1], c.nx[l],
-                          c.ny[l], 0, j / P, j % P);
-            image[j] = out[j];
+            const int ch = j / P, i = j - ch * P;
+            const T r = resize_value(src + static_cast<size_t>(ch) * c.nx[l - 1] * c.ny[l - 1], rows[i / c.nx[l]],
+                                     cols[i % c.nx[l]]);
+            out[j] = r;
+            image[j] = r;
         }
+        at += c.ny[l] + c.nx[l];
         __syncthreads();
     }
 }
 
 template <typename T>
 size_t resize_chain_smem(const ResizeChain<T>& c) {
-    size_t words = 0;
-    for (int l = c.first; l <= c.last; ++l) words += static_cast<size_t>(c.channels) * c.nx[l] * c.ny[l];
-    return words * sizeof(T);
+    size_t words = 0, taps = 0;
+    for (int l = c.first; l <= c.last; ++l) {
+        words += static_cast<size_t>(c.channels) * c.nx[l] * c.ny[l];
+        taps += static_cast<size_t>(c.nx[l] + c.ny[l]);
+    }
+    return ((words * sizeof(T) + 15) & ~size_t(15)) + taps * sizeof(AxisTaps<T>);
 }
 
 // Opt the leg, coarse-cycle and chain kernels in to more than 48 KB of dynamic

@@ -646,6 +646,11 @@ int csg_rotation_triangle_records(const float* triangles, int n_tri, float* reco
     return CSG_OK;
 }
 
+size_t csg_rotation_status_offset(int n_surfaces) {
+    if (n_surfaces < 1) return 0;
+    return align256(sizeof(RotSurface) * n_surfaces) + align256(sizeof(long long) * n_surfaces);
+}
+
 int csg_rotation_status(const void* scratch, int n_surfaces, csg_stream_t stream, int* status) {
     if (!scratch || !status || n_surfaces < 1) return csg::fail(CSG_ERR_ARG, "rotation status: bad arguments");
     const size_t off = align256(sizeof(RotSurface) * n_surfaces) + align256(sizeof(long long) * n_surfaces);

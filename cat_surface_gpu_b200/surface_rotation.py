@@ -214,6 +214,11 @@ class _Costing:
         self.scratch = torch.empty(int(need), dtype=torch.uint8, device=dev)
         self.pinned = torch.empty(self.capacity, dtype=torch.float64, pin_memory=True)
         self.staging = torch.empty((self.capacity, 9), dtype=torch.float32, pin_memory=True)
+        self.staging_host = self.staging.numpy()
+        # the kernel's coverage status word, read back with the costs in one synchronisation
+        offset = int(_native.library().csg_rotation_status_offset(1))
+        self.status_device = self.scratch[offset:offset + 4].view(torch.int32)
+        self.status_host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
 
     def evaluate(self, angles: np.ndarray, *, host: bool = False):
         """Costs of these candidates: a device tensor, or (``host``) a NumPy copy read back in the
@@ -225,7 +230,7 @@ class _Costing:
             raise ValueError("more candidates than this costing context holds")
         # page-locked staging: an asynchronous upload (the previous call's status read has
         # synchronised, so the staging rows are free)
-        self.staging[:count].copy_(torch.from_numpy(mats))
+        np.copyto(self.staging_host[:count], mats)
         self.matrices[:count].copy_(self.staging[:count], non_blocking=True)
         surface = _native.RotationSurface(
             self.inputs.source_points.data_ptr(), self.inputs.source_values.data_ptr(),
@@ -245,10 +250,9 @@ class _Costing:
         )
         if host:
             self.pinned[:count].copy_(self.costs[:count], non_blocking=True)
-        status = ctypes.c_int(0)
-        _native.check(lib.csg_rotation_status(self.scratch.data_ptr(), 1, stream, ctypes.addressof(status)),
-                      "csg_rotation_status")
-        if status.value != 0:
+        self.status_host.copy_(self.status_device, non_blocking=True)
+        torch.cuda.current_stream(self.costs.device).synchronize()
+        if int(self.status_host[0]) != 0:
             raise RuntimeError("Rotation is not covered by target sphere candidate index")
         if host:
             return self.pinned[:count].numpy().copy()

@@ -453,6 +453,12 @@ CSG_API size_t csg_rotation_scratch_bytes(int n_surfaces, const int *n_src, cons
 CSG_API int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface *surfaces, double *costs, int tile,
                                     int n_ctas, void *scratch, size_t scratch_bytes, csg_stream_t stream);
 
+/* Byte offset in the scratch of csg_rotation_cost_batch(n_surfaces, ...) of the
+ * int coverage status that csg_rotation_status reads (0 for n_surfaces < 1), so
+ * a caller can copy it with its own asynchronous readback.  No reference
+ * counterpart. */
+CSG_API size_t csg_rotation_status_offset(int n_surfaces);
+
 /* Synchronously read the coverage status of the last csg_rotation_cost_batch
  * that used this scratch (CSG_OK or CSG_ERR_COVERAGE). */
 CSG_API int csg_rotation_status(const void *scratch, int n_surfaces, csg_stream_t stream, int *status);
