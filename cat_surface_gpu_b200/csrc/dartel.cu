@@ -696,17 +696,30 @@ struct CoarseCycle {
 };
 
 // Resize of one batch element's two planes with the target rows' and columns' taps tabled.
-template <typename T>
+// The threads that work a phase of the coarse cycle and their barrier: the whole CTA,
+// or (levels of at most 32 points) warp 0 alone with a warp barrier.
+template <bool WARP>
+struct Team {
+    static __device__ __forceinline__ int rank() { return WARP ? (threadIdx.x & 31) : threadIdx.x; }
+    static __device__ __forceinline__ int size() { return WARP ? 32 : blockDim.x; }
+    static __device__ __forceinline__ void sync() {
+        if (WARP) __syncwarp();
+        else __syncthreads();
+    }
+};
+
+// Resize of one batch element's two planes with the target rows' and columns' taps tabled.
+template <bool WARP, typename T>
 __device__ __forceinline__ void taps_resize(const T* src, int snx, int sny, T* dst, int tnx, int tny,
                                             const AxisTaps<T>* rows, const AxisTaps<T>* cols, int accumulate) {
     const int P = tnx * tny;
-    for (int j = threadIdx.x; j < 2 * P; j += blockDim.x) {
+    for (int j = Team<WARP>::rank(); j < 2 * P; j += Team<WARP>::size()) {
         const int c = j >= P ? 1 : 0, i = j - c * P;
         const T r = resize_value(src + static_cast<size_t>(c) * snx * sny, rows[i / tnx], cols[i % tnx]);
         T* o = dst + static_cast<size_t>(c) * P;
         o[i] = accumulate ? o[i] + r : r;
     }
-    __syncthreads();
+    Team<WARP>::sync();
 }
 
 // The shared-memory image of level L (one batch element, batch index 0).
@@ -723,18 +736,48 @@ __device__ __forceinline__ CoarseLevel<T> shared_level(const CoarseLevel<T>& L, 
 }
 
 // Red-black relaxation of a shared-memory level with tabled neighbour offsets.
-template <typename T>
+template <bool WARP, typename T>
 __device__ __forceinline__ void table_relax(const CoarseLevel<T>& L, const int4* tab, int nit) {
     const int P = L.nx * L.ny;
     for (int it = 0; it < 2 * nit; ++it) {
         const int colour = it % 2 == 0 ? 1 : 0;
-        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        for (int i = Team<WARP>::rank(); i < P; i += Team<WARP>::size()) {
             const int4 t = tab[i];
             if (((i % L.nx + i / L.nx) & 1) == colour)
                 relax_core(L.A, L.B, L.U, P, 0, i, Nbr4{t.x, t.y, t.z, t.w}, L.w00, L.w01, L.w10);
         }
-        __syncthreads();
+        Team<WARP>::sync();
     }
+}
+
+// The down half of the V-cycle at level l: relaxation, residual, its restriction to
+// level l + 1 and that level's zero solution.
+template <bool WARP, typename T>
+__device__ __forceinline__ void coarse_down(const CoarseCycle<T>& c, int l, T* base, const int4* tab,
+                                            const AxisTaps<T>* rows, const AxisTaps<T>* cols) {
+    const CoarseLevel<T> L = shared_level(c.lv[l], base);
+    table_relax<WARP>(L, tab, c.nit);
+    const int P = L.nx * L.ny;
+    for (int i = Team<WARP>::rank(); i < P; i += Team<WARP>::size()) {
+        const int4 t = tab[i];
+        membrane_core(L.A, L.U, L.B, L.R, P, i, Nbr4{t.x, t.y, t.z, t.w}, L.rw);
+    }
+    Team<WARP>::sync();
+    const CoarseLevel<T> N = shared_level(c.lv[l + 1], base);
+    taps_resize<WARP>(L.R, L.nx, L.ny, N.B, N.nx, N.ny, rows, cols, 0);
+    const int Pn = N.nx * N.ny;
+    for (int j = Team<WARP>::rank(); j < 2 * Pn; j += Team<WARP>::size()) N.U[j] = T(0);
+    Team<WARP>::sync();
+}
+
+// The up half at level l: prolongation of level l + 1's solution, then relaxation.
+template <bool WARP, typename T>
+__device__ __forceinline__ void coarse_up(const CoarseCycle<T>& c, int l, T* base, const int4* tab,
+                                          const AxisTaps<T>* rows, const AxisTaps<T>* cols) {
+    const CoarseLevel<T> L = shared_level(c.lv[l], base);
+    const CoarseLevel<T> N = shared_level(c.lv[l + 1], base);
+    taps_resize<WARP>(N.U, N.nx, N.ny, L.U, L.nx, L.ny, rows, cols, 1);
+    table_relax<WARP>(L, tab, c.nit);
 }
 
 // cycle(first) of Fmg (host side) restricted to levels first..last, for batch element blockIdx.x.
@@ -801,29 +844,21 @@ __global__ void __launch_bounds__(kCoarseCycleThreads) k_fmg_coarse_cycle(Coarse
         }
     }
     __syncthreads();
-    for (int l = c.first; l < c.last; ++l) {
-        const CoarseLevel<T> L = shared_level(c.lv[l], base);
-        const int4* tab = table + level_toff[l];
-        table_relax(L, tab, c.nit);
-        const int P = L.nx * L.ny;
-        for (int i = threadIdx.x; i < P; i += blockDim.x) {
-            const int4 t = tab[i];
-            membrane_core(L.A, L.U, L.B, L.R, P, i, Nbr4{t.x, t.y, t.z, t.w}, L.rw);
-        }
-        __syncthreads();
-        const CoarseLevel<T> N = shared_level(c.lv[l + 1], base);
-        taps_resize(L.R, L.nx, L.ny, N.B, N.nx, N.ny, taps + down_rows[l], taps + down_cols[l], 0);
-        const int Pn = N.nx * N.ny;
-        for (int j = threadIdx.x; j < 2 * Pn; j += blockDim.x) N.U[j] = T(0);
-        __syncthreads();
+    // levels from `tail` on hold at most 32 points: warp 0 runs them with warp barriers
+    int tail = c.last;
+    while (tail > c.first && c.lv[tail - 1].nx * c.lv[tail - 1].ny <= 32) --tail;
+    for (int l = c.first; l < tail; ++l)
+        coarse_down<false>(c, l, base, table + level_toff[l], taps + down_rows[l], taps + down_cols[l]);
+    if (threadIdx.x < 32) {
+        for (int l = tail; l < c.last; ++l)
+            coarse_down<true>(c, l, base, table + level_toff[l], taps + down_rows[l], taps + down_cols[l]);
+        table_relax<true>(shared_level(c.lv[c.last], base), table + level_toff[c.last], c.nit);
+        for (int l = c.last; l-- > tail;)
+            coarse_up<true>(c, l, base, table + level_toff[l], taps + up_rows[l], taps + up_cols[l]);
     }
-    table_relax(shared_level(c.lv[c.last], base), table + level_toff[c.last], c.nit);
-    for (int l = c.last; l-- > c.first;) {
-        const CoarseLevel<T> L = shared_level(c.lv[l], base);
-        const CoarseLevel<T> N = shared_level(c.lv[l + 1], base);
-        taps_resize(N.U, N.nx, N.ny, L.U, L.nx, L.ny, taps + up_rows[l], taps + up_cols[l], 1);
-        table_relax(L, table + level_toff[l], c.nit);
-    }
+    __syncthreads();
+    for (int l = tail; l-- > c.first;)
+        coarse_up<false>(c, l, base, table + level_toff[l], taps + up_rows[l], taps + up_cols[l]);
     const CoarseLevel<T>& F = c.lv[c.first];
     const int P = F.nx * F.ny;
     const T* su = base + F.off + 5 * P;
