@@ -177,6 +177,8 @@ __device__ __forceinline__ float candidate_record(const float* q, const float* r
 // terms (the float32 values candidate() forms), then a bounding sphere: centre and a
 // radius that also covers the closest-polygon test's 1e-3 parametric tolerance.
 constexpr int kRecordFloats = 20;
+constexpr int kMaxCompact = 64;  // candidates per cell whose reaches the cost scan keeps
+static_assert(kMaxCompact <= 64, "the survivors of a cell are one 64-bit mask");
 
 __global__ void k_triangle_records(const float* __restrict__ tri, int n, float* __restrict__ rec) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,17 +276,24 @@ __global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __rest
                 float best_point[3] = {0.0f, 0.0f, 0.0f};
                 // With records: the candidate of least reach gives a distance d0 that the first
                 // minimum cannot exceed, and a candidate whose reach is clearly above sqrt(d0)
-                // cannot be it, so the ordered scan skips it; every other candidate is tested
-                // in cell order exactly as without the bound.
+                // cannot be it, so the scan skips it; every other candidate is tested in cell
+                // order exactly as without the bound. Cells of at most kMaxCompact candidates
+                // keep the reaches of the first pass and test the survivors of a bit mask, so
+                // the threads of a warp loop over their own short lists.
+                const int count = end - begin;
+                const bool compact = S.records != nullptr && count <= kMaxCompact;
+                float reach[kMaxCompact];
                 float limit = INFINITY;
                 if (S.records) {
                     float least = INFINITY;
                     int pick = -1;
-                    for (int k = begin; k < end; ++k) {
-                        const float reach = record_reach(q, S.records + kRecordFloats * static_cast<long long>(S.grid_faces[k]));
-                        if (reach < least) {
-                            least = reach;
-                            pick = S.grid_faces[k];
+                    for (int k = 0; k < count; ++k) {
+                        const int f = S.grid_faces[begin + k];
+                        const float r = record_reach(q, S.records + kRecordFloats * static_cast<long long>(f));
+                        if (compact) reach[k] = r;
+                        if (r < least) {
+                            least = r;
+                            pick = f;
                         }
                     }
                     if (pick >= 0) {
@@ -296,11 +305,8 @@ __global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __rest
                         if (d0 >= 0.0f && d0 < INFINITY) limit = sqrtf(d0) * 1.0001f + 1.0e-6f * scale;
                     }
                 }
-                for (int k = begin; k < end; ++k) {
-                    const int f = S.grid_faces[k];
+                auto test = [&](int f) {
                     float point[3];
-                    if (S.records && record_reach(q, S.records + kRecordFloats * static_cast<long long>(f)) > limit)
-                        continue;
                     const float d = S.records ? candidate_record(q, S.records + kRecordFloats * static_cast<long long>(f), point)
                                               : candidate(q, S.triangles + 9 * static_cast<long long>(f), point);
                     if (d < best) {
@@ -309,6 +315,23 @@ __global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __rest
                         best_point[0] = point[0];
                         best_point[1] = point[1];
                         best_point[2] = point[2];
+                    }
+                };
+                if (compact) {
+                    unsigned long long live = 0;
+                    for (int k = 0; k < count; ++k)
+                        if (!(reach[k] > limit)) live |= 1ull << k;
+                    while (live) {
+                        const int k = __ffsll(static_cast<long long>(live)) - 1;
+                        live &= live - 1;
+                        test(S.grid_faces[begin + k]);
+                    }
+                } else {
+                    for (int k = begin; k < end; ++k) {
+                        const int f = S.grid_faces[k];
+                        if (S.records && record_reach(q, S.records + kRecordFloats * static_cast<long long>(f)) > limit)
+                            continue;
+                        test(f);
                     }
                 }
                 if (best_face < 0) {  // every candidate produced NaN
