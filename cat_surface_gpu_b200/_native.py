@@ -21,6 +21,7 @@ CSG_ERR_LAUNCH = -4
 CSG_ERR_TOPOLOGY = -5
 CSG_ERR_UNSUPPORTED = -6
 CSG_ERR_COVERAGE = -7
+CSG_ERR_FORMAT = -8
 
 ARITH = {"cat": 0, "fp32": 1, "fp64": 2}
 CSG_DTYPE_F32 = 0
@@ -104,6 +105,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_stencil_scratch_bytes": (c_size_t, [_I, _I, _I, _I, _I, _I]),
     "csg_stencil_build_device": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P,
                                       c_size_t, _P]),
+    "csg_gifti_decode": (_I, [_P, c_size_t, _I, _P, _I, ctypes.c_longlong, _P, c_size_t, _P]),
     "csg_read_status": (_I, [_P, _P, _P, _P]),
 }
 

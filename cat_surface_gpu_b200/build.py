@@ -64,7 +64,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if failed:
         raise RuntimeError("nvcc failed:\n" + "\n".join(failed))
     tmp = LIBRARY.with_suffix(".so.tmp")
-    subprocess.run([nvcc, *ARCH, "-shared", "-o", str(tmp), *objects], check=True)
+    subprocess.run([nvcc, *ARCH, "-shared", "-o", str(tmp), *objects, "-lz"], check=True)
     os.replace(tmp, LIBRARY)
     return LIBRARY
 

@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import base64
 from collections import OrderedDict
+import ctypes
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 import os
@@ -142,44 +143,40 @@ def _chunk_lengths(element: ET.Element) -> list[int] | None:
     return None
 
 
-def _inflate(raw: bytes, lengths: list[int] | None) -> bytes:
-    """zlib.decompress(raw), with the chunks of a chunk-indexed stream inflated in parallel.
+def _decode_payload(payload: bytes, gzip: bool, lengths: list[int] | None, out: np.ndarray) -> int:
+    """Decode base64 ``payload`` (inflating it when ``gzip``) into the bytes of ``out``; returns their Adler-32.
 
-    The result is checked against the stream's Adler-32 like zlib's own; a
-    stream whose index does not fit it is inflated as one stream.
+    Runs in the native library without the interpreter lock (the chunks of a
+    chunk-indexed stream on several threads); ``ValueError`` when the payload
+    is not base64, the stream is corrupt or truncated (Adler-32 checked as
+    zlib does), or it decodes to another size than ``out``.  An index that
+    does not fit the stream is ignored and the stream inflates as one.
     """
 
-    body = len(raw) - 6
-    if not lengths or len(lengths) < 2 or body < 0 or sum(lengths) != body or (raw[0] * 256 + raw[1]) % 31 != 0:
-        return zlib.decompress(raw)
-    starts = [2]
-    for n in lengths[:-1]:
-        starts.append(starts[-1] + n)
-    last = len(lengths) - 1
+    from . import _native
 
-    def one(index):
-        stream = zlib.decompressobj(-15)
-        out = stream.decompress(raw[starts[index]: starts[index] + lengths[index]])
-        if stream.eof != (index == last) or stream.unused_data:
-            raise zlib.error("chunk boundaries do not match the deflate stream")
-        return out
-
-    out = b"".join(_pool().map(one, range(len(lengths))))
-    if zlib.adler32(out) != int.from_bytes(raw[-4:], "big"):
-        raise zlib.error("incorrect data check")
-    return out
+    index = (ctypes.c_longlong * len(lengths))(*lengths) if lengths else None
+    check = ctypes.c_uint(0)
+    status = _native.library().csg_gifti_decode(payload, len(payload), int(bool(gzip)), index,
+                                                len(lengths) if lengths else 0, _CHUNK, out.ctypes.data, out.nbytes,
+                                                ctypes.byref(check))
+    if status != _native.CSG_OK:
+        raise ValueError(_native.last_error())
+    return check.value
 
 
 # Encoded payloads of the int32 arrays decoded most recently (face arrays): writing an
 # array with the same bytes reuses its payload instead of compressing it again.  Keyed
-# by (DataType, shape, CRC-32); a hit is confirmed by comparing the bytes themselves.
+# by (DataType, shape, Adler-32 of the bytes) -- the check value a zlib stream carries,
+# so a read gets it for free; a hit is confirmed by comparing the bytes themselves.
 _PAYLOADS: OrderedDict = OrderedDict()
 _PAYLOADS_MAX = 8
 _PAYLOADS_LOCK = threading.Lock()
 
 
-def _remember_payload(dtype_name: str, shape: tuple, raw: bytes, payload: str, lengths: list[int] | None) -> None:
-    key = (dtype_name, shape, zlib.crc32(raw))
+def _remember_payload(dtype_name: str, shape: tuple, raw: bytes, check: int, payload: bytes,
+                      lengths: list[int] | None) -> None:
+    key = (dtype_name, shape, check)
     with _PAYLOADS_LOCK:
         _PAYLOADS[key] = (raw, payload, lengths)
         _PAYLOADS.move_to_end(key)
@@ -187,15 +184,15 @@ def _remember_payload(dtype_name: str, shape: tuple, raw: bytes, payload: str, l
             _PAYLOADS.popitem(last=False)
 
 
-def _known_payload(dtype_name: str, shape: tuple, raw: bytes) -> tuple[str, list[int] | None] | None:
+def _known_payload(dtype_name: str, shape: tuple, raw: bytes) -> tuple[bytes, list[int] | None] | None:
     with _PAYLOADS_LOCK:
-        hit = _PAYLOADS.get((dtype_name, shape, zlib.crc32(raw)))
+        hit = _PAYLOADS.get((dtype_name, shape, zlib.adler32(raw)))
     if hit is not None and hit[0] == raw:
         return hit[1], hit[2]
     return None
 
 
-def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
+def _decode_array(element: ET.Element, payloads: list[bytes] = ()) -> tuple[np.ndarray, int]:
     attrs = element.attrib
     dtype_name = attrs.get("DataType", "NIFTI_TYPE_FLOAT32")
     if dtype_name not in _DTYPES:
@@ -206,26 +203,26 @@ def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
     encoding = attrs.get("Encoding", "ASCII")
     endian = attrs.get("Endian", "LittleEndian")
     order = "F" if attrs.get("ArrayIndexingOrder", "RowMajorOrder") == "ColumnMajorOrder" else "C"
-    data_element = element.find("Data")
-    text = "" if data_element is None or data_element.text is None else data_element.text
     count = int(np.prod(shape)) if shape else 0
     if encoding == "ASCII":
+        data_element = element.find("Data")
+        text = "" if data_element is None or data_element.text is None else data_element.text
         values = np.array(text.split(), dtype=np.float64 if dtype.kind == "f" else np.int64)
         values = values.astype(dtype)
+        if values.size != count:
+            raise ValueError(f"GIFTI array holds {values.size} values, header says {count}")
     elif encoding in ("Base64Binary", "GZipBase64Binary"):
-        payload = "".join(text.split()) if any(c in text for c in " \t\r\n") else text
-        raw = base64.b64decode(payload)
-        if encoding == "GZipBase64Binary":
-            lengths = _chunk_lengths(element)
-            raw = _inflate(raw, lengths)
-            if dtype_name == "NIFTI_TYPE_INT32" and endian == "LittleEndian" and order == "C":
-                _remember_payload(dtype_name, shape, raw, payload, lengths)
+        payload = _payload(element, payloads)
+        gzip = encoding == "GZipBase64Binary"
+        lengths = _chunk_lengths(element) if gzip else None
+        out = np.empty(count * dtype.itemsize, dtype=np.uint8)
+        check = _decode_payload(payload, gzip, lengths, out)
+        if gzip and dtype_name == "NIFTI_TYPE_INT32" and endian == "LittleEndian" and order == "C":
+            _remember_payload(dtype_name, shape, out.tobytes(), check, _without_whitespace(payload), lengths)
         wire = dtype.newbyteorder("<" if endian == "LittleEndian" else ">")
-        values = np.frombuffer(raw, dtype=wire).astype(dtype)
+        values = out.view(wire).astype(dtype, copy=False)
     else:
         raise ValueError(f"Unsupported GIFTI encoding {encoding}")
-    if values.size != count:
-        raise ValueError(f"GIFTI array holds {values.size} values, header says {count}")
     intent_attr = attrs.get("Intent", "NIFTI_INTENT_NONE")
     intent = _INTENT_CODES.get(intent_attr, 0)
     return np.ascontiguousarray(values.reshape(shape, order=order)), intent
@@ -234,14 +231,15 @@ def _decode_array(element: ET.Element) -> tuple[np.ndarray, int]:
 _BASE64_BYTES = frozenset(b"ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/=")
 
 
-def _parse_root(data: bytes) -> ET.Element:
-    """The GIFTI document's element tree, its encoded payloads cut out before parsing.
+def _parse_document(data: bytes) -> tuple[ET.Element, list[bytes]]:
+    """The GIFTI document's element tree and its encoded payloads, cut out before parsing.
 
     Every ``<Data>`` payload that is plain base64 text (no markup, entities or
-    CDATA) is replaced by a placeholder, the rest of the document -- a few
-    kilobytes -- is parsed by ElementTree (so the document is still checked
-    for well-formedness), and the payloads are put back as the Data texts.
-    Parsing the megabytes of payload text was most of a mesh read.
+    CDATA) is replaced by a placeholder ``@k@``, the rest of the document -- a
+    few kilobytes -- is parsed by ElementTree (so the document is still
+    checked for well-formedness), and payload ``k`` is returned as bytes for
+    :func:`_payload`.  Parsing the megabytes of payload text was most of a
+    mesh read.
     """
 
     pieces, payloads, at = [], [], 0
@@ -249,12 +247,14 @@ def _parse_root(data: bytes) -> ET.Element:
         start = data.find(b"<Data>", at)
         if start < 0:
             break
-        end = data.find(b"</Data>", start + 6)
+        # the first '<' after the tag ends a payload without markup (a byte search, far
+        # faster than one for the whole closing tag); anything else takes the full parse
+        end = data.find(b"<", start + 6)
         if end < 0:
             break
         payload = data[start + 6:end]
-        if len(payload) < 4096 or not _BASE64_BYTES.issuperset(payload.translate(None, b" \t\r\n")[:4096]) \
-                or b"<" in payload or b"&" in payload:
+        if not data.startswith(b"</Data>", end) or len(payload) < 4096 \
+                or not _BASE64_BYTES.issuperset(payload[:8192].translate(None, b" \t\r\n")[:4096]) or b"&" in payload:
             pieces.append(data[at:end])
             at = end
             continue
@@ -263,13 +263,25 @@ def _parse_root(data: bytes) -> ET.Element:
         payloads.append(payload)
         at = end
     pieces.append(data[at:])
-    root = ET.fromstring(b"".join(pieces))
-    if payloads:
-        for element in root.iter("Data"):
-            text = element.text or ""
-            if text.startswith("@") and text.endswith("@") and text[1:-1].isdigit():
-                element.text = payloads[int(text[1:-1])].decode("ascii")
-    return root
+    return ET.fromstring(b"".join(pieces)), payloads
+
+
+def _payload(element: ET.Element, payloads: list[bytes]) -> bytes:
+    """The encoded text of a DataArray's Data element, as bytes (a cut-out payload or the parsed text)."""
+
+    data = element.find("Data")
+    text = "" if data is None or data.text is None else data.text
+    if payloads and text.startswith("@") and text.endswith("@") and text[1:-1].isdigit():
+        index = int(text[1:-1])
+        if index < len(payloads):
+            return payloads[index]
+    return text.encode("utf-8")
+
+
+def _without_whitespace(payload: bytes) -> bytes:
+    if any(c in payload for c in (b" ", b"\t", b"\r", b"\n")):
+        return payload.translate(None, b" \t\r\n")
+    return payload
 
 
 def read_gifti_arrays(path: str | Path) -> list[tuple[np.ndarray, int]]:
@@ -281,13 +293,13 @@ def read_gifti_arrays(path: str | Path) -> list[tuple[np.ndarray, int]]:
     """
 
     try:
-        root = _parse_root(Path(path).read_bytes())
+        root, payloads = _parse_document(Path(path).read_bytes())
     except ET.ParseError as error:
         raise ValueError(f"Not a GIFTI file (XML: {error}): {path}") from error
     if root.tag != "GIFTI":
         raise ValueError(f"Not a GIFTI file: {path}")
     try:
-        return [_decode_array(item) for item in root.findall("DataArray")]
+        return [_decode_array(item, payloads) for item in root.findall("DataArray")]
     except (zlib.error, KeyError, TypeError) as error:
         raise ValueError(f"Corrupt GIFTI data array ({error}): {path}") from error
     except ValueError as error:
@@ -318,8 +330,8 @@ def read_gifti_mesh(path: str | Path) -> GiftiMesh:
 
 
 def _encode_array(values: np.ndarray, intent: int, dtype_name: str,
-                  stored: tuple[str, list[int] | None] | None = None) -> str:
-    """One DataArray; ``stored`` is a (payload, chunk lengths) pair to write as it is."""
+                  stored: tuple[bytes, list[int] | None] | None = None) -> list[bytes]:
+    """One DataArray, as pieces of the document; ``stored`` is a (payload, chunk lengths) pair to write as it is."""
 
     if stored is None:
         raw = np.ascontiguousarray(values).astype(values.dtype.newbyteorder("<")).tobytes()
@@ -330,7 +342,7 @@ def _encode_array(values: np.ndarray, intent: int, dtype_name: str,
             # per 61k-vertex array), so they go in stored blocks, a zlib stream every reader
             # inflates, at a millisecond each way
             compressed, lengths = _deflate(raw, 0 if values.dtype.kind == "f" else 1)
-            stored = base64.b64encode(compressed).decode("ascii"), lengths
+            stored = base64.b64encode(compressed), lengths
     payload, lengths = stored
     dims = "".join(f' Dim{i}="{size}"' for i, size in enumerate(values.shape))
     intent_name = _INTENT_NAMES.get(intent, "NIFTI_INTENT_NONE")
@@ -343,13 +355,13 @@ def _encode_array(values: np.ndarray, intent: int, dtype_name: str,
             "<MatrixData>1 0 0 0 0 1 0 0 0 0 1 0 0 0 0 1</MatrixData>"
             "</CoordinateSystemTransformMatrix>\n"
         )
-    return (
+    head = (
         f'<DataArray Intent="{intent_name}" DataType="{dtype_name}" '
         f'ArrayIndexingOrder="RowMajorOrder" Dimensionality="{values.ndim}"{dims} '
         'Encoding="GZipBase64Binary" Endian="LittleEndian" ExternalFileName="" ExternalFileOffset="">\n'
-        + _chunk_metadata(lengths) +
-        f"{transform}<Data>{payload}</Data>\n</DataArray>\n"
+        + _chunk_metadata(lengths) + f"{transform}<Data>"
     )
+    return [head.encode("ascii"), payload, b"</Data>\n</DataArray>\n"]
 
 
 def write_gifti_mesh(
@@ -367,17 +379,17 @@ def write_gifti_mesh(
     intents = None
     if reference_path is not None:
         intents = [_INTENT_CODES.get(item.attrib.get("Intent", "NIFTI_INTENT_NONE"), 0)
-                   for item in _data_arrays(reference_path)]
+                   for item in _data_arrays(reference_path)[0]]
     _write_mesh(path, mesh, intents)
 
 
-def _data_arrays(path) -> list[ET.Element]:
-    """The DataArray elements of a GIFTI file, payloads not decoded."""
+def _data_arrays(path) -> tuple[list[ET.Element], list[bytes]]:
+    """The DataArray elements of a GIFTI file and its cut-out payloads, not decoded."""
 
-    root = _parse_root(Path(path).read_bytes())
+    root, payloads = _parse_document(Path(path).read_bytes())
     if root.tag != "GIFTI":
         raise ValueError(f"Not a GIFTI file: {path}")
-    return root.findall("DataArray")
+    return root.findall("DataArray"), payloads
 
 
 def _shape(element: ET.Element) -> tuple[int, ...]:
@@ -385,7 +397,7 @@ def _shape(element: ET.Element) -> tuple[int, ...]:
     return tuple(int(attrs[f"Dim{i}"]) for i in range(int(attrs.get("Dimensionality", "1"))))
 
 
-def _verbatim_faces(element: ET.Element) -> tuple[str, list[int] | None] | None:
+def _verbatim_faces(element: ET.Element, payloads: list[bytes]) -> tuple[bytes, list[int] | None] | None:
     """The payload (and chunk index) of an [m, 3] int32 little-endian row-major gzip face array, as stored."""
 
     attrs = element.attrib
@@ -394,13 +406,13 @@ def _verbatim_faces(element: ET.Element) -> tuple[str, list[int] | None] | None:
             and attrs.get("Endian", "LittleEndian") == "LittleEndian"
             and attrs.get("ArrayIndexingOrder", "RowMajorOrder") == "RowMajorOrder"
             and len(shape) == 2 and shape[1] == 3):
-        data = element.find("Data")
-        if data is not None and data.text:
-            return "".join(data.text.split()), _chunk_lengths(element)
+        payload = _without_whitespace(_payload(element, payloads))
+        if payload:
+            return payload, _chunk_lengths(element)
     return None
 
 
-def _write_mesh(path, mesh: GiftiMesh, intents, faces_payload: tuple[str, list[int] | None] | None = None) -> None:
+def _write_mesh(path, mesh: GiftiMesh, intents, faces_payload: tuple[bytes, list[int] | None] | None = None) -> None:
     point_intent = _INTENT_CODES["NIFTI_INTENT_POINTSET"]
     triangle_intent = _INTENT_CODES["NIFTI_INTENT_TRIANGLE"]
     if intents is not None:
@@ -412,17 +424,17 @@ def _write_mesh(path, mesh: GiftiMesh, intents, faces_payload: tuple[str, list[i
     faces = np.ascontiguousarray(mesh.faces, dtype=np.int32)
     if vertices.ndim != 2 or vertices.shape[1] != 3 or faces.ndim != 2 or faces.shape[1] != 3:
         raise ValueError("GIFTI mesh arrays must have shape [n, 3] and [m, 3]")
-    text = (
-        '<?xml version="1.0" encoding="UTF-8"?>\n'
-        '<!DOCTYPE GIFTI SYSTEM "http://www.nitrc.org/frs/download.php/115/gifti.dtd">\n'
-        '<GIFTI Version="1.0" NumberOfDataArrays="2">\n<MetaData/>\n<LabelTable/>\n'
-        + _encode_array(vertices, point_intent, "NIFTI_TYPE_FLOAT32")
-        + _encode_array(faces, triangle_intent, "NIFTI_TYPE_INT32", faces_payload)
-        + "</GIFTI>\n"
-    )
+    document = b"".join([
+        b'<?xml version="1.0" encoding="UTF-8"?>\n'
+        b'<!DOCTYPE GIFTI SYSTEM "http://www.nitrc.org/frs/download.php/115/gifti.dtd">\n'
+        b'<GIFTI Version="1.0" NumberOfDataArrays="2">\n<MetaData/>\n<LabelTable/>\n',
+        *_encode_array(vertices, point_intent, "NIFTI_TYPE_FLOAT32"),
+        *_encode_array(faces, triangle_intent, "NIFTI_TYPE_INT32", faces_payload),
+        b"</GIFTI>\n",
+    ])
     output = Path(path)
     output.parent.mkdir(parents=True, exist_ok=True)
-    output.write_text(text, encoding="utf-8")
+    output.write_bytes(document)
 
 
 def write_vertices_like(reference_path: str | Path, output_path: str | Path, vertices: np.ndarray) -> None:
@@ -433,17 +445,17 @@ def write_vertices_like(reference_path: str | Path, output_path: str | Path, ver
     ``reference_path`` unchanged, so triangle arrays are exact by construction.
     """
 
-    elements = _data_arrays(reference_path)
+    elements, payloads = _data_arrays(reference_path)
     if len(elements) < 2:
         raise ValueError(f"GIFTI file must contain vertex and face arrays: {reference_path}")
     values = np.ascontiguousarray(vertices, dtype=np.float32)
     if values.shape != _shape(elements[0]):
         raise ValueError(f"vertices shape {values.shape} does not match {_shape(elements[0])}")
     intents = [_INTENT_CODES.get(item.attrib.get("Intent", "NIFTI_INTENT_NONE"), 0) for item in elements]
-    payload = _verbatim_faces(elements[1])
+    payload = _verbatim_faces(elements[1], payloads)
     if payload is not None:
         # the reference's own face payload, copied as stored: the same bytes without re-encoding
         faces = np.empty(_shape(elements[1]), dtype=np.int32)
     else:
-        faces = np.ascontiguousarray(_decode_array(elements[1])[0], dtype=np.int32)
+        faces = np.ascontiguousarray(_decode_array(elements[1], payloads)[0], dtype=np.int32)
     _write_mesh(output_path, GiftiMesh(values, faces), intents, payload)

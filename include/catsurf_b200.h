@@ -38,6 +38,7 @@ typedef struct CUstream_st *csg_stream_t;
 #define CSG_ERR_TOPOLOGY (-5)    /* face indices out of range / not a mesh */
 #define CSG_ERR_UNSUPPORTED (-6) /* option not supported */
 #define CSG_ERR_COVERAGE (-7)    /* a query point found no candidate triangle */
+#define CSG_ERR_FORMAT (-8)      /* a file payload that does not decode */
 
 #define CSG_DTYPE_F32 0 /* DARTEL / warp element type */
 #define CSG_DTYPE_F64 1
@@ -554,6 +555,27 @@ CSG_API int csg_stencil_build_device(const float *sphere, int n_sphere, const in
                                      double *surface_weights_out, int32_t *sheet_indices_out,
                                      double *sheet_weights_out, float *unit_points_out, void *scratch,
                                      size_t scratch_bytes, csg_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * GIFTI payloads (host only; replaces the decode inside nibabel's GIFTI
+ * reader that src/cat_surface_gpu/gpu_pipeline.py:52-71 read_gifti_mesh calls).
+ * ------------------------------------------------------------------------ */
+
+/* Decode one DataArray payload: `text` is its base64 text (whitespace allowed
+ * anywhere, '=' padding only at the end), `gzip` 1 for GZipBase64Binary (a
+ * zlib stream, Adler-32 checked) or 0 for Base64Binary.  `out` receives exactly
+ * `out_bytes` bytes, the array's size from its header; a payload that decodes
+ * to any other size is CSG_ERR_FORMAT, as is bad base64 or a corrupt or
+ * truncated stream.  When `chunk_lengths` [n_chunks] gives the compressed
+ * lengths of a stream deflated in raw chunks of `chunk_bytes` input bytes
+ * (each ended by a sync flush, the last by the final block) and fits the
+ * stream, the chunks inflate on up to 8 threads; an index that does not fit
+ * is ignored and the stream inflates as one.  `adler32_out` (may be null)
+ * receives the Adler-32 of the array's bytes (for a zlib stream, its verified
+ * check value).  Holds no lock and touches no device. */
+CSG_API int csg_gifti_decode(const char *text, size_t text_bytes, int gzip, const long long *chunk_lengths,
+                             int n_chunks, long long chunk_bytes, void *out, size_t out_bytes,
+                             unsigned int *adler32_out);
 
 /* Synchronously read a persistent kernel's status word from its scratch. */
 CSG_API int csg_read_status(const void *scratch, csg_stream_t stream, int *status, int *where);

@@ -69,6 +69,7 @@ OPTIONAL = {
     "csg_dartel_squaring": {"map_out", "jac_out", "scratch_map_out"},
     "csg_depth_potential": {"normals", "areas"},
     "csg_read_status": {"where"},
+    "csg_gifti_decode": {"chunk_lengths", "adler32_out"},
     "csg_rotation_grid_build": {"cell_faces"},
     "csg_rotation_grid_build_device": {"cell_faces"},
     # host builders read the neighbour array only where an offset range is non-empty
@@ -84,7 +85,8 @@ DATA_CHECKED = {"csg_feature_smooth_values", "csg_normalise_sphere", "csg_rotati
 INT_VALUES = {"dtype": 0, "arithmetic": 0, "stop_at": 1, "tile": 256, "solver": 0, "series": 1, "k": 1, "n_levels": 1,
               "level_stride": 1, "iterations": 2, "project_every": 0, "code": 0, "rtype": 1, "checkpoint_every": 1,
               "n_candidates": 1, "n_surfaces": 1, "capacity": 1 << 16, "grid_size": 4, "margin": 1,
-              "threads_per_cta": 0, "lanes_per_vertex": 0, "lanes_per_row": 0, "n_ctas": 0, "max_iter": 1}
+              "threads_per_cta": 0, "lanes_per_vertex": 0, "lanes_per_row": 0, "n_ctas": 0, "max_iter": 1,
+              "gzip": 0}
 
 
 @pytest.mark.skipif(__import__("torch").cuda.is_available(),

@@ -258,15 +258,22 @@ def test_gifti_large_arrays_parallel_deflate_and_payload_reuse(tmp_path):
         z, lengths = gifti._deflate(raw, 1)
         assert zlib.decompress(z) == raw
         assert zlib.decompressobj().decompress(z) == raw
+        text = base64.b64encode(z)
+
+        def native(index):
+            out = np.empty(len(raw), dtype=np.uint8)
+            assert gifti._decode_payload(text, True, index, out) == zlib.adler32(raw)
+            return out.tobytes()
+
         # the chunk index inflates the chunks apart to the same bytes; an index that does not
         # fit the stream falls back to one inflate, and a wrong one fails the check
-        assert gifti._inflate(z, lengths) == raw
+        assert native(lengths) == raw
         assert (lengths is None) == (len(raw) < gifti._PARALLEL_MIN)
         if lengths:
-            assert gifti._inflate(z, lengths[:-1]) == raw
+            assert native(lengths[:-1]) == raw
             bad = [lengths[0] + 1, lengths[1] - 1] + lengths[2:]
-            with pytest.raises(zlib.error):
-                gifti._inflate(z, bad)
+            with pytest.raises(ValueError):
+                native(bad)
     write_gifti_mesh(tmp_path / "a.gii", GiftiMesh(v, f))
     a = read_gifti_mesh(tmp_path / "a.gii")
     np.testing.assert_array_equal(a.vertices, v)
