@@ -212,26 +212,42 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
         slot_tri[4 * s + 2] = t[2];
         slot_tri[4 * s + 3] = inc[s];
     }
-    // Levels over the face 1-ring (the vertices a sweep update reads).
+    // Unique lower and higher face neighbours of every vertex (the vertices a sweep
+    // update reads), as two CSR arrays.  Each face neighbour of v appears in two of its
+    // faces: a per-vertex stamp drops the repeats.  Their order does not matter: every
+    // use below takes a maximum over them.
+    std::vector<int32_t> lo_off(n + 1, 0), hi_off(n + 1, 0);
+    std::vector<int32_t> lo_nb, hi_nb;
+    lo_nb.reserve(static_cast<size_t>(3) * n_faces);
+    hi_nb.reserve(static_cast<size_t>(3) * n_faces);
+    {
+        std::vector<int32_t> stamp(n, -1);
+        for (int v = 0; v < n; ++v) {
+            stamp[v] = v;
+            for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
+                for (int k = 0; k < 3; ++k) {
+                    const int32_t u = slot_tri[4 * s + k];
+                    if (stamp[u] != v) {
+                        stamp[u] = v;
+                        (u < v ? lo_nb : hi_nb).push_back(u);
+                    }
+                }
+            lo_off[v + 1] = static_cast<int32_t>(lo_nb.size());
+            hi_off[v + 1] = static_cast<int32_t>(hi_nb.size());
+        }
+    }
+    // Levels: the longest chain of lower neighbours.
     std::vector<int32_t> levels(n, 0);
     int n_levels = 0;
     for (int v = 0; v < n; ++v) {
         int level = 0;
-        for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
-            for (int k = 0; k < 3; ++k) {
-                int u = slot_tri[4 * s + k];
-                if (u < v) level = std::max(level, levels[u] + 1);
-            }
+        for (int k = lo_off[v]; k < lo_off[v + 1]; ++k) level = std::max(level, levels[lo_nb[k]] + 1);
         levels[v] = level;
         n_levels = std::max(n_levels, level + 1);
     }
     int stride = 1;
     for (int v = 0; v < n; ++v)
-        for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
-            for (int k = 0; k < 3; ++k) {
-                int w = slot_tri[4 * s + k];
-                if (w > v) stride = std::max(stride, levels[w] - levels[v] + 1);
-            }
+        for (int k = hi_off[v]; k < hi_off[v + 1]; ++k) stride = std::max(stride, levels[hi_nb[k]] - levels[v] + 1);
     // Tighten the stride.  Any integer schedule f with 1 <= f(w) - f(v) <= D - 1
     // on every edge v < w runs vertex v of sweep s at step s D + f(v) with the
     // sequential read versions (lower neighbours this sweep, higher ones the
@@ -241,36 +257,8 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
     // (a non-converging relaxation means a positive cycle, or too slow a
     // convergence to be worth it; both keep the last feasible D).
     {
-        // unique lower and higher face neighbours of every vertex, as two CSR arrays
-        std::vector<int32_t> lo_off(n + 1, 0), hi_off(n + 1, 0);
-        std::vector<int32_t> lo_nb, hi_nb;
-        lo_nb.reserve(static_cast<size_t>(3) * n_faces);
-        hi_nb.reserve(static_cast<size_t>(3) * n_faces);
-        {
-            // each face neighbour of v appears in two of its faces: a per-vertex stamp
-            // drops the repeats, and only the few unique neighbours are sorted
-            std::vector<int32_t> ring, stamp(n, -1);
-            for (int v = 0; v < n; ++v) {
-                ring.clear();
-                stamp[v] = v;
-                for (int s = slot_off[v]; s < slot_off[v + 1]; ++s)
-                    for (int k = 0; k < 3; ++k) {
-                        const int32_t u = slot_tri[4 * s + k];
-                        if (stamp[u] != v) {
-                            stamp[u] = v;
-                            ring.push_back(u);
-                        }
-                    }
-                std::sort(ring.begin(), ring.end());
-                for (int32_t u : ring) {
-                    if (u < v) lo_nb.push_back(u);
-                    if (u > v) hi_nb.push_back(u);
-                }
-                lo_off[v + 1] = static_cast<int32_t>(lo_nb.size());
-                hi_off[v + 1] = static_cast<int32_t>(hi_nb.size());
-            }
-        }
         std::vector<int32_t> best = levels, f;
+        std::vector<uint8_t> fwd_dirty(n), bwd_dirty(n);
         int last_iterations = 64;
         for (int trial = stride - 1; trial >= 2; --trial) {
             f = best;
@@ -282,6 +270,15 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
             const int cap = std::min(4000, last_iterations + 8);
             bool converged = false;
             int it = 0;
+            // Gauss-Seidel passes over a worklist: a vertex is evaluated only when a
+            // neighbour its constraint reads changed since its last evaluation in that
+            // pass direction (a clean vertex would keep its value), so every pass ends
+            // with the values a full pass gives and the iteration counts are the same.
+            // A forward pass only marks higher vertices (still ahead of it) and a
+            // backward pass lower ones.  Byte flags measured faster than bitmaps scanned
+            // by word (34 vs 38 ms on the 61k hull), and both than full passes (39 ms).
+            std::fill(fwd_dirty.begin(), fwd_dirty.end(), 1);
+            std::fill(bwd_dirty.begin(), bwd_dirty.end(), 1);
             for (; it < cap && !converged; ++it) {
                 // In the forward pass no lower neighbour of v changes while v is
                 // processed (and no higher one in the backward pass), so taking the
@@ -290,16 +287,26 @@ int csg_areal_plan_build(int n_vertices, const int32_t* faces, int n_faces, int3
                 bool changed = false;
                 int32_t* fv = f.data();
                 for (int v = 0; v < n; ++v) {  // f(v) >= f(u) + 1 for lower neighbours u
+                    if (!fwd_dirty[v]) continue;
+                    fwd_dirty[v] = 0;
                     int32_t need = fv[v];
                     for (int k = lo_off[v]; k < lo_off[v + 1]; ++k) need = std::max(need, fv[lo_nb[k]] + 1);
-                    changed |= need != fv[v];
+                    if (need == fv[v]) continue;
                     fv[v] = need;
+                    changed = true;
+                    for (int k = hi_off[v]; k < hi_off[v + 1]; ++k) fwd_dirty[hi_nb[k]] = 1;  // later this pass
+                    for (int k = lo_off[v]; k < lo_off[v + 1]; ++k) bwd_dirty[lo_nb[k]] = 1;
                 }
                 for (int v = n - 1; v >= 0; --v) {  // f(v) >= f(w) - (D - 1) for higher neighbours w
+                    if (!bwd_dirty[v]) continue;
+                    bwd_dirty[v] = 0;
                     int32_t need = fv[v];
                     for (int k = hi_off[v]; k < hi_off[v + 1]; ++k) need = std::max(need, fv[hi_nb[k]] - (trial - 1));
-                    changed |= need != fv[v];
+                    if (need == fv[v]) continue;
                     fv[v] = need;
+                    changed = true;
+                    for (int k = lo_off[v]; k < lo_off[v + 1]; ++k) bwd_dirty[lo_nb[k]] = 1;  // later this pass
+                    for (int k = hi_off[v]; k < hi_off[v + 1]; ++k) fwd_dirty[hi_nb[k]] = 1;
                 }
                 converged = !changed;
             }
