@@ -371,9 +371,20 @@ __global__ void k_rotation_finalize(const RotSurface* __restrict__ surfaces, int
     const RotSurface& S = surfaces[s];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= S.n_candidates) return;
+    // the partials in tile order, loaded kAhead at a time before they are added (the
+    // additions stay in that order; the loads no longer wait on one another)
+    constexpr int kAhead = 32;
     double total = 0.0;
     const double* p = S.partials + static_cast<long long>(c) * S.tiles;
-    for (int t = 0; t < S.tiles; ++t) total += p[t];
+    int t = 0;
+    for (; t + kAhead <= S.tiles; t += kAhead) {
+        double part[kAhead];
+#pragma unroll
+        for (int j = 0; j < kAhead; ++j) part[j] = p[t + j];
+#pragma unroll
+        for (int j = 0; j < kAhead; ++j) total += part[j];
+    }
+    for (; t < S.tiles; ++t) total += p[t];
     costs[cost_offsets[s] + c] = total;
 }
 
