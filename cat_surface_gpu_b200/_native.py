@@ -22,6 +22,7 @@ CSG_ERR_TOPOLOGY = -5
 CSG_ERR_UNSUPPORTED = -6
 CSG_ERR_COVERAGE = -7
 CSG_ERR_FORMAT = -8
+CSG_ROTATION_HOST_MAX_CANDIDATES = 31
 
 ARITH = {"cat": 0, "fp32": 1, "fp64": 2}
 CSG_DTYPE_F32 = 0
@@ -90,6 +91,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "csg_rotation_cost_batch": (_I, [_I, _P, _P, _I, _I, _P, c_size_t, _P]),
     "csg_rotation_triangle_records": (_I, [_P, _I, _P, _P]),
     "csg_rotation_status_offset": (c_size_t, [_I]),
+    "csg_rotation_cost_host": (_I, [_P, _P, _P, _P, _I, _P, c_size_t, _P]),
     "csg_rotation_status": (_I, [_P, _I, _P, _P]),
     "csg_feature_resample": (_I, [_I, _I, _P, _P, _P, _P, _P]),
     "csg_feature_sheet_map": (_I, [_I, _P, _P, _P, _P, _P]),

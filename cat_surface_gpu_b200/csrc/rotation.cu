@@ -48,6 +48,14 @@ struct RotSurface {
     long long item_begin;        // first flat work item of this surface
 };
 
+// Up to kInlineSurfaces surfaces travel to the kernels as a launch parameter (no host-to-device
+// copy per call); more are read from the scratch copy.
+constexpr int kInlineSurfaces = 4;
+struct SurfaceTable {
+    RotSurface s[kInlineSurfaces];
+    long long cost_off[kInlineSurfaces];
+};
+
 __device__ __forceinline__ float dot3(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
 
 __device__ __forceinline__ void cross3(const float* a, const float* b, float* out) {
@@ -241,9 +249,11 @@ __device__ __forceinline__ void barycentric(const float* point, const float* t, 
 }
 
 template <int TILE>
-__global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __restrict__ surfaces, int n_surfaces,
+__global__ void __launch_bounds__(TILE) k_rotation_cost(const __grid_constant__ SurfaceTable table,
+                                                        const RotSurface* __restrict__ many, int n_surfaces,
                                                         long long n_items, int* __restrict__ error) {
     __shared__ double red[TILE / 32];
+    const RotSurface* surfaces = n_surfaces <= kInlineSurfaces ? table.s : many;
     for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
         // locate the surface of this item (few surfaces: linear scan)
         int s = 0;
@@ -364,10 +374,13 @@ __global__ void __launch_bounds__(TILE) k_rotation_cost(const RotSurface* __rest
     }
 }
 
-__global__ void k_rotation_finalize(const RotSurface* __restrict__ surfaces, int n_surfaces, double* __restrict__ costs,
-                                    const long long* __restrict__ cost_offsets) {
+__global__ void k_rotation_finalize(const __grid_constant__ SurfaceTable table, const RotSurface* __restrict__ many,
+                                    int n_surfaces, double* __restrict__ costs, const long long* __restrict__ many_offsets) {
     const int s = blockIdx.y;
     if (s >= n_surfaces) return;
+    const bool inline_table = n_surfaces <= kInlineSurfaces;
+    const RotSurface* surfaces = inline_table ? table.s : many;
+    const long long* cost_offsets = inline_table ? table.cost_off : many_offsets;
     const RotSurface& S = surfaces[s];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= S.n_candidates) return;
@@ -610,8 +623,16 @@ int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces
         max_c = std::max(max_c, r.n_candidates);
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    CSG_CUDA_CHECK(cudaMemcpyAsync(d_surf, host.data(), sizeof(RotSurface) * n_surfaces, cudaMemcpyHostToDevice, st));
-    CSG_CUDA_CHECK(cudaMemcpyAsync(d_off, cost_off.data(), sizeof(long long) * n_surfaces, cudaMemcpyHostToDevice, st));
+    SurfaceTable table{};
+    if (n_surfaces <= kInlineSurfaces) {
+        for (int s = 0; s < n_surfaces; ++s) {
+            table.s[s] = host[s];
+            table.cost_off[s] = cost_off[s];
+        }
+    } else {
+        CSG_CUDA_CHECK(cudaMemcpyAsync(d_surf, host.data(), sizeof(RotSurface) * n_surfaces, cudaMemcpyHostToDevice, st));
+        CSG_CUDA_CHECK(cudaMemcpyAsync(d_off, cost_off.data(), sizeof(long long) * n_surfaces, cudaMemcpyHostToDevice, st));
+    }
     CSG_CUDA_CHECK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     int device = 0, sms = 0;
     CSG_CUDA_CHECK(cudaGetDevice(&device));
@@ -619,11 +640,11 @@ int csg_rotation_cost_batch(int n_surfaces, const csg_rotation_surface* surfaces
     const long long want = n_ctas > 0 ? n_ctas : static_cast<long long>(sms) * (2048 / tile);
     const unsigned blocks = static_cast<unsigned>(std::min<long long>(std::max<long long>(1, want), items));
     switch (tile) {
-        case 128: (csg::note_launch(), k_rotation_cost<128><<<blocks, 128, 0, st>>>(d_surf, n_surfaces, items, d_err)); break;
-        case 512: (csg::note_launch(), k_rotation_cost<512><<<blocks, 512, 0, st>>>(d_surf, n_surfaces, items, d_err)); break;
-        default: (csg::note_launch(), k_rotation_cost<256><<<blocks, 256, 0, st>>>(d_surf, n_surfaces, items, d_err)); break;
+        case 128: (csg::note_launch(), k_rotation_cost<128><<<blocks, 128, 0, st>>>(table, d_surf, n_surfaces, items, d_err)); break;
+        case 512: (csg::note_launch(), k_rotation_cost<512><<<blocks, 512, 0, st>>>(table, d_surf, n_surfaces, items, d_err)); break;
+        default: (csg::note_launch(), k_rotation_cost<256><<<blocks, 256, 0, st>>>(table, d_surf, n_surfaces, items, d_err)); break;
     }
-    (csg::note_launch(), k_rotation_finalize<<<dim3((max_c + 127) / 128, n_surfaces), 128, 0, st>>>(d_surf, n_surfaces, costs, d_off));
+    (csg::note_launch(), k_rotation_finalize<<<dim3((max_c + 127) / 128, n_surfaces), 128, 0, st>>>(table, d_surf, n_surfaces, costs, d_off));
     CSG_CUDA_CHECK(cudaGetLastError());
     return CSG_OK;
 }
@@ -690,6 +711,31 @@ int csg_rotation_status(const void* scratch, int n_surfaces, csg_stream_t stream
     const size_t off = align256(sizeof(RotSurface) * n_surfaces) + align256(sizeof(long long) * n_surfaces);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     CSG_CUDA_CHECK(cudaMemcpyAsync(status, static_cast<const char*>(scratch) + off, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CSG_CUDA_CHECK(cudaStreamSynchronize(st));
+    return CSG_OK;
+}
+
+int csg_rotation_cost_host(const csg_rotation_surface* surface, const float* matrices_host, float* matrices_device,
+                           void* readback_host, int tile, void* scratch, size_t scratch_bytes, csg_stream_t stream) {
+    if (!surface || !matrices_host || !matrices_device || !readback_host || !scratch)
+        return csg::fail(CSG_ERR_ARG, "rotation cost (host): bad arguments");
+    const int count = surface->n_candidates;
+    if (count < 1 || count > CSG_ROTATION_HOST_MAX_CANDIDATES)
+        return csg::fail(CSG_ERR_ARG, "rotation cost (host): %d candidates (1 to %d; use csg_rotation_cost_batch)",
+                         count, CSG_ROTATION_HOST_MAX_CANDIDATES);
+    // the status word's 256-byte slot in the scratch holds the costs behind it, so one
+    // copy brings both back
+    char* slot = static_cast<char*>(scratch) + csg_rotation_status_offset(1);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    csg_rotation_surface local = *surface;
+    local.matrices = matrices_device;
+    CSG_CUDA_CHECK(cudaMemcpyAsync(matrices_device, matrices_host, sizeof(float) * 9 * static_cast<size_t>(count),
+                                   cudaMemcpyHostToDevice, st));
+    const int rc = csg_rotation_cost_batch(1, &local, reinterpret_cast<double*>(slot + 8), tile, 0, scratch,
+                                           scratch_bytes, stream);
+    if (rc) return rc;
+    CSG_CUDA_CHECK(cudaMemcpyAsync(readback_host, slot, 8 + sizeof(double) * static_cast<size_t>(count),
+                                   cudaMemcpyDeviceToHost, st));
     CSG_CUDA_CHECK(cudaStreamSynchronize(st));
     return CSG_OK;
 }

@@ -219,6 +219,18 @@ class _Costing:
         offset = int(_native.library().csg_rotation_status_offset(1))
         self.status_device = self.scratch[offset:offset + 4].view(torch.int32)
         self.status_host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        # host-driven evaluations (csg_rotation_cost_host): one page-locked block for the
+        # status and the costs, and the surface description built once
+        self.readback = torch.zeros(8 + 8 * _native.CSG_ROTATION_HOST_MAX_CANDIDATES, dtype=torch.uint8,
+                                    pin_memory=True)
+        self.readback_host = self.readback.numpy()
+        self.surface = _native.RotationSurface(
+            inputs.source_points.data_ptr(), inputs.source_values.data_ptr(), index.target_triangles.data_ptr(),
+            index.target_faces.data_ptr(), inputs.target_values.data_ptr(), index.candidate_offsets.data_ptr(),
+            index.candidate_faces.data_ptr(), self.matrices.data_ptr(), int(inputs.source_points.shape[0]),
+            int(index.grid_size), 1, int(inputs.n_features), int(index.target_points.shape[0]),
+            index.target_records.data_ptr(),
+        )
 
     def evaluate(self, angles: np.ndarray, *, host: bool = False):
         """Costs of these candidates: a device tensor, or (``host``) a NumPy copy read back in the
@@ -228,6 +240,21 @@ class _Costing:
         count = mats.shape[0]
         if count > self.capacity:
             raise ValueError("more candidates than this costing context holds")
+        if host and count <= _native.CSG_ROTATION_HOST_MAX_CANDIDATES:
+            # one native call: upload from the staging rows, the cost launches, one readback, synchronise
+            np.copyto(self.staging_host[:count], mats)
+            self.surface.n_candidates = count
+            lib = _native.library()
+            _native.check(
+                lib.csg_rotation_cost_host(ctypes.addressof(self.surface), self.staging.data_ptr(),
+                                           self.matrices.data_ptr(), self.readback.data_ptr(), self.tile,
+                                           self.scratch.data_ptr(), self.scratch.numel(),
+                                           _native.stream_handle(like=self.costs)),
+                "csg_rotation_cost_host",
+            )
+            if int(self.readback_host[:4].view(np.int32)[0]) != 0:
+                raise RuntimeError("Rotation is not covered by target sphere candidate index")
+            return self.readback_host[8:8 + 8 * count].view(np.float64).copy()
         # page-locked staging: an asynchronous upload (the previous call's status read has
         # synchronised, so the staging rows are free)
         np.copyto(self.staging_host[:count], mats)

@@ -464,6 +464,22 @@ CSG_API size_t csg_rotation_status_offset(int n_surfaces);
  * that used this scratch (CSG_OK or CSG_ERR_COVERAGE). */
 CSG_API int csg_rotation_status(const void *scratch, int n_surfaces, csg_stream_t stream, int *status);
 
+/* One surface's costs for a few candidates whose matrices are in host memory,
+ * for searches that decide on the host between evaluations (the reference's
+ * Nelder-Mead loop calls cost_batch_prepared once per decision,
+ * src/cat_surface_gpu/surface_rotation.py:650-699).  Copies the
+ * surface->n_candidates (1 .. CSG_ROTATION_HOST_MAX_CANDIDATES) float32
+ * matrices from `matrices_host` (page-locked for an asynchronous copy) to
+ * `matrices_device`, which replaces surface->matrices, runs
+ * csg_rotation_cost_batch (one surface; scratch sized by
+ * csg_rotation_scratch_bytes), copies the coverage status (int32 at byte 0)
+ * and the float64 costs (from byte 8) to `readback_host`
+ * (8 + 8 * n_candidates bytes) and synchronises `stream`. */
+#define CSG_ROTATION_HOST_MAX_CANDIDATES 31
+CSG_API int csg_rotation_cost_host(const csg_rotation_surface *surface, const float *matrices_host,
+                                   float *matrices_device, void *readback_host, int tile, void *scratch,
+                                   size_t scratch_bytes, csg_stream_t stream);
+
 /* ------------------------------------------------------------------------
  * SurfWarp: stencil feature operators (device).
  * Replace SurfaceStencilDevice's operators

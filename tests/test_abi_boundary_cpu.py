@@ -80,7 +80,7 @@ OPTIONAL = {
 # Entry points whose other arguments, zero-filled, already fail a data check
 # (zero sphere points, an empty surface record): one-at-a-time says nothing there.
 DATA_CHECKED = {"csg_feature_smooth_values", "csg_normalise_sphere", "csg_rotation_cost_batch", "csg_stencil_build",
-                "csg_stencil_build_device"}
+                "csg_stencil_build_device", "csg_rotation_cost_host"}
 # Small valid values for integer parameters (by name); others are 8.
 INT_VALUES = {"dtype": 0, "arithmetic": 0, "stop_at": 1, "tile": 256, "solver": 0, "series": 1, "k": 1, "n_levels": 1,
               "level_stride": 1, "iterations": 2, "project_every": 0, "code": 0, "rtype": 1, "checkpoint_every": 1,

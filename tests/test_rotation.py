@@ -266,3 +266,21 @@ def test_triangle_records_give_the_same_costs(native_library):
     records = index.target_records.cpu().numpy()
     tri = index.target_triangles.reshape(-1, 9).cpu().numpy()
     assert np.array_equal(records[:, :9], tri)
+
+
+@pytest.mark.gpu
+def test_host_driven_evaluations_equal_the_batched_costs(device_index):
+    """csg_rotation_cost_host (the Nelder-Mead evaluations: matrices from page-locked host memory,
+    status and costs back in one copy) gives the batched device path's costs bit for bit, for 1 to
+    31 candidates, and the batched path takes over above that."""
+
+    inputs = device_index.prepare_cost_inputs(R["source_points"], R["source_values"], R["target_values"])
+    costing = device_index._costing(inputs, 64)
+    rng = np.random.default_rng(21)
+    for count in (1, 3, 4, 31, 32, 40):
+        angles = rng.uniform(-0.8, 0.8, size=(count, 3))
+        host = costing.evaluate(angles, host=True)
+        device = costing.evaluate(angles).cpu().numpy()
+        assert host.shape == (count,)
+        np.testing.assert_array_equal(host, device)
+        np.testing.assert_allclose(host, _oracle_cost(angles), rtol=1e-12)
