@@ -8,6 +8,7 @@ edge length to derive the heat-kernel iteration count (``_heat_parameters``).
 
 from __future__ import annotations
 
+from collections import OrderedDict
 import math
 
 import numpy as np
@@ -16,9 +17,27 @@ import torch
 from . import _native
 from .surface_stencil import SurfaceStencil, SurfaceStencilDevice
 
-_TOPOLOGY_CACHE: dict[tuple, tuple[torch.Tensor, ...]] = {}
-_TOPOLOGY_BY_ID: dict[tuple, tuple] = {}
-_FACES_BY_ID: dict[tuple, tuple] = {}
+# Device topology tables of the meshes used most recently, as least-recently-used caches of a
+# few entries: a batch of many subjects keeps only the shared resampling sphere's tables and
+# the last few subjects' instead of every mesh it has seen.
+_CACHE_ENTRIES = 8
+_TOPOLOGY_CACHE: OrderedDict = OrderedDict()
+_TOPOLOGY_BY_ID: OrderedDict = OrderedDict()
+_FACES_BY_ID: OrderedDict = OrderedDict()
+
+
+def _cache_get(cache: OrderedDict, key):
+    hit = cache.get(key)
+    if hit is not None:
+        cache.move_to_end(key)
+    return hit
+
+
+def _cache_put(cache: OrderedDict, key, value) -> None:
+    cache[key] = value
+    cache.move_to_end(key)
+    while len(cache) > _CACHE_ENTRIES:
+        cache.popitem(last=False)
 
 
 def _shared_faces(faces) -> bool:
@@ -40,15 +59,15 @@ def _stable_order(keys: np.ndarray, n_keys: int) -> np.ndarray:
 def _topology(faces: np.ndarray, n_points: int, device: torch.device):
     ident = (id(faces), n_points, device.type, device.index) if _shared_faces(faces) else None
     if ident is not None:
-        hit = _TOPOLOGY_BY_ID.get(ident)
+        hit = _cache_get(_TOPOLOGY_BY_ID, ident)
         if hit is not None and hit[0] is faces:
             return hit[1]
     f = np.ascontiguousarray(faces, dtype=np.int32)
     key = (device.type, device.index, f.shape, n_points, f.tobytes())
-    cached = _TOPOLOGY_CACHE.get(key)
+    cached = _cache_get(_TOPOLOGY_CACHE, key)
     if cached is not None:
         if ident is not None:
-            _TOPOLOGY_BY_ID[ident] = (faces, cached)
+            _cache_put(_TOPOLOGY_BY_ID, ident, (faces, cached))
         return cached
     lib = _native.library()
     off = np.zeros(n_points + 1, dtype=np.int32)
@@ -67,9 +86,9 @@ def _topology(faces: np.ndarray, n_points: int, device: torch.device):
     tensors = tuple(torch.from_numpy(a).to(device) for a in (off, nbr, inc_off, inc))
     max_degree = int(np.diff(off).max()) if n_points else 0
     cached = tensors + (max_degree,)
-    _TOPOLOGY_CACHE[key] = cached
+    _cache_put(_TOPOLOGY_CACHE, key, cached)
     if ident is not None:
-        _TOPOLOGY_BY_ID[ident] = (faces, cached)
+        _cache_put(_TOPOLOGY_BY_ID, ident, (faces, cached))
     return cached
 
 
@@ -78,11 +97,11 @@ def _device_faces(faces, device: torch.device) -> torch.Tensor:
 
     if _shared_faces(faces):
         ident = (id(faces), device.type, device.index)
-        hit = _FACES_BY_ID.get(ident)
+        hit = _cache_get(_FACES_BY_ID, ident)
         if hit is not None and hit[0] is faces:
             return hit[1]
         tensor = torch.from_numpy(faces.copy()).to(device)
-        _FACES_BY_ID[ident] = (faces, tensor)
+        _cache_put(_FACES_BY_ID, ident, (faces, tensor))
         return tensor
     return torch.as_tensor(np.ascontiguousarray(faces, dtype=np.int32), device=device).contiguous()
 

@@ -357,3 +357,25 @@ def test_gifti_reader_handles_wrapped_and_marked_up_payloads(tmp_path):
         mesh = read_gifti_mesh(tmp_path / name)
         np.testing.assert_array_equal(mesh.vertices, np.asarray(vertices, dtype=np.float32))
         np.testing.assert_array_equal(mesh.faces, np.asarray(faces, dtype=np.int32))
+
+
+def test_topology_caches_stay_bounded(native_library):
+    """Many distinct meshes keep only the most recently used topology tables."""
+
+    import torch
+
+    from cat_surface_gpu_b200 import features, synthetic
+
+    device = torch.device("cpu")
+    first = None
+    for seed in range(3 * features._CACHE_ENTRIES):
+        vertices, faces = synthetic.folded_icosphere(1, seed=seed)
+        faces = np.ascontiguousarray(faces, dtype=np.int32)[np.random.default_rng(seed).permutation(len(faces))]
+        tables = features._topology(faces, vertices.shape[0], device)
+        first = first if first is not None else (faces, tables)
+        assert len(features._TOPOLOGY_CACHE) <= features._CACHE_ENTRIES
+    again = features._topology(faces, vertices.shape[0], device)
+    assert again is tables  # the latest mesh is still cached
+    rebuilt = features._topology(first[0], vertices.shape[0], device)
+    for a, b in zip(rebuilt[:4], first[1][:4]):  # the first one was evicted and is rebuilt the same
+        assert torch.equal(a, b)
