@@ -17,10 +17,10 @@ import torch
 from . import _native
 from .surface_stencil import SurfaceStencil, SurfaceStencilDevice
 
-# Device topology tables of the meshes used most recently, as least-recently-used caches of a
-# few entries: a batch of many subjects keeps only the shared resampling sphere's tables and
-# the last few subjects' instead of every mesh it has seen.
-_CACHE_ENTRIES = 8
+# Device topology tables of the meshes used most recently, as least-recently-used caches: a
+# stream of many subjects keeps the shared resampling sphere's tables and the last 32 meshes'
+# (a batch of 16 subjects and its template fit) instead of every mesh it has seen.
+_CACHE_ENTRIES = 32
 _TOPOLOGY_CACHE: OrderedDict = OrderedDict()
 _TOPOLOGY_BY_ID: OrderedDict = OrderedDict()
 _FACES_BY_ID: OrderedDict = OrderedDict()
