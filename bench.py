@@ -86,8 +86,8 @@ def parse_args(argv: list[str] | None = None):
     parser.add_argument("--profile", action="store_true",
                         help="for profilers: --warmup then --steps hemispheres with the default sweep launch shape, "
                              "no parity, e2e, CPU or batched legs; prints the step times only")
-    parser.add_argument("--case", choices=("sweeps", "preprocess", "dartel", "rotation", "depth", "features",
-                                           "stencil", "warp"),
+    parser.add_argument("--case", choices=("sweeps", "preprocess", "dartel", "rotation", "rotation-nm", "depth",
+                                           "features", "stencil", "warp"),
                         help="for kernel profilers: run one small case of one kernel family three times "
                              "(the third run is the one to capture) and exit")
     return parser.parse_args(argv)
@@ -173,6 +173,28 @@ def run_case(name: str) -> int:
                                 False)
             else:
                 apply_flow_to_stenciled_sphere(current, flow, st, inverse=True, device=device, dtype=torch.float64)
+        torch.cuda.synchronize()
+    elif name == "rotation-nm":
+        # Nelder-Mead-sized evaluations (csg_rotation_cost_host): 3 candidates of the source hemisphere's
+        # 40,962 stencil points against the target's rotation index, five evaluations per run
+        from cat_surface_gpu_b200.gpu_pipeline import normalise_sphere
+        from cat_surface_gpu_b200.surface_rotation import RotationGridIndexDevice
+        from cat_surface_gpu_b200.surface_stencil import build_surface_stencil
+
+        nx, ny = SHEET
+        src = build_surface_stencil(normalise_sphere(meshes["binary_sphere"]), meshes["faces"], nx=nx, ny=ny,
+                                    normalize=False, device=device)
+        tgt = build_surface_stencil(normalise_sphere(meshes["target_sphere"]), meshes["target_faces"], nx=nx,
+                                    ny=ny, normalize=False, device=device)
+        index = RotationGridIndexDevice.build(tgt.sphere_points, tgt.faces, device=device)
+        rng = np.random.default_rng(1)
+        inputs = index.prepare_cost_inputs(src.sphere_points.astype(np.float32),
+                                           rng.normal(size=src.sphere_points.shape[0]),
+                                           rng.normal(size=tgt.sphere_points.shape[0]))
+        costing = index._costing(inputs, 64)
+        for _ in range(3):
+            for _ in range(5):
+                costing.evaluate(rng.uniform(-0.3, 0.3, size=(3, 3)), host=True)
         torch.cuda.synchronize()
     else:
         # 256 quaternion candidates on one 102,400-point surface against the resampling sphere
