@@ -335,7 +335,9 @@ class RotationGridIndexDevice:
         from .features import _device_faces
 
         lib = _native.library()
-        d_pts = torch.from_numpy(pts).to(target)
+        # torch.from_numpy refuses to wrap a read-only array without a warning; the upload
+        # only reads it, but a caller's read-only view (np.load mmap, a frozen golden) gets a copy
+        d_pts = torch.from_numpy(pts if pts.flags.writeable else pts.copy()).to(target)
         d_faces = _device_faces(tri, target)
         offsets = torch.empty(grid_size ** 3 + 1, dtype=torch.int32, device=target)
         scratch = torch.empty(int(lib.csg_rotation_grid_scratch_bytes(grid_size)), dtype=torch.uint8, device=target)
